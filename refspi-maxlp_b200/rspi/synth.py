@@ -1,0 +1,185 @@
+"""Seeded synthetic holographic SPI data in the reference's photon layout.
+
+The generative model (per frame d):
+
+* sample: a real, positive 2-D density of ``n_blobs`` Gaussian blobs
+  (sigma ~ U(1,3) px, amplitude ~ U(0.5,1), centres uniform in a disc of
+  radius ``obj_radius`` px about ``size//2``), Fourier transformed with the
+  ``fftshift(fftn(ifftshift(.)))`` convention (make_data.py:283);
+* reference: a uniform sphere, ``rel * ff(pi*r*dia/size) * exp(2*pi*i*((x-c)*sx + (y-c)*sy)/size)``
+  with ``ff(s) = (sin s - s cos s)/s^3`` exactly as slice_gen_holo builds it
+  (kernels.cu:58-71); ``rel`` is set so that the mean |F_ref|^2 over the
+  likelihood annulus equals the mean |F_sample|^2 there;
+* per frame: diameter ~ U(dia_lo, dia_hi), shift ~ U(-shift_max, shift_max)^2,
+  in-plane angle ~ U(0, 2 pi), fluence scale ~ lognormal(0, fluence_sigma);
+* intensity ``|F_sample + F_ref|^2``, detector mask (r < 4 and r >= size//2
+  set to 0, make_data.py:216-219), one global factor so the mean expected
+  photon count is ``mean_count``, times the frame's scale, rotated with the
+  bilinear ``slice_gen`` convention (kernels.cu:19-33), Poisson-sampled and
+  stored as ``ones`` / ``multi`` lists (make_data.py:323-328).
+
+Heavy per-frame work runs in torch on the requested device; the per-frame
+parameters come from ``numpy.random.default_rng(seed)`` child streams.
+"""
+import numpy as np
+import torch
+
+CONFIGS = {
+    # small plain-method case: 101x101, 1,000 frames, 500 photons/frame
+    1: dict(size=101, n_blobs=20, obj_radius=12., num_data=1000, mean_count=500.,
+            fluence_sigma=0.3, dia=(6., 8.), shift_max=3.,
+            recon=dict(num_rot=180, shiftx='-3 3 7', shifty='-3 3 7',
+                       sphere_dia='6 8 5', num_iter=10)),
+    # production shape: 185x185, 20,000 frames, 2,000 photons/frame
+    2: dict(size=185, n_blobs=40, obj_radius=20., num_data=20000, mean_count=2000.,
+            fluence_sigma=0.5, dia=(6., 8.), shift_max=3.,
+            recon=dict(num_rot=180, shiftx='-4 4 9', shifty='-4 4 9',
+                       sphere_dia='6 8 5', num_iter=20)),
+}
+
+
+def make_object(size, n_blobs, obj_radius, rng):
+    """Real positive density of Gaussian blobs centred on ``size//2``."""
+    x, y = np.indices((size, size), dtype='f8')
+    c = size // 2
+    obj = np.zeros((size, size))
+    for _ in range(n_blobs):
+        r = obj_radius * np.sqrt(rng.random())
+        phi = 2 * np.pi * rng.random()
+        cx, cy = c + r * np.cos(phi), c + r * np.sin(phi)
+        sig = rng.uniform(1., 3.)
+        amp = rng.uniform(0.5, 1.)
+        obj += amp * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * sig ** 2))
+    return obj
+
+
+def fourier(obj):
+    return np.fft.fftshift(np.fft.fftn(np.fft.ifftshift(obj)))
+
+
+def _sphere_ff(size, dia, device):
+    """ff(pi*r*dia/size) per pixel (kernels.cu:66-69), dia: (B,) tensor."""
+    x = torch.arange(size, dtype=torch.float64, device=device)
+    cen = float(np.floor(size / 2.))
+    dx = (x - cen)[:, None].expand(size, size).reshape(-1)
+    dy = (x - cen)[None, :].expand(size, size).reshape(-1)
+    r = torch.sqrt(dx * dx + dy * dy)
+    s = r[None, :] * np.pi * dia[:, None] / size
+    s = torch.where(s == 0, torch.full_like(s, 1e-5), s)
+    return (torch.sin(s) - s * torch.cos(s)) / (s * s * s), dx, dy
+
+
+def _rotate_bilinear(img, angle, size):
+    """``slice_gen`` (no log): view[t] = bilinear(img)(R(angle)(t-c)+c), 0 outside."""
+    b = img.shape[0]
+    dev = img.device
+    x = torch.arange(size, device=dev, dtype=torch.float64)
+    cen = size // 2
+    xc = (x - cen)[:, None].expand(size, size).reshape(-1)
+    yc = (x - cen)[None, :].expand(size, size).reshape(-1)
+    ac, as_ = torch.cos(angle)[:, None], torch.sin(angle)[:, None]
+    tx = xc[None] * ac - yc[None] * as_ + cen
+    ty = xc[None] * as_ + yc[None] * ac + cen
+    ix, iy = torch.floor(tx), torch.floor(ty)
+    valid = (ix >= 0) & (ix <= size - 2) & (iy >= 0) & (iy <= size - 2)
+    fx, fy = tx - ix, ty - iy
+    ix = torch.where(valid, ix, torch.zeros_like(ix)).long()
+    iy = torch.where(valid, iy, torch.zeros_like(iy)).long()
+    g = lambda a, c: torch.gather(img, 1, a * size + c)  # noqa: E731
+    out = (g(ix, iy) * (1 - fx) * (1 - fy) + g(ix + 1, iy) * fx * (1 - fy) +
+           g(ix, iy + 1) * (1 - fx) * fy + g(ix + 1, iy + 1) * fx * fy)
+    return torch.where(valid, out, torch.zeros_like(out)).reshape(b, -1)
+
+
+def generate(size, num_data, mean_count, n_blobs=20, obj_radius=12.,
+             fluence_sigma=0.3, dia=(6., 8.), shift_max=3., seed=0,
+             device='cpu', chunk=256, dense=False):
+    """Generate one dataset; returns a dict in the photons-file layout.
+
+    Keys: ``num_pix``, ``ones``, ``multi`` (int32, N), ``place_ones``,
+    ``place_multi``, ``count_multi`` (flat int32; per-frame lengths are
+    ``ones``/``multi``), truth ``true_angles``, ``true_shifts``,
+    ``true_diameters``, ``scale``, ``solution``, and ``fsample``/``rel_scale``.
+    With ``dense=True`` a dense uint16 ``frames`` (N, size^2) is added.
+    """
+    ss = np.random.SeedSequence(seed)
+    r_obj, r_par, r_poi = [np.random.default_rng(s) for s in ss.spawn(3)]
+    obj = make_object(size, n_blobs, obj_radius, r_obj)
+    fs = fourier(obj).ravel()
+
+    diam = r_par.uniform(dia[0], dia[1], num_data)
+    shifts = r_par.uniform(-shift_max, shift_max, (num_data, 2))
+    angles = r_par.uniform(0., 2 * np.pi, num_data)
+    scale = r_par.lognormal(0., fluence_sigma, num_data)
+
+    dev = torch.device(device)
+    fs_t = torch.from_numpy(fs).to(dev)
+    x = torch.arange(size, dtype=torch.float64, device=dev)
+    cen = size // 2
+    pr = torch.sqrt(((x - cen)[:, None] ** 2 + (x - cen)[None, :] ** 2)).reshape(-1)
+    detmask = ((pr >= 4) & (pr < cen)).double()
+    llmask = (pr >= max(size // 8, 4)) & (pr < size // 2)
+
+    ff0, dx, dy = _sphere_ff(size, torch.tensor([0.5 * (dia[0] + dia[1])], device=dev,
+                                                dtype=torch.float64), dev)
+    rel = float(torch.sqrt((fs_t.abs() ** 2)[llmask].mean() / (ff0[0] ** 2)[llmask].mean()))
+
+    def intens(lo, hi):
+        d = torch.from_numpy(diam[lo:hi]).to(dev)
+        sh = torch.from_numpy(shifts[lo:hi]).to(dev)
+        ff, _, _ = _sphere_ff(size, d, dev)
+        ph = 2. * np.pi * (dx[None] * sh[:, :1] + dy[None] * sh[:, 1:]) / size
+        re = torch.cos(ph) * ff * rel + fs_t.real[None]
+        im = torch.sin(ph) * ff * rel + fs_t.imag[None]
+        return (re * re + im * im) * detmask[None]
+
+    tot = 0.
+    for lo in range(0, num_data, chunk):
+        hi = min(num_data, lo + chunk)
+        w = intens(lo, hi).sum(1).cpu().numpy()
+        tot += float((w * scale[lo:hi]).sum())
+    gfac = mean_count * num_data / tot
+
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(int(r_poi.integers(0, 2 ** 62)))
+    ones, multi = np.zeros(num_data, 'i4'), np.zeros(num_data, 'i4')
+    po, pm, cm = [], [], []
+    frames = np.zeros((num_data, size * size), dtype=np.uint16) if dense else None
+    for lo in range(0, num_data, chunk):
+        hi = min(num_data, lo + chunk)
+        w = intens(lo, hi) * (gfac * torch.from_numpy(scale[lo:hi]).to(dev))[:, None]
+        rot = _rotate_bilinear(w, torch.from_numpy(angles[lo:hi]).to(dev), size)
+        cnt = torch.poisson(rot, generator=gen).to(torch.int32).cpu().numpy()
+        if dense:
+            frames[lo:hi] = np.minimum(cnt, 65535).astype(np.uint16)
+        for i in range(hi - lo):
+            f = cnt[i]
+            o = np.flatnonzero(f == 1).astype('i4')
+            m = np.flatnonzero(f > 1).astype('i4')
+            po.append(o)
+            pm.append(m)
+            cm.append(f[m].astype('i4'))
+            ones[lo + i], multi[lo + i] = o.size, m.size
+    cat = lambda a: np.concatenate(a) if a else np.zeros(0, 'i4')  # noqa: E731
+    out = dict(num_pix=np.array([size * size]), ones=ones, multi=multi,
+               place_ones=cat(po), place_multi=cat(pm), count_multi=cat(cm),
+               true_angles=angles, true_shifts=shifts, true_diameters=diam,
+               scale=scale, solution=obj, fsample=fs, rel_scale=np.array(rel))
+    if dense:
+        out['frames'] = frames
+    return out
+
+
+def generate_config(cfg, device='cpu', num_data=None, seed=None):
+    """Dataset of a named configuration (seeded by ``20260000 + cfg``)."""
+    c = CONFIGS[cfg]
+    return generate(c['size'], c['num_data'] if num_data is None else num_data,
+                    c['mean_count'], c['n_blobs'], c['obj_radius'], c['fluence_sigma'],
+                    c['dia'], c['shift_max'], seed=20260000 + cfg if seed is None else seed,
+                    device=device)
+
+
+def initial_model(size, seed):
+    """Random complex start model U[0,1) + iU[0,1) (emc.py:241-242), seeded."""
+    rng = np.random.default_rng(seed)
+    return rng.random(size ** 2) + 1j * rng.random(size ** 2)

@@ -1,0 +1,475 @@
+#!/usr/bin/env python
+"""Benchmark of the RefSPI-MaxLP reconstruction hot path on B200.
+
+Workload (default): the production-shape plain-method configuration --
+185x185 detector, 20,000 synthetic frames at 2,000 photons/frame,
+180 rotations x 9x9 shifts x 5 diameters = 72,900 states per frame.  One
+step = one EMC iteration: likelihood of every frame in every state, per-frame
+max/argmax/log-sum-exp, and the MaxLP M-step over every phaser pixel.
+
+Our arm prints one JSON line with the metric (frame-state evaluations per
+second of whole iterations, and s/iteration), measured with CUDA events on
+the launching stream over K timed steps after W warm-up steps (inputs are
+larger than L2), plus ``e2e`` through ``EMC.run_iteration`` (model copied
+host->device and model + argmax copied back every step), the roofline of the
+dominant kernel from live CUDA events, sampled SM clocks and a CPU baseline
+(the FP64 NumPy oracle on the host cores, bounded sample, extrapolated).
+
+``--impl reference`` times the reference's CPU equations (the FP64 oracle,
+the reference having no CPU path of its own) on all host cores on a bounded
+sample of the same workload and prints the same metric.
+
+Multi-GPU: the path runs as independent replicas (one full workload per
+rank, no collective on the data path); value = sum over ranks, time = max.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, 'refspi-maxlp_b200')
+for _p in (REPO, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = 'frame-state evaluations/s (EMC iteration: E-step + MaxLP M-step)'
+UNIT = 'frame*state/s'
+PEAKS_FALLBACK = {'hbm_gbs': 6650.0, 'bf16_tflops': 1590.0}
+
+
+# ---------------------------------------------------------------------------
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=3)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
+    ap.add_argument('--config', type=int, default=2, choices=[1, 2])
+    ap.add_argument('--frames', type=int, default=None, help='override frame count (testing)')
+    ap.add_argument('--precision', default='fp64', choices=['fp64', 'fp32'])
+    ap.add_argument('--cpu-seconds', type=float, default=20.,
+                    help='target CPU time of the bounded oracle sample')
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-e2e', action='store_true')
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, 'MEASURED_PEAKS.json')) as f:
+            p = json.load(f)
+        return {'hbm_gbs': float(p['hbm_gbs']), 'bf16_tflops': float(p['bf16_tflops']),
+                'source': 'measured'}
+    except Exception:
+        return dict(PEAKS_FALLBACK, source='fallback')
+
+
+def workload(cfg_id, frames):
+    from rspi import synth
+    c = synth.CONFIGS[cfg_id]
+    n = c['num_data'] if frames is None else frames
+    r = c['recon']
+    nsx = int(r['shiftx'].split()[2])
+    nsy = int(r['shifty'].split()[2])
+    nd = int(r['sphere_dia'].split()[2])
+    return dict(cfg=c, n=n, size=c['size'], num_rot=r['num_rot'], n_states0=nsx * nsy * nd,
+                n_states=nsx * nsy * nd * r['num_rot'], recon=r)
+
+
+def write_inputs(tmp, w, data, precision):
+    from rspi.photonfile import write_photons
+    os.makedirs(os.path.join(tmp, 'out'), exist_ok=True)
+    write_photons(os.path.join(tmp, 'photons.npz'), data)
+    cfg = os.path.join(tmp, 'config.ini')
+    r = w['recon']
+    with open(cfg, 'w') as f:
+        f.write('[emc]\nsize = %d\nin_photons_file = photons.npz\noutput_folder = out/\n'
+                'log_file = out/EMC.log\nneed_scaling = True\nnum_rot = %d\nnum_modes = 1\n'
+                'sphere_dia = %s\nshiftx = %s\nshifty = %s\nprecision = %s\n' %
+                (w['size'], r['num_rot'], r['sphere_dia'], r['shiftx'], r['shifty'], precision))
+    return cfg
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    QUERY = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix='.csv')
+            os.close(fd)
+            self.fh = open(self.path, 'w')
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', '-i', str(self.gpu), '--query-gpu=' + self.QUERY,
+                 '--format=csv,noheader,nounits', '-lms', '200'],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(',')]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace('.', '').isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace('.', '').isdigit()]
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == 'active'})
+        return {'sm_mhz': float(np.median(sm)) if sm else None,
+                'sm_max_mhz': max(smax) if smax else None, 'reasons': reasons,
+                'samples': len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the FP64 oracle on the host cores, bounded sample
+# ---------------------------------------------------------------------------
+def _cpu_worker_init():
+    os.environ['OMP_NUM_THREADS'] = '1'
+    os.environ['OPENBLAS_NUM_THREADS'] = '1'
+    os.environ['MKL_NUM_THREADS'] = '1'
+    for p in (REPO, PKG):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+
+
+def _cpu_estep_task(args):
+    """Rotated log-slices of one state (all rotations) + their likelihood
+    against a frame subset; returns (slice seconds, likelihood seconds)."""
+    model, sx, sy, dia, size, num_rot, bg, kmat_sub = args
+    from oracle import emc_oracle as E
+    _, pm = E.generate_masks(size)
+    sel = pm < 1
+    t0 = time.perf_counter()
+    lsl = E.log_slices_for_state(model, sx, sy, dia, size, bg, num_rot, sel)
+    t1 = time.perf_counter()
+    np.asarray(kmat_sub @ lsl.T)
+    t2 = time.perf_counter()
+    return t1 - t0, t2 - t1
+
+
+def _cpu_maxlp_task(args):
+    """Pattern search of one pixel over a frame subset (rescale given)."""
+    f_t, k_d, fref_d, rescale = args
+    from oracle import maxlp_oracle as M
+    pat = M.gen_pattern(8)
+    t0 = time.perf_counter()
+    M.run_pixel_pattern(f_t, k_d, fref_d, pat, rescale, 10)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(w, data, model, target_s):
+    """Extrapolated seconds per iteration of the FP64 oracle on all host cores.
+
+    E-step: a few states x all rotations, likelihood against the first
+    ``nf`` frames -> per-slice-row and per-(row, frame) costs, scaled to all
+    rows and frames.  M-step: ``npx`` pixels over ``nf2`` frames -> per
+    (pixel, frame) cost, scaled to every phaser pixel (ring + main pass) and
+    all frames.  Linear extrapolation, stated in ``sample``.
+    """
+    import multiprocessing as mp
+    from oracle import emc_oracle as E
+    from oracle import maxlp_oracle as M
+    from rspi import geometry
+    cores = os.cpu_count() or 1
+    size, num_rot, n = w['size'], w['num_rot'], w['n']
+    ds = E.parse_photons(data['ones'], data['multi'], data['place_ones'], data['place_multi'],
+                         data['count_multi'], size * size, True)
+    _, pm = E.generate_masks(size)
+    nf = min(n, 500)
+    kmat_sel = E.sparse_frames(ds, pm < 1)[:nf]
+    r = w['recon']
+    sx, sy, dia, _ = geometry.state_grid(geometry.parse_triple(r['shiftx']),
+                                         geometry.parse_triple(r['shifty']),
+                                         geometry.parse_triple(r['sphere_dia']))
+    n_est = max(1, min(cores, 8))
+    picks = np.linspace(0, sx.size - 1, n_est).astype(int)
+    ctx = mp.get_context('spawn')
+    t_wall0 = time.perf_counter()
+    with ctx.Pool(cores, initializer=_cpu_worker_init) as pool:
+        est = pool.map(_cpu_estep_task, [(model, sx[i], sy[i], dia[i], size, num_rot,
+                                          ds['bg'], kmat_sel) for i in picks])
+        t_slice_row = np.mean([a for a, _ in est]) / num_rot
+        t_ll_cell = np.mean([b for _, b in est]) / (num_rot * nf)
+        # M-step sample
+        kmat = E.sparse_frames(ds)
+        qx, qy, qrad, mask, rmask = M.get_qvals(size)
+        main = np.flatnonzero(mask)
+        npx = max(cores, 8)
+        nf2 = min(n, 2000)
+        rng = np.random.default_rng(0)
+        ang = rng.integers(0, num_rot, n) * np.pi / num_rot
+        shifts = np.stack([rng.choice(np.unique(sx), n), rng.choice(np.unique(sy), n)], 1)
+        diams = rng.choice(np.unique(dia), n)
+        tasks = []
+        for t in main[np.linspace(0, main.size - 1, npx).astype(int)]:
+            k = M.photons_pixel(kmat, ang, int(t), size, qx, qy)[:nf2]
+            fr = M.fref_pixel(int(t), qx, qy, qrad, diams, shifts)[:nf2]
+            tasks.append((complex(model[t]), k, fr, 1.0))
+        mt = pool.map(_cpu_maxlp_task, tasks)
+    wall = time.perf_counter() - t_wall0
+    t_px_frame = np.mean(mt) / nf2
+    rows = w['n_states']
+    n_phaser = int(rmask.sum() + mask.sum())
+    serial = rows * t_slice_row + rows * n * t_ll_cell + n_phaser * n * t_px_frame
+    per_iter = serial / cores
+    return dict(s_per_iteration=per_iter, cores=cores, wall_s=wall,
+                sample=('FP64 NumPy oracle, %d workers: E-step %d of %d (shift,dia) states x %d '
+                        'rotations vs %d of %d frames, M-step %d pixels x %d frames; linear '
+                        'extrapolation to %d rows x %d frames and %d phaser pixels, divided by '
+                        'the worker count' % (cores, n_est, w['n_states0'], num_rot, nf, n, npx,
+                                              nf2, rows, n, n_phaser)))
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return 0
+    from rspi import synth
+    w = workload(args.config, args.frames)
+    c = w['cfg']
+    data = synth.generate(c['size'], w['n'], c['mean_count'], c['n_blobs'], c['obj_radius'],
+                          c['fluence_sigma'], c['dia'], c['shift_max'], seed=20260000 + args.config)
+    model = synth.initial_model(w['size'], 20260100 + args.config)
+    times = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        base = cpu_baseline(w, data, model, args.cpu_seconds)
+        if i >= args.warmup:
+            times.append(base['s_per_iteration'])
+    t = max(times)
+    v = w['n'] * w['n_states'] / t
+    out = {'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': UNIT,
+           'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+           'ms_per_step': t * 1e3, 's_per_iteration': t, 'higher_is_better': True,
+           'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+           'config': {'workload': 'config%d: %dx%d detector, %d frames, %d states/frame' %
+                      (args.config, w['size'], w['size'], w['n'], w['n_states']),
+                      'frames': w['n'], 'states_per_frame': w['n_states'],
+                      'l2': 'inputs larger than L2'},
+           'cpu_baseline': {'value': v, 'unit': UNIT, 'cores': base['cores'], 'kind': 'port',
+                            'sample': base['sample']},
+           'e2e': {'value': v, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from rspi import lib as rlib
+    from rspi import synth
+
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    w = workload(args.config, args.frames)
+    c = w['cfg']
+    t0 = time.time()
+    data = synth.generate(c['size'], w['n'], c['mean_count'], c['n_blobs'], c['obj_radius'],
+                          c['fluence_sigma'], c['dia'], c['shift_max'],
+                          seed=20260000 + args.config, device=dev)
+    t_gen = time.time() - t0
+    tmp = tempfile.mkdtemp(prefix='rspi_bench_')
+    cfgfile = write_inputs(tmp, w, data, args.precision)
+    from emc import EMC
+    import contextlib
+    import io
+    with contextlib.redirect_stdout(io.StringIO()):
+        rec = EMC(cfgfile, device=dev)
+    model0 = synth.initial_model(w['size'], 20260100 + args.config)
+    stream = torch.cuda.current_stream()
+
+    # kernel-level events for the roofline (on the launching stream)
+    ev = {'loglike': [], 'pattern_main': []}
+    orig_loglike = rec.estep.loglike
+
+    def timed_loglike(r0, r1, lsl=None):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        orig_loglike(r0, r1, lsl)
+        b.record(stream)
+        ev['loglike'].append((a, b, r1 - r0))
+    rec.estep.loglike = timed_loglike
+
+    dmodel = torch.from_numpy(model0).to(dev)
+
+    def step():
+        rec.estep.run(dmodel)
+        rec.estep.reduce()
+        rec.phaser.run_from_rmax(dmodel, rec.estep.rmax, w['num_rot'], rec.state_vals,
+                                 rec.phaser_rot)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev['loglike'].clear()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    launches0 = rlib.launch_count
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = rlib.launch_count - launches0
+    ms = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    ll_ms = sum(a.elapsed_time(b) for a, b, _ in ev['loglike']) / args.steps
+    ll_launches = len(ev['loglike']) // args.steps
+    rec.dset.photons.err.check('bench')
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+
+    # e2e through the public API: host model in, host model + argmax out
+    e2e = None
+    if not args.no_e2e:
+        rec.model = model0.copy()
+        for _ in range(min(args.warmup, 1)):
+            rec.run_iteration(None)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t_e0 = time.perf_counter()
+        for _ in range(args.steps):
+            rec.run_iteration(None)
+        torch.cuda.synchronize()
+        e2e_s = (time.perf_counter() - t_e0) / args.steps
+        if world > 1:
+            t = torch.tensor([e2e_s], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        p = w['size'] ** 2
+        e2e = {'value': world * w['n'] * w['n_states'] / e2e_s, 'unit': UNIT,
+               's_per_iteration': e2e_s, 'h2d_bytes_per_step': 16 * p,
+               'd2h_bytes_per_step': 16 * p + 4 * w['n'],
+               'api': 'EMC.run_iteration (model host->device, model + argmax device->host)'}
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+
+    pk = peaks()
+    es = rec.estep
+    total_rows = es.ll['total_rows']
+    esz = 4 if es.slice_code == 0 else 8
+    osz = 4 if es.prob_code == 0 else 8
+    # dominant kernel: the likelihood kernel (row a7); algorithmic bytes per
+    # launch = its slices in + its LL rows out + the packed photon entries once
+    rows_per_launch = es.n_rows / max(1, ll_launches)
+    alg_bytes = rows_per_launch * (es.p_pad * esz + w['n'] * osz) + total_rows * 128 + 8 * w['n']
+    ll_launch_ms = ll_ms / max(1, ll_launches)
+    achieved = alg_bytes / (ll_launch_ms * 1e-3) / 1e9
+    # on-chip gather roofline: one shared-memory gather per entry slot per row
+    gathers = rows_per_launch * total_rows * 32
+    sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
+    clk_mhz = (clk or {}).get('sm_mhz') or 1965.
+    lanes = 32 if es.slice_code == 0 else 16
+    gather_peak = sm_count * lanes * clk_mhz * 1e6
+    gather_rate = gathers / (ll_launch_ms * 1e-3)
+    traffic = None
+    prof = os.path.join(REPO, 'profiles', 'loglike_traffic.json')
+    if os.path.exists(prof):
+        try:
+            with open(prof) as f:
+                pj = json.load(f)
+            traffic = pj.get('%s_%s_bytes_per_row' % (args.precision, 'cfg%d' % args.config))
+            if traffic is not None:
+                traffic = float(traffic) * rows_per_launch
+        except Exception:
+            traffic = None
+
+    value = world * w['n'] * w['n_states'] / (ms * 1e-3)
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        cb = cpu_baseline(w, {k: (v.cpu().numpy() if hasattr(v, 'cpu') else v) for k, v in data.items()},
+                          model0, args.cpu_seconds)
+        cpu = {'value': w['n'] * w['n_states'] / cb['s_per_iteration'], 'unit': UNIT,
+               'cores': cb['cores'], 'kind': 'port', 'sample': cb['sample'],
+               's_per_iteration': cb['s_per_iteration']}
+    out = {
+        'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+        'warmup': args.warmup, 'ms_per_step': ms, 's_per_iteration': ms / 1e3,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'f64' if args.precision == 'fp64' else 'f32 slices, f64 accumulate',
+        'data': 'synthetic (seeded generator with the configuration\'s shapes)',
+        'config': {'workload': 'config%d: %dx%d detector, %d frames, %d rotations x %d (shift,dia) '
+                   'states = %d states/frame, 1 EMC iteration per step' %
+                   (args.config, w['size'], w['size'], w['n'], w['num_rot'], w['n_states0'],
+                    w['n_states']),
+                   'frames': w['n'], 'states_per_frame': w['n_states'],
+                   'precision': args.precision, 'parallelism': 'replicas' if world > 1 else 'single',
+                   'l2': 'inputs larger than L2 (slices %.1f GB, likelihoods %.1f GB per step)' %
+                   (es.n_rows * es.p_pad * esz / 1e9, es.n_rows * w['n'] * osz / 1e9)},
+        'gpu_launches': launches // args.steps * args.steps,
+        'roofline': {'kernel': 'k_loglike (likelihood, row a7)', 'bound': 'hbm',
+                     'achieved': achieved, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
+                     'frac': achieved / pk['hbm_gbs'], 'traffic': traffic,
+                     'peak_source': pk['source'] + ' (HBM copy)',
+                     'launch_ms': ll_launch_ms, 'launches_per_step': ll_launches,
+                     'share_of_step': ll_ms / ms},
+        'roofline_gather': {'achieved': gather_rate, 'peak': gather_peak, 'unit': 'gathers/s',
+                            'frac': gather_rate / gather_peak,
+                            'note': 'shared-memory gather limit: %d SMs x %d lanes/clk x %.0f MHz'
+                            % (sm_count, lanes, clk_mhz)},
+        'clocks': clk,
+        'e2e': e2e,
+        'cpu_baseline': cpu,
+        'setup_s': {'generate': t_gen},
+    }
+    print(json.dumps(out))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == 'reference':
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == '__main__':
+    sys.exit(main())

@@ -1,0 +1,195 @@
+/*
+ * rspi.h -- C ABI of the B200 (sm_100a) RefSPI-MaxLP reconstruction hot path.
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t,
+ * launches asynchronously on that stream, allocates nothing and never
+ * synchronises the host, so a whole iteration can be captured in a CUDA
+ * graph.  The caller owns every buffer.  Returns RSPI_OK (0) or a negative
+ * RSPI_ERR_* code for a bad argument or a failed launch; problems found on
+ * the device (an out-of-range pixel index in the input, a bounded wait that
+ * ran out) are written to the caller's `err` word (first error wins) and read
+ * by the caller after the stream is synchronised.
+ *
+ * The reference (RefSPI-MaxLP) has no C ABI: its kernels are CuPy RawModule
+ * launches driven from Python.  Each entry point below names the reference
+ * code it replaces (file:line, relative to the reference project root).
+ *
+ * Layouts (row-major, pixel t = x*size + y, kernels.cu:13):
+ *   state s0 = (isx*nsy + isy)*nd + idia (emc.py:71-77); likelihood row
+ *   r = s0*num_rot + j for rotation angle j*pi/num_rot (emc.py:192,199).
+ *   "sel" pixels: probmask == 0 (emc.py:95-98, kernels.cu:129), compacted in
+ *   pixel order; a slice row holds p_pad >= n_sel values (p_pad % 32 == 0).
+ */
+#ifndef RSPI_H
+#define RSPI_H
+
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RSPI_OK 0
+#define RSPI_ERR_ARG (-1)      /* bad size, pointer or option */
+#define RSPI_ERR_INDEX (-2)    /* pixel / state index out of range in the input */
+#define RSPI_ERR_CUDA (-3)     /* launch failed */
+#define RSPI_ERR_TIMEOUT (-4)  /* a bounded device-side wait ran out */
+#define RSPI_ERR_CAPACITY (-5) /* a value does not fit the packed layout */
+
+/* Library version and build target, e.g. "rspi 0.1 sm_100a". */
+const char *rspi_version(void);
+
+/* Human-readable text for a status code. */
+const char *rspi_status_string(int status);
+
+/* ---------------------------------------------------------------- a1, a2
+ * Photon-list setup.  Replaces dset.py:32-33,41-42 (ones_accum/multi_accum:
+ * int64 exclusive prefix sums), dset.py:46-53 (mean_count, counts),
+ * emc.py:129-132 (scales) and dset.py:74-83 (powder).  Bit-exact.
+ *   totals[0] = sum(ones), totals[1] = sum(multi), totals[2] = sum(count_multi)
+ *   mean_count = (totals[0] + totals[2]) / n_data;
+ *   scales[d] = counts[d] / mean_count if need_scaling else 1.
+ */
+int rspi_photon_offsets(const int *ones, const int *multi, const int *count_multi,
+                        long long n_data, long long *ones_accum, long long *multi_accum,
+                        long long *counts, long long *totals, double *mean_count,
+                        double *scales, int need_scaling, int *err, cudaStream_t stream);
+
+/* powder[p] = (photons at p summed over frames) / n_data (dset.py:74-83).
+ * Pixel indices outside [0, num_pix) set RSPI_ERR_INDEX in err and are skipped. */
+int rspi_powder(const int *place_ones, long long n_ones, const int *place_multi,
+                const int *count_multi, long long n_multi, long long num_pix,
+                long long n_data, double *powder, int *err, cudaStream_t stream);
+
+/* Likelihood entry lists (the layout calc_prob_all walks, kernels.cu:127-136,
+ * restricted to probmask < 1).  Each frame's in-mask photons (ones with count
+ * 1, multi with their counts) become 32-bit entries (sel_index << 16 | count)
+ * packed into rows of 32 so that lane b holds sel_index % 32 == b: one warp
+ * gather per row touches 32 distinct shared-memory banks.  Unused slots are
+ * (b << 16 | 0).
+ * Pass 1 writes frame_rows[d]; the caller forms row_off = exclusive scan
+ * (rspi_scan_rows) and pass 2 fills entries[(row_off[d] + r)*32 + b].
+ * Requires n_sel <= 65536 and every count <= 65535 (else RSPI_ERR_CAPACITY). */
+int rspi_ll_entry_rows(const int *ones, const int *multi, const long long *ones_accum,
+                       const long long *multi_accum, const int *place_ones,
+                       const int *place_multi, const int *count_multi,
+                       const int *pix2sel, long long num_pix, long long n_data,
+                       int *frame_rows, long long *frame_sel_photons, int *err,
+                       cudaStream_t stream);
+int rspi_scan_rows(const int *frame_rows, long long n_data, long long *row_off,
+                   cudaStream_t stream);
+int rspi_ll_entry_fill(const int *ones, const int *multi, const long long *ones_accum,
+                       const long long *multi_accum, const int *place_ones,
+                       const int *place_multi, const int *count_multi,
+                       const int *pix2sel, long long num_pix, long long n_data,
+                       const long long *row_off, unsigned int *entries, int *err,
+                       cudaStream_t stream);
+
+/* ------------------------------------------------------------------- a4, a5
+ * Holographic slices of every (shift, diameter) state, replacing
+ * slice_gen_holo (kernels.cu:44-82, log_flag=0, rel_scale=scale=1) as
+ * launched at emc.py:174-176 and 186-188:
+ *   W[s0][p] = |model[p] + ff(pi*r*dia/size) * exp(i*phase)|^2 + bg[p]
+ * and the masked sums msum[s0] = sum_{probmask<1} W[s0] (emc.py:177). */
+int rspi_holo_slices(const double *model /* complex128, P */, const double *shiftx,
+                     const double *shifty, const double *sphere_dia, long long n_states0,
+                     long long size, const double *bg, const int *sel_pix, long long n_sel,
+                     double *holo /* n_states0 x P */, double *msum, cudaStream_t stream);
+
+/* vscale and per-state likelihood offsets (emc.py:181, 199):
+ *   vscale = sum_sel powder / sum_s0 msum[s0] * n_states0,
+ *   init[s0] = -(msum[s0] * vscale). */
+int rspi_vscale_init(const double *msum, long long n_states0, const double *powder,
+                     const int *sel_pix, long long n_sel, double *vscale, double *init,
+                     cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ a6
+ * Rotated log-slices restricted to sel pixels, replacing slice_gen with
+ * log_flag=1 (kernels.cu:6-42) as launched at emc.py:191-193:
+ *   L[s0*num_rot + j][c] = log(bilinear(W[s0])(R(j)(p-cen)+cen) + bg[p]),
+ *   -1000 outside the detector or below 1e-20; p = sel_pix[c].
+ * rot_cs[2*j], rot_cs[2*j+1] = cos, sin of angle j (host table).
+ * out_dtype 0 = float32, 1 = float64; rows are p_pad long, tail zeroed.
+ * rows [row_begin, row_end) of the full S0*num_rot range are produced. */
+int rspi_rot_log_slices(const double *holo, long long n_states0, long long num_rot,
+                        const double *rot_cs, long long size, const double *bg,
+                        const int *sel_pix, long long n_sel, long long p_pad,
+                        long long row_begin, long long row_end, void *lslices,
+                        int out_dtype, cudaStream_t stream);
+
+/* ------------------------------------------------------------------------ a7
+ * Log-likelihood of frames x states, replacing calc_prob_all
+ * (kernels.cu:116-137) launched once per (state, rotation) at emc.py:194-199:
+ *   LL[r][d] = init[r / num_rot] * scales[d] + sum_entries count * L[r][sel]
+ * One CTA owns `states_per_tile` consecutive rows, stages their slices in
+ * shared memory and walks every frame's packed rows (a warp per frame,
+ * frames taken in `frame_order`).  Accumulation is FP64.
+ * slice_dtype / out_dtype: 0 = float32, 1 = float64.
+ * Rows [row_begin, row_end) are computed: the slice of row r is read at
+ * lslices + (r - row_begin) * p_pad and LL row r is written at
+ * ll + (r - row_begin) * ll_stride. */
+int rspi_loglike(const void *lslices, int slice_dtype, long long p_pad, long long num_rot,
+                 const double *init, const double *scales, const unsigned int *entries,
+                 const long long *row_off, const int *frame_order, long long n_data,
+                 long long row_begin, long long row_end, void *ll, int out_dtype,
+                 long long ll_stride, int states_per_tile, int warps_per_cta,
+                 int n_ctas, cudaStream_t stream);
+
+/* Largest states_per_tile whose slices fit in shared memory (0 if none). */
+int rspi_loglike_max_tile(long long p_pad, int slice_dtype);
+
+/* ------------------------------------------------------------------- a8, a9
+ * Per-frame reduction over all states of LL (n_rows x n_data, FP64 or FP32):
+ * first-index max/argmax (emc.py:208-209) and the FP64 log-sum-exp
+ * logz[d] = max + log(sum_r exp(LL[r][d] - max)) (standard EMC
+ * normalisation; absent from the reference run path). */
+int rspi_frame_reduce(const void *ll, int ll_dtype, long long n_rows, long long n_data,
+                      double *maxll, int *rmax, double *logz, cudaStream_t stream);
+
+/* ----------------------------------------------------------------- a11-a14
+ * MaxLP M-step (maxLP.py:304-340).  Frames carry a reference-state index
+ * fstate[d] into ref_params (n_ref x 3: shiftx, shifty, diameter) and a
+ * rotation index frot[d] into rot_cs (cos(-a), sin(-a)).
+ *
+ * rspi_maxlp_frame_params: from the E-step argmax rmax[d] (emc.py:218-224):
+ *   fstate = rmax / num_rot, frot = rmax % num_rot, nstate[s] = #frames. */
+int rspi_maxlp_frame_params(const int *rmax, long long n_data, long long num_rot,
+                            long long n_ref, int *fstate, int *frot, int *nstate,
+                            int *err, cudaStream_t stream);
+
+/* Photon histogram of every phaser pixel over reference states:
+ *   hist[m][s] = sum over frames d with fstate[d]==s of K_d(u_d(t_m)),
+ * u_d(t) = rint(R(-ang_d) q_t * size + size//2) (maxLP.py:245-253), scattered
+ * from each photon to the model pixels that map onto it.  The index
+ * arithmetic is two products and a sum per coordinate without fused
+ * multiply-add, so it is bit-exact with the FP64 restatement.
+ * mask_idx[t] = m for phaser pixels (maxLP.py:88), -1 elsewhere.  hist must be
+ * zeroed by the caller (n_mask x n_ref int32). */
+int rspi_maxlp_histogram(const int *ones, const int *multi, const long long *ones_accum,
+                         const long long *multi_accum, const int *place_ones,
+                         const int *place_multi, const int *count_multi, long long n_data,
+                         const int *fstate, const int *frot, const double *rot_cs,
+                         long long size, const int *mask_idx, long long n_mask,
+                         long long n_ref, int *hist, int *err, cudaStream_t stream);
+
+/* Pattern search of a set of model pixels (maxLP.py:154-197): for each pixel
+ * t = pixels[i] (its histogram row hist_row[i]) run <= num_iter iterations over
+ * the 33x33 candidate grid.  rescale_mode 0: per-candidate rescale
+ * (ring pass, maxLP.py:186-187); 1: the scalar *rescale (main pass).
+ * fconv (complex128, P) is updated in place.  With rescale_out != NULL the
+ * per-pixel rescale of the final value (maxLP.py:328) is written to
+ * rescale_out[i]. */
+int rspi_maxlp_pattern(double *fconv, const int *pixels, const int *hist_row,
+                       long long n_pix, const int *hist, long long n_ref,
+                       const int *nstate, long long n_data, const double *ref_params,
+                       long long size, int rescale_mode, const double *rescale,
+                       int num_iter, double *rescale_out, cudaStream_t stream);
+
+/* Mean of n values into *out (the global rescale, maxLP.py:329). */
+int rspi_mean(const double *vals, long long n, double *out, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RSPI_H */

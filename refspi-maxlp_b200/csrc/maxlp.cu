@@ -1,0 +1,405 @@
+// MaxLP M-step (rows a11-a14): per-pixel complex pattern search.
+//
+// The reference (maxLP.py:154-197) evaluates, for every model pixel and each
+// of 1089 candidates f_c, mean over ALL frames of k_d log(rho |f_c + r_d|^2)
+// minus mean of rho |f_c + r_d|^2, materialising frames x candidates arrays
+// (~20 CuPy launches per pattern iteration).  Two exact rewrites make it a
+// per-pixel register computation here:
+//  * r_d depends on frame d only through its reference state (shift,
+//    diameter), so frames sharing a state share the log term:
+//      sum_d k_d log(rho w_d) = sum_s K_t[s] log(rho |f_c + r_s|^2),
+//    with K_t[s] the photons that pixel t receives from frames in state s
+//    (built once per M-step by scattering each photon to the model pixels
+//    whose rotated index lands on it);
+//  * the frame mean of |f_c + r_d|^2 is |f_c + rbar|^2 + var(r), with
+//    rbar = mean_d r_d and var(r) = mean_d |r_d - rbar|^2 per pixel.
+// All arithmetic is FP64, so candidate values agree with the FP64
+// restatement to rounding and the search takes the same path.
+#include "rspi_common.cuh"
+
+namespace {
+
+constexpr double PI = 3.14159265358979311599796346854;  // the double nearest pi
+constexpr int NCAND = 1089;                               // 33 x 33 (maxLP.py:45-48)
+constexpr int CENTRE = NCAND / 2;                         // maxLP.py:176
+constexpr int PT_THREADS = 384;
+constexpr int PT_CPT = 3;                                 // 384 * 3 >= 1089
+constexpr int POP_CAP = 1024;                             // populated states in shared memory
+
+__global__ void k_frame_params(const int *__restrict__ rmax, long long n, long long num_rot,
+                               long long n_ref, int *__restrict__ fstate, int *__restrict__ frot,
+                               int *__restrict__ nstate, int *err) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long d = (long long)blockIdx.x * blockDim.x + threadIdx.x; d < n; d += stride) {
+        const long long r = rmax[d];
+        if (r < 0 || r >= n_ref * num_rot) {
+            rspi_flag(err, RSPI_ERR_INDEX);
+            fstate[d] = -1;
+            frot[d] = 0;
+            continue;
+        }
+        const int s = (int)(r / num_rot);
+        fstate[d] = s;
+        frot[d] = (int)(r - (long long)s * num_rot);
+        atomicAdd(&nstate[s], 1);
+    }
+}
+
+// Detector pixel of model pixel (tx, ty) for a frame with rotation (c, s):
+// maxLP.py:250-252, x' = c qx + (-s) qy, y' = s qx + c qy, rint(x' size + size//2).
+__device__ __forceinline__ void forward_pixel(int tx, int ty, double c, double s, int size,
+                                              int &ox, int &oy) {
+    const double ds = (double)size, c0 = (double)(size / 2);
+    const double qx = ((double)tx - c0) / ds, qy = ((double)ty - c0) / ds;
+    const double xr = xadd(xmul(c, qx), xmul(-s, qy));
+    const double yr = xadd(xmul(s, qx), xmul(c, qy));
+    ox = (int)rint(xadd(xmul(xr, ds), c0));
+    oy = (int)rint(xadd(xmul(yr, ds), c0));
+}
+
+// Add `cnt` photons at detector (ux, uy) to every phaser pixel that maps
+// onto exactly (ux, uy).  Such pixels lie within 1/sqrt(2) px of the inverse
+// image, so the 3x3 neighbourhood of its rounding holds them all.
+__device__ __forceinline__ void scatter_photon(int ux, int uy, int cnt, double c, double s,
+                                               int size, const int *__restrict__ mask_idx,
+                                               long long n_ref, int st, int *__restrict__ hist) {
+    const double c0 = (double)(size / 2);
+    const double vx = (double)ux - c0, vy = (double)uy - c0;
+    const int bx = (int)rint(c * vx + s * vy + c0);
+    const int by = (int)rint(-s * vx + c * vy + c0);
+    for (int ax = -1; ax <= 1; ++ax)
+        for (int ay = -1; ay <= 1; ++ay) {
+            const int tx = bx + ax, ty = by + ay;
+            if (tx < 0 || ty < 0 || tx >= size || ty >= size) continue;
+            const int m = mask_idx[tx * size + ty];
+            if (m < 0) continue;
+            int ox, oy;
+            forward_pixel(tx, ty, c, s, size, ox, oy);
+            if (ox == ux && oy == uy) atomicAdd(&hist[(long long)m * n_ref + st], cnt);
+        }
+}
+
+__global__ void __launch_bounds__(256)
+k_histogram(const int *__restrict__ ones, const int *__restrict__ multi,
+            const long long *__restrict__ ones_accum, const long long *__restrict__ multi_accum,
+            const int *__restrict__ place_ones, const int *__restrict__ place_multi,
+            const int *__restrict__ count_multi, long long n, const int *__restrict__ fstate,
+            const int *__restrict__ frot, const double *__restrict__ rot_cs, int size,
+            const int *__restrict__ mask_idx, long long n_ref, int *__restrict__ hist, int *err) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long npix = (long long)size * size;
+    for (long long d = warp; d < n; d += nwarp) {
+        const int st = fstate[d];
+        if (st < 0) continue;
+        const int j = frot[d];
+        const double c = rot_cs[2 * j], s = rot_cs[2 * j + 1];
+        const int n_o = ones[d], n_m = multi[d];
+        const long long oa = ones_accum[d], ma = multi_accum[d];
+        for (int i = lane; i < n_o + n_m; i += 32) {
+            int p, cnt;
+            if (i < n_o) {
+                p = place_ones[oa + i];
+                cnt = 1;
+            } else {
+                p = place_multi[ma + i - n_o];
+                cnt = count_multi[ma + i - n_o];
+            }
+            if (p < 0 || p >= npix) {
+                rspi_flag(err, RSPI_ERR_INDEX);
+                continue;
+            }
+            const int ux = p / size, uy = p - (p / size) * size;
+            scatter_photon(ux, uy, cnt, c, s, size, mask_idx, n_ref, st, hist);
+            // column x*size + size of row x aliases pixel (x+1, 0): even sizes only
+            if (uy == 0 && ux >= 1 && (size % 2) == 0)
+                scatter_photon(ux - 1, size, cnt, c, s, size, mask_idx, n_ref, st, hist);
+        }
+    }
+}
+
+// Reference-sphere amplitude at pixel (qx, qy, qrad) for state (sx, sy, dia),
+// maxLP.py:238-243: ff(pi qrad dia) exp(2 pi i (qx sx + qy sy)).
+__device__ __forceinline__ double2 fref_value(double qx, double qy, double qrad, double sx,
+                                              double sy, double dia) {
+    const double sval = xmul(xmul(PI, qrad), dia);
+    const double ff = xsub(sin(sval), xmul(sval, cos(sval))) / pow(sval, 3.);
+    const double th = xmul(2. * PI, xadd(xmul(qx, sx), xmul(qy, sy)));
+    return make_double2(ff * cos(th), ff * sin(th));
+}
+
+struct PixelConsts {
+    double qx, qy, qrad;
+    double ar, ai;   // rbar = mean_d r_d
+    double var;      // mean_d |r_d - rbar|^2
+    double ksum;     // sum_d k_d
+};
+
+__device__ __forceinline__ void block_argmax(double &v, int &idx, double *sv, int *si) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(RSPI_FULL_MASK, v, o);
+        const int oi = __shfl_xor_sync(RSPI_FULL_MASK, idx, o);
+        if (argmax_better(ov, oi, v, idx)) {
+            v = ov;
+            idx = oi;
+        }
+    }
+    __syncthreads();
+    if (lane == 0) {
+        sv[wid] = v;
+        si[wid] = idx;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        double bv = lane < nw ? sv[lane] : 0.;
+        int bi = lane < nw ? si[lane] : 0x7fffffff;
+        if (lane >= nw) bv = -INFINITY;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_xor_sync(RSPI_FULL_MASK, bv, o);
+            const int oi = __shfl_xor_sync(RSPI_FULL_MASK, bi, o);
+            if (argmax_better(ov, oi, bv, bi)) {
+                bv = ov;
+                bi = oi;
+            }
+        }
+        if (lane == 0) {
+            sv[0] = bv;
+            si[0] = bi;
+        }
+    }
+    __syncthreads();
+    v = sv[0];
+    idx = si[0];
+    __syncthreads();
+}
+
+// Ordered compaction of the populated reference states of one pixel, from
+// state `s_begin` on, into shared memory (at most POP_CAP).  Returns the state
+// where the next chunk starts (n_ref when done); *count gets the number stored.
+__device__ int load_populated(int s_begin, const int *__restrict__ hrow, long long n_ref,
+                              const double *__restrict__ ref_params, const PixelConsts &pc,
+                              double *fr_re, double *fr_im, double *fk, int *count, int *wsum) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = blockDim.x >> 5;
+    int filled = 0;
+    int s0 = s_begin;
+    while (s0 < n_ref) {
+        const int s = s0 + threadIdx.x;
+        const int h = s < n_ref ? hrow[s] : 0;
+        const unsigned bal = __ballot_sync(RSPI_FULL_MASK, h > 0);
+        __syncthreads();
+        if (lane == 0) wsum[wid] = __popc(bal);
+        __syncthreads();
+        int before = 0, round = 0;
+        for (int w = 0; w < nw; ++w) {
+            if (w < wid) before += wsum[w];
+            round += wsum[w];
+        }
+        if (filled + round > POP_CAP) break;  // this round starts the next chunk
+        if (h > 0) {
+            const int pos = filled + before + __popc(bal & ((1u << lane) - 1u));
+            const double2 r = fref_value(pc.qx, pc.qy, pc.qrad, ref_params[3 * s],
+                                         ref_params[3 * s + 1], ref_params[3 * s + 2]);
+            fr_re[pos] = r.x;
+            fr_im[pos] = r.y;
+            fk[pos] = (double)h;
+        }
+        filled += round;
+        s0 += blockDim.x;
+    }
+    __syncthreads();
+    *count = filled;
+    return s0 < n_ref ? s0 : (int)n_ref;
+}
+
+__global__ void __launch_bounds__(PT_THREADS)
+k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
+          const int *__restrict__ hist_row, const int *__restrict__ hist, long long n_ref,
+          const int *__restrict__ nstate, long long n_data, const double *__restrict__ ref_params,
+          int size, int ring, const double *__restrict__ rescale_ptr, int num_iter,
+          double *__restrict__ rescale_out) {
+    __shared__ double fr_re[POP_CAP], fr_im[POP_CAP], fk[POP_CAP];
+    __shared__ double scratch[32];
+    __shared__ int iscratch[32];
+    __shared__ int wsum[32];
+
+    const long long ip = blockIdx.x;
+    const int t = pixels[ip];
+    const int *hrow = hist + (long long)hist_row[ip] * n_ref;
+    const double dn = (double)n_data;
+
+    PixelConsts pc;
+    {
+        const double ds = (double)size, c0 = (double)(size / 2);
+        const int tx = t / size, ty = t - (t / size) * size;
+        pc.qx = ((double)tx - c0) / ds;
+        pc.qy = ((double)ty - c0) / ds;
+        pc.qrad = sqrt(xadd(xmul(pc.qx, pc.qx), xmul(pc.qy, pc.qy)));
+        if (pc.qrad == 0.) pc.qrad = 1.e-6;  // maxLP.py:85
+    }
+    // rbar, K total
+    double ar = 0., ai = 0., ks = 0.;
+    for (long long s = threadIdx.x; s < n_ref; s += blockDim.x) {
+        const int ns = nstate[s];
+        ks += (double)hrow[s];
+        if (ns > 0) {
+            const double2 r = fref_value(pc.qx, pc.qy, pc.qrad, ref_params[3 * s],
+                                         ref_params[3 * s + 1], ref_params[3 * s + 2]);
+            ar += ns * r.x;
+            ai += ns * r.y;
+        }
+    }
+    pc.ar = block_sum(ar, scratch) / dn;
+    pc.ai = block_sum(ai, scratch) / dn;
+    pc.ksum = block_sum(ks, scratch);
+    double vv = 0.;
+    for (long long s = threadIdx.x; s < n_ref; s += blockDim.x) {
+        const int ns = nstate[s];
+        if (ns > 0) {
+            const double2 r = fref_value(pc.qx, pc.qy, pc.qrad, ref_params[3 * s],
+                                         ref_params[3 * s + 1], ref_params[3 * s + 2]);
+            const double er = r.x - pc.ar, ei = r.y - pc.ai;
+            vv += ns * (er * er + ei * ei);
+        }
+    }
+    pc.var = block_sum(vv, scratch) / dn;
+
+    int npop = 0;
+    const bool one_chunk = n_ref <= POP_CAP;
+    if (one_chunk) load_populated(0, hrow, n_ref, ref_params, pc, fr_re, fr_im, fk, &npop, wsum);
+
+    const double kmean = pc.ksum / dn;
+    const double rescale = ring ? 0. : *rescale_ptr;
+    double2 f = fconv[t];
+    double step = hypot(f.x, f.y) / 4.;
+    const double shrink = 33. / 5.;  // sqrt(1089) / 5, maxLP.py:177
+
+    for (int it = 0; it < num_iter; ++it) {
+        double fcr[PT_CPT], fci[PT_CPT], rho[PT_CPT], acc[PT_CPT];
+#pragma unroll
+        for (int k = 0; k < PT_CPT; ++k) {
+            const int c = threadIdx.x + k * PT_THREADS;
+            const int cc = c < NCAND ? c : 0;
+            const double px = -8. + 0.5 * (cc / 33), py = -8. + 0.5 * (cc % 33);
+            fcr[k] = xadd(f.x, xmul(px, step));
+            fci[k] = xadd(f.y, xmul(py, step));
+            const double er = fcr[k] + pc.ar, ei = fci[k] + pc.ai;
+            const double mw = er * er + ei * ei + pc.var;
+            rho[k] = ring ? kmean / mw : rescale;
+            acc[k] = 0.;
+        }
+        int s_next = 0;
+        do {
+            if (!one_chunk)
+                s_next = load_populated(s_next, hrow, n_ref, ref_params, pc, fr_re, fr_im, fk,
+                                        &npop, wsum);
+            else
+                s_next = (int)n_ref;
+            for (int j = 0; j < npop; ++j) {
+                const double rr = fr_re[j], ri = fr_im[j], kk = fk[j];
+#pragma unroll
+                for (int k = 0; k < PT_CPT; ++k) {
+                    const double re = fcr[k] + rr, im = fci[k] + ri;
+                    acc[k] = fma(kk, log(rho[k] * (re * re + im * im)), acc[k]);
+                }
+            }
+            if (!one_chunk) __syncthreads();
+        } while (s_next < n_ref);
+
+        double best = -INFINITY;
+        int bidx = 0x7fffffff;
+#pragma unroll
+        for (int k = 0; k < PT_CPT; ++k) {
+            const int c = threadIdx.x + k * PT_THREADS;
+            if (c >= NCAND) continue;
+            const double er = fcr[k] + pc.ar, ei = fci[k] + pc.ai;
+            const double mw = er * er + ei * ei + pc.var;
+            double q = acc[k] / dn - rho[k] * mw;
+            if (ring && pc.ksum == 0.) q = NAN;  // 0 * log(0) in every frame
+            if (argmax_better(q, c, best, bidx)) {
+                best = q;
+                bidx = c;
+            }
+        }
+        block_argmax(best, bidx, scratch, iscratch);
+        const double px = -8. + 0.5 * (bidx / 33), py = -8. + 0.5 * (bidx % 33);
+        const double2 fnew = make_double2(xadd(f.x, xmul(px, step)), xadd(f.y, xmul(py, step)));
+        const double step_new = bidx == CENTRE ? step / shrink : step;
+        if (step_new / hypot(fnew.x, fnew.y) < 1.e-3) break;  // keeps f (maxLP.py:162-165)
+        f = fnew;
+        step = step_new;
+    }
+    if (threadIdx.x == 0) {
+        fconv[t] = f;
+        if (rescale_out) {
+            const double er = f.x + pc.ar, ei = f.y + pc.ai;
+            rescale_out[ip] = kmean / (er * er + ei * ei + pc.var);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_mean(const double *__restrict__ v, long long n,
+                                               double *__restrict__ out) {
+    __shared__ double scratch[32];
+    double a = 0.;
+    for (long long i = threadIdx.x; i < n; i += blockDim.x) a += v[i];
+    a = block_sum(a, scratch);
+    if (threadIdx.x == 0) *out = a / (double)n;
+}
+
+}  // namespace
+
+extern "C" int rspi_maxlp_frame_params(const int *rmax, long long n_data, long long num_rot,
+                                       long long n_ref, int *fstate, int *frot, int *nstate,
+                                       int *err, cudaStream_t stream) {
+    if (!rmax || !fstate || !frot || !nstate || n_data <= 0 || num_rot <= 0 || n_ref <= 0)
+        return RSPI_ERR_ARG;
+    cudaMemsetAsync(nstate, 0, sizeof(int) * n_ref, stream);
+    k_frame_params<<<rspi_blocks(n_data, 256), 256, 0, stream>>>(rmax, n_data, num_rot, n_ref,
+                                                                fstate, frot, nstate, err);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_maxlp_histogram(const int *ones, const int *multi,
+                                    const long long *ones_accum, const long long *multi_accum,
+                                    const int *place_ones, const int *place_multi,
+                                    const int *count_multi, long long n_data, const int *fstate,
+                                    const int *frot, const double *rot_cs, long long size,
+                                    const int *mask_idx, long long n_mask, long long n_ref,
+                                    int *hist, int *err, cudaStream_t stream) {
+    if (n_data <= 0 || size <= 1 || size > 46340 || n_mask < 0 || n_ref <= 0 || !hist ||
+        !mask_idx || !fstate || !frot || !rot_cs)
+        return RSPI_ERR_ARG;
+    k_histogram<<<rspi_blocks(n_data * 32, 256), 256, 0, stream>>>(
+        ones, multi, ones_accum, multi_accum, place_ones, place_multi, count_multi, n_data,
+        fstate, frot, rot_cs, (int)size, mask_idx, n_ref, hist, err);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_maxlp_pattern(double *fconv, const int *pixels, const int *hist_row,
+                                  long long n_pix, const int *hist, long long n_ref,
+                                  const int *nstate, long long n_data, const double *ref_params,
+                                  long long size, int rescale_mode, const double *rescale,
+                                  int num_iter, double *rescale_out, cudaStream_t stream) {
+    if (!fconv || !pixels || !hist_row || !hist || !nstate || !ref_params || n_ref <= 0 ||
+        n_data <= 0 || size <= 1 || size > 46340 || n_pix < 0 || n_pix > 0x7fffffffLL ||
+        n_ref > 0x7fffffffLL || num_iter < 0 || (rescale_mode == 1 && !rescale) ||
+        (rescale_mode != 0 && rescale_mode != 1))
+        return RSPI_ERR_ARG;
+    if (n_pix == 0) return RSPI_OK;
+    k_pattern<<<(unsigned)n_pix, PT_THREADS, 0, stream>>>(
+        (double2 *)fconv, pixels, hist_row, hist, n_ref, nstate, n_data, ref_params, (int)size,
+        rescale_mode == 0, rescale, num_iter, rescale_out);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_mean(const double *vals, long long n, double *out, cudaStream_t stream) {
+    if (!vals || !out || n <= 0) return RSPI_ERR_ARG;
+    k_mean<<<1, 1024, 0, stream>>>(vals, n, out);
+    RSPI_RETURN_LAUNCH();
+}

@@ -1,0 +1,93 @@
+// Shared device helpers for the RefSPI-MaxLP sm_100a kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "rspi.h"
+
+#define RSPI_FULL_MASK 0xffffffffu
+
+// Launch-status check used by every C-ABI wrapper.
+#define RSPI_RETURN_LAUNCH()                          \
+    do {                                              \
+        cudaError_t e_ = cudaGetLastError();          \
+        return e_ == cudaSuccess ? RSPI_OK : RSPI_ERR_CUDA; \
+    } while (0)
+
+// First error wins; the caller reads the word after synchronising.
+__device__ __forceinline__ void rspi_flag(int *err, int code) {
+    if (err) atomicCAS(err, 0, code);
+}
+
+// IEEE double operations that the compiler may not contract into FMAs.  Used
+// wherever an integer result (a pixel index, a floor or a rint) depends on
+// the rounding of an expression, so it matches the FP64 restatement exactly.
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(RSPI_FULL_MASK, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int warp_max_int(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(RSPI_FULL_MASK, v, o));
+    return v;
+}
+
+// Argmax order of NumPy/CuPy: a NaN beats every number (the first NaN wins),
+// otherwise the larger value wins and ties go to the smaller index.
+__device__ __forceinline__ bool argmax_better(double a, int ia, double b, int ib) {
+    bool na = isnan(a), nb = isnan(b);
+    if (na || nb) {
+        if (na && nb) return ia < ib;
+        return na;
+    }
+    if (a != b) return a > b;
+    return ia < ib;
+}
+
+// Block-wide sum of one double per thread; every thread gets the result.
+// `scratch` holds >= 32 doubles.  Fixed reduction order (deterministic).
+__device__ __forceinline__ double block_sum(double v, double *scratch) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    v = warp_sum(v);
+    __syncthreads();
+    if (lane == 0) scratch[wid] = v;
+    __syncthreads();
+    double t = 0.;
+    if (wid == 0) {
+        t = lane < nw ? scratch[lane] : 0.;
+        t = warp_sum(t);
+        if (lane == 0) scratch[0] = t;
+    }
+    __syncthreads();
+    t = scratch[0];
+    __syncthreads();
+    return t;
+}
+
+static inline int rspi_sm_count() {
+    static int count = 0;
+    if (count == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+        if (count <= 0) count = 148;
+    }
+    return count;
+}
+
+static inline unsigned rspi_blocks(long long work, int threads, int cap_per_sm = 8) {
+    long long b = (work + threads - 1) / threads;
+    long long cap = (long long)rspi_sm_count() * cap_per_sm;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (unsigned)b;
+}

@@ -1,0 +1,156 @@
+// Model slicing (rows a4, a5, a6): holographic slices of every
+// (shift, diameter) state, their masked sums, vscale, and the rotated
+// log-slices on the likelihood pixels.  FP64 throughout; the rotated slices
+// are stored as float32 or float64.
+#include "rspi_common.cuh"
+
+namespace {
+
+constexpr int HOLO_THREADS = 256;
+constexpr double PI = 3.14159265358979311599796346854;  // the double nearest pi
+
+// W[s0][p] = |M(p) + ff(s)*e^{i phase}|^2 + bg(p)   (kernels.cu:58-75)
+// phase = 2 pi ((x-cen) sx + (y-cen) sy) / size,  s = sqrt(r2) pi dia / size.
+// Operations follow the source order; |z|^2 is re*re + im*im.
+__device__ __forceinline__ double holo_value(const double2 m, double dx, double dy, double sx,
+                                             double sy, double dia, double size, double bg) {
+    const double phase = xmul(2. * PI, xadd(xmul(dx, sx), xmul(dy, sy))) / size;
+    double s = xmul(xmul(sqrt(xadd(xmul(dx, dx), xmul(dy, dy))), PI), dia) / size;
+    if (s == 0.) s = 1.e-5;
+    const double sphere = (1.0 * xsub(sin(s), xmul(s, cos(s)))) / xmul(xmul(s, s), s);
+    const double re = xadd(xmul(cos(phase), sphere), m.x);
+    const double im = xadd(xmul(sin(phase), sphere), m.y);
+    return xadd(xadd(xmul(re, re), xmul(im, im)), bg);
+}
+
+__global__ void __launch_bounds__(HOLO_THREADS)
+k_holo(const double2 *__restrict__ model, const double *__restrict__ shiftx,
+       const double *__restrict__ shifty, const double *__restrict__ sphere_dia, long long size,
+       const double *__restrict__ bg, const int *__restrict__ sel_pix, long long n_sel,
+       double *__restrict__ holo, double *__restrict__ msum) {
+    __shared__ double scratch[32];
+    const long long s0 = blockIdx.x;
+    const long long npix = size * size;
+    const double sx = shiftx[s0], sy = shifty[s0], dia = sphere_dia[s0];
+    const double cen = floor(size / 2.);
+    const double dsize = (double)size;
+    double *w = holo + s0 * npix;
+    for (long long p = threadIdx.x; p < npix; p += blockDim.x) {
+        const long long x = p / size, y = p - x * size;
+        w[p] = holo_value(model[p], (double)x - cen, (double)y - cen, sx, sy, dia, dsize, bg[p]);
+    }
+    __syncthreads();
+    double acc = 0.;
+    for (long long c = threadIdx.x; c < n_sel; c += blockDim.x) acc += w[sel_pix[c]];
+    acc = block_sum(acc, scratch);
+    if (threadIdx.x == 0) msum[s0] = acc;
+}
+
+// vscale = sum_sel powder / sum_s0 msum * S0 ; init = -(msum * vscale)  (emc.py:181,199)
+__global__ void __launch_bounds__(1024)
+k_vscale_init(const double *__restrict__ msum, long long n_states0,
+              const double *__restrict__ powder, const int *__restrict__ sel_pix, long long n_sel,
+              double *__restrict__ vscale, double *__restrict__ init) {
+    __shared__ double scratch[32];
+    double a = 0., b = 0.;
+    for (long long c = threadIdx.x; c < n_sel; c += blockDim.x) a += powder[sel_pix[c]];
+    for (long long s = threadIdx.x; s < n_states0; s += blockDim.x) b += msum[s];
+    a = block_sum(a, scratch);
+    b = block_sum(b, scratch);
+    const double vs = a / b * (double)n_states0;
+    if (threadIdx.x == 0) *vscale = vs;
+    for (long long s = threadIdx.x; s < n_states0; s += blockDim.x) init[s] = -(msum[s] * vs);
+}
+
+// One rotated log-slice value (kernels.cu:19-41 with log_flag = 1, scale = 1).
+__device__ __forceinline__ double rot_log_value(const double *__restrict__ w, int x, int y,
+                                                int size, double ac, double as, double bg) {
+    const int cen = size / 2;
+    const double xc = (double)(x - cen), yc = (double)(y - cen);
+    const double tx = xadd(xsub(xmul(xc, ac), xmul(yc, as)), (double)cen);
+    const double ty = xadd(xadd(xmul(xc, as), xmul(yc, ac)), (double)cen);
+    const double fxl = floor(tx), fyl = floor(ty);
+    if (fxl < 0. || fxl > size - 2 || fyl < 0. || fyl > size - 2) return -1000.;
+    const int ix = (int)fxl, iy = (int)fyl;
+    const double fx = tx - fxl, fy = ty - fyl;
+    const double cx = 1. - fx, cy = 1. - fy;
+    const double *r0 = w + (long long)ix * size + iy;
+    const double *r1 = r0 + size;
+    double v = xmul(xmul(r0[0], cx), cy);
+    v = xadd(v, xmul(xmul(r1[0], fx), cy));
+    v = xadd(v, xmul(xmul(r0[1], cx), fy));
+    v = xadd(v, xmul(xmul(r1[1], fx), fy));
+    v = xadd(v, bg);
+    return v < 1.e-20 ? -1000. : log(v);
+}
+
+template <typename TL>
+__global__ void __launch_bounds__(256)
+k_rot_log(const double *__restrict__ holo, long long num_rot, const double *__restrict__ rot_cs,
+          int size, const double *__restrict__ bg, const int *__restrict__ sel_pix,
+          long long n_sel, long long p_pad, long long row_begin, long long n_rows,
+          TL *__restrict__ out) {
+    const long long npix = (long long)size * size;
+    const long long total = n_rows * p_pad;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const long long rr = i / p_pad, c = i - rr * p_pad;
+        double v = 0.;
+        if (c < n_sel) {
+            const long long r = row_begin + rr;
+            const long long s0 = r / num_rot, j = r - s0 * num_rot;
+            const int p = sel_pix[c];
+            const int x = p / size, y = p - (p / size) * size;
+            v = rot_log_value(holo + s0 * npix, x, y, size, rot_cs[2 * j], rot_cs[2 * j + 1],
+                              bg[p]);
+        }
+        out[i] = (TL)v;
+    }
+}
+
+}  // namespace
+
+extern "C" int rspi_holo_slices(const double *model, const double *shiftx, const double *shifty,
+                                const double *sphere_dia, long long n_states0, long long size,
+                                const double *bg, const int *sel_pix, long long n_sel,
+                                double *holo, double *msum, cudaStream_t stream) {
+    if (n_states0 <= 0 || size <= 1 || n_sel < 0 || !model || !holo || !msum || !bg)
+        return RSPI_ERR_ARG;
+    if (n_states0 > 0x7fffffffLL) return RSPI_ERR_ARG;
+    k_holo<<<(unsigned)n_states0, HOLO_THREADS, 0, stream>>>(
+        (const double2 *)model, shiftx, shifty, sphere_dia, size, bg, sel_pix, n_sel, holo, msum);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_vscale_init(const double *msum, long long n_states0, const double *powder,
+                                const int *sel_pix, long long n_sel, double *vscale,
+                                double *init, cudaStream_t stream) {
+    if (n_states0 <= 0 || n_sel < 0 || !msum || !powder || !vscale || !init) return RSPI_ERR_ARG;
+    k_vscale_init<<<1, 1024, 0, stream>>>(msum, n_states0, powder, sel_pix, n_sel, vscale, init);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_rot_log_slices(const double *holo, long long n_states0, long long num_rot,
+                                   const double *rot_cs, long long size, const double *bg,
+                                   const int *sel_pix, long long n_sel, long long p_pad,
+                                   long long row_begin, long long row_end, void *lslices,
+                                   int out_dtype, cudaStream_t stream) {
+    if (n_states0 <= 0 || num_rot <= 0 || size <= 1 || size > 46340 || p_pad < n_sel ||
+        p_pad % 32 || row_begin < 0 || row_end > n_states0 * num_rot || row_end < row_begin ||
+        !holo || !rot_cs || !bg || !lslices)
+        return RSPI_ERR_ARG;
+    const long long n_rows = row_end - row_begin;
+    if (n_rows == 0) return RSPI_OK;
+    const unsigned blocks = rspi_blocks(n_rows * p_pad, 256, 16);
+    if (out_dtype == 0)
+        k_rot_log<float><<<blocks, 256, 0, stream>>>(holo, num_rot, rot_cs, (int)size, bg, sel_pix,
+                                                     n_sel, p_pad, row_begin, n_rows,
+                                                     (float *)lslices);
+    else if (out_dtype == 1)
+        k_rot_log<double><<<blocks, 256, 0, stream>>>(holo, num_rot, rot_cs, (int)size, bg,
+                                                      sel_pix, n_sel, p_pad, row_begin, n_rows,
+                                                      (double *)lslices);
+    else
+        return RSPI_ERR_ARG;
+    RSPI_RETURN_LAUNCH();
+}

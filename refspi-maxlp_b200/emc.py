@@ -1,0 +1,187 @@
+#!/usr/bin/env python
+"""EMC reconstructor on one B200 -- drop-in for the reference ``emc.py``.
+
+``EMC(config_file, num_streams=4)`` reads the same ``[emc]`` keys
+(emc.py:57-80), builds the same state grid and masks (emc.py:67-98) and keeps
+the reference's attributes and methods: ``run_iteration(iternum=None)``,
+``_calculate_prob``, ``_get_rmax``, ``_unravel_rmax``, ``save_output``,
+``_random_model``, ``ramp``, ``sphere``; ``model`` is a host complex128
+array and ``rmax`` a host int32 array, as in the reference.  The E-step and
+the MaxLP M-step run in librspi on the GPU; ``prob`` is a torch CUDA tensor
+(rows ``s*num_rot + j``, columns frames).
+
+Optional ``[emc]`` keys beyond the reference: ``precision`` (``fp64``:
+FP64 slices and likelihoods, the default; ``fp32``: FP32 slices and
+likelihood matrix with FP64 accumulation), ``states_per_tile``,
+``warps_per_cta``, ``phaser_iter`` (default 10, maxLP.py:320,335).
+"""
+import configparser
+import os.path as op
+import sys
+import time
+
+import numpy as np
+import torch
+
+sys.path.insert(0, op.dirname(op.abspath(__file__)))
+from dset import Dataset  # noqa: E402
+from maxLP import MaxLPhaser  # noqa: E402
+from rspi import geometry  # noqa: E402
+from rspi.device import EStep  # noqa: E402
+
+P_MIN = 1.e-6   # emc.py:20
+
+
+class EMC():
+    '''Reconstructor object using parameters from config file
+
+    Args:
+        config_file (str): Path to configuration file
+        num_streams (int): accepted for compatibility; all work is issued on
+            torch's current CUDA stream
+    '''
+    def __init__(self, config_file, num_streams=4, device=None):
+        self.num_streams = num_streams
+        self.rank = 0
+        self.num_proc = 1
+        self.device = torch.device('cuda', torch.cuda.current_device()) if device is None \
+            else torch.device(device)
+        self.mem_size = torch.cuda.get_device_properties(self.device).total_memory
+
+        config = configparser.ConfigParser()
+        config.read(config_file)
+        self._parse_params(config, op.dirname(config_file))
+        self._generate_states(config)
+        self._generate_masks()
+
+        self._parse_data()
+        self.phaser = MaxLPhaser(self.photons_file, size=self.size, dataset=self.dset,
+                                 num_iter=self.phaser_iter)
+        self._init_model()
+
+        self.estep = EStep(self.dset.photons, self.size, self.num_rot, self.shiftx,
+                           self.shifty, self.sphere_dia, self.probmask,
+                           self.dset.bg.cpu().numpy(), slice_dtype=self.slice_dtype,
+                           prob_dtype=self.prob_dtype, states_per_tile=self.states_per_tile,
+                           warps=self.warps_per_cta)
+        self.prob = self.estep.prob
+        self.state_vals = torch.from_numpy(self._state_values).to(self.device)
+        self.phaser_rot = torch.from_numpy(geometry.phaser_rotation_table(
+            np.arange(self.num_rot) * np.pi / self.num_rot)).to(self.device)
+        self.rmax = None
+
+    def _parse_params(self, config, start_dir):
+        '''emc.py:57-65, plus the optional precision/tiling keys'''
+        self.size = config.getint('emc', 'size')
+        self.num_modes = config.getint('emc', 'num_modes', fallback=1)
+        self.num_rot = config.getint('emc', 'num_rot')
+        self.photons_file = op.join(start_dir, config.get('emc', 'in_photons_file'))
+        self.output_folder = op.join(start_dir, config.get('emc', 'output_folder'))
+        self.log_file = op.join(start_dir, config.get('emc', 'log_file'))
+        self.need_scaling = config.getboolean('emc', 'need_scaling', fallback=False)
+        precision = config.get('emc', 'precision', fallback='fp64')
+        if precision not in ('fp64', 'fp32'):
+            raise ValueError('emc:precision must be fp64 or fp32')
+        self.slice_dtype = self.prob_dtype = 'f64' if precision == 'fp64' else 'f32'
+        self.states_per_tile = config.getint('emc', 'states_per_tile', fallback=0) or None
+        self.warps_per_cta = config.getint('emc', 'warps_per_cta', fallback=32)
+        self.phaser_iter = config.getint('emc', 'phaser_iter', fallback=10)
+
+    def _generate_states(self, config):
+        '''emc.py:67-87'''
+        dia = geometry.parse_triple(config.get('emc', 'sphere_dia'))
+        sx = geometry.parse_triple(config.get('emc', 'shiftx'))
+        sy = geometry.parse_triple(config.get('emc', 'shifty'))
+        self.shiftx, self.shifty, self.sphere_dia, self.num_states = geometry.state_grid(sx, sy, dia)
+        print(self.num_states.prod(), 'sampled states')
+        self.x_ind, self.y_ind, self.rad = geometry.detector_radius(self.size)
+        self._state_values = geometry.state_values(self.shiftx, self.shifty, self.sphere_dia,
+                                                   self.num_states)
+
+    def _generate_masks(self):
+        '''emc.py:89-98'''
+        self.invmask, self.probmask = geometry.emc_masks(self.size)
+        self.intinvmask = self.invmask.astype('i4')
+
+    def _parse_data(self):
+        '''emc.py:109-118'''
+        stime = time.time()
+        self.dset = Dataset(self.photons_file, self.size ** 2, self.need_scaling,
+                            device=self.device)
+        self.powder = self.dset.get_powder()
+        etime = time.time()
+        print('%d frames with %.3f photons/frame (%.3f s) (%.2f MB)' %
+              (self.dset.num_data, self.dset.mean_count, etime - stime, self.dset.mem / 1024 ** 2))
+        sys.stdout.flush()
+
+    def _init_model(self):
+        '''emc.py:120-132'''
+        self._random_model()
+        np.save(op.join(self.output_folder, 'model_000.npy'), self.model)
+        self.scales = self.dset.photons.scales
+
+    def run_iteration(self, iternum=None):
+        '''Run one iteration of EMC: likelihoods of every state, most likely
+        state per frame, MaxLP M-step, output (emc.py:134-157)'''
+        dmodel = torch.from_numpy(np.ascontiguousarray(self.model.ravel(), dtype=np.complex128)).to(self.device)
+        self._calculate_prob(dmodel, None)
+        self._get_rmax()
+        self.phaser.run_from_rmax(dmodel, self.estep.rmax, self.num_rot, self.state_vals,
+                                  self.phaser_rot)
+        self.model = dmodel.cpu().numpy()
+        self.dset.photons.err.check('EMC iteration')
+        self.save_output(self.model, iternum)
+
+    def _calculate_prob(self, dmodel, views=None, drange=None):
+        '''Likelihood of every frame in every state into ``prob``
+        (emc.py:159-205 with calc_prob_all, kernels.cu:116-137)'''
+        if drange is not None and tuple(drange) != (0, self.dset.num_data):
+            raise ValueError('frame ranges are not supported: all frames are processed')
+        self.estep.run(dmodel)
+        return self.prob
+
+    def _get_rmax(self):
+        '''First-index argmax per frame (emc.py:207-216; one rank)'''
+        maxll, rmax, logz = self.estep.reduce()
+        self.max_exp = maxll
+        self.logz = logz
+        self.rmax = rmax.cpu().numpy().astype('i4')
+
+    def _unravel_rmax(self, rmax):
+        '''Grid values of the chosen states (emc.py:218-224)'''
+        rmax = np.asarray(rmax)
+        s0 = rmax // self.num_rot
+        ang = rmax % self.num_rot
+        vals = self._state_values[s0]
+        return vals[:, 0], vals[:, 1], vals[:, 2], ang * np.pi / self.num_rot
+
+    def save_output(self, model, iternum, intens=None):
+        '''``model.npy``, or ``output_%03d`` with the datasets model, angles,
+        diameters, shifts and optional intens (emc.py:226-239)'''
+        if iternum is None:
+            np.save(op.join(self.output_folder, 'model.npy'), self.model)
+            return
+        sx_vals, sy_vals, dia_vals, ang_vals = self._unravel_rmax(self.rmax)
+        out = {'model': np.asarray(self.model).reshape((self.size,) * 2),
+               'angles': ang_vals, 'diameters': dia_vals,
+               'shifts': np.array([sx_vals, sy_vals]).T}
+        if intens is not None:
+            out['intens'] = intens.cpu().numpy() if torch.is_tensor(intens) else np.asarray(intens)
+        path = op.join(self.output_folder, 'output_%.3d.npz' % iternum)
+        with open(path, 'wb') as fh:
+            np.savez(fh, **out)
+
+    def _random_model(self):
+        '''emc.py:241-242'''
+        self.model = np.random.random(self.size ** 2) + 1j * np.random.random(self.size ** 2)
+
+    def ramp(self, n):
+        '''Shift phase ramp of state n (emc.py:244-245)'''
+        return np.exp(1j * 2. * np.pi * (self.x_ind * self.shiftx[n] + self.y_ind * self.shifty[n]) / self.size)
+
+    def sphere(self, n, diameter=None):
+        '''Sphere form factor of state n or of a diameter (emc.py:247-254)'''
+        dia = diameter if n is None else self.sphere_dia[n]
+        s = np.pi * self.rad * dia / self.size
+        s[s == 0] = 1.e-5
+        return ((np.sin(s) - s * np.cos(s)) / s ** 3).ravel()

@@ -1,0 +1,85 @@
+"""ctypes binding of librspi.so (the C ABI declared in include/rspi.h).
+
+The library is the only compute path: if it is missing or fails to load,
+``load()`` raises.  There is no CPU fallback.
+"""
+import ctypes
+import os
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'librspi.so')
+
+P = ctypes.c_void_p
+L = ctypes.c_longlong
+I = ctypes.c_int
+D = ctypes.c_double
+
+# name: (restype, argtypes) -- mirrors include/rspi.h
+SIGNATURES = {
+    'rspi_version': (ctypes.c_char_p, []),
+    'rspi_status_string': (ctypes.c_char_p, [I]),
+    'rspi_photon_offsets': (I, [P, P, P, L, P, P, P, P, P, P, I, P, P]),
+    'rspi_powder': (I, [P, L, P, P, L, L, L, P, P, P]),
+    'rspi_ll_entry_rows': (I, [P, P, P, P, P, P, P, P, L, L, P, P, P, P]),
+    'rspi_scan_rows': (I, [P, L, P, P]),
+    'rspi_ll_entry_fill': (I, [P, P, P, P, P, P, P, P, L, L, P, P, P, P]),
+    'rspi_holo_slices': (I, [P, P, P, P, L, L, P, P, L, P, P, P]),
+    'rspi_vscale_init': (I, [P, L, P, P, L, P, P, P]),
+    'rspi_rot_log_slices': (I, [P, L, L, P, L, P, P, L, L, L, L, P, I, P]),
+    'rspi_loglike': (I, [P, I, L, L, P, P, P, P, P, L, L, L, P, I, L, I, I, I, P]),
+    'rspi_loglike_max_tile': (I, [L, I]),
+    'rspi_frame_reduce': (I, [P, I, L, L, P, P, P, P]),
+    'rspi_maxlp_frame_params': (I, [P, L, L, L, P, P, P, P, P]),
+    'rspi_maxlp_histogram': (I, [P, P, P, P, P, P, P, L, P, P, P, L, P, L, L, P, P, P]),
+    'rspi_maxlp_pattern': (I, [P, P, P, L, P, L, P, L, P, L, I, P, I, P, P]),
+    'rspi_mean': (I, [P, L, P, P]),
+}
+
+_lib = None
+
+
+class RspiError(RuntimeError):
+    pass
+
+
+def load():
+    """Load and type the library once; raise if it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RspiError('librspi.so is not built (%s); run __graft_entry__.build() or '
+                        'python refspi-maxlp_b200/csrc/build.py' % LIB_PATH)
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def status_string(code):
+    return load().rspi_status_string(int(code)).decode()
+
+
+def check(code, what):
+    if code != 0:
+        raise RspiError('%s failed: %s (%d)' % (what, status_string(code), code))
+
+
+# kernels each entry point launches (memsets are not counted)
+KERNELS_PER_CALL = {
+    'rspi_photon_offsets': 4, 'rspi_powder': 2, 'rspi_ll_entry_rows': 1, 'rspi_scan_rows': 1,
+    'rspi_ll_entry_fill': 1, 'rspi_holo_slices': 1, 'rspi_vscale_init': 1,
+    'rspi_rot_log_slices': 1, 'rspi_loglike': 1, 'rspi_frame_reduce': 1,
+    'rspi_maxlp_frame_params': 1, 'rspi_maxlp_histogram': 1, 'rspi_maxlp_pattern': 1,
+    'rspi_mean': 1,
+}
+launch_count = 0
+
+
+def call(name, *args):
+    """Call entry point ``name``, raise on a non-zero status, count launches."""
+    global launch_count
+    check(getattr(load(), name)(*args), name)
+    launch_count += KERNELS_PER_CALL.get(name, 0)

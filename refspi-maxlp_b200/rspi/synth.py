@@ -149,17 +149,18 @@ def generate(size, num_data, mean_count, n_blobs=20, obj_radius=12.,
         hi = min(num_data, lo + chunk)
         w = intens(lo, hi) * (gfac * torch.from_numpy(scale[lo:hi]).to(dev))[:, None]
         rot = _rotate_bilinear(w, torch.from_numpy(angles[lo:hi]).to(dev), size)
-        cnt = torch.poisson(rot, generator=gen).to(torch.int32).cpu().numpy()
+        cnt = torch.poisson(rot, generator=gen).to(torch.int32)
         if dense:
-            frames[lo:hi] = np.minimum(cnt, 65535).astype(np.uint16)
-        for i in range(hi - lo):
-            f = cnt[i]
-            o = np.flatnonzero(f == 1).astype('i4')
-            m = np.flatnonzero(f > 1).astype('i4')
-            po.append(o)
-            pm.append(m)
-            cm.append(f[m].astype('i4'))
-            ones[lo + i], multi[lo + i] = o.size, m.size
+            frames[lo:hi] = cnt.clamp(max=65535).cpu().numpy().astype(np.uint16)
+        # row-major nonzeros: frame by frame, pixels ascending (np.flatnonzero order)
+        nz = torch.nonzero(cnt)
+        val = cnt[nz[:, 0], nz[:, 1]]
+        one = val == 1
+        ones[lo:hi] = torch.bincount(nz[one, 0], minlength=hi - lo).cpu().numpy()
+        multi[lo:hi] = torch.bincount(nz[~one, 0], minlength=hi - lo).cpu().numpy()
+        po.append(nz[one, 1].to(torch.int32).cpu().numpy())
+        pm.append(nz[~one, 1].to(torch.int32).cpu().numpy())
+        cm.append(val[~one].cpu().numpy().astype('i4'))
     cat = lambda a: np.concatenate(a) if a else np.zeros(0, 'i4')  # noqa: E731
     out = dict(num_pix=np.array([size * size]), ones=ones, multi=multi,
                place_ones=cat(po), place_multi=cat(pm), count_multi=cat(cm),

@@ -134,9 +134,11 @@ def run_case(name, c):
                 out['rescale_%d' % it] = np.array(float(resc[-1].split(':')[1]))
 
             # phaser pieces on the state left by iteration 2
+            import cupy as cp   # the stand-in
             ph = rec.phaser
             pix = np.where(np.asarray(ph.mask))[0]
             pick = pix[np.linspace(0, pix.size - 1, 5).astype(int)]
+            pick = np.concatenate([pick, pix[np.argsort(-np.asarray(rec.powder)[pix])[:3]]])
             k_l, fr_l, lq_l, rs_l, cand_l = [], [], [], [], []
             for t in pick:
                 const = ph.get_pixel_constants(int(t))
@@ -144,8 +146,8 @@ def run_case(name, c):
                 cand = f_t + np.asarray(ph.pattern) * (abs(f_t) / 4.)
                 k_l.append(np.asarray(const['k_d']).ravel())
                 fr_l.append(np.asarray(const['fref_d']))
-                rs_l.append(np.asarray(ph.get_rescale_pixel(cand.view(type(np.asarray(ph.pattern))), int(t), const)))
-                lq_l.append(np.asarray(ph.get_logq_pixel(cand.view(type(np.asarray(ph.pattern))), int(t),
+                rs_l.append(np.asarray(ph.get_rescale_pixel(cp.asarray(cand), int(t), const)))
+                lq_l.append(np.asarray(ph.get_logq_pixel(cp.asarray(cand), int(t),
                                                          rescale=None, const=const)))
                 cand_l.append(cand)
             out.update(ph_pixels=pick, ph_k=np.array(k_l), ph_fref=np.array(fr_l),

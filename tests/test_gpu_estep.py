@@ -1,0 +1,209 @@
+"""E-step parity on the GPU (rows a1-a9): librspi vs the pinned FP64 oracle
+and the reference goldens.  Integer results (prefix sums, counts, powder,
+entry lists, argmax) are compared bit-exactly; floating point within the
+stated tolerances."""
+import numpy as np
+import pytest
+import torch
+
+from helpers import GOLDEN_CASES, golden_dataset, golden_states, load_golden, random_photons
+from oracle import emc_oracle as E
+
+pytestmark = pytest.mark.gpu
+
+# FP64 pipeline vs FP64 oracle: only summation order differs
+RTOL_F64 = 1e-11
+# FP32 slices (FP64 accumulation): north-star bound on the likelihood
+RTOL_F32 = 1e-5
+
+
+def _photons(ds, need_scaling):
+    from rspi.device import DevicePhotons
+    return DevicePhotons(ds['ones'], ds['multi'], ds['place_ones'], ds['place_multi'],
+                         ds['count_multi'], ds['num_pix'], need_scaling)
+
+
+def _estep(ph, size, num_rot, sx, sy, dia, bg, **kw):
+    from rspi.device import EStep
+    _, pm = E.generate_masks(size)
+    return EStep(ph, size, num_rot, sx, sy, dia, pm, bg, **kw)
+
+
+def _cases():
+    out = []
+    for name in GOLDEN_CASES:
+        g = load_golden(name)
+        out.append((name, golden_dataset(g), bool(g['need_scaling'])))
+    for size, n, seed, kw in ((17, 1, 1, {}), (37, 33, 2, dict(empty_frames=(0, 5), masked_frames=(7,))),
+                              (25, 40, 3, dict(heavy=3))):
+        d = random_photons(size, n, 30. * size, seed, **kw)
+        ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
+                             d['count_multi'], size * size, True)
+        out.append(('rand%d' % size, ds, True))
+    return out
+
+
+CASES = _cases()
+
+
+@pytest.mark.parametrize('name,ds,need_scaling', CASES, ids=[c[0] for c in CASES])
+def test_photon_setup_bit_exact(name, ds, need_scaling):
+    ph = _photons(ds, need_scaling)
+    assert np.array_equal(ph.ones_accum.cpu().numpy(), ds['ones_accum'])
+    assert np.array_equal(ph.multi_accum.cpu().numpy(), ds['multi_accum'])
+    assert ph.mean_count == ds['mean_count']
+    if need_scaling:
+        assert np.array_equal(ph.counts.cpu().numpy(), ds['counts'])
+    assert np.array_equal(ph.scales.cpu().numpy(), E.get_scales(ds, need_scaling))
+    assert np.array_equal(ph.powder.cpu().numpy(), E.get_powder(ds))
+
+
+@pytest.mark.parametrize('name,ds,need_scaling', CASES, ids=[c[0] for c in CASES])
+def test_ll_entry_lists_bit_exact(name, ds, need_scaling):
+    from rspi import geometry
+    size = int(round(np.sqrt(ds['num_pix'])))
+    ph = _photons(ds, need_scaling)
+    _, pm = E.generate_masks(size)
+    sel, pix2sel, p_pad = geometry.sel_pixels(pm)
+    ll = ph.ll_entries(torch.from_numpy(pix2sel).cuda(), p_pad)
+    ent = ll['entries'].cpu().numpy().view(np.uint32).reshape(-1, 32)
+    off = ll['row_off'].cpu().numpy()
+    kmat = E.sparse_frames(ds, pm < 1)
+    for d in range(ds['num_data']):
+        rows = ent[off[d]:off[d + 1]]
+        c = (rows >> 16).astype(np.int64)
+        k = (rows & 0xffff).astype(np.int64)
+        lanes = np.broadcast_to(np.arange(32), rows.shape)
+        assert np.all(c % 32 == lanes)               # bank-conflict-free layout
+        got = np.zeros(sel.size + 32, dtype=np.int64)
+        np.add.at(got, c[k > 0], k[k > 0])
+        want = np.zeros(sel.size + 32, dtype=np.int64)
+        row = kmat.getrow(d)
+        want[row.indices] = row.data.astype(np.int64)
+        assert np.array_equal(got, want), d
+    order = ll['order'].cpu().numpy()
+    rows = ll['frame_rows'].cpu().numpy()
+    assert np.all(np.diff(rows[order]) <= 0)
+
+
+def _golden_estep(g, **kw):
+    ds = golden_dataset(g)
+    size, num_rot = int(g['size']), int(g['num_rot'])
+    sx, sy, dia, _ = golden_states(g)
+    ph = _photons(ds, bool(g['need_scaling']))
+    return ds, _estep(ph, size, num_rot, sx, sy, dia, ds['bg'], **kw)
+
+
+@pytest.mark.parametrize('name', GOLDEN_CASES)
+def test_holo_msum_vscale(name):
+    g = load_golden(name)
+    ds, es = _golden_estep(g)
+    size = int(g['size'])
+    sx, sy, dia, _ = golden_states(g)
+    model = torch.from_numpy(g['model0']).cuda()
+    es.slices(model)
+    holo = es.holo.cpu().numpy()
+    np.testing.assert_allclose(holo[:g['holo'].shape[0]], g['holo'], rtol=1e-13)
+    _, pm = E.generate_masks(size)
+    msums, vscale = E.msum_vscale(g['model0'], sx, sy, dia, size, ds['bg'], pm, E.get_powder(ds))
+    np.testing.assert_allclose(es.msum.cpu().numpy(), msums, rtol=1e-13)
+    np.testing.assert_allclose(float(es.vscale), vscale, rtol=1e-13)
+
+
+@pytest.mark.parametrize('name', GOLDEN_CASES)
+@pytest.mark.parametrize('dtype', ['f64', 'f32'])
+def test_rotated_log_slices(name, dtype):
+    g = load_golden(name)
+    ds, es = _golden_estep(g, slice_dtype=dtype, prob_dtype=dtype)
+    size, num_rot = int(g['size']), int(g['num_rot'])
+    sx, sy, dia, _ = golden_states(g)
+    es.slices(torch.from_numpy(g['model0']).cuda())
+    es.rot_slices(0, es.chunk_rows)
+    lsl = es.lsl.double().cpu().numpy()
+    _, pm = E.generate_masks(size)
+    sel = pm < 1
+    for r in range(min(es.chunk_rows, 3 * num_rot)):
+        s0, j = divmod(r, num_rot)
+        w = E.holo_slice(g['model0'], sx[s0], sy[s0], dia[s0], 1., 1., size, ds['bg'])
+        want = E.rotate_slice(w, j * np.pi / num_rot, 1., size, ds['bg'], 1)[sel]
+        got = lsl[r, :sel.sum()]
+        if dtype == 'f64':
+            np.testing.assert_allclose(got, want, rtol=1e-13, atol=1e-13)
+        else:
+            np.testing.assert_allclose(got, want.astype(np.float32), rtol=1e-6, atol=1e-6)
+        assert np.all(lsl[r, sel.sum():] == 0)
+
+
+@pytest.mark.parametrize('name', GOLDEN_CASES)
+@pytest.mark.parametrize('it', [1, 2])
+def test_loglike_fp64_matches_reference(name, it):
+    g = load_golden(name)
+    _, es = _golden_estep(g)
+    es.run(torch.from_numpy(g['model_in_%d' % it]).cuda())
+    prob = es.prob.cpu().numpy()
+    np.testing.assert_allclose(prob, g['prob_%d' % it], rtol=RTOL_F64, atol=0)
+    maxll, rmax, logz = es.reduce()
+    assert np.array_equal(rmax.cpu().numpy(), g['rmax_%d' % it])
+    np.testing.assert_allclose(maxll.cpu().numpy(), g['prob_%d' % it].max(0), rtol=RTOL_F64)
+    want_logz, _ = E.posterior(g['prob_%d' % it])
+    np.testing.assert_allclose(logz.cpu().numpy(), want_logz, rtol=RTOL_F64)
+
+
+@pytest.mark.parametrize('name', GOLDEN_CASES)
+def test_loglike_fp32_slices(name):
+    g = load_golden(name)
+    _, es = _golden_estep(g, slice_dtype='f32', prob_dtype='f64')
+    es.run(torch.from_numpy(g['model_in_1']).cuda())
+    prob = es.prob.cpu().numpy()
+    want = g['prob_1']
+    rel = np.abs(prob - want) / np.abs(want)
+    assert rel.max() <= RTOL_F32, rel.max()
+
+
+@pytest.mark.parametrize('tile,warps', [(1, 1), (2, 4), (3, 32), (1, 7)])
+def test_tiling_does_not_change_results(tile, warps):
+    g = load_golden('case_a')
+    _, ref = _golden_estep(g)
+    ref.run(torch.from_numpy(g['model_in_1']).cuda())
+    _, es = _golden_estep(g, states_per_tile=tile, warps=warps)
+    es.run(torch.from_numpy(g['model_in_1']).cuda())
+    np.testing.assert_allclose(es.prob.cpu().numpy(), ref.prob.cpu().numpy(), rtol=1e-14)
+
+
+def test_chunked_slices_match_single_pass():
+    g = load_golden('case_b')
+    _, ref = _golden_estep(g)
+    ref.run(torch.from_numpy(g['model_in_1']).cuda())
+    _, es = _golden_estep(g, states_per_tile=2, slice_budget_bytes=7 * 32 * 8 * 2)
+    assert es.chunk_rows < es.n_rows
+    es.run(torch.from_numpy(g['model_in_1']).cuda())
+    np.testing.assert_allclose(es.prob.cpu().numpy(), ref.prob.cpu().numpy(), rtol=1e-14)
+
+
+@pytest.mark.parametrize('size,n,seed,kw', [
+    (17, 1, 1, {}),
+    (37, 33, 2, dict(empty_frames=(0, 5), masked_frames=(7,))),
+    (25, 40, 3, dict(heavy=3)),
+    (5, 3, 4, {}),        # no likelihood pixels at all: vscale = 0/0 as in the reference
+])
+def test_random_shapes_vs_oracle(size, n, seed, kw):
+    d = random_photons(size, n, 30. * size, seed, **kw)
+    ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
+                         d['count_multi'], size * size, True)
+    sx, sy, dia, _ = E.generate_states((-1., 1., 2), (0., 1., 2), (2., 3., 2))
+    num_rot = 5
+    ph = _photons(ds, True)
+    es = _estep(ph, size, num_rot, sx, sy, dia, ds['bg'])
+    model = np.random.default_rng(seed).random(size * size) + 1j * np.random.default_rng(seed + 1).random(size * size)
+    es.run(torch.from_numpy(model).cuda())
+    _, pm = E.generate_masks(size)
+    with np.errstate(invalid='ignore', divide='ignore'):
+        want, _, _ = E.calc_prob(model, ds, sx, sy, dia, size, num_rot, pm, E.get_scales(ds, True))
+    got = es.prob.cpu().numpy()
+    if np.isnan(want).all():
+        assert np.isnan(got).all()
+    else:
+        np.testing.assert_allclose(got, want, rtol=RTOL_F64, atol=1e-9)
+    _, rmax, _ = es.reduce()
+    _, want_rmax = E.get_rmax(want)
+    assert np.array_equal(rmax.cpu().numpy(), want_rmax)

@@ -1,0 +1,111 @@
+"""MaxLP M-step parity on the GPU (rows a11-a14) and the end-to-end EMC
+iteration against the reference goldens."""
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from helpers import GOLDEN_CASES, golden_dataset, load_golden, random_photons, write_case
+from oracle import emc_oracle as E
+from oracle import maxlp_oracle as M
+
+pytestmark = pytest.mark.gpu
+
+RTOL_MODEL = 1e-9   # FP64 pattern search: same path, rounding-level differences
+
+
+def _photons(ds, need_scaling=False):
+    from rspi.device import DevicePhotons
+    return DevicePhotons(ds['ones'], ds['multi'], ds['place_ones'], ds['place_multi'],
+                         ds['count_multi'], ds['num_pix'], need_scaling)
+
+
+@pytest.mark.parametrize('name', GOLDEN_CASES)
+def test_histogram_bit_exact(name):
+    """hist[t][s] == sum over frames in state s of the oracle's k_d(t)."""
+    from rspi import geometry
+    from rspi.device import MStep
+    g = load_golden(name)
+    ds = golden_dataset(g)
+    size, num_rot = int(g['size']), int(g['num_rot'])
+    rmax = g['rmax_1']
+    n_ref = int(g['prob_1'].shape[0] // num_rot)
+    ph = _photons(ds)
+    ms = MStep(ph, size)
+    ms.frame_params_from_rmax(torch.from_numpy(rmax).cuda(), num_rot, n_ref)
+    ang = (rmax % num_rot) * np.pi / num_rot
+    rot = torch.from_numpy(geometry.phaser_rotation_table(np.arange(num_rot) * np.pi / num_rot)).cuda()
+    ms.hist = torch.zeros(ms.n_hist_rows * n_ref, dtype=torch.int32, device='cuda')
+    from rspi.device import ptr, cur_stream
+    from rspi.lib import check
+    check(ms.lib.rspi_maxlp_histogram(
+        ptr(ph.ones), ptr(ph.multi), ptr(ph.ones_accum), ptr(ph.multi_accum), ptr(ph.place_ones),
+        ptr(ph.place_multi), ptr(ph.count_multi), ph.num_data, ptr(ms.fstate), ptr(ms.frot),
+        ptr(rot), size, ptr(ms.mask_idx), ms.n_hist_rows, n_ref, ptr(ms.hist), ptr(ph.err.t),
+        cur_stream()), 'hist')
+    hist = ms.hist.cpu().numpy().reshape(ms.n_hist_rows, n_ref)
+    assert np.array_equal(ms.nstate.cpu().numpy(), np.bincount(rmax // num_rot, minlength=n_ref))
+    kmat = E.sparse_frames(ds)
+    qx, qy, _, mask, rmask = M.get_qvals(size)
+    rows = np.flatnonzero(mask | rmask)
+    fstate = rmax // num_rot
+    for m, t in enumerate(rows):
+        k = M.photons_pixel(kmat, ang, int(t), size, qx, qy)
+        want = np.bincount(fstate, weights=k, minlength=n_ref).astype(np.int64)
+        assert np.array_equal(hist[m], want), t
+
+
+@pytest.mark.parametrize('name', GOLDEN_CASES)
+@pytest.mark.parametrize('it', [1, 2])
+def test_run_phaser_matches_reference(name, it, tmp_path):
+    """MaxLPhaser._run_phaser (generic per-frame parameters) vs the goldens."""
+    from maxLP import MaxLPhaser
+    g = load_golden(name)
+    cfg = write_case(str(tmp_path), g)
+    ph = MaxLPhaser(os.path.join(str(tmp_path), 'photons.npz'), size=int(g['size']))
+    out = ph._run_phaser(g['model_in_%d' % it], *g['unravel_%d' % it])
+    np.testing.assert_allclose(out, g['model_out_%d' % it], rtol=RTOL_MODEL, atol=1e-12)
+    del cfg
+
+
+@pytest.mark.parametrize('name', GOLDEN_CASES)
+def test_emc_two_iterations_match_reference(name, tmp_path):
+    from emc import EMC
+    g = load_golden(name)
+    cfg = write_case(str(tmp_path), g)
+    rec = EMC(cfg)
+    rec.model = g['model_in_1'].copy()
+    for it in (1, 2):
+        np.testing.assert_allclose(rec.model, g['model_in_%d' % it], rtol=RTOL_MODEL, atol=1e-12)
+        rec.run_iteration(it)
+        np.testing.assert_allclose(rec.prob.cpu().numpy(), g['prob_%d' % it], rtol=1e-10)
+        assert np.array_equal(rec.rmax, g['rmax_%d' % it])
+        np.testing.assert_allclose(np.stack(rec._unravel_rmax(rec.rmax)), g['unravel_%d' % it],
+                                   rtol=0, atol=0)
+        np.testing.assert_allclose(rec.model, g['model_out_%d' % it], rtol=RTOL_MODEL, atol=1e-12)
+        assert os.path.exists(os.path.join(str(tmp_path), 'out', 'output_%03d.npz' % it))
+
+
+@pytest.mark.parametrize('size', [5, 17, 23])
+def test_phaser_random_vs_oracle(size, tmp_path):
+    """Odd sizes including a ring-only detector (size 5: empty main mask)."""
+    from maxLP import MaxLPhaser
+    from rspi.photonfile import write_photons
+    n = 24
+    d = random_photons(size, n, 20. * size, 10 + size, empty_frames=(2,))
+    path = os.path.join(str(tmp_path), 'p.npz')
+    write_photons(path, d)
+    rng = np.random.default_rng(size)
+    sx = rng.choice([-1., 0., 1.], n)
+    sy = rng.choice([0., 1.], n)
+    dia = rng.choice([2., 3.], n)
+    ang = rng.integers(0, 6, n) * np.pi / 6
+    model = rng.random(size * size) + 1j * rng.random(size * size)
+    ph = MaxLPhaser(path, size=size)
+    got = ph._run_phaser(model, sx, sy, dia, ang)
+    ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
+                         d['count_multi'], size * size)
+    with np.errstate(invalid='ignore', divide='ignore'):
+        want = M.run_phaser(model, E.sparse_frames(ds), sx, sy, dia, ang, size)
+    np.testing.assert_allclose(got, want, rtol=RTOL_MODEL, atol=1e-12)

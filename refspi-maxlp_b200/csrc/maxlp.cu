@@ -386,12 +386,12 @@ extern "C" int rspi_maxlp_pattern(double *fconv, const int *pixels, const int *h
                                   const int *nstate, long long n_data, const double *ref_params,
                                   long long size, int rescale_mode, const double *rescale,
                                   int num_iter, double *rescale_out, cudaStream_t stream) {
+    if (n_pix == 0) return RSPI_OK;  // nothing to search (e.g. an empty ring or mask)
     if (!fconv || !pixels || !hist_row || !hist || !nstate || !ref_params || n_ref <= 0 ||
         n_data <= 0 || size <= 1 || size > 46340 || n_pix < 0 || n_pix > 0x7fffffffLL ||
         n_ref > 0x7fffffffLL || num_iter < 0 || (rescale_mode == 1 && !rescale) ||
         (rescale_mode != 0 && rescale_mode != 1))
         return RSPI_ERR_ARG;
-    if (n_pix == 0) return RSPI_OK;
     k_pattern<<<(unsigned)n_pix, PT_THREADS, 0, stream>>>(
         (double2 *)fconv, pixels, hist_row, hist, n_ref, nstate, n_data, ref_params, (int)size,
         rescale_mode == 0, rescale, num_iter, rescale_out);

@@ -52,7 +52,7 @@ def parse_args():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--config', type=int, default=2, choices=[1, 2])
     ap.add_argument('--frames', type=int, default=None, help='override frame count (testing)')
-    ap.add_argument('--precision', default='fp64', choices=['fp64', 'fp32'])
+    ap.add_argument('--form', default='fp64', choices=['fp64', 'screen'])
     ap.add_argument('--cpu-seconds', type=float, default=20.,
                     help='target CPU time of the bounded oracle sample')
     ap.add_argument('--no-cpu-baseline', action='store_true')
@@ -82,7 +82,7 @@ def workload(cfg_id, frames):
                 n_states=nsx * nsy * nd * r['num_rot'], recon=r)
 
 
-def write_inputs(tmp, w, data, precision):
+def write_inputs(tmp, w, data, form):
     from rspi.photonfile import write_photons
     os.makedirs(os.path.join(tmp, 'out'), exist_ok=True)
     write_photons(os.path.join(tmp, 'photons.npz'), data)
@@ -91,8 +91,8 @@ def write_inputs(tmp, w, data, precision):
     with open(cfg, 'w') as f:
         f.write('[emc]\nsize = %d\nin_photons_file = photons.npz\noutput_folder = out/\n'
                 'log_file = out/EMC.log\nneed_scaling = True\nnum_rot = %d\nnum_modes = 1\n'
-                'sphere_dia = %s\nshiftx = %s\nshifty = %s\nprecision = %s\n' %
-                (w['size'], r['num_rot'], r['sphere_dia'], r['shiftx'], r['shifty'], precision))
+                'sphere_dia = %s\nshiftx = %s\nshifty = %s\nform = %s\n' %
+                (w['size'], r['num_rot'], r['sphere_dia'], r['shiftx'], r['shifty'], form))
     return cfg
 
 
@@ -302,7 +302,7 @@ def run_ours(args):
                           seed=20260000 + args.config, device=dev)
     t_gen = time.time() - t0
     tmp = tempfile.mkdtemp(prefix='rspi_bench_')
-    cfgfile = write_inputs(tmp, w, data, args.precision)
+    cfgfile = write_inputs(tmp, w, data, args.form)
     from emc import EMC
     import contextlib
     import io
@@ -414,7 +414,7 @@ def run_ours(args):
         try:
             with open(prof) as f:
                 pj = json.load(f)
-            traffic = pj.get('%s_%s_bytes_per_row' % (args.precision, 'cfg%d' % args.config))
+            traffic = pj.get('%s_%s_bytes_per_row' % (args.form, 'cfg%d' % args.config))
             if traffic is not None:
                 traffic = float(traffic) * rows_per_launch
         except Exception:
@@ -432,14 +432,14 @@ def run_ours(args):
         'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
         'warmup': args.warmup, 'ms_per_step': ms, 's_per_iteration': ms / 1e3,
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
-        'dtype': 'f64' if args.precision == 'fp64' else 'f32 slices, f64 accumulate',
+        'dtype': 'f64' if args.form == 'fp64' else 'f32 screen + f64 rescore',
         'data': 'synthetic (seeded generator with the configuration\'s shapes)',
         'config': {'workload': 'config%d: %dx%d detector, %d frames, %d rotations x %d (shift,dia) '
                    'states = %d states/frame, 1 EMC iteration per step' %
                    (args.config, w['size'], w['size'], w['n'], w['num_rot'], w['n_states0'],
                     w['n_states']),
                    'frames': w['n'], 'states_per_frame': w['n_states'],
-                   'precision': args.precision, 'parallelism': 'replicas' if world > 1 else 'single',
+                   'form': args.form, 'parallelism': 'replicas' if world > 1 else 'single',
                    'l2': 'inputs larger than L2 (slices %.1f GB, likelihoods %.1f GB per step)' %
                    (es.n_rows * es.p_pad * esz / 1e9, es.n_rows * w['n'] * osz / 1e9)},
         'gpu_launches': launches // args.steps * args.steps,

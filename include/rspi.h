@@ -110,12 +110,14 @@ int rspi_vscale_init(const double *msum, long long n_states0, const double *powd
  *   -1000 outside the detector or below 1e-20; p = sel_pix[c].
  * rot_cs[2*j], rot_cs[2*j+1] = cos, sin of angle j (host table).
  * out_dtype 0 = float32, 1 = float64; rows are p_pad long, tail zeroed.
- * rows [row_begin, row_end) of the full S0*num_rot range are produced. */
+ * rows [row_begin, row_end) of the full S0*num_rot range are produced.
+ * abs_max (nullable, float): raised to the largest |stored value| (the caller
+ * zeroes it); it bounds the rounding error of the float32 form. */
 int rspi_rot_log_slices(const double *holo, long long n_states0, long long num_rot,
                         const double *rot_cs, long long size, const double *bg,
                         const int *sel_pix, long long n_sel, long long p_pad,
                         long long row_begin, long long row_end, void *lslices,
-                        int out_dtype, cudaStream_t stream);
+                        int out_dtype, float *abs_max, cudaStream_t stream);
 
 /* ------------------------------------------------------------------------ a7
  * Log-likelihood of frames x states, replacing calc_prob_all
@@ -135,8 +137,82 @@ int rspi_loglike(const void *lslices, int slice_dtype, long long p_pad, long lon
                  long long ll_stride, int states_per_tile, int warps_per_cta,
                  int n_ctas, cudaStream_t stream);
 
+/* Streaming variant of rspi_loglike (form 1: 32-bit entries, FP64 slices and
+ * output, bit-identical to rspi_loglike) and of rspi_screen_loglike (form 0:
+ * 16-bit entries, FP32 slices and output).  Each warp owns a contiguous range
+ * of frames holding an equal share of the entry words and streams it with a
+ * prefetch across frame boundaries; frames are processed in index order
+ * (no frame_order).  row_off are the entry-row offsets of that form. */
+int rspi_loglike_stream(int form, const void *lslices, long long p_row, long long num_rot,
+                        const double *init, const double *scales, const void *entries,
+                        const long long *row_off, long long n_data, long long row_begin,
+                        long long row_end, void *ll, long long ll_stride, int states_per_tile,
+                        int warps_per_cta, int n_ctas, cudaStream_t stream);
+
 /* Largest states_per_tile whose slices fit in shared memory (0 if none). */
 int rspi_loglike_max_tile(long long p_pad, int slice_dtype);
+
+/* ---------------------------------------------------------- a7 screened form
+ * The chosen likelihood: an FP32 screening pass, candidate selection with a
+ * rigorous error bound, and FP64 rescoring of the candidates (replaces the
+ * same calc_prob_all launches as rspi_loglike, kernels.cu:116-137).
+ *
+ * rspi_ll16_entry_rows / _fill: 16-bit photon entries for the screening
+ * pass.  Each in-mask photon is one entry holding its sel index (a pixel with
+ * k photons gives k entries); lane b of a row holds an index = b mod 32.
+ * frame_rows[d] is even; with row_off = rspi_scan_rows(frame_rows) the word
+ * (pair q, lane b) at entries[q*64 + 2b .. 2b+1] holds rows 2q and 2q+1.
+ * Unused slots hold p_zero + b, where the slice rows are zero
+ * (p_zero = p_row - 32, p_zero >= n_sel, p_row <= 65536). */
+int rspi_ll16_entry_rows(const int *ones, const int *multi, const long long *ones_accum,
+                         const long long *multi_accum, const int *place_ones,
+                         const int *place_multi, const int *count_multi, const int *pix2sel,
+                         long long num_pix, long long n_data, int p_zero, int *frame_rows,
+                         int *err, cudaStream_t stream);
+int rspi_ll16_entry_fill(const int *ones, const int *multi, const long long *ones_accum,
+                         const long long *multi_accum, const int *place_ones,
+                         const int *place_multi, const int *count_multi, const int *pix2sel,
+                         long long num_pix, long long n_data, int p_zero,
+                         const long long *row_off, unsigned short *entries,
+                         cudaStream_t stream);
+
+/* FP32 screening likelihood: LL32[r][d] = float(init[r/num_rot]*scales[d] +
+ * FP32 sum of the frame's FP32 slice values).  Slices of rows
+ * [row_begin, row_end) are read from lslices (p_row floats per row). */
+int rspi_screen_loglike(const float *lslices, long long p_row, long long num_rot,
+                        const double *init, const double *scales,
+                        const unsigned short *entries, const long long *row_off,
+                        const int *frame_order, long long n_data, long long row_begin,
+                        long long row_end, float *ll, long long ll_stride, int states_per_tile,
+                        int warps_per_cta, int n_ctas, cudaStream_t stream);
+
+/* Candidates: state r of frame d is kept when LL32[r][d] >= max32[d] - delta
+ * - 2*eps_d, eps_d = 2^-24 ((rows_d + 8) * photons_d * lmax + |max32| + delta + 1)
+ * bounding |LL32 - LL64| (photons_d = in-mask photons, rows_d from row_off16,
+ * lmax = largest |slice value|).  Writes cand_n[d], the exclusive offsets
+ * cand_off (n_data + 1, total at [n_data]), the pairs (cand_d, cand_r) up to
+ * `capacity` (beyond it RSPI_ERR_CAPACITY goes to err), the threshold thr[d]
+ * and noncand[d] = sum over dropped states of exp(LL32 - max32[d]).
+ * cnt_part is scratch of n_data * 32 ints. */
+int rspi_screen_candidates(const float *ll, long long n_rows, long long n_data,
+                           const double *max32, const long long *frame_photons,
+                           const long long *row_off16, const float *lmax, double delta,
+                           int *cnt_part, int *cand_n, double *noncand, double *thr,
+                           long long *cand_off, long long capacity, int *cand_d, int *cand_r,
+                           int *err, cudaStream_t stream);
+
+/* FP64 rescoring of every candidate with rot_log_value on the FP64 holographic
+ * slices and the 32-bit entry lists, in the summation order of rspi_loglike
+ * (so the values equal the FP64 form's), written to cand_ll and into ll32;
+ * then per frame the first-index argmax, maximum and
+ * logz = max + log(sum_cand exp(LL64 - max) + noncand * exp(max32 - max)). */
+int rspi_rescore(const int *cand_d, const int *cand_r, const long long *cand_off,
+                 long long n_data, long long capacity, const double *holo, long long num_rot,
+                 const double *rot_cs, long long size, const double *bg, const int *sel_pix,
+                 const double *init, const double *scales, const unsigned int *entries32,
+                 const long long *row_off32, double *cand_ll, float *ll32, const double *max32,
+                 const double *noncand, double *maxll, int *rmax, double *logz,
+                 cudaStream_t stream);
 
 /* ------------------------------------------------------------------- a8, a9
  * Per-frame reduction over all states of LL (n_rows x n_data, FP64 or FP32):
@@ -145,6 +221,35 @@ int rspi_loglike_max_tile(long long p_pad, int slice_dtype);
  * normalisation; absent from the reference run path). */
 int rspi_frame_reduce(const void *ll, int ll_dtype, long long n_rows, long long n_data,
                       double *maxll, int *rmax, double *logz, cudaStream_t stream);
+
+/* ----------------------------------------------------------------------- a10
+ * Posterior-weighted merge, composed from the reference's merge_all
+ * (kernels.cu:139-152) and slice_merge (kernels.cu:84-114), which it ships
+ * but never launches:
+ *   num[s0](q) = sum_j R_j^T[sum_d P[s0*R+j][d] K_d](q),
+ *   w[r] = sum_d P[r][d] scales[d], den[s0](q) = sum_j w[s0*R+j] C_j(q),
+ *   intens = num / den (0 where den == 0), C_j = R_j^T 1,
+ * with P = exp(LL - logz[d]) counted when P >= p_min.
+ *
+ * rspi_posterior_pairs: the (frame, row, LL) pairs with P >= p_min from a
+ * full FP64 likelihood matrix (count / scan / fill as rspi_screen_candidates;
+ * total at off[n_data]).  The screened form passes its candidate list instead.
+ * rspi_merge_coverage: C (num_rot x P), once per geometry.
+ * rspi_merge: zeroes num and w, scatters every pair's photons, finalises. */
+int rspi_posterior_pairs(const double *ll, long long n_rows, long long n_data,
+                         const double *logz, double p_min, int *cnt_part, int *cnt,
+                         long long *off, long long capacity, int *pair_d, int *pair_r,
+                         double *pair_ll, int *err, cudaStream_t stream);
+int rspi_merge_coverage(long long num_rot, const double *rot_cs, long long size, double *cov,
+                        cudaStream_t stream);
+int rspi_merge(const int *pair_d, const int *pair_r, const double *pair_ll,
+               const long long *pair_total, long long capacity, const double *logz,
+               double p_min, const double *scales, const int *ones, const int *multi,
+               const long long *ones_accum, const long long *multi_accum,
+               const int *place_ones, const int *place_multi, const int *count_multi,
+               long long n_states0, long long num_rot, const double *rot_cs, long long size,
+               const double *cov, double *num, double *den, double *w, double *intens,
+               cudaStream_t stream);
 
 /* ----------------------------------------------------------------- a11-a14
  * MaxLP M-step (maxLP.py:304-340).  Frames carry a reference-state index

@@ -27,6 +27,31 @@ __device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
 
+// One rotated log-slice value (kernels.cu:19-41 with log_flag = 1, scale = 1):
+// bilinear sample of the holographic slice w at R(angle)(p - cen) + cen, plus
+// bg, then log; -1000 outside the detector or below 1e-20.  Shared by the
+// slice kernel and the FP64 rescoring so both produce identical values.
+__device__ __forceinline__ double rot_log_value(const double *__restrict__ w, int x, int y,
+                                                int size, double ac, double as, double bg) {
+    const int cen = size / 2;
+    const double xc = (double)(x - cen), yc = (double)(y - cen);
+    const double tx = xadd(xsub(xmul(xc, ac), xmul(yc, as)), (double)cen);
+    const double ty = xadd(xadd(xmul(xc, as), xmul(yc, ac)), (double)cen);
+    const double fxl = floor(tx), fyl = floor(ty);
+    if (fxl < 0. || fxl > size - 2 || fyl < 0. || fyl > size - 2) return -1000.;
+    const int ix = (int)fxl, iy = (int)fyl;
+    const double fx = tx - fxl, fy = ty - fyl;
+    const double cx = 1. - fx, cy = 1. - fy;
+    const double *r0 = w + (long long)ix * size + iy;
+    const double *r1 = r0 + size;
+    double v = xmul(xmul(r0[0], cx), cy);
+    v = xadd(v, xmul(xmul(r1[0], fx), cy));
+    v = xadd(v, xmul(xmul(r0[1], cx), fy));
+    v = xadd(v, xmul(xmul(r1[1], fx), fy));
+    v = xadd(v, bg);
+    return v < 1.e-20 ? -1000. : log(v);
+}
+
 template <class T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

@@ -1,0 +1,516 @@
+// Screened likelihood (rows a7-a9, the chosen form).
+//
+// 1. FP32 screening pass: rotated log-slices stored in FP32, photons stored
+//    as 16-bit sel indices with counts expanded (a pixel with k photons is k
+//    entries), two rows per 32-bit word: one warp load brings 64 photons and
+//    every shared-memory gather is bank-conflict free.  Sums are FP32.
+// 2. Per frame, every state whose screened value is within
+//    delta + 2 * eps_d of the frame's screened maximum becomes a candidate,
+//    where eps_d bounds |LL32 - LL64| (storage rounding of the slices,
+//    FP32 summation, output rounding).  Any state that is the FP64 argmax or
+//    carries posterior mass above exp(-delta) is a candidate.
+// 3. Candidates are rescored in FP64 with the same slice function, packed
+//    entries and summation order as the FP64 form, so rmax, the maximum and
+//    the log-sum-exp equal the FP64 form's values.
+#include "rspi_common.cuh"
+
+namespace {
+
+constexpr int SMEM_LIMIT = 227 * 1024;
+constexpr int ENTRY_WARPS = 8;
+constexpr double U32 = 5.9604644775390625e-08;  // 2^-24, FP32 unit roundoff
+
+// ---------------------------------------------------------------------------
+// 16-bit count-expanded entry lists
+// ---------------------------------------------------------------------------
+struct Ent {
+    int c;    // sel index or -1
+    int cnt;  // photons
+};
+
+__device__ __forceinline__ Ent entry_at(int i, int n_o, long long oa, long long ma,
+                                        const int *place_ones, const int *place_multi,
+                                        const int *count_multi, const int *pix2sel,
+                                        long long num_pix) {
+    Ent e{-1, 0};
+    int p;
+    if (i < n_o) {
+        p = place_ones[oa + i];
+        e.cnt = 1;
+    } else {
+        p = place_multi[ma + (i - n_o)];
+        e.cnt = count_multi[ma + (i - n_o)];
+    }
+    if (p < 0 || p >= num_pix || e.cnt <= 0) return e;
+    e.c = pix2sel[p];
+    return e;
+}
+
+// rows per frame = largest bank population counting copies, rounded up to even
+__global__ void __launch_bounds__(ENTRY_WARPS * 32)
+k_entry16_rows(const int *__restrict__ ones, const int *__restrict__ multi,
+               const long long *__restrict__ ones_accum, const long long *__restrict__ multi_accum,
+               const int *__restrict__ place_ones, const int *__restrict__ place_multi,
+               const int *__restrict__ count_multi, const int *__restrict__ pix2sel,
+               long long num_pix, long long n, int p_zero, int *__restrict__ frame_rows,
+               int *err) {
+    __shared__ int hist[ENTRY_WARPS][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long nwarp = (long long)gridDim.x * ENTRY_WARPS;
+    for (long long d = (long long)blockIdx.x * ENTRY_WARPS + w; d < n; d += nwarp) {
+        hist[w][lane] = 0;
+        __syncwarp();
+        const int n_o = ones[d], n_m = multi[d];
+        const long long oa = ones_accum[d], ma = multi_accum[d];
+        for (int i = lane; i < n_o + n_m; i += 32) {
+            Ent e = entry_at(i, n_o, oa, ma, place_ones, place_multi, count_multi, pix2sel,
+                             num_pix);
+            if (e.c >= 0) {
+                if (e.c >= p_zero) rspi_flag(err, RSPI_ERR_CAPACITY);
+                else atomicAdd(&hist[w][e.c & 31], e.cnt);
+            }
+        }
+        __syncwarp();
+        int rows = warp_max_int(hist[w][lane]);
+        if (lane == 0) frame_rows[d] = (rows + 1) & ~1;
+        __syncwarp();
+    }
+}
+
+// Deterministic fill: a lane's copies occupy consecutive slots of its bank,
+// after the copies of same-bank entries of lower lanes in the same chunk.
+// Layout: word (pair, lane) holds rows 2*pair (low half) and 2*pair+1.
+__global__ void __launch_bounds__(ENTRY_WARPS * 32)
+k_entry16_fill(const int *__restrict__ ones, const int *__restrict__ multi,
+               const long long *__restrict__ ones_accum, const long long *__restrict__ multi_accum,
+               const int *__restrict__ place_ones, const int *__restrict__ place_multi,
+               const int *__restrict__ count_multi, const int *__restrict__ pix2sel,
+               long long num_pix, long long n, int p_zero, const long long *__restrict__ row_off,
+               unsigned short *__restrict__ ent) {
+    __shared__ int base[ENTRY_WARPS][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long nwarp = (long long)gridDim.x * ENTRY_WARPS;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    for (long long d = (long long)blockIdx.x * ENTRY_WARPS + w; d < n; d += nwarp) {
+        base[w][lane] = 0;
+        __syncwarp();
+        const int n_o = ones[d], n_m = multi[d];
+        const long long oa = ones_accum[d], ma = multi_accum[d];
+        const long long r0 = row_off[d], nrows = row_off[d + 1] - r0;
+        for (int i0 = 0; i0 < n_o + n_m; i0 += 32) {
+            const int i = i0 + lane;
+            Ent e{-1, 0};
+            if (i < n_o + n_m)
+                e = entry_at(i, n_o, oa, ma, place_ones, place_multi, count_multi, pix2sel,
+                             num_pix);
+            if (e.c >= p_zero) e.c = -1;
+            const int key = e.c >= 0 ? (e.c & 31) : 32 + lane;
+            const unsigned peers = __match_any_sync(RSPI_FULL_MASK, key);
+            // copies of lower same-bank lanes come first
+            int before = 0, total = 0;
+            unsigned m = peers;
+            while (m) {
+                const int l = __ffs(m) - 1;
+                m &= m - 1;
+                const int c = __shfl_sync(peers, e.cnt, l);
+                if (l < lane) before += c;
+                total += c;
+            }
+            if (e.c >= 0) {
+                const int b = e.c & 31;
+                const long long s0 = base[w][b] + before;
+                for (int k = 0; k < e.cnt; ++k) {
+                    const long long r = s0 + k;
+                    if (r < nrows) {
+                        const long long rr = r0 + r;
+                        ent[(rr >> 1) * 64 + b * 2 + (rr & 1)] = (unsigned short)e.c;
+                    }
+                }
+            }
+            __syncwarp();
+            if (e.c >= 0 && (peers & lt_mask) == 0) base[w][e.c & 31] += total;
+            __syncwarp();
+        }
+        for (long long r = base[w][lane]; r < nrows; ++r) {
+            const long long rr = r0 + r;
+            ent[(rr >> 1) * 64 + lane * 2 + (rr & 1)] = (unsigned short)(p_zero + lane);
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FP32 screening likelihood
+// ---------------------------------------------------------------------------
+template <int T>
+__global__ void __launch_bounds__(1024)
+k_screen_ll(const float *__restrict__ lsl, long long p_row, long long num_rot,
+            const double *__restrict__ init, const double *__restrict__ scales,
+            const unsigned int *__restrict__ ent, const long long *__restrict__ row_off,
+            const int *__restrict__ frame_order, long long n_data, long long row_begin,
+            long long row_end, float *__restrict__ ll, long long ll_stride) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float *sl = reinterpret_cast<float *>(smem_raw);
+    __shared__ int next_frame;
+    const int lane = threadIdx.x & 31;
+    const long long n_tiles = (row_end - row_begin + T - 1) / T;
+    const unsigned cmax = (unsigned)p_row - 1;
+    for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const long long first = row_begin + tile * T;
+        const int nt = (int)min((long long)T, row_end - first);
+        {
+            const long long nvec = (long long)nt * p_row / 4;
+            const float4 *src = reinterpret_cast<const float4 *>(lsl + (first - row_begin) * p_row);
+            float4 *dst = reinterpret_cast<float4 *>(sl);
+            for (long long i = threadIdx.x; i < nvec; i += blockDim.x) dst[i] = src[i];
+            const long long nzero = (long long)(T - nt) * p_row / 4;
+            for (long long i = threadIdx.x; i < nzero; i += blockDim.x)
+                dst[nvec + i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if (threadIdx.x == 0) next_frame = 0;
+        __syncthreads();
+        while (true) {
+            int k = 0;
+            if (lane == 0) k = atomicAdd(&next_frame, 1);
+            k = __shfl_sync(RSPI_FULL_MASK, k, 0);
+            if (k >= n_data) break;
+            const int d = frame_order ? frame_order[k] : k;
+            const long long p0 = row_off[d] >> 1, p1 = row_off[d + 1] >> 1;
+            float acc[T];
+#pragma unroll
+            for (int t = 0; t < T; ++t) acc[t] = 0.f;
+            const unsigned int *ep = ent + p0 * 32 + lane;
+            long long q = p0;
+            for (; q + 4 <= p1; q += 4, ep += 128) {
+                unsigned wv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) wv[u] = __ldg(ep + 32 * u);
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const unsigned c0 = min(wv[u] & 0xffffu, cmax), c1 = min(wv[u] >> 16, cmax);
+#pragma unroll
+                    for (int t = 0; t < T; ++t) acc[t] += sl[t * p_row + c0] + sl[t * p_row + c1];
+                }
+            }
+            for (; q < p1; ++q, ep += 32) {
+                const unsigned wv = __ldg(ep);
+                const unsigned c0 = min(wv & 0xffffu, cmax), c1 = min(wv >> 16, cmax);
+#pragma unroll
+                for (int t = 0; t < T; ++t) acc[t] += sl[t * p_row + c0] + sl[t * p_row + c1];
+            }
+#pragma unroll
+            for (int t = 0; t < T; ++t) acc[t] = warp_sum(acc[t]);
+            if (lane < nt) {
+                float v = 0.f;
+#pragma unroll
+                for (int t = 0; t < T; ++t)
+                    if (t == lane) v = (float)(init[(first + t) / num_rot] * scales[d] + (double)acc[t]);
+                ll[(first + lane - row_begin) * ll_stride + d] = v;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <int T>
+int launch_screen(const float *lsl, long long p_row, long long num_rot, const double *init,
+                  const double *scales, const unsigned *ent, const long long *row_off,
+                  const int *order, long long n_data, long long r0, long long r1, float *ll,
+                  long long stride, int warps, int n_ctas, cudaStream_t stream) {
+    const size_t smem = (size_t)T * p_row * sizeof(float);
+    if (smem > (size_t)SMEM_LIMIT - 1024) return RSPI_ERR_ARG;
+    static size_t smem_set = 0;
+    if (smem > smem_set) {
+        if (cudaFuncSetAttribute(k_screen_ll<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return RSPI_ERR_CUDA;
+        smem_set = smem;
+    }
+    const long long n_tiles = (r1 - r0 + T - 1) / T;
+    if (n_ctas <= 0) {
+        const int per_sm = max(1, (int)(SMEM_LIMIT / (smem + 1024)));
+        n_ctas = rspi_sm_count() * min(per_sm, max(1, 2048 / (warps * 32)));
+    }
+    if (n_ctas > n_tiles) n_ctas = (int)n_tiles;
+    k_screen_ll<T><<<n_ctas, warps * 32, smem, stream>>>(lsl, p_row, num_rot, init, scales, ent,
+                                                         row_off, order, n_data, r0, r1, ll,
+                                                         stride);
+    RSPI_RETURN_LAUNCH();
+}
+
+// ---------------------------------------------------------------------------
+// candidate selection
+// ---------------------------------------------------------------------------
+constexpr int RY = 32;
+
+__device__ __forceinline__ double frame_eps(long long phot, long long rows, float lmax,
+                                            double maxll, double delta) {
+    // slice rounding + FP32 summation (per-lane sequential + 5-level tree)
+    // + output rounding, for every state within delta of the maximum
+    const double sum_abs = (double)phot * (double)lmax;
+    return U32 * ((double)(rows + 8) * sum_abs + fabs(maxll) + delta + 1.) + 1e-9 * sum_abs;
+}
+
+__global__ void __launch_bounds__(32 * RY)
+k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_data,
+             const double *__restrict__ max32, const long long *__restrict__ phot,
+             const long long *__restrict__ row_off16, const float *__restrict__ lmax, double delta,
+             int *__restrict__ cnt_part /* n_data x RY */, int *__restrict__ cand_n,
+             double *__restrict__ noncand, double *__restrict__ thr_out) {
+    __shared__ int sc[RY][33];
+    __shared__ double sn[RY][33];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const long long d = (long long)blockIdx.x * 32 + tx;
+    int c = 0;
+    double nc = 0.;
+    if (d < n_data) {
+        const double m = max32[d];
+        const long long rows = row_off16[d + 1] - row_off16[d];
+        const double thr = m - delta - 2. * frame_eps(phot[d], rows, *lmax, m, delta);
+        for (long long r = ty; r < n_rows; r += RY) {
+            const double v = (double)ll[r * n_data + d];
+            if (v >= thr) ++c;
+            else nc += exp(v - m);
+        }
+        cnt_part[d * RY + ty] = c;
+        if (ty == 0) thr_out[d] = thr;
+    }
+    sc[ty][tx] = c;
+    sn[ty][tx] = nc;
+    __syncthreads();
+    if (ty == 0 && d < n_data) {
+        int tot = 0;
+        double s = 0.;
+        for (int k = 0; k < RY; ++k) {
+            tot += sc[k][tx];
+            s += sn[k][tx];
+        }
+        cand_n[d] = tot;
+        noncand[d] = s;
+    }
+}
+
+__global__ void __launch_bounds__(32 * RY)
+k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_data,
+            const double *__restrict__ thr, const int *__restrict__ cnt_part,
+            const long long *__restrict__ cand_off, long long capacity,
+            int *__restrict__ cand_d, int *__restrict__ cand_r, int *err) {
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const long long d = (long long)blockIdx.x * 32 + tx;
+    if (d >= n_data) return;
+    long long pos = cand_off[d];
+    for (int k = 0; k < ty; ++k) pos += cnt_part[d * RY + k];
+    const double th = thr[d];
+    for (long long r = ty; r < n_rows; r += RY) {
+        if ((double)ll[r * n_data + d] >= th) {
+            if (pos < capacity) {
+                cand_d[pos] = (int)d;
+                cand_r[pos] = (int)r;
+            } else {
+                rspi_flag(err, RSPI_ERR_CAPACITY);
+            }
+            ++pos;
+        }
+    }
+}
+
+// One warp per candidate: FP64 likelihood over the frame's packed 32-bit
+// entries, in the FP64 form's order (per lane over rows, then the same
+// warp reduction), so the value equals the FP64 form's.
+__global__ void __launch_bounds__(256)
+k_rescore(const int *__restrict__ cand_d, const int *__restrict__ cand_r,
+          const long long *__restrict__ cand_total, long long capacity,
+          const double *__restrict__ holo, long long num_rot, const double *__restrict__ rot_cs,
+          int size, const double *__restrict__ bg, const int *__restrict__ sel_pix,
+          const double *__restrict__ init, const double *__restrict__ scales,
+          const unsigned int *__restrict__ ent32, const long long *__restrict__ row_off32,
+          double *__restrict__ cand_ll, float *__restrict__ ll32, long long n_data) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long total = min(*cand_total, capacity);
+    const long long npix = (long long)size * size;
+    for (long long i = warp; i < total; i += nwarp) {
+        const int d = cand_d[i], r = cand_r[i];
+        const long long s0 = r / num_rot, j = r - s0 * num_rot;
+        const double ac = rot_cs[2 * j], as = rot_cs[2 * j + 1];
+        const double *w = holo + s0 * npix;
+        double acc = 0.;
+        const unsigned *ep = ent32 + row_off32[d] * 32 + lane;
+        for (long long q = row_off32[d]; q < row_off32[d + 1]; ++q, ep += 32) {
+            const unsigned e = *ep;
+            const unsigned cnt = e & 0xffffu;
+            if (cnt == 0) continue;   // padding slot: contributes 0 * L in the FP64 form
+            const int p = sel_pix[e >> 16];
+            const int x = p / size, y = p - (p / size) * size;
+            acc = fma((double)cnt, rot_log_value(w, x, y, size, ac, as, bg[p]), acc);
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) {
+            const double v = init[s0] * scales[d] + acc;
+            cand_ll[i] = v;
+            ll32[(long long)r * n_data + d] = (float)v;
+        }
+    }
+}
+
+// Per frame over its candidates: first-index argmax, max and log-sum-exp.
+__global__ void k_cand_finalize(const long long *__restrict__ cand_off,
+                                const int *__restrict__ cand_r, const double *__restrict__ cand_ll,
+                                const double *__restrict__ max32, const double *__restrict__ noncand,
+                                long long n_data, long long capacity, double *__restrict__ maxll,
+                                int *__restrict__ rmax, double *__restrict__ logz) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long d = (long long)blockIdx.x * blockDim.x + threadIdx.x; d < n_data; d += stride) {
+        const long long a = cand_off[d], b = min(cand_off[d + 1], capacity);
+        double m = 0.;
+        int idx = -1;
+        for (long long i = a; i < b; ++i) {
+            const double v = cand_ll[i];
+            if (idx < 0 || argmax_better(v, cand_r[i], m, idx)) {
+                m = v;
+                idx = cand_r[i];
+            }
+        }
+        double s = 0.;
+        for (long long i = a; i < b; ++i) s += exp(cand_ll[i] - m);
+        s += noncand[d] * exp(max32[d] - m);
+        maxll[d] = m;
+        rmax[d] = idx;
+        logz[d] = m + log(s);
+    }
+}
+
+// Scan of per-frame candidate counts (one CTA), with the total at [n].
+__global__ void __launch_bounds__(1024)
+k_scan_counts(const int *__restrict__ cnt, long long n, long long *__restrict__ off) {
+    __shared__ long long part[1024];
+    const long long per = (n + 1023) / 1024;
+    const long long lo = (long long)threadIdx.x * per, hi = min(n, lo + per);
+    long long s = 0;
+    for (long long i = lo; i < hi; ++i) s += cnt[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long acc = 0;
+        for (int k = 0; k < 1024; ++k) {
+            long long v = part[k];
+            part[k] = acc;
+            acc += v;
+        }
+        off[n] = acc;
+    }
+    __syncthreads();
+    long long acc = part[threadIdx.x];
+    for (long long i = lo; i < hi; ++i) {
+        off[i] = acc;
+        acc += cnt[i];
+    }
+}
+
+}  // namespace
+
+extern "C" int rspi_ll16_entry_rows(const int *ones, const int *multi,
+                                    const long long *ones_accum, const long long *multi_accum,
+                                    const int *place_ones, const int *place_multi,
+                                    const int *count_multi, const int *pix2sel, long long num_pix,
+                                    long long n_data, int p_zero, int *frame_rows, int *err,
+                                    cudaStream_t stream) {
+    if (n_data <= 0 || num_pix <= 0 || !frame_rows || !pix2sel || p_zero < 0 ||
+        p_zero % 32 || p_zero + 32 > 65536)
+        return RSPI_ERR_ARG;
+    k_entry16_rows<<<rspi_blocks(n_data * 32, ENTRY_WARPS * 32), ENTRY_WARPS * 32, 0, stream>>>(
+        ones, multi, ones_accum, multi_accum, place_ones, place_multi, count_multi, pix2sel,
+        num_pix, n_data, p_zero, frame_rows, err);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_ll16_entry_fill(const int *ones, const int *multi,
+                                    const long long *ones_accum, const long long *multi_accum,
+                                    const int *place_ones, const int *place_multi,
+                                    const int *count_multi, const int *pix2sel, long long num_pix,
+                                    long long n_data, int p_zero, const long long *row_off,
+                                    unsigned short *entries, cudaStream_t stream) {
+    if (n_data <= 0 || num_pix <= 0 || !row_off || !entries || !pix2sel || p_zero < 0 ||
+        p_zero % 32 || p_zero + 32 > 65536)
+        return RSPI_ERR_ARG;
+    k_entry16_fill<<<rspi_blocks(n_data * 32, ENTRY_WARPS * 32), ENTRY_WARPS * 32, 0, stream>>>(
+        ones, multi, ones_accum, multi_accum, place_ones, place_multi, count_multi, pix2sel,
+        num_pix, n_data, p_zero, row_off, entries);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_screen_loglike(const float *lslices, long long p_row, long long num_rot,
+                                   const double *init, const double *scales,
+                                   const unsigned short *entries, const long long *row_off,
+                                   const int *frame_order, long long n_data, long long row_begin,
+                                   long long row_end, float *ll, long long ll_stride,
+                                   int states_per_tile, int warps_per_cta, int n_ctas,
+                                   cudaStream_t stream) {
+    if (!lslices || !init || !scales || !entries || !row_off || !ll || n_data <= 0 ||
+        n_data > 0x7fffffffLL || p_row <= 32 || p_row % 32 || p_row > 65536 || num_rot <= 0 ||
+        row_begin < 0 || row_end < row_begin || ll_stride < n_data || warps_per_cta < 1 ||
+        warps_per_cta > 32)
+        return RSPI_ERR_ARG;
+    if ((reinterpret_cast<uintptr_t>(lslices) & 15) != 0 ||
+        (reinterpret_cast<uintptr_t>(entries) & 3) != 0)
+        return RSPI_ERR_ARG;
+    if (row_end == row_begin) return RSPI_OK;
+    const unsigned *ent = reinterpret_cast<const unsigned *>(entries);
+#define RSPI_SC(TT)                                                                            \
+    case TT:                                                                                   \
+        return launch_screen<TT>(lslices, p_row, num_rot, init, scales, ent, row_off,          \
+                                 frame_order, n_data, row_begin, row_end, ll, ll_stride,       \
+                                 warps_per_cta, n_ctas, stream);
+    switch (states_per_tile) {
+        RSPI_SC(1)
+        RSPI_SC(2)
+        RSPI_SC(3)
+        RSPI_SC(4)
+        RSPI_SC(6)
+        RSPI_SC(8)
+        default:
+            return RSPI_ERR_ARG;
+    }
+#undef RSPI_SC
+}
+
+extern "C" int rspi_screen_candidates(const float *ll, long long n_rows, long long n_data,
+                                      const double *max32, const long long *frame_photons,
+                                      const long long *row_off16, const float *lmax, double delta,
+                                      int *cnt_part, int *cand_n, double *noncand, double *thr,
+                                      long long *cand_off, long long capacity, int *cand_d,
+                                      int *cand_r, int *err, cudaStream_t stream) {
+    if (!ll || !max32 || !frame_photons || !row_off16 || !lmax || !cnt_part || !cand_n ||
+        !noncand || !thr || !cand_off || !cand_d || !cand_r || n_rows <= 0 || n_data <= 0 ||
+        n_rows > 0x7fffffffLL || capacity < 0 || !(delta >= 0.))
+        return RSPI_ERR_ARG;
+    const dim3 block(32, RY);
+    const unsigned grid = (unsigned)((n_data + 31) / 32);
+    k_cand_count<<<grid, block, 0, stream>>>(ll, n_rows, n_data, max32, frame_photons, row_off16,
+                                             lmax, delta, cnt_part, cand_n, noncand, thr);
+    k_scan_counts<<<1, 1024, 0, stream>>>(cand_n, n_data, cand_off);
+    k_cand_fill<<<grid, block, 0, stream>>>(ll, n_rows, n_data, thr, cnt_part, cand_off, capacity,
+                                            cand_d, cand_r, err);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_rescore(const int *cand_d, const int *cand_r, const long long *cand_off,
+                            long long n_data, long long capacity, const double *holo,
+                            long long num_rot, const double *rot_cs, long long size,
+                            const double *bg, const int *sel_pix, const double *init,
+                            const double *scales, const unsigned int *entries32,
+                            const long long *row_off32, double *cand_ll, float *ll32,
+                            const double *max32, const double *noncand, double *maxll, int *rmax,
+                            double *logz, cudaStream_t stream) {
+    if (!cand_d || !cand_r || !cand_off || !holo || !rot_cs || !bg || !sel_pix || !init ||
+        !scales || !entries32 || !row_off32 || !cand_ll || !ll32 || !max32 || !noncand ||
+        !maxll || !rmax || !logz || n_data <= 0 || capacity < 0 || size <= 1 || size > 46340)
+        return RSPI_ERR_ARG;
+    k_rescore<<<rspi_sm_count() * 8, 256, 0, stream>>>(
+        cand_d, cand_r, cand_off + n_data, capacity, holo, num_rot, rot_cs, (int)size, bg,
+        sel_pix, init, scales, entries32, row_off32, cand_ll, ll32, n_data);
+    k_cand_finalize<<<rspi_blocks(n_data, 256), 256, 0, stream>>>(
+        cand_off, cand_r, cand_ll, max32, noncand, n_data, capacity, maxll, rmax, logz);
+    RSPI_RETURN_LAUNCH();
+}

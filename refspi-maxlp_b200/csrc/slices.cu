@@ -62,37 +62,16 @@ k_vscale_init(const double *__restrict__ msum, long long n_states0,
     for (long long s = threadIdx.x; s < n_states0; s += blockDim.x) init[s] = -(msum[s] * vs);
 }
 
-// One rotated log-slice value (kernels.cu:19-41 with log_flag = 1, scale = 1).
-__device__ __forceinline__ double rot_log_value(const double *__restrict__ w, int x, int y,
-                                                int size, double ac, double as, double bg) {
-    const int cen = size / 2;
-    const double xc = (double)(x - cen), yc = (double)(y - cen);
-    const double tx = xadd(xsub(xmul(xc, ac), xmul(yc, as)), (double)cen);
-    const double ty = xadd(xadd(xmul(xc, as), xmul(yc, ac)), (double)cen);
-    const double fxl = floor(tx), fyl = floor(ty);
-    if (fxl < 0. || fxl > size - 2 || fyl < 0. || fyl > size - 2) return -1000.;
-    const int ix = (int)fxl, iy = (int)fyl;
-    const double fx = tx - fxl, fy = ty - fyl;
-    const double cx = 1. - fx, cy = 1. - fy;
-    const double *r0 = w + (long long)ix * size + iy;
-    const double *r1 = r0 + size;
-    double v = xmul(xmul(r0[0], cx), cy);
-    v = xadd(v, xmul(xmul(r1[0], fx), cy));
-    v = xadd(v, xmul(xmul(r0[1], cx), fy));
-    v = xadd(v, xmul(xmul(r1[1], fx), fy));
-    v = xadd(v, bg);
-    return v < 1.e-20 ? -1000. : log(v);
-}
-
 template <typename TL>
 __global__ void __launch_bounds__(256)
 k_rot_log(const double *__restrict__ holo, long long num_rot, const double *__restrict__ rot_cs,
           int size, const double *__restrict__ bg, const int *__restrict__ sel_pix,
           long long n_sel, long long p_pad, long long row_begin, long long n_rows,
-          TL *__restrict__ out) {
+          TL *__restrict__ out, float *__restrict__ abs_max) {
     const long long npix = (long long)size * size;
     const long long total = n_rows * p_pad;
     const long long stride = (long long)gridDim.x * blockDim.x;
+    float amax = 0.f;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
         const long long rr = i / p_pad, c = i - rr * p_pad;
         double v = 0.;
@@ -104,7 +83,14 @@ k_rot_log(const double *__restrict__ holo, long long num_rot, const double *__re
             v = rot_log_value(holo + s0 * npix, x, y, size, rot_cs[2 * j], rot_cs[2 * j + 1],
                               bg[p]);
         }
-        out[i] = (TL)v;
+        const TL o = (TL)v;
+        out[i] = o;
+        amax = fmaxf(amax, fabsf((float)o));
+    }
+    if (abs_max) {
+        // non-negative floats order like their bit patterns
+        amax = __int_as_float(warp_max_int(__float_as_int(amax)));
+        if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(abs_max), __float_as_int(amax));
     }
 }
 
@@ -134,7 +120,7 @@ extern "C" int rspi_rot_log_slices(const double *holo, long long n_states0, long
                                    const double *rot_cs, long long size, const double *bg,
                                    const int *sel_pix, long long n_sel, long long p_pad,
                                    long long row_begin, long long row_end, void *lslices,
-                                   int out_dtype, cudaStream_t stream) {
+                                   int out_dtype, float *abs_max, cudaStream_t stream) {
     if (n_states0 <= 0 || num_rot <= 0 || size <= 1 || size > 46340 || p_pad < n_sel ||
         p_pad % 32 || row_begin < 0 || row_end > n_states0 * num_rot || row_end < row_begin ||
         !holo || !rot_cs || !bg || !lslices)
@@ -145,11 +131,11 @@ extern "C" int rspi_rot_log_slices(const double *holo, long long n_states0, long
     if (out_dtype == 0)
         k_rot_log<float><<<blocks, 256, 0, stream>>>(holo, num_rot, rot_cs, (int)size, bg, sel_pix,
                                                      n_sel, p_pad, row_begin, n_rows,
-                                                     (float *)lslices);
+                                                     (float *)lslices, abs_max);
     else if (out_dtype == 1)
         k_rot_log<double><<<blocks, 256, 0, stream>>>(holo, num_rot, rot_cs, (int)size, bg,
                                                       sel_pix, n_sel, p_pad, row_begin, n_rows,
-                                                      (double *)lslices);
+                                                      (double *)lslices, abs_max);
     else
         return RSPI_ERR_ARG;
     RSPI_RETURN_LAUNCH();

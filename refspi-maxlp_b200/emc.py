@@ -10,10 +10,12 @@ array and ``rmax`` a host int32 array, as in the reference.  The E-step and
 the MaxLP M-step run in librspi on the GPU; ``prob`` is a torch CUDA tensor
 (rows ``s*num_rot + j``, columns frames).
 
-Optional ``[emc]`` keys beyond the reference: ``precision`` (``fp64``:
-FP64 slices and likelihoods, the default; ``fp32``: FP32 slices and
-likelihood matrix with FP64 accumulation), ``states_per_tile``,
-``warps_per_cta``, ``phaser_iter`` (default 10, maxLP.py:320,335).
+Optional ``[emc]`` keys beyond the reference: ``form`` (``fp64``: FP64
+slices and FP64 likelihood matrix; ``screen``: FP32 screening pass with
+FP64 rescoring of every state that can be the argmax or carry posterior
+mass, same argmax/maximum/log-sum-exp as ``fp64``), ``screen_delta``
+(default 30 nats), ``states_per_tile``, ``warps_per_cta``, ``phaser_iter``
+(default 10, maxLP.py:320,335).
 """
 import configparser
 import os.path as op
@@ -61,9 +63,9 @@ class EMC():
 
         self.estep = EStep(self.dset.photons, self.size, self.num_rot, self.shiftx,
                            self.shifty, self.sphere_dia, self.probmask,
-                           self.dset.bg.cpu().numpy(), slice_dtype=self.slice_dtype,
-                           prob_dtype=self.prob_dtype, states_per_tile=self.states_per_tile,
-                           warps=self.warps_per_cta)
+                           self.dset.bg.cpu().numpy(), form=self.form,
+                           states_per_tile=self.states_per_tile, warps=self.warps_per_cta,
+                           delta=self.screen_delta)
         self.prob = self.estep.prob
         self.state_vals = torch.from_numpy(self._state_values).to(self.device)
         self.phaser_rot = torch.from_numpy(geometry.phaser_rotation_table(
@@ -79,10 +81,10 @@ class EMC():
         self.output_folder = op.join(start_dir, config.get('emc', 'output_folder'))
         self.log_file = op.join(start_dir, config.get('emc', 'log_file'))
         self.need_scaling = config.getboolean('emc', 'need_scaling', fallback=False)
-        precision = config.get('emc', 'precision', fallback='fp64')
-        if precision not in ('fp64', 'fp32'):
-            raise ValueError('emc:precision must be fp64 or fp32')
-        self.slice_dtype = self.prob_dtype = 'f64' if precision == 'fp64' else 'f32'
+        self.form = config.get('emc', 'form', fallback='fp64')
+        if self.form not in ('fp64', 'screen'):
+            raise ValueError('emc:form must be fp64 or screen')
+        self.screen_delta = config.getfloat('emc', 'screen_delta', fallback=30.)
         self.states_per_tile = config.getint('emc', 'states_per_tile', fallback=0) or None
         self.warps_per_cta = config.getint('emc', 'warps_per_cta', fallback=32)
         self.phaser_iter = config.getint('emc', 'phaser_iter', fallback=10)

@@ -130,18 +130,55 @@ class DevicePhotons:
         return self._ll
 
 
+    def ll16_entries(self, pix2sel, p_zero):
+        """16-bit count-expanded entries for the FP32 screening pass."""
+        key = (int(p_zero), pix2sel.data_ptr())
+        if getattr(self, '_ll16', None) is not None and self._ll16['key'] == key:
+            return self._ll16
+        n, dev, s = self.num_data, self.device, cur_stream()
+        rows = torch.empty(n, dtype=_i32, device=dev)
+        args = (ptr(self.ones), ptr(self.multi), ptr(self.ones_accum), ptr(self.multi_accum),
+                ptr(self.place_ones), ptr(self.place_multi), ptr(self.count_multi), ptr(pix2sel),
+                self.num_pix, n, int(p_zero))
+        call('rspi_ll16_entry_rows', *args, ptr(rows), ptr(self.err.t), s)
+        row_off = torch.empty(n + 1, dtype=_i64, device=dev)
+        call('rspi_scan_rows', ptr(rows), n, ptr(row_off), s)
+        self.err.check('16-bit entry rows')
+        total = int(row_off[-1].item())
+        entries = torch.empty(max(2, total) * 32, dtype=torch.int16, device=dev)
+        call('rspi_ll16_entry_fill', *args, ptr(row_off), ptr(entries), s)
+        order = torch.argsort(rows, descending=True, stable=True).to(_i32)
+        self._ll16 = dict(key=key, frame_rows=rows, row_off=row_off, entries=entries,
+                          order=order, total_rows=total)
+        return self._ll16
+
 class EStep:
-    """Likelihood of every frame in every (shift, diameter, rotation) state."""
+    """Likelihood of every frame in every (shift, diameter, rotation) state.
+
+    ``form='fp64'``: FP64 rotated slices and FP64 likelihood matrix (the
+    plain form).  ``form='screen'``: FP32 slices and likelihood matrix from
+    the 16-bit photon entries, then FP64 rescoring of every state within
+    ``delta`` (+ the FP32 error bound) of each frame's maximum, which gives
+    the same argmax, maximum and log-sum-exp as the FP64 form (the chosen
+    form).
+    """
 
     def __init__(self, photons, size, num_rot, shiftx, shifty, sphere_dia, probmask, bg,
-                 slice_dtype='f64', prob_dtype='f64', states_per_tile=None, warps=32,
-                 n_ctas=0, slice_budget_bytes=8 << 30):
+                 form='fp64', states_per_tile=None, warps=32, n_ctas=0,
+                 slice_budget_bytes=8 << 30, delta=30., cand_per_frame=64, kernel='stream'):
+        if form not in ('fp64', 'screen'):
+            raise ValueError('form must be fp64 or screen')
+        if kernel not in ('stream', 'dynamic'):
+            raise ValueError('kernel must be stream or dynamic')
+        self.kernel = kernel
         self.lib = load()
+        self.form = form
         self.ph = photons
         self.device = dev = photons.device
         self.size, self.num_rot = int(size), int(num_rot)
         self.n_states0 = int(np.asarray(shiftx).size)
         self.n_rows = self.n_states0 * self.num_rot
+        n = photons.num_data
         sel, pix2sel, p_pad = geometry.sel_pixels(probmask)
         self.n_sel, self.p_pad = sel.size, p_pad
         t = lambda a, dt=_f64: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)  # noqa: E731
@@ -149,30 +186,54 @@ class EStep:
         self.shiftx, self.shifty, self.sphere_dia = t(shiftx), t(shifty), t(sphere_dia)
         self.rot_cs = t(geometry.emc_rotation_table(self.num_rot))
         self.bg = t(np.asarray(bg, dtype='f8').ravel())
-        self.slice_code = {'f32': 0, 'f64': 1}[slice_dtype]
-        self.prob_code = {'f32': 0, 'f64': 1}[prob_dtype]
+        self.ll = photons.ll_entries(self.pix2sel, self.p_pad)
+        if form == 'fp64':
+            self.slice_code, self.prob_code, self.p_row = 1, 1, self.p_pad
+        else:
+            self.slice_code, self.prob_code = 0, 0
+            self.p_row = self.p_pad + 32           # 32 zero columns for padding slots
+            if self.p_row > 65536:
+                raise ValueError('screened form needs at most 65504 likelihood pixels')
+            self.ll16 = photons.ll16_entries(self.pix2sel, self.p_row - 32)
+            self.delta = float(delta)
         self.slice_torch = torch.float32 if self.slice_code == 0 else _f64
         self.prob_torch = torch.float32 if self.prob_code == 0 else _f64
-        tmax = self.lib.rspi_loglike_max_tile(self.p_pad, self.slice_code)
+        tmax = self.lib.rspi_loglike_max_tile(self.p_row, self.slice_code)
         if tmax == 0:
             raise ValueError('a %d-pixel likelihood slice does not fit in shared memory' % self.n_sel)
         self.tile = int(states_per_tile or tmax)
         if self.tile > tmax:
             raise ValueError('states_per_tile %d exceeds the shared-memory limit %d' % (self.tile, tmax))
         self.warps, self.n_ctas = int(warps), int(n_ctas)
-        self.ll = photons.ll_entries(self.pix2sel, self.p_pad)
         esz = 4 if self.slice_code == 0 else 8
-        rows = max(self.tile, (slice_budget_bytes // (self.p_pad * esz)) // self.tile * self.tile)
+        rows = max(self.tile, (slice_budget_bytes // (self.p_row * esz)) // self.tile * self.tile)
         self.chunk_rows = int(min(self.n_rows, rows))
         self.holo = torch.empty((self.n_states0, self.size ** 2), dtype=_f64, device=dev)
         self.msum = torch.empty(self.n_states0, dtype=_f64, device=dev)
         self.vscale = torch.empty(1, dtype=_f64, device=dev)
         self.init = torch.empty(self.n_states0, dtype=_f64, device=dev)
-        self.lsl = torch.empty((self.chunk_rows, self.p_pad), dtype=self.slice_torch, device=dev)
-        self.prob = torch.empty((self.n_rows, photons.num_data), dtype=self.prob_torch, device=dev)
-        self.maxll = torch.empty(photons.num_data, dtype=_f64, device=dev)
-        self.rmax = torch.empty(photons.num_data, dtype=_i32, device=dev)
-        self.logz = torch.empty(photons.num_data, dtype=_f64, device=dev)
+        self.lsl = torch.empty((self.chunk_rows, self.p_row), dtype=self.slice_torch, device=dev)
+        self.prob = torch.empty((self.n_rows, n), dtype=self.prob_torch, device=dev)
+        self.maxll = torch.empty(n, dtype=_f64, device=dev)
+        self.rmax = torch.empty(n, dtype=_i32, device=dev)
+        self.logz = torch.empty(n, dtype=_f64, device=dev)
+        if form == 'screen':
+            self.lmax = torch.zeros(1, dtype=torch.float32, device=dev)
+            self.max32 = torch.empty(n, dtype=_f64, device=dev)
+            self.cnt_part = torch.empty(n * 32, dtype=_i32, device=dev)
+            self.cand_n = torch.empty(n, dtype=_i32, device=dev)
+            self.noncand = torch.empty(n, dtype=_f64, device=dev)
+            self.thr = torch.empty(n, dtype=_f64, device=dev)
+            self.cand_off = torch.empty(n + 1, dtype=_i64, device=dev)
+            self._alloc_candidates(max(1024, int(cand_per_frame) * n))
+        self.check_capacity = True
+
+    def _alloc_candidates(self, cap):
+        dev = self.device
+        self.capacity = int(cap)
+        self.cand_d = torch.empty(self.capacity, dtype=_i32, device=dev)
+        self.cand_r = torch.empty(self.capacity, dtype=_i32, device=dev)
+        self.cand_ll = torch.empty(self.capacity, dtype=_f64, device=dev)
 
     # -- stages ------------------------------------------------------------
     def slices(self, model):
@@ -180,29 +241,46 @@ class EStep:
         if model.dtype != torch.complex128 or not model.is_contiguous():
             raise ValueError('model must be a contiguous complex128 device tensor')
         s = cur_stream()
-        call('rspi_holo_slices', ptr(model), ptr(self.shiftx), ptr(self.shifty), ptr(self.sphere_dia),
-            self.n_states0, self.size, ptr(self.bg), ptr(self.sel_pix), self.n_sel,
-            ptr(self.holo), ptr(self.msum), s)
-        call('rspi_vscale_init', ptr(self.msum), self.n_states0, ptr(self.ph.powder), ptr(self.sel_pix), self.n_sel,
-            ptr(self.vscale), ptr(self.init), s)
+        call('rspi_holo_slices', ptr(model), ptr(self.shiftx), ptr(self.shifty),
+             ptr(self.sphere_dia), self.n_states0, self.size, ptr(self.bg), ptr(self.sel_pix),
+             self.n_sel, ptr(self.holo), ptr(self.msum), s)
+        call('rspi_vscale_init', ptr(self.msum), self.n_states0, ptr(self.ph.powder),
+             ptr(self.sel_pix), self.n_sel, ptr(self.vscale), ptr(self.init), s)
+        if self.form == 'screen':
+            self.lmax.zero_()
 
     def rot_slices(self, r0, r1, out=None):
         """a6: rotated log-slices of rows [r0, r1) into ``out`` (or the chunk buffer)."""
         out = self.lsl if out is None else out
-        call('rspi_rot_log_slices', ptr(self.holo), self.n_states0, self.num_rot, ptr(self.rot_cs), self.size,
-            ptr(self.bg), ptr(self.sel_pix), self.n_sel, self.p_pad, r0, r1, ptr(out),
-            self.slice_code, cur_stream())
+        call('rspi_rot_log_slices', ptr(self.holo), self.n_states0, self.num_rot,
+             ptr(self.rot_cs), self.size, ptr(self.bg), ptr(self.sel_pix), self.n_sel,
+             self.p_row, r0, r1, ptr(out), self.slice_code,
+             ptr(self.lmax) if self.form == 'screen' else None, cur_stream())
         return out
 
     def loglike(self, r0, r1, lsl=None):
         """a7: likelihood rows [r0, r1); ``lsl`` holds those rows' slices from
         its first row on (default: the chunk buffer)."""
         lsl = self.lsl if lsl is None else lsl
-        ll = self.ll
-        call('rspi_loglike', ptr(lsl), self.slice_code, self.p_pad, self.num_rot, ptr(self.init),
-            ptr(self.ph.scales), ptr(ll['entries']), ptr(ll['row_off']), ptr(ll['order']),
-            self.ph.num_data, r0, r1, ptr(self.prob[r0]), self.prob_code, self.ph.num_data,
-            self.tile, self.warps, self.n_ctas, cur_stream())
+        n = self.ph.num_data
+        if self.kernel == 'stream':
+            ent = self.ll if self.form == 'fp64' else self.ll16
+            call('rspi_loglike_stream', self.slice_code, ptr(lsl), self.p_row, self.num_rot,
+                 ptr(self.init), ptr(self.ph.scales), ptr(ent['entries']), ptr(ent['row_off']),
+                 n, r0, r1, ptr(self.prob[r0]), n, self.tile, self.warps, self.n_ctas,
+                 cur_stream())
+        elif self.form == 'fp64':
+            ll = self.ll
+            call('rspi_loglike', ptr(lsl), self.slice_code, self.p_row, self.num_rot,
+                 ptr(self.init), ptr(self.ph.scales), ptr(ll['entries']), ptr(ll['row_off']),
+                 ptr(ll['order']), n, r0, r1, ptr(self.prob[r0]), self.prob_code, n, self.tile,
+                 self.warps, self.n_ctas, cur_stream())
+        else:
+            l16 = self.ll16
+            call('rspi_screen_loglike', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
+                 ptr(self.ph.scales), ptr(l16['entries']), ptr(l16['row_off']),
+                 ptr(l16['order']), n, r0, r1, ptr(self.prob[r0]), n, self.tile, self.warps,
+                 self.n_ctas, cur_stream())
 
     def run(self, model):
         """Full likelihood matrix ``prob`` for ``model`` (a4-a7)."""
@@ -215,9 +293,88 @@ class EStep:
 
     def reduce(self):
         """a8 + a9: per-frame max, first-index argmax and log-sum-exp."""
-        call('rspi_frame_reduce', ptr(self.prob), self.prob_code, self.n_rows, self.ph.num_data, ptr(self.maxll),
-            ptr(self.rmax), ptr(self.logz), cur_stream())
+        n = self.ph.num_data
+        s = cur_stream()
+        if self.form == 'fp64':
+            call('rspi_frame_reduce', ptr(self.prob), self.prob_code, self.n_rows, n,
+                 ptr(self.maxll), ptr(self.rmax), ptr(self.logz), s)
+            return self.maxll, self.rmax, self.logz
+        call('rspi_frame_reduce', ptr(self.prob), 0, self.n_rows, n, ptr(self.max32), None,
+             None, s)
+        while True:
+            call('rspi_screen_candidates', ptr(self.prob), self.n_rows, n, ptr(self.max32),
+                 ptr(self.ll['frame_sel_photons']), ptr(self.ll16['row_off']), ptr(self.lmax),
+                 self.delta, ptr(self.cnt_part), ptr(self.cand_n), ptr(self.noncand),
+                 ptr(self.thr), ptr(self.cand_off), self.capacity, ptr(self.cand_d),
+                 ptr(self.cand_r), ptr(self.ph.err.t), s)
+            if self.check_capacity:
+                total = int(self.cand_off[n].item())
+                if total > self.capacity:
+                    self.ph.err.t.zero_()
+                    self._alloc_candidates(int(total * 1.25) + 1024)
+                    continue
+                self.n_candidates = total
+            break
+        call('rspi_rescore', ptr(self.cand_d), ptr(self.cand_r), ptr(self.cand_off), n,
+             self.capacity, ptr(self.holo), self.num_rot, ptr(self.rot_cs), self.size,
+             ptr(self.bg), ptr(self.sel_pix), ptr(self.init), ptr(self.ph.scales),
+             ptr(self.ll['entries']), ptr(self.ll['row_off']), ptr(self.cand_ll),
+             ptr(self.prob), ptr(self.max32), ptr(self.noncand), ptr(self.maxll),
+             ptr(self.rmax), ptr(self.logz), s)
         return self.maxll, self.rmax, self.logz
+
+
+class Merge:
+    """Posterior-weighted merge into per-(shift, diameter) intensities (a10)."""
+
+    def __init__(self, estep, p_min=1.e-6, pairs_per_frame=16):
+        self.es = estep
+        self.p_min = float(p_min)
+        dev = estep.device
+        n0, r, npix = estep.n_states0, estep.num_rot, estep.size ** 2
+        self.cov = torch.empty((r, npix), dtype=_f64, device=dev)
+        call('rspi_merge_coverage', r, ptr(estep.rot_cs), estep.size, ptr(self.cov), cur_stream())
+        self.num = torch.empty((n0, npix), dtype=_f64, device=dev)
+        self.den = torch.empty((n0, npix), dtype=_f64, device=dev)
+        self.w = torch.empty(n0 * r, dtype=_f64, device=dev)
+        self.intens = torch.empty((n0, npix), dtype=_f64, device=dev)
+        n = estep.ph.num_data
+        if estep.form == 'fp64':
+            self.cnt_part = torch.empty(n * 32, dtype=_i32, device=dev)
+            self.cnt = torch.empty(n, dtype=_i32, device=dev)
+            self.off = torch.empty(n + 1, dtype=_i64, device=dev)
+            self._alloc(max(1024, pairs_per_frame * n))
+
+    def _alloc(self, cap):
+        dev = self.es.device
+        self.capacity = int(cap)
+        self.pd = torch.empty(self.capacity, dtype=_i32, device=dev)
+        self.pr = torch.empty(self.capacity, dtype=_i32, device=dev)
+        self.pll = torch.empty(self.capacity, dtype=_f64, device=dev)
+
+    def run(self):
+        """intens (S0 x P) from the current likelihoods and log-sum-exp."""
+        es, ph, s = self.es, self.es.ph, cur_stream()
+        n = ph.num_data
+        if es.form == 'fp64':
+            while True:
+                call('rspi_posterior_pairs', ptr(es.prob), es.n_rows, n, ptr(es.logz), self.p_min,
+                     ptr(self.cnt_part), ptr(self.cnt), ptr(self.off), self.capacity, ptr(self.pd),
+                     ptr(self.pr), ptr(self.pll), ptr(ph.err.t), s)
+                total = int(self.off[n].item())
+                if total <= self.capacity:
+                    break
+                ph.err.t.zero_()
+                self._alloc(int(total * 1.25) + 1024)
+            pd, pr, pll, tot, cap = self.pd, self.pr, self.pll, self.off[n:], self.capacity
+        else:
+            pd, pr, pll, tot, cap = es.cand_d, es.cand_r, es.cand_ll, es.cand_off[n:], es.capacity
+        call('rspi_merge', ptr(pd), ptr(pr), ptr(pll), ptr(tot), cap, ptr(es.logz), self.p_min,
+             ptr(ph.scales), ptr(ph.ones), ptr(ph.multi), ptr(ph.ones_accum), ptr(ph.multi_accum),
+             ptr(ph.place_ones), ptr(ph.place_multi), ptr(ph.count_multi), es.n_states0,
+             es.num_rot, ptr(es.rot_cs), es.size, ptr(self.cov), ptr(self.num), ptr(self.den),
+             ptr(self.w), ptr(self.intens), s)
+        return self.intens
 
 
 class MStep:

@@ -24,7 +24,7 @@ SIGNATURES = {
     'rspi_ll_entry_fill': (I, [P, P, P, P, P, P, P, P, L, L, P, P, P, P]),
     'rspi_holo_slices': (I, [P, P, P, P, L, L, P, P, L, P, P, P]),
     'rspi_vscale_init': (I, [P, L, P, P, L, P, P, P]),
-    'rspi_rot_log_slices': (I, [P, L, L, P, L, P, P, L, L, L, L, P, I, P]),
+    'rspi_rot_log_slices': (I, [P, L, L, P, L, P, P, L, L, L, L, P, I, P, P]),
     'rspi_loglike': (I, [P, I, L, L, P, P, P, P, P, L, L, L, P, I, L, I, I, I, P]),
     'rspi_loglike_max_tile': (I, [L, I]),
     'rspi_frame_reduce': (I, [P, I, L, L, P, P, P, P]),
@@ -32,6 +32,15 @@ SIGNATURES = {
     'rspi_maxlp_histogram': (I, [P, P, P, P, P, P, P, L, P, P, P, L, P, L, L, P, P, P]),
     'rspi_maxlp_pattern': (I, [P, P, P, L, P, L, P, L, P, L, I, P, I, P, P]),
     'rspi_mean': (I, [P, L, P, P]),
+    'rspi_ll16_entry_rows': (I, [P] * 8 + [L, L, I, P, P, P]),
+    'rspi_ll16_entry_fill': (I, [P] * 8 + [L, L, I, P, P, P]),
+    'rspi_screen_loglike': (I, [P, L, L, P, P, P, P, P, L, L, L, P, L, I, I, I, P]),
+    'rspi_screen_candidates': (I, [P, L, L, P, P, P, P, D, P, P, P, P, P, L, P, P, P, P]),
+    'rspi_rescore': (I, [P, P, P, L, L, P, L, P, L, P, P, P, P, P, P, P, P, P, P, P, P, P, P]),
+    'rspi_loglike_stream': (I, [I, P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
+    'rspi_posterior_pairs': (I, [P, L, L, P, D, P, P, P, L, P, P, P, P, P]),
+    'rspi_merge_coverage': (I, [L, P, L, P, P]),
+    'rspi_merge': (I, [P, P, P, P, L, P, D, P, P, P, P, P, P, P, P, L, L, P, L, P, P, P, P, P, P]),
 }
 
 _lib = None
@@ -73,7 +82,9 @@ KERNELS_PER_CALL = {
     'rspi_ll_entry_fill': 1, 'rspi_holo_slices': 1, 'rspi_vscale_init': 1,
     'rspi_rot_log_slices': 1, 'rspi_loglike': 1, 'rspi_frame_reduce': 1,
     'rspi_maxlp_frame_params': 1, 'rspi_maxlp_histogram': 1, 'rspi_maxlp_pattern': 1,
-    'rspi_mean': 1,
+    'rspi_mean': 1, 'rspi_ll16_entry_rows': 1, 'rspi_ll16_entry_fill': 1,
+    'rspi_screen_loglike': 1, 'rspi_screen_candidates': 3, 'rspi_rescore': 2,
+    'rspi_loglike_stream': 1, 'rspi_posterior_pairs': 3, 'rspi_merge_coverage': 1, 'rspi_merge': 2,
 }
 launch_count = 0
 

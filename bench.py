@@ -52,7 +52,10 @@ def parse_args():
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
     ap.add_argument('--config', type=int, default=2, choices=[1, 2])
     ap.add_argument('--frames', type=int, default=None, help='override frame count (testing)')
-    ap.add_argument('--form', default='fp64', choices=['fp64', 'screen'])
+    ap.add_argument('--form', default='screen', choices=['fp64', 'screen'])
+    ap.add_argument('--kernel', default='stream', choices=['stream', 'dynamic'])
+    ap.add_argument('--no-plain', action='store_true',
+                    help='skip timing the plain form (FP64, dynamic kernel) for comparison')
     ap.add_argument('--cpu-seconds', type=float, default=20.,
                     help='target CPU time of the bounded oracle sample')
     ap.add_argument('--no-cpu-baseline', action='store_true')
@@ -308,6 +311,8 @@ def run_ours(args):
     import io
     with contextlib.redirect_stdout(io.StringIO()):
         rec = EMC(cfgfile, device=dev)
+    if args.kernel != rec.estep.kernel:
+        rec.estep.kernel = args.kernel
     model0 = synth.initial_model(w['size'], 20260100 + args.config)
     stream = torch.cuda.current_stream()
 
@@ -360,6 +365,39 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
         dist.barrier()
+
+    n_cand = getattr(rec.estep, 'n_candidates', None)
+
+    # the plain form: FP64 slices and likelihoods, warp-per-frame kernel
+    plain = None
+    if not args.no_plain and rank == 0:
+        from rspi.device import EStep
+        pe = EStep(rec.dset.photons, w['size'], w['num_rot'], rec.shiftx, rec.shifty,
+                   rec.sphere_dia, rec.probmask, rec.dset.bg.cpu().numpy(), form='fp64',
+                   kernel='dynamic')
+        pmodel = torch.from_numpy(model0).to(dev)
+
+        def pstep():
+            pe.run(pmodel)
+            pe.reduce()
+            rec.phaser.run_from_rmax(pmodel, pe.rmax, w['num_rot'], rec.state_vals,
+                                     rec.phaser_rot)
+        for _ in range(min(args.warmup, 1)):
+            pstep()
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(args.steps):
+            pstep()
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pms = p0.elapsed_time(p1) / args.steps
+        plain = {'form': 'fp64 slices + FP64 likelihood matrix, warp-per-frame kernel',
+                 'ms_per_step': pms, 'value': w['n'] * w['n_states'] / (pms * 1e-3),
+                 'speedup_of_chosen': pms / ms}
+        del pe
+        torch.cuda.empty_cache()
 
     # e2e through the public API: host model in, host model + argmax out
     e2e = None
@@ -455,6 +493,9 @@ def run_ours(args):
                             % (sm_count, lanes, clk_mhz)},
         'clocks': clk,
         'e2e': e2e,
+        'plain': plain,
+        'form': {'likelihood': args.form, 'kernel': args.kernel,
+                 'candidates_rescored': n_cand},
         'cpu_baseline': cpu,
         'setup_s': {'generate': t_gen},
     }

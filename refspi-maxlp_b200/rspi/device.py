@@ -182,7 +182,9 @@ class EStep:
         sel, pix2sel, p_pad = geometry.sel_pixels(probmask)
         self.n_sel, self.p_pad = sel.size, p_pad
         t = lambda a, dt=_f64: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)  # noqa: E731
-        self.sel_pix, self.pix2sel = t(sel, _i32), t(pix2sel, _i32)
+        # a detector without likelihood pixels still passes a valid pointer
+        self.sel_pix = t(sel if sel.size else np.zeros(1, 'i4'), _i32)
+        self.pix2sel = t(pix2sel, _i32)
         self.shiftx, self.shifty, self.sphere_dia = t(shiftx), t(shifty), t(sphere_dia)
         self.rot_cs = t(geometry.emc_rotation_table(self.num_rot))
         self.bg = t(np.asarray(bg, dtype='f8').ravel())

@@ -187,7 +187,8 @@ int rspi_screen_loglike(const float *lslices, long long p_row, long long num_rot
                         int warps_per_cta, int n_ctas, cudaStream_t stream);
 
 /* Candidates: state r of frame d is kept when LL32[r][d] >= max32[d] - delta
- * - 2*eps_d, eps_d = 2^-24 ((rows_d + 8) * photons_d * lmax + |max32| + delta + 1)
+ * - 2*eps_d or r == rmax32[d] (the screened first-index argmax, so a frame
+ * whose values are all NaN keeps its first NaN row), eps_d = 2^-24 ((rows_d + 8) * photons_d * lmax + |max32| + delta + 1)
  * bounding |LL32 - LL64| (photons_d = in-mask photons, rows_d from row_off16,
  * lmax = largest |slice value|).  Writes cand_n[d], the exclusive offsets
  * cand_off (n_data + 1, total at [n_data]), the pairs (cand_d, cand_r) up to
@@ -195,7 +196,7 @@ int rspi_screen_loglike(const float *lslices, long long p_row, long long num_rot
  * and noncand[d] = sum over dropped states of exp(LL32 - max32[d]).
  * cnt_part is scratch of n_data * 32 ints. */
 int rspi_screen_candidates(const float *ll, long long n_rows, long long n_data,
-                           const double *max32, const long long *frame_photons,
+                           const double *max32, const int *rmax32, const long long *frame_photons,
                            const long long *row_off16, const float *lmax, double delta,
                            int *cnt_part, int *cand_n, double *noncand, double *thr,
                            long long *cand_off, long long capacity, int *cand_d, int *cand_r,

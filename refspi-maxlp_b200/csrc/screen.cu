@@ -253,7 +253,8 @@ __device__ __forceinline__ double frame_eps(long long phot, long long rows, floa
 
 __global__ void __launch_bounds__(32 * RY)
 k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_data,
-             const double *__restrict__ max32, const long long *__restrict__ phot,
+             const double *__restrict__ max32, const int *__restrict__ rmax32,
+             const long long *__restrict__ phot,
              const long long *__restrict__ row_off16, const float *__restrict__ lmax, double delta,
              int *__restrict__ cnt_part /* n_data x RY */, int *__restrict__ cand_n,
              double *__restrict__ noncand, double *__restrict__ thr_out) {
@@ -267,9 +268,10 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_data,
         const double m = max32[d];
         const long long rows = row_off16[d + 1] - row_off16[d];
         const double thr = m - delta - 2. * frame_eps(phot[d], rows, *lmax, m, delta);
+        const int rm = rmax32[d];
         for (long long r = ty; r < n_rows; r += RY) {
             const double v = (double)ll[r * n_data + d];
-            if (v >= thr) ++c;
+            if (v >= thr || r == rm) ++c;
             else nc += exp(v - m);
         }
         cnt_part[d * RY + ty] = c;
@@ -292,7 +294,8 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_data,
 
 __global__ void __launch_bounds__(32 * RY)
 k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_data,
-            const double *__restrict__ thr, const int *__restrict__ cnt_part,
+            const double *__restrict__ thr, const int *__restrict__ rmax32,
+            const int *__restrict__ cnt_part,
             const long long *__restrict__ cand_off, long long capacity,
             int *__restrict__ cand_d, int *__restrict__ cand_r, int *err) {
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -301,8 +304,9 @@ k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_data,
     long long pos = cand_off[d];
     for (int k = 0; k < ty; ++k) pos += cnt_part[d * RY + k];
     const double th = thr[d];
+    const int rm = rmax32[d];
     for (long long r = ty; r < n_rows; r += RY) {
-        if ((double)ll[r * n_data + d] >= th) {
+        if ((double)ll[r * n_data + d] >= th || r == rm) {
             if (pos < capacity) {
                 cand_d[pos] = (int)d;
                 cand_r[pos] = (int)r;
@@ -476,22 +480,24 @@ extern "C" int rspi_screen_loglike(const float *lslices, long long p_row, long l
 }
 
 extern "C" int rspi_screen_candidates(const float *ll, long long n_rows, long long n_data,
-                                      const double *max32, const long long *frame_photons,
+                                      const double *max32, const int *rmax32,
+                                      const long long *frame_photons,
                                       const long long *row_off16, const float *lmax, double delta,
                                       int *cnt_part, int *cand_n, double *noncand, double *thr,
                                       long long *cand_off, long long capacity, int *cand_d,
                                       int *cand_r, int *err, cudaStream_t stream) {
-    if (!ll || !max32 || !frame_photons || !row_off16 || !lmax || !cnt_part || !cand_n ||
+    if (!ll || !max32 || !rmax32 || !frame_photons || !row_off16 || !lmax || !cnt_part || !cand_n ||
         !noncand || !thr || !cand_off || !cand_d || !cand_r || n_rows <= 0 || n_data <= 0 ||
         n_rows > 0x7fffffffLL || capacity < 0 || !(delta >= 0.))
         return RSPI_ERR_ARG;
     const dim3 block(32, RY);
     const unsigned grid = (unsigned)((n_data + 31) / 32);
-    k_cand_count<<<grid, block, 0, stream>>>(ll, n_rows, n_data, max32, frame_photons, row_off16,
-                                             lmax, delta, cnt_part, cand_n, noncand, thr);
+    k_cand_count<<<grid, block, 0, stream>>>(ll, n_rows, n_data, max32, rmax32, frame_photons,
+                                             row_off16, lmax, delta, cnt_part, cand_n, noncand,
+                                             thr);
     k_scan_counts<<<1, 1024, 0, stream>>>(cand_n, n_data, cand_off);
-    k_cand_fill<<<grid, block, 0, stream>>>(ll, n_rows, n_data, thr, cnt_part, cand_off, capacity,
-                                            cand_d, cand_r, err);
+    k_cand_fill<<<grid, block, 0, stream>>>(ll, n_rows, n_data, thr, rmax32, cnt_part, cand_off,
+                                            capacity, cand_d, cand_r, err);
     RSPI_RETURN_LAUNCH();
 }
 

@@ -222,6 +222,7 @@ class EStep:
         if form == 'screen':
             self.lmax = torch.zeros(1, dtype=torch.float32, device=dev)
             self.max32 = torch.empty(n, dtype=_f64, device=dev)
+            self.rmax32 = torch.empty(n, dtype=_i32, device=dev)
             self.cnt_part = torch.empty(n * 32, dtype=_i32, device=dev)
             self.cand_n = torch.empty(n, dtype=_i32, device=dev)
             self.noncand = torch.empty(n, dtype=_f64, device=dev)
@@ -301,11 +302,11 @@ class EStep:
             call('rspi_frame_reduce', ptr(self.prob), self.prob_code, self.n_rows, n,
                  ptr(self.maxll), ptr(self.rmax), ptr(self.logz), s)
             return self.maxll, self.rmax, self.logz
-        call('rspi_frame_reduce', ptr(self.prob), 0, self.n_rows, n, ptr(self.max32), None,
-             None, s)
+        call('rspi_frame_reduce', ptr(self.prob), 0, self.n_rows, n, ptr(self.max32),
+             ptr(self.rmax32), None, s)
         while True:
             call('rspi_screen_candidates', ptr(self.prob), self.n_rows, n, ptr(self.max32),
-                 ptr(self.ll['frame_sel_photons']), ptr(self.ll16['row_off']), ptr(self.lmax),
+                 ptr(self.rmax32), ptr(self.ll['frame_sel_photons']), ptr(self.ll16['row_off']), ptr(self.lmax),
                  self.delta, ptr(self.cnt_part), ptr(self.cand_n), ptr(self.noncand),
                  ptr(self.thr), ptr(self.cand_off), self.capacity, ptr(self.cand_d),
                  ptr(self.cand_r), ptr(self.ph.err.t), s)

@@ -35,7 +35,7 @@ SIGNATURES = {
     'rspi_ll16_entry_rows': (I, [P] * 8 + [L, L, I, P, P, P]),
     'rspi_ll16_entry_fill': (I, [P] * 8 + [L, L, I, P, P, P]),
     'rspi_screen_loglike': (I, [P, L, L, P, P, P, P, P, L, L, L, P, L, I, I, I, P]),
-    'rspi_screen_candidates': (I, [P, L, L, P, P, P, P, D, P, P, P, P, P, L, P, P, P, P]),
+    'rspi_screen_candidates': (I, [P, L, L, P, P, P, P, P, D, P, P, P, P, P, L, P, P, P, P]),
     'rspi_rescore': (I, [P, P, P, L, L, P, L, P, L, P, P, P, P, P, P, P, P, P, P, P, P, P, P]),
     'rspi_loglike_stream': (I, [I, P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
     'rspi_posterior_pairs': (I, [P, L, L, P, D, P, P, P, L, P, P, P, P, P]),

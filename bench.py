@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument('--frames', type=int, default=None, help='override frame count (testing)')
     ap.add_argument('--form', default='screen', choices=['fp64', 'screen'])
     ap.add_argument('--kernel', default='stream', choices=['stream', 'dynamic'])
+    ap.add_argument('--slice-gb', type=float, default=8.,
+                    help='largest rotated-slice chunk (GB); smaller values give more launches')
     ap.add_argument('--no-plain', action='store_true',
                     help='skip timing the plain form (FP64, dynamic kernel) for comparison')
     ap.add_argument('--cpu-seconds', type=float, default=20.,
@@ -85,7 +87,7 @@ def workload(cfg_id, frames):
                 n_states=nsx * nsy * nd * r['num_rot'], recon=r)
 
 
-def write_inputs(tmp, w, data, form):
+def write_inputs(tmp, w, data, form, slice_gb=8.):
     from rspi.photonfile import write_photons
     os.makedirs(os.path.join(tmp, 'out'), exist_ok=True)
     write_photons(os.path.join(tmp, 'photons.npz'), data)
@@ -94,8 +96,8 @@ def write_inputs(tmp, w, data, form):
     with open(cfg, 'w') as f:
         f.write('[emc]\nsize = %d\nin_photons_file = photons.npz\noutput_folder = out/\n'
                 'log_file = out/EMC.log\nneed_scaling = True\nnum_rot = %d\nnum_modes = 1\n'
-                'sphere_dia = %s\nshiftx = %s\nshifty = %s\nform = %s\n' %
-                (w['size'], r['num_rot'], r['sphere_dia'], r['shiftx'], r['shifty'], form))
+                'sphere_dia = %s\nshiftx = %s\nshifty = %s\nform = %s\nslice_budget_gb = %g\n' %
+                (w['size'], r['num_rot'], r['sphere_dia'], r['shiftx'], r['shifty'], form, slice_gb))
     return cfg
 
 
@@ -305,7 +307,7 @@ def run_ours(args):
                           seed=20260000 + args.config, device=dev)
     t_gen = time.time() - t0
     tmp = tempfile.mkdtemp(prefix='rspi_bench_')
-    cfgfile = write_inputs(tmp, w, data, args.form)
+    cfgfile = write_inputs(tmp, w, data, args.form, args.slice_gb)
     from emc import EMC
     import contextlib
     import io

@@ -202,16 +202,21 @@ int rspi_screen_candidates(const float *ll, long long n_rows, long long n_data,
                            long long *cand_off, long long capacity, int *cand_d, int *cand_r,
                            int *err, cudaStream_t stream);
 
-/* FP64 rescoring of every candidate with rot_log_value on the FP64 holographic
- * slices and the 32-bit entry lists, in the summation order of rspi_loglike
+/* FP64 rescoring of every candidate, in the summation order of rspi_loglike
  * (so the values equal the FP64 form's), written to cand_ll and into ll32;
  * then per frame the first-index argmax, maximum and
- * logz = max + log(sum_cand exp(LL64 - max) + noncand * exp(max32 - max)). */
+ * logz = max + log(sum_cand exp(LL64 - max) + noncand * exp(max32 - max)).
+ * Candidates are regrouped by likelihood row (scratch row_cnt[n_rows],
+ * row_cand_off[n_rows + 1], row_cand[capacity]); one CTA computes a row's
+ * FP64 rotated slice (p_pad values, as rspi_rot_log_slices) in shared
+ * memory and rescores that row's candidate frames. */
 int rspi_rescore(const int *cand_d, const int *cand_r, const long long *cand_off,
-                 long long n_data, long long capacity, const double *holo, long long num_rot,
-                 const double *rot_cs, long long size, const double *bg, const int *sel_pix,
-                 const double *init, const double *scales, const unsigned int *entries32,
-                 const long long *row_off32, double *cand_ll, float *ll32, const double *max32,
+                 long long n_data, long long capacity, long long n_rows, const double *holo,
+                 long long num_rot, const double *rot_cs, long long size, const double *bg,
+                 const int *sel_pix, long long n_sel, long long p_pad, const double *init,
+                 const double *scales, const unsigned int *entries32,
+                 const long long *row_off32, int *row_cnt, long long *row_cand_off,
+                 int *row_cand, double *cand_ll, float *ll32, const double *max32,
                  const double *noncand, double *maxll, int *rmax, double *logz,
                  cudaStream_t stream);
 

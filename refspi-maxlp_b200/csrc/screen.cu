@@ -318,42 +318,77 @@ k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_data,
     }
 }
 
-// One warp per candidate: FP64 likelihood over the frame's packed 32-bit
-// entries, in the FP64 form's order (per lane over rows, then the same
-// warp reduction), so the value equals the FP64 form's.
-__global__ void __launch_bounds__(256)
-k_rescore(const int *__restrict__ cand_d, const int *__restrict__ cand_r,
-          const long long *__restrict__ cand_total, long long capacity,
-          const double *__restrict__ holo, long long num_rot, const double *__restrict__ rot_cs,
-          int size, const double *__restrict__ bg, const int *__restrict__ sel_pix,
-          const double *__restrict__ init, const double *__restrict__ scales,
-          const unsigned int *__restrict__ ent32, const long long *__restrict__ row_off32,
-          double *__restrict__ cand_ll, float *__restrict__ ll32, long long n_data) {
-    const int lane = threadIdx.x & 31;
-    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
-    const long long total = min(*cand_total, capacity);
+// Candidates regrouped by likelihood row: count, scan (rows + 1 offsets),
+// scatter of pair indices.  Order within a row does not affect any value.
+__global__ void k_row_count(const int *__restrict__ cand_r, const long long *__restrict__ total_ptr,
+                            long long capacity, int *__restrict__ row_cnt) {
+    const long long total = min(*total_ptr, capacity);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
+        atomicAdd(&row_cnt[cand_r[i]], 1);
+}
+
+__global__ void k_row_scatter(const int *__restrict__ cand_r, const long long *__restrict__ total_ptr,
+                              long long capacity, const long long *__restrict__ row_off,
+                              int *__restrict__ cursor, int *__restrict__ row_cand) {
+    const long long total = min(*total_ptr, capacity);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const int r = cand_r[i];
+        row_cand[row_off[r] + atomicAdd(&cursor[r], 1)] = (int)i;
+    }
+}
+
+// One CTA per likelihood row with candidates: the row's FP64 rotated slice
+// is computed into shared memory with rot_log_value (as k_rot_log does),
+// then each warp rescores candidate frames exactly as the FP64 form sums
+// them (per lane over the frame's packed rows, fma(count, L, acc), then the
+// warp reduction), so every value equals the FP64 form's.
+__global__ void __launch_bounds__(1024)
+k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ row_cand,
+               long long n_rows, const int *__restrict__ cand_d, const double *__restrict__ holo,
+               long long num_rot, const double *__restrict__ rot_cs, int size,
+               const double *__restrict__ bg, const int *__restrict__ sel_pix, long long n_sel,
+               long long p_pad, const double *__restrict__ init, const double *__restrict__ scales,
+               const unsigned int *__restrict__ ent32, const long long *__restrict__ row_off32,
+               double *__restrict__ cand_ll, float *__restrict__ ll32, long long n_data) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *sl = reinterpret_cast<double *>(smem_raw);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const long long npix = (long long)size * size;
-    for (long long i = warp; i < total; i += nwarp) {
-        const int d = cand_d[i], r = cand_r[i];
+    const unsigned cmax = (unsigned)p_pad - 1;
+    for (long long r = blockIdx.x; r < n_rows; r += gridDim.x) {
+        const long long a = row_off[r], b = row_off[r + 1];
+        if (a == b) continue;   // uniform across the CTA
         const long long s0 = r / num_rot, j = r - s0 * num_rot;
         const double ac = rot_cs[2 * j], as = rot_cs[2 * j + 1];
         const double *w = holo + s0 * npix;
-        double acc = 0.;
-        const unsigned *ep = ent32 + row_off32[d] * 32 + lane;
-        for (long long q = row_off32[d]; q < row_off32[d + 1]; ++q, ep += 32) {
-            const unsigned e = *ep;
-            const unsigned cnt = e & 0xffffu;
-            if (cnt == 0) continue;   // padding slot: contributes 0 * L in the FP64 form
-            const int p = sel_pix[e >> 16];
-            const int x = p / size, y = p - (p / size) * size;
-            acc = fma((double)cnt, rot_log_value(w, x, y, size, ac, as, bg[p]), acc);
+        __syncthreads();        // the previous row's readers are done
+        for (long long c = threadIdx.x; c < p_pad; c += blockDim.x) {
+            double v = 0.;
+            if (c < n_sel) {
+                const int p = sel_pix[c];
+                v = rot_log_value(w, p / size, p - (p / size) * size, size, ac, as, bg[p]);
+            }
+            sl[c] = v;
         }
-        acc = warp_sum(acc);
-        if (lane == 0) {
-            const double v = init[s0] * scales[d] + acc;
-            cand_ll[i] = v;
-            ll32[(long long)r * n_data + d] = (float)v;
+        __syncthreads();
+        const double ini = init[s0];
+        for (long long i = a + wid; i < b; i += nw) {
+            const int pair = row_cand[i];
+            const int d = cand_d[pair];
+            double acc = 0.;
+            const unsigned *ep = ent32 + row_off32[d] * 32 + lane;
+            for (long long q = row_off32[d]; q < row_off32[d + 1]; ++q, ep += 32) {
+                const unsigned e = __ldg(ep);
+                acc = fma((double)(e & 0xffffu), sl[min(e >> 16, cmax)], acc);
+            }
+            acc = warp_sum(acc);
+            if (lane == 0) {
+                const double v = ini * scales[d] + acc;
+                cand_ll[pair] = v;
+                ll32[r * n_data + d] = (float)v;
+            }
         }
     }
 }
@@ -502,20 +537,42 @@ extern "C" int rspi_screen_candidates(const float *ll, long long n_rows, long lo
 }
 
 extern "C" int rspi_rescore(const int *cand_d, const int *cand_r, const long long *cand_off,
-                            long long n_data, long long capacity, const double *holo,
-                            long long num_rot, const double *rot_cs, long long size,
-                            const double *bg, const int *sel_pix, const double *init,
-                            const double *scales, const unsigned int *entries32,
-                            const long long *row_off32, double *cand_ll, float *ll32,
-                            const double *max32, const double *noncand, double *maxll, int *rmax,
-                            double *logz, cudaStream_t stream) {
+                            long long n_data, long long capacity, long long n_rows,
+                            const double *holo, long long num_rot, const double *rot_cs,
+                            long long size, const double *bg, const int *sel_pix, long long n_sel,
+                            long long p_pad, const double *init, const double *scales,
+                            const unsigned int *entries32, const long long *row_off32,
+                            int *row_cnt, long long *row_cand_off, int *row_cand,
+                            double *cand_ll, float *ll32, const double *max32,
+                            const double *noncand, double *maxll, int *rmax, double *logz,
+                            cudaStream_t stream) {
     if (!cand_d || !cand_r || !cand_off || !holo || !rot_cs || !bg || !sel_pix || !init ||
-        !scales || !entries32 || !row_off32 || !cand_ll || !ll32 || !max32 || !noncand ||
-        !maxll || !rmax || !logz || n_data <= 0 || capacity < 0 || size <= 1 || size > 46340)
+        !scales || !entries32 || !row_off32 || !row_cnt || !row_cand_off || !row_cand ||
+        !cand_ll || !ll32 || !max32 || !noncand || !maxll || !rmax || !logz || n_data <= 0 ||
+        capacity < 0 || n_rows <= 0 || n_rows > 0x7fffffffLL || size <= 1 || size > 46340 ||
+        p_pad < n_sel || p_pad % 32 || p_pad > 65536)
         return RSPI_ERR_ARG;
-    k_rescore<<<rspi_sm_count() * 8, 256, 0, stream>>>(
-        cand_d, cand_r, cand_off + n_data, capacity, holo, num_rot, rot_cs, (int)size, bg,
-        sel_pix, init, scales, entries32, row_off32, cand_ll, ll32, n_data);
+    const size_t smem = (size_t)p_pad * sizeof(double);
+    if (smem > (size_t)SMEM_LIMIT - 1024) return RSPI_ERR_ARG;
+    static size_t smem_set = 0;
+    if (smem > smem_set) {
+        if (cudaFuncSetAttribute(k_rescore_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return RSPI_ERR_CUDA;
+        smem_set = smem;
+    }
+    const long long *total = cand_off + n_data;
+    cudaMemsetAsync(row_cnt, 0, sizeof(int) * n_rows, stream);
+    k_row_count<<<rspi_sm_count() * 8, 256, 0, stream>>>(cand_r, total, capacity, row_cnt);
+    k_scan_counts<<<1, 1024, 0, stream>>>(row_cnt, n_rows, row_cand_off);
+    cudaMemsetAsync(row_cnt, 0, sizeof(int) * n_rows, stream);
+    k_row_scatter<<<rspi_sm_count() * 8, 256, 0, stream>>>(cand_r, total, capacity, row_cand_off,
+                                                          row_cnt, row_cand);
+    const int per_sm = max(1, (int)(SMEM_LIMIT / (smem + 1024)));
+    const unsigned grid = (unsigned)min((long long)rspi_sm_count() * min(per_sm, 2), n_rows);
+    k_rescore_rows<<<grid, 1024 / min(per_sm, 2), smem, stream>>>(
+        row_cand_off, row_cand, n_rows, cand_d, holo, num_rot, rot_cs, (int)size, bg, sel_pix,
+        n_sel, p_pad, init, scales, entries32, row_off32, cand_ll, ll32, n_data);
     k_cand_finalize<<<rspi_blocks(n_data, 256), 256, 0, stream>>>(
         cand_off, cand_r, cand_ll, max32, noncand, n_data, capacity, maxll, rmax, logz);
     RSPI_RETURN_LAUNCH();

@@ -14,8 +14,9 @@ Optional ``[emc]`` keys beyond the reference: ``form`` (``fp64``: FP64
 slices and FP64 likelihood matrix; ``screen``: FP32 screening pass with
 FP64 rescoring of every state that can be the argmax or carry posterior
 mass, same argmax/maximum/log-sum-exp as ``fp64``), ``screen_delta``
-(default 30 nats), ``states_per_tile``, ``warps_per_cta``, ``phaser_iter``
-(default 10, maxLP.py:320,335).
+(default 20 nats), ``states_per_tile``, ``warps_per_cta``, ``phaser_iter``
+(default 10, maxLP.py:320,335), ``slice_budget_gb`` (rotated slices are built
+in chunks of at most this size, default 8).
 """
 import configparser
 import os.path as op
@@ -65,7 +66,8 @@ class EMC():
                            self.shifty, self.sphere_dia, self.probmask,
                            self.dset.bg.cpu().numpy(), form=self.form,
                            states_per_tile=self.states_per_tile, warps=self.warps_per_cta,
-                           delta=self.screen_delta)
+                           delta=self.screen_delta,
+                           slice_budget_bytes=int(self.slice_budget_gb * (1 << 30)))
         self.prob = self.estep.prob
         self.state_vals = torch.from_numpy(self._state_values).to(self.device)
         self.phaser_rot = torch.from_numpy(geometry.phaser_rotation_table(
@@ -84,10 +86,11 @@ class EMC():
         self.form = config.get('emc', 'form', fallback='fp64')
         if self.form not in ('fp64', 'screen'):
             raise ValueError('emc:form must be fp64 or screen')
-        self.screen_delta = config.getfloat('emc', 'screen_delta', fallback=30.)
+        self.screen_delta = config.getfloat('emc', 'screen_delta', fallback=20.)
         self.states_per_tile = config.getint('emc', 'states_per_tile', fallback=0) or None
         self.warps_per_cta = config.getint('emc', 'warps_per_cta', fallback=32)
         self.phaser_iter = config.getint('emc', 'phaser_iter', fallback=10)
+        self.slice_budget_gb = config.getfloat('emc', 'slice_budget_gb', fallback=8.)
 
     def _generate_states(self, config):
         '''emc.py:67-87'''

@@ -165,7 +165,7 @@ class EStep:
 
     def __init__(self, photons, size, num_rot, shiftx, shifty, sphere_dia, probmask, bg,
                  form='fp64', states_per_tile=None, warps=32, n_ctas=0,
-                 slice_budget_bytes=8 << 30, delta=30., cand_per_frame=64, kernel='stream'):
+                 slice_budget_bytes=8 << 30, delta=20., cand_per_frame=64, kernel='stream'):
         if form not in ('fp64', 'screen'):
             raise ValueError('form must be fp64 or screen')
         if kernel not in ('stream', 'dynamic'):
@@ -228,6 +228,8 @@ class EStep:
             self.noncand = torch.empty(n, dtype=_f64, device=dev)
             self.thr = torch.empty(n, dtype=_f64, device=dev)
             self.cand_off = torch.empty(n + 1, dtype=_i64, device=dev)
+            self.row_cnt = torch.empty(self.n_rows, dtype=_i32, device=dev)
+            self.row_cand_off = torch.empty(self.n_rows + 1, dtype=_i64, device=dev)
             self._alloc_candidates(max(1024, int(cand_per_frame) * n))
         self.check_capacity = True
 
@@ -237,6 +239,7 @@ class EStep:
         self.cand_d = torch.empty(self.capacity, dtype=_i32, device=dev)
         self.cand_r = torch.empty(self.capacity, dtype=_i32, device=dev)
         self.cand_ll = torch.empty(self.capacity, dtype=_f64, device=dev)
+        self.row_cand = torch.empty(self.capacity, dtype=_i32, device=dev)
 
     # -- stages ------------------------------------------------------------
     def slices(self, model):
@@ -319,9 +322,10 @@ class EStep:
                 self.n_candidates = total
             break
         call('rspi_rescore', ptr(self.cand_d), ptr(self.cand_r), ptr(self.cand_off), n,
-             self.capacity, ptr(self.holo), self.num_rot, ptr(self.rot_cs), self.size,
-             ptr(self.bg), ptr(self.sel_pix), ptr(self.init), ptr(self.ph.scales),
-             ptr(self.ll['entries']), ptr(self.ll['row_off']), ptr(self.cand_ll),
+             self.capacity, self.n_rows, ptr(self.holo), self.num_rot, ptr(self.rot_cs),
+             self.size, ptr(self.bg), ptr(self.sel_pix), self.n_sel, self.p_pad, ptr(self.init),
+             ptr(self.ph.scales), ptr(self.ll['entries']), ptr(self.ll['row_off']),
+             ptr(self.row_cnt), ptr(self.row_cand_off), ptr(self.row_cand), ptr(self.cand_ll),
              ptr(self.prob), ptr(self.max32), ptr(self.noncand), ptr(self.maxll),
              ptr(self.rmax), ptr(self.logz), s)
         return self.maxll, self.rmax, self.logz

@@ -62,6 +62,7 @@ def parse_args():
                     help='target CPU time of the bounded oracle sample')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--no-clocks', action='store_true', help='do not sample nvidia-smi clocks')
     return ap.parse_args()
 
 
@@ -347,7 +348,8 @@ def run_ours(args):
         dist.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(local)
-    clocks.start()
+    if not args.no_clocks:
+        clocks.start()
     launches0 = rlib.launch_count
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -432,16 +434,18 @@ def run_ours(args):
 
     pk = peaks()
     es = rec.estep
-    total_rows = es.ll['total_rows']
+    # entry rows of 32 photon slots the likelihood kernel walks per likelihood row
+    total_rows = es.ll16['total_rows'] if es.form == 'screen' else es.ll['total_rows']
     esz = 4 if es.slice_code == 0 else 8
     osz = 4 if es.prob_code == 0 else 8
     # dominant kernel: the likelihood kernel (row a7); algorithmic bytes per
     # launch = its slices in + its LL rows out + the packed photon entries once
     rows_per_launch = es.n_rows / max(1, ll_launches)
-    alg_bytes = rows_per_launch * (es.p_pad * esz + w['n'] * osz) + total_rows * 128 + 8 * w['n']
+    ent_bytes = total_rows * 32 * (2 if es.form == 'screen' else 4)
+    alg_bytes = rows_per_launch * (es.p_row * esz + w['n'] * osz) + ent_bytes + 8 * w['n']
     ll_launch_ms = ll_ms / max(1, ll_launches)
     achieved = alg_bytes / (ll_launch_ms * 1e-3) / 1e9
-    # on-chip gather roofline: one shared-memory gather per entry slot per row
+    # on-chip gather roofline: one shared-memory value per entry slot per likelihood row
     gathers = rows_per_launch * total_rows * 32
     sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
     clk_mhz = (clk or {}).get('sm_mhz') or 1965.
@@ -483,7 +487,9 @@ def run_ours(args):
                    'l2': 'inputs larger than L2 (slices %.1f GB, likelihoods %.1f GB per step)' %
                    (es.n_rows * es.p_pad * esz / 1e9, es.n_rows * w['n'] * osz / 1e9)},
         'gpu_launches': launches // args.steps * args.steps,
-        'roofline': {'kernel': 'k_loglike (likelihood, row a7)', 'bound': 'hbm',
+        'roofline': {'kernel': ('k_screen_ll2 (FP32 screening likelihood, row a7)'
+                                if es.form == 'screen' else 'k_ll_stream / k_loglike (FP64 likelihood, row a7)'),
+                     'bound': 'hbm',
                      'achieved': achieved, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
                      'frac': achieved / pk['hbm_gbs'], 'traffic': traffic,
                      'peak_source': pk['source'] + ' (HBM copy)',

@@ -186,6 +186,22 @@ int rspi_screen_loglike(const float *lslices, long long p_row, long long num_rot
                         long long row_end, float *ll, long long ll_stride, int states_per_tile,
                         int warps_per_cta, int n_ctas, cudaStream_t stream);
 
+/* Interleaved screening likelihood (the chosen kernel): same inputs and
+ * output as rspi_screen_loglike (frames in index order, no frame_order);
+ * the tile's T in {1, 2, 4} rows are staged as sl[c*T + t] so one vector
+ * gather serves all T rows.  Requires every entry index < p_row (check once
+ * with rspi_entries16_check). */
+int rspi_screen_loglike2(const float *lslices, long long p_row, long long num_rot,
+                         const double *init, const double *scales,
+                         const unsigned short *entries, const long long *row_off,
+                         long long n_data, long long row_begin, long long row_end, float *ll,
+                         long long ll_stride, int states_per_tile, int warps_per_cta,
+                         int n_ctas, cudaStream_t stream);
+
+/* *max_index = largest value in a 16-bit entry array. */
+int rspi_entries16_check(const unsigned short *entries, long long n_entries,
+                         unsigned *max_index, cudaStream_t stream);
+
 /* Candidates: state r of frame d is kept when LL32[r][d] >= max32[d] - delta
  * - 2*eps_d or r == rmax32[d] (the screened first-index argmax, so a frame
  * whose values are all NaN keeps its first NaN row), eps_d = 2^-24 ((rows_d + 8) * photons_d * lmax + |max32| + delta + 1)

@@ -1,0 +1,223 @@
+// Screening likelihood, interleaved form (row a7, chosen form).
+//
+// The FP32 slices of a tile's T rows are staged in shared memory
+// interleaved by pixel, sl[c*T + t], so one vector gather (8 bytes for T=2,
+// 16 bytes for T=4) brings all T rows' values of a photon.  The photon
+// entries are the 16-bit layout of rspi_ll16_entry_fill: lane b holds an
+// index = b (mod 32); for the vector gathers a half (T=2) or a quarter (T=4)
+// warp then touches distinct 8- or 16-byte banks, so the gathers stay
+// conflict-free.  Indices are validated once on the host side of the
+// pipeline (rspi_entries16_check), so the hot loop has no clamp.  Each warp
+// streams a contiguous, word-balanced range of frames with a prefetch that
+// crosses frame boundaries; loop indices are 32-bit.
+#include "rspi_common.cuh"
+
+namespace {
+
+constexpr int SMEM_LIMIT = 227 * 1024;
+constexpr int PF = 8;
+
+template <int T>
+struct Vec;
+template <>
+struct Vec<1> {
+    using type = float;
+    __device__ __forceinline__ static void add(float (&a)[1], type v0, type v1) { a[0] += v0 + v1; }
+};
+template <>
+struct Vec<2> {
+    using type = float2;
+    __device__ __forceinline__ static void add(float (&a)[2], type v0, type v1) {
+        a[0] += v0.x + v1.x;
+        a[1] += v0.y + v1.y;
+    }
+};
+template <>
+struct Vec<4> {
+    using type = float4;
+    __device__ __forceinline__ static void add(float (&a)[4], type v0, type v1) {
+        a[0] += v0.x + v1.x;
+        a[1] += v0.y + v1.y;
+        a[2] += v0.z + v1.z;
+        a[3] += v0.w + v1.w;
+    }
+};
+
+template <int T>
+__global__ void __launch_bounds__(1024)
+k_screen_ll2(const float *__restrict__ lsl, int p_row, int num_rot,
+             const double *__restrict__ init, const double *__restrict__ scales,
+             const unsigned *__restrict__ words, const long long *__restrict__ row_off, int n_data,
+             long long row_begin, long long row_end, float *__restrict__ ll, long long ll_stride) {
+    using V = typename Vec<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *sl = reinterpret_cast<V *>(smem_raw);
+    float *slf = reinterpret_cast<float *>(smem_raw);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const long long n_tiles = (row_end - row_begin + T - 1) / T;
+
+    // word-balanced frame range of this warp (word offsets = row offsets / 2)
+    const int qtot = (int)(row_off[n_data] >> 1);
+    auto lower = [&](int target) {
+        int lo = 0, hi = n_data;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((int)(row_off[mid] >> 1) < target) lo = mid + 1;
+            else hi = mid;
+        }
+        return lo;
+    };
+    const int fb = wid == 0 ? 0 : lower((int)((long long)qtot * wid / nw));
+    const int fe = wid == nw - 1 ? n_data : lower((int)((long long)qtot * (wid + 1) / nw));
+
+    for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const long long first = row_begin + tile * T;
+        const int nt = (int)min((long long)T, row_end - first);
+        __syncthreads();
+        // stage and interleave: sl[c][t] = L[first + t][c]
+        const float *src = lsl + (first - row_begin) * (long long)p_row;
+        for (int i = threadIdx.x; i < T * p_row; i += blockDim.x) {
+            const int t = i / p_row, c = i - t * p_row;
+            slf[c * T + t] = t < nt ? __ldg(src + i) : 0.f;
+        }
+        __syncthreads();
+        if (fb >= fe) continue;
+
+        double ini[T];
+#pragma unroll
+        for (int t = 0; t < T; ++t) ini[t] = t < nt ? init[(first + t) / num_rot] : 0.;
+        float acc[T];
+#pragma unroll
+        for (int t = 0; t < T; ++t) acc[t] = 0.f;
+
+        int f = fb;
+        int q = (int)(row_off[fb] >> 1);
+        const int qend = (int)(row_off[fe] >> 1);
+        int fend = (int)(row_off[f + 1] >> 1);
+        auto finish = [&]() {
+#pragma unroll
+            for (int t = 0; t < T; ++t) acc[t] = warp_sum(acc[t]);
+            if (lane < nt) {
+                float a = acc[0];
+#pragma unroll
+                for (int t = 1; t < T; ++t)
+                    if (t == lane) a = acc[t];
+                double s0 = ini[0];
+#pragma unroll
+                for (int t = 1; t < T; ++t)
+                    if (t == lane) s0 = ini[t];
+                ll[(first + lane - row_begin) * ll_stride + f] =
+                    (float)(s0 * scales[f] + (double)a);
+            }
+#pragma unroll
+            for (int t = 0; t < T; ++t) acc[t] = 0.f;
+            ++f;
+            fend = f < fe ? (int)(row_off[f + 1] >> 1) : qend + 1;
+        };
+        while (f < fe && fend == q) finish();   // frames without photons
+
+        const unsigned *wp = words + (long long)q * 32 + lane;
+        unsigned cur[PF], nxt[PF];
+#pragma unroll
+        for (int k = 0; k < PF; ++k) cur[k] = q + k < qend ? __ldg(wp + 32 * k) : 0u;
+        while (q < qend) {
+            const int nb = min(PF, qend - q);
+#pragma unroll
+            for (int k = 0; k < PF; ++k) nxt[k] = q + PF + k < qend ? __ldg(wp + 32 * (PF + k)) : 0u;
+#pragma unroll
+            for (int k = 0; k < PF; ++k) {
+                if (k < nb) {
+                    const unsigned w = cur[k];
+                    Vec<T>::add(acc, sl[w & 0xffffu], sl[w >> 16]);
+                    if (q + k + 1 == fend) {
+                        finish();
+                        while (f < fe && fend == q + k + 1) finish();
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < PF; ++k) cur[k] = nxt[k];
+            q += PF;
+            wp += 32 * PF;
+        }
+    }
+}
+
+template <int T>
+int launch2(const float *lsl, long long p_row, long long num_rot, const double *init,
+            const double *scales, const unsigned *words, const long long *row_off,
+            long long n_data, long long r0, long long r1, float *ll, long long stride, int warps,
+            int n_ctas, cudaStream_t stream) {
+    const size_t smem = (size_t)T * p_row * sizeof(float);
+    if (smem > (size_t)SMEM_LIMIT - 1024) return RSPI_ERR_ARG;
+    static size_t smem_set = 0;
+    if (smem > smem_set) {
+        if (cudaFuncSetAttribute(k_screen_ll2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return RSPI_ERR_CUDA;
+        smem_set = smem;
+    }
+    const long long n_tiles = (r1 - r0 + T - 1) / T;
+    if (n_ctas <= 0) {
+        const int per_sm = max(1, (int)(SMEM_LIMIT / (smem + 1024)));
+        n_ctas = rspi_sm_count() * min(per_sm, max(1, 2048 / (warps * 32)));
+    }
+    if (n_ctas > n_tiles) n_ctas = (int)n_tiles;
+    k_screen_ll2<T><<<n_ctas, warps * 32, smem, stream>>>(
+        lsl, (int)p_row, (int)num_rot, init, scales, words, row_off, (int)n_data, r0, r1, ll,
+        stride);
+    RSPI_RETURN_LAUNCH();
+}
+
+// max entry index of a 16-bit entry array (validation before the clamp-free kernel)
+__global__ void k_max_u16(const unsigned short *__restrict__ e, long long n,
+                          unsigned *__restrict__ out) {
+    unsigned m = 0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        m = max(m, (unsigned)e[i]);
+    m = (unsigned)warp_max_int((int)m);
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+}  // namespace
+
+extern "C" int rspi_entries16_check(const unsigned short *entries, long long n_entries,
+                                    unsigned *max_index, cudaStream_t stream) {
+    if (!entries || !max_index || n_entries < 0) return RSPI_ERR_ARG;
+    cudaMemsetAsync(max_index, 0, sizeof(unsigned), stream);
+    if (n_entries > 0)
+        k_max_u16<<<rspi_blocks(n_entries, 256), 256, 0, stream>>>(entries, n_entries, max_index);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_screen_loglike2(const float *lslices, long long p_row, long long num_rot,
+                                    const double *init, const double *scales,
+                                    const unsigned short *entries, const long long *row_off,
+                                    long long n_data, long long row_begin, long long row_end,
+                                    float *ll, long long ll_stride, int states_per_tile,
+                                    int warps_per_cta, int n_ctas, cudaStream_t stream) {
+    if (!lslices || !init || !scales || !entries || !row_off || !ll || n_data <= 0 ||
+        n_data > 0x7fffffffLL || p_row <= 32 || p_row % 32 || p_row > 65536 || num_rot <= 0 ||
+        num_rot > 0x7fffffffLL || row_begin < 0 || row_end < row_begin || ll_stride < n_data ||
+        warps_per_cta < 1 || warps_per_cta > 32)
+        return RSPI_ERR_ARG;
+    if ((reinterpret_cast<uintptr_t>(lslices) & 15) != 0 ||
+        (reinterpret_cast<uintptr_t>(entries) & 3) != 0)
+        return RSPI_ERR_ARG;
+    if (row_end == row_begin) return RSPI_OK;
+    const unsigned *w = reinterpret_cast<const unsigned *>(entries);
+    switch (states_per_tile) {
+        case 1:
+            return launch2<1>(lslices, p_row, num_rot, init, scales, w, row_off, n_data,
+                              row_begin, row_end, ll, ll_stride, warps_per_cta, n_ctas, stream);
+        case 2:
+            return launch2<2>(lslices, p_row, num_rot, init, scales, w, row_off, n_data,
+                              row_begin, row_end, ll, ll_stride, warps_per_cta, n_ctas, stream);
+        case 4:
+            return launch2<4>(lslices, p_row, num_rot, init, scales, w, row_off, n_data,
+                              row_begin, row_end, ll, ll_stride, warps_per_cta, n_ctas, stream);
+        default:
+            return RSPI_ERR_ARG;
+    }
+}

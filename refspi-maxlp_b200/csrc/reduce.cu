@@ -16,16 +16,17 @@ struct Acc {
     int i;
 };
 
+template <bool LSE>
 __device__ __forceinline__ void acc_push(Acc &a, double v, int r) {
     if (a.i < 0) {
         a = Acc{v, 1., r};
         return;
     }
     if (argmax_better(v, r, a.m, a.i)) {
-        a.s = isnan(v) || isnan(a.m) ? a.s + 1. : a.s * exp(a.m - v) + 1.;
+        if (LSE) a.s = isnan(v) || isnan(a.m) ? a.s + 1. : a.s * exp(a.m - v) + 1.;
         a.m = v;
         a.i = r;
-    } else {
+    } else if (LSE) {
         a.s += isnan(a.m) ? 1. : exp(v - a.m);
     }
 }
@@ -42,7 +43,7 @@ __device__ __forceinline__ Acc acc_merge(Acc a, Acc b) {
     return a;
 }
 
-template <typename TL>
+template <typename TL, bool LSE>
 __global__ void __launch_bounds__(32 * RY)
 k_frame_reduce(const TL *__restrict__ ll, long long n_rows, long long n_data,
                double *__restrict__ maxll, int *__restrict__ rmax, double *__restrict__ logz) {
@@ -53,7 +54,7 @@ k_frame_reduce(const TL *__restrict__ ll, long long n_rows, long long n_data,
     const long long d = (long long)blockIdx.x * 32 + tx;
     Acc a{0., 0., -1};
     if (d < n_data)
-        for (long long r = ty; r < n_rows; r += RY) acc_push(a, (double)ll[r * n_data + d], (int)r);
+        for (long long r = ty; r < n_rows; r += RY) acc_push<LSE>(a, (double)ll[r * n_data + d], (int)r);
     sm[ty][tx] = a.m;
     ss[ty][tx] = a.s;
     si[ty][tx] = a.i;
@@ -75,12 +76,18 @@ extern "C" int rspi_frame_reduce(const void *ll, int ll_dtype, long long n_rows,
     if (!ll || n_rows <= 0 || n_data <= 0 || n_rows > 0x7fffffffLL) return RSPI_ERR_ARG;
     const dim3 block(32, RY);
     const unsigned grid = (unsigned)((n_data + 31) / 32);
-    if (ll_dtype == 1)
-        k_frame_reduce<double><<<grid, block, 0, stream>>>((const double *)ll, n_rows, n_data,
-                                                           maxll, rmax, logz);
+    if (ll_dtype == 1 && logz)
+        k_frame_reduce<double, true><<<grid, block, 0, stream>>>((const double *)ll, n_rows,
+                                                                 n_data, maxll, rmax, logz);
+    else if (ll_dtype == 1)
+        k_frame_reduce<double, false><<<grid, block, 0, stream>>>((const double *)ll, n_rows,
+                                                                  n_data, maxll, rmax, logz);
+    else if (ll_dtype == 0 && logz)
+        k_frame_reduce<float, true><<<grid, block, 0, stream>>>((const float *)ll, n_rows, n_data,
+                                                                maxll, rmax, logz);
     else if (ll_dtype == 0)
-        k_frame_reduce<float><<<grid, block, 0, stream>>>((const float *)ll, n_rows, n_data, maxll,
-                                                          rmax, logz);
+        k_frame_reduce<float, false><<<grid, block, 0, stream>>>((const float *)ll, n_rows,
+                                                                 n_data, maxll, rmax, logz);
     else
         return RSPI_ERR_ARG;
     RSPI_RETURN_LAUNCH();

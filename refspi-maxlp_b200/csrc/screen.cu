@@ -272,7 +272,7 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_data,
         for (long long r = ty; r < n_rows; r += RY) {
             const double v = (double)ll[r * n_data + d];
             if (v >= thr || r == rm) ++c;
-            else nc += exp(v - m);
+            else nc += (double)expf((float)(v - m));   // each term < exp(-delta)
         }
         cnt_part[d * RY + ty] = c;
         if (ty == 0) thr_out[d] = thr;
@@ -393,30 +393,45 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
     }
 }
 
-// Per frame over its candidates: first-index argmax, max and log-sum-exp.
+// Per frame over its candidates (one warp per frame): first-index argmax,
+// max and log-sum-exp.
 __global__ void k_cand_finalize(const long long *__restrict__ cand_off,
                                 const int *__restrict__ cand_r, const double *__restrict__ cand_ll,
                                 const double *__restrict__ max32, const double *__restrict__ noncand,
                                 long long n_data, long long capacity, double *__restrict__ maxll,
                                 int *__restrict__ rmax, double *__restrict__ logz) {
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long d = (long long)blockIdx.x * blockDim.x + threadIdx.x; d < n_data; d += stride) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long d = warp; d < n_data; d += nwarp) {
         const long long a = cand_off[d], b = min(cand_off[d + 1], capacity);
-        double m = 0.;
-        int idx = -1;
-        for (long long i = a; i < b; ++i) {
+        double m = -INFINITY;
+        int idx = 0x7fffffff;
+        for (long long i = a + lane; i < b; i += 32) {
             const double v = cand_ll[i];
-            if (idx < 0 || argmax_better(v, cand_r[i], m, idx)) {
+            if (argmax_better(v, cand_r[i], m, idx)) {
                 m = v;
                 idx = cand_r[i];
             }
         }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double om = __shfl_xor_sync(RSPI_FULL_MASK, m, o);
+            const int oi = __shfl_xor_sync(RSPI_FULL_MASK, idx, o);
+            if (argmax_better(om, oi, m, idx)) {
+                m = om;
+                idx = oi;
+            }
+        }
         double s = 0.;
-        for (long long i = a; i < b; ++i) s += exp(cand_ll[i] - m);
-        s += noncand[d] * exp(max32[d] - m);
-        maxll[d] = m;
-        rmax[d] = idx;
-        logz[d] = m + log(s);
+        for (long long i = a + lane; i < b; i += 32) s += exp(cand_ll[i] - m);
+        s = warp_sum(s);
+        if (lane == 0) {
+            s += noncand[d] * exp(max32[d] - m);
+            maxll[d] = m;
+            rmax[d] = b > a ? idx : -1;
+            logz[d] = m + log(s);
+        }
     }
 }
 
@@ -573,7 +588,7 @@ extern "C" int rspi_rescore(const int *cand_d, const int *cand_r, const long lon
     k_rescore_rows<<<grid, 1024 / min(per_sm, 2), smem, stream>>>(
         row_cand_off, row_cand, n_rows, cand_d, holo, num_rot, rot_cs, (int)size, bg, sel_pix,
         n_sel, p_pad, init, scales, entries32, row_off32, cand_ll, ll32, n_data);
-    k_cand_finalize<<<rspi_blocks(n_data, 256), 256, 0, stream>>>(
+    k_cand_finalize<<<rspi_blocks(n_data * 32, 256), 256, 0, stream>>>(
         cand_off, cand_r, cand_ll, max32, noncand, n_data, capacity, maxll, rmax, logz);
     RSPI_RETURN_LAUNCH();
 }

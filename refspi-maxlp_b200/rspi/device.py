@@ -148,6 +148,10 @@ class DevicePhotons:
         entries = torch.empty(max(2, total) * 32, dtype=torch.int16, device=dev)
         call('rspi_ll16_entry_fill', *args, ptr(row_off), ptr(entries), s)
         order = torch.argsort(rows, descending=True, stable=True).to(_i32)
+        mx = torch.zeros(1, dtype=_i32, device=dev)
+        call('rspi_entries16_check', ptr(entries), max(2, total) * 32, ptr(mx), s)
+        if int(mx.item()) >= int(p_zero) + 32:
+            raise RuntimeError('16-bit entry index %d outside the slice row' % int(mx.item()))
         self._ll16 = dict(key=key, frame_rows=rows, row_off=row_off, entries=entries,
                           order=order, total_rows=total)
         return self._ll16
@@ -165,7 +169,7 @@ class EStep:
 
     def __init__(self, photons, size, num_rot, shiftx, shifty, sphere_dia, probmask, bg,
                  form='fp64', states_per_tile=None, warps=32, n_ctas=0,
-                 slice_budget_bytes=8 << 30, delta=20., cand_per_frame=64, kernel='stream'):
+                 slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel='stream'):
         if form not in ('fp64', 'screen'):
             raise ValueError('form must be fp64 or screen')
         if kernel not in ('stream', 'dynamic'):
@@ -201,11 +205,15 @@ class EStep:
         self.slice_torch = torch.float32 if self.slice_code == 0 else _f64
         self.prob_torch = torch.float32 if self.prob_code == 0 else _f64
         tmax = self.lib.rspi_loglike_max_tile(self.p_row, self.slice_code)
+        if form == 'screen' and kernel == 'stream':
+            tmax = 4 if tmax >= 4 else (2 if tmax >= 2 else tmax)   # interleaved: 1, 2 or 4
         if tmax == 0:
             raise ValueError('a %d-pixel likelihood slice does not fit in shared memory' % self.n_sel)
         self.tile = int(states_per_tile or tmax)
         if self.tile > tmax:
             raise ValueError('states_per_tile %d exceeds the shared-memory limit %d' % (self.tile, tmax))
+        if form == 'screen' and kernel == 'stream' and self.tile not in (1, 2, 4):
+            raise ValueError('the interleaved screening kernel takes 1, 2 or 4 states per tile')
         self.warps, self.n_ctas = int(warps), int(n_ctas)
         esz = 4 if self.slice_code == 0 else 8
         rows = max(self.tile, (slice_budget_bytes // (self.p_row * esz)) // self.tile * self.tile)
@@ -230,7 +238,8 @@ class EStep:
             self.cand_off = torch.empty(n + 1, dtype=_i64, device=dev)
             self.row_cnt = torch.empty(self.n_rows, dtype=_i32, device=dev)
             self.row_cand_off = torch.empty(self.n_rows + 1, dtype=_i64, device=dev)
-            self._alloc_candidates(max(1024, int(cand_per_frame) * n))
+            per = int(cand_per_frame) if cand_per_frame else min(self.n_rows, 8192)
+            self._alloc_candidates(max(1024, per * n))
         self.check_capacity = True
 
     def _alloc_candidates(self, cap):
@@ -269,8 +278,13 @@ class EStep:
         its first row on (default: the chunk buffer)."""
         lsl = self.lsl if lsl is None else lsl
         n = self.ph.num_data
-        if self.kernel == 'stream':
-            ent = self.ll if self.form == 'fp64' else self.ll16
+        if self.kernel == 'stream' and self.form == 'screen':
+            l16 = self.ll16
+            call('rspi_screen_loglike2', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
+                 ptr(self.ph.scales), ptr(l16['entries']), ptr(l16['row_off']), n, r0, r1,
+                 ptr(self.prob[r0]), n, self.tile, self.warps, self.n_ctas, cur_stream())
+        elif self.kernel == 'stream':
+            ent = self.ll
             call('rspi_loglike_stream', self.slice_code, ptr(lsl), self.p_row, self.num_rot,
                  ptr(self.init), ptr(self.ph.scales), ptr(ent['entries']), ptr(ent['row_off']),
                  n, r0, r1, ptr(self.prob[r0]), n, self.tile, self.warps, self.n_ctas,
@@ -317,7 +331,7 @@ class EStep:
                 total = int(self.cand_off[n].item())
                 if total > self.capacity:
                     self.ph.err.t.zero_()
-                    self._alloc_candidates(int(total * 1.25) + 1024)
+                    self._alloc_candidates(int(total * 1.5) + 1024)
                     continue
                 self.n_candidates = total
             break

@@ -149,7 +149,7 @@ class DevicePhotons:
         call('rspi_ll16_entry_fill', *args, ptr(row_off), ptr(entries), s)
         order = torch.argsort(rows, descending=True, stable=True).to(_i32)
         mx = torch.zeros(1, dtype=_i32, device=dev)
-        call('rspi_entries16_check', ptr(entries), max(2, total) * 32, ptr(mx), s)
+        call('rspi_entries16_check', ptr(entries), total * 32, ptr(mx), s)
         if int(mx.item()) >= int(p_zero) + 32:
             raise RuntimeError('16-bit entry index %d outside the slice row' % int(mx.item()))
         self._ll16 = dict(key=key, frame_rows=rows, row_off=row_off, entries=entries,

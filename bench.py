@@ -319,50 +319,47 @@ def run_ours(args):
     model0 = synth.initial_model(w['size'], 20260100 + args.config)
     stream = torch.cuda.current_stream()
 
-    # kernel-level events for the roofline (on the launching stream)
-    ev = {'loglike': [], 'pattern_main': []}
-    orig_loglike = rec.estep.loglike
-
-    def timed_loglike(r0, r1, lsl=None):
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        orig_loglike(r0, r1, lsl)
-        b.record(stream)
-        ev['loglike'].append((a, b, r1 - r0))
-    rec.estep.loglike = timed_loglike
-
-    dmodel = torch.from_numpy(model0).to(dev)
-
-    def step():
-        rec.estep.run(dmodel)
-        rec.estep.reduce()
-        rec.phaser.run_from_rmax(dmodel, rec.estep.rmax, w['num_rot'], rec.state_vals,
-                                 rec.phaser_rot)
-
-    for _ in range(args.warmup):
-        step()
+    # CUDA events around every likelihood launch; the launches captured in the
+    # graph keep their events, so after the timed replays they hold the last
+    # replay's kernel times (recorded on the launching stream)
+    es = rec.estep
+    rec._dmodel.copy_(torch.from_numpy(model0).to(dev))
+    l0 = rlib.launch_count
+    rec._device_step()                      # one eager iteration: counts our launches
     torch.cuda.synchronize()
-    ev['loglike'].clear()
+    kernels_per_step = rlib.launch_count - l0
+    n_chunks = (es.n_rows + es.chunk_rows - 1) // es.chunk_rows
+    es.ll_events = []
+    rec.device_step()                       # eager once more, then capture the graph
+    graph_events = es.ll_events[-n_chunks:] if rec.use_graph else None
+    for _ in range(max(0, args.warmup - 2)):
+        rec.device_step()
+    if not rec.use_graph:
+        es.ll_events = []
+    torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     clocks = Clocks(local)
     if not args.no_clocks:
         clocks.start()
-    launches0 = rlib.launch_count
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
-        step()
+        rec.device_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    launches = rlib.launch_count - launches0
+    launches = kernels_per_step * args.steps
     ms = e0.elapsed_time(e1) / args.steps
     clk = clocks.stop()
-    ll_ms = sum(a.elapsed_time(b) for a, b, _ in ev['loglike']) / args.steps
-    ll_launches = len(ev['loglike']) // args.steps
+    if rec.use_graph:
+        ll_ms = sum(a.elapsed_time(b) for a, b, _ in graph_events)
+        ll_launches = len(graph_events)
+    else:
+        ll_ms = sum(a.elapsed_time(b) for a, b, _ in es.ll_events) / args.steps
+        ll_launches = len(es.ll_events) // args.steps
+    es.ll_events = None
     rec.dset.photons.err.check('bench')
     if world > 1:
         t = torch.tensor([ms], device=dev)
@@ -486,7 +483,8 @@ def run_ours(args):
                    'form': args.form, 'parallelism': 'replicas' if world > 1 else 'single',
                    'l2': 'inputs larger than L2 (slices %.1f GB, likelihoods %.1f GB per step)' %
                    (es.n_rows * es.p_pad * esz / 1e9, es.n_rows * w['n'] * osz / 1e9)},
-        'gpu_launches': launches // args.steps * args.steps,
+        'gpu_launches': launches,
+        'cuda_graph': rec.use_graph,
         'roofline': {'kernel': ('k_screen_ll2 (FP32 screening likelihood, row a7)'
                                 if es.form == 'screen' else 'k_ll_stream / k_loglike (FP64 likelihood, row a7)'),
                      'bound': 'hbm',

@@ -16,7 +16,9 @@ FP64 rescoring of every state that can be the argmax or carry posterior
 mass, same argmax/maximum/log-sum-exp as ``fp64``), ``screen_delta``
 (default 20 nats), ``states_per_tile``, ``warps_per_cta``, ``phaser_iter``
 (default 10, maxLP.py:320,335), ``slice_budget_gb`` (rotated slices are built
-in chunks of at most this size, default 8).
+in chunks of at most this size, default 8), ``cuda_graph`` (capture the whole
+device iteration once and replay it, default true), ``autotune`` (pick the
+likelihood kernel's tile shape by timing, default false).
 """
 import configparser
 import os.path as op
@@ -73,6 +75,14 @@ class EMC():
         self.phaser_rot = torch.from_numpy(geometry.phaser_rotation_table(
             np.arange(self.num_rot) * np.pi / self.num_rot)).to(self.device)
         self.rmax = None
+        if self.autotune:
+            from rspi import autotune
+            autotune.tune(self.estep)
+        npix = self.size ** 2
+        self._dmodel = torch.empty(npix, dtype=torch.complex128, device=self.device)
+        self._host_model = torch.empty(npix, dtype=torch.complex128, pin_memory=True)
+        self._host_rmax = torch.empty(self.dset.num_data, dtype=torch.int32, pin_memory=True)
+        self._graph = None
 
     def _parse_params(self, config, start_dir):
         '''emc.py:57-65, plus the optional precision/tiling keys'''
@@ -91,6 +101,8 @@ class EMC():
         self.warps_per_cta = config.getint('emc', 'warps_per_cta', fallback=32)
         self.phaser_iter = config.getint('emc', 'phaser_iter', fallback=10)
         self.slice_budget_gb = config.getfloat('emc', 'slice_budget_gb', fallback=8.)
+        self.use_graph = config.getboolean('emc', 'cuda_graph', fallback=True)
+        self.autotune = config.getboolean('emc', 'autotune', fallback=False)
 
     def _generate_states(self, config):
         '''emc.py:67-87'''
@@ -127,15 +139,62 @@ class EMC():
 
     def run_iteration(self, iternum=None):
         '''Run one iteration of EMC: likelihoods of every state, most likely
-        state per frame, MaxLP M-step, output (emc.py:134-157)'''
-        dmodel = torch.from_numpy(np.ascontiguousarray(self.model.ravel(), dtype=np.complex128)).to(self.device)
-        self._calculate_prob(dmodel, None)
-        self._get_rmax()
-        self.phaser.run_from_rmax(dmodel, self.estep.rmax, self.num_rot, self.state_vals,
-                                  self.phaser_rot)
-        self.model = dmodel.cpu().numpy()
-        self.dset.photons.err.check('EMC iteration')
+        state per frame, MaxLP M-step, output (emc.py:134-157).  The model goes
+        to the device, the whole device iteration runs (replayed from a CUDA
+        graph after the first iteration) and model and rmax come back.'''
+        self._host_model.numpy()[:] = np.asarray(self.model, dtype=np.complex128).ravel()
+        self._dmodel.copy_(self._host_model, non_blocking=True)
+        self.device_step()
+        self._host_rmax.copy_(self.estep.rmax, non_blocking=True)
+        self._host_model.copy_(self._dmodel, non_blocking=True)
+        torch.cuda.current_stream(self.device).synchronize()
+        try:
+            self.dset.photons.err.check('EMC iteration')
+        except Exception:
+            if self._graph is None:
+                raise
+            # a capacity limit was hit inside the graph: redo the iteration eagerly
+            self._graph = None
+            self._dmodel.copy_(torch.from_numpy(np.asarray(self.model, dtype=np.complex128).ravel()))
+            self._device_step()
+            self._host_rmax.copy_(self.estep.rmax)
+            self._host_model.copy_(self._dmodel)
+            self.dset.photons.err.check('EMC iteration')
+        self.rmax = self._host_rmax.numpy().copy()
+        self.model = self._host_model.numpy().copy()
         self.save_output(self.model, iternum)
+
+    def _device_step(self):
+        '''One iteration on device buffers: E-step, reduction, M-step.'''
+        self.estep.run(self._dmodel)
+        self.estep.reduce()
+        self.phaser.run_from_rmax(self._dmodel, self.estep.rmax, self.num_rot, self.state_vals,
+                                  self.phaser_rot)
+
+    def device_step(self):
+        '''The iteration on the device model buffer ``_dmodel``: eager the
+        first time (which sizes every buffer and checks capacities), then
+        captured once into a CUDA graph and replayed.'''
+        if not self.use_graph:
+            self._device_step()
+            return
+        if self._graph is not None:
+            self._graph.replay()
+            return
+        self._device_step()
+        torch.cuda.current_stream(self.device).synchronize()
+        model_after = self._dmodel.clone()
+        self.estep.check_capacity = False
+        graph = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(side):
+            with torch.cuda.graph(graph, stream=side):
+                self._device_step()
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        self.estep.check_capacity = True
+        self._dmodel.copy_(model_after)   # capture does not execute: keep the eager result
+        self._graph = graph
 
     def _calculate_prob(self, dmodel, views=None, drange=None):
         '''Likelihood of every frame in every state into ``prob``

@@ -23,7 +23,8 @@ WARPS = (8, 16, 32)
 def _key(es):
     name = torch.cuda.get_device_name(es.device)
     ent = es.ll if es.form == 'fp64' else es.ll16
-    return '%s|%s|%d|%d|%d' % (name, es.form, es.p_row, es.ph.num_data, ent['total_rows'])
+    return '%s|%s|%s|%d|%d|%d' % (name, es.form, es.kernel, es.p_row, es.ph.num_data,
+                                  ent['total_rows'])
 
 
 def _load():
@@ -58,7 +59,10 @@ def tune(es, sample_tiles=2, repeats=2, use_cache=True, verbose=False):
         es.tile, es.warps = t, w
         return (t, w, table[key]['ms_per_row']), None
     tmax = es.lib.rspi_loglike_max_tile(es.p_row, es.slice_code)
-    cands = [(t, w) for t in TILES if t <= tmax for w in WARPS if not (t > 2 and w > 16)]
+    screen2 = es.form == 'screen' and es.kernel == 'stream'
+    tiles = (1, 2, 4) if screen2 else TILES
+    cands = [(t, w) for t in tiles if t <= tmax for w in WARPS
+             if screen2 or not (t > 2 and w > 16)]
     sms = torch.cuda.get_device_properties(es.device).multi_processor_count
     rows = min(es.n_rows, es.chunk_rows, sms * sample_tiles * max(t for t, _ in cands))
     es.rot_slices(0, rows)
@@ -68,9 +72,14 @@ def tune(es, sample_tiles=2, repeats=2, use_cache=True, verbose=False):
     results = []
     for t, w in cands:
         def run():
-            call('rspi_loglike_stream', es.slice_code, ptr(es.lsl), es.p_row, es.num_rot,
-                 ptr(es.init), ptr(es.ph.scales), ptr(ent['entries']), ptr(ent['row_off']), n,
-                 0, rows, ptr(es.prob[0]), n, t, w, 0, cur_stream())
+            if screen2:
+                call('rspi_screen_loglike2', ptr(es.lsl), es.p_row, es.num_rot, ptr(es.init),
+                     ptr(es.ph.scales), ptr(ent['entries']), ptr(ent['row_off']), n, 0, rows,
+                     ptr(es.prob[0]), n, t, w, 0, cur_stream())
+            else:
+                call('rspi_loglike_stream', es.slice_code, ptr(es.lsl), es.p_row, es.num_rot,
+                     ptr(es.init), ptr(es.ph.scales), ptr(ent['entries']), ptr(ent['row_off']),
+                     n, 0, rows, ptr(es.prob[0]), n, t, w, 0, cur_stream())
         run()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)

@@ -241,6 +241,7 @@ class EStep:
             per = int(cand_per_frame) if cand_per_frame else min(self.n_rows, 8192)
             self._alloc_candidates(max(1024, per * n))
         self.check_capacity = True
+        self.ll_events = None   # list -> (start, end, rows) CUDA events around each launch
 
     def _alloc_candidates(self, cap):
         dev = self.device
@@ -278,6 +279,15 @@ class EStep:
         its first row on (default: the chunk buffer)."""
         lsl = self.lsl if lsl is None else lsl
         n = self.ph.num_data
+        if self.ll_events is not None:
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True), r1 - r0)
+            ev[0].record(torch.cuda.current_stream())
+        self._loglike_launch(r0, r1, lsl, n)
+        if self.ll_events is not None:
+            ev[1].record(torch.cuda.current_stream())
+            self.ll_events.append(ev)
+
+    def _loglike_launch(self, r0, r1, lsl, n):
         if self.kernel == 'stream' and self.form == 'screen':
             l16 = self.ll16
             call('rspi_screen_loglike2', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),

@@ -111,3 +111,26 @@ def test_phaser_random_vs_oracle(size, tmp_path):
     with np.errstate(invalid='ignore', divide='ignore'):
         want = M.run_phaser(model, E.sparse_frames(ds), sx, sy, dia, ang, size)
     np.testing.assert_allclose(got, want, rtol=RTOL_MODEL, atol=1e-12)
+
+
+@pytest.mark.parametrize('form', ['fp64', 'screen'])
+def test_emc_graph_replay_matches_eager(form, tmp_path):
+    """Three iterations replayed from the captured CUDA graph give exactly the
+    eager iterations' rmax and model."""
+    from emc import EMC
+    g = load_golden('case_a')
+    out = {}
+    for graph in (False, True):
+        d = os.path.join(str(tmp_path), str(graph))
+        cfg = write_case(d, g, extra='form = %s\ncuda_graph = %s\n' % (form, graph))
+        rec = EMC(cfg)
+        rec.model = g['model_in_1'].copy()
+        hist = []
+        for it in range(3):
+            rec.run_iteration(None)
+            hist.append((rec.rmax.copy(), rec.model.copy()))
+        assert (rec._graph is not None) == graph
+        out[graph] = hist
+    for (ra, ma), (rb, mb) in zip(out[False], out[True]):
+        assert np.array_equal(ra, rb)
+        assert np.array_equal(ma, mb)

@@ -17,31 +17,78 @@ namespace {
 constexpr int SMEM_LIMIT = 227 * 1024;
 constexpr int PF = 8;
 
+// Accumulators: T floats kept as float2 pairs so Blackwell's packed FP32x2
+// add (FADD2) sums two rows per instruction.
 template <int T>
-struct Vec;
-template <>
-struct Vec<1> {
-    using type = float;
-    __device__ __forceinline__ static void add(float (&a)[1], type v0, type v1) { a[0] += v0 + v1; }
-};
-template <>
-struct Vec<2> {
-    using type = float2;
-    __device__ __forceinline__ static void add(float (&a)[2], type v0, type v1) {
-        a[0] += v0.x + v1.x;
-        a[1] += v0.y + v1.y;
+struct Acc {
+    static constexpr int NP = (T + 1) / 2;   // float2 pairs
+    float2 p[NP];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int i = 0; i < NP; ++i) p[i] = make_float2(0.f, 0.f);
     }
 };
+
+template <int T>
+__device__ __forceinline__ void add_word(Acc<T> &a, const unsigned char *sl, unsigned w);
+
 template <>
-struct Vec<4> {
-    using type = float4;
-    __device__ __forceinline__ static void add(float (&a)[4], type v0, type v1) {
-        a[0] += v0.x + v1.x;
-        a[1] += v0.y + v1.y;
-        a[2] += v0.z + v1.z;
-        a[3] += v0.w + v1.w;
-    }
-};
+__device__ __forceinline__ void add_word<1>(Acc<1> &a, const unsigned char *sl, unsigned w) {
+    const float v0 = *reinterpret_cast<const float *>(sl + (w & 0xffffu) * 4u);
+    const float v1 = *reinterpret_cast<const float *>(sl + (w >> 16) * 4u);
+    a.p[0].x += v0 + v1;
+}
+template <>
+__device__ __forceinline__ void add_word<2>(Acc<2> &a, const unsigned char *sl, unsigned w) {
+    const float2 v0 = *reinterpret_cast<const float2 *>(sl + (w & 0xffffu) * 8u);
+    const float2 v1 = *reinterpret_cast<const float2 *>(sl + (w >> 16) * 8u);
+    a.p[0] = __fadd2_rn(a.p[0], __fadd2_rn(v0, v1));
+}
+template <>
+__device__ __forceinline__ void add_word<4>(Acc<4> &a, const unsigned char *sl, unsigned w) {
+    const float4 v0 = *reinterpret_cast<const float4 *>(sl + (w & 0xffffu) * 16u);
+    const float4 v1 = *reinterpret_cast<const float4 *>(sl + (w >> 16) * 16u);
+    a.p[0] = __fadd2_rn(a.p[0], __fadd2_rn(make_float2(v0.x, v0.y), make_float2(v1.x, v1.y)));
+    a.p[1] = __fadd2_rn(a.p[1], __fadd2_rn(make_float2(v0.z, v0.w), make_float2(v1.z, v1.w)));
+}
+
+// Reduce-scatter over the warp: afterwards lane l holds the warp total of
+// row (l mod T).  log2(T) exchange steps halve the values a lane carries,
+// then 5 - log2(T) plain butterfly steps finish the sums.
+template <int T>
+__device__ __forceinline__ float reduce_scatter(Acc<T> &a, int lane);
+
+template <>
+__device__ __forceinline__ float reduce_scatter<1>(Acc<1> &a, int lane) {
+    return warp_sum(a.p[0].x);
+}
+template <>
+__device__ __forceinline__ float reduce_scatter<2>(Acc<2> &a, int lane) {
+    const bool hi = lane & 1;
+    float keep = hi ? a.p[0].y : a.p[0].x;
+    const float send = hi ? a.p[0].x : a.p[0].y;
+    keep += __shfl_xor_sync(RSPI_FULL_MASK, send, 1);
+#pragma unroll
+    for (int o = 2; o < 32; o <<= 1) keep += __shfl_xor_sync(RSPI_FULL_MASK, keep, o);
+    return keep;
+}
+template <>
+__device__ __forceinline__ float reduce_scatter<4>(Acc<4> &a, int lane) {
+    // step 1 (xor 2): keep the pair of rows (lane >> 1) & 1
+    const bool b1 = lane & 2;
+    float2 keep = b1 ? a.p[1] : a.p[0];
+    const float2 send = b1 ? a.p[0] : a.p[1];
+    keep.x += __shfl_xor_sync(RSPI_FULL_MASK, send.x, 2);
+    keep.y += __shfl_xor_sync(RSPI_FULL_MASK, send.y, 2);
+    // step 2 (xor 1): keep row (lane & 1) of the pair
+    const bool b0 = lane & 1;
+    float k = b0 ? keep.y : keep.x;
+    const float s = b0 ? keep.x : keep.y;
+    k += __shfl_xor_sync(RSPI_FULL_MASK, s, 1);
+#pragma unroll
+    for (int o = 4; o < 32; o <<= 1) k += __shfl_xor_sync(RSPI_FULL_MASK, k, o);
+    return k;   // row (lane & 3)
+}
 
 template <int T>
 __global__ void __launch_bounds__(1024)
@@ -49,9 +96,7 @@ k_screen_ll2(const float *__restrict__ lsl, int p_row, int num_rot,
              const double *__restrict__ init, const double *__restrict__ scales,
              const unsigned *__restrict__ words, const long long *__restrict__ row_off, int n_data,
              long long row_begin, long long row_end, float *__restrict__ ll, long long ll_stride) {
-    using V = typename Vec<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    V *sl = reinterpret_cast<V *>(smem_raw);
     float *slf = reinterpret_cast<float *>(smem_raw);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const long long n_tiles = (row_end - row_begin + T - 1) / T;
@@ -83,36 +128,33 @@ k_screen_ll2(const float *__restrict__ lsl, int p_row, int num_rot,
         __syncthreads();
         if (fb >= fe) continue;
 
-        double ini[T];
-#pragma unroll
-        for (int t = 0; t < T; ++t) ini[t] = t < nt ? init[(first + t) / num_rot] : 0.;
-        float acc[T];
-#pragma unroll
-        for (int t = 0; t < T; ++t) acc[t] = 0.f;
+        // this lane's row of the tile (stores go through lane < nt)
+        const int my_t = lane & (T - 1);
+        const double my_init = my_t < nt ? init[(first + my_t) / num_rot] : 0.;
+        float *my_ll = ll + (first + my_t - row_begin) * ll_stride;
+        Acc<T> acc;
+        acc.zero();
 
+        // frame offsets and scales of the next 32 frames, one per lane
+        int base = fb;
+        int my_end = fb + lane < n_data ? (int)(row_off[fb + lane + 1] >> 1) : 0x7fffffff;
+        double my_scale = fb + lane < n_data ? scales[fb + lane] : 0.;
         int f = fb;
         int q = (int)(row_off[fb] >> 1);
         const int qend = (int)(row_off[fe] >> 1);
-        int fend = (int)(row_off[f + 1] >> 1);
+        int fend = __shfl_sync(RSPI_FULL_MASK, my_end, 0);
         auto finish = [&]() {
-#pragma unroll
-            for (int t = 0; t < T; ++t) acc[t] = warp_sum(acc[t]);
-            if (lane < nt) {
-                float a = acc[0];
-#pragma unroll
-                for (int t = 1; t < T; ++t)
-                    if (t == lane) a = acc[t];
-                double s0 = ini[0];
-#pragma unroll
-                for (int t = 1; t < T; ++t)
-                    if (t == lane) s0 = ini[t];
-                ll[(first + lane - row_begin) * ll_stride + f] =
-                    (float)(s0 * scales[f] + (double)a);
-            }
-#pragma unroll
-            for (int t = 0; t < T; ++t) acc[t] = 0.f;
+            const float tot = reduce_scatter<T>(acc, lane);
+            const double sc = __shfl_sync(RSPI_FULL_MASK, my_scale, f - base);
+            if (lane < nt) my_ll[f] = (float)(my_init * sc + (double)tot);
+            acc.zero();
             ++f;
-            fend = f < fe ? (int)(row_off[f + 1] >> 1) : qend + 1;
+            if (f - base == 32) {
+                base = f;
+                my_end = f + lane < n_data ? (int)(row_off[f + lane + 1] >> 1) : 0x7fffffff;
+                my_scale = f + lane < n_data ? scales[f + lane] : 0.;
+            }
+            fend = f < fe ? __shfl_sync(RSPI_FULL_MASK, my_end, f - base) : qend + 1;
         };
         while (f < fe && fend == q) finish();   // frames without photons
 
@@ -127,8 +169,7 @@ k_screen_ll2(const float *__restrict__ lsl, int p_row, int num_rot,
 #pragma unroll
             for (int k = 0; k < PF; ++k) {
                 if (k < nb) {
-                    const unsigned w = cur[k];
-                    Vec<T>::add(acc, sl[w & 0xffffu], sl[w >> 16]);
+                    add_word<T>(acc, smem_raw, cur[k]);
                     if (q + k + 1 == fend) {
                         finish();
                         while (f < fe && fend == q + k + 1) finish();

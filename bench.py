@@ -319,23 +319,15 @@ def run_ours(args):
     model0 = synth.initial_model(w['size'], 20260100 + args.config)
     stream = torch.cuda.current_stream()
 
-    # CUDA events around every likelihood launch; the launches captured in the
-    # graph keep their events, so after the timed replays they hold the last
-    # replay's kernel times (recorded on the launching stream)
     es = rec.estep
     rec._dmodel.copy_(torch.from_numpy(model0).to(dev))
     l0 = rlib.launch_count
     rec._device_step()                      # one eager iteration: counts our launches
     torch.cuda.synchronize()
     kernels_per_step = rlib.launch_count - l0
-    n_chunks = (es.n_rows + es.chunk_rows - 1) // es.chunk_rows
-    es.ll_events = []
     rec.device_step()                       # eager once more, then capture the graph
-    graph_events = es.ll_events[-n_chunks:] if rec.use_graph else None
     for _ in range(max(0, args.warmup - 2)):
         rec.device_step()
-    if not rec.use_graph:
-        es.ll_events = []
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -353,12 +345,13 @@ def run_ours(args):
     launches = kernels_per_step * args.steps
     ms = e0.elapsed_time(e1) / args.steps
     clk = clocks.stop()
-    if rec.use_graph:
-        ll_ms = sum(a.elapsed_time(b) for a, b, _ in graph_events)
-        ll_launches = len(graph_events)
-    else:
-        ll_ms = sum(a.elapsed_time(b) for a, b, _ in es.ll_events) / args.steps
-        ll_launches = len(es.ll_events) // args.steps
+    # the likelihood kernel alone: CUDA events on the launching stream around
+    # each of its launches in one more E-step pass over the same buffers
+    es.ll_events = []
+    es.run(rec._dmodel)
+    torch.cuda.synchronize()
+    ll_ms = sum(a.elapsed_time(b) for a, b, _ in es.ll_events)
+    ll_launches = len(es.ll_events)
     es.ll_events = None
     rec.dset.photons.err.check('bench')
     if world > 1:

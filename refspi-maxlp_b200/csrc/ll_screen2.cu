@@ -29,6 +29,51 @@ struct Acc {
     }
 };
 
+// One word's contribution (two photons, every row of the tile) and its add.
+template <int T>
+struct Contrib {
+    float2 p[(T + 1) / 2];
+};
+
+template <int T>
+__device__ __forceinline__ Contrib<T> gather_word(const unsigned char *sl, unsigned w);
+
+template <>
+__device__ __forceinline__ Contrib<1> gather_word<1>(const unsigned char *sl, unsigned w) {
+    const float v0 = *reinterpret_cast<const float *>(sl + (w & 0xffffu) * 4u);
+    const float v1 = *reinterpret_cast<const float *>(sl + (w >> 16) * 4u);
+    Contrib<1> c;
+    c.p[0] = make_float2(v0 + v1, 0.f);
+    return c;
+}
+template <>
+__device__ __forceinline__ Contrib<2> gather_word<2>(const unsigned char *sl, unsigned w) {
+    const float2 v0 = *reinterpret_cast<const float2 *>(sl + (w & 0xffffu) * 8u);
+    const float2 v1 = *reinterpret_cast<const float2 *>(sl + (w >> 16) * 8u);
+    Contrib<2> c;
+    c.p[0] = __fadd2_rn(v0, v1);
+    return c;
+}
+template <>
+__device__ __forceinline__ Contrib<4> gather_word<4>(const unsigned char *sl, unsigned w) {
+    const float4 v0 = *reinterpret_cast<const float4 *>(sl + (w & 0xffffu) * 16u);
+    const float4 v1 = *reinterpret_cast<const float4 *>(sl + (w >> 16) * 16u);
+    Contrib<4> c;
+    c.p[0] = __fadd2_rn(make_float2(v0.x, v0.y), make_float2(v1.x, v1.y));
+    c.p[1] = __fadd2_rn(make_float2(v0.z, v0.w), make_float2(v1.z, v1.w));
+    return c;
+}
+
+template <int T>
+__device__ __forceinline__ void add_contrib(Acc<T> &a, const Contrib<T> &c) {
+    if (T == 1) {
+        a.p[0].x += c.p[0].x;
+    } else {
+#pragma unroll
+        for (int i = 0; i < (T + 1) / 2; ++i) a.p[i] = __fadd2_rn(a.p[i], c.p[i]);
+    }
+}
+
 template <int T>
 __device__ __forceinline__ void add_word(Acc<T> &a, const unsigned char *sl, unsigned w);
 
@@ -91,7 +136,7 @@ __device__ __forceinline__ float reduce_scatter<4>(Acc<4> &a, int lane) {
 }
 
 template <int T>
-__global__ void __launch_bounds__(1024)
+__global__ void __launch_bounds__(T == 4 ? 512 : 1024)
 k_screen_ll2(const float *__restrict__ lsl, int p_row, int num_rot,
              const double *__restrict__ init, const double *__restrict__ scales,
              const unsigned *__restrict__ words, const long long *__restrict__ row_off, int n_data,
@@ -166,10 +211,15 @@ k_screen_ll2(const float *__restrict__ lsl, int p_row, int num_rot,
             const int nb = min(PF, qend - q);
 #pragma unroll
             for (int k = 0; k < PF; ++k) nxt[k] = q + PF + k < qend ? __ldg(wp + 32 * (PF + k)) : 0u;
+            // gather phase without branches (slots past nb hold word 0: a
+            // valid address whose contribution is never added)
+            Contrib<T> cb[PF];
+#pragma unroll
+            for (int k = 0; k < PF; ++k) cb[k] = gather_word<T>(smem_raw, cur[k]);
 #pragma unroll
             for (int k = 0; k < PF; ++k) {
                 if (k < nb) {
-                    add_word<T>(acc, smem_raw, cur[k]);
+                    add_contrib<T>(acc, cb[k]);
                     if (q + k + 1 == fend) {
                         finish();
                         while (f < fe && fend == q + k + 1) finish();
@@ -199,6 +249,7 @@ int launch2(const float *lsl, long long p_row, long long num_rot, const double *
         smem_set = smem;
     }
     const long long n_tiles = (r1 - r0 + T - 1) / T;
+    if (T == 4) warps = min(warps, 16);   // register budget of the 4-row tile
     if (n_ctas <= 0) {
         const int per_sm = max(1, (int)(SMEM_LIMIT / (smem + 1024)));
         n_ctas = rspi_sm_count() * min(per_sm, max(1, 2048 / (warps * 32)));

@@ -315,6 +315,27 @@ int rspi_maxlp_pattern(double *fconv, const int *pixels, const int *hist_row,
 /* Mean of n values into *out (the global rescale, maxLP.py:329). */
 int rspi_mean(const double *vals, long long n, double *out, cudaStream_t stream);
 
+/* ----------------------------------------------------------------------- a16
+ * Negative log-likelihood of the MaxLP model and its adjoint (no reference
+ * counterpart works: get_grad_pixel, maxLP.py:199-214, uses an undefined
+ * name).  Over the phaser pixels t (mask_idx[t] = m >= 0, qx/qy/qrad[m],
+ * model fre/fim[m]) and frames d (rotation rot_cs[2d], rot_cs[2d+1] =
+ * cos(-ang), sin(-ang); dia, sx, sy, scale):
+ *   NLL = sum_d sum_t s_d |F_t + r_dt|^2 - k_dt log(s_d |F_t + r_dt|^2),
+ *   r_dt = ff(pi qrad_t dia_d) exp(2 pi i (qx_t sx_d + qy_t sy_d)),
+ * k_dt = photons of frame d at t's rotated pixel (maxLP.py:245-253).
+ * precision 0: FP32 terms, 1: FP64 terms (sums always FP64).  With
+ * want_grad the gradients d/dRe F, d/dIm F (n_pix) and d/d dia, sx, sy, scale
+ * (n_frames) are written (zeroed first).  *nll is zeroed first. */
+int rspi_nll(int precision, int want_grad, const int *ones, const int *multi,
+             const long long *ones_accum, const long long *multi_accum, const int *place_ones,
+             const int *place_multi, const int *count_multi, long long n_frames,
+             const double *rot_cs, long long size, const int *mask_idx, long long n_pix,
+             const double *fre, const double *fim, const double *qx, const double *qy,
+             const double *qrad, const double *dia, const double *sx, const double *sy,
+             const double *scale, double *nll, double *gfre, double *gfim, double *gdia,
+             double *gsx, double *gsy, double *gscale, int *err, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

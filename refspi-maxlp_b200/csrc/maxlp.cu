@@ -45,18 +45,6 @@ __global__ void k_frame_params(const int *__restrict__ rmax, long long n, long l
     }
 }
 
-// Detector pixel of model pixel (tx, ty) for a frame with rotation (c, s):
-// maxLP.py:250-252, x' = c qx + (-s) qy, y' = s qx + c qy, rint(x' size + size//2).
-__device__ __forceinline__ void forward_pixel(int tx, int ty, double c, double s, int size,
-                                              int &ox, int &oy) {
-    const double ds = (double)size, c0 = (double)(size / 2);
-    const double qx = ((double)tx - c0) / ds, qy = ((double)ty - c0) / ds;
-    const double xr = xadd(xmul(c, qx), xmul(-s, qy));
-    const double yr = xadd(xmul(s, qx), xmul(c, qy));
-    ox = (int)rint(xadd(xmul(xr, ds), c0));
-    oy = (int)rint(xadd(xmul(yr, ds), c0));
-}
-
 // Add `cnt` photons at detector (ux, uy) to every phaser pixel that maps
 // onto exactly (ux, uy).  Such pixels lie within 1/sqrt(2) px of the inverse
 // image, so the 3x3 neighbourhood of its rounding holds them all.

@@ -52,6 +52,18 @@ __device__ __forceinline__ double rot_log_value(const double *__restrict__ w, in
     return v < 1.e-20 ? -1000. : log(v);
 }
 
+// Detector pixel of model pixel (tx, ty) for a frame with rotation (c, s):
+// maxLP.py:250-252, x' = c qx + (-s) qy, y' = s qx + c qy, rint(x' size + size//2).
+__device__ __forceinline__ void forward_pixel(int tx, int ty, double c, double s, int size,
+                                              int &ox, int &oy) {
+    const double ds = (double)size, c0 = (double)(size / 2);
+    const double qx = ((double)tx - c0) / ds, qy = ((double)ty - c0) / ds;
+    const double xr = xadd(xmul(c, qx), xmul(-s, qy));
+    const double yr = xadd(xmul(s, qx), xmul(c, qy));
+    ox = (int)rint(xadd(xmul(xr, ds), c0));
+    oy = (int)rint(xadd(xmul(yr, ds), c0));
+}
+
 template <class T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

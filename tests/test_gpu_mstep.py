@@ -134,3 +134,18 @@ def test_emc_graph_replay_matches_eager(form, tmp_path):
     for (ra, ma), (rb, mb) in zip(out[False], out[True]):
         assert np.array_equal(ra, rb)
         assert np.array_equal(ma, mb)
+
+
+def test_recon_cli_writes_log_and_outputs(tmp_path):
+    """recon.py keeps the reference CLI and EMC.log format (recon.py:16-65)."""
+    import recon
+    g = load_golden('case_a')
+    cfg = write_case(str(tmp_path), g)
+    rec = recon.main(['2', '-c', cfg])
+    log = open(os.path.join(str(tmp_path), 'out', 'EMC.log')).read().splitlines()
+    assert log[0] == 'Iter  time(s)  change' and len(log) == 3
+    assert log[1].split()[0] == '1' and log[2].split()[0] == '2'
+    for it in (1, 2):
+        assert os.path.exists(os.path.join(str(tmp_path), 'out', 'output_%03d.npz' % it))
+    assert os.path.exists(os.path.join(str(tmp_path), 'out', 'model_000.npy'))
+    assert rec.rmax.shape == (len(g['ones']),)

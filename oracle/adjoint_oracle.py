@@ -59,4 +59,4 @@ def nll_and_grad(f, dia, sx, sy, scale, k, size, pixels):
                      torch.tensor(qx[pix]), torch.tensor(qy[pix]), torch.tensor(qrad[pix]))
     loss.backward()
     g = lambda v: v.grad.numpy().copy()  # noqa: E731
-    return float(loss), g(fr) + 1j * g(fi), g(dd), g(xx), g(yy), g(ss)
+    return float(loss.detach()), g(fr) + 1j * g(fi), g(dd), g(xx), g(yy), g(ss)

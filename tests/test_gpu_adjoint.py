@@ -88,8 +88,9 @@ def test_autograd_function_gradcheck():
     fre, fim = pr.model_pixels(model)
     inputs = [x.clone().requires_grad_(True) for x in
               (fre, fim, _t(par['dia']), _t(par['sx']), _t(par['sy']), _t(par['scale']))]
+    # FP64 atomics make repeated backward passes differ in the last bits
     assert torch.autograd.gradcheck(lambda *a: MaxLPNLL.apply(*a, pr), inputs, eps=1e-6,
-                                    atol=1e-4, rtol=1e-5)
+                                    atol=1e-4, rtol=1e-5, nondet_tol=1e-9)
 
 
 def test_fp32_terms_close_to_fp64():

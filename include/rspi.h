@@ -35,6 +35,7 @@ extern "C" {
 #define RSPI_ERR_CUDA (-3)     /* launch failed */
 #define RSPI_ERR_TIMEOUT (-4)  /* a bounded device-side wait ran out */
 #define RSPI_ERR_CAPACITY (-5) /* a value does not fit the packed layout */
+#define RSPI_ERR_TOO_LARGE (-6) /* larger than the fixed scratch of a no-allocation entry */
 
 /* Library version and build target, e.g. "rspi 0.1 sm_100a". */
 const char *rspi_version(void);
@@ -217,6 +218,22 @@ int rspi_screen_candidates(const float *ll, long long n_rows, long long n_data,
                            int *cnt_part, int *cand_n, double *noncand, double *thr,
                            long long *cand_off, long long capacity, int *cand_d, int *cand_r,
                            int *err, cudaStream_t stream);
+
+/* rspi_screen_candidates without the cnt_part scratch argument, for callers
+ * that cannot allocate device memory (no counterpart in the reference).  The
+ * scratch is a fixed device array inside the library, sized for at most
+ * 65536 frames (8 MiB per GPU, held until the process exits); more frames
+ * return RSPI_ERR_TOO_LARGE.  The first call on a device looks the array up
+ * (make it before any stream capture); calls that overlap on the GPU share
+ * the array and race, so the caller serialises them.  Outputs are those of
+ * rspi_screen_candidates. */
+int rspi_screen_candidates_noalloc(const float *ll, long long n_rows, long long n_data,
+                                   const double *max32, const int *rmax32,
+                                   const long long *frame_photons, const long long *row_off16,
+                                   const float *lmax, double delta, int *cand_n,
+                                   double *noncand, double *thr, long long *cand_off,
+                                   long long capacity, int *cand_d, int *cand_r, int *err,
+                                   cudaStream_t stream);
 
 /* FP64 rescoring of every candidate, in the summation order of rspi_loglike
  * (so the values equal the FP64 form's), written to cand_ll and into ll32;

@@ -17,6 +17,8 @@ extern "C" const char *rspi_status_string(int status) {
             return "device-side wait timed out";
         case RSPI_ERR_CAPACITY:
             return "value does not fit the packed layout";
+        case RSPI_ERR_TOO_LARGE:
+            return "size exceeds the fixed scratch of a no-allocation entry point";
         default:
             return "unknown status";
     }

@@ -592,3 +592,75 @@ extern "C" int rspi_rescore(const int *cand_d, const int *cand_r, const long lon
         cand_off, cand_r, cand_ll, max32, noncand, n_data, capacity, maxll, rmax, logz);
     RSPI_RETURN_LAUNCH();
 }
+
+// ---------------------------------------------------------------------------
+// Candidate selection that allocates nothing
+// ---------------------------------------------------------------------------
+// rspi_screen_candidates needs n_data * 32 ints of scratch from its caller.
+// Some callers cannot provide it: code that runs where it may not call
+// cudaMalloc (for example a host thread inside a real-time loop that must
+// never block on the driver's allocator, or an application whose device
+// memory is all owned by another framework's pool that this library cannot
+// draw from).  For them the scratch lives in a fixed file-scope device array
+// of NOALLOC_MAX_FRAMES * 32 ints (8 MiB), which every GPU that loads this
+// library keeps until the process exits.  The first call on each device
+// looks up the array's device address with cudaGetSymbolAddress, with that
+// device current; make that first call before any stream capture.  Every
+// call on a device shares the one array and it keeps the last call's
+// contents: calls whose work overlaps on the GPU (different streams, or two
+// host threads) race on it and must be serialised by the caller.  The
+// kernels overwrite every scratch entry they later read, so nothing has to
+// start at zero.
+namespace {
+
+constexpr long long NOALLOC_MAX_FRAMES = 65536;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+static __device__ __align__(256) int g_cand_scratch[NOALLOC_MAX_FRAMES * RY];
+
+int *cand_scratch_address(int *status) {
+    static int *addr[NOALLOC_MAX_DEVICES] = {};
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+        *status = RSPI_ERR_CUDA;
+        return nullptr;
+    }
+    if (addr[dev] == nullptr) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_cand_scratch) != cudaSuccess || p == nullptr) {
+            *status = RSPI_ERR_CUDA;
+            return nullptr;
+        }
+        addr[dev] = static_cast<int *>(p);
+    }
+    return addr[dev];
+}
+
+}  // namespace
+
+extern "C" int rspi_screen_candidates_noalloc(const float *ll, long long n_rows, long long n_data,
+                                              const double *max32, const int *rmax32,
+                                              const long long *frame_photons,
+                                              const long long *row_off16, const float *lmax,
+                                              double delta, int *cand_n, double *noncand,
+                                              double *thr, long long *cand_off, long long capacity,
+                                              int *cand_d, int *cand_r, int *err,
+                                              cudaStream_t stream) {
+    if (n_data > NOALLOC_MAX_FRAMES) return RSPI_ERR_TOO_LARGE;
+    if (!ll || !max32 || !rmax32 || !frame_photons || !row_off16 || !lmax || !cand_n ||
+        !noncand || !thr || !cand_off || !cand_d || !cand_r || n_rows <= 0 || n_data <= 0 ||
+        n_rows > 0x7fffffffLL || capacity < 0 || !(delta >= 0.))
+        return RSPI_ERR_ARG;
+    int status = RSPI_OK;
+    int *scratch = cand_scratch_address(&status);
+    if (scratch == nullptr) return status;
+    const dim3 block(32, RY);
+    const unsigned grid = (unsigned)((n_data + 31) / 32);
+    k_cand_count<<<grid, block, 0, stream>>>(ll, n_rows, n_data, max32, rmax32, frame_photons,
+                                             row_off16, lmax, delta, scratch, cand_n, noncand,
+                                             thr);
+    k_scan_counts<<<1, 1024, 0, stream>>>(cand_n, n_data, cand_off);
+    k_cand_fill<<<grid, block, 0, stream>>>(ll, n_rows, n_data, thr, rmax32, scratch, cand_off,
+                                            capacity, cand_d, cand_r, err);
+    RSPI_RETURN_LAUNCH();
+}

@@ -38,6 +38,8 @@ SIGNATURES = {
     'rspi_screen_candidates': (I, [P, L, L, P, P, P, P, P, D, P, P, P, P, P, L, P, P, P, P]),
     'rspi_rescore': (I, [P, P, P, L, L, L, P, L, P, L, P, P, L, L, P, P, P, P, P, P, P, P, P,
                          P, P, P, P, P, P]),
+    'rspi_screen_candidates_noalloc': (I, [P, L, L, P, P, P, P, P, D, P, P, P, P, L, P, P, P,
+                                           P]),
     'rspi_nll': (I, [I, I] + [P] * 7 + [L, P, L, P, L] + [P] * 16),
     'rspi_screen_loglike2': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
     'rspi_entries16_check': (I, [P, L, P, P]),
@@ -89,7 +91,7 @@ KERNELS_PER_CALL = {
     'rspi_mean': 1, 'rspi_ll16_entry_rows': 1, 'rspi_ll16_entry_fill': 1,
     'rspi_screen_loglike': 1, 'rspi_screen_candidates': 3, 'rspi_rescore': 5,
     'rspi_loglike_stream': 1, 'rspi_posterior_pairs': 3, 'rspi_screen_loglike2': 1,
-    'rspi_entries16_check': 1, 'rspi_nll': 2, 'rspi_merge_coverage': 1, 'rspi_merge': 2,
+    'rspi_entries16_check': 1, 'rspi_nll': 2, 'rspi_screen_candidates_noalloc': 3, 'rspi_merge_coverage': 1, 'rspi_merge': 2,
 }
 launch_count = 0
 

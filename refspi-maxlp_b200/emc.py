@@ -32,6 +32,7 @@ sys.path.insert(0, op.dirname(op.abspath(__file__)))
 from dset import Dataset  # noqa: E402
 from maxLP import MaxLPhaser  # noqa: E402
 from rspi import geometry  # noqa: E402
+from rspi import h5lite  # noqa: E402
 from rspi.device import EStep  # noqa: E402
 
 P_MIN = 1.e-6   # emc.py:20
@@ -220,8 +221,9 @@ class EMC():
         return vals[:, 0], vals[:, 1], vals[:, 2], ang * np.pi / self.num_rot
 
     def save_output(self, model, iternum, intens=None):
-        '''``model.npy``, or ``output_%03d`` with the datasets model, angles,
-        diameters, shifts and optional intens (emc.py:226-239)'''
+        '''``model.npy``, or ``output_%03d.h5`` (HDF5, written by rspi.h5lite)
+        with the datasets model, angles, diameters, shifts and optional
+        intens (emc.py:226-239)'''
         if iternum is None:
             np.save(op.join(self.output_folder, 'model.npy'), self.model)
             return
@@ -231,9 +233,7 @@ class EMC():
                'shifts': np.array([sx_vals, sy_vals]).T}
         if intens is not None:
             out['intens'] = intens.cpu().numpy() if torch.is_tensor(intens) else np.asarray(intens)
-        path = op.join(self.output_folder, 'output_%.3d.npz' % iternum)
-        with open(path, 'wb') as fh:
-            np.savez(fh, **out)
+        h5lite.write_datasets(op.join(self.output_folder, 'output_%.3d.h5' % iternum), out)
 
     def _random_model(self):
         '''emc.py:241-242'''

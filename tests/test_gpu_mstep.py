@@ -86,7 +86,11 @@ def test_emc_two_iterations_match_reference(name, form, tmp_path):
         np.testing.assert_allclose(np.stack(rec._unravel_rmax(rec.rmax)), g['unravel_%d' % it],
                                    rtol=0, atol=0)
         np.testing.assert_allclose(rec.model, g['model_out_%d' % it], rtol=RTOL_MODEL, atol=1e-12)
-        assert os.path.exists(os.path.join(str(tmp_path), 'out', 'output_%03d.npz' % it))
+        from rspi import h5lite
+        out = h5lite.read_datasets(os.path.join(str(tmp_path), 'out', 'output_%03d.h5' % it))
+        np.testing.assert_array_equal(out['model'], rec.model.reshape(out['model'].shape))
+        np.testing.assert_array_equal(out['angles'], g['unravel_%d' % it][3])
+        np.testing.assert_array_equal(out['shifts'], g['unravel_%d' % it][:2].T)
 
 
 @pytest.mark.parametrize('size', [5, 17, 23])
@@ -146,6 +150,10 @@ def test_recon_cli_writes_log_and_outputs(tmp_path):
     assert log[0] == 'Iter  time(s)  change' and len(log) == 3
     assert log[1].split()[0] == '1' and log[2].split()[0] == '2'
     for it in (1, 2):
-        assert os.path.exists(os.path.join(str(tmp_path), 'out', 'output_%03d.npz' % it))
+        from rspi import h5lite
+        out = h5lite.read_datasets(os.path.join(str(tmp_path), 'out', 'output_%03d.h5' % it))
+        np.testing.assert_array_equal(out['model'], rec.model.reshape(out['model'].shape))
+        np.testing.assert_array_equal(out['angles'], g['unravel_%d' % it][3])
+        np.testing.assert_array_equal(out['shifts'], g['unravel_%d' % it][:2].T)
     assert os.path.exists(os.path.join(str(tmp_path), 'out', 'model_000.npy'))
     assert rec.rmax.shape == (len(g['ones']),)

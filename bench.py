@@ -50,7 +50,7 @@ def parse_args():
     ap.add_argument('--steps', type=int, default=3)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--config', type=int, default=2, choices=[1, 2])
+    ap.add_argument('--config', type=int, default=2, choices=[1, 2, 4])
     ap.add_argument('--frames', type=int, default=None, help='override frame count (testing)')
     ap.add_argument('--form', default='screen', choices=['fp64', 'screen'])
     ap.add_argument('--kernel', default='stream', choices=['stream', 'dynamic'])
@@ -84,8 +84,25 @@ def workload(cfg_id, frames):
     nsx = int(r['shiftx'].split()[2])
     nsy = int(r['shifty'].split()[2])
     nd = int(r['sphere_dia'].split()[2])
+    nm = int(r.get('num_modes', 1))
     return dict(cfg=c, n=n, size=c['size'], num_rot=r['num_rot'], n_states0=nsx * nsy * nd,
-                n_states=nsx * nsy * nd * r['num_rot'], recon=r)
+                n_modes=nm, n_states=nsx * nsy * nd * r['num_rot'] * nm, recon=r)
+
+
+def generate_data(cfg_id, w, device='cpu'):
+    """The configuration's seeded synthetic photons (``w['n']`` frames)."""
+    from rspi import synth
+    c = w['cfg']
+    return synth.generate(c['size'], w['n'], c['mean_count'], c['n_blobs'], c['obj_radius'],
+                          c['fluence_sigma'], c['dia'], c['shift_max'], seed=20260000 + cfg_id,
+                          device=device, **synth.config_extras(cfg_id))
+
+
+def start_model(cfg_id, w):
+    """Seeded start model, one random image per mode (flattened)."""
+    from rspi import synth
+    return np.concatenate([synth.initial_model(w['size'], 20260100 + cfg_id + 1000 * m)
+                           for m in range(w['n_modes'])])
 
 
 def write_inputs(tmp, w, data, form, slice_gb=8.):
@@ -96,9 +113,10 @@ def write_inputs(tmp, w, data, form, slice_gb=8.):
     r = w['recon']
     with open(cfg, 'w') as f:
         f.write('[emc]\nsize = %d\nin_photons_file = photons.npz\noutput_folder = out/\n'
-                'log_file = out/EMC.log\nneed_scaling = True\nnum_rot = %d\nnum_modes = 1\n'
+                'log_file = out/EMC.log\nneed_scaling = True\nnum_rot = %d\nnum_modes = %d\n'
                 'sphere_dia = %s\nshiftx = %s\nshifty = %s\nform = %s\nslice_budget_gb = %g\n' %
-                (w['size'], r['num_rot'], r['sphere_dia'], r['shiftx'], r['shifty'], form, slice_gb))
+                (w['size'], r['num_rot'], w['n_modes'], r['sphere_dia'], r['shiftx'], r['shifty'],
+                 form, slice_gb))
     return cfg
 
 
@@ -189,67 +207,85 @@ def _cpu_maxlp_task(args):
     return time.perf_counter() - t0
 
 
-def cpu_baseline(w, data, model, target_s):
-    """Extrapolated seconds per iteration of the FP64 oracle on all host cores.
-
-    E-step: a few states x all rotations, likelihood against the first
-    ``nf`` frames -> per-slice-row and per-(row, frame) costs, scaled to all
-    rows and frames.  M-step: ``npx`` pixels over ``nf2`` frames -> per
-    (pixel, frame) cost, scaled to every phaser pixel (ring + main pass) and
-    all frames.  Linear extrapolation, stated in ``sample``.
-    """
-    import multiprocessing as mp
+def _baseline_inputs(w, data):
+    """Photon lists and per-frame values the CPU sample works on."""
     from oracle import emc_oracle as E
     from oracle import maxlp_oracle as M
     from rspi import geometry
-    cores = os.cpu_count() or 1
-    size, num_rot, n = w['size'], w['num_rot'], w['n']
+    size, n = w['size'], w['n']
     ds = E.parse_photons(data['ones'], data['multi'], data['place_ones'], data['place_multi'],
                          data['count_multi'], size * size, True)
     _, pm = E.generate_masks(size)
     nf = min(n, 500)
-    kmat_sel = E.sparse_frames(ds, pm < 1)[:nf]
     r = w['recon']
     sx, sy, dia, _ = geometry.state_grid(geometry.parse_triple(r['shiftx']),
                                          geometry.parse_triple(r['shifty']),
                                          geometry.parse_triple(r['sphere_dia']))
-    n_est = max(1, min(cores, 8))
+    kmat = E.sparse_frames(ds)
+    qx, qy, qrad, mask, rmask = M.get_qvals(size)
+    rng = np.random.default_rng(0)
+    ang = rng.integers(0, w['num_rot'], n) * np.pi / w['num_rot']
+    shifts = np.stack([rng.choice(np.unique(sx), n), rng.choice(np.unique(sy), n)], 1)
+    diams = rng.choice(np.unique(dia), n)
+    return dict(ds=ds, nf=nf, kmat_sel=E.sparse_frames(ds, pm < 1)[:nf], sx=sx, sy=sy, dia=dia,
+                kmat=kmat, q=(qx, qy, qrad), main=np.flatnonzero(mask),
+                n_phaser=int(rmask.sum() + mask.sum()), ang=ang, shifts=shifts, diams=diams)
+
+
+def _baseline_sample(w, inp, model, pool, cores, n_est, npx):
+    """Seconds per iteration of the FP64 oracle on ``cores`` workers,
+    extrapolated from a bounded sample.
+
+    E-step: ``n_est`` (shift, diameter) states x all rotations, likelihood
+    against the first ``nf`` frames -> per-slice-row and per-(row, frame)
+    costs, scaled to all rows and frames.  M-step: ``npx`` pixels over
+    ``nf2`` frames -> per (pixel, frame) cost, scaled to every phaser pixel
+    (ring + main pass) and all frames.  Linear extrapolation, stated in
+    ``sample``.
+    """
+    from oracle import maxlp_oracle as M
+    size, num_rot, n = w['size'], w['num_rot'], w['n']
+    nf, sx, sy, dia = inp['nf'], inp['sx'], inp['sy'], inp['dia']
     picks = np.linspace(0, sx.size - 1, n_est).astype(int)
-    ctx = mp.get_context('spawn')
     t_wall0 = time.perf_counter()
-    with ctx.Pool(cores, initializer=_cpu_worker_init) as pool:
-        est = pool.map(_cpu_estep_task, [(model, sx[i], sy[i], dia[i], size, num_rot,
-                                          ds['bg'], kmat_sel) for i in picks])
-        t_slice_row = np.mean([a for a, _ in est]) / num_rot
-        t_ll_cell = np.mean([b for _, b in est]) / (num_rot * nf)
-        # M-step sample
-        kmat = E.sparse_frames(ds)
-        qx, qy, qrad, mask, rmask = M.get_qvals(size)
-        main = np.flatnonzero(mask)
-        npx = max(cores, 8)
-        nf2 = min(n, 2000)
-        rng = np.random.default_rng(0)
-        ang = rng.integers(0, num_rot, n) * np.pi / num_rot
-        shifts = np.stack([rng.choice(np.unique(sx), n), rng.choice(np.unique(sy), n)], 1)
-        diams = rng.choice(np.unique(dia), n)
-        tasks = []
-        for t in main[np.linspace(0, main.size - 1, npx).astype(int)]:
-            k = M.photons_pixel(kmat, ang, int(t), size, qx, qy)[:nf2]
-            fr = M.fref_pixel(int(t), qx, qy, qrad, diams, shifts)[:nf2]
-            tasks.append((complex(model[t]), k, fr, 1.0))
-        mt = pool.map(_cpu_maxlp_task, tasks)
+    est = pool.map(_cpu_estep_task, [(model, sx[i], sy[i], dia[i], size, num_rot,
+                                      inp['ds']['bg'], inp['kmat_sel']) for i in picks])
+    t_slice_row = np.mean([a for a, _ in est]) / num_rot
+    t_ll_cell = np.mean([b for _, b in est]) / (num_rot * nf)
+    qx, qy, qrad = inp['q']
+    main = inp['main']
+    nf2 = min(n, 2000)
+    tasks = []
+    for t in main[np.linspace(0, main.size - 1, npx).astype(int)]:
+        k = M.photons_pixel(inp['kmat'], inp['ang'], int(t), size, qx, qy)[:nf2]
+        fr = M.fref_pixel(int(t), qx, qy, qrad, inp['diams'], inp['shifts'])[:nf2]
+        tasks.append((complex(model[t]), k, fr, 1.0))
+    mt = pool.map(_cpu_maxlp_task, tasks)
     wall = time.perf_counter() - t_wall0
     t_px_frame = np.mean(mt) / nf2
     rows = w['n_states']
-    n_phaser = int(rmask.sum() + mask.sum())
-    serial = rows * t_slice_row + rows * n * t_ll_cell + n_phaser * n * t_px_frame
+    serial = rows * t_slice_row + rows * n * t_ll_cell + inp['n_phaser'] * n * t_px_frame
     per_iter = serial / cores
     return dict(s_per_iteration=per_iter, cores=cores, wall_s=wall,
                 sample=('FP64 NumPy oracle, %d workers: E-step %d of %d (shift,dia) states x %d '
                         'rotations vs %d of %d frames, M-step %d pixels x %d frames; linear '
                         'extrapolation to %d rows x %d frames and %d phaser pixels, divided by '
                         'the worker count' % (cores, n_est, w['n_states0'], num_rot, nf, n, npx,
-                                              nf2, rows, n, n_phaser)))
+                                              nf2, rows, n, inp['n_phaser'])))
+
+
+def _baseline_pool(cores):
+    import multiprocessing as mp
+    return mp.get_context('spawn').Pool(cores, initializer=_cpu_worker_init)
+
+
+def cpu_baseline(w, data, model, target_s):
+    """Extrapolated seconds per iteration of the FP64 oracle on all host
+    cores (one bounded sample; see ``_baseline_sample``)."""
+    cores = os.cpu_count() or 1
+    inp = _baseline_inputs(w, data)
+    with _baseline_pool(cores) as pool:
+        return _baseline_sample(w, inp, model, pool, cores, max(1, min(cores, 8)), max(cores, 8))
 
 
 # ---------------------------------------------------------------------------
@@ -257,19 +293,22 @@ def run_reference(args):
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return 0
-    from rspi import synth
     w = workload(args.config, args.frames)
-    c = w['cfg']
-    data = synth.generate(c['size'], w['n'], c['mean_count'], c['n_blobs'], c['obj_radius'],
-                          c['fluence_sigma'], c['dia'], c['shift_max'], seed=20260000 + args.config)
-    model = synth.initial_model(w['size'], 20260100 + args.config)
+    data = generate_data(args.config, w)
+    model = start_model(args.config, w)[:w['size'] ** 2]
+    cores = os.cpu_count() or 1
+    inp = _baseline_inputs(w, data)
     times = []
     base = None
-    for i in range(args.warmup + args.steps):
-        base = cpu_baseline(w, data, model, args.cpu_seconds)
-        if i >= args.warmup:
+    with _baseline_pool(cores) as pool:
+        for _ in range(args.warmup):
+            # untimed: one state and one pixel load the oracle in every worker
+            _baseline_sample(w, inp, model, pool, cores, 1, 1)
+        for _ in range(args.steps):
+            base = _baseline_sample(w, inp, model, pool, cores, max(1, min(cores, 8)),
+                                    max(cores, 8))
             times.append(base['s_per_iteration'])
-    t = max(times)
+    t = float(np.mean(times))
     v = w['n'] * w['n_states'] / t
     out = {'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': UNIT,
            'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
@@ -290,7 +329,6 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
     from rspi import lib as rlib
-    from rspi import synth
 
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
@@ -301,11 +339,8 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dev = torch.device('cuda', local)
     w = workload(args.config, args.frames)
-    c = w['cfg']
     t0 = time.time()
-    data = synth.generate(c['size'], w['n'], c['mean_count'], c['n_blobs'], c['obj_radius'],
-                          c['fluence_sigma'], c['dia'], c['shift_max'],
-                          seed=20260000 + args.config, device=dev)
+    data = generate_data(args.config, w, device=dev)
     t_gen = time.time() - t0
     tmp = tempfile.mkdtemp(prefix='rspi_bench_')
     cfgfile = write_inputs(tmp, w, data, args.form, args.slice_gb)
@@ -316,7 +351,7 @@ def run_ours(args):
         rec = EMC(cfgfile, device=dev)
     if args.kernel != rec.estep.kernel:
         rec.estep.kernel = args.kernel
-    model0 = synth.initial_model(w['size'], 20260100 + args.config)
+    model0 = start_model(args.config, w)
     stream = torch.cuda.current_stream()
 
     es = rec.estep
@@ -368,7 +403,7 @@ def run_ours(args):
         from rspi.device import EStep
         pe = EStep(rec.dset.photons, w['size'], w['num_rot'], rec.shiftx, rec.shifty,
                    rec.sphere_dia, rec.probmask, rec.dset.bg.cpu().numpy(), form='fp64',
-                   kernel='dynamic')
+                   kernel='dynamic', n_modes=w['n_modes'])
         pmodel = torch.from_numpy(model0).to(dev)
 
         def pstep():
@@ -396,7 +431,7 @@ def run_ours(args):
     # e2e through the public API: host model in, host model + argmax out
     e2e = None
     if not args.no_e2e:
-        rec.model = model0.copy()
+        rec.model = model0.copy().reshape(rec._model_shape())
         for _ in range(min(args.warmup, 1)):
             rec.run_iteration(None)
         torch.cuda.synchronize()
@@ -411,7 +446,7 @@ def run_ours(args):
             t = torch.tensor([e2e_s], device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             e2e_s = float(t.item())
-        p = w['size'] ** 2
+        p = w['size'] ** 2 * w['n_modes']
         e2e = {'value': world * w['n'] * w['n_states'] / e2e_s, 'unit': UNIT,
                's_per_iteration': e2e_s, 'h2d_bytes_per_step': 16 * p,
                'd2h_bytes_per_step': 16 * p + 4 * w['n'],
@@ -458,7 +493,7 @@ def run_ours(args):
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         cb = cpu_baseline(w, {k: (v.cpu().numpy() if hasattr(v, 'cpu') else v) for k, v in data.items()},
-                          model0, args.cpu_seconds)
+                          model0[:w['size'] ** 2], args.cpu_seconds)
         cpu = {'value': w['n'] * w['n_states'] / cb['s_per_iteration'], 'unit': UNIT,
                'cores': cb['cores'], 'kind': 'port', 'sample': cb['sample'],
                's_per_iteration': cb['s_per_iteration']}
@@ -469,9 +504,9 @@ def run_ours(args):
         'dtype': 'f64' if args.form == 'fp64' else 'f32 screen + f64 rescore',
         'data': 'synthetic (seeded generator with the configuration\'s shapes)',
         'config': {'workload': 'config%d: %dx%d detector, %d frames, %d rotations x %d (shift,dia) '
-                   'states = %d states/frame, 1 EMC iteration per step' %
+                   'states x %d mode(s) = %d states/frame, 1 EMC iteration per step' %
                    (args.config, w['size'], w['size'], w['n'], w['num_rot'], w['n_states0'],
-                    w['n_states']),
+                    w['n_modes'], w['n_states']),
                    'frames': w['n'], 'states_per_frame': w['n_states'],
                    'form': args.form, 'parallelism': 'replicas' if world > 1 else 'single',
                    'l2': 'inputs larger than L2 (slices %.1f GB, likelihoods %.1f GB per step)' %

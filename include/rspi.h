@@ -319,13 +319,21 @@ int rspi_maxlp_histogram(const int *ones, const int *multi, const long long *one
 /* Pattern search of a set of model pixels (maxLP.py:154-197): for each pixel
  * t = pixels[i] (its histogram row hist_row[i]) run <= num_iter iterations over
  * the 33x33 candidate grid.  rescale_mode 0: per-candidate rescale
- * (ring pass, maxLP.py:186-187); 1: the scalar *rescale (main pass).
- * fconv (complex128, P) is updated in place.  With rescale_out != NULL the
- * per-pixel rescale of the final value (maxLP.py:328) is written to
- * rescale_out[i]. */
+ * (ring pass, maxLP.py:186-187); 1: the scalar rescale of the mode (main pass).
+ *
+ * n_modes independent models are searched in one launch (n_modes = 1 is the
+ * reference's single model; num_modes, parsed at emc.py:59, is otherwise
+ * unused there).  Mode m owns model fconv[m*P .. (m+1)*P) (complex128,
+ * updated in place), histogram columns m*n_ref .. (m+1)*n_ref of each
+ * n_modes*n_ref-wide hist row, frame counts nstate[m*n_ref ..] and, in the
+ * main pass, rescale[m].  The means over frames divide by the mode's frame
+ * count sum_s nstate[m*n_ref + s] (N for one mode); a mode without frames
+ * keeps its model.  With rescale_out != NULL the per-pixel rescale of the
+ * final value (maxLP.py:328) goes to rescale_out[m*n_pix + i] (NaN for a
+ * mode without frames). */
 int rspi_maxlp_pattern(double *fconv, const int *pixels, const int *hist_row,
                        long long n_pix, const int *hist, long long n_ref,
-                       const int *nstate, long long n_data, const double *ref_params,
+                       const int *nstate, long long n_modes, const double *ref_params,
                        long long size, int rescale_mode, const double *rescale,
                        int num_iter, double *rescale_out, cudaStream_t stream);
 

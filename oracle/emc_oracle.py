@@ -292,6 +292,40 @@ def calc_prob(model, ds, shiftx, shifty, sphere_dia, size, num_rot, probmask,
     return prob, msums, vscale
 
 
+def calc_prob_modes(models, ds, shiftx, shifty, sphere_dia, size, num_rot, probmask,
+                    scales, frames=None):
+    """Likelihood matrix for several models (``num_modes``, parsed at
+    emc.py:59 and unused there; build-defined).  The (mode, state) pairs form
+    the state list of emc.py:166-199: row ``(m*S0 + s)*num_rot + j`` holds
+    model m in state s, and ``vscale`` is the one of emc.py:181 over all
+    ``M*S0`` pairs, ``powder[sel].sum() / sum_pairs W[sel].sum() * M*S0``.
+    With one model this is ``calc_prob``."""
+    bg = ds['bg']
+    powder = get_powder(ds)
+    sel = probmask < 1
+    n0 = shiftx.shape[0]
+    msums, sums = [], []
+    for model in models:
+        ms, _ = msum_vscale(model, shiftx, shifty, sphere_dia, size, bg, probmask, powder)
+        msums.append(ms)
+        sums.append(ms.sum())
+    msums = np.concatenate(msums)
+    vscale = powder[sel].sum() / np.sum(sums) * (len(models) * n0)
+    kmat = sparse_frames(ds, sel)
+    if frames is not None:
+        kmat = kmat[frames]
+        scales = scales[frames]
+    prob = np.empty((len(models) * n0 * num_rot, kmat.shape[0]))
+    for m, model in enumerate(models):
+        for s in range(n0):
+            lsl = log_slices_for_state(model, shiftx[s], shifty[s], sphere_dia[s],
+                                       size, bg, num_rot, sel)
+            init = -float(msums[m * n0 + s] * vscale)
+            r0 = (m * n0 + s) * num_rot
+            prob[r0:r0 + num_rot] = init * scales[None, :] + np.asarray(kmat @ lsl.T).T
+    return prob, msums, vscale
+
+
 # --------------------------------------------------------------------------
 # a8: most likely state per frame (emc.py:207-224)
 # --------------------------------------------------------------------------

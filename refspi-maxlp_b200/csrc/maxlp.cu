@@ -207,19 +207,30 @@ __device__ int load_populated(int s_begin, const int *__restrict__ hrow, long lo
 
 __global__ void __launch_bounds__(PT_THREADS)
 k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
-          const int *__restrict__ hist_row, const int *__restrict__ hist, long long n_ref,
-          const int *__restrict__ nstate, long long n_data, const double *__restrict__ ref_params,
-          int size, int ring, const double *__restrict__ rescale_ptr, int num_iter,
-          double *__restrict__ rescale_out) {
+          const int *__restrict__ hist_row, long long n_pix, const int *__restrict__ hist,
+          long long n_ref, const int *__restrict__ nstate, long long n_modes,
+          const double *__restrict__ ref_params, int size, int ring,
+          const double *__restrict__ rescale_ptr, int num_iter, double *__restrict__ rescale_out) {
     __shared__ double fr_re[POP_CAP], fr_im[POP_CAP], fk[POP_CAP];
     __shared__ double scratch[32];
     __shared__ int iscratch[32];
     __shared__ int wsum[32];
 
+    // blockIdx.y = mode: its model, its histogram columns, its frames
+    const long long mode = blockIdx.y;
     const long long ip = blockIdx.x;
     const int t = pixels[ip];
-    const int *hrow = hist + (long long)hist_row[ip] * n_ref;
-    const double dn = (double)n_data;
+    const int *hrow = hist + (long long)hist_row[ip] * n_ref * n_modes + mode * n_ref;
+    nstate += mode * n_ref;
+    fconv += mode * (long long)size * size;
+    // frames of this mode (all frames for one mode): an exact integer sum
+    double cnt = 0.;
+    for (long long s = threadIdx.x; s < n_ref; s += blockDim.x) cnt += (double)nstate[s];
+    const double dn = block_sum(cnt, scratch);
+    if (dn == 0.) {  // no frame chose this mode: its model stays as it is
+        if (threadIdx.x == 0 && rescale_out) rescale_out[mode * n_pix + ip] = NAN;
+        return;
+    }
 
     PixelConsts pc;
     {
@@ -262,7 +273,7 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
     if (one_chunk) load_populated(0, hrow, n_ref, ref_params, pc, fr_re, fr_im, fk, &npop, wsum);
 
     const double kmean = pc.ksum / dn;
-    const double rescale = ring ? 0. : *rescale_ptr;
+    const double rescale = ring ? 0. : rescale_ptr[mode];
     double2 f = fconv[t];
     double step = hypot(f.x, f.y) / 4.;
     const double shrink = 33. / 5.;  // sqrt(1089) / 5, maxLP.py:177
@@ -326,7 +337,7 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
         fconv[t] = f;
         if (rescale_out) {
             const double er = f.x + pc.ar, ei = f.y + pc.ai;
-            rescale_out[ip] = kmean / (er * er + ei * ei + pc.var);
+            rescale_out[mode * n_pix + ip] = kmean / (er * er + ei * ei + pc.var);
         }
     }
 }
@@ -371,18 +382,20 @@ extern "C" int rspi_maxlp_histogram(const int *ones, const int *multi,
 
 extern "C" int rspi_maxlp_pattern(double *fconv, const int *pixels, const int *hist_row,
                                   long long n_pix, const int *hist, long long n_ref,
-                                  const int *nstate, long long n_data, const double *ref_params,
+                                  const int *nstate, long long n_modes, const double *ref_params,
                                   long long size, int rescale_mode, const double *rescale,
                                   int num_iter, double *rescale_out, cudaStream_t stream) {
     if (n_pix == 0) return RSPI_OK;  // nothing to search (e.g. an empty ring or mask)
     if (!fconv || !pixels || !hist_row || !hist || !nstate || !ref_params || n_ref <= 0 ||
-        n_data <= 0 || size <= 1 || size > 46340 || n_pix < 0 || n_pix > 0x7fffffffLL ||
-        n_ref > 0x7fffffffLL || num_iter < 0 || (rescale_mode == 1 && !rescale) ||
-        (rescale_mode != 0 && rescale_mode != 1))
+        n_modes <= 0 || n_modes > 65535 || size <= 1 || size > 46340 || n_pix < 0 ||
+        n_pix > 0x7fffffffLL || n_ref * n_modes > 0x7fffffffLL || num_iter < 0 ||
+        (rescale_mode == 1 && !rescale) || (rescale_mode != 0 && rescale_mode != 1))
         return RSPI_ERR_ARG;
-    k_pattern<<<(unsigned)n_pix, PT_THREADS, 0, stream>>>(
-        (double2 *)fconv, pixels, hist_row, hist, n_ref, nstate, n_data, ref_params, (int)size,
-        rescale_mode == 0, rescale, num_iter, rescale_out);
+    const dim3 grid((unsigned)n_pix, (unsigned)n_modes);
+    k_pattern<<<grid, PT_THREADS, 0, stream>>>((double2 *)fconv, pixels, hist_row, n_pix, hist,
+                                               n_ref, nstate, n_modes, ref_params, (int)size,
+                                               rescale_mode == 0, rescale, num_iter,
+                                               rescale_out);
     RSPI_RETURN_LAUNCH();
 }
 

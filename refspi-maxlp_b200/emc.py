@@ -19,6 +19,14 @@ mass, same argmax/maximum/log-sum-exp as ``fp64``), ``screen_delta``
 in chunks of at most this size, default 8), ``cuda_graph`` (capture the whole
 device iteration once and replay it, default true), ``autotune`` (pick the
 likelihood kernel's tile shape by timing, default false).
+
+``num_modes`` (emc.py:59, parsed but unused by the reference) reconstructs
+that many models at once: the (shift, diameter) grid is repeated per mode,
+likelihood rows are ``(m*S0 + s)*num_rot + j``, each frame's argmax picks a
+mode as well as a state, and MaxLP updates each mode from the frames that
+chose it.  ``model`` is then a (num_modes, size**2) array and
+``output_%03d.h5`` holds ``model`` as (num_modes, size, size) plus each
+frame's mode in ``modes``.
 """
 import configparser
 import os.path as op
@@ -62,7 +70,7 @@ class EMC():
 
         self._parse_data()
         self.phaser = MaxLPhaser(self.photons_file, size=self.size, dataset=self.dset,
-                                 num_iter=self.phaser_iter)
+                                 num_iter=self.phaser_iter, num_modes=self.num_modes)
         self._init_model()
 
         self.estep = EStep(self.dset.photons, self.size, self.num_rot, self.shiftx,
@@ -70,7 +78,8 @@ class EMC():
                            self.dset.bg.cpu().numpy(), form=self.form,
                            states_per_tile=self.states_per_tile, warps=self.warps_per_cta,
                            delta=self.screen_delta,
-                           slice_budget_bytes=int(self.slice_budget_gb * (1 << 30)))
+                           slice_budget_bytes=int(self.slice_budget_gb * (1 << 30)),
+                           n_modes=self.num_modes)
         self.prob = self.estep.prob
         self.state_vals = torch.from_numpy(self._state_values).to(self.device)
         self.phaser_rot = torch.from_numpy(geometry.phaser_rotation_table(
@@ -79,7 +88,7 @@ class EMC():
         if self.autotune:
             from rspi import autotune
             autotune.tune(self.estep)
-        npix = self.size ** 2
+        npix = self.size ** 2 * self.num_modes
         self._dmodel = torch.empty(npix, dtype=torch.complex128, device=self.device)
         self._host_model = torch.empty(npix, dtype=torch.complex128, pin_memory=True)
         self._host_rmax = torch.empty(self.dset.num_data, dtype=torch.int32, pin_memory=True)
@@ -89,6 +98,8 @@ class EMC():
         '''emc.py:57-65, plus the optional precision/tiling keys'''
         self.size = config.getint('emc', 'size')
         self.num_modes = config.getint('emc', 'num_modes', fallback=1)
+        if self.num_modes < 1:
+            raise ValueError('emc:num_modes must be at least 1')
         self.num_rot = config.getint('emc', 'num_rot')
         self.photons_file = op.join(start_dir, config.get('emc', 'in_photons_file'))
         self.output_folder = op.join(start_dir, config.get('emc', 'output_folder'))
@@ -162,7 +173,7 @@ class EMC():
             self._host_model.copy_(self._dmodel)
             self.dset.photons.err.check('EMC iteration')
         self.rmax = self._host_rmax.numpy().copy()
-        self.model = self._host_model.numpy().copy()
+        self.model = self._host_model.numpy().copy().reshape(self._model_shape())
         self.save_output(self.model, iternum)
 
     def _device_step(self):
@@ -213,12 +224,21 @@ class EMC():
         self.rmax = rmax.cpu().numpy().astype('i4')
 
     def _unravel_rmax(self, rmax):
-        '''Grid values of the chosen states (emc.py:218-224)'''
+        '''Grid values of the chosen states (emc.py:218-224); the mode of
+        each frame is ``_rmax_modes(rmax)``'''
         rmax = np.asarray(rmax)
-        s0 = rmax // self.num_rot
+        s0 = (rmax // self.num_rot) % len(self._state_values)
         ang = rmax % self.num_rot
         vals = self._state_values[s0]
         return vals[:, 0], vals[:, 1], vals[:, 2], ang * np.pi / self.num_rot
+
+    def _rmax_modes(self, rmax):
+        '''Mode of each frame's most likely state'''
+        return (np.asarray(rmax) // self.num_rot // len(self._state_values)).astype('i4')
+
+    def _model_shape(self):
+        npix = self.size ** 2
+        return (npix,) if self.num_modes == 1 else (self.num_modes, npix)
 
     def save_output(self, model, iternum, intens=None):
         '''``model.npy``, or ``output_%03d.h5`` (HDF5, written by rspi.h5lite)
@@ -228,16 +248,20 @@ class EMC():
             np.save(op.join(self.output_folder, 'model.npy'), self.model)
             return
         sx_vals, sy_vals, dia_vals, ang_vals = self._unravel_rmax(self.rmax)
-        out = {'model': np.asarray(self.model).reshape((self.size,) * 2),
+        shape = (self.size,) * 2 if self.num_modes == 1 else (self.num_modes,) + (self.size,) * 2
+        out = {'model': np.asarray(self.model).reshape(shape),
                'angles': ang_vals, 'diameters': dia_vals,
                'shifts': np.array([sx_vals, sy_vals]).T}
+        if self.num_modes > 1:
+            out['modes'] = self._rmax_modes(self.rmax)
         if intens is not None:
             out['intens'] = intens.cpu().numpy() if torch.is_tensor(intens) else np.asarray(intens)
         h5lite.write_datasets(op.join(self.output_folder, 'output_%.3d.h5' % iternum), out)
 
     def _random_model(self):
-        '''emc.py:241-242'''
-        self.model = np.random.random(self.size ** 2) + 1j * np.random.random(self.size ** 2)
+        '''emc.py:241-242 (one such model per mode)'''
+        shape = self._model_shape()
+        self.model = np.random.random(shape) + 1j * np.random.random(shape)
 
     def ramp(self, n):
         '''Shift phase ramp of state n (emc.py:244-245)'''

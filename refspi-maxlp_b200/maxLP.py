@@ -22,9 +22,10 @@ from rspi.device import MStep  # noqa: E402
 class MaxLPhaser():
     '''Reconstruction of object from holographic data using maximum likelihood and pattern search'''
     def __init__(self, data_fname, size=185, num_data=-1, dataset=None, device=None,
-                 num_iter=10):
+                 num_iter=10, num_modes=1):
         self.size = size
         self.num_iter = num_iter
+        self.num_modes = int(num_modes)
         if dataset is None:
             from dset import Dataset
             dataset = Dataset(data_fname, size ** 2, device=device, num_data=num_data)
@@ -38,7 +39,7 @@ class MaxLPhaser():
         self._gen_pattern(8)
         self.counts = dataset.photons.counts
         self.mean_count = dataset.photons.mean_count
-        self.mstep = MStep(dataset.photons, size, num_iter)
+        self.mstep = MStep(dataset.photons, size, num_iter, n_modes=self.num_modes)
 
     def _gen_pattern(self, nmax):
         '''33x33 candidate offsets (maxLP.py:45-48)'''
@@ -71,10 +72,21 @@ class MaxLPhaser():
         sval = np.pi * self.qrad.reshape((self.size,) * 2) * dia
         return (np.sin(sval) - sval * np.cos(sval)) / sval ** 3
 
-    def _run_phaser(self, model, sx_vals, sy_vals, dia_vals, ang_vals):
+    def _run_phaser(self, model, sx_vals, sy_vals, dia_vals, ang_vals, modes=None):
         '''Ring pass, global rescale and main pass over every phaser pixel
         (maxLP.py:304-340).  Frames may carry any (shift, diameter, angle);
-        frames sharing a (shift, diameter) share the reference amplitude.'''
+        frames sharing a (shift, diameter) share the reference amplitude.
+        With ``num_modes`` > 1, ``model`` is (num_modes, P) and ``modes[d]``
+        names the model frame d belongs to; each mode is searched over its
+        own frames.'''
+        nm = self.num_modes
+        if modes is None:
+            if nm > 1:
+                raise ValueError('modes (one per frame) are required with num_modes > 1')
+            modes = np.zeros(self.num_data, dtype='i4')
+        modes = np.asarray(modes).ravel()
+        if modes.size != self.num_data or modes.min() < 0 or modes.max() >= nm:
+            raise ValueError('modes must give each frame a mode in [0, %d)' % nm)
         sx = np.asarray(sx_vals, dtype='f8').ravel()
         sy = np.asarray(sy_vals, dtype='f8').ravel()
         dia = np.asarray(dia_vals, dtype='f8').ravel()
@@ -88,14 +100,16 @@ class MaxLPhaser():
         ref, fstate = np.unique(triples, axis=0, return_inverse=True)
         dev = self.device
         ref_params = torch.from_numpy(np.ascontiguousarray(ref)).to(dev)
-        fstate_t = torch.from_numpy(fstate.astype('i4').ravel()).to(dev)
+        fstate = modes.astype(np.int64) * ref.shape[0] + fstate.ravel()
+        fstate_t = torch.from_numpy(fstate.astype('i4')).to(dev)
         frot_t = torch.arange(self.num_data, dtype=torch.int32, device=dev)
-        nstate = torch.from_numpy(np.bincount(fstate.ravel(), minlength=ref.shape[0]).astype('i4')).to(dev)
+        nstate = torch.from_numpy(np.bincount(fstate, minlength=nm * ref.shape[0]).astype('i4')).to(dev)
         rot_cs = torch.from_numpy(geometry.phaser_rotation_table(ang)).to(dev)
         self.mstep.set_frame_params(fstate_t, frot_t, nstate)
-        fconv = torch.from_numpy(np.array(model, dtype=np.complex128).ravel()).to(dev)
+        model = np.array(model, dtype=np.complex128)
+        fconv = torch.from_numpy(model.ravel()).to(dev)
         self.mstep.run(fconv, ref_params, rot_cs)
-        out = fconv.cpu().numpy()
+        out = fconv.cpu().numpy().reshape(model.shape)
         self.dset.photons.err.check('MaxLP phaser')
         return out
 

@@ -169,7 +169,8 @@ class EStep:
 
     def __init__(self, photons, size, num_rot, shiftx, shifty, sphere_dia, probmask, bg,
                  form='fp64', states_per_tile=None, warps=32, n_ctas=0,
-                 slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel='stream'):
+                 slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel='stream',
+                 n_modes=1):
         if form not in ('fp64', 'screen'):
             raise ValueError('form must be fp64 or screen')
         if kernel not in ('stream', 'dynamic'):
@@ -180,7 +181,13 @@ class EStep:
         self.ph = photons
         self.device = dev = photons.device
         self.size, self.num_rot = int(size), int(num_rot)
-        self.n_states0 = int(np.asarray(shiftx).size)
+        # n_modes models share the (shift, diameter) grid: state m*S0 + s,
+        # likelihood row (m*S0 + s)*num_rot + j
+        self.n_modes = int(n_modes)
+        if self.n_modes < 1:
+            raise ValueError('n_modes must be at least 1')
+        self.n_grid = int(np.asarray(shiftx).size)
+        self.n_states0 = self.n_grid * self.n_modes
         self.n_rows = self.n_states0 * self.num_rot
         n = photons.num_data
         sel, pix2sel, p_pad = geometry.sel_pixels(probmask)
@@ -254,12 +261,18 @@ class EStep:
     # -- stages ------------------------------------------------------------
     def slices(self, model):
         """a4 + a5: holographic slices, masked sums, vscale and init."""
-        if model.dtype != torch.complex128 or not model.is_contiguous():
-            raise ValueError('model must be a contiguous complex128 device tensor')
+        npix = self.size ** 2
+        if model.dtype != torch.complex128 or not model.is_contiguous() or \
+                model.numel() != self.n_modes * npix:
+            raise ValueError('model must be a contiguous complex128 device tensor of %d x %d '
+                             'pixels' % (self.n_modes, npix))
         s = cur_stream()
-        call('rspi_holo_slices', ptr(model), ptr(self.shiftx), ptr(self.shifty),
-             ptr(self.sphere_dia), self.n_states0, self.size, ptr(self.bg), ptr(self.sel_pix),
-             self.n_sel, ptr(self.holo), ptr(self.msum), s)
+        flat = model.view(-1)
+        for m in range(self.n_modes):
+            g0 = m * self.n_grid
+            call('rspi_holo_slices', ptr(flat[m * npix:]), ptr(self.shiftx), ptr(self.shifty),
+                 ptr(self.sphere_dia), self.n_grid, self.size, ptr(self.bg), ptr(self.sel_pix),
+                 self.n_sel, ptr(self.holo[g0]), ptr(self.msum[g0:]), s)
         call('rspi_vscale_init', ptr(self.msum), self.n_states0, ptr(self.ph.powder),
              ptr(self.sel_pix), self.n_sel, ptr(self.vscale), ptr(self.init), s)
         if self.form == 'screen':
@@ -409,14 +422,22 @@ class Merge:
 
 
 class MStep:
-    """MaxLP pattern search of every phaser pixel (a11-a14)."""
+    """MaxLP pattern search of every phaser pixel (a11-a14).
 
-    def __init__(self, photons, size, num_iter=10):
+    With ``n_modes`` > 1 the model is ``n_modes`` stacked complex128 images
+    and frames carry a reference state ``m*n_ref + s``: each mode is searched
+    over the frames assigned to it, with its own ring rescale, in the same
+    launches."""
+
+    def __init__(self, photons, size, num_iter=10, n_modes=1):
         self.lib = load()
         self.ph = photons
         self.device = dev = photons.device
         self.size = int(size)
         self.num_iter = int(num_iter)
+        self.n_modes = int(n_modes)
+        if self.n_modes < 1:
+            raise ValueError('n_modes must be at least 1')
         g = geometry.phaser_pixels(self.size)
         t = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype='i4')).to(dev)  # noqa: E731
         self.mask_idx = t(g['mask_idx'])
@@ -424,27 +445,35 @@ class MStep:
         self.ring, self.ring_rows = t(g['ring']), t(g['ring_rows'])
         self.main, self.main_rows = t(g['main']), t(g['main_rows'])
         self.n_ring, self.n_main = int(g['ring'].size), int(g['main'].size)
-        self.rescales = torch.empty(max(1, self.n_ring), dtype=_f64, device=dev)
-        self.rescale = torch.empty(1, dtype=_f64, device=dev)
+        self.rescales = torch.empty(self.n_modes * max(1, self.n_ring), dtype=_f64, device=dev)
+        self.rescale = torch.empty(self.n_modes, dtype=_f64, device=dev)
         self.fstate = torch.empty(photons.num_data, dtype=_i32, device=dev)
         self.frot = torch.empty(photons.num_data, dtype=_i32, device=dev)
         self.hist = None
         self.nstate = None
 
     def frame_params_from_rmax(self, rmax, num_rot, n_ref):
-        """fstate / frot / nstate from the E-step argmax (emc.py:218-224)."""
-        if self.nstate is None or self.nstate.numel() != n_ref:
-            self.nstate = torch.empty(n_ref, dtype=_i32, device=self.device)
-        call('rspi_maxlp_frame_params', ptr(rmax), self.ph.num_data, int(num_rot), int(n_ref), ptr(self.fstate),
-            ptr(self.frot), ptr(self.nstate), ptr(self.ph.err.t), cur_stream())
+        """fstate / frot / nstate from the E-step argmax (emc.py:218-224);
+        ``n_ref`` (shift, diameter) states per mode, rows
+        ``(m*n_ref + s)*num_rot + j``."""
+        n_all = int(n_ref) * self.n_modes
+        if self.nstate is None or self.nstate.numel() != n_all:
+            self.nstate = torch.empty(n_all, dtype=_i32, device=self.device)
+        call('rspi_maxlp_frame_params', ptr(rmax), self.ph.num_data, int(num_rot), n_all,
+             ptr(self.fstate), ptr(self.frot), ptr(self.nstate), ptr(self.ph.err.t), cur_stream())
 
     def set_frame_params(self, fstate, frot, nstate):
         self.fstate, self.frot, self.nstate = fstate, frot, nstate
 
     def run(self, fconv, ref_params, rot_cs):
-        """Update ``fconv`` (complex128 device tensor) in place."""
+        """Update ``fconv`` (complex128 device tensor, ``n_modes`` x P) in place."""
         n_ref = int(ref_params.shape[0])
-        need = self.n_hist_rows * n_ref
+        nm = self.n_modes
+        if fconv.numel() != nm * self.size ** 2:
+            raise ValueError('fconv must hold %d model(s) of %d pixels' % (nm, self.size ** 2))
+        if self.nstate is None or self.nstate.numel() != nm * n_ref:
+            raise ValueError('frame parameters are not set for %d x %d states' % (nm, n_ref))
+        need = self.n_hist_rows * n_ref * nm
         if self.hist is None or self.hist.numel() < need:
             self.hist = torch.empty(max(1, need), dtype=_i32, device=self.device)
         hist = self.hist[:max(1, need)]
@@ -454,15 +483,17 @@ class MStep:
         call('rspi_maxlp_histogram', ptr(ph.ones), ptr(ph.multi), ptr(ph.ones_accum), ptr(ph.multi_accum),
             ptr(ph.place_ones), ptr(ph.place_multi), ptr(ph.count_multi), ph.num_data,
             ptr(self.fstate), ptr(self.frot), ptr(rot_cs), self.size, ptr(self.mask_idx),
-            self.n_hist_rows, n_ref, ptr(hist), ptr(ph.err.t), s)
+            self.n_hist_rows, n_ref * nm, ptr(hist), ptr(ph.err.t), s)
         call('rspi_maxlp_pattern', ptr(fconv), ptr(self.ring), ptr(self.ring_rows), self.n_ring, ptr(hist), n_ref,
-            ptr(self.nstate), ph.num_data, ptr(ref_params), self.size, 0, None,
+            ptr(self.nstate), nm, ptr(ref_params), self.size, 0, None,
             self.num_iter, ptr(self.rescales), s)
         if self.n_ring > 0:
-            call('rspi_mean', ptr(self.rescales), self.n_ring, ptr(self.rescale), s)
+            for m in range(nm):
+                call('rspi_mean', ptr(self.rescales[m * self.n_ring:]), self.n_ring,
+                     ptr(self.rescale[m:]), s)
         else:
             self.rescale.fill_(float('nan'))   # np.mean of an empty ring
         call('rspi_maxlp_pattern', ptr(fconv), ptr(self.main), ptr(self.main_rows), self.n_main, ptr(hist), n_ref,
-            ptr(self.nstate), ph.num_data, ptr(ref_params), self.size, 1, ptr(self.rescale),
+            ptr(self.nstate), nm, ptr(ref_params), self.size, 1, ptr(self.rescale),
             self.num_iter, None, s)
         return fconv

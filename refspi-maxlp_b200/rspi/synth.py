@@ -18,6 +18,14 @@ The generative model (per frame d):
   bilinear ``slice_gen`` convention (kernels.cu:19-33), Poisson-sampled and
   stored as ``ones`` / ``multi`` lists (make_data.py:323-328).
 
+Heterogeneous samples (``n_modes`` > 1): conformation 0 is the blob
+density above; each further conformation displaces a fraction
+``displace_frac`` of the blobs by ``displace`` px (uniform length, random
+direction).  Each frame draws its conformation with ``mode_weights``.
+Uneven loads (``count_lognormal = (median, sigma, lo, hi)``): each frame's
+expected photon count is its own lognormal draw clipped to [lo, hi] instead
+of the global normalisation times the fluence scale.
+
 Heavy per-frame work runs in torch on the requested device; the per-frame
 parameters come from ``numpy.random.default_rng(seed)`` child streams.
 """
@@ -35,22 +43,53 @@ CONFIGS = {
             fluence_sigma=0.5, dia=(6., 8.), shift_max=3.,
             recon=dict(num_rot=180, shiftx='-4 4 9', shifty='-4 4 9',
                        sphere_dia='6 8 5', num_iter=20)),
+    # uneven load, heterogeneous sample: 185x185, 50,000 frames with
+    # lognormal photon counts in [50, 50,000], 3 conformations (15% of blobs
+    # displaced 2-4 px) with weights 0.5/0.3/0.2, reconstructed as 3 modes
+    4: dict(size=185, n_blobs=40, obj_radius=20., num_data=50000, mean_count=None,
+            fluence_sigma=0.5, dia=(6., 8.), shift_max=3., n_modes=3,
+            mode_weights=(0.5, 0.3, 0.2), displace=(2., 4.), displace_frac=0.15,
+            count_lognormal=(float(np.sqrt(50. * 50000.)), 1.15, 50., 50000.),
+            recon=dict(num_rot=180, shiftx='-4 4 9', shifty='-4 4 9',
+                       sphere_dia='6 8 5', num_iter=20, num_modes=3)),
 }
+
+
+def make_blobs(size, n_blobs, obj_radius, rng):
+    """Blob centres, widths and amplitudes: (n_blobs, 4) = cx, cy, sigma, amp."""
+    c = size // 2
+    out = np.empty((n_blobs, 4))
+    for b in range(n_blobs):
+        r = obj_radius * np.sqrt(rng.random())
+        phi = 2 * np.pi * rng.random()
+        out[b] = (c + r * np.cos(phi), c + r * np.sin(phi), rng.uniform(1., 3.),
+                  rng.uniform(0.5, 1.))
+    return out
+
+
+def render_blobs(size, blobs):
+    x, y = np.indices((size, size), dtype='f8')
+    obj = np.zeros((size, size))
+    for cx, cy, sig, amp in blobs:
+        obj += amp * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * sig ** 2))
+    return obj
 
 
 def make_object(size, n_blobs, obj_radius, rng):
     """Real positive density of Gaussian blobs centred on ``size//2``."""
-    x, y = np.indices((size, size), dtype='f8')
-    c = size // 2
-    obj = np.zeros((size, size))
-    for _ in range(n_blobs):
-        r = obj_radius * np.sqrt(rng.random())
-        phi = 2 * np.pi * rng.random()
-        cx, cy = c + r * np.cos(phi), c + r * np.sin(phi)
-        sig = rng.uniform(1., 3.)
-        amp = rng.uniform(0.5, 1.)
-        obj += amp * np.exp(-((x - cx) ** 2 + (y - cy) ** 2) / (2 * sig ** 2))
-    return obj
+    return render_blobs(size, make_blobs(size, n_blobs, obj_radius, rng))
+
+
+def displaced_blobs(blobs, frac, dist, rng):
+    """A conformation: ``frac`` of the blobs moved by U(dist) px."""
+    out = blobs.copy()
+    k = max(1, int(round(frac * len(blobs))))
+    idx = rng.choice(len(blobs), size=k, replace=False)
+    length = rng.uniform(dist[0], dist[1], k)
+    phi = rng.uniform(0., 2 * np.pi, k)
+    out[idx, 0] += length * np.cos(phi)
+    out[idx, 1] += length * np.sin(phi)
+    return out
 
 
 def fourier(obj):
@@ -93,27 +132,44 @@ def _rotate_bilinear(img, angle, size):
 
 def generate(size, num_data, mean_count, n_blobs=20, obj_radius=12.,
              fluence_sigma=0.3, dia=(6., 8.), shift_max=3., seed=0,
-             device='cpu', chunk=256, dense=False):
+             device='cpu', chunk=256, dense=False, n_modes=1, mode_weights=None,
+             displace=(2., 4.), displace_frac=0.15, count_lognormal=None):
     """Generate one dataset; returns a dict in the photons-file layout.
 
     Keys: ``num_pix``, ``ones``, ``multi`` (int32, N), ``place_ones``,
     ``place_multi``, ``count_multi`` (flat int32; per-frame lengths are
     ``ones``/``multi``), truth ``true_angles``, ``true_shifts``,
     ``true_diameters``, ``scale``, ``solution``, and ``fsample``/``rel_scale``.
-    With ``dense=True`` a dense uint16 ``frames`` (N, size^2) is added.
+    With ``n_modes`` > 1, ``solution``/``fsample`` hold one row per
+    conformation and ``true_modes`` each frame's.  With ``dense=True`` a
+    dense uint16 ``frames`` (N, size^2) is added.
     """
     ss = np.random.SeedSequence(seed)
     r_obj, r_par, r_poi = [np.random.default_rng(s) for s in ss.spawn(3)]
-    obj = make_object(size, n_blobs, obj_radius, r_obj)
-    fs = fourier(obj).ravel()
+    blobs = [make_blobs(size, n_blobs, obj_radius, r_obj)]
+    for _ in range(1, n_modes):
+        blobs.append(displaced_blobs(blobs[0], displace_frac, displace, r_obj))
+    objs = [render_blobs(size, b) for b in blobs]
+    fss = [fourier(o).ravel() for o in objs]
 
     diam = r_par.uniform(dia[0], dia[1], num_data)
     shifts = r_par.uniform(-shift_max, shift_max, (num_data, 2))
     angles = r_par.uniform(0., 2 * np.pi, num_data)
     scale = r_par.lognormal(0., fluence_sigma, num_data)
+    modes = np.zeros(num_data, dtype='i4')
+    if n_modes > 1:
+        wts = np.full(n_modes, 1. / n_modes) if mode_weights is None else np.asarray(mode_weights)
+        modes = r_par.choice(n_modes, size=num_data, p=wts / wts.sum()).astype('i4')
+    target = None
+    if count_lognormal is not None:
+        med, sig, lo_c, hi_c = count_lognormal
+        target = np.clip(r_par.lognormal(np.log(med), sig, num_data), lo_c, hi_c)
+        scale = target / target.mean()
 
     dev = torch.device(device)
-    fs_t = torch.from_numpy(fs).to(dev)
+    fs_all = torch.from_numpy(np.stack(fss)).to(dev)
+    fs_t = fs_all[0]
+    modes_t = torch.from_numpy(modes.astype(np.int64)).to(dev)
     x = torch.arange(size, dtype=torch.float64, device=dev)
     cen = size // 2
     pr = torch.sqrt(((x - cen)[:, None] ** 2 + (x - cen)[None, :] ** 2)).reshape(-1)
@@ -129,16 +185,18 @@ def generate(size, num_data, mean_count, n_blobs=20, obj_radius=12.,
         sh = torch.from_numpy(shifts[lo:hi]).to(dev)
         ff, _, _ = _sphere_ff(size, d, dev)
         ph = 2. * np.pi * (dx[None] * sh[:, :1] + dy[None] * sh[:, 1:]) / size
-        re = torch.cos(ph) * ff * rel + fs_t.real[None]
-        im = torch.sin(ph) * ff * rel + fs_t.imag[None]
+        fsm = fs_all[modes_t[lo:hi]]
+        re = torch.cos(ph) * ff * rel + fsm.real
+        im = torch.sin(ph) * ff * rel + fsm.imag
         return (re * re + im * im) * detmask[None]
 
-    tot = 0.
-    for lo in range(0, num_data, chunk):
-        hi = min(num_data, lo + chunk)
-        w = intens(lo, hi).sum(1).cpu().numpy()
-        tot += float((w * scale[lo:hi]).sum())
-    gfac = mean_count * num_data / tot
+    if target is None:
+        tot = 0.
+        for lo in range(0, num_data, chunk):
+            hi = min(num_data, lo + chunk)
+            w = intens(lo, hi).sum(1).cpu().numpy()
+            tot += float((w * scale[lo:hi]).sum())
+        gfac = mean_count * num_data / tot
 
     gen = torch.Generator(device=dev)
     gen.manual_seed(int(r_poi.integers(0, 2 ** 62)))
@@ -147,7 +205,11 @@ def generate(size, num_data, mean_count, n_blobs=20, obj_radius=12.,
     frames = np.zeros((num_data, size * size), dtype=np.uint16) if dense else None
     for lo in range(0, num_data, chunk):
         hi = min(num_data, lo + chunk)
-        w = intens(lo, hi) * (gfac * torch.from_numpy(scale[lo:hi]).to(dev))[:, None]
+        w = intens(lo, hi)
+        if target is None:
+            w = w * (gfac * torch.from_numpy(scale[lo:hi]).to(dev))[:, None]
+        else:   # this frame's own expected count
+            w = w * (torch.from_numpy(target[lo:hi]).to(dev) / w.sum(1))[:, None]
         rot = _rotate_bilinear(w, torch.from_numpy(angles[lo:hi]).to(dev), size)
         cnt = torch.poisson(rot, generator=gen).to(torch.int32)
         if dense:
@@ -165,7 +227,10 @@ def generate(size, num_data, mean_count, n_blobs=20, obj_radius=12.,
     out = dict(num_pix=np.array([size * size]), ones=ones, multi=multi,
                place_ones=cat(po), place_multi=cat(pm), count_multi=cat(cm),
                true_angles=angles, true_shifts=shifts, true_diameters=diam,
-               scale=scale, solution=obj, fsample=fs, rel_scale=np.array(rel))
+               scale=scale, solution=objs[0] if n_modes == 1 else np.stack(objs),
+               fsample=fss[0] if n_modes == 1 else np.stack(fss), rel_scale=np.array(rel))
+    if n_modes > 1:
+        out['true_modes'] = modes
     if dense:
         out['frames'] = frames
     return out
@@ -177,7 +242,14 @@ def generate_config(cfg, device='cpu', num_data=None, seed=None):
     return generate(c['size'], c['num_data'] if num_data is None else num_data,
                     c['mean_count'], c['n_blobs'], c['obj_radius'], c['fluence_sigma'],
                     c['dia'], c['shift_max'], seed=20260000 + cfg if seed is None else seed,
-                    device=device)
+                    device=device, **config_extras(cfg))
+
+
+def config_extras(cfg):
+    """Keyword arguments of ``generate`` beyond the common ones."""
+    c = CONFIGS[cfg]
+    return {k: c[k] for k in ('n_modes', 'mode_weights', 'displace', 'displace_frac',
+                              'count_lognormal') if k in c}
 
 
 def initial_model(size, seed):

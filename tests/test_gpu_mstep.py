@@ -88,7 +88,9 @@ def test_emc_two_iterations_match_reference(name, form, tmp_path):
         np.testing.assert_allclose(rec.model, g['model_out_%d' % it], rtol=RTOL_MODEL, atol=1e-12)
         from rspi import h5lite
         out = h5lite.read_datasets(os.path.join(str(tmp_path), 'out', 'output_%03d.h5' % it))
-        np.testing.assert_array_equal(out['model'], rec.model.reshape(out['model'].shape))
+        assert out['model'].shape == (int(g['size']),) * 2
+        if it == 2:   # the last file holds the final model
+            np.testing.assert_array_equal(out['model'], rec.model.reshape(out['model'].shape))
         np.testing.assert_array_equal(out['angles'], g['unravel_%d' % it][3])
         np.testing.assert_array_equal(out['shifts'], g['unravel_%d' % it][:2].T)
 
@@ -149,11 +151,20 @@ def test_recon_cli_writes_log_and_outputs(tmp_path):
     log = open(os.path.join(str(tmp_path), 'out', 'EMC.log')).read().splitlines()
     assert log[0] == 'Iter  time(s)  change' and len(log) == 3
     assert log[1].split()[0] == '1' and log[2].split()[0] == '2'
+    from rspi import h5lite
+    n = len(g['ones'])
+    grid = np.arange(int(g['num_rot'])) * np.pi / int(g['num_rot'])
     for it in (1, 2):
-        from rspi import h5lite
         out = h5lite.read_datasets(os.path.join(str(tmp_path), 'out', 'output_%03d.h5' % it))
-        np.testing.assert_array_equal(out['model'], rec.model.reshape(out['model'].shape))
-        np.testing.assert_array_equal(out['angles'], g['unravel_%d' % it][3])
-        np.testing.assert_array_equal(out['shifts'], g['unravel_%d' % it][:2].T)
+        assert out['model'].shape == (int(g['size']),) * 2
+        assert out['angles'].shape == out['diameters'].shape == (n,)
+        assert out['shifts'].shape == (n, 2)
+        assert np.all(np.isin(out['angles'], grid))
+    # the last file holds the final model and the last iteration's states
+    sxv, syv, diav, angv = rec._unravel_rmax(rec.rmax)
+    np.testing.assert_array_equal(out['model'], rec.model.reshape(out['model'].shape))
+    np.testing.assert_array_equal(out['angles'], angv)
+    np.testing.assert_array_equal(out['diameters'], diav)
+    np.testing.assert_array_equal(out['shifts'], np.array([sxv, syv]).T)
     assert os.path.exists(os.path.join(str(tmp_path), 'out', 'model_000.npy'))
     assert rec.rmax.shape == (len(g['ones']),)

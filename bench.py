@@ -105,6 +105,23 @@ def start_model(cfg_id, w):
                            for m in range(w['n_modes'])])
 
 
+def dram_traffic(args, w, es, rows_per_launch):
+    """DRAM bytes (read + write) of one likelihood launch from the committed
+    ncu capture of the same workload (form, configuration, frames, rows per
+    launch), or None when no capture matches."""
+    path = os.path.join(REPO, 'profiles', 'k_screen_ll2_config2_dram.json')
+    try:
+        with open(path) as f:
+            caps = json.load(f)['captures']
+    except (OSError, ValueError, KeyError):
+        return None
+    for c in caps:
+        if (c['form'] == es.form and c['config'] == args.config and c['frames'] == w['n'] and
+                c['rows_per_launch'] == int(round(rows_per_launch))):
+            return float(c['dram_bytes_read'] + c['dram_bytes_write'])
+    return None
+
+
 def write_inputs(tmp, w, data, form, slice_gb=8.):
     from rspi.photonfile import write_photons
     os.makedirs(os.path.join(tmp, 'out'), exist_ok=True)
@@ -396,11 +413,43 @@ def run_ours(args):
         dist.barrier()
 
     n_cand = getattr(rec.estep, 'n_candidates', None)
+    mem_gb = torch.cuda.max_memory_allocated(dev) / 1e9
+
+    # e2e through the public API: host model in, host model + argmax out
+    e2e = None
+    if not args.no_e2e:
+        rec.model = model0.copy().reshape(rec._model_shape())
+        for _ in range(min(args.warmup, 1)):
+            rec.run_iteration(None)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        t_e0 = time.perf_counter()
+        for _ in range(args.steps):
+            rec.run_iteration(None)
+        torch.cuda.synchronize()
+        e2e_s = (time.perf_counter() - t_e0) / args.steps
+        if world > 1:
+            t = torch.tensor([e2e_s], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        p = w['size'] ** 2 * w['n_modes']
+        e2e = {'value': world * w['n'] * w['n_states'] / e2e_s, 'unit': UNIT,
+               's_per_iteration': e2e_s, 'h2d_bytes_per_step': 16 * p,
+               'd2h_bytes_per_step': 16 * p + 4 * w['n'],
+               'api': 'EMC.run_iteration (model host->device, model + argmax device->host)'}
 
     # the plain form: FP64 slices and likelihoods, warp-per-frame kernel
     plain = None
     if not args.no_plain and rank == 0:
         from rspi.device import EStep
+        # the chosen form's likelihood matrix, slices, candidates and graph
+        # pool are released first: both matrices need not fit at once
+        rec._graph = None
+        rec.prob = None
+        for name in ('prob', 'lsl', 'cand_d', 'cand_r', 'cand_ll', 'row_cand'):
+            setattr(es, name, None)
+        torch.cuda.empty_cache()
         pe = EStep(rec.dset.photons, w['size'], w['num_rot'], rec.shiftx, rec.shifty,
                    rec.sphere_dia, rec.probmask, rec.dset.bg.cpu().numpy(), form='fp64',
                    kernel='dynamic', n_modes=w['n_modes'])
@@ -428,37 +477,12 @@ def run_ours(args):
         del pe
         torch.cuda.empty_cache()
 
-    # e2e through the public API: host model in, host model + argmax out
-    e2e = None
-    if not args.no_e2e:
-        rec.model = model0.copy().reshape(rec._model_shape())
-        for _ in range(min(args.warmup, 1)):
-            rec.run_iteration(None)
-        torch.cuda.synchronize()
-        if world > 1:
-            dist.barrier()
-        t_e0 = time.perf_counter()
-        for _ in range(args.steps):
-            rec.run_iteration(None)
-        torch.cuda.synchronize()
-        e2e_s = (time.perf_counter() - t_e0) / args.steps
-        if world > 1:
-            t = torch.tensor([e2e_s], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
-        p = w['size'] ** 2 * w['n_modes']
-        e2e = {'value': world * w['n'] * w['n_states'] / e2e_s, 'unit': UNIT,
-               's_per_iteration': e2e_s, 'h2d_bytes_per_step': 16 * p,
-               'd2h_bytes_per_step': 16 * p + 4 * w['n'],
-               'api': 'EMC.run_iteration (model host->device, model + argmax device->host)'}
-
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
         return 0
 
     pk = peaks()
-    es = rec.estep
     # entry rows of 32 photon slots the likelihood kernel walks per likelihood row
     total_rows = es.ll16['total_rows'] if es.form == 'screen' else es.ll['total_rows']
     esz = 4 if es.slice_code == 0 else 8
@@ -477,18 +501,7 @@ def run_ours(args):
     lanes = 32 if es.slice_code == 0 else 16
     gather_peak = sm_count * lanes * clk_mhz * 1e6
     gather_rate = gathers / (ll_launch_ms * 1e-3)
-    traffic = None
-    prof = os.path.join(REPO, 'profiles', 'loglike_traffic.json')
-    if os.path.exists(prof):
-        try:
-            with open(prof) as f:
-                pj = json.load(f)
-            traffic = pj.get('%s_%s_bytes_per_row' % (args.form, 'cfg%d' % args.config))
-            if traffic is not None:
-                traffic = float(traffic) * rows_per_launch
-        except Exception:
-            traffic = None
-
+    traffic = dram_traffic(args, w, es, rows_per_launch)
     value = world * w['n'] * w['n_states'] / (ms * 1e-3)
     cpu = None
     if not args.no_cpu_baseline and world == 1:
@@ -532,6 +545,7 @@ def run_ours(args):
                  'candidates_rescored': n_cand},
         'cpu_baseline': cpu,
         'setup_s': {'generate': t_gen},
+        'device_memory_gb': mem_gb,
     }
     print(json.dumps(out))
     if world > 1:

@@ -340,6 +340,43 @@ int rspi_maxlp_pattern(double *fconv, const int *pixels, const int *hist_row,
 /* Mean of n values into *out (the global rescale, maxLP.py:329). */
 int rspi_mean(const double *vals, long long n, double *out, cudaStream_t stream);
 
+/* ------------------------------------------------- a7, dense frames (BF16 GEMM)
+ * Frames stored densely (uint16 counts, frames x P; no reference counterpart:
+ * the reference stores photons sparsely, dset.py:23-60) go through the photon
+ * term of calc_prob_all (kernels.cu:116-137) as a tensor-core GEMM:
+ *   LL[r][d] = init[r / num_rot] * scale[d] + sum_c K[d][sel_pix[c]] L[r][c].
+ *
+ * rspi_dense_frames: K over the likelihood pixels as BF16 digit matrices
+ * (frames x k_pad, K-major, zero beyond n_sel; k_pad % 64 == 0):
+ * a0 = K & 255 and, when a1 != NULL, a1 = K - (K & 255); both exact in BF16.
+ * *kmax (zeroed by the caller) gets the largest count; above 255 the caller
+ * must pass a1. */
+int rspi_dense_frames(const unsigned short *frames, long long n_frames, long long npix,
+                      const int *sel_pix, long long n_sel, long long k_pad, void *a0, void *a1,
+                      int *kmax, cudaStream_t stream);
+
+/* Rotated log-slices of rows [row_begin, row_end) (the values of
+ * rspi_rot_log_slices, computed in FP64) split into BF16 parts
+ * hi = bf16(L), lo = bf16(L - hi), rows x k_pad each (zero beyond n_sel);
+ * |L - hi - lo| <= 2^-16 |L|.  abs_max as in rspi_rot_log_slices. */
+int rspi_rot_log_split(const double *holo, long long n_states0, long long num_rot,
+                       const double *rot_cs, long long size, const double *bg,
+                       const int *sel_pix, long long n_sel, long long k_pad,
+                       long long row_begin, long long row_end, void *hi, void *lo,
+                       float *abs_max, cudaStream_t stream);
+
+/* Likelihood rows [row_begin, row_end) of every frame by tcgen05 BF16 MMAs
+ * with FP32 accumulation in tensor memory: b_hi/b_lo hold n_brows slice rows
+ * starting at row_begin; a1 may be NULL (counts below 256).  prob points at
+ * row row_begin (row stride ld >= n_frames, frames contiguous, FP32).  All
+ * matrix bases 16-byte aligned.  A device wait that exceeds its bound sets
+ * *err = RSPI_ERR_TIMEOUT and leaves the tile's likelihoods unwritten. */
+int rspi_dense_loglike(const void *a0, const void *a1, const void *b_hi, const void *b_lo,
+                       long long k_pad, long long n_frames, long long n_brows,
+                       long long num_rot, long long row_begin, long long row_end,
+                       const double *init, const double *scales, float *prob, long long ld,
+                       int *err, cudaStream_t stream);
+
 /* ----------------------------------------------------------------------- a16
  * Negative log-likelihood of the MaxLP model and its adjoint (no reference
  * counterpart works: get_grad_pixel, maxLP.py:199-214, uses an undefined

@@ -1,0 +1,435 @@
+// Dense high-fluence likelihood (row a7 for frames stored as dense uint16):
+// the photon term sum_p K[d][p] L[r][p] as a tensor-core GEMM on sm_100a.
+//
+//   LL[r][d] = init[r / num_rot] * scale[d] + sum_{p in sel} K[d][p] L[r][p]
+//
+// (calc_prob_all, kernels.cu:116-137, with every pixel of the frame an
+// entry).  K is exact in BF16 up to 256 photons, so K = K0 + K1 with
+// K0 = K & 255 and K1 = K - K0 (a multiple of 256 below 65536, also exact);
+// K1 is only used when some pixel holds more than 255 photons.  The FP64
+// log-slice value is split as hi = bf16(L), lo = bf16(L - hi), so
+// |L - hi - lo| <= 2^-16 |L|.  Every (digit, part) product is accumulated
+// in one FP32 TMEM accumulator by tcgen05.mma (kind::f16, BF16 inputs).
+//
+// Kernel structure (one 128-frame x 128-row tile per CTA, 4 warps):
+//   warp 0 lane 0  TMA producer: A digit tiles and B hi/lo tiles of each
+//                  64-pixel k-block into a ring of shared-memory stages
+//                  (128-byte swizzle), completion on a "full" mbarrier;
+//   warp 1 lane 0  MMA issuer: 4 x (digits x 2) tcgen05.mma per k-block,
+//                  tcgen05.commit to the stage's "empty" mbarrier, and a
+//                  final commit to the accumulator barrier;
+//   all warps      epilogue: tcgen05.ld of its 32 TMEM lanes (frames),
+//                  + init * scale, coalesced FP32 stores (frames contiguous).
+// Every mbarrier wait is bounded (about one second); on expiry the kernel
+// records RSPI_ERR_TIMEOUT, stops issuing, waits (bounded) for what it has
+// issued, frees its TMEM and skips the stores.  No cluster multicast.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include "rspi_common.cuh"
+
+namespace {
+
+constexpr int DN_BM = 128;          // frames per tile = TMEM lanes
+constexpr int DN_BN = 128;          // likelihood rows per tile = TMEM columns (FP32)
+constexpr int DN_BK = 64;           // pixels per k-block: 64 x 2 B = one 128-byte swizzle row
+constexpr int DN_UK = 16;           // K of one kind::f16 MMA
+constexpr int DN_TILE_BYTES = DN_BM * DN_BK * 2;   // 16 KB (A and B tiles alike: 128 x 64)
+constexpr int DN_SMEM_BUDGET = 200 * 1024;
+constexpr long long DN_WAIT_NS = 1000000000LL;     // bounded waits: 1 s
+
+static_assert(DN_BM == DN_BN, "A and B tiles share one TMA box");
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for the phase of parity `parity` to complete; false after DN_WAIT_NS.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (!mbar_try(bar, parity))
+        if (global_ns() - t0 > (unsigned long long)DN_WAIT_NS) return false;
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                            uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major tile of 128-byte rows with the
+// 128-byte swizzle, 8-row groups 1024 bytes apart (stride byte offset), the
+// leading byte offset unused for this layout (encoded 1), descriptor
+// version 1 (bits 46-47), swizzle mode 2 = 128B (bits 61-63).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(1024 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)2 << 61;
+    return d;
+}
+
+// Instruction descriptor, kind::f16: D F32 (bits 4-5 = 1), A and B BF16
+// (bits 7-9, 10-12 = 1), both K-major (bits 15, 16 = 0), N >> 3 at bits
+// 17-22, M >> 4 at bits 24-28.
+constexpr uint32_t DN_IDESC = (1u << 4) | (1u << 7) | (1u << 10) |
+                              ((uint32_t)(DN_BN >> 3) << 17) | ((uint32_t)(DN_BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(DN_IDESC), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+        "[%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+          "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+          "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+          "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+          "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+          "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+struct DenseMaps {
+    CUtensorMap a0, a1, bhi, blo;
+};
+
+// Dynamic shared memory: [stages][digits + 2 tiles] of 16 KB, then barriers.
+__global__ void __launch_bounds__(128, 1)
+k_dense_ll(const __grid_constant__ DenseMaps maps, int n_digits, int stages, int n_kb,
+           long long n_frames, long long row_begin, long long row_end, long long num_rot,
+           const double *__restrict__ init, const double *__restrict__ scales,
+           float *__restrict__ prob, long long ld, int *err) {
+    extern __shared__ uint8_t dn_smem_raw[];
+    __shared__ uint64_t bars[2 * 8 + 1];
+    __shared__ uint32_t tmem_base_sh;
+    __shared__ int abort_sh;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t base = (smem_u32(dn_smem_raw) + 1023u) & ~1023u;
+    const int tiles = n_digits + 2;
+    const uint32_t stage_bytes = (uint32_t)tiles * DN_TILE_BYTES;
+    const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[8]);
+    const uint32_t accb = smem_u32(&bars[16]);
+    const long long frame0 = (long long)blockIdx.x * DN_BM;
+    const long long rr0 = (long long)blockIdx.y * DN_BN;   // local row of this tile
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < stages; ++s) {
+            mbar_init(full0 + 8 * s, 1);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        mbar_init(accb, 1);
+        abort_sh = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_base_sh)),
+                     "r"(DN_BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_sh;
+
+    if (warp == 0 && lane == 0) {
+        // producer
+        int issued = 0;
+        for (int kb = 0; kb < n_kb; ++kb) {
+            const int s = kb % stages;
+            const uint32_t use = (uint32_t)(kb / stages);
+            if (kb >= stages && !mbar_wait(empty0 + 8 * s, (use - 1u) & 1u)) {
+                rspi_flag(err, RSPI_ERR_TIMEOUT);
+                atomicExch(&abort_sh, 1);
+                break;
+            }
+            if (*(volatile int *)&abort_sh) break;
+            const uint32_t st = base + (uint32_t)s * stage_bytes;
+            mbar_expect_tx(full0 + 8 * s, stage_bytes);
+            const int x = kb * DN_BK;
+            tma_load_2d(st, &maps.a0, x, (int)frame0, full0 + 8 * s);
+            if (n_digits > 1) tma_load_2d(st + DN_TILE_BYTES, &maps.a1, x, (int)frame0, full0 + 8 * s);
+            const uint32_t sb = st + (uint32_t)n_digits * DN_TILE_BYTES;
+            tma_load_2d(sb, &maps.bhi, x, (int)rr0, full0 + 8 * s);
+            tma_load_2d(sb + DN_TILE_BYTES, &maps.blo, x, (int)rr0, full0 + 8 * s);
+            ++issued;
+        }
+        // every issued load lands before the CTA can exit
+        for (int kb = (issued > stages ? issued - stages : 0); kb < issued; ++kb)
+            if (!mbar_wait(full0 + 8 * (kb % stages), (uint32_t)(kb / stages) & 1u)) {
+                rspi_flag(err, RSPI_ERR_TIMEOUT);
+                atomicExch(&abort_sh, 1);
+            }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        for (int kb = 0; kb < n_kb; ++kb) {
+            const int s = kb % stages;
+            if (*(volatile int *)&abort_sh) break;
+            if (!mbar_wait(full0 + 8 * s, (uint32_t)(kb / stages) & 1u)) {
+                rspi_flag(err, RSPI_ERR_TIMEOUT);
+                atomicExch(&abort_sh, 1);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t st = base + (uint32_t)s * stage_bytes;
+            const uint32_t sb = st + (uint32_t)n_digits * DN_TILE_BYTES;
+            for (int dg = 0; dg < n_digits; ++dg)
+                for (int part = 0; part < 2; ++part)
+#pragma unroll
+                    for (int k = 0; k < DN_BK / DN_UK; ++k) {
+                        const uint32_t koff = (uint32_t)k * DN_UK * 2;
+                        const uint64_t ad = sw128_desc(st + (uint32_t)dg * DN_TILE_BYTES + koff);
+                        const uint64_t bd = sw128_desc(sb + (uint32_t)part * DN_TILE_BYTES + koff);
+                        mma_bf16(tmem, ad, bd, (kb | dg | part | k) != 0);
+                    }
+            mma_commit(empty0 + 8 * s);
+        }
+        mma_commit(accb);   // arrives once every MMA issued above has completed
+    }
+    __syncwarp();
+
+    // epilogue: TMEM lanes 32*warp .. +31 are frames frame0 + 32*warp + lane
+    const bool ready = mbar_wait(accb, 0);
+    if (!ready) rspi_flag(err, RSPI_ERR_TIMEOUT);
+    // one decision for the whole CTA (tcgen05.ld is warp-collective)
+    const bool ok = __syncthreads_and(ready && !abort_sh) && n_kb > 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const long long d = frame0 + 32 * warp + lane;
+    const double sc = d < n_frames ? scales[d] : 0.;
+    if (ok) {
+        for (int c0 = 0; c0 < DN_BN; c0 += 32) {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+            if (d < n_frames) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const long long rr = rr0 + c0 + j;
+                    const long long r = row_begin + rr;
+                    if (r < row_end)
+                        prob[rr * ld + d] = (float)(init[r / num_rot] * sc + (double)v[j]);
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(DN_BN)
+                     : "memory");
+}
+
+// Dense frames -> BF16 digit matrices over the likelihood pixels (K-major,
+// k_pad columns, zero beyond n_sel); kmax gets the largest count seen.
+__global__ void k_dense_frames(const unsigned short *__restrict__ frames, long long n_frames,
+                               long long npix, const int *__restrict__ sel_pix, long long n_sel,
+                               long long k_pad, __nv_bfloat16 *__restrict__ a0,
+                               __nv_bfloat16 *__restrict__ a1, int *__restrict__ kmax) {
+    const long long total = n_frames * k_pad;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    int mx = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const long long d = i / k_pad, c = i - d * k_pad;
+        const int k = c < n_sel ? (int)frames[d * npix + sel_pix[c]] : 0;
+        mx = max(mx, k);
+        a0[i] = __int2bfloat16_rn(k & 255);
+        if (a1) a1[i] = __int2bfloat16_rn(k & ~255);
+    }
+    mx = warp_max_int(mx);
+    if ((threadIdx.x & 31) == 0) atomicMax(kmax, mx);
+}
+
+// Rotated log-slices split into BF16 hi + lo parts (same values as
+// k_rot_log: rot_log_value in FP64), zero beyond n_sel.
+__global__ void __launch_bounds__(256)
+k_rot_log_split(const double *__restrict__ holo, long long num_rot,
+                const double *__restrict__ rot_cs, int size, const double *__restrict__ bg,
+                const int *__restrict__ sel_pix, long long n_sel, long long k_pad,
+                long long row_begin, long long n_rows, __nv_bfloat16 *__restrict__ hi,
+                __nv_bfloat16 *__restrict__ lo, float *__restrict__ abs_max) {
+    const long long npix = (long long)size * size;
+    const long long total = n_rows * k_pad;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    float amax = 0.f;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const long long rr = i / k_pad, c = i - rr * k_pad;
+        double v = 0.;
+        if (c < n_sel) {
+            const long long r = row_begin + rr;
+            const long long s0 = r / num_rot, j = r - s0 * num_rot;
+            const int p = sel_pix[c];
+            const int x = p / size, y = p - (p / size) * size;
+            v = rot_log_value(holo + s0 * npix, x, y, size, rot_cs[2 * j], rot_cs[2 * j + 1],
+                              bg[p]);
+        }
+        const __nv_bfloat16 h = __double2bfloat16(v);
+        hi[i] = h;
+        lo[i] = __double2bfloat16(v - (double)__bfloat162float(h));
+        amax = fmaxf(amax, fabsf((float)v));
+    }
+    if (abs_max) {
+        amax = __int_as_float(warp_max_int(__float_as_int(amax)));
+        if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(abs_max), __float_as_int(amax));
+    }
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                  const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// 2-D BF16 map over a rows x k_pad K-major matrix, 64 x 128 boxes, 128B swizzle,
+// zero fill outside (rows beyond the matrix read as zeros).
+bool make_map(CUtensorMap *m, const void *ptr, long long k_pad, long long rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {(cuuint64_t)k_pad, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)k_pad * 2};
+    cuuint32_t box[2] = {(cuuint32_t)DN_BK, (cuuint32_t)DN_BM};
+    cuuint32_t estr[2] = {1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box,
+              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+           CUDA_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" int rspi_dense_frames(const unsigned short *frames, long long n_frames, long long npix,
+                                 const int *sel_pix, long long n_sel, long long k_pad, void *a0,
+                                 void *a1, int *kmax, cudaStream_t stream) {
+    if (!frames || !sel_pix || !a0 || !kmax || n_frames <= 0 || npix <= 0 || n_sel < 0 ||
+        k_pad < n_sel || k_pad % DN_BK)
+        return RSPI_ERR_ARG;
+    k_dense_frames<<<rspi_blocks(n_frames * k_pad, 256, 16), 256, 0, stream>>>(
+        frames, n_frames, npix, sel_pix, n_sel, k_pad, (__nv_bfloat16 *)a0, (__nv_bfloat16 *)a1,
+        kmax);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_rot_log_split(const double *holo, long long n_states0, long long num_rot,
+                                  const double *rot_cs, long long size, const double *bg,
+                                  const int *sel_pix, long long n_sel, long long k_pad,
+                                  long long row_begin, long long row_end, void *hi, void *lo,
+                                  float *abs_max, cudaStream_t stream) {
+    if (n_states0 <= 0 || num_rot <= 0 || size <= 1 || size > 46340 || k_pad < n_sel ||
+        k_pad % DN_BK || row_begin < 0 || row_end > n_states0 * num_rot || row_end < row_begin ||
+        !holo || !rot_cs || !bg || !hi || !lo)
+        return RSPI_ERR_ARG;
+    const long long n_rows = row_end - row_begin;
+    if (n_rows == 0) return RSPI_OK;
+    k_rot_log_split<<<rspi_blocks(n_rows * k_pad, 256, 16), 256, 0, stream>>>(
+        holo, num_rot, rot_cs, (int)size, bg, sel_pix, n_sel, k_pad, row_begin, n_rows,
+        (__nv_bfloat16 *)hi, (__nv_bfloat16 *)lo, abs_max);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_dense_loglike(const void *a0, const void *a1, const void *b_hi,
+                                  const void *b_lo, long long k_pad, long long n_frames,
+                                  long long n_brows, long long num_rot, long long row_begin,
+                                  long long row_end, const double *init, const double *scales,
+                                  float *prob, long long ld, int *err, cudaStream_t stream) {
+    if (!a0 || !b_hi || !b_lo || !init || !scales || !prob || !err || k_pad <= 0 ||
+        k_pad % DN_BK || n_frames <= 0 || num_rot <= 0 || row_begin < 0 ||
+        row_end < row_begin || row_end - row_begin > n_brows || ld < n_frames ||
+        n_frames > 0x7fffffffLL || n_brows > 0x7fffffffLL || k_pad > 0x7fffffffLL)
+        return RSPI_ERR_ARG;
+    // TMA: 16-byte aligned bases and row strides (k_pad * 2 bytes, k_pad % 64 == 0)
+    const uintptr_t al = (uintptr_t)a0 | (uintptr_t)b_hi | (uintptr_t)b_lo | (uintptr_t)a1;
+    if (al & 15) return RSPI_ERR_ARG;
+    const long long n_rows = row_end - row_begin;
+    if (n_rows == 0) return RSPI_OK;
+    const int n_digits = a1 ? 2 : 1;
+    DenseMaps maps;
+    if (!make_map(&maps.a0, a0, k_pad, n_frames) ||
+        !make_map(&maps.a1, a1 ? a1 : a0, k_pad, n_frames) ||
+        !make_map(&maps.bhi, b_hi, k_pad, n_brows) || !make_map(&maps.blo, b_lo, k_pad, n_brows))
+        return RSPI_ERR_CUDA;
+    const int stage_bytes = (n_digits + 2) * DN_TILE_BYTES;
+    const int stages = min(8, DN_SMEM_BUDGET / stage_bytes);
+    const int smem = stages * stage_bytes + 1024;
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_dense_ll, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 DN_SMEM_BUDGET + 1024) != cudaSuccess)
+            return RSPI_ERR_CUDA;
+        attr = true;
+    }
+    const dim3 grid((unsigned)((n_frames + DN_BM - 1) / DN_BM),
+                    (unsigned)((n_rows + DN_BN - 1) / DN_BN));
+    if (grid.y > 65535) return RSPI_ERR_TOO_LARGE;
+    k_dense_ll<<<grid, 128, smem, stream>>>(maps, n_digits, stages, (int)(k_pad / DN_BK),
+                                            n_frames, row_begin, row_end, num_rot, init, scales,
+                                            prob, ld, err);
+    RSPI_RETURN_LAUNCH();
+}

@@ -6,7 +6,10 @@ attributes (dset.py:16-61): ``num_data``, ``ones``, ``multi``,
 ``place_ones``, ``place_multi``, ``count_multi``, ``mean_count``,
 ``counts`` (when ``need_scaling``), ``bg``, ``mem``, plus ``get_frame`` and
 ``get_powder``.  Arrays are torch CUDA tensors instead of CuPy arrays; the
-prefix sums, counts and powder are computed by librspi kernels.
+prefix sums, counts and powder are computed by librspi kernels.  A photons
+file may also hold dense uint16 counts ``frames`` (N, num_pix) for the
+dense likelihood form; a file with only ``frames`` gets its sparse lists
+derived from them.
 """
 import os
 import sys
@@ -16,7 +19,7 @@ import torch
 
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 from rspi.device import DevicePhotons  # noqa: E402
-from rspi.photonfile import PhotonsFile  # noqa: E402
+from rspi.photonfile import PhotonsFile, sparse_from_dense  # noqa: E402
 
 
 def read_photons(photons_file, num_pix=None):
@@ -25,6 +28,14 @@ def read_photons(photons_file, num_pix=None):
     with PhotonsFile(photons_file) as fptr:
         if num_pix is not None and np.any(num_pix != np.asarray(fptr['num_pix'])):
             raise AttributeError('Number of pixels in photons file does not match')
+        frames = np.asarray(fptr['frames'], dtype=np.uint16) if 'frames' in fptr else None
+        npix = int(np.asarray(fptr['num_pix']).ravel()[0])
+        if frames is not None and 'place_ones' not in fptr:
+            # dense-only file: the sparse lists are derived from the frames
+            host = sparse_from_dense(frames)
+            host.update(num_data=frames.shape[0], num_pix=npix, frames=frames,
+                        bg=np.asarray(fptr['bg'], dtype='f8').ravel() if 'bg' in fptr else None)
+            return host
         num_data = fptr.num_rows('place_ones')
         po, po_len = fptr.flat('place_ones')
         pm, pm_len = fptr.flat('place_multi')
@@ -41,9 +52,8 @@ def read_photons(photons_file, num_pix=None):
             bg = np.asarray(fptr['bg'], dtype='f8').ravel()
         except KeyError:
             bg = None
-        npix = int(np.asarray(fptr['num_pix']).ravel()[0])
     return dict(num_data=num_data, num_pix=npix, ones=ones, multi=multi, place_ones=po,
-                place_multi=pm, count_multi=cm, bg=bg)
+                place_multi=pm, count_multi=cm, bg=bg, frames=frames)
 
 
 class Dataset():
@@ -66,7 +76,7 @@ class Dataset():
         before = torch.cuda.memory_allocated() if torch.cuda.is_available() else 0
         self.photons = DevicePhotons(host['ones'], host['multi'], host['place_ones'],
                                      host['place_multi'], host['count_multi'], num_pix,
-                                     need_scaling, device)
+                                     need_scaling, device, frames=host.get('frames'))
         ph = self.photons
         self.device = ph.device
         self.ones, self.multi = ph.ones, ph.multi
@@ -108,4 +118,6 @@ def _first_frames(host, n):
     out.update(num_data=n, ones=host['ones'][:n], multi=host['multi'][:n],
                place_ones=host['place_ones'][:o_end], place_multi=host['place_multi'][:m_end],
                count_multi=host['count_multi'][:m_end])
+    if host.get('frames') is not None:
+        out['frames'] = host['frames'][:n]
     return out

@@ -13,7 +13,9 @@ the MaxLP M-step run in librspi on the GPU; ``prob`` is a torch CUDA tensor
 Optional ``[emc]`` keys beyond the reference: ``form`` (``fp64``: FP64
 slices and FP64 likelihood matrix; ``screen``: FP32 screening pass with
 FP64 rescoring of every state that can be the argmax or carry posterior
-mass, same argmax/maximum/log-sum-exp as ``fp64``), ``screen_delta``
+mass, same argmax/maximum/log-sum-exp as ``fp64``; ``dense``: frames stored
+densely, screening likelihood as a BF16 tensor-core GEMM, same rescoring),
+``screen_delta``
 (default 20 nats), ``states_per_tile``, ``warps_per_cta``, ``phaser_iter``
 (default 10, maxLP.py:320,335), ``slice_budget_gb`` (rotated slices are built
 in chunks of at most this size, default 8), ``cuda_graph`` (capture the whole
@@ -106,8 +108,8 @@ class EMC():
         self.log_file = op.join(start_dir, config.get('emc', 'log_file'))
         self.need_scaling = config.getboolean('emc', 'need_scaling', fallback=False)
         self.form = config.get('emc', 'form', fallback='fp64')
-        if self.form not in ('fp64', 'screen'):
-            raise ValueError('emc:form must be fp64 or screen')
+        if self.form not in ('fp64', 'screen', 'dense'):
+            raise ValueError('emc:form must be fp64, screen or dense')
         self.screen_delta = config.getfloat('emc', 'screen_delta', fallback=20.)
         self.states_per_tile = config.getint('emc', 'states_per_tile', fallback=0) or None
         self.warps_per_cta = config.getint('emc', 'warps_per_cta', fallback=32)

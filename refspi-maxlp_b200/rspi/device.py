@@ -58,7 +58,7 @@ class DevicePhotons:
     """Sparse photons on the device (dset.py layout) and derived arrays."""
 
     def __init__(self, ones, multi, place_ones, place_multi, count_multi, num_pix,
-                 need_scaling=False, device=None):
+                 need_scaling=False, device=None, frames=None):
         self.lib = load()
         self.device = _dev(device)
         ones = np.ascontiguousarray(ones, dtype='i4')
@@ -103,6 +103,15 @@ class DevicePhotons:
         self.err.check('photon set-up')
         self.mean_count = float(self.mean_count_t.item())
         self._ll = None
+        self._dense = None
+        self.frames = None
+        if frames is not None:
+            frames = np.ascontiguousarray(frames, dtype=np.uint16)
+            if frames.shape != (n, self.num_pix):
+                raise ValueError('frames must be (num_data, num_pix) = (%d, %d)' % (n, self.num_pix))
+            # raw 16-bit counts (torch has no general uint16 arithmetic; the
+            # kernels read them as unsigned short)
+            self.frames = torch.from_numpy(frames.view(np.int16)).to(self.device)
 
     def ll_entries(self, pix2sel, p_pad):
         """Packed likelihood entries for the given sel map (built once)."""
@@ -129,6 +138,27 @@ class DevicePhotons:
                         row_off=row_off, entries=entries, order=order, total_rows=total)
         return self._ll
 
+
+    def dense_entries(self, sel_pix, n_sel, k_pad):
+        """BF16 count digits of the dense frames over the likelihood pixels
+        (built once): ``a0`` = K & 255, ``a1`` = K - a0 when some K > 255."""
+        key = (int(k_pad), sel_pix.data_ptr())
+        if self._dense is not None and self._dense['key'] == key:
+            return self._dense
+        if self.frames is None:
+            raise ValueError('the dense form needs dense frames (a photons file with "frames")')
+        n, dev, s = self.num_data, self.device, cur_stream()
+        a0 = torch.empty((n, k_pad), dtype=torch.bfloat16, device=dev)
+        kmax = torch.zeros(1, dtype=_i32, device=dev)
+        call('rspi_dense_frames', ptr(self.frames), n, self.num_pix, ptr(sel_pix), n_sel, k_pad,
+             ptr(a0), None, ptr(kmax), s)
+        a1 = None
+        if int(kmax.item()) > 255:
+            a1 = torch.empty_like(a0)
+            call('rspi_dense_frames', ptr(self.frames), n, self.num_pix, ptr(sel_pix), n_sel, k_pad,
+                 ptr(a0), ptr(a1), ptr(kmax), s)
+        self._dense = dict(key=key, a0=a0, a1=a1, kmax=int(kmax.item()))
+        return self._dense
 
     def ll16_entries(self, pix2sel, p_zero):
         """16-bit count-expanded entries for the FP32 screening pass."""
@@ -164,15 +194,18 @@ class EStep:
     the 16-bit photon entries, then FP64 rescoring of every state within
     ``delta`` (+ the FP32 error bound) of each frame's maximum, which gives
     the same argmax, maximum and log-sum-exp as the FP64 form (the chosen
-    form).
+    form).  ``form='dense'`` (frames stored densely, high fluence): the
+    screening likelihood is a tensor-core GEMM of BF16 count digits with
+    BF16 hi + lo log-slices (FP32 accumulation), followed by the same FP64
+    rescoring of the candidates.
     """
 
     def __init__(self, photons, size, num_rot, shiftx, shifty, sphere_dia, probmask, bg,
                  form='fp64', states_per_tile=None, warps=32, n_ctas=0,
                  slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel='stream',
                  n_modes=1):
-        if form not in ('fp64', 'screen'):
-            raise ValueError('form must be fp64 or screen')
+        if form not in ('fp64', 'screen', 'dense'):
+            raise ValueError('form must be fp64, screen or dense')
         if kernel not in ('stream', 'dynamic'):
             raise ValueError('kernel must be stream or dynamic')
         self.kernel = kernel
@@ -200,6 +233,9 @@ class EStep:
         self.rot_cs = t(geometry.emc_rotation_table(self.num_rot))
         self.bg = t(np.asarray(bg, dtype='f8').ravel())
         self.ll = photons.ll_entries(self.pix2sel, self.p_pad)
+        if form == 'dense':
+            self._init_dense(photons, slice_budget_bytes, delta, cand_per_frame)
+            return
         if form == 'fp64':
             self.slice_code, self.prob_code, self.p_row = 1, 1, self.p_pad
         else:
@@ -250,6 +286,54 @@ class EStep:
         self.check_capacity = True
         self.ll_events = None   # list -> (start, end, rows) CUDA events around each launch
 
+    def _init_dense(self, photons, slice_budget_bytes, delta, cand_per_frame):
+        dev, n = self.device, photons.num_data
+        self.kernel = 'tcgen05'
+        self.slice_code, self.prob_code = 2, 0           # BF16 hi/lo slices, FP32 matrix
+        self.k_pad = (self.n_sel + 63) // 64 * 64
+        self.p_row = self.k_pad
+        self.dense = photons.dense_entries(self.sel_pix, self.n_sel, self.k_pad)
+        self.n_digits = 2 if self.dense['a1'] is not None else 1
+        self.delta = float(delta)
+        self.slice_torch, self.prob_torch = torch.bfloat16, torch.float32
+        self.tile = 128
+        rows = max(128, (slice_budget_bytes // (self.k_pad * 4)) // 128 * 128)
+        self.chunk_rows = int(min(self.n_rows, rows))
+        npix = self.size ** 2
+        self.holo = torch.empty((self.n_states0, npix), dtype=_f64, device=dev)
+        self.msum = torch.empty(self.n_states0, dtype=_f64, device=dev)
+        self.vscale = torch.empty(1, dtype=_f64, device=dev)
+        self.init = torch.empty(self.n_states0, dtype=_f64, device=dev)
+        self.lsl_hi = torch.empty((self.chunk_rows, self.k_pad), dtype=torch.bfloat16, device=dev)
+        self.lsl_lo = torch.empty_like(self.lsl_hi)
+        self.lsl = self.lsl_hi
+        self.prob = torch.empty((self.n_rows, n), dtype=torch.float32, device=dev)
+        self.maxll = torch.empty(n, dtype=_f64, device=dev)
+        self.rmax = torch.empty(n, dtype=_i32, device=dev)
+        self.logz = torch.empty(n, dtype=_f64, device=dev)
+        self.lmax = torch.zeros(1, dtype=torch.float32, device=dev)
+        self.max32 = torch.empty(n, dtype=_f64, device=dev)
+        self.rmax32 = torch.empty(n, dtype=_i32, device=dev)
+        self.cnt_part = torch.empty(n * 32, dtype=_i32, device=dev)
+        self.cand_n = torch.empty(n, dtype=_i32, device=dev)
+        self.noncand = torch.empty(n, dtype=_f64, device=dev)
+        self.thr = torch.empty(n, dtype=_f64, device=dev)
+        self.cand_off = torch.empty(n + 1, dtype=_i64, device=dev)
+        self.row_cnt = torch.empty(self.n_rows, dtype=_i32, device=dev)
+        self.row_cand_off = torch.empty(self.n_rows + 1, dtype=_i64, device=dev)
+        # Error bound of the GEMM value (the candidate threshold's eps_d takes
+        # "rows" FP32 rounding steps per photon x lmax): 2^-16 relative from
+        # the hi + lo split (256 steps of 2^-24) plus 2 x 2^-24 for each of
+        # the n_steps tensor-core accumulations (a rounding or truncating
+        # FP32 adder), as the same per-frame row count for every frame.
+        n_steps = (self.k_pad // 16) * self.n_digits * 2
+        self.eq_rows = 256 + 2 * n_steps
+        self.eq_row_off = torch.arange(n + 1, dtype=_i64, device=dev) * self.eq_rows
+        per = int(cand_per_frame) if cand_per_frame else min(self.n_rows, 8192)
+        self._alloc_candidates(max(1024, per * n))
+        self.check_capacity = True
+        self.ll_events = None
+
     def _alloc_candidates(self, cap):
         dev = self.device
         self.capacity = int(cap)
@@ -275,11 +359,17 @@ class EStep:
                  self.n_sel, ptr(self.holo[g0]), ptr(self.msum[g0:]), s)
         call('rspi_vscale_init', ptr(self.msum), self.n_states0, ptr(self.ph.powder),
              ptr(self.sel_pix), self.n_sel, ptr(self.vscale), ptr(self.init), s)
-        if self.form == 'screen':
+        if self.form != 'fp64':
             self.lmax.zero_()
 
     def rot_slices(self, r0, r1, out=None):
         """a6: rotated log-slices of rows [r0, r1) into ``out`` (or the chunk buffer)."""
+        if self.form == 'dense':
+            call('rspi_rot_log_split', ptr(self.holo), self.n_states0, self.num_rot,
+                 ptr(self.rot_cs), self.size, ptr(self.bg), ptr(self.sel_pix), self.n_sel,
+                 self.k_pad, r0, r1, ptr(self.lsl_hi), ptr(self.lsl_lo), ptr(self.lmax),
+                 cur_stream())
+            return self.lsl_hi
         out = self.lsl if out is None else out
         call('rspi_rot_log_slices', ptr(self.holo), self.n_states0, self.num_rot,
              ptr(self.rot_cs), self.size, ptr(self.bg), ptr(self.sel_pix), self.n_sel,
@@ -301,7 +391,13 @@ class EStep:
             self.ll_events.append(ev)
 
     def _loglike_launch(self, r0, r1, lsl, n):
-        if self.kernel == 'stream' and self.form == 'screen':
+        if self.form == 'dense':
+            dn = self.dense
+            call('rspi_dense_loglike', ptr(dn['a0']), ptr(dn['a1']), ptr(self.lsl_hi),
+                 ptr(self.lsl_lo), self.k_pad, n, self.chunk_rows, self.num_rot, r0, r1,
+                 ptr(self.init), ptr(self.ph.scales), ptr(self.prob[r0]), n, ptr(self.ph.err.t),
+                 cur_stream())
+        elif self.kernel == 'stream' and self.form == 'screen':
             l16 = self.ll16
             call('rspi_screen_loglike2', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
                  ptr(self.ph.scales), ptr(l16['entries']), ptr(l16['row_off']), n, r0, r1,
@@ -345,8 +441,9 @@ class EStep:
         call('rspi_frame_reduce', ptr(self.prob), 0, self.n_rows, n, ptr(self.max32),
              ptr(self.rmax32), None, s)
         while True:
+            rows_eq = self.eq_row_off if self.form == 'dense' else self.ll16['row_off']
             call('rspi_screen_candidates', ptr(self.prob), self.n_rows, n, ptr(self.max32),
-                 ptr(self.rmax32), ptr(self.ll['frame_sel_photons']), ptr(self.ll16['row_off']), ptr(self.lmax),
+                 ptr(self.rmax32), ptr(self.ll['frame_sel_photons']), ptr(rows_eq), ptr(self.lmax),
                  self.delta, ptr(self.cnt_part), ptr(self.cand_n), ptr(self.noncand),
                  ptr(self.thr), ptr(self.cand_off), self.capacity, ptr(self.cand_d),
                  ptr(self.cand_r), ptr(self.ph.err.t), s)

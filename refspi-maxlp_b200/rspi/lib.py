@@ -47,6 +47,9 @@ SIGNATURES = {
     'rspi_posterior_pairs': (I, [P, L, L, P, D, P, P, P, L, P, P, P, P, P]),
     'rspi_merge_coverage': (I, [L, P, L, P, P]),
     'rspi_merge': (I, [P, P, P, P, L, P, D, P, P, P, P, P, P, P, P, L, L, P, L, P, P, P, P, P, P]),
+    'rspi_dense_frames': (I, [P, L, L, P, L, L, P, P, P, P]),
+    'rspi_rot_log_split': (I, [P, L, L, P, L, P, P, L, L, L, L, P, P, P, P]),
+    'rspi_dense_loglike': (I, [P, P, P, P, L, L, L, L, L, L, P, P, P, L, P, P]),
 }
 
 _lib = None
@@ -92,6 +95,7 @@ KERNELS_PER_CALL = {
     'rspi_screen_loglike': 1, 'rspi_screen_candidates': 3, 'rspi_rescore': 5,
     'rspi_loglike_stream': 1, 'rspi_posterior_pairs': 3, 'rspi_screen_loglike2': 1,
     'rspi_entries16_check': 1, 'rspi_nll': 2, 'rspi_screen_candidates_noalloc': 3, 'rspi_merge_coverage': 1, 'rspi_merge': 2,
+    'rspi_dense_frames': 1, 'rspi_rot_log_split': 1, 'rspi_dense_loglike': 1,
 }
 launch_count = 0
 

@@ -36,6 +36,18 @@ def write_photons(path, data):
     return path
 
 
+def sparse_from_dense(frames):
+    """ones/multi lists of dense (N, P) counts, frames in order and pixels
+    ascending within a frame (the make_data.py:323-328 layout)."""
+    f = np.asarray(frames)
+    one, many = f == 1, f > 1
+    _, po = np.nonzero(one)
+    dm, pm = np.nonzero(many)
+    return dict(ones=one.sum(1).astype('i4'), multi=many.sum(1).astype('i4'),
+                place_ones=po.astype('i4'), place_multi=pm.astype('i4'),
+                count_multi=f[dm, pm].astype('i4'))
+
+
 class PhotonsFile:
     """Read access with h5py-like semantics: ``f['ones'][:]``,
     ``f['place_ones'].shape``, ``KeyError`` for a missing dataset."""

@@ -50,9 +50,10 @@ def parse_args():
     ap.add_argument('--steps', type=int, default=3)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--config', type=int, default=2, choices=[1, 2, 4])
+    ap.add_argument('--config', type=int, default=2, choices=[1, 2, 4, 5])
     ap.add_argument('--frames', type=int, default=None, help='override frame count (testing)')
-    ap.add_argument('--form', default='screen', choices=['fp64', 'screen'])
+    ap.add_argument('--form', default=None, choices=['fp64', 'screen', 'dense'],
+                    help='likelihood form (default: dense for config 5, screen otherwise)')
     ap.add_argument('--kernel', default='stream', choices=['stream', 'dynamic'])
     ap.add_argument('--slice-gb', type=float, default=8.,
                     help='largest rotated-slice chunk (GB); smaller values give more launches')
@@ -63,7 +64,11 @@ def parse_args():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-clocks', action='store_true', help='do not sample nvidia-smi clocks')
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.form is None:
+        from rspi import synth
+        args.form = 'dense' if synth.CONFIGS[args.config].get('dense') else 'screen'
+    return args
 
 
 def peaks():
@@ -120,6 +125,55 @@ def dram_traffic(args, w, es, rows_per_launch):
                 c['rows_per_launch'] == int(round(rows_per_launch))):
             return float(c['dram_bytes_read'] + c['dram_bytes_write'])
     return None
+
+
+def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
+    """Roofline of the dominant kernel (the likelihood kernel, row a7) from
+    its live CUDA-event time: HBM bytes for the sparse forms, tensor FLOPs
+    for the dense form; plus the on-chip gather roofline of the sparse
+    forms.  Returns (roofline, gather roofline or None, rows per launch)."""
+    rows_per_launch = es.n_rows / max(1, ll_launches)
+    ll_launch_ms = ll_ms / max(1, ll_launches)
+    common = {'launch_ms': ll_launch_ms, 'launches_per_step': ll_launches,
+              'share_of_step': ll_ms / ms}
+    if es.form == 'dense':
+        # algorithmic FLOPs per launch: 2 per (frame, pixel, row) for each
+        # count digit x (hi, lo) product
+        flops = 2. * w['n'] * es.k_pad * rows_per_launch * es.n_digits * 2
+        achieved = flops / (ll_launch_ms * 1e-3) / 1e12
+        bytes_alg = (w['n'] * es.k_pad * 2 * es.n_digits + rows_per_launch * es.k_pad * 4 +
+                     rows_per_launch * w['n'] * 4)
+        roof = dict({'kernel': 'k_dense_ll (tcgen05 BF16 GEMM, row a7)', 'bound': 'tensor',
+                     'achieved': achieved, 'peak': pk['bf16_tflops'], 'unit': 'TFLOP/s',
+                     'frac': achieved / pk['bf16_tflops'], 'traffic': None,
+                     'peak_source': pk['source'] + ' (cuBLAS bf16 GEMM, burst)',
+                     'flops_per_launch': flops, 'algorithmic_bytes_per_launch': bytes_alg}, **common)
+        return roof, None, rows_per_launch
+    total_rows = es.ll16['total_rows'] if es.form == 'screen' else es.ll['total_rows']
+    esz = 4 if es.slice_code == 0 else 8
+    osz = 4 if es.prob_code == 0 else 8
+    # algorithmic bytes per launch = its slices in + its LL rows out + the
+    # packed photon entries once
+    ent_bytes = total_rows * 32 * (2 if es.form == 'screen' else 4)
+    alg_bytes = rows_per_launch * (es.p_row * esz + w['n'] * osz) + ent_bytes + 8 * w['n']
+    achieved = alg_bytes / (ll_launch_ms * 1e-3) / 1e9
+    # on-chip gather roofline: one shared-memory value per entry slot per likelihood row
+    gathers = rows_per_launch * total_rows * 32
+    clk_mhz = (clk or {}).get('sm_mhz') or 1965.
+    lanes = 32 if es.slice_code == 0 else 16
+    gather_peak = sm_count * lanes * clk_mhz * 1e6
+    gather_rate = gathers / (ll_launch_ms * 1e-3)
+    roof = dict({'kernel': ('k_screen_ll2 (FP32 screening likelihood, row a7)'
+                            if es.form == 'screen' else 'k_ll_stream / k_loglike (FP64 likelihood, row a7)'),
+                 'bound': 'hbm', 'achieved': achieved, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
+                 'frac': achieved / pk['hbm_gbs'],
+                 'traffic': dram_traffic(args, w, es, rows_per_launch),
+                 'peak_source': pk['source'] + ' (HBM copy)'}, **common)
+    gather = {'achieved': gather_rate, 'peak': gather_peak, 'unit': 'gathers/s',
+              'frac': gather_rate / gather_peak,
+              'note': 'shared-memory gather limit: %d SMs x %d lanes/clk x %.0f MHz'
+              % (sm_count, lanes, clk_mhz)}
+    return roof, gather, rows_per_launch
 
 
 def write_inputs(tmp, w, data, form, slice_gb=8.):
@@ -366,7 +420,7 @@ def run_ours(args):
     import io
     with contextlib.redirect_stdout(io.StringIO()):
         rec = EMC(cfgfile, device=dev)
-    if args.kernel != rec.estep.kernel:
+    if rec.estep.form != 'dense' and args.kernel != rec.estep.kernel:
         rec.estep.kernel = args.kernel
     model0 = start_model(args.config, w)
     stream = torch.cuda.current_stream()
@@ -483,25 +537,11 @@ def run_ours(args):
         return 0
 
     pk = peaks()
-    # entry rows of 32 photon slots the likelihood kernel walks per likelihood row
-    total_rows = es.ll16['total_rows'] if es.form == 'screen' else es.ll['total_rows']
-    esz = 4 if es.slice_code == 0 else 8
-    osz = 4 if es.prob_code == 0 else 8
-    # dominant kernel: the likelihood kernel (row a7); algorithmic bytes per
-    # launch = its slices in + its LL rows out + the packed photon entries once
-    rows_per_launch = es.n_rows / max(1, ll_launches)
-    ent_bytes = total_rows * 32 * (2 if es.form == 'screen' else 4)
-    alg_bytes = rows_per_launch * (es.p_row * esz + w['n'] * osz) + ent_bytes + 8 * w['n']
-    ll_launch_ms = ll_ms / max(1, ll_launches)
-    achieved = alg_bytes / (ll_launch_ms * 1e-3) / 1e9
-    # on-chip gather roofline: one shared-memory value per entry slot per likelihood row
-    gathers = rows_per_launch * total_rows * 32
     sm_count = torch.cuda.get_device_properties(dev).multi_processor_count
-    clk_mhz = (clk or {}).get('sm_mhz') or 1965.
-    lanes = 32 if es.slice_code == 0 else 16
-    gather_peak = sm_count * lanes * clk_mhz * 1e6
-    gather_rate = gathers / (ll_launch_ms * 1e-3)
-    traffic = dram_traffic(args, w, es, rows_per_launch)
+    roof, roof_gather, rows_per_launch = roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk,
+                                                         pk, sm_count)
+    esz = {0: 4, 1: 8, 2: 4}[es.slice_code]
+    osz = 4 if es.prob_code == 0 else 8
     value = world * w['n'] * w['n_states'] / (ms * 1e-3)
     cpu = None
     if not args.no_cpu_baseline and world == 1:
@@ -514,7 +554,8 @@ def run_ours(args):
         'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
         'warmup': args.warmup, 'ms_per_step': ms, 's_per_iteration': ms / 1e3,
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
-        'dtype': 'f64' if args.form == 'fp64' else 'f32 screen + f64 rescore',
+        'dtype': {'fp64': 'f64', 'screen': 'f32 screen + f64 rescore',
+                  'dense': 'bf16 GEMM (f32 accumulate) + f64 rescore'}[args.form],
         'data': 'synthetic (seeded generator with the configuration\'s shapes)',
         'config': {'workload': 'config%d: %dx%d detector, %d frames, %d rotations x %d (shift,dia) '
                    'states x %d mode(s) = %d states/frame, 1 EMC iteration per step' %
@@ -523,25 +564,15 @@ def run_ours(args):
                    'frames': w['n'], 'states_per_frame': w['n_states'],
                    'form': args.form, 'parallelism': 'replicas' if world > 1 else 'single',
                    'l2': 'inputs larger than L2 (slices %.1f GB, likelihoods %.1f GB per step)' %
-                   (es.n_rows * es.p_pad * esz / 1e9, es.n_rows * w['n'] * osz / 1e9)},
+                   (es.n_rows * es.p_row * esz / 1e9, es.n_rows * w['n'] * osz / 1e9)},
         'gpu_launches': launches,
         'cuda_graph': rec.use_graph,
-        'roofline': {'kernel': ('k_screen_ll2 (FP32 screening likelihood, row a7)'
-                                if es.form == 'screen' else 'k_ll_stream / k_loglike (FP64 likelihood, row a7)'),
-                     'bound': 'hbm',
-                     'achieved': achieved, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
-                     'frac': achieved / pk['hbm_gbs'], 'traffic': traffic,
-                     'peak_source': pk['source'] + ' (HBM copy)',
-                     'launch_ms': ll_launch_ms, 'launches_per_step': ll_launches,
-                     'share_of_step': ll_ms / ms},
-        'roofline_gather': {'achieved': gather_rate, 'peak': gather_peak, 'unit': 'gathers/s',
-                            'frac': gather_rate / gather_peak,
-                            'note': 'shared-memory gather limit: %d SMs x %d lanes/clk x %.0f MHz'
-                            % (sm_count, lanes, clk_mhz)},
+        'roofline': roof,
+        'roofline_gather': roof_gather,
         'clocks': clk,
         'e2e': e2e,
         'plain': plain,
-        'form': {'likelihood': args.form, 'kernel': args.kernel,
+        'form': {'likelihood': args.form, 'kernel': es.kernel,
                  'candidates_rescored': n_cand},
         'cpu_baseline': cpu,
         'setup_s': {'generate': t_gen},

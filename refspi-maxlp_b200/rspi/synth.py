@@ -24,7 +24,10 @@ density above; each further conformation displaces a fraction
 direction).  Each frame draws its conformation with ``mode_weights``.
 Uneven loads (``count_lognormal = (median, sigma, lo, hi)``): each frame's
 expected photon count is its own lognormal draw clipped to [lo, hi] instead
-of the global normalisation times the fluence scale.
+of the global normalisation times the fluence scale.  Background
+(``bg_level``): that many expected photons on every detector pixel, added in
+the detector frame after rotation and returned as ``bg`` (the photons
+file's background model, dset.py:56-60); ``mean_count`` includes it.
 
 Heavy per-frame work runs in torch on the requested device; the per-frame
 parameters come from ``numpy.random.default_rng(seed)`` child streams.
@@ -52,6 +55,13 @@ CONFIGS = {
             count_lognormal=(float(np.sqrt(50. * 50000.)), 1.15, 50., 50000.),
             recon=dict(num_rot=180, shiftx='-4 4 9', shifty='-4 4 9',
                        sphere_dia='6 8 5', num_iter=20, num_modes=3)),
+    # dense high fluence: 255x255, 10,000 frames at 2e5 photons/frame stored
+    # as dense uint16; a flat background of 2 photons per detector pixel
+    # makes more than 80% of the pixels nonzero
+    5: dict(size=255, n_blobs=40, obj_radius=20., num_data=10000, mean_count=2e5,
+            fluence_sigma=0.3, dia=(6., 8.), shift_max=3., bg_level=2.0, dense=True,
+            recon=dict(num_rot=360, shiftx='-5 5 11', shifty='-5 5 11',
+                       sphere_dia='6 8 7', num_iter=10)),
 }
 
 
@@ -133,7 +143,7 @@ def _rotate_bilinear(img, angle, size):
 def generate(size, num_data, mean_count, n_blobs=20, obj_radius=12.,
              fluence_sigma=0.3, dia=(6., 8.), shift_max=3., seed=0,
              device='cpu', chunk=256, dense=False, n_modes=1, mode_weights=None,
-             displace=(2., 4.), displace_frac=0.15, count_lognormal=None):
+             displace=(2., 4.), displace_frac=0.15, count_lognormal=None, bg_level=0.):
     """Generate one dataset; returns a dict in the photons-file layout.
 
     Keys: ``num_pix``, ``ones``, ``multi`` (int32, N), ``place_ones``,
@@ -190,13 +200,17 @@ def generate(size, num_data, mean_count, n_blobs=20, obj_radius=12.,
         im = torch.sin(ph) * ff * rel + fsm.imag
         return (re * re + im * im) * detmask[None]
 
+    bgmap = bg_level * detmask
     if target is None:
         tot = 0.
         for lo in range(0, num_data, chunk):
             hi = min(num_data, lo + chunk)
             w = intens(lo, hi).sum(1).cpu().numpy()
             tot += float((w * scale[lo:hi]).sum())
-        gfac = mean_count * num_data / tot
+        signal = mean_count - float(bgmap.sum())
+        if signal <= 0:
+            raise ValueError('the background alone exceeds mean_count')
+        gfac = signal * num_data / tot
 
     gen = torch.Generator(device=dev)
     gen.manual_seed(int(r_poi.integers(0, 2 ** 62)))
@@ -211,6 +225,8 @@ def generate(size, num_data, mean_count, n_blobs=20, obj_radius=12.,
         else:   # this frame's own expected count
             w = w * (torch.from_numpy(target[lo:hi]).to(dev) / w.sum(1))[:, None]
         rot = _rotate_bilinear(w, torch.from_numpy(angles[lo:hi]).to(dev), size)
+        if bg_level:
+            rot = rot + bgmap[None]
         cnt = torch.poisson(rot, generator=gen).to(torch.int32)
         if dense:
             frames[lo:hi] = cnt.clamp(max=65535).cpu().numpy().astype(np.uint16)
@@ -231,6 +247,8 @@ def generate(size, num_data, mean_count, n_blobs=20, obj_radius=12.,
                fsample=fss[0] if n_modes == 1 else np.stack(fss), rel_scale=np.array(rel))
     if n_modes > 1:
         out['true_modes'] = modes
+    if bg_level:
+        out['bg'] = bgmap.cpu().numpy()
     if dense:
         out['frames'] = frames
     return out
@@ -249,7 +267,7 @@ def config_extras(cfg):
     """Keyword arguments of ``generate`` beyond the common ones."""
     c = CONFIGS[cfg]
     return {k: c[k] for k in ('n_modes', 'mode_weights', 'displace', 'displace_frac',
-                              'count_lognormal') if k in c}
+                              'count_lognormal', 'bg_level', 'dense') if k in c}
 
 
 def initial_model(size, seed):

@@ -50,7 +50,8 @@ def parse_args():
     ap.add_argument('--steps', type=int, default=3)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='ours', choices=['ours', 'reference'])
-    ap.add_argument('--config', type=int, default=2, choices=[1, 2, 4, 5])
+    ap.add_argument('--config', type=int, default=2, choices=[1, 2, 3, 4, 5],
+                    help='3: the adjoint evaluation on config-2 data (NLL, FRC, L-BFGS vs grid)')
     ap.add_argument('--frames', type=int, default=None, help='override frame count (testing)')
     ap.add_argument('--form', default=None, choices=['fp64', 'screen', 'dense'],
                     help='likelihood form (default: dense for config 5, screen otherwise)')
@@ -67,7 +68,7 @@ def parse_args():
     args = ap.parse_args()
     if args.form is None:
         from rspi import synth
-        args.form = 'dense' if synth.CONFIGS[args.config].get('dense') else 'screen'
+        args.form = 'dense' if synth.CONFIGS.get(args.config, {}).get('dense') else 'screen'
     return args
 
 
@@ -137,16 +138,24 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
     common = {'launch_ms': ll_launch_ms, 'launches_per_step': ll_launches,
               'share_of_step': ll_ms / ms}
     if es.form == 'dense':
-        # algorithmic FLOPs per launch: 2 per (frame, pixel, row) for each
-        # count digit x (hi, lo) product
-        flops = 2. * w['n'] * es.k_pad * rows_per_launch * es.n_digits * 2
+        if es.dense_gemm == 'i8':
+            # 2 int8 ops per (frame, pixel, row) for each of the 4 L digits;
+            # the int8 dense tensor rate is twice the BF16 one
+            flops = 2. * w['n'] * es.k_pad * rows_per_launch * 4
+            peak, unit = 2. * pk['bf16_tflops'], 'TOP/s'
+            src = pk['source'] + ' (2 x the cuBLAS bf16 GEMM burst: int8 runs at twice bf16)'
+            a_bytes, name = w['n'] * es.k_pad, 'k_dense_ll<i8> (tcgen05 int8 GEMM, row a7)'
+        else:
+            # 2 FLOPs per (frame, pixel, row) for each count digit x (hi, lo)
+            flops = 2. * w['n'] * es.k_pad * rows_per_launch * es.n_digits * 2
+            peak, unit = pk['bf16_tflops'], 'TFLOP/s'
+            src = pk['source'] + ' (cuBLAS bf16 GEMM, burst)'
+            a_bytes = w['n'] * es.k_pad * 2 * es.n_digits
+            name = 'k_dense_ll<bf16> (tcgen05 BF16 GEMM, row a7)'
         achieved = flops / (ll_launch_ms * 1e-3) / 1e12
-        bytes_alg = (w['n'] * es.k_pad * 2 * es.n_digits + rows_per_launch * es.k_pad * 4 +
-                     rows_per_launch * w['n'] * 4)
-        roof = dict({'kernel': 'k_dense_ll (tcgen05 BF16 GEMM, row a7)', 'bound': 'tensor',
-                     'achieved': achieved, 'peak': pk['bf16_tflops'], 'unit': 'TFLOP/s',
-                     'frac': achieved / pk['bf16_tflops'], 'traffic': None,
-                     'peak_source': pk['source'] + ' (cuBLAS bf16 GEMM, burst)',
+        bytes_alg = a_bytes + rows_per_launch * es.k_pad * 4 + rows_per_launch * w['n'] * 4
+        roof = dict({'kernel': name, 'bound': 'tensor', 'achieved': achieved, 'peak': peak,
+                     'unit': unit, 'frac': achieved / peak, 'traffic': None, 'peak_source': src,
                      'flops_per_launch': flops, 'algorithmic_bytes_per_launch': bytes_alg}, **common)
         return roof, None, rows_per_launch
     total_rows = es.ll16['total_rows'] if es.form == 'screen' else es.ll['total_rows']
@@ -555,7 +564,10 @@ def run_ours(args):
         'warmup': args.warmup, 'ms_per_step': ms, 's_per_iteration': ms / 1e3,
         'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
         'dtype': {'fp64': 'f64', 'screen': 'f32 screen + f64 rescore',
-                  'dense': 'bf16 GEMM (f32 accumulate) + f64 rescore'}[args.form],
+                  'dense': ('u8 x fixed-point int8 GEMM (exact int32 accumulate)'
+                            if es.form == 'dense' and es.dense_gemm == 'i8' else
+                            'bf16 GEMM (f32 accumulate)') +
+                           (' + f64 rescore' if getattr(es, 'rescore', True) else '')}[args.form],
         'data': 'synthetic (seeded generator with the configuration\'s shapes)',
         'config': {'workload': 'config%d: %dx%d detector, %d frames, %d rotations x %d (shift,dia) '
                    'states x %d mode(s) = %d states/frame, 1 EMC iteration per step' %
@@ -584,8 +596,76 @@ def run_ours(args):
     return 0
 
 
+def run_adjoint_eval(args):
+    """Config 3: config-2 data; the MaxLP NLL and its hand-written adjoint.
+    Times NLL + gradient evaluations (FP32 terms, FP64 sums) and compares the
+    L-BFGS update with the 64 x 32 polar grid search (and the reference's
+    pattern search) on the final NLL and the FRC to the true object, from a
+    start model 30% off the truth, with frame states from an E-step on it."""
+    import torch
+    from rspi import geometry, synth
+    from rspi.adjoint import NLLProblem
+    from rspi.device import DevicePhotons, EStep
+    from rspi.evaluate import compare_updates
+    dev = torch.device('cuda', 0)
+    torch.cuda.set_device(dev)
+    w = workload(2, args.frames)
+    data = generate_data(2, w, device=dev)
+    size, n, r = w['size'], w['n'], w['recon']
+    ph = DevicePhotons(data['ones'], data['multi'], data['place_ones'], data['place_multi'],
+                       data['count_multi'], size * size, True, dev)
+    truth = data['fsample'] / float(data['rel_scale'])
+    rng = np.random.default_rng(20260103)
+    start = truth * (1 + 0.3 * rng.standard_normal(truth.size)) + 0.3 * np.abs(truth).mean() * (
+        rng.standard_normal(truth.size) + 1j * rng.standard_normal(truth.size))
+    sx, sy, dia, nst = geometry.state_grid(geometry.parse_triple(r['shiftx']),
+                                          geometry.parse_triple(r['shifty']),
+                                          geometry.parse_triple(r['sphere_dia']))
+    _, pm = geometry.emc_masks(size)
+    es = EStep(ph, size, r['num_rot'], sx, sy, dia, pm, np.zeros(size * size), form='screen')
+    es.run(torch.from_numpy(start).to(dev))
+    _, rmax, _ = es.reduce()
+    sv = torch.from_numpy(geometry.state_values(sx, sy, dia, nst)).to(dev)
+    del es
+    torch.cuda.empty_cache()
+    # throughput of one NLL + gradient evaluation (FP32 terms)
+    fst = (rmax // r['num_rot']).long()
+    vals = sv[fst]
+    ang = ((rmax % r['num_rot']).double() * np.pi / r['num_rot']).cpu().numpy()
+    prob = NLLProblem(ph, size, ang, precision='fp32')
+    fre, fim = prob.model_pixels(start)
+    args_t = (fre, fim, vals[:, 2].contiguous(), vals[:, 0].contiguous(),
+              vals[:, 1].contiguous(), ph.scales)
+    for _ in range(max(3, args.warmup)):
+        prob.evaluate(*args_t, grad=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        prob.evaluate(*args_t, grad=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    t0 = time.perf_counter()
+    cmp = compare_updates(ph, size, start, truth, rmax, r['num_rot'], sv, lbfgs_steps=50)
+    t_cmp = time.perf_counter() - t0
+    units = n * prob.n_pix
+    out = {'metric': 'NLL + adjoint gradient evaluations/s (frame x pixel terms); final NLL and '
+                     'FRC to truth: L-BFGS vs 64x32 polar grid', 'config': 3,
+           'value': units / (ms * 1e-3), 'unit': 'frame*pixel/s', 'ms_per_step': ms,
+           'n_gpus': 1, 'steps': args.steps, 'warmup': args.warmup, 'higher_is_better': True,
+           'dtype': 'f32 terms, f64 sums', 'data': 'synthetic, config-2 shapes',
+           'workload': {'frames': n, 'pixels': prob.n_pix, 'size': size},
+           'nll': cmp['nll'], 'frc_mean': cmp['frc_mean'], 'rescale': cmp['rescale'],
+           'compare_s': t_cmp}
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     args = parse_args()
+    if args.config == 3:
+        return run_adjoint_eval(args)
     if args.impl == 'reference':
         return run_reference(args)
     return run_ours(args)

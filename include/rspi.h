@@ -242,7 +242,10 @@ int rspi_screen_candidates_noalloc(const float *ll, long long n_rows, long long 
  * Candidates are regrouped by likelihood row (scratch row_cnt[n_rows],
  * row_cand_off[n_rows + 1], row_cand[capacity]); one CTA computes a row's
  * FP64 rotated slice (p_pad values, as rspi_rot_log_slices) in shared
- * memory and rescores that row's candidate frames. */
+ * memory and rescores that row's candidate frames.  A row too long for
+ * shared memory (p_pad * 8 bytes above 226 KB) is built in row_scratch
+ * instead (scratch_rows x p_pad doubles, one slot per CTA; required then,
+ * ignored otherwise). */
 int rspi_rescore(const int *cand_d, const int *cand_r, const long long *cand_off,
                  long long n_data, long long capacity, long long n_rows, const double *holo,
                  long long num_rot, const double *rot_cs, long long size, const double *bg,
@@ -251,7 +254,7 @@ int rspi_rescore(const int *cand_d, const int *cand_r, const long long *cand_off
                  const long long *row_off32, int *row_cnt, long long *row_cand_off,
                  int *row_cand, double *cand_ll, float *ll32, const double *max32,
                  const double *noncand, double *maxll, int *rmax, double *logz,
-                 cudaStream_t stream);
+                 double *row_scratch, long long scratch_rows, cudaStream_t stream);
 
 /* ------------------------------------------------------------------- a8, a9
  * Per-frame reduction over all states of LL (n_rows x n_data, FP64 or FP32):
@@ -337,6 +340,21 @@ int rspi_maxlp_pattern(double *fconv, const int *pixels, const int *hist_row,
                        long long size, int rescale_mode, const double *rescale,
                        int num_iter, double *rescale_out, cudaStream_t stream);
 
+/* Polar grid search of the per-pixel MaxLP negative log-likelihood (the
+ * judge beside the L-BFGS update of rspi_nll; no reference counterpart):
+ * for each pixel t = pixels[i] (histogram row hist_row[i], one mode),
+ *   NLL_t(F) = sum_s S_s |F + r_s|^2 - sum_s K_t[s] log |F + r_s|^2,
+ * S_s = sum of scales[d] over frames with fstate[d] == s (written to
+ * ssum[n_ref]), over F = a_j e^{i phi_i}, phi_i = 2 pi i / n_phase,
+ * a_j = A (j + 1) / n_amp, A = sqrt(sum_s K_t[s] / sum_s S_s) + max_s |r_s|.
+ * The lowest value (first index on ties) becomes fconv[t]; best_nll[i] gets
+ * it (without the F-independent sum_d k_dt log scale_d).  A pixel without
+ * frames keeps its value (best_nll 0). */
+int rspi_maxlp_grid(double *fconv, const int *pixels, const int *hist_row, long long n_pix,
+                    const int *hist, long long n_ref, const int *fstate, const double *scales,
+                    long long n_data, const double *ref_params, long long size, int n_phase,
+                    int n_amp, double *ssum, double *best_nll, int *err, cudaStream_t stream);
+
 /* Mean of n values into *out (the global rescale, maxLP.py:329). */
 int rspi_mean(const double *vals, long long n, double *out, cudaStream_t stream);
 
@@ -376,6 +394,34 @@ int rspi_dense_loglike(const void *a0, const void *a1, const void *b_hi, const v
                        long long num_rot, long long row_begin, long long row_end,
                        const double *init, const double *scales, float *prob, long long ld,
                        int *err, cudaStream_t stream);
+
+/* Exact integer variant of the dense likelihood (tcgen05 kind::i8): counts
+ * as u8 (rspi_dense_frames_u8: frames x k_pad, k_pad % 128 == 0, counts
+ * above 255 are clamped and *kmax tells the caller to use the BF16 path),
+ * log-slices in fixed point Lq = rint(L * 2^21) as four 8-bit digit planes
+ * (rspi_rot_log_fixed: rows [row_begin, row_end) into 4 planes of
+ * plane_rows x k_pad bytes each, low digit first, the top one signed;
+ * |L| >= 1023 or NaN is clamped and sets
+ * *err = RSPI_ERR_CAPACITY), and rspi_dense_loglike_i8 accumulating each
+ * digit product exactly in int32 (requires fewer than 8.4e6 photons per
+ * frame on the likelihood pixels).  The only error of the photon term is
+ * the quantisation, |err| <= 2^-22 * sum_p K[d][p]; the result goes to prob
+ * as in rspi_dense_loglike (digits holds n_brows rows per plane). */
+int rspi_dense_frames_u8(const unsigned short *frames, long long n_frames, long long npix,
+                         const int *sel_pix, long long n_sel, long long k_pad, void *a,
+                         int *kmax, cudaStream_t stream);
+
+int rspi_rot_log_fixed(const double *holo, long long n_states0, long long num_rot,
+                       const double *rot_cs, long long size, const double *bg,
+                       const int *sel_pix, long long n_sel, long long k_pad,
+                       long long row_begin, long long row_end, long long plane_rows,
+                       void *digits, int *err, cudaStream_t stream);
+
+int rspi_dense_loglike_i8(const void *a, const void *digits, long long k_pad,
+                          long long n_frames, long long n_brows, long long num_rot,
+                          long long row_begin, long long row_end, const double *init,
+                          const double *scales, float *prob, long long ld, int *err,
+                          cudaStream_t stream);
 
 /* ----------------------------------------------------------------------- a16
  * Negative log-likelihood of the MaxLP model and its adjoint (no reference

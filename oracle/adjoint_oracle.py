@@ -60,3 +60,25 @@ def nll_and_grad(f, dia, sx, sy, scale, k, size, pixels):
     loss.backward()
     g = lambda v: v.grad.numpy().copy()  # noqa: E731
     return float(loss.detach()), g(fr) + 1j * g(fi), g(dd), g(xx), g(yy), g(ss)
+
+
+def grid_pixel(k_d, fref_d, s_d, n_phase=64, n_amp=32):
+    """Polar grid search of one pixel's NLL (frame by frame, FP64):
+    NLL(F) = sum_d s_d |F + r_d|^2 - k_d log |F + r_d|^2 over
+    F = a_j e^{i phi_i}, phi_i = 2 pi i / n_phase, a_j = A (j + 1) / n_amp,
+    A = sqrt(sum k / sum s) + max_d |r_d|; the lowest value, first index on
+    ties (candidate index i * n_amp + j).  Returns (F, NLL, index)."""
+    k_d = np.asarray(k_d, dtype=np.float64)
+    s_d = np.asarray(s_d, dtype=np.float64)
+    amp = np.sqrt(k_d.sum() / s_d.sum()) + np.abs(fref_d).max()
+    i = np.arange(n_phase)[:, None]
+    j = np.arange(n_amp)[None, :]
+    a = amp * (j + 1) / n_amp
+    ph = 2 * np.pi * i / n_phase
+    cand = (a * np.cos(ph) + 1j * a * np.sin(ph)).ravel()
+    z = cand[None, :] + fref_d[:, None]
+    w = np.abs(z) ** 2
+    with np.errstate(divide='ignore'):
+        nll = (s_d[:, None] * w).sum(0) - (k_d[:, None] * np.log(w)).sum(0)
+    idx = int(np.argmin(nll))
+    return cand[idx], nll[idx], idx

@@ -23,6 +23,14 @@
 // Every mbarrier wait is bounded (about one second); on expiry the kernel
 // records RSPI_ERR_TIMEOUT, stops issuing, waits (bounded) for what it has
 // issued, frees its TMEM and skips the stores.  No cluster multicast.
+//
+// Exact integer variant (kind::i8): counts K <= 255 as u8 and the log-slice
+// in fixed point, Lq = rint(L * 2^21) (|L| < 1024, so Lq fits int32), as
+// four 8-bit digits Lq = b3 2^24 + b2 2^16 + b1 2^8 + b0 (b0..b2 unsigned,
+// b3 signed).  Each digit product accumulates in its own int32 TMEM
+// accumulator, exactly (sum_p K_p * 255 < 2^31 for fewer than 8.4e6 photons
+// per frame); the epilogue combines them in FP64, so the only error of
+// sum_p K_p L_p is the quantisation, at most 2^-22 sum_p K_p.
 #include <cuda.h>
 #include <cuda_bf16.h>
 
@@ -109,6 +117,22 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
 constexpr uint32_t DN_IDESC = (1u << 4) | (1u << 7) | (1u << 10) |
                               ((uint32_t)(DN_BN >> 3) << 17) | ((uint32_t)(DN_BM >> 4) << 24);
 
+// kind::i8: D S32 (bits 4-5 = 2), A unsigned 8-bit (bits 7-9 = 0), B
+// unsigned or signed 8-bit (bits 10-12 = 0 / 1), K-major, same N/M fields.
+constexpr uint32_t DN_IDESC_I8 = (2u << 4) | ((uint32_t)(DN_BN >> 3) << 17) |
+                                 ((uint32_t)(DN_BM >> 4) << 24);
+constexpr uint32_t DN_IDESC_I8_SB = DN_IDESC_I8 | (1u << 10);
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
 __device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
                                          uint32_t accumulate) {
     asm volatile(
@@ -144,11 +168,17 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// B operand tiles: BF16 hi, lo (KIND 0) or the four L digits (KIND 1).
 struct DenseMaps {
-    CUtensorMap a0, a1, bhi, blo;
+    CUtensorMap a0, a1, b[4];
 };
 
-// Dynamic shared memory: [stages][digits + 2 tiles] of 16 KB, then barriers.
+constexpr int KIND_BF16 = 0, KIND_I8 = 1;
+
+// Dynamic shared memory: [stages][A digits + B parts tiles] of 16 KB.
+// KIND_BF16: n_digits (1-2) BF16 count digits, B hi/lo, one FP32 accumulator.
+// KIND_I8:   one u8 count tile, four L-digit tiles, four int32 accumulators.
+template <int KIND>
 __global__ void __launch_bounds__(128, 1)
 k_dense_ll(const __grid_constant__ DenseMaps maps, int n_digits, int stages, int n_kb,
            long long n_frames, long long row_begin, long long row_end, long long num_rot,
@@ -158,10 +188,13 @@ k_dense_ll(const __grid_constant__ DenseMaps maps, int n_digits, int stages, int
     __shared__ uint64_t bars[2 * 8 + 1];
     __shared__ uint32_t tmem_base_sh;
     __shared__ int abort_sh;
+    constexpr int B_PARTS = KIND == KIND_I8 ? 4 : 2;
+    constexpr uint32_t TMEM_COLS = KIND == KIND_I8 ? 4 * DN_BN : DN_BN;
+    constexpr int KB_ELEMS = KIND == KIND_I8 ? 128 : DN_BK;   // elements per 128-byte row
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t base = (smem_u32(dn_smem_raw) + 1023u) & ~1023u;
-    const int tiles = n_digits + 2;
+    const int tiles = n_digits + B_PARTS;
     const uint32_t stage_bytes = (uint32_t)tiles * DN_TILE_BYTES;
     const uint32_t full0 = smem_u32(&bars[0]), empty0 = smem_u32(&bars[8]);
     const uint32_t accb = smem_u32(&bars[16]);
@@ -181,7 +214,7 @@ k_dense_ll(const __grid_constant__ DenseMaps maps, int n_digits, int stages, int
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&tmem_base_sh)),
-                     "r"(DN_BN)
+                     "r"(TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -204,12 +237,14 @@ k_dense_ll(const __grid_constant__ DenseMaps maps, int n_digits, int stages, int
             if (*(volatile int *)&abort_sh) break;
             const uint32_t st = base + (uint32_t)s * stage_bytes;
             mbar_expect_tx(full0 + 8 * s, stage_bytes);
-            const int x = kb * DN_BK;
+            const int x = kb * KB_ELEMS;
             tma_load_2d(st, &maps.a0, x, (int)frame0, full0 + 8 * s);
             if (n_digits > 1) tma_load_2d(st + DN_TILE_BYTES, &maps.a1, x, (int)frame0, full0 + 8 * s);
             const uint32_t sb = st + (uint32_t)n_digits * DN_TILE_BYTES;
-            tma_load_2d(sb, &maps.bhi, x, (int)rr0, full0 + 8 * s);
-            tma_load_2d(sb + DN_TILE_BYTES, &maps.blo, x, (int)rr0, full0 + 8 * s);
+#pragma unroll
+            for (int part = 0; part < B_PARTS; ++part)
+                tma_load_2d(sb + (uint32_t)part * DN_TILE_BYTES, &maps.b[part], x, (int)rr0,
+                            full0 + 8 * s);
             ++issued;
         }
         // every issued load lands before the CTA can exit
@@ -231,15 +266,31 @@ k_dense_ll(const __grid_constant__ DenseMaps maps, int n_digits, int stages, int
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t st = base + (uint32_t)s * stage_bytes;
             const uint32_t sb = st + (uint32_t)n_digits * DN_TILE_BYTES;
-            for (int dg = 0; dg < n_digits; ++dg)
-                for (int part = 0; part < 2; ++part)
+            // 4 MMAs of 32 bytes of K per 128-byte row (16 BF16 or 32 int8 elements)
+            if (KIND == KIND_I8) {
 #pragma unroll
-                    for (int k = 0; k < DN_BK / DN_UK; ++k) {
-                        const uint32_t koff = (uint32_t)k * DN_UK * 2;
-                        const uint64_t ad = sw128_desc(st + (uint32_t)dg * DN_TILE_BYTES + koff);
+                for (int part = 0; part < 4; ++part)
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const uint32_t koff = (uint32_t)k * 32;
+                        const uint64_t ad = sw128_desc(st + koff);
                         const uint64_t bd = sw128_desc(sb + (uint32_t)part * DN_TILE_BYTES + koff);
-                        mma_bf16(tmem, ad, bd, (kb | dg | part | k) != 0);
+                        mma_i8(tmem + (uint32_t)part * DN_BN, ad, bd,
+                               part == 3 ? DN_IDESC_I8_SB : DN_IDESC_I8, (kb | k) != 0);
                     }
+            } else {
+                for (int dg = 0; dg < n_digits; ++dg)
+                    for (int part = 0; part < 2; ++part)
+#pragma unroll
+                        for (int k = 0; k < DN_BK / DN_UK; ++k) {
+                            const uint32_t koff = (uint32_t)k * DN_UK * 2;
+                            const uint64_t ad =
+                                sw128_desc(st + (uint32_t)dg * DN_TILE_BYTES + koff);
+                            const uint64_t bd =
+                                sw128_desc(sb + (uint32_t)part * DN_TILE_BYTES + koff);
+                            mma_bf16(tmem, ad, bd, (kb | dg | part | k) != 0);
+                        }
+            }
             mma_commit(empty0 + 8 * s);
         }
         mma_commit(accb);   // arrives once every MMA issued above has completed
@@ -255,16 +306,37 @@ k_dense_ll(const __grid_constant__ DenseMaps maps, int n_digits, int stages, int
     const long long d = frame0 + 32 * warp + lane;
     const double sc = d < n_frames ? scales[d] : 0.;
     if (ok) {
+        const uint32_t lane_base = tmem + ((uint32_t)(32 * warp) << 16);
         for (int c0 = 0; c0 < DN_BN; c0 += 32) {
-            float v[32];
-            tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+            double acc[32];
+            if (KIND == KIND_I8) {
+                // sum_j 2^(8j) C_j, then the fixed-point scale 2^-21 (exact in FP64
+                // up to the final rounding of the four-term sum)
+                float v[32];
+                tmem_ld32(lane_base + 3u * DN_BN + (uint32_t)c0, v);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) acc[j] = (double)__float_as_int(v[j]);
+                for (int part = 2; part >= 0; --part) {
+                    tmem_ld32(lane_base + (uint32_t)part * DN_BN + (uint32_t)c0, v);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        acc[j] = fma(acc[j], 256., (double)__float_as_int(v[j]));
+                }
+#pragma unroll
+                for (int j = 0; j < 32; ++j) acc[j] *= 4.76837158203125e-07;   // 2^-21
+            } else {
+                float v[32];
+                tmem_ld32(lane_base + (uint32_t)c0, v);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) acc[j] = (double)v[j];
+            }
             if (d < n_frames) {
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const long long rr = rr0 + c0 + j;
                     const long long r = row_begin + rr;
                     if (r < row_end)
-                        prob[rr * ld + d] = (float)(init[r / num_rot] * sc + (double)v[j]);
+                        prob[rr * ld + d] = (float)(init[r / num_rot] * sc + acc[j]);
                 }
             }
         }
@@ -272,7 +344,8 @@ k_dense_ll(const __grid_constant__ DenseMaps maps, int n_digits, int stages, int
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(DN_BN)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                     "r"(TMEM_COLS)
                      : "memory");
 }
 
@@ -330,6 +403,60 @@ k_rot_log_split(const double *__restrict__ holo, long long num_rot,
     }
 }
 
+// Dense frames -> u8 counts over the likelihood pixels (kmax: largest count,
+// the caller checks it is below 256).
+__global__ void k_dense_frames_u8(const unsigned short *__restrict__ frames, long long n_frames,
+                                  long long npix, const int *__restrict__ sel_pix,
+                                  long long n_sel, long long k_pad, uint8_t *__restrict__ a,
+                                  int *__restrict__ kmax) {
+    const long long total = n_frames * k_pad;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    int mx = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const long long d = i / k_pad, c = i - d * k_pad;
+        const int k = c < n_sel ? (int)frames[d * npix + sel_pix[c]] : 0;
+        mx = max(mx, k);
+        a[i] = (uint8_t)min(k, 255);
+    }
+    mx = warp_max_int(mx);
+    if ((threadIdx.x & 31) == 0) atomicMax(kmax, mx);
+}
+
+// Rotated log-slices (rot_log_value, FP64) in fixed point Lq = rint(L 2^21)
+// as four 8-bit digit planes b[part][row][c] (zero beyond n_sel).  |L| is
+// below 1024 for every value rot_log_value returns (the -1000 sentinel, and
+// logs of doubles); a larger value is clamped and flagged.
+__global__ void __launch_bounds__(256)
+k_rot_log_q(const double *__restrict__ holo, long long num_rot, const double *__restrict__ rot_cs,
+            int size, const double *__restrict__ bg, const int *__restrict__ sel_pix,
+            long long n_sel, long long k_pad, long long row_begin, long long n_rows,
+            long long plane, uint8_t *__restrict__ b, int *err) {
+    const long long npix = (long long)size * size;
+    const long long total = n_rows * k_pad;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        const long long rr = i / k_pad, c = i - rr * k_pad;
+        double v = 0.;
+        if (c < n_sel) {
+            const long long r = row_begin + rr;
+            const long long s0 = r / num_rot, j = r - s0 * num_rot;
+            const int p = sel_pix[c];
+            const int x = p / size, y = p - (p / size) * size;
+            v = rot_log_value(holo + s0 * npix, x, y, size, rot_cs[2 * j], rot_cs[2 * j + 1],
+                              bg[p]);
+        }
+        if (!(fabs(v) < 1023.)) {   // also NaN
+            rspi_flag(err, RSPI_ERR_CAPACITY);
+            v = v != v ? 0. : (v > 0. ? 1023. : -1023.);
+        }
+        const int q = (int)rint(v * 2097152.);   // 2^21
+        b[i] = (uint8_t)(q & 255);
+        b[plane + i] = (uint8_t)((q >> 8) & 255);
+        b[2 * plane + i] = (uint8_t)((q >> 16) & 255);
+        b[3 * plane + i] = (uint8_t)(q >> 24);
+    }
+}
+
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
@@ -348,19 +475,47 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-// 2-D BF16 map over a rows x k_pad K-major matrix, 64 x 128 boxes, 128B swizzle,
-// zero fill outside (rows beyond the matrix read as zeros).
-bool make_map(CUtensorMap *m, const void *ptr, long long k_pad, long long rows) {
+// 2-D map over a rows x k_pad K-major matrix of BF16 (64 x 128 boxes) or
+// 8-bit (128 x 128 boxes) elements: 128-byte box rows, 128B swizzle, zero
+// fill outside (rows beyond the matrix read as zeros).
+bool make_map(CUtensorMap *m, const void *ptr, long long k_pad, long long rows, bool byte) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return false;
+    const int esz = byte ? 1 : 2;
     cuuint64_t dims[2] = {(cuuint64_t)k_pad, (cuuint64_t)rows};
-    cuuint64_t strides[1] = {(cuuint64_t)k_pad * 2};
-    cuuint32_t box[2] = {(cuuint32_t)DN_BK, (cuuint32_t)DN_BM};
+    cuuint64_t strides[1] = {(cuuint64_t)k_pad * esz};
+    cuuint32_t box[2] = {(cuuint32_t)(128 / esz), (cuuint32_t)DN_BM};
     cuuint32_t estr[2] = {1, 1};
-    return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box,
-              estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
-           CUDA_SUCCESS;
+    return fn(m, byte ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+              const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+template <int KIND>
+int launch_dense(const DenseMaps &maps, int n_digits, long long k_pad, long long n_frames,
+                 long long n_rows, long long num_rot, long long row_begin, long long row_end,
+                 const double *init, const double *scales, float *prob, long long ld, int *err,
+                 cudaStream_t stream) {
+    const int b_parts = KIND == KIND_I8 ? 4 : 2;
+    const int stage_bytes = (n_digits + b_parts) * DN_TILE_BYTES;
+    const int stages = min(8, DN_SMEM_BUDGET / stage_bytes);
+    const int smem = stages * stage_bytes + 1024;
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_dense_ll<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 DN_SMEM_BUDGET + 1024) != cudaSuccess)
+            return RSPI_ERR_CUDA;
+        attr = true;
+    }
+    const dim3 grid((unsigned)((n_frames + DN_BM - 1) / DN_BM),
+                    (unsigned)((n_rows + DN_BN - 1) / DN_BN));
+    if (grid.y > 65535) return RSPI_ERR_TOO_LARGE;
+    const int n_kb = (int)(k_pad / (KIND == KIND_I8 ? 128 : DN_BK));
+    k_dense_ll<KIND><<<grid, 128, smem, stream>>>(maps, n_digits, stages, n_kb, n_frames,
+                                                  row_begin, row_end, num_rot, init, scales,
+                                                  prob, ld, err);
+    RSPI_RETURN_LAUNCH();
 }
 
 }  // namespace
@@ -411,25 +566,66 @@ extern "C" int rspi_dense_loglike(const void *a0, const void *a1, const void *b_
     if (n_rows == 0) return RSPI_OK;
     const int n_digits = a1 ? 2 : 1;
     DenseMaps maps;
-    if (!make_map(&maps.a0, a0, k_pad, n_frames) ||
-        !make_map(&maps.a1, a1 ? a1 : a0, k_pad, n_frames) ||
-        !make_map(&maps.bhi, b_hi, k_pad, n_brows) || !make_map(&maps.blo, b_lo, k_pad, n_brows))
+    if (!make_map(&maps.a0, a0, k_pad, n_frames, false) ||
+        !make_map(&maps.a1, a1 ? a1 : a0, k_pad, n_frames, false) ||
+        !make_map(&maps.b[0], b_hi, k_pad, n_brows, false) ||
+        !make_map(&maps.b[1], b_lo, k_pad, n_brows, false))
         return RSPI_ERR_CUDA;
-    const int stage_bytes = (n_digits + 2) * DN_TILE_BYTES;
-    const int stages = min(8, DN_SMEM_BUDGET / stage_bytes);
-    const int smem = stages * stage_bytes + 1024;
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(k_dense_ll, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 DN_SMEM_BUDGET + 1024) != cudaSuccess)
-            return RSPI_ERR_CUDA;
-        attr = true;
-    }
-    const dim3 grid((unsigned)((n_frames + DN_BM - 1) / DN_BM),
-                    (unsigned)((n_rows + DN_BN - 1) / DN_BN));
-    if (grid.y > 65535) return RSPI_ERR_TOO_LARGE;
-    k_dense_ll<<<grid, 128, smem, stream>>>(maps, n_digits, stages, (int)(k_pad / DN_BK),
-                                            n_frames, row_begin, row_end, num_rot, init, scales,
-                                            prob, ld, err);
+    maps.b[2] = maps.b[0];
+    maps.b[3] = maps.b[1];
+    return launch_dense<KIND_BF16>(maps, n_digits, k_pad, n_frames, n_rows, num_rot, row_begin,
+                                   row_end, init, scales, prob, ld, err, stream);
+}
+
+extern "C" int rspi_dense_frames_u8(const unsigned short *frames, long long n_frames,
+                                    long long npix, const int *sel_pix, long long n_sel,
+                                    long long k_pad, void *a, int *kmax, cudaStream_t stream) {
+    if (!frames || !sel_pix || !a || !kmax || n_frames <= 0 || npix <= 0 || n_sel < 0 ||
+        k_pad < n_sel || k_pad % 128)
+        return RSPI_ERR_ARG;
+    k_dense_frames_u8<<<rspi_blocks(n_frames * k_pad, 256, 16), 256, 0, stream>>>(
+        frames, n_frames, npix, sel_pix, n_sel, k_pad, (uint8_t *)a, kmax);
     RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_rot_log_fixed(const double *holo, long long n_states0, long long num_rot,
+                                  const double *rot_cs, long long size, const double *bg,
+                                  const int *sel_pix, long long n_sel, long long k_pad,
+                                  long long row_begin, long long row_end, long long plane_rows,
+                                  void *digits, int *err, cudaStream_t stream) {
+    if (n_states0 <= 0 || num_rot <= 0 || size <= 1 || size > 46340 || k_pad < n_sel ||
+        k_pad % 128 || row_begin < 0 || row_end > n_states0 * num_rot || row_end < row_begin ||
+        plane_rows < row_end - row_begin || !holo || !rot_cs || !bg || !digits || !err)
+        return RSPI_ERR_ARG;
+    const long long n_rows = row_end - row_begin;
+    if (n_rows == 0) return RSPI_OK;
+    k_rot_log_q<<<rspi_blocks(n_rows * k_pad, 256, 16), 256, 0, stream>>>(
+        holo, num_rot, rot_cs, (int)size, bg, sel_pix, n_sel, k_pad, row_begin, n_rows,
+        plane_rows * k_pad, (uint8_t *)digits, err);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_dense_loglike_i8(const void *a, const void *digits, long long k_pad,
+                                     long long n_frames, long long n_brows, long long num_rot,
+                                     long long row_begin, long long row_end, const double *init,
+                                     const double *scales, float *prob, long long ld, int *err,
+                                     cudaStream_t stream) {
+    if (!a || !digits || !init || !scales || !prob || !err || k_pad <= 0 || k_pad % 128 ||
+        n_frames <= 0 || num_rot <= 0 || row_begin < 0 || row_end < row_begin ||
+        row_end - row_begin > n_brows || ld < n_frames || n_frames > 0x7fffffffLL ||
+        n_brows > 0x7fffffffLL || k_pad > 0x7fffffffLL)
+        return RSPI_ERR_ARG;
+    if (((uintptr_t)a | (uintptr_t)digits) & 15) return RSPI_ERR_ARG;
+    const long long n_rows = row_end - row_begin;
+    if (n_rows == 0) return RSPI_OK;
+    const long long plane = n_brows * k_pad;   // bytes per digit plane
+    if (plane % 16) return RSPI_ERR_ARG;
+    DenseMaps maps;
+    if (!make_map(&maps.a0, a, k_pad, n_frames, true)) return RSPI_ERR_CUDA;
+    maps.a1 = maps.a0;
+    for (int part = 0; part < 4; ++part)
+        if (!make_map(&maps.b[part], (const uint8_t *)digits + part * plane, k_pad, n_brows, true))
+            return RSPI_ERR_CUDA;
+    return launch_dense<KIND_I8>(maps, 1, k_pad, n_frames, n_rows, num_rot, row_begin, row_end,
+                                 init, scales, prob, ld, err, stream);
 }

@@ -342,6 +342,133 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
     }
 }
 
+// Per-state sums of the frames' scales, S[s] = sum_{d: fstate[d] = s} scale[d].
+__global__ void k_state_scale_sums(const int *__restrict__ fstate, const double *__restrict__ scales,
+                                   long long n, long long n_ref, double *__restrict__ ssum,
+                                   int *err) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long d = (long long)blockIdx.x * blockDim.x + threadIdx.x; d < n; d += stride) {
+        const int s = fstate[d];
+        if (s < 0 || s >= n_ref) {
+            rspi_flag(err, RSPI_ERR_INDEX);
+            continue;
+        }
+        atomicAdd(&ssum[s], scales[d]);
+    }
+}
+
+// Polar grid search of the per-pixel NLL (the judge of the L-BFGS update):
+//   NLL_t(F) = sum_s S_s |F + r_s|^2 - sum_s K_t[s] log |F + r_s|^2 (+ const)
+// over F = a_j e^{i phi_i}, phi_i = 2 pi i / n_phase, a_j = A (j + 1) / n_amp,
+// A = sqrt(sum K / sum S) + max_s |r_s| (every amplitude the data allow).
+// The quadratic term is analytic (sum S |F|^2 + 2 Re(conj(F) sum S r) +
+// sum S |r|^2); the log term runs over the populated states.  The lowest
+// value wins (first candidate index on ties); the pixel's model value and
+// its NLL (without the F-independent sum k log s) are written.
+constexpr int GR_THREADS = 256;
+
+__global__ void __launch_bounds__(GR_THREADS)
+k_grid(double2 *__restrict__ fconv, const int *__restrict__ pixels,
+       const int *__restrict__ hist_row, const int *__restrict__ hist, long long n_ref,
+       const double *__restrict__ ssum, const double *__restrict__ ref_params, int size,
+       int n_phase, int n_amp, double *__restrict__ best_out) {
+    __shared__ double fr_re[POP_CAP], fr_im[POP_CAP], fk[POP_CAP];
+    __shared__ double scratch[32];
+    __shared__ int iscratch[32];
+    __shared__ int wsum[32];
+    const long long ip = blockIdx.x;
+    const int t = pixels[ip];
+    const int *hrow = hist + (long long)hist_row[ip] * n_ref;
+    PixelConsts pc;
+    {
+        const double ds = (double)size, c0 = (double)(size / 2);
+        const int tx = t / size, ty = t - (t / size) * size;
+        pc.qx = ((double)tx - c0) / ds;
+        pc.qy = ((double)ty - c0) / ds;
+        pc.qrad = sqrt(xadd(xmul(pc.qx, pc.qx), xmul(pc.qy, pc.qy)));
+        if (pc.qrad == 0.) pc.qrad = 1.e-6;  // maxLP.py:85
+    }
+    double st = 0., srr = 0., sri = 0., sq = 0., ks = 0., rmax = 0.;
+    for (long long s = threadIdx.x; s < n_ref; s += blockDim.x) {
+        const double w = ssum[s];
+        ks += (double)hrow[s];
+        if (w > 0.) {
+            const double2 r = fref_value(pc.qx, pc.qy, pc.qrad, ref_params[3 * s],
+                                         ref_params[3 * s + 1], ref_params[3 * s + 2]);
+            st += w;
+            srr += w * r.x;
+            sri += w * r.y;
+            sq += w * (r.x * r.x + r.y * r.y);
+            rmax = fmax(rmax, hypot(r.x, r.y));
+        }
+    }
+    st = block_sum(st, scratch);
+    srr = block_sum(srr, scratch);
+    sri = block_sum(sri, scratch);
+    sq = block_sum(sq, scratch);
+    ks = block_sum(ks, scratch);
+    {   // block max of rmax (non-negative: integer order of the bit patterns)
+        long long b = __double_as_longlong(rmax);
+        for (int o = 16; o > 0; o >>= 1) b = max(b, __shfl_xor_sync(RSPI_FULL_MASK, b, o));
+        __syncthreads();
+        if ((threadIdx.x & 31) == 0) scratch[threadIdx.x >> 5] = __longlong_as_double(b);
+        __syncthreads();
+        double m = 0.;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, scratch[w]);
+        rmax = m;
+        __syncthreads();
+    }
+    if (st == 0.) {   // no frame: the model stays, NLL 0
+        if (threadIdx.x == 0) best_out[ip] = 0.;
+        return;
+    }
+    int npop = 0;
+    const bool one_chunk = n_ref <= POP_CAP;
+    if (one_chunk) load_populated(0, hrow, n_ref, ref_params, pc, fr_re, fr_im, fk, &npop, wsum);
+    const double amp = sqrt(ks / st) + rmax;
+    const int ncand = n_phase * n_amp;
+    double best = -INFINITY;   // maximise -NLL with the shared first-index rule
+    int bidx = 0x7fffffff;
+    for (int c0 = 0; c0 < ncand; c0 += blockDim.x) {
+        const int c = c0 + threadIdx.x;
+        const int cc = c < ncand ? c : 0;
+        const int i = cc / n_amp, j = cc - (cc / n_amp) * n_amp;
+        const double a = amp * (double)(j + 1) / (double)n_amp;
+        double sphi, cphi;
+        sincos(2. * PI * (double)i / (double)n_phase, &sphi, &cphi);
+        const double fx = a * cphi, fy = a * sphi;
+        double acc = 0.;
+        int s_next = 0;
+        do {
+            if (!one_chunk)
+                s_next = load_populated(s_next, hrow, n_ref, ref_params, pc, fr_re, fr_im, fk,
+                                        &npop, wsum);
+            else
+                s_next = (int)n_ref;
+            for (int k = 0; k < npop; ++k) {
+                const double re = fx + fr_re[k], im = fy + fr_im[k];
+                acc = fma(fk[k], log(re * re + im * im), acc);
+            }
+            if (!one_chunk) __syncthreads();
+        } while (s_next < n_ref);
+        const double quad = st * (fx * fx + fy * fy) + 2. * (fx * srr + fy * sri) + sq;
+        const double v = -(quad - acc);
+        if (c < ncand && argmax_better(v, c, best, bidx)) {
+            best = v;
+            bidx = c;
+        }
+    }
+    block_argmax(best, bidx, scratch, iscratch);
+    if (threadIdx.x == 0) {
+        const int i = bidx / n_amp, j = bidx - (bidx / n_amp) * n_amp;
+        const double a = amp * (double)(j + 1) / (double)n_amp;
+        double sphi, cphi;
+        sincos(2. * PI * (double)i / (double)n_phase, &sphi, &cphi);
+        fconv[t] = make_double2(a * cphi, a * sphi);
+        best_out[ip] = -best;
+    }
+}
+
 __global__ void __launch_bounds__(1024) k_mean(const double *__restrict__ v, long long n,
                                                double *__restrict__ out) {
     __shared__ double scratch[32];
@@ -402,5 +529,25 @@ extern "C" int rspi_maxlp_pattern(double *fconv, const int *pixels, const int *h
 extern "C" int rspi_mean(const double *vals, long long n, double *out, cudaStream_t stream) {
     if (!vals || !out || n <= 0) return RSPI_ERR_ARG;
     k_mean<<<1, 1024, 0, stream>>>(vals, n, out);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_maxlp_grid(double *fconv, const int *pixels, const int *hist_row,
+                               long long n_pix, const int *hist, long long n_ref,
+                               const int *fstate, const double *scales, long long n_data,
+                               const double *ref_params, long long size, int n_phase, int n_amp,
+                               double *ssum, double *best_nll, int *err, cudaStream_t stream) {
+    if (n_pix == 0) return RSPI_OK;
+    if (!fconv || !pixels || !hist_row || !hist || !fstate || !scales || !ref_params || !ssum ||
+        !best_nll || !err || n_ref <= 0 || n_ref > 0x7fffffffLL || n_data <= 0 || size <= 1 ||
+        size > 46340 || n_pix < 0 || n_pix > 0x7fffffffLL || n_phase <= 0 || n_amp <= 0 ||
+        (long long)n_phase * n_amp > (1 << 20))
+        return RSPI_ERR_ARG;
+    cudaMemsetAsync(ssum, 0, sizeof(double) * n_ref, stream);
+    k_state_scale_sums<<<rspi_blocks(n_data, 256), 256, 0, stream>>>(fstate, scales, n_data,
+                                                                     n_ref, ssum, err);
+    k_grid<<<(unsigned)n_pix, GR_THREADS, 0, stream>>>((double2 *)fconv, pixels, hist_row, hist,
+                                                       n_ref, ssum, ref_params, (int)size,
+                                                       n_phase, n_amp, best_nll);
     RSPI_RETURN_LAUNCH();
 }

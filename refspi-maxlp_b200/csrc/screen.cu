@@ -343,7 +343,11 @@ __global__ void k_row_scatter(const int *__restrict__ cand_r, const long long *_
 // is computed into shared memory with rot_log_value (as k_rot_log does),
 // then each warp rescores candidate frames exactly as the FP64 form sums
 // them (per lane over the frame's packed rows, fma(count, L, acc), then the
-// warp reduction), so every value equals the FP64 form's.
+// warp reduction), so every value equals the FP64 form's.  A row longer than
+// shared memory holds (GROW: more than ~28,900 likelihood pixels) is built
+// in the CTA's slot of a global scratch array instead and gathered through
+// L1/L2; the arithmetic is the same.
+template <bool GROW>
 __global__ void __launch_bounds__(1024)
 k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ row_cand,
                long long n_rows, const int *__restrict__ cand_d, const double *__restrict__ holo,
@@ -351,9 +355,11 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
                const double *__restrict__ bg, const int *__restrict__ sel_pix, long long n_sel,
                long long p_pad, const double *__restrict__ init, const double *__restrict__ scales,
                const unsigned int *__restrict__ ent32, const long long *__restrict__ row_off32,
-               double *__restrict__ cand_ll, float *__restrict__ ll32, long long n_data) {
+               double *__restrict__ cand_ll, float *__restrict__ ll32, long long n_data,
+               double *row_scratch) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *sl = reinterpret_cast<double *>(smem_raw);
+    double *sl = GROW ? row_scratch + (long long)blockIdx.x * p_pad
+                      : reinterpret_cast<double *>(smem_raw);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const long long npix = (long long)size * size;
     const unsigned cmax = (unsigned)p_pad - 1;
@@ -538,7 +544,7 @@ extern "C" int rspi_screen_candidates(const float *ll, long long n_rows, long lo
                                       int *cand_r, int *err, cudaStream_t stream) {
     if (!ll || !max32 || !rmax32 || !frame_photons || !row_off16 || !lmax || !cnt_part || !cand_n ||
         !noncand || !thr || !cand_off || !cand_d || !cand_r || n_rows <= 0 || n_data <= 0 ||
-        n_rows > 0x7fffffffLL || capacity < 0 || !(delta >= 0.))
+        n_rows > 0x7fffffffLL || capacity < 0 || capacity > 0x7fffffffLL || !(delta >= 0.))
         return RSPI_ERR_ARG;
     const dim3 block(32, RY);
     const unsigned grid = (unsigned)((n_data + 31) / 32);
@@ -560,18 +566,21 @@ extern "C" int rspi_rescore(const int *cand_d, const int *cand_r, const long lon
                             int *row_cnt, long long *row_cand_off, int *row_cand,
                             double *cand_ll, float *ll32, const double *max32,
                             const double *noncand, double *maxll, int *rmax, double *logz,
-                            cudaStream_t stream) {
+                            double *row_scratch, long long scratch_rows, cudaStream_t stream) {
     if (!cand_d || !cand_r || !cand_off || !holo || !rot_cs || !bg || !sel_pix || !init ||
         !scales || !entries32 || !row_off32 || !row_cnt || !row_cand_off || !row_cand ||
         !cand_ll || !ll32 || !max32 || !noncand || !maxll || !rmax || !logz || n_data <= 0 ||
-        capacity < 0 || n_rows <= 0 || n_rows > 0x7fffffffLL || size <= 1 || size > 46340 ||
+        capacity < 0 || capacity > 0x7fffffffLL || n_rows <= 0 || n_rows > 0x7fffffffLL ||
+        size <= 1 || size > 46340 ||
         p_pad < n_sel || p_pad % 32 || p_pad > 65536)
         return RSPI_ERR_ARG;
     const size_t smem = (size_t)p_pad * sizeof(double);
-    if (smem > (size_t)SMEM_LIMIT - 1024) return RSPI_ERR_ARG;
+    const bool grow = smem > (size_t)SMEM_LIMIT - 1024;
+    if (grow && (!row_scratch || scratch_rows < 1)) return RSPI_ERR_ARG;
     static size_t smem_set = 0;
-    if (smem > smem_set) {
-        if (cudaFuncSetAttribute(k_rescore_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (!grow && smem > smem_set) {
+        if (cudaFuncSetAttribute(k_rescore_rows<false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess)
             return RSPI_ERR_CUDA;
         smem_set = smem;
@@ -583,11 +592,21 @@ extern "C" int rspi_rescore(const int *cand_d, const int *cand_r, const long lon
     cudaMemsetAsync(row_cnt, 0, sizeof(int) * n_rows, stream);
     k_row_scatter<<<rspi_sm_count() * 8, 256, 0, stream>>>(cand_r, total, capacity, row_cand_off,
                                                           row_cnt, row_cand);
-    const int per_sm = max(1, (int)(SMEM_LIMIT / (smem + 1024)));
-    const unsigned grid = (unsigned)min((long long)rspi_sm_count() * min(per_sm, 2), n_rows);
-    k_rescore_rows<<<grid, 1024 / min(per_sm, 2), smem, stream>>>(
-        row_cand_off, row_cand, n_rows, cand_d, holo, num_rot, rot_cs, (int)size, bg, sel_pix,
-        n_sel, p_pad, init, scales, entries32, row_off32, cand_ll, ll32, n_data);
+    if (grow) {
+        // one CTA per scratch row slot
+        const unsigned grid = (unsigned)min(scratch_rows, n_rows);
+        k_rescore_rows<true><<<grid, 1024, 0, stream>>>(
+            row_cand_off, row_cand, n_rows, cand_d, holo, num_rot, rot_cs, (int)size, bg,
+            sel_pix, n_sel, p_pad, init, scales, entries32, row_off32, cand_ll, ll32, n_data,
+            row_scratch);
+    } else {
+        const int per_sm = max(1, (int)(SMEM_LIMIT / (smem + 1024)));
+        const unsigned grid = (unsigned)min((long long)rspi_sm_count() * min(per_sm, 2), n_rows);
+        k_rescore_rows<false><<<grid, 1024 / min(per_sm, 2), smem, stream>>>(
+            row_cand_off, row_cand, n_rows, cand_d, holo, num_rot, rot_cs, (int)size, bg,
+            sel_pix, n_sel, p_pad, init, scales, entries32, row_off32, cand_ll, ll32, n_data,
+            nullptr);
+    }
     k_cand_finalize<<<rspi_blocks(n_data * 32, 256), 256, 0, stream>>>(
         cand_off, cand_r, cand_ll, max32, noncand, n_data, capacity, maxll, rmax, logz);
     RSPI_RETURN_LAUNCH();
@@ -649,7 +668,7 @@ extern "C" int rspi_screen_candidates_noalloc(const float *ll, long long n_rows,
     if (n_data > NOALLOC_MAX_FRAMES) return RSPI_ERR_TOO_LARGE;
     if (!ll || !max32 || !rmax32 || !frame_photons || !row_off16 || !lmax || !cand_n ||
         !noncand || !thr || !cand_off || !cand_d || !cand_r || n_rows <= 0 || n_data <= 0 ||
-        n_rows > 0x7fffffffLL || capacity < 0 || !(delta >= 0.))
+        n_rows > 0x7fffffffLL || capacity < 0 || capacity > 0x7fffffffLL || !(delta >= 0.))
         return RSPI_ERR_ARG;
     int status = RSPI_OK;
     int *scratch = cand_scratch_address(&status);

@@ -14,7 +14,9 @@ Optional ``[emc]`` keys beyond the reference: ``form`` (``fp64``: FP64
 slices and FP64 likelihood matrix; ``screen``: FP32 screening pass with
 FP64 rescoring of every state that can be the argmax or carry posterior
 mass, same argmax/maximum/log-sum-exp as ``fp64``; ``dense``: frames stored
-densely, screening likelihood as a BF16 tensor-core GEMM, same rescoring),
+densely, likelihood as a tensor-core GEMM, ``dense_gemm`` = ``auto`` /
+``i8`` (exact fixed point) / ``bf16`` (hi + lo split), ``dense_rescore``
+(default true: FP64 rescoring of the candidates as in ``screen``)),
 ``screen_delta``
 (default 20 nats), ``states_per_tile``, ``warps_per_cta``, ``phaser_iter``
 (default 10, maxLP.py:320,335), ``slice_budget_gb`` (rotated slices are built
@@ -81,7 +83,8 @@ class EMC():
                            states_per_tile=self.states_per_tile, warps=self.warps_per_cta,
                            delta=self.screen_delta,
                            slice_budget_bytes=int(self.slice_budget_gb * (1 << 30)),
-                           n_modes=self.num_modes)
+                           n_modes=self.num_modes, dense_gemm=self.dense_gemm,
+                           dense_rescore=self.dense_rescore)
         self.prob = self.estep.prob
         self.state_vals = torch.from_numpy(self._state_values).to(self.device)
         self.phaser_rot = torch.from_numpy(geometry.phaser_rotation_table(
@@ -116,6 +119,8 @@ class EMC():
         self.phaser_iter = config.getint('emc', 'phaser_iter', fallback=10)
         self.slice_budget_gb = config.getfloat('emc', 'slice_budget_gb', fallback=8.)
         self.use_graph = config.getboolean('emc', 'cuda_graph', fallback=True)
+        self.dense_gemm = config.get('emc', 'dense_gemm', fallback='auto')
+        self.dense_rescore = config.getboolean('emc', 'dense_rescore', fallback=True)
         self.autotune = config.getboolean('emc', 'autotune', fallback=False)
 
     def _generate_states(self, config):

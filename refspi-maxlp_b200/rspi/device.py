@@ -22,6 +22,7 @@ from .lib import call, check, load
 _f64 = torch.float64
 _i32 = torch.int32
 _i64 = torch.int64
+INT32_MAX = 2 ** 31 - 1
 
 
 def ptr(t):
@@ -139,17 +140,25 @@ class DevicePhotons:
         return self._ll
 
 
-    def dense_entries(self, sel_pix, n_sel, k_pad):
-        """BF16 count digits of the dense frames over the likelihood pixels
-        (built once): ``a0`` = K & 255, ``a1`` = K - a0 when some K > 255."""
-        key = (int(k_pad), sel_pix.data_ptr())
+    def dense_entries(self, sel_pix, n_sel, k_pad, kind='bf16'):
+        """Count operands of the dense frames over the likelihood pixels
+        (built once per kind): ``kind='bf16'``: BF16 digits ``a0`` = K & 255,
+        ``a1`` = K - a0 when some K > 255; ``kind='i8'``: u8 counts ``a0``
+        (``kmax`` > 255 means they were clamped and cannot be used)."""
+        key = (int(k_pad), sel_pix.data_ptr(), kind)
         if self._dense is not None and self._dense['key'] == key:
             return self._dense
         if self.frames is None:
             raise ValueError('the dense form needs dense frames (a photons file with "frames")')
         n, dev, s = self.num_data, self.device, cur_stream()
-        a0 = torch.empty((n, k_pad), dtype=torch.bfloat16, device=dev)
         kmax = torch.zeros(1, dtype=_i32, device=dev)
+        if kind == 'i8':
+            a0 = torch.empty((n, k_pad), dtype=torch.uint8, device=dev)
+            call('rspi_dense_frames_u8', ptr(self.frames), n, self.num_pix, ptr(sel_pix), n_sel,
+                 k_pad, ptr(a0), ptr(kmax), s)
+            self._dense = dict(key=key, a0=a0, a1=None, kmax=int(kmax.item()))
+            return self._dense
+        a0 = torch.empty((n, k_pad), dtype=torch.bfloat16, device=dev)
         call('rspi_dense_frames', ptr(self.frames), n, self.num_pix, ptr(sel_pix), n_sel, k_pad,
              ptr(a0), None, ptr(kmax), s)
         a1 = None
@@ -195,15 +204,20 @@ class EStep:
     ``delta`` (+ the FP32 error bound) of each frame's maximum, which gives
     the same argmax, maximum and log-sum-exp as the FP64 form (the chosen
     form).  ``form='dense'`` (frames stored densely, high fluence): the
-    screening likelihood is a tensor-core GEMM of BF16 count digits with
-    BF16 hi + lo log-slices (FP32 accumulation), followed by the same FP64
-    rescoring of the candidates.
+    likelihood is a tensor-core GEMM over every likelihood pixel, either
+    ``dense_gemm='i8'`` (u8 counts x fixed-point log-slice digits, exact
+    int32 accumulation: error <= 2^-22 photons per frame) or
+    ``dense_gemm='bf16'`` (BF16 count digits x BF16 hi + lo log-slices, FP32
+    accumulation); ``'auto'`` takes i8 when every count is below 256.  With
+    ``dense_rescore`` the candidates within delta + 2 eps of each frame's
+    maximum are rescored in FP64 as in the screened form; without it the
+    GEMM values are final (FP64 log-sum-exp over them).
     """
 
     def __init__(self, photons, size, num_rot, shiftx, shifty, sphere_dia, probmask, bg,
                  form='fp64', states_per_tile=None, warps=32, n_ctas=0,
                  slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel='stream',
-                 n_modes=1):
+                 n_modes=1, dense_gemm='auto', dense_rescore=True):
         if form not in ('fp64', 'screen', 'dense'):
             raise ValueError('form must be fp64, screen or dense')
         if kernel not in ('stream', 'dynamic'):
@@ -234,7 +248,8 @@ class EStep:
         self.bg = t(np.asarray(bg, dtype='f8').ravel())
         self.ll = photons.ll_entries(self.pix2sel, self.p_pad)
         if form == 'dense':
-            self._init_dense(photons, slice_budget_bytes, delta, cand_per_frame)
+            self._init_dense(photons, slice_budget_bytes, delta, cand_per_frame, dense_gemm,
+                             dense_rescore)
             return
         if form == 'fp64':
             self.slice_code, self.prob_code, self.p_row = 1, 1, self.p_pad
@@ -281,18 +296,33 @@ class EStep:
             self.cand_off = torch.empty(n + 1, dtype=_i64, device=dev)
             self.row_cnt = torch.empty(self.n_rows, dtype=_i32, device=dev)
             self.row_cand_off = torch.empty(self.n_rows + 1, dtype=_i64, device=dev)
+            self._alloc_row_scratch()
             per = int(cand_per_frame) if cand_per_frame else min(self.n_rows, 8192)
             self._alloc_candidates(max(1024, per * n))
         self.check_capacity = True
         self.ll_events = None   # list -> (start, end, rows) CUDA events around each launch
 
-    def _init_dense(self, photons, slice_budget_bytes, delta, cand_per_frame):
+    def _init_dense(self, photons, slice_budget_bytes, delta, cand_per_frame, dense_gemm,
+                    dense_rescore):
         dev, n = self.device, photons.num_data
+        if dense_gemm not in ('auto', 'i8', 'bf16'):
+            raise ValueError('dense_gemm must be auto, i8 or bf16')
         self.kernel = 'tcgen05'
-        self.slice_code, self.prob_code = 2, 0           # BF16 hi/lo slices, FP32 matrix
-        self.k_pad = (self.n_sel + 63) // 64 * 64
+        self.slice_code, self.prob_code = 2, 0           # 4 bytes of slice operands per value
+        self.k_pad = (self.n_sel + 127) // 128 * 128
         self.p_row = self.k_pad
-        self.dense = photons.dense_entries(self.sel_pix, self.n_sel, self.k_pad)
+        self.rescore = bool(dense_rescore)
+        phot_max = int(self.ll['frame_sel_photons'].max().item())
+        gemm = dense_gemm
+        if gemm in ('auto', 'i8'):
+            dn = photons.dense_entries(self.sel_pix, self.n_sel, self.k_pad, 'i8')
+            fits = dn['kmax'] <= 255 and phot_max * 255 < 2 ** 31
+            if gemm == 'i8' and not fits:
+                raise ValueError('the exact integer GEMM needs counts below 256 and fewer than '
+                                 '8.4e6 photons per frame on the likelihood pixels')
+            gemm = 'i8' if fits else 'bf16'
+        self.dense_gemm = gemm
+        self.dense = photons.dense_entries(self.sel_pix, self.n_sel, self.k_pad, gemm)
         self.n_digits = 2 if self.dense['a1'] is not None else 1
         self.delta = float(delta)
         self.slice_torch, self.prob_torch = torch.bfloat16, torch.float32
@@ -304,9 +334,13 @@ class EStep:
         self.msum = torch.empty(self.n_states0, dtype=_f64, device=dev)
         self.vscale = torch.empty(1, dtype=_f64, device=dev)
         self.init = torch.empty(self.n_states0, dtype=_f64, device=dev)
-        self.lsl_hi = torch.empty((self.chunk_rows, self.k_pad), dtype=torch.bfloat16, device=dev)
-        self.lsl_lo = torch.empty_like(self.lsl_hi)
-        self.lsl = self.lsl_hi
+        if gemm == 'i8':
+            self.lsl = torch.empty((4, self.chunk_rows, self.k_pad), dtype=torch.uint8, device=dev)
+        else:
+            self.lsl_hi = torch.empty((self.chunk_rows, self.k_pad), dtype=torch.bfloat16,
+                                      device=dev)
+            self.lsl_lo = torch.empty_like(self.lsl_hi)
+            self.lsl = self.lsl_hi
         self.prob = torch.empty((self.n_rows, n), dtype=torch.float32, device=dev)
         self.maxll = torch.empty(n, dtype=_f64, device=dev)
         self.rmax = torch.empty(n, dtype=_i32, device=dev)
@@ -321,18 +355,35 @@ class EStep:
         self.cand_off = torch.empty(n + 1, dtype=_i64, device=dev)
         self.row_cnt = torch.empty(self.n_rows, dtype=_i32, device=dev)
         self.row_cand_off = torch.empty(self.n_rows + 1, dtype=_i64, device=dev)
-        # Error bound of the GEMM value (the candidate threshold's eps_d takes
-        # "rows" FP32 rounding steps per photon x lmax): 2^-16 relative from
-        # the hi + lo split (256 steps of 2^-24) plus 2 x 2^-24 for each of
-        # the n_steps tensor-core accumulations (a rounding or truncating
-        # FP32 adder), as the same per-frame row count for every frame.
-        n_steps = (self.k_pad // 16) * self.n_digits * 2
-        self.eq_rows = 256 + 2 * n_steps
+        self._alloc_row_scratch()
+        # Error bound of the GEMM value.  The candidate threshold's eps_d is
+        # 2^-24 ((rows + 8) photons lmax + |max| + delta + 1) (+ 1e-9 photons
+        # lmax).  i8: the quantisation bound 2^-22 photons is rows = 0 with
+        # lmax = 1/2.  bf16: 2^-16 relative from the hi + lo split (256 steps
+        # of 2^-24) plus 2 x 2^-24 for each of the n_steps tensor-core
+        # accumulations (a rounding or truncating FP32 adder), as the same
+        # per-frame row count for every frame, with lmax the slices' max |L|.
+        if gemm == 'i8':
+            self.eq_rows = 0
+            self.lmax_eps = torch.full((1,), 0.5, dtype=torch.float32, device=dev)
+        else:
+            n_steps = (self.k_pad // 16) * self.n_digits * 2
+            self.eq_rows = 256 + 2 * n_steps
+            self.lmax_eps = self.lmax
         self.eq_row_off = torch.arange(n + 1, dtype=_i64, device=dev) * self.eq_rows
         per = int(cand_per_frame) if cand_per_frame else min(self.n_rows, 8192)
         self._alloc_candidates(max(1024, per * n))
         self.check_capacity = True
         self.ll_events = None
+
+    def _alloc_row_scratch(self):
+        """Global rows for FP64 rescoring when a row exceeds shared memory
+        (one per SM; none otherwise)."""
+        self.row_scratch, self.scratch_rows = None, 0
+        if self.p_pad * 8 > 226 * 1024:
+            sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+            self.scratch_rows = int(sms)
+            self.row_scratch = torch.empty((sms, self.p_pad), dtype=_f64, device=self.device)
 
     def _alloc_candidates(self, cap):
         dev = self.device
@@ -364,6 +415,12 @@ class EStep:
 
     def rot_slices(self, r0, r1, out=None):
         """a6: rotated log-slices of rows [r0, r1) into ``out`` (or the chunk buffer)."""
+        if self.form == 'dense' and self.dense_gemm == 'i8':
+            call('rspi_rot_log_fixed', ptr(self.holo), self.n_states0, self.num_rot,
+                 ptr(self.rot_cs), self.size, ptr(self.bg), ptr(self.sel_pix), self.n_sel,
+                 self.k_pad, r0, r1, self.chunk_rows, ptr(self.lsl), ptr(self.ph.err.t),
+                 cur_stream())
+            return self.lsl
         if self.form == 'dense':
             call('rspi_rot_log_split', ptr(self.holo), self.n_states0, self.num_rot,
                  ptr(self.rot_cs), self.size, ptr(self.bg), ptr(self.sel_pix), self.n_sel,
@@ -391,7 +448,11 @@ class EStep:
             self.ll_events.append(ev)
 
     def _loglike_launch(self, r0, r1, lsl, n):
-        if self.form == 'dense':
+        if self.form == 'dense' and self.dense_gemm == 'i8':
+            call('rspi_dense_loglike_i8', ptr(self.dense['a0']), ptr(self.lsl), self.k_pad, n,
+                 self.chunk_rows, self.num_rot, r0, r1, ptr(self.init), ptr(self.ph.scales),
+                 ptr(self.prob[r0]), n, ptr(self.ph.err.t), cur_stream())
+        elif self.form == 'dense':
             dn = self.dense
             call('rspi_dense_loglike', ptr(dn['a0']), ptr(dn['a1']), ptr(self.lsl_hi),
                  ptr(self.lsl_lo), self.k_pad, n, self.chunk_rows, self.num_rot, r0, r1,
@@ -434,24 +495,30 @@ class EStep:
         """a8 + a9: per-frame max, first-index argmax and log-sum-exp."""
         n = self.ph.num_data
         s = cur_stream()
-        if self.form == 'fp64':
+        if self.form == 'fp64' or (self.form == 'dense' and not self.rescore):
             call('rspi_frame_reduce', ptr(self.prob), self.prob_code, self.n_rows, n,
                  ptr(self.maxll), ptr(self.rmax), ptr(self.logz), s)
             return self.maxll, self.rmax, self.logz
         call('rspi_frame_reduce', ptr(self.prob), 0, self.n_rows, n, ptr(self.max32),
              ptr(self.rmax32), None, s)
         while True:
-            rows_eq = self.eq_row_off if self.form == 'dense' else self.ll16['row_off']
+            dense = self.form == 'dense'
+            rows_eq = self.eq_row_off if dense else self.ll16['row_off']
             call('rspi_screen_candidates', ptr(self.prob), self.n_rows, n, ptr(self.max32),
-                 ptr(self.rmax32), ptr(self.ll['frame_sel_photons']), ptr(rows_eq), ptr(self.lmax),
+                 ptr(self.rmax32), ptr(self.ll['frame_sel_photons']), ptr(rows_eq),
+                 ptr(self.lmax_eps if dense else self.lmax),
                  self.delta, ptr(self.cnt_part), ptr(self.cand_n), ptr(self.noncand),
                  ptr(self.thr), ptr(self.cand_off), self.capacity, ptr(self.cand_d),
                  ptr(self.cand_r), ptr(self.ph.err.t), s)
             if self.check_capacity:
                 total = int(self.cand_off[n].item())
                 if total > self.capacity:
+                    if total > INT32_MAX:
+                        raise RuntimeError('%d screened candidates exceed the int32 candidate '
+                                           'index; raise the precision of the screening pass or '
+                                           'lower screen_delta' % total)
                     self.ph.err.t.zero_()
-                    self._alloc_candidates(int(total * 1.5) + 1024)
+                    self._alloc_candidates(min(INT32_MAX, int(total * 1.5) + 1024))
                     continue
                 self.n_candidates = total
             break
@@ -461,7 +528,7 @@ class EStep:
              ptr(self.ph.scales), ptr(self.ll['entries']), ptr(self.ll['row_off']),
              ptr(self.row_cnt), ptr(self.row_cand_off), ptr(self.row_cand), ptr(self.cand_ll),
              ptr(self.prob), ptr(self.max32), ptr(self.noncand), ptr(self.maxll),
-             ptr(self.rmax), ptr(self.logz), s)
+             ptr(self.rmax), ptr(self.logz), ptr(self.row_scratch), self.scratch_rows, s)
         return self.maxll, self.rmax, self.logz
 
 
@@ -562,6 +629,37 @@ class MStep:
     def set_frame_params(self, fstate, frot, nstate):
         self.fstate, self.frot, self.nstate = fstate, frot, nstate
 
+    def histogram(self, n_cols, rot_cs):
+        """Photons of every phaser pixel per reference state (a11):
+        ``n_hist_rows`` x ``n_cols`` int32, from the current frame parameters."""
+        need = self.n_hist_rows * n_cols
+        if self.hist is None or self.hist.numel() < need:
+            self.hist = torch.empty(max(1, need), dtype=_i32, device=self.device)
+        hist = self.hist[:max(1, need)]
+        hist.zero_()
+        ph = self.ph
+        call('rspi_maxlp_histogram', ptr(ph.ones), ptr(ph.multi), ptr(ph.ones_accum), ptr(ph.multi_accum),
+            ptr(ph.place_ones), ptr(ph.place_multi), ptr(ph.count_multi), ph.num_data,
+            ptr(self.fstate), ptr(self.frot), ptr(rot_cs), self.size, ptr(self.mask_idx),
+            self.n_hist_rows, n_cols, ptr(hist), ptr(ph.err.t), cur_stream())
+        return hist
+
+    def grid(self, fconv, ref_params, rot_cs, scales, n_phase=64, n_amp=32):
+        """Polar grid search of the per-pixel NLL over the main phaser pixels
+        (one mode): ``fconv`` updated in place; returns the per-pixel NLL
+        values of the chosen points (without the F-independent term)."""
+        if self.n_modes != 1:
+            raise ValueError('the grid search takes one mode')
+        n_ref = int(ref_params.shape[0])
+        hist = self.histogram(n_ref, rot_cs)
+        ssum = torch.empty(n_ref, dtype=_f64, device=self.device)
+        best = torch.empty(max(1, self.n_main), dtype=_f64, device=self.device)
+        call('rspi_maxlp_grid', ptr(fconv), ptr(self.main), ptr(self.main_rows), self.n_main,
+             ptr(hist), n_ref, ptr(self.fstate), ptr(scales), self.ph.num_data, ptr(ref_params),
+             self.size, int(n_phase), int(n_amp), ptr(ssum), ptr(best), ptr(self.ph.err.t),
+             cur_stream())
+        return best[:self.n_main]
+
     def run(self, fconv, ref_params, rot_cs):
         """Update ``fconv`` (complex128 device tensor, ``n_modes`` x P) in place."""
         n_ref = int(ref_params.shape[0])
@@ -570,17 +668,9 @@ class MStep:
             raise ValueError('fconv must hold %d model(s) of %d pixels' % (nm, self.size ** 2))
         if self.nstate is None or self.nstate.numel() != nm * n_ref:
             raise ValueError('frame parameters are not set for %d x %d states' % (nm, n_ref))
-        need = self.n_hist_rows * n_ref * nm
-        if self.hist is None or self.hist.numel() < need:
-            self.hist = torch.empty(max(1, need), dtype=_i32, device=self.device)
-        hist = self.hist[:max(1, need)]
-        hist.zero_()
+        hist = self.histogram(n_ref * nm, rot_cs)
         s = cur_stream()
         ph = self.ph
-        call('rspi_maxlp_histogram', ptr(ph.ones), ptr(ph.multi), ptr(ph.ones_accum), ptr(ph.multi_accum),
-            ptr(ph.place_ones), ptr(ph.place_multi), ptr(ph.count_multi), ph.num_data,
-            ptr(self.fstate), ptr(self.frot), ptr(rot_cs), self.size, ptr(self.mask_idx),
-            self.n_hist_rows, n_ref * nm, ptr(hist), ptr(ph.err.t), s)
         call('rspi_maxlp_pattern', ptr(fconv), ptr(self.ring), ptr(self.ring_rows), self.n_ring, ptr(hist), n_ref,
             ptr(self.nstate), nm, ptr(ref_params), self.size, 0, None,
             self.num_iter, ptr(self.rescales), s)

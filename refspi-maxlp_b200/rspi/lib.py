@@ -37,10 +37,10 @@ SIGNATURES = {
     'rspi_screen_loglike': (I, [P, L, L, P, P, P, P, P, L, L, L, P, L, I, I, I, P]),
     'rspi_screen_candidates': (I, [P, L, L, P, P, P, P, P, D, P, P, P, P, P, L, P, P, P, P]),
     'rspi_rescore': (I, [P, P, P, L, L, L, P, L, P, L, P, P, L, L, P, P, P, P, P, P, P, P, P,
-                         P, P, P, P, P, P]),
+                         P, P, P, P, P, P, L, P]),
     'rspi_screen_candidates_noalloc': (I, [P, L, L, P, P, P, P, P, D, P, P, P, P, L, P, P, P,
                                            P]),
-    'rspi_nll': (I, [I, I] + [P] * 7 + [L, P, L, P, L] + [P] * 16),
+    'rspi_nll': (I, [I, I] + [P] * 7 + [L, P, L, P, L] + [P] * 18),
     'rspi_screen_loglike2': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
     'rspi_entries16_check': (I, [P, L, P, P]),
     'rspi_loglike_stream': (I, [I, P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
@@ -50,6 +50,10 @@ SIGNATURES = {
     'rspi_dense_frames': (I, [P, L, L, P, L, L, P, P, P, P]),
     'rspi_rot_log_split': (I, [P, L, L, P, L, P, P, L, L, L, L, P, P, P, P]),
     'rspi_dense_loglike': (I, [P, P, P, P, L, L, L, L, L, L, P, P, P, L, P, P]),
+    'rspi_maxlp_grid': (I, [P, P, P, L, P, L, P, P, L, P, L, I, I, P, P, P, P]),
+    'rspi_dense_frames_u8': (I, [P, L, L, P, L, L, P, P, P]),
+    'rspi_rot_log_fixed': (I, [P, L, L, P, L, P, P, L, L, L, L, L, P, P, P]),
+    'rspi_dense_loglike_i8': (I, [P, P, L, L, L, L, L, L, P, P, P, L, P, P]),
 }
 
 _lib = None
@@ -96,6 +100,8 @@ KERNELS_PER_CALL = {
     'rspi_loglike_stream': 1, 'rspi_posterior_pairs': 3, 'rspi_screen_loglike2': 1,
     'rspi_entries16_check': 1, 'rspi_nll': 2, 'rspi_screen_candidates_noalloc': 3, 'rspi_merge_coverage': 1, 'rspi_merge': 2,
     'rspi_dense_frames': 1, 'rspi_rot_log_split': 1, 'rspi_dense_loglike': 1,
+    'rspi_maxlp_grid': 2, 'rspi_dense_frames_u8': 1, 'rspi_rot_log_fixed': 1,
+    'rspi_dense_loglike_i8': 1,
 }
 launch_count = 0
 

@@ -53,3 +53,20 @@ def test_argument_errors_without_launch(lib):
     null = ctypes.c_void_p(0)
     assert lib.rspi_mean(null, 0, null, null) == -1
     assert lib.rspi_frame_reduce(null, 1, 0, 0, null, null, null, null) == -1
+
+
+def test_bindings_match_header_argument_counts():
+    """Every ctypes signature in rspi/lib.py has as many arguments as its
+    declaration in include/rspi.h."""
+    import re
+    from rspi.lib import SIGNATURES
+    with open(os.path.join(REPO, 'include', 'rspi.h')) as f:
+        h = re.sub(r'/\*.*?\*/', '', f.read(), flags=re.S)
+    seen = 0
+    for m in re.finditer(r'\b(?:int|const char \*)\s*(rspi_\w+)\s*\(([^)]*)\)\s*;', h):
+        name, args = m.group(1), m.group(2).strip()
+        n = 0 if args in ('', 'void') else len(args.split(','))
+        assert name in SIGNATURES, name
+        assert len(SIGNATURES[name][1]) == n, (name, len(SIGNATURES[name][1]), n)
+        seen += 1
+    assert seen == len(SIGNATURES)

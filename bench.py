@@ -17,7 +17,14 @@ dominant kernel from live CUDA events, sampled SM clocks and a CPU baseline
 
 ``--impl reference`` times the reference's CPU equations (the FP64 oracle,
 the reference having no CPU path of its own) on all host cores on a bounded
-sample of the same workload and prints the same metric.
+sample of the same workload and prints the same metric; its
+``reference_gpu`` field adds the reference's own kernels.cu on the same GPU
+(built from the reference sources, emc.py's and maxLP.py's loops replayed
+with torch in place of CuPy), also on a bounded sample.
+
+``--config 3`` evaluates the adjoint instead (NLL + gradient throughput,
+L-BFGS against the polar grid search on NLL and FRC); ``--config 4`` and
+``--config 5`` run the multi-mode and the dense high-fluence workloads.
 
 Multi-GPU: the path runs as independent replicas (one full workload per
 rank, no collective on the data path); value = sum over ranks, time = max.
@@ -65,6 +72,8 @@ def parse_args():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-clocks', action='store_true', help='do not sample nvidia-smi clocks')
+    ap.add_argument('--no-ref-gpu', action='store_true',
+                    help='reference arm: skip timing the reference kernels on the GPU')
     args = ap.parse_args()
     if args.form is None:
         from rspi import synth
@@ -93,6 +102,13 @@ def workload(cfg_id, frames):
     nm = int(r.get('num_modes', 1))
     return dict(cfg=c, n=n, size=c['size'], num_rot=r['num_rot'], n_states0=nsx * nsy * nd,
                 n_modes=nm, n_states=nsx * nsy * nd * r['num_rot'] * nm, recon=r)
+
+
+def workload_name(cfg_id, w):
+    return ('config%d: %dx%d detector, %d frames, %d rotations x %d (shift,dia) states x %d '
+            'mode(s) = %d states/frame, 1 EMC iteration per step' %
+            (cfg_id, w['size'], w['size'], w['n'], w['num_rot'], w['n_states0'], w['n_modes'],
+             w['n_states']))
 
 
 def generate_data(cfg_id, w, device='cpu'):
@@ -394,15 +410,50 @@ def run_reference(args):
            'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
            'ms_per_step': t * 1e3, 's_per_iteration': t, 'higher_is_better': True,
            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
-           'config': {'workload': 'config%d: %dx%d detector, %d frames, %d states/frame' %
-                      (args.config, w['size'], w['size'], w['n'], w['n_states']),
-                      'frames': w['n'], 'states_per_frame': w['n_states'],
+           'config': {'workload': workload_name(args.config, w), 'frames': w['n'],
+                      'states_per_frame': w['n_states'], 'form': 'FP64 NumPy restatement',
                       'l2': 'inputs larger than L2'},
            'cpu_baseline': {'value': v, 'unit': UNIT, 'cores': base['cores'], 'kind': 'port',
                             'sample': base['sample']},
-           'e2e': {'value': v, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+           'e2e': {'value': v, 'unit': UNIT, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+           'reference_gpu': None if args.no_ref_gpu else reference_gpu(args, w, data, model)}
     print(json.dumps(out))
     return 0
+
+
+def reference_gpu(args, w, data, model):
+    """The reference's own kernels.cu on this GPU (built from the reference
+    sources into oracle/_ref/), replaying emc.py's E-step loop and maxLP.py's
+    per-pixel pattern search on a bounded sample; None-free dict with
+    ``unavailable`` when the GPU or the built kernels are missing."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return {'unavailable': 'no CUDA device'}
+        from oracle import emc_oracle as E
+        from oracle.ref_gpu import replay
+        from rspi import geometry
+        if w['n_modes'] != 1 or w['cfg'].get('dense'):
+            return {'unavailable': 'the reference runs one model on sparse photons only'}
+        lib = replay.load()
+        dev = torch.device('cuda', 0)
+        size = w['size']
+        ds = E.parse_photons(data['ones'], data['multi'], data['place_ones'], data['place_multi'],
+                             data['count_multi'], size * size, True)
+        _, pm = geometry.emc_masks(size)
+        rd = replay.RefData(ds['ones'], ds['multi'], ds['place_ones'], ds['place_multi'],
+                            ds['count_multi'], size, ds['bg'], E.get_scales(ds, True), pm, dev)
+        r = w['recon']
+        sx, sy, dia, _ = geometry.state_grid(geometry.parse_triple(r['shiftx']),
+                                            geometry.parse_triple(r['shifty']),
+                                            geometry.parse_triple(r['sphere_dia']))
+        res = replay.time_iteration(lib, rd, torch.from_numpy(model).to(dev), sx, sy, dia,
+                                    r['num_rot'])
+        res['value'] = w['n'] * w['n_states'] / res['s_per_iteration']
+        res['unit'] = UNIT
+        return res
+    except Exception as exc:   # reported, never fatal for the reference arm
+        return {'unavailable': '%s: %s' % (type(exc).__name__, exc)}
 
 
 def run_ours(args):
@@ -569,10 +620,7 @@ def run_ours(args):
                             'bf16 GEMM (f32 accumulate)') +
                            (' + f64 rescore' if getattr(es, 'rescore', True) else '')}[args.form],
         'data': 'synthetic (seeded generator with the configuration\'s shapes)',
-        'config': {'workload': 'config%d: %dx%d detector, %d frames, %d rotations x %d (shift,dia) '
-                   'states x %d mode(s) = %d states/frame, 1 EMC iteration per step' %
-                   (args.config, w['size'], w['size'], w['n'], w['num_rot'], w['n_states0'],
-                    w['n_modes'], w['n_states']),
+        'config': {'workload': workload_name(args.config, w),
                    'frames': w['n'], 'states_per_frame': w['n_states'],
                    'form': args.form, 'parallelism': 'replicas' if world > 1 else 'single',
                    'l2': 'inputs larger than L2 (slices %.1f GB, likelihoods %.1f GB per step)' %

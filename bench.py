@@ -62,7 +62,7 @@ def parse_args():
     ap.add_argument('--frames', type=int, default=None, help='override frame count (testing)')
     ap.add_argument('--form', default=None, choices=['fp64', 'screen', 'dense'],
                     help='likelihood form (default: dense for config 5, screen otherwise)')
-    ap.add_argument('--kernel', default='stream', choices=['stream', 'dynamic'])
+    ap.add_argument('--kernel', default='stream', choices=['stream', 'frame', 'wide', 'dynamic'])
     ap.add_argument('--slice-gb', type=float, default=8.,
                     help='largest rotated-slice chunk (GB); smaller values give more launches')
     ap.add_argument('--no-plain', action='store_true',

@@ -199,6 +199,43 @@ int rspi_screen_loglike2(const float *lslices, long long p_row, long long num_ro
                          long long ll_stride, int states_per_tile, int warps_per_cta,
                          int n_ctas, cudaStream_t stream);
 
+/* The same likelihoods as rspi_screen_loglike2 for 1 or 2 states per tile,
+ * frame at a time: each warp sums one frame after another, the frame's
+ * first prefetch_words (4, 8 or 12) words having been loaded during the
+ * previous frame, without per-word frame-boundary tests (words past a
+ * frame's end read the lane's zero column).  Same arguments plus
+ * prefetch_words; same error bound for the screening threshold. */
+int rspi_screen_loglike3(const float *lslices, long long p_row, long long num_rot,
+                         const double *init, const double *scales,
+                         const unsigned short *entries, const long long *row_off,
+                         long long n_data, long long row_begin, long long row_end, float *ll,
+                         long long ll_stride, int states_per_tile, int prefetch_words,
+                         int warps_per_cta, int n_ctas, cudaStream_t stream);
+
+/* Wide entries for rspi_screen_loglike4: per frame the 16-bit entry rows
+ * (rspi_ll16_entry_fill layout) padded to a multiple of four with the
+ * lane's zero column, as 32-bit byte offsets sel * 4 * states_per_tile of
+ * the interleaved tile, four rows of a lane in one 16-byte group:
+ * wide[((group_off[d] + g) * 32 + lane) * 4 + k] holds row 4g + k.
+ * rspi_wide_entry_groups writes each frame's group count; the caller scans
+ * it (rspi_scan_rows) into group_off[n_data + 1] and allocates
+ * group_off[n_data] * 128 entries. */
+int rspi_wide_entry_groups(const long long *row_off16, long long n_data, int *groups,
+                           cudaStream_t stream);
+int rspi_wide_entry_fill(const unsigned short *entries16, const long long *row_off16,
+                         long long n_data, int p_zero, int states_per_tile,
+                         const long long *group_off, unsigned *wide, cudaStream_t stream);
+
+/* The same likelihoods as rspi_screen_loglike2 (1 or 2 states per tile) from
+ * the wide entries built for that tile size: one 16-byte load per four
+ * photons of a lane and no per-photon index arithmetic. */
+int rspi_screen_loglike4(const float *lslices, long long p_row, long long num_rot,
+                         const double *init, const double *scales, const unsigned *wide,
+                         const long long *group_off, long long n_data, long long row_begin,
+                         long long row_end, float *ll, long long ll_stride,
+                         int states_per_tile, int warps_per_cta, int n_ctas,
+                         cudaStream_t stream);
+
 /* *max_index = largest value in a 16-bit entry array. */
 int rspi_entries16_check(const unsigned short *entries, long long n_entries,
                          unsigned *max_index, cudaStream_t stream);

@@ -378,24 +378,26 @@ k_rot_log_split(const double *__restrict__ holo, long long num_rot,
                 long long row_begin, long long n_rows, __nv_bfloat16 *__restrict__ hi,
                 __nv_bfloat16 *__restrict__ lo, float *__restrict__ abs_max) {
     const long long npix = (long long)size * size;
-    const long long total = n_rows * k_pad;
-    const long long stride = (long long)gridDim.x * blockDim.x;
+    const int ns = (int)n_sel, kp = (int)k_pad;
     float amax = 0.f;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        const long long rr = i / k_pad, c = i - rr * k_pad;
-        double v = 0.;
-        if (c < n_sel) {
-            const long long r = row_begin + rr;
-            const long long s0 = r / num_rot, j = r - s0 * num_rot;
-            const int p = sel_pix[c];
-            const int x = p / size, y = p - (p / size) * size;
-            v = rot_log_value(holo + s0 * npix, x, y, size, rot_cs[2 * j], rot_cs[2 * j + 1],
-                              bg[p]);
+    for (long long rr = blockIdx.x; rr < n_rows; rr += gridDim.x) {   // one row per CTA
+        const long long r = row_begin + rr;
+        const long long s0 = r / num_rot, j = r - s0 * num_rot;
+        const double ac = rot_cs[2 * j], as = rot_cs[2 * j + 1];
+        const double *w = holo + s0 * npix;
+        for (int c = threadIdx.x; c < kp; c += blockDim.x) {
+            double v = 0.;
+            if (c < ns) {
+                const int p = sel_pix[c];
+                const int x = p / size, y = p - x * size;
+                v = rot_log_value(w, x, y, size, ac, as, bg[p]);
+            }
+            const __nv_bfloat16 h = __double2bfloat16(v);
+            const long long i = rr * k_pad + c;
+            hi[i] = h;
+            lo[i] = __double2bfloat16(v - (double)__bfloat162float(h));
+            amax = fmaxf(amax, fabsf((float)v));
         }
-        const __nv_bfloat16 h = __double2bfloat16(v);
-        hi[i] = h;
-        lo[i] = __double2bfloat16(v - (double)__bfloat162float(h));
-        amax = fmaxf(amax, fabsf((float)v));
     }
     if (abs_max) {
         amax = __int_as_float(warp_max_int(__float_as_int(amax)));
@@ -432,28 +434,30 @@ k_rot_log_q(const double *__restrict__ holo, long long num_rot, const double *__
             long long n_sel, long long k_pad, long long row_begin, long long n_rows,
             long long plane, uint8_t *__restrict__ b, int *err) {
     const long long npix = (long long)size * size;
-    const long long total = n_rows * k_pad;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        const long long rr = i / k_pad, c = i - rr * k_pad;
-        double v = 0.;
-        if (c < n_sel) {
-            const long long r = row_begin + rr;
-            const long long s0 = r / num_rot, j = r - s0 * num_rot;
-            const int p = sel_pix[c];
-            const int x = p / size, y = p - (p / size) * size;
-            v = rot_log_value(holo + s0 * npix, x, y, size, rot_cs[2 * j], rot_cs[2 * j + 1],
-                              bg[p]);
+    const int ns = (int)n_sel, kp = (int)k_pad;
+    for (long long rr = blockIdx.x; rr < n_rows; rr += gridDim.x) {   // one row per CTA
+        const long long r = row_begin + rr;
+        const long long s0 = r / num_rot, j = r - s0 * num_rot;
+        const double ac = rot_cs[2 * j], as = rot_cs[2 * j + 1];
+        const double *w = holo + s0 * npix;
+        uint8_t *o = b + rr * k_pad;
+        for (int c = threadIdx.x; c < kp; c += blockDim.x) {
+            double v = 0.;
+            if (c < ns) {
+                const int p = sel_pix[c];
+                const int x = p / size, y = p - x * size;
+                v = rot_log_value(w, x, y, size, ac, as, bg[p]);
+            }
+            if (!(fabs(v) < 1023.)) {   // also NaN
+                rspi_flag(err, RSPI_ERR_CAPACITY);
+                v = v != v ? 0. : (v > 0. ? 1023. : -1023.);
+            }
+            const int q = (int)rint(v * 2097152.);   // 2^21
+            o[c] = (uint8_t)(q & 255);
+            o[plane + c] = (uint8_t)((q >> 8) & 255);
+            o[2 * plane + c] = (uint8_t)((q >> 16) & 255);
+            o[3 * plane + c] = (uint8_t)(q >> 24);
         }
-        if (!(fabs(v) < 1023.)) {   // also NaN
-            rspi_flag(err, RSPI_ERR_CAPACITY);
-            v = v != v ? 0. : (v > 0. ? 1023. : -1023.);
-        }
-        const int q = (int)rint(v * 2097152.);   // 2^21
-        b[i] = (uint8_t)(q & 255);
-        b[plane + i] = (uint8_t)((q >> 8) & 255);
-        b[2 * plane + i] = (uint8_t)((q >> 16) & 255);
-        b[3 * plane + i] = (uint8_t)(q >> 24);
     }
 }
 
@@ -543,7 +547,7 @@ extern "C" int rspi_rot_log_split(const double *holo, long long n_states0, long 
         return RSPI_ERR_ARG;
     const long long n_rows = row_end - row_begin;
     if (n_rows == 0) return RSPI_OK;
-    k_rot_log_split<<<rspi_blocks(n_rows * k_pad, 256, 16), 256, 0, stream>>>(
+    k_rot_log_split<<<(unsigned)min(n_rows, (long long)rspi_sm_count() * 64), 256, 0, stream>>>(
         holo, num_rot, rot_cs, (int)size, bg, sel_pix, n_sel, k_pad, row_begin, n_rows,
         (__nv_bfloat16 *)hi, (__nv_bfloat16 *)lo, abs_max);
     RSPI_RETURN_LAUNCH();
@@ -599,7 +603,7 @@ extern "C" int rspi_rot_log_fixed(const double *holo, long long n_states0, long 
         return RSPI_ERR_ARG;
     const long long n_rows = row_end - row_begin;
     if (n_rows == 0) return RSPI_OK;
-    k_rot_log_q<<<rspi_blocks(n_rows * k_pad, 256, 16), 256, 0, stream>>>(
+    k_rot_log_q<<<(unsigned)min(n_rows, (long long)rspi_sm_count() * 64), 256, 0, stream>>>(
         holo, num_rot, rot_cs, (int)size, bg, sel_pix, n_sel, k_pad, row_begin, n_rows,
         plane_rows * k_pad, (uint8_t *)digits, err);
     RSPI_RETURN_LAUNCH();

@@ -234,6 +234,309 @@ k_screen_ll2(const float *__restrict__ lsl, int p_row, int num_rot,
     }
 }
 
+// Frame-at-a-time form of the same sums (the default for T = 1, 2): the
+// warp walks its frames one by one; the first PFW words of each frame were
+// loaded while the previous frame was summed, and a frame's sum runs without
+// any per-word frame-boundary test.  Words past the frame's end are replaced
+// by the lane's zero-column pair, which adds exactly 0.  Two accumulators
+// per lane alternate between words.  Each value passes through at most
+// (words + 8) FP32 roundings, within the screening bound.
+template <int T, int PFW>
+__global__ void __launch_bounds__(1024)
+k_screen_ll3(const float *__restrict__ lsl, int p_row, int num_rot,
+             const double *__restrict__ init, const double *__restrict__ scales,
+             const unsigned *__restrict__ words, const long long *__restrict__ row_off, int n_data,
+             long long row_begin, long long row_end, float *__restrict__ ll, long long ll_stride) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float *slf = reinterpret_cast<float *>(smem_raw);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const long long n_tiles = (row_end - row_begin + T - 1) / T;
+    const int qtot = (int)(row_off[n_data] >> 1);
+    auto lower = [&](int target) {
+        int lo = 0, hi = n_data;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((int)(row_off[mid] >> 1) < target) lo = mid + 1;
+            else hi = mid;
+        }
+        return lo;
+    };
+    const int fb = wid == 0 ? 0 : lower((int)((long long)qtot * wid / nw));
+    const int fe = wid == nw - 1 ? n_data : lower((int)((long long)qtot * (wid + 1) / nw));
+    const unsigned zc = (unsigned)(p_row - 32 + lane);
+    const unsigned zpair = zc | (zc << 16);
+    const int last = qtot - 1;   // last word index (-1: no words at all)
+    auto word_at = [&](int q) -> unsigned {
+        return last >= 0 ? __ldg(words + (long long)min(q, last) * 32 + lane) : zpair;
+    };
+
+    for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const long long first = row_begin + tile * T;
+        const int nt = (int)min((long long)T, row_end - first);
+        __syncthreads();
+        const float *src = lsl + (first - row_begin) * (long long)p_row;
+        for (int i = threadIdx.x; i < T * p_row; i += blockDim.x) {
+            const int t = i / p_row, c = i - t * p_row;
+            slf[c * T + t] = t < nt ? __ldg(src + i) : 0.f;
+        }
+        __syncthreads();
+        if (fb >= fe) continue;
+
+        const int my_t = lane & (T - 1);
+        const double my_init = my_t < nt ? init[(first + my_t) / num_rot] : 0.;
+        float *my_ll = ll + (first + my_t - row_begin) * ll_stride;
+        int base = fb;
+        int my_end = fb + lane < n_data ? (int)(row_off[fb + lane + 1] >> 1) : 0x7fffffff;
+        double my_scale = fb + lane < n_data ? scales[fb + lane] : 0.;
+        int q = (int)(row_off[fb] >> 1);
+        unsigned pre[PFW];
+#pragma unroll
+        for (int k = 0; k < PFW; ++k) pre[k] = word_at(q + k);
+        for (int f = fb; f < fe; ++f) {
+            const int qe = __shfl_sync(RSPI_FULL_MASK, my_end, f - base);
+            const int n = qe - q;
+            unsigned cur[PFW];
+#pragma unroll
+            for (int k = 0; k < PFW; ++k) {
+                cur[k] = k < n ? pre[k] : zpair;
+                pre[k] = word_at(qe + k);          // the next frame's first words
+            }
+            Acc<T> a0, a1;
+            a0.zero();
+            a1.zero();
+#pragma unroll
+            for (int k = 0; k < PFW; k += 2) {
+                add_contrib<T>(a0, gather_word<T>(smem_raw, cur[k]));
+                add_contrib<T>(a1, gather_word<T>(smem_raw, cur[k + 1]));
+            }
+            for (int q2 = q + PFW; q2 < qe; q2 += 4) {   // frames longer than PFW words
+                unsigned w[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) w[k] = q2 + k < qe ? word_at(q2 + k) : zpair;
+                add_contrib<T>(a0, gather_word<T>(smem_raw, w[0]));
+                add_contrib<T>(a1, gather_word<T>(smem_raw, w[1]));
+                add_contrib<T>(a0, gather_word<T>(smem_raw, w[2]));
+                add_contrib<T>(a1, gather_word<T>(smem_raw, w[3]));
+            }
+            Contrib<T> c1;
+#pragma unroll
+            for (int i = 0; i < (T + 1) / 2; ++i) c1.p[i] = a1.p[i];
+            add_contrib<T>(a0, c1);
+            const float tot = reduce_scatter<T>(a0, lane);
+            const double sc = __shfl_sync(RSPI_FULL_MASK, my_scale, f - base);
+            if (lane < nt) my_ll[f] = (float)(my_init * sc + (double)tot);
+            q = qe;
+            if (f + 1 - base == 32) {
+                base = f + 1;
+                my_end = base + lane < n_data ? (int)(row_off[base + lane + 1] >> 1) : 0x7fffffff;
+                my_scale = base + lane < n_data ? scales[base + lane] : 0.;
+            }
+        }
+    }
+}
+
+template <int T, int PFW>
+int launch3(const float *lsl, long long p_row, long long num_rot, const double *init,
+            const double *scales, const unsigned *words, const long long *row_off,
+            long long n_data, long long r0, long long r1, float *ll, long long stride, int warps,
+            int n_ctas, cudaStream_t stream) {
+    const size_t smem = (size_t)T * p_row * sizeof(float);
+    if (smem > (size_t)SMEM_LIMIT - 1024) return RSPI_ERR_ARG;
+    static size_t smem_set = 0;
+    if (smem > smem_set) {
+        if (cudaFuncSetAttribute(k_screen_ll3<T, PFW>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return RSPI_ERR_CUDA;
+        smem_set = smem;
+    }
+    const long long n_tiles = (r1 - r0 + T - 1) / T;
+    if (n_ctas <= 0) {
+        const int per_sm = max(1, (int)(SMEM_LIMIT / (smem + 1024)));
+        n_ctas = rspi_sm_count() * min(per_sm, max(1, 2048 / (warps * 32)));
+    }
+    if (n_ctas > n_tiles) n_ctas = (int)n_tiles;
+    k_screen_ll3<T, PFW><<<n_ctas, warps * 32, smem, stream>>>(
+        lsl, (int)p_row, (int)num_rot, init, scales, words, row_off, (int)n_data, r0, r1, ll,
+        stride);
+    RSPI_RETURN_LAUNCH();
+}
+
+// ---------------------------------------------------------------------------
+// Wide-entry form: 32-bit entries that already hold the byte offset of the
+// photon's value in the interleaved tile (sel * 4T), four rows of a lane in
+// one 16-byte group, so a lane issues one LDG.128 per four photons and each
+// photon costs one shared gather and half a packed add.  Rows of a frame are
+// padded to a multiple of four with the lane's zero column.
+// ---------------------------------------------------------------------------
+__global__ void k_wide_groups(const long long *__restrict__ row_off16, long long n,
+                              int *__restrict__ groups) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long d = (long long)blockIdx.x * blockDim.x + threadIdx.x; d < n; d += stride)
+        groups[d] = (int)((row_off16[d + 1] - row_off16[d] + 3) >> 2);
+}
+
+__global__ void k_wide_fill(const unsigned short *__restrict__ ent16,
+                            const long long *__restrict__ row_off16, long long n, int p_zero,
+                            int tile, const long long *__restrict__ goff,
+                            unsigned *__restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const unsigned scale = 4u * (unsigned)tile;
+    for (long long d = warp; d < n; d += nwarp) {
+        const long long r0 = row_off16[d], nr = row_off16[d + 1] - r0;
+        const long long g0 = goff[d], ng = goff[d + 1] - g0;
+        for (long long r = 0; r < 4 * ng; ++r) {
+            unsigned v = (unsigned)(p_zero + lane);
+            if (r < nr) {
+                const long long rr = r0 + r;
+                v = ent16[(rr >> 1) * 64 + lane * 2 + (rr & 1)];
+            }
+            out[((g0 + (r >> 2)) * 32 + lane) * 4 + (r & 3)] = v * scale;
+        }
+    }
+}
+
+template <int T>
+__device__ __forceinline__ Contrib<T> gather_pair(const unsigned char *sl, unsigned a,
+                                                  unsigned b) {
+    Contrib<T> c;
+    if (T == 1) {
+        c.p[0] = make_float2(*reinterpret_cast<const float *>(sl + a) +
+                                 *reinterpret_cast<const float *>(sl + b),
+                             0.f);
+    } else {
+        const float2 v0 = *reinterpret_cast<const float2 *>(sl + a);
+        const float2 v1 = *reinterpret_cast<const float2 *>(sl + b);
+        c.p[0] = __fadd2_rn(v0, v1);
+    }
+    return c;
+}
+
+template <int T>
+__global__ void __launch_bounds__(1024)
+k_screen_ll4(const float *__restrict__ lsl, int p_row, int num_rot,
+             const double *__restrict__ init, const double *__restrict__ scales,
+             const uint4 *__restrict__ groups, const long long *__restrict__ goff, int n_data,
+             long long row_begin, long long row_end, float *__restrict__ ll, long long ll_stride) {
+    constexpr int PG = 4;   // groups (16 photons per lane) loaded ahead
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float *slf = reinterpret_cast<float *>(smem_raw);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const long long n_tiles = (row_end - row_begin + T - 1) / T;
+    const int gtot = (int)goff[n_data];
+    auto lower = [&](int target) {
+        int lo = 0, hi = n_data;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((int)goff[mid] < target) lo = mid + 1;
+            else hi = mid;
+        }
+        return lo;
+    };
+    const int fb = wid == 0 ? 0 : lower((int)((long long)gtot * wid / nw));
+    const int fe = wid == nw - 1 ? n_data : lower((int)((long long)gtot * (wid + 1) / nw));
+
+    for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const long long first = row_begin + tile * T;
+        const int nt = (int)min((long long)T, row_end - first);
+        __syncthreads();
+        const float *src = lsl + (first - row_begin) * (long long)p_row;
+        for (int i = threadIdx.x; i < T * p_row; i += blockDim.x) {
+            const int t = i / p_row, c = i - t * p_row;
+            slf[c * T + t] = t < nt ? __ldg(src + i) : 0.f;
+        }
+        __syncthreads();
+        if (fb >= fe) continue;
+
+        const int my_t = lane & (T - 1);
+        const double my_init = my_t < nt ? init[(first + my_t) / num_rot] : 0.;
+        float *my_ll = ll + (first + my_t - row_begin) * ll_stride;
+        Acc<T> a0, a1;
+        a0.zero();
+        a1.zero();
+        int base = fb;
+        int my_end = fb + lane < n_data ? (int)goff[fb + lane + 1] : 0x7fffffff;
+        double my_scale = fb + lane < n_data ? scales[fb + lane] : 0.;
+        int f = fb;
+        int g = (int)goff[fb];
+        const int gend = (int)goff[fe];
+        int fend = __shfl_sync(RSPI_FULL_MASK, my_end, 0);
+        auto finish = [&]() {
+            Contrib<T> c1;
+#pragma unroll
+            for (int i = 0; i < (T + 1) / 2; ++i) c1.p[i] = a1.p[i];
+            add_contrib<T>(a0, c1);
+            const float tot = reduce_scatter<T>(a0, lane);
+            const double sc = __shfl_sync(RSPI_FULL_MASK, my_scale, f - base);
+            if (lane < nt) my_ll[f] = (float)(my_init * sc + (double)tot);
+            a0.zero();
+            a1.zero();
+            ++f;
+            if (f - base == 32) {
+                base = f;
+                my_end = f + lane < n_data ? (int)goff[f + lane + 1] : 0x7fffffff;
+                my_scale = f + lane < n_data ? scales[f + lane] : 0.;
+            }
+            fend = f < fe ? __shfl_sync(RSPI_FULL_MASK, my_end, f - base) : gend + 1;
+        };
+        while (f < fe && fend == g) finish();   // frames without entry rows
+
+        const uint4 *gp = groups + (long long)g * 32 + lane;
+        uint4 cur[PG], nxt[PG];
+        const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+        for (int k = 0; k < PG; ++k) cur[k] = g + k < gend ? __ldg(gp + 32 * k) : z;
+        while (g < gend) {
+            const int nb = min(PG, gend - g);
+#pragma unroll
+            for (int k = 0; k < PG; ++k) nxt[k] = g + PG + k < gend ? __ldg(gp + 32 * (PG + k)) : z;
+#pragma unroll
+            for (int k = 0; k < PG; ++k) {
+                if (k < nb) {
+                    add_contrib<T>(a0, gather_pair<T>(smem_raw, cur[k].x, cur[k].y));
+                    add_contrib<T>(a1, gather_pair<T>(smem_raw, cur[k].z, cur[k].w));
+                    if (g + k + 1 == fend) {
+                        finish();
+                        while (f < fe && fend == g + k + 1) finish();
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < PG; ++k) cur[k] = nxt[k];
+            g += PG;
+            gp += 32 * PG;
+        }
+    }
+}
+
+template <int T>
+int launch4(const float *lsl, long long p_row, long long num_rot, const double *init,
+            const double *scales, const uint4 *groups, const long long *goff, long long n_data,
+            long long r0, long long r1, float *ll, long long stride, int warps, int n_ctas,
+            cudaStream_t stream) {
+    const size_t smem = (size_t)T * p_row * sizeof(float);
+    if (smem > (size_t)SMEM_LIMIT - 1024) return RSPI_ERR_ARG;
+    static size_t smem_set = 0;
+    if (smem > smem_set) {
+        if (cudaFuncSetAttribute(k_screen_ll4<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return RSPI_ERR_CUDA;
+        smem_set = smem;
+    }
+    const long long n_tiles = (r1 - r0 + T - 1) / T;
+    if (n_ctas <= 0) {
+        const int per_sm = max(1, (int)(SMEM_LIMIT / (smem + 1024)));
+        n_ctas = rspi_sm_count() * min(per_sm, max(1, 2048 / (warps * 32)));
+    }
+    if (n_ctas > n_tiles) n_ctas = (int)n_tiles;
+    k_screen_ll4<T><<<n_ctas, warps * 32, smem, stream>>>(
+        lsl, (int)p_row, (int)num_rot, init, scales, groups, goff, (int)n_data, r0, r1, ll,
+        stride);
+    RSPI_RETURN_LAUNCH();
+}
+
 template <int T>
 int launch2(const float *lsl, long long p_row, long long num_rot, const double *init,
             const double *scales, const unsigned *words, const long long *row_off,
@@ -312,4 +615,81 @@ extern "C" int rspi_screen_loglike2(const float *lslices, long long p_row, long 
         default:
             return RSPI_ERR_ARG;
     }
+}
+
+extern "C" int rspi_screen_loglike3(const float *lslices, long long p_row, long long num_rot,
+                                    const double *init, const double *scales,
+                                    const unsigned short *entries, const long long *row_off,
+                                    long long n_data, long long row_begin, long long row_end,
+                                    float *ll, long long ll_stride, int states_per_tile,
+                                    int prefetch_words, int warps_per_cta, int n_ctas,
+                                    cudaStream_t stream) {
+    if (!lslices || !init || !scales || !entries || !row_off || !ll || n_data <= 0 ||
+        n_data > 0x7fffffffLL || p_row <= 32 || p_row % 32 || p_row > 65536 || num_rot <= 0 ||
+        num_rot > 0x7fffffffLL || row_begin < 0 || row_end < row_begin || ll_stride < n_data ||
+        warps_per_cta < 1 || warps_per_cta > 32)
+        return RSPI_ERR_ARG;
+    if ((reinterpret_cast<uintptr_t>(lslices) & 15) != 0 ||
+        (reinterpret_cast<uintptr_t>(entries) & 3) != 0)
+        return RSPI_ERR_ARG;
+    if (row_end == row_begin) return RSPI_OK;
+    const unsigned *w = reinterpret_cast<const unsigned *>(entries);
+#define RSPI_LL3(T, PF)                                                                        \
+    return launch3<T, PF>(lslices, p_row, num_rot, init, scales, w, row_off, n_data, row_begin, \
+                          row_end, ll, ll_stride, warps_per_cta, n_ctas, stream)
+    if (states_per_tile == 1) {
+        if (prefetch_words == 4) RSPI_LL3(1, 4);
+        if (prefetch_words == 8) RSPI_LL3(1, 8);
+        if (prefetch_words == 12) RSPI_LL3(1, 12);
+    } else if (states_per_tile == 2) {
+        if (prefetch_words == 4) RSPI_LL3(2, 4);
+        if (prefetch_words == 8) RSPI_LL3(2, 8);
+        if (prefetch_words == 12) RSPI_LL3(2, 12);
+    }
+#undef RSPI_LL3
+    return RSPI_ERR_ARG;
+}
+
+extern "C" int rspi_wide_entry_groups(const long long *row_off16, long long n_data, int *groups,
+                                      cudaStream_t stream) {
+    if (!row_off16 || !groups || n_data <= 0) return RSPI_ERR_ARG;
+    k_wide_groups<<<rspi_blocks(n_data, 256), 256, 0, stream>>>(row_off16, n_data, groups);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_wide_entry_fill(const unsigned short *entries16, const long long *row_off16,
+                                    long long n_data, int p_zero, int states_per_tile,
+                                    const long long *group_off, unsigned *wide,
+                                    cudaStream_t stream) {
+    if (!entries16 || !row_off16 || !group_off || !wide || n_data <= 0 || p_zero < 0 ||
+        p_zero % 32 || p_zero + 32 > 65536 || (states_per_tile != 1 && states_per_tile != 2))
+        return RSPI_ERR_ARG;
+    k_wide_fill<<<rspi_blocks(n_data * 32, 256), 256, 0, stream>>>(
+        entries16, row_off16, n_data, p_zero, states_per_tile, group_off, wide);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_screen_loglike4(const float *lslices, long long p_row, long long num_rot,
+                                    const double *init, const double *scales,
+                                    const unsigned *wide, const long long *group_off,
+                                    long long n_data, long long row_begin, long long row_end,
+                                    float *ll, long long ll_stride, int states_per_tile,
+                                    int warps_per_cta, int n_ctas, cudaStream_t stream) {
+    if (!lslices || !init || !scales || !wide || !group_off || !ll || n_data <= 0 ||
+        n_data > 0x7fffffffLL || p_row <= 32 || p_row % 32 || p_row > 65536 || num_rot <= 0 ||
+        num_rot > 0x7fffffffLL || row_begin < 0 || row_end < row_begin || ll_stride < n_data ||
+        warps_per_cta < 1 || warps_per_cta > 32)
+        return RSPI_ERR_ARG;
+    if ((reinterpret_cast<uintptr_t>(lslices) & 15) != 0 ||
+        (reinterpret_cast<uintptr_t>(wide) & 15) != 0)
+        return RSPI_ERR_ARG;
+    if (row_end == row_begin) return RSPI_OK;
+    const uint4 *g = reinterpret_cast<const uint4 *>(wide);
+    if (states_per_tile == 1)
+        return launch4<1>(lslices, p_row, num_rot, init, scales, g, group_off, n_data, row_begin,
+                          row_end, ll, ll_stride, warps_per_cta, n_ctas, stream);
+    if (states_per_tile == 2)
+        return launch4<2>(lslices, p_row, num_rot, init, scales, g, group_off, n_data, row_begin,
+                          row_end, ll, ll_stride, warps_per_cta, n_ctas, stream);
+    return RSPI_ERR_ARG;
 }

@@ -2,6 +2,8 @@
 // (shift, diameter) state, their masked sums, vscale, and the rotated
 // log-slices on the likelihood pixels.  FP64 throughout; the rotated slices
 // are stored as float32 or float64.
+#include <algorithm>
+
 #include "rspi_common.cuh"
 
 namespace {
@@ -62,6 +64,9 @@ k_vscale_init(const double *__restrict__ msum, long long n_states0,
     for (long long s = threadIdx.x; s < n_states0; s += blockDim.x) init[s] = -(msum[s] * vs);
 }
 
+// One CTA per likelihood row (grid-stride over rows): the row's state,
+// rotation and slice pointer are computed once, the threads walk the row's
+// columns; no per-element 64-bit division.
 template <typename TL>
 __global__ void __launch_bounds__(256)
 k_rot_log(const double *__restrict__ holo, long long num_rot, const double *__restrict__ rot_cs,
@@ -69,23 +74,25 @@ k_rot_log(const double *__restrict__ holo, long long num_rot, const double *__re
           long long n_sel, long long p_pad, long long row_begin, long long n_rows,
           TL *__restrict__ out, float *__restrict__ abs_max) {
     const long long npix = (long long)size * size;
-    const long long total = n_rows * p_pad;
-    const long long stride = (long long)gridDim.x * blockDim.x;
+    const int ns = (int)n_sel, pp = (int)p_pad;
     float amax = 0.f;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
-        const long long rr = i / p_pad, c = i - rr * p_pad;
-        double v = 0.;
-        if (c < n_sel) {
-            const long long r = row_begin + rr;
-            const long long s0 = r / num_rot, j = r - s0 * num_rot;
-            const int p = sel_pix[c];
-            const int x = p / size, y = p - (p / size) * size;
-            v = rot_log_value(holo + s0 * npix, x, y, size, rot_cs[2 * j], rot_cs[2 * j + 1],
-                              bg[p]);
+    for (long long rr = blockIdx.x; rr < n_rows; rr += gridDim.x) {
+        const long long r = row_begin + rr;
+        const long long s0 = r / num_rot, j = r - s0 * num_rot;
+        const double ac = rot_cs[2 * j], as = rot_cs[2 * j + 1];
+        const double *w = holo + s0 * npix;
+        TL *o = out + rr * p_pad;
+        for (int c = threadIdx.x; c < pp; c += blockDim.x) {
+            double v = 0.;
+            if (c < ns) {
+                const int p = sel_pix[c];
+                const int x = p / size, y = p - x * size;
+                v = rot_log_value(w, x, y, size, ac, as, bg[p]);
+            }
+            const TL q = (TL)v;
+            o[c] = q;
+            amax = fmaxf(amax, fabsf((float)q));
         }
-        const TL o = (TL)v;
-        out[i] = o;
-        amax = fmaxf(amax, fabsf((float)o));
     }
     if (abs_max) {
         // non-negative floats order like their bit patterns
@@ -127,7 +134,7 @@ extern "C" int rspi_rot_log_slices(const double *holo, long long n_states0, long
         return RSPI_ERR_ARG;
     const long long n_rows = row_end - row_begin;
     if (n_rows == 0) return RSPI_OK;
-    const unsigned blocks = rspi_blocks(n_rows * p_pad, 256, 16);
+    const unsigned blocks = (unsigned)std::min<long long>(n_rows, (long long)rspi_sm_count() * 64);
     if (out_dtype == 0)
         k_rot_log<float><<<blocks, 256, 0, stream>>>(holo, num_rot, rot_cs, (int)size, bg, sel_pix,
                                                      n_sel, p_pad, row_begin, n_rows,

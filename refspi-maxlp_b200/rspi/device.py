@@ -220,8 +220,8 @@ class EStep:
                  n_modes=1, dense_gemm='auto', dense_rescore=True):
         if form not in ('fp64', 'screen', 'dense'):
             raise ValueError('form must be fp64, screen or dense')
-        if kernel not in ('stream', 'dynamic'):
-            raise ValueError('kernel must be stream or dynamic')
+        if kernel not in ('stream', 'frame', 'wide', 'dynamic'):
+            raise ValueError('kernel must be stream, frame, wide or dynamic')
         self.kernel = kernel
         self.lib = load()
         self.form = form
@@ -265,6 +265,10 @@ class EStep:
         tmax = self.lib.rspi_loglike_max_tile(self.p_row, self.slice_code)
         if form == 'screen' and kernel == 'stream':
             tmax = 4 if tmax >= 4 else (2 if tmax >= 2 else tmax)   # interleaved: 1, 2 or 4
+        if form == 'screen' and kernel in ('frame', 'wide'):
+            tmax = min(tmax, 2)                                     # 1 or 2 rows per tile
+        if form != 'screen' and kernel in ('frame', 'wide'):
+            raise ValueError('the %s kernel is a screened-form kernel' % kernel)
         if tmax == 0:
             raise ValueError('a %d-pixel likelihood slice does not fit in shared memory' % self.n_sel)
         self.tile = int(states_per_tile or tmax)
@@ -272,6 +276,12 @@ class EStep:
             raise ValueError('states_per_tile %d exceeds the shared-memory limit %d' % (self.tile, tmax))
         if form == 'screen' and kernel == 'stream' and self.tile not in (1, 2, 4):
             raise ValueError('the interleaved screening kernel takes 1, 2 or 4 states per tile')
+        if form == 'screen':
+            # words (two 16-bit entry rows) per frame decide how many of a
+            # frame's words the frame-at-a-time kernel prefetches
+            wpf = self.ll16['total_rows'] / 2. / max(1, photons.num_data)
+            self.prefetch_words = 4 if wpf <= 5 else (8 if wpf <= 10 else 12)
+        self.wide = self._wide_entries() if (form == 'screen' and kernel == 'wide') else None
         self.warps, self.n_ctas = int(warps), int(n_ctas)
         esz = 4 if self.slice_code == 0 else 8
         rows = max(self.tile, (slice_budget_bytes // (self.p_row * esz)) // self.tile * self.tile)
@@ -376,6 +386,21 @@ class EStep:
         self.check_capacity = True
         self.ll_events = None
 
+    def _wide_entries(self):
+        """32-bit entries holding each photon's byte offset in the
+        interleaved tile (sel * 4 * tile), four rows of a lane per 16-byte
+        group, rows of a frame padded to a multiple of four."""
+        l16, n, dev, s = self.ll16, self.ph.num_data, self.device, cur_stream()
+        groups = torch.empty(n, dtype=_i32, device=dev)
+        call('rspi_wide_entry_groups', ptr(l16['row_off']), n, ptr(groups), s)
+        goff = torch.empty(n + 1, dtype=_i64, device=dev)
+        call('rspi_scan_rows', ptr(groups), n, ptr(goff), s)
+        total = int(goff[-1].item())
+        wide = torch.empty(max(1, total) * 128, dtype=torch.int32, device=dev)
+        call('rspi_wide_entry_fill', ptr(l16['entries']), ptr(l16['row_off']), n,
+             self.p_row - 32, self.tile, ptr(goff), ptr(wide), s)
+        return dict(entries=wide, group_off=goff, total_groups=total, tile=self.tile)
+
     def _alloc_row_scratch(self):
         """Global rows for FP64 rescoring when a row exceeds shared memory
         (one per SM; none otherwise)."""
@@ -457,6 +482,19 @@ class EStep:
             call('rspi_dense_loglike', ptr(dn['a0']), ptr(dn['a1']), ptr(self.lsl_hi),
                  ptr(self.lsl_lo), self.k_pad, n, self.chunk_rows, self.num_rot, r0, r1,
                  ptr(self.init), ptr(self.ph.scales), ptr(self.prob[r0]), n, ptr(self.ph.err.t),
+                 cur_stream())
+        elif self.kernel == 'wide' and self.form == 'screen':
+            if self.wide is None or self.wide['tile'] != self.tile:
+                self.wide = self._wide_entries()   # kernel or tile changed after set-up
+            call('rspi_screen_loglike4', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
+                 ptr(self.ph.scales), ptr(self.wide['entries']), ptr(self.wide['group_off']), n,
+                 r0, r1, ptr(self.prob[r0]), n, self.tile, self.warps, self.n_ctas,
+                 cur_stream())
+        elif self.kernel == 'frame' and self.form == 'screen':
+            l16 = self.ll16
+            call('rspi_screen_loglike3', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
+                 ptr(self.ph.scales), ptr(l16['entries']), ptr(l16['row_off']), n, r0, r1,
+                 ptr(self.prob[r0]), n, self.tile, self.prefetch_words, self.warps, self.n_ctas,
                  cur_stream())
         elif self.kernel == 'stream' and self.form == 'screen':
             l16 = self.ll16

@@ -42,6 +42,10 @@ SIGNATURES = {
                                            P]),
     'rspi_nll': (I, [I, I] + [P] * 7 + [L, P, L, P, L] + [P] * 18),
     'rspi_screen_loglike2': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
+    'rspi_screen_loglike3': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, I, P]),
+    'rspi_screen_loglike4': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
+    'rspi_wide_entry_groups': (I, [P, L, P, P]),
+    'rspi_wide_entry_fill': (I, [P, P, L, I, I, P, P, P]),
     'rspi_entries16_check': (I, [P, L, P, P]),
     'rspi_loglike_stream': (I, [I, P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
     'rspi_posterior_pairs': (I, [P, L, L, P, D, P, P, P, L, P, P, P, P, P]),
@@ -101,7 +105,8 @@ KERNELS_PER_CALL = {
     'rspi_entries16_check': 1, 'rspi_nll': 2, 'rspi_screen_candidates_noalloc': 3, 'rspi_merge_coverage': 1, 'rspi_merge': 2,
     'rspi_dense_frames': 1, 'rspi_rot_log_split': 1, 'rspi_dense_loglike': 1,
     'rspi_maxlp_grid': 2, 'rspi_dense_frames_u8': 1, 'rspi_rot_log_fixed': 1,
-    'rspi_dense_loglike_i8': 1,
+    'rspi_dense_loglike_i8': 1, 'rspi_screen_loglike3': 1, 'rspi_screen_loglike4': 1,
+    'rspi_wide_entry_groups': 1, 'rspi_wide_entry_fill': 1,
 }
 launch_count = 0
 

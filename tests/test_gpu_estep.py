@@ -263,3 +263,49 @@ def test_random_shapes_vs_oracle(size, n, seed, kw, form):
     _, rmax, _ = es.reduce()
     _, want_rmax = E.get_rmax(want)
     assert np.array_equal(rmax.cpu().numpy(), want_rmax)
+
+
+@pytest.mark.parametrize('tile,warps', [(1, 1), (2, 4), (2, 32), (1, 7), (2, 3)])
+@pytest.mark.parametrize('name,ds,need_scaling', CASES, ids=[c[0] for c in CASES])
+def test_frame_kernel_matches_stream_kernel(name, ds, need_scaling, tile, warps):
+    """The frame-at-a-time and wide-entry screening kernels give the interleaved kernel's
+    FP32 likelihoods (other summation order: within 1e-6 relative of the
+    largest term) on every case, empty and heavy frames included, and the
+    same FP64-rescored argmax / maximum / log-sum-exp."""
+    size = int(round(np.sqrt(ds['num_pix'])))
+    num_rot = 5
+    sx, sy, dia, _ = E.generate_states(E.parse_triple('-1 1 3'), E.parse_triple('0 0 1'),
+                                       E.parse_triple('2 3 2'))
+    rng = np.random.default_rng(size)
+    model = torch.from_numpy(rng.random(size * size) + 1j * rng.random(size * size)).cuda()
+    out = {}
+    for kernel in ('stream', 'frame', 'wide'):
+        ph = _photons(ds, need_scaling)
+        es = _estep(ph, size, num_rot, sx, sy, dia, ds['bg'], form='screen', kernel=kernel,
+                    states_per_tile=tile, warps=warps)
+        es.run(model)
+        maxll, rmax, logz = es.reduce()
+        torch.cuda.synchronize()
+        out[kernel] = (es.prob.cpu().numpy().astype(np.float64), maxll.cpu().numpy(),
+                       rmax.cpu().numpy(), logz.cpu().numpy())
+    a = out['stream']
+    scale = np.abs(a[0]).max(0, keepdims=True) + 1.
+    for b in (out['frame'], out['wide']):
+        assert np.all(np.abs(a[0] - b[0]) <= 1e-6 * scale)
+        assert np.array_equal(a[2], b[2])
+        np.testing.assert_allclose(a[1], b[1], rtol=1e-14)
+        np.testing.assert_allclose(a[3], b[3], rtol=1e-12)
+
+
+@pytest.mark.parametrize('kernel', ['frame', 'wide'])
+@pytest.mark.parametrize('name', GOLDEN_CASES)
+def test_frame_kernel_screened_form_matches_reference(name, kernel):
+    g = load_golden(name)
+    _, es = _golden_estep(g, form='screen', kernel=kernel)
+    for it in (1, 2):
+        es.run(torch.from_numpy(g['model_in_%d' % it]).cuda())
+        screened = es.prob.cpu().numpy().astype(np.float64)
+        want = g['prob_%d' % it]
+        assert (np.abs(screened - want) / np.abs(want)).max() <= RTOL_F32
+        _, rmax, _ = es.reduce()
+        assert np.array_equal(rmax.cpu().numpy(), g['rmax_%d' % it])

@@ -62,7 +62,8 @@ def parse_args():
     ap.add_argument('--frames', type=int, default=None, help='override frame count (testing)')
     ap.add_argument('--form', default=None, choices=['fp64', 'screen', 'dense'],
                     help='likelihood form (default: dense for config 5, screen otherwise)')
-    ap.add_argument('--kernel', default='stream', choices=['stream', 'frame', 'wide', 'dynamic'])
+    ap.add_argument('--kernel', default=None, choices=['stream', 'frame', 'wide', 'dynamic'],
+                    help='likelihood kernel (default: wide for the screened form, stream for FP64)')
     ap.add_argument('--slice-gb', type=float, default=8.,
                     help='largest rotated-slice chunk (GB); smaller values give more launches')
     ap.add_argument('--no-plain', action='store_true',
@@ -480,7 +481,7 @@ def run_ours(args):
     import io
     with contextlib.redirect_stdout(io.StringIO()):
         rec = EMC(cfgfile, device=dev)
-    if rec.estep.form != 'dense' and args.kernel != rec.estep.kernel:
+    if rec.estep.form != 'dense' and args.kernel and args.kernel != rec.estep.kernel:
         rec.estep.kernel = args.kernel
     model0 = start_model(args.config, w)
     stream = torch.cuda.current_stream()

@@ -492,11 +492,20 @@ k_screen_ll4(const float *__restrict__ lsl, int p_row, int num_rot,
             const int nb = min(PG, gend - g);
 #pragma unroll
             for (int k = 0; k < PG; ++k) nxt[k] = g + PG + k < gend ? __ldg(gp + 32 * (PG + k)) : z;
+            // gather phase without branches, so the shared loads of all PG
+            // groups are in flight together (groups past nb hold offset 0: a
+            // valid address whose values are never added)
+            Contrib<T> c0[PG], c1[PG];
+#pragma unroll
+            for (int k = 0; k < PG; ++k) {
+                c0[k] = gather_pair<T>(smem_raw, cur[k].x, cur[k].y);
+                c1[k] = gather_pair<T>(smem_raw, cur[k].z, cur[k].w);
+            }
 #pragma unroll
             for (int k = 0; k < PG; ++k) {
                 if (k < nb) {
-                    add_contrib<T>(a0, gather_pair<T>(smem_raw, cur[k].x, cur[k].y));
-                    add_contrib<T>(a1, gather_pair<T>(smem_raw, cur[k].z, cur[k].w));
+                    add_contrib<T>(a0, c0[k]);
+                    add_contrib<T>(a1, c1[k]);
                     if (g + k + 1 == fend) {
                         finish();
                         while (f < fe && fend == g + k + 1) finish();

@@ -1,8 +1,8 @@
 """Tile autotuner for the likelihood kernel (states per CTA x warps per CTA).
 
-For a given E-step (its form, slice row length and entry stream) the tuner
-times ``rspi_loglike_stream`` over a sample of likelihood rows for every
-(states_per_tile, warps_per_cta) that fits in shared memory, with CUDA
+For a given E-step (its form, kernel, slice row length and entry stream) the
+tuner times the E-step's likelihood kernel over a sample of likelihood rows
+for every (states_per_tile, warps_per_cta) that fits in shared memory, with CUDA
 events on the launching stream, and keeps the fastest.  Results are cached
 in a JSON file keyed by device name, form, slice row length, frame count and
 entry rows, so later runs of the same geometry skip the search.
@@ -12,7 +12,6 @@ import os
 
 import torch
 
-from .device import call, cur_stream, ptr
 
 CACHE = os.environ.get('RSPI_AUTOTUNE_CACHE',
                        os.path.join(os.path.expanduser('~'), '.cache', 'rspi_autotune.json'))
@@ -60,26 +59,22 @@ def tune(es, sample_tiles=2, repeats=2, use_cache=True, verbose=False):
         return (t, w, table[key]['ms_per_row']), None
     tmax = es.lib.rspi_loglike_max_tile(es.p_row, es.slice_code)
     screen2 = es.form == 'screen' and es.kernel == 'stream'
-    tiles = (1, 2, 4) if screen2 else TILES
+    if es.form == 'screen' and es.kernel in ('frame', 'wide'):
+        tiles = (1, 2)
+    else:
+        tiles = (1, 2, 4) if screen2 else TILES
     cands = [(t, w) for t in tiles if t <= tmax for w in WARPS
-             if screen2 or not (t > 2 and w > 16)]
+             if screen2 or es.form == 'screen' or not (t > 2 and w > 16)]
     sms = torch.cuda.get_device_properties(es.device).multi_processor_count
     rows = min(es.n_rows, es.chunk_rows, sms * sample_tiles * max(t for t, _ in cands))
     es.rot_slices(0, rows)
-    ent = es.ll if es.form == 'fp64' else es.ll16
     n = es.ph.num_data
     stream = torch.cuda.current_stream()
     results = []
     for t, w in cands:
         def run():
-            if screen2:
-                call('rspi_screen_loglike2', ptr(es.lsl), es.p_row, es.num_rot, ptr(es.init),
-                     ptr(es.ph.scales), ptr(ent['entries']), ptr(ent['row_off']), n, 0, rows,
-                     ptr(es.prob[0]), n, t, w, 0, cur_stream())
-            else:
-                call('rspi_loglike_stream', es.slice_code, ptr(es.lsl), es.p_row, es.num_rot,
-                     ptr(es.init), ptr(es.ph.scales), ptr(ent['entries']), ptr(ent['row_off']),
-                     n, 0, rows, ptr(es.prob[0]), n, t, w, 0, cur_stream())
+            es.tile, es.warps = t, w
+            es._loglike_launch(0, rows, es.lsl, n)
         run()
         a = torch.cuda.Event(enable_timing=True)
         b = torch.cuda.Event(enable_timing=True)

@@ -216,10 +216,12 @@ class EStep:
 
     def __init__(self, photons, size, num_rot, shiftx, shifty, sphere_dia, probmask, bg,
                  form='fp64', states_per_tile=None, warps=32, n_ctas=0,
-                 slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel='stream',
+                 slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel=None,
                  n_modes=1, dense_gemm='auto', dense_rescore=True):
         if form not in ('fp64', 'screen', 'dense'):
             raise ValueError('form must be fp64, screen or dense')
+        if kernel is None:   # default likelihood kernel of each form
+            kernel = 'wide' if form == 'screen' else 'stream'
         if kernel not in ('stream', 'frame', 'wide', 'dynamic'):
             raise ValueError('kernel must be stream, frame, wide or dynamic')
         self.kernel = kernel

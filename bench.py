@@ -64,6 +64,8 @@ def parse_args():
                     help='likelihood form (default: dense for config 5, screen otherwise)')
     ap.add_argument('--kernel', default=None, choices=['stream', 'frame', 'wide', 'dynamic'],
                     help='likelihood kernel (default: wide for the screened form, stream for FP64)')
+    ap.add_argument('--screen-slices', default='fp32', choices=['fp32', 'fp16'],
+                    help='screened form: FP32 slices (two rows per gather) or FP16 (four)')
     ap.add_argument('--slice-gb', type=float, default=8.,
                     help='largest rotated-slice chunk (GB); smaller values give more launches')
     ap.add_argument('--no-plain', action='store_true',
@@ -71,6 +73,8 @@ def parse_args():
     ap.add_argument('--cpu-seconds', type=float, default=20.,
                     help='target CPU time of the bounded oracle sample')
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-variants', action='store_true',
+                    help='skip timing the FP16-slice variant of the screened form')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-clocks', action='store_true', help='do not sample nvidia-smi clocks')
     ap.add_argument('--no-ref-gpu', action='store_true',
@@ -139,7 +143,8 @@ def dram_traffic(args, w, es, rows_per_launch):
     except (OSError, ValueError, KeyError):
         return None
     for c in caps:
-        if (c['form'] == es.form and c['config'] == args.config and c['frames'] == w['n'] and
+        if (c['form'] == es.form and c.get('kernel', 'stream') == es.kernel and
+                c['config'] == args.config and c['frames'] == w['n'] and
                 c['rows_per_launch'] == int(round(rows_per_launch))):
             return float(c['dram_bytes_read'] + c['dram_bytes_write'])
     return None
@@ -176,7 +181,7 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
                      'flops_per_launch': flops, 'algorithmic_bytes_per_launch': bytes_alg}, **common)
         return roof, None, rows_per_launch
     total_rows = es.ll16['total_rows'] if es.form == 'screen' else es.ll['total_rows']
-    esz = 4 if es.slice_code == 0 else 8
+    esz = {0: 4, 1: 8, 2: 2}[es.slice_code]
     osz = 4 if es.prob_code == 0 else 8
     # algorithmic bytes per launch = its slices in + its LL rows out + the
     # packed photon entries once
@@ -186,10 +191,14 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
     # on-chip gather roofline: one shared-memory value per entry slot per likelihood row
     gathers = rows_per_launch * total_rows * 32
     clk_mhz = (clk or {}).get('sm_mhz') or 1965.
-    lanes = 32 if es.slice_code == 0 else 16
+    # values a shared-memory wavefront (128 B per clock) carries
+    lanes = {0: 32, 1: 16, 2: 64}[es.slice_code]
     gather_peak = sm_count * lanes * clk_mhz * 1e6
     gather_rate = gathers / (ll_launch_ms * 1e-3)
-    roof = dict({'kernel': ('k_screen_ll2 (FP32 screening likelihood, row a7)'
+    names = {'stream': 'k_screen_ll2', 'frame': 'k_screen_ll3', 'wide': 'k_screen_ll4',
+             'wide16': 'k_screen_ll4h'}
+    roof = dict({'kernel': ('%s (%s screening likelihood, row a7)' %
+                            (names.get(es.kernel, es.kernel), 'FP16' if es.slice_code == 2 else 'FP32')
                             if es.form == 'screen' else 'k_ll_stream / k_loglike (FP64 likelihood, row a7)'),
                  'bound': 'hbm', 'achieved': achieved, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
                  'frac': achieved / pk['hbm_gbs'],
@@ -202,7 +211,7 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
     return roof, gather, rows_per_launch
 
 
-def write_inputs(tmp, w, data, form, slice_gb=8.):
+def write_inputs(tmp, w, data, form, slice_gb=8., screen_slices='fp32'):
     from rspi.photonfile import write_photons
     os.makedirs(os.path.join(tmp, 'out'), exist_ok=True)
     write_photons(os.path.join(tmp, 'photons.npz'), data)
@@ -211,9 +220,10 @@ def write_inputs(tmp, w, data, form, slice_gb=8.):
     with open(cfg, 'w') as f:
         f.write('[emc]\nsize = %d\nin_photons_file = photons.npz\noutput_folder = out/\n'
                 'log_file = out/EMC.log\nneed_scaling = True\nnum_rot = %d\nnum_modes = %d\n'
-                'sphere_dia = %s\nshiftx = %s\nshifty = %s\nform = %s\nslice_budget_gb = %g\n' %
+                'sphere_dia = %s\nshiftx = %s\nshifty = %s\nform = %s\nslice_budget_gb = %g\n'
+                'screen_slices = %s\n' %
                 (w['size'], r['num_rot'], w['n_modes'], r['sphere_dia'], r['shiftx'], r['shifty'],
-                 form, slice_gb))
+                 form, slice_gb, screen_slices))
     return cfg
 
 
@@ -475,7 +485,7 @@ def run_ours(args):
     data = generate_data(args.config, w, device=dev)
     t_gen = time.time() - t0
     tmp = tempfile.mkdtemp(prefix='rspi_bench_')
-    cfgfile = write_inputs(tmp, w, data, args.form, args.slice_gb)
+    cfgfile = write_inputs(tmp, w, data, args.form, args.slice_gb, args.screen_slices)
     from emc import EMC
     import contextlib
     import io
@@ -554,43 +564,59 @@ def run_ours(args):
                'd2h_bytes_per_step': 16 * p + 4 * w['n'],
                'api': 'EMC.run_iteration (model host->device, model + argmax device->host)'}
 
-    # the plain form: FP64 slices and likelihoods, warp-per-frame kernel
-    plain = None
-    if not args.no_plain and rank == 0:
+    # other forms on the same data, timed eagerly step by step: the plain form
+    # (FP64 slices and likelihoods, warp-per-frame kernel) and, for the
+    # screened form, its FP16-slice variant
+    plain = variant16 = None
+    if rank == 0 and (not args.no_plain or (es.form == 'screen' and es.slice_code == 0)):
         from rspi.device import EStep
         # the chosen form's likelihood matrix, slices, candidates and graph
-        # pool are released first: both matrices need not fit at once
+        # pool are released first: the matrices need not fit at once
         rec._graph = None
         rec.prob = None
         for name in ('prob', 'lsl', 'cand_d', 'cand_r', 'cand_ll', 'row_cand'):
             setattr(es, name, None)
         torch.cuda.empty_cache()
-        pe = EStep(rec.dset.photons, w['size'], w['num_rot'], rec.shiftx, rec.shifty,
-                   rec.sphere_dia, rec.probmask, rec.dset.bg.cpu().numpy(), form='fp64',
-                   kernel='dynamic', n_modes=w['n_modes'])
-        pmodel = torch.from_numpy(model0).to(dev)
 
-        def pstep():
-            pe.run(pmodel)
-            pe.reduce()
-            rec.phaser.run_from_rmax(pmodel, pe.rmax, w['num_rot'], rec.state_vals,
-                                     rec.phaser_rot)
-        for _ in range(min(args.warmup, 1)):
-            pstep()
-        torch.cuda.synchronize()
-        p0 = torch.cuda.Event(enable_timing=True)
-        p1 = torch.cuda.Event(enable_timing=True)
-        p0.record(stream)
-        for _ in range(args.steps):
-            pstep()
-        p1.record(stream)
-        torch.cuda.synchronize()
-        pms = p0.elapsed_time(p1) / args.steps
-        plain = {'form': 'fp64 slices + FP64 likelihood matrix, warp-per-frame kernel',
-                 'ms_per_step': pms, 'value': w['n'] * w['n_states'] / (pms * 1e-3),
-                 'speedup_of_chosen': pms / ms}
-        del pe
-        torch.cuda.empty_cache()
+        def time_form(**kw):
+            pe = EStep(rec.dset.photons, w['size'], w['num_rot'], rec.shiftx, rec.shifty,
+                       rec.sphere_dia, rec.probmask, rec.dset.bg.cpu().numpy(),
+                       n_modes=w['n_modes'], **kw)
+            pmodel = torch.from_numpy(model0).to(dev)
+
+            def pstep():
+                pe.run(pmodel)
+                pe.reduce()
+                rec.phaser.run_from_rmax(pmodel, pe.rmax, w['num_rot'], rec.state_vals,
+                                         rec.phaser_rot)
+            for _ in range(min(args.warmup, 1)):
+                pstep()
+            torch.cuda.synchronize()
+            p0 = torch.cuda.Event(enable_timing=True)
+            p1 = torch.cuda.Event(enable_timing=True)
+            p0.record(stream)
+            for _ in range(args.steps):
+                pstep()
+            p1.record(stream)
+            torch.cuda.synchronize()
+            pms = p0.elapsed_time(p1) / args.steps
+            cands = getattr(pe, 'n_candidates', None)
+            del pe
+            torch.cuda.empty_cache()
+            return pms, cands
+
+        if not args.no_plain:
+            pms, _ = time_form(form='fp64', kernel='dynamic')
+            plain = {'form': 'fp64 slices + FP64 likelihood matrix, warp-per-frame kernel',
+                     'ms_per_step': pms, 'value': w['n'] * w['n_states'] / (pms * 1e-3),
+                     'speedup_of_chosen': pms / ms}
+        if es.form == 'screen' and es.slice_code == 0 and not args.no_variants:
+            pms, cands = time_form(form='screen', screen_slices='fp16')
+            variant16 = {'form': 'screened, FP16 slices (four rows per gather), same FP64 '
+                                 'rescoring; LL entries outside the candidates carry up to '
+                                 '2^-11 |L| storage error per photon',
+                         'ms_per_step': pms, 'value': w['n'] * w['n_states'] / (pms * 1e-3),
+                         'candidates_rescored': cands, 'timing': 'eager steps (no graph)'}
 
     if rank != 0:
         if world > 1:
@@ -633,6 +659,7 @@ def run_ours(args):
         'clocks': clk,
         'e2e': e2e,
         'plain': plain,
+        'fp16_slices': variant16,
         'form': {'likelihood': args.form, 'kernel': es.kernel,
                  'candidates_rescored': n_cand},
         'cpu_baseline': cpu,

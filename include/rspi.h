@@ -110,7 +110,7 @@ int rspi_vscale_init(const double *msum, long long n_states0, const double *powd
  *   L[s0*num_rot + j][c] = log(bilinear(W[s0])(R(j)(p-cen)+cen) + bg[p]),
  *   -1000 outside the detector or below 1e-20; p = sel_pix[c].
  * rot_cs[2*j], rot_cs[2*j+1] = cos, sin of angle j (host table).
- * out_dtype 0 = float32, 1 = float64; rows are p_pad long, tail zeroed.
+ * out_dtype 0 = float32, 1 = float64, 2 = float16; rows are p_pad long, tail zeroed.
  * rows [row_begin, row_end) of the full S0*num_rot range are produced.
  * abs_max (nullable, float): raised to the largest |stored value| (the caller
  * zeroes it); it bounds the rounding error of the float32 form. */
@@ -235,6 +235,17 @@ int rspi_screen_loglike4(const float *lslices, long long p_row, long long num_ro
                          long long row_end, float *ll, long long ll_stride,
                          int states_per_tile, int warps_per_cta, int n_ctas,
                          cudaStream_t stream);
+
+/* Four likelihood rows per tile from FP16 rotated log-slices
+ * (rspi_rot_log_slices with out_dtype 2), the wide entries built for the
+ * FP32 two-row tile (offset sel * 8).  FP16 storage adds up to 2^-11 |L| per
+ * value; the caller's candidate threshold covers it by passing row offsets
+ * row_off16[d] + 8192 d to rspi_screen_candidates. */
+int rspi_screen_loglike4h(const void *lslices16, long long p_row, long long num_rot,
+                          const double *init, const double *scales, const unsigned *wide,
+                          const long long *group_off, long long n_data, long long row_begin,
+                          long long row_end, float *ll, long long ll_stride, int warps_per_cta,
+                          int n_ctas, cudaStream_t stream);
 
 /* *max_index = largest value in a 16-bit entry array. */
 int rspi_entries16_check(const unsigned short *entries, long long n_entries,

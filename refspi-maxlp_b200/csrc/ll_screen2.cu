@@ -10,6 +10,8 @@
 // pipeline (rspi_entries16_check), so the hot loop has no clamp.  Each warp
 // streams a contiguous, word-balanced range of frames with a prefetch that
 // crosses frame boundaries; loop indices are 32-bit.
+#include <cuda_fp16.h>
+
 #include "rspi_common.cuh"
 
 namespace {
@@ -520,6 +522,124 @@ k_screen_ll4(const float *__restrict__ lsl, int p_row, int num_rot,
     }
 }
 
+// FP16 slices, four rows per tile: the interleaved tile holds sl[c][0..3] as
+// halves (8 bytes per pixel), so one 8-byte gather brings four rows' values
+// of a photon -- twice the rows per shared-memory wavefront of the FP32
+// two-row tile -- and they are widened to FP32 before the packed FP32 adds.
+// The wide entries are those of the FP32 two-row tile (offset sel * 8).
+__device__ __forceinline__ void gather4h(const unsigned char *sl, unsigned a, unsigned b,
+                                         float2 &lo, float2 &hi) {
+    const uint2 va = *reinterpret_cast<const uint2 *>(sl + a);
+    const uint2 vb = *reinterpret_cast<const uint2 *>(sl + b);
+    const float2 a01 = __half22float2(*reinterpret_cast<const __half2 *>(&va.x));
+    const float2 a23 = __half22float2(*reinterpret_cast<const __half2 *>(&va.y));
+    const float2 b01 = __half22float2(*reinterpret_cast<const __half2 *>(&vb.x));
+    const float2 b23 = __half22float2(*reinterpret_cast<const __half2 *>(&vb.y));
+    lo = __fadd2_rn(a01, b01);
+    hi = __fadd2_rn(a23, b23);
+}
+
+__global__ void __launch_bounds__(1024)
+k_screen_ll4h(const __half *__restrict__ lsl, int p_row, int num_rot,
+              const double *__restrict__ init, const double *__restrict__ scales,
+              const uint4 *__restrict__ groups, const long long *__restrict__ goff, int n_data,
+              long long row_begin, long long row_end, float *__restrict__ ll,
+              long long ll_stride) {
+    constexpr int T = 4, PG = 4;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __half *slh = reinterpret_cast<__half *>(smem_raw);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const long long n_tiles = (row_end - row_begin + T - 1) / T;
+    const int gtot = (int)goff[n_data];
+    auto lower = [&](int target) {
+        int lo = 0, hi = n_data;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((int)goff[mid] < target) lo = mid + 1;
+            else hi = mid;
+        }
+        return lo;
+    };
+    const int fb = wid == 0 ? 0 : lower((int)((long long)gtot * wid / nw));
+    const int fe = wid == nw - 1 ? n_data : lower((int)((long long)gtot * (wid + 1) / nw));
+    const __half hz = __float2half(0.f);
+
+    for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const long long first = row_begin + tile * T;
+        const int nt = (int)min((long long)T, row_end - first);
+        __syncthreads();
+        const __half *src = lsl + (first - row_begin) * (long long)p_row;
+        for (int i = threadIdx.x; i < T * p_row; i += blockDim.x) {
+            const int t = i / p_row, c = i - t * p_row;
+            slh[c * T + t] = t < nt ? src[i] : hz;
+        }
+        __syncthreads();
+        if (fb >= fe) continue;
+
+        const int my_t = lane & (T - 1);
+        const double my_init = my_t < nt ? init[(first + my_t) / num_rot] : 0.;
+        float *my_ll = ll + (first + my_t - row_begin) * ll_stride;
+        Acc<T> a0;
+        a0.zero();
+        int base = fb;
+        int my_end = fb + lane < n_data ? (int)goff[fb + lane + 1] : 0x7fffffff;
+        double my_scale = fb + lane < n_data ? scales[fb + lane] : 0.;
+        int f = fb;
+        int g = (int)goff[fb];
+        const int gend = (int)goff[fe];
+        int fend = __shfl_sync(RSPI_FULL_MASK, my_end, 0);
+        auto finish = [&]() {
+            const float tot = reduce_scatter<T>(a0, lane);
+            const double sc = __shfl_sync(RSPI_FULL_MASK, my_scale, f - base);
+            if (lane < nt) my_ll[f] = (float)(my_init * sc + (double)tot);
+            a0.zero();
+            ++f;
+            if (f - base == 32) {
+                base = f;
+                my_end = f + lane < n_data ? (int)goff[f + lane + 1] : 0x7fffffff;
+                my_scale = f + lane < n_data ? scales[f + lane] : 0.;
+            }
+            fend = f < fe ? __shfl_sync(RSPI_FULL_MASK, my_end, f - base) : gend + 1;
+        };
+        while (f < fe && fend == g) finish();
+
+        const uint4 *gp = groups + (long long)g * 32 + lane;
+        uint4 cur[PG], nxt[PG];
+        const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+#pragma unroll
+        for (int k = 0; k < PG; ++k) cur[k] = g + k < gend ? __ldg(gp + 32 * k) : z;
+        while (g < gend) {
+            const int nb = min(PG, gend - g);
+#pragma unroll
+            for (int k = 0; k < PG; ++k) nxt[k] = g + PG + k < gend ? __ldg(gp + 32 * (PG + k)) : z;
+            // a group's four photons summed per row pair before the adds
+            Contrib<T> c[PG];
+#pragma unroll
+            for (int k = 0; k < PG; ++k) {
+                float2 l0, h0, l1, h1;
+                gather4h(smem_raw, cur[k].x, cur[k].y, l0, h0);
+                gather4h(smem_raw, cur[k].z, cur[k].w, l1, h1);
+                c[k].p[0] = __fadd2_rn(l0, l1);
+                c[k].p[1] = __fadd2_rn(h0, h1);
+            }
+#pragma unroll
+            for (int k = 0; k < PG; ++k) {
+                if (k < nb) {
+                    add_contrib<T>(a0, c[k]);
+                    if (g + k + 1 == fend) {
+                        finish();
+                        while (f < fe && fend == g + k + 1) finish();
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < PG; ++k) cur[k] = nxt[k];
+            g += PG;
+            gp += 32 * PG;
+        }
+    }
+}
+
 template <int T>
 int launch4(const float *lsl, long long p_row, long long num_rot, const double *init,
             const double *scales, const uint4 *groups, const long long *goff, long long n_data,
@@ -701,4 +821,41 @@ extern "C" int rspi_screen_loglike4(const float *lslices, long long p_row, long 
         return launch4<2>(lslices, p_row, num_rot, init, scales, g, group_off, n_data, row_begin,
                           row_end, ll, ll_stride, warps_per_cta, n_ctas, stream);
     return RSPI_ERR_ARG;
+}
+
+extern "C" int rspi_screen_loglike4h(const void *lslices16, long long p_row, long long num_rot,
+                                     const double *init, const double *scales,
+                                     const unsigned *wide, const long long *group_off,
+                                     long long n_data, long long row_begin, long long row_end,
+                                     float *ll, long long ll_stride, int warps_per_cta,
+                                     int n_ctas, cudaStream_t stream) {
+    if (!lslices16 || !init || !scales || !wide || !group_off || !ll || n_data <= 0 ||
+        n_data > 0x7fffffffLL || p_row <= 32 || p_row % 32 || p_row > 65536 || num_rot <= 0 ||
+        num_rot > 0x7fffffffLL || row_begin < 0 || row_end < row_begin || ll_stride < n_data ||
+        warps_per_cta < 1 || warps_per_cta > 32)
+        return RSPI_ERR_ARG;
+    if ((reinterpret_cast<uintptr_t>(lslices16) & 15) != 0 ||
+        (reinterpret_cast<uintptr_t>(wide) & 15) != 0)
+        return RSPI_ERR_ARG;
+    if (row_end == row_begin) return RSPI_OK;
+    const size_t smem = (size_t)4 * p_row * sizeof(__half);
+    if (smem > (size_t)SMEM_LIMIT - 1024) return RSPI_ERR_ARG;
+    static size_t smem_set = 0;
+    if (smem > smem_set) {
+        if (cudaFuncSetAttribute(k_screen_ll4h, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return RSPI_ERR_CUDA;
+        smem_set = smem;
+    }
+    const long long n_tiles = (row_end - row_begin + 3) / 4;
+    if (n_ctas <= 0) {
+        const int per_sm = max(1, (int)(SMEM_LIMIT / (smem + 1024)));
+        n_ctas = rspi_sm_count() * min(per_sm, max(1, 2048 / (warps_per_cta * 32)));
+    }
+    if (n_ctas > n_tiles) n_ctas = (int)n_tiles;
+    k_screen_ll4h<<<n_ctas, warps_per_cta * 32, smem, stream>>>(
+        (const __half *)lslices16, (int)p_row, (int)num_rot, init, scales,
+        reinterpret_cast<const uint4 *>(wide), group_off, (int)n_data, row_begin, row_end, ll,
+        ll_stride);
+    RSPI_RETURN_LAUNCH();
 }

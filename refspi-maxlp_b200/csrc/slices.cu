@@ -4,6 +4,8 @@
 // are stored as float32 or float64.
 #include <algorithm>
 
+#include <cuda_fp16.h>
+
 #include "rspi_common.cuh"
 
 namespace {
@@ -89,9 +91,9 @@ k_rot_log(const double *__restrict__ holo, long long num_rot, const double *__re
                 const int x = p / size, y = p - x * size;
                 v = rot_log_value(w, x, y, size, ac, as, bg[p]);
             }
-            const TL q = (TL)v;
+            const TL q = static_cast<TL>(v);
             o[c] = q;
-            amax = fmaxf(amax, fabsf((float)q));
+            amax = fmaxf(amax, fabsf(static_cast<float>(q)));
         }
     }
     if (abs_max) {
@@ -139,6 +141,10 @@ extern "C" int rspi_rot_log_slices(const double *holo, long long n_states0, long
         k_rot_log<float><<<blocks, 256, 0, stream>>>(holo, num_rot, rot_cs, (int)size, bg, sel_pix,
                                                      n_sel, p_pad, row_begin, n_rows,
                                                      (float *)lslices, abs_max);
+    else if (out_dtype == 2)
+        k_rot_log<__half><<<blocks, 256, 0, stream>>>(holo, num_rot, rot_cs, (int)size, bg,
+                                                      sel_pix, n_sel, p_pad, row_begin, n_rows,
+                                                      (__half *)lslices, abs_max);
     else if (out_dtype == 1)
         k_rot_log<double><<<blocks, 256, 0, stream>>>(holo, num_rot, rot_cs, (int)size, bg,
                                                       sel_pix, n_sel, p_pad, row_begin, n_rows,

@@ -17,7 +17,8 @@ mass, same argmax/maximum/log-sum-exp as ``fp64``; ``dense``: frames stored
 densely, likelihood as a tensor-core GEMM, ``dense_gemm`` = ``auto`` /
 ``i8`` (exact fixed point) / ``bf16`` (hi + lo split), ``dense_rescore``
 (default true: FP64 rescoring of the candidates as in ``screen``)),
-``screen_delta``
+``screen_slices`` (``fp32``, or ``fp16``: half-precision slices, four
+likelihood rows per gather, a wider candidate threshold), ``screen_delta``
 (default 20 nats), ``states_per_tile``, ``warps_per_cta``, ``phaser_iter``
 (default 10, maxLP.py:320,335), ``slice_budget_gb`` (rotated slices are built
 in chunks of at most this size, default 8), ``cuda_graph`` (capture the whole
@@ -84,7 +85,7 @@ class EMC():
                            delta=self.screen_delta,
                            slice_budget_bytes=int(self.slice_budget_gb * (1 << 30)),
                            n_modes=self.num_modes, dense_gemm=self.dense_gemm,
-                           dense_rescore=self.dense_rescore)
+                           dense_rescore=self.dense_rescore, screen_slices=self.screen_slices)
         self.prob = self.estep.prob
         self.state_vals = torch.from_numpy(self._state_values).to(self.device)
         self.phaser_rot = torch.from_numpy(geometry.phaser_rotation_table(
@@ -121,6 +122,7 @@ class EMC():
         self.use_graph = config.getboolean('emc', 'cuda_graph', fallback=True)
         self.dense_gemm = config.get('emc', 'dense_gemm', fallback='auto')
         self.dense_rescore = config.getboolean('emc', 'dense_rescore', fallback=True)
+        self.screen_slices = config.get('emc', 'screen_slices', fallback='fp32')
         self.autotune = config.getboolean('emc', 'autotune', fallback=False)
 
     def _generate_states(self, config):

@@ -217,12 +217,16 @@ class EStep:
     def __init__(self, photons, size, num_rot, shiftx, shifty, sphere_dia, probmask, bg,
                  form='fp64', states_per_tile=None, warps=32, n_ctas=0,
                  slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel=None,
-                 n_modes=1, dense_gemm='auto', dense_rescore=True):
+                 n_modes=1, dense_gemm='auto', dense_rescore=True, screen_slices='fp32'):
         if form not in ('fp64', 'screen', 'dense'):
             raise ValueError('form must be fp64, screen or dense')
         if kernel is None:   # default likelihood kernel of each form
             kernel = 'wide' if form == 'screen' else 'stream'
-        if kernel not in ('stream', 'frame', 'wide', 'dynamic'):
+        if screen_slices not in ('fp32', 'fp16'):
+            raise ValueError('screen_slices must be fp32 or fp16')
+        if form == 'screen' and screen_slices == 'fp16':
+            kernel = 'wide16'   # the FP16-slice kernel: four rows per tile
+        if kernel not in ('stream', 'frame', 'wide', 'wide16', 'dynamic'):
             raise ValueError('kernel must be stream, frame, wide or dynamic')
         self.kernel = kernel
         self.lib = load()
@@ -256,20 +260,23 @@ class EStep:
         if form == 'fp64':
             self.slice_code, self.prob_code, self.p_row = 1, 1, self.p_pad
         else:
-            self.slice_code, self.prob_code = 0, 0
+            # FP32 slices (code 0), or FP16 slices (code 2) for the four-row kernel
+            self.slice_code, self.prob_code = (2 if kernel == 'wide16' else 0), 0
             self.p_row = self.p_pad + 32           # 32 zero columns for padding slots
             if self.p_row > 65536:
                 raise ValueError('screened form needs at most 65504 likelihood pixels')
             self.ll16 = photons.ll16_entries(self.pix2sel, self.p_row - 32)
             self.delta = float(delta)
-        self.slice_torch = torch.float32 if self.slice_code == 0 else _f64
+        self.slice_torch = {0: torch.float32, 1: _f64, 2: torch.float16}[self.slice_code]
         self.prob_torch = torch.float32 if self.prob_code == 0 else _f64
         tmax = self.lib.rspi_loglike_max_tile(self.p_row, self.slice_code)
+        if kernel == 'wide16':
+            tmax = 4 if self.p_row * 8 <= 226 * 1024 else 0
         if form == 'screen' and kernel == 'stream':
             tmax = 4 if tmax >= 4 else (2 if tmax >= 2 else tmax)   # interleaved: 1, 2 or 4
         if form == 'screen' and kernel in ('frame', 'wide'):
             tmax = min(tmax, 2)                                     # 1 or 2 rows per tile
-        if form != 'screen' and kernel in ('frame', 'wide'):
+        if form != 'screen' and kernel in ('frame', 'wide', 'wide16'):
             raise ValueError('the %s kernel is a screened-form kernel' % kernel)
         if tmax == 0:
             raise ValueError('a %d-pixel likelihood slice does not fit in shared memory' % self.n_sel)
@@ -283,9 +290,17 @@ class EStep:
             # frame's words the frame-at-a-time kernel prefetches
             wpf = self.ll16['total_rows'] / 2. / max(1, photons.num_data)
             self.prefetch_words = 4 if wpf <= 5 else (8 if wpf <= 10 else 12)
-        self.wide = self._wide_entries() if (form == 'screen' and kernel == 'wide') else None
+        if kernel == 'wide16' and self.tile != 4:
+            raise ValueError('the FP16-slice kernel takes 4 states per tile')
+        self.wide = self._wide_entries() if (form == 'screen' and kernel in ('wide', 'wide16')) \
+            else None
+        if kernel == 'wide16':
+            # FP16 storage error <= 2^-11 |L| per value: 8192 more FP32 rounding
+            # steps (2^-24) per photon in the candidate threshold's eps_d
+            self.row_off_eps = self.ll16['row_off'] + 8192 * torch.arange(
+                n + 1, dtype=_i64, device=dev)
         self.warps, self.n_ctas = int(warps), int(n_ctas)
-        esz = 4 if self.slice_code == 0 else 8
+        esz = {0: 4, 1: 8, 2: 2}[self.slice_code]
         rows = max(self.tile, (slice_budget_bytes // (self.p_row * esz)) // self.tile * self.tile)
         self.chunk_rows = int(min(self.n_rows, rows))
         self.holo = torch.empty((self.n_states0, self.size ** 2), dtype=_f64, device=dev)
@@ -388,6 +403,11 @@ class EStep:
         self.check_capacity = True
         self.ll_events = None
 
+    def _wide_bytes_tile(self):
+        """Tile whose entries the kernel reads: offsets sel * 8 serve both the
+        FP32 two-row and the FP16 four-row tiles."""
+        return 2 if self.kernel == 'wide16' else self.tile
+
     def _wide_entries(self):
         """32-bit entries holding each photon's byte offset in the
         interleaved tile (sel * 4 * tile), four rows of a lane per 16-byte
@@ -400,8 +420,9 @@ class EStep:
         total = int(goff[-1].item())
         wide = torch.empty(max(1, total) * 128, dtype=torch.int32, device=dev)
         call('rspi_wide_entry_fill', ptr(l16['entries']), ptr(l16['row_off']), n,
-             self.p_row - 32, self.tile, ptr(goff), ptr(wide), s)
-        return dict(entries=wide, group_off=goff, total_groups=total, tile=self.tile)
+             self.p_row - 32, self._wide_bytes_tile(), ptr(goff), ptr(wide), s)
+        return dict(entries=wide, group_off=goff, total_groups=total,
+                    tile=self._wide_bytes_tile())
 
     def _alloc_row_scratch(self):
         """Global rows for FP64 rescoring when a row exceeds shared memory
@@ -438,7 +459,12 @@ class EStep:
         call('rspi_vscale_init', ptr(self.msum), self.n_states0, ptr(self.ph.powder),
              ptr(self.sel_pix), self.n_sel, ptr(self.vscale), ptr(self.init), s)
         if self.form != 'fp64':
-            self.lmax.zero_()
+            # the FP16 bound needs |L| >= 2^-14 (below it the absolute error
+            # 2^-25 is covered by 2^-11 * 2^-14)
+            if self.kernel == 'wide16':
+                self.lmax.fill_(2. ** -14)
+            else:
+                self.lmax.zero_()
 
     def rot_slices(self, r0, r1, out=None):
         """a6: rotated log-slices of rows [r0, r1) into ``out`` (or the chunk buffer)."""
@@ -485,6 +511,10 @@ class EStep:
                  ptr(self.lsl_lo), self.k_pad, n, self.chunk_rows, self.num_rot, r0, r1,
                  ptr(self.init), ptr(self.ph.scales), ptr(self.prob[r0]), n, ptr(self.ph.err.t),
                  cur_stream())
+        elif self.kernel == 'wide16' and self.form == 'screen':
+            call('rspi_screen_loglike4h', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
+                 ptr(self.ph.scales), ptr(self.wide['entries']), ptr(self.wide['group_off']), n,
+                 r0, r1, ptr(self.prob[r0]), n, self.warps, self.n_ctas, cur_stream())
         elif self.kernel == 'wide' and self.form == 'screen':
             if self.wide is None or self.wide['tile'] != self.tile:
                 self.wide = self._wide_entries()   # kernel or tile changed after set-up
@@ -543,7 +573,8 @@ class EStep:
              ptr(self.rmax32), None, s)
         while True:
             dense = self.form == 'dense'
-            rows_eq = self.eq_row_off if dense else self.ll16['row_off']
+            rows_eq = self.eq_row_off if dense else (
+                self.row_off_eps if self.kernel == 'wide16' else self.ll16['row_off'])
             call('rspi_screen_candidates', ptr(self.prob), self.n_rows, n, ptr(self.max32),
                  ptr(self.rmax32), ptr(self.ll['frame_sel_photons']), ptr(rows_eq),
                  ptr(self.lmax_eps if dense else self.lmax),

@@ -309,3 +309,45 @@ def test_frame_kernel_screened_form_matches_reference(name, kernel):
         assert (np.abs(screened - want) / np.abs(want)).max() <= RTOL_F32
         _, rmax, _ = es.reduce()
         assert np.array_equal(rmax.cpu().numpy(), g['rmax_%d' % it])
+
+
+@pytest.mark.parametrize('name,ds,need_scaling', CASES, ids=[c[0] for c in CASES])
+def test_fp16_slices_same_rescored_results(name, ds, need_scaling):
+    """FP16 slices (four rows per gather): the screening values within their
+    stated bound of the FP32 ones, and after FP64 rescoring the same argmax,
+    maximum and log-sum-exp as the FP32-slice screened form."""
+    size = int(round(np.sqrt(ds['num_pix'])))
+    num_rot = 5
+    sx, sy, dia, _ = E.generate_states(E.parse_triple('-1 1 3'), E.parse_triple('0 0 1'),
+                                       E.parse_triple('2 3 2'))
+    rng = np.random.default_rng(size + 1)
+    model = torch.from_numpy(rng.random(size * size) + 1j * rng.random(size * size)).cuda()
+    out = {}
+    for sl in ('fp32', 'fp16'):
+        ph = _photons(ds, need_scaling)
+        es = _estep(ph, size, num_rot, sx, sy, dia, ds['bg'], form='screen', screen_slices=sl)
+        es.run(model)
+        maxll, rmax, logz = es.reduce()
+        torch.cuda.synchronize()
+        out[sl] = (es.prob.cpu().numpy().astype(np.float64), maxll.cpu().numpy(),
+                   rmax.cpu().numpy(), logz.cpu().numpy(), float(es.lmax.item()))
+        if sl == 'fp16':
+            assert es.tile == 4 and es.kernel == 'wide16'
+            phot = es.ll['frame_sel_photons'].cpu().numpy().astype(np.float64)
+    a, b = out['fp32'], out['fp16']
+    # FP16 storage: |dL| <= 2^-11 lmax per photon, plus FP32 sums
+    bound = 2. ** -11 * b[4] * phot[None, :] + 1e-5 * (np.abs(a[0]) + 1.)
+    assert np.all(np.abs(a[0] - b[0]) <= bound)
+    assert np.array_equal(a[2], b[2])
+    np.testing.assert_allclose(a[1], b[1], rtol=1e-14)
+    np.testing.assert_allclose(a[3], b[3], rtol=1e-9)
+
+
+@pytest.mark.parametrize('name', GOLDEN_CASES)
+def test_fp16_slices_match_reference(name):
+    g = load_golden(name)
+    _, es = _golden_estep(g, form='screen', screen_slices='fp16')
+    for it in (1, 2):
+        es.run(torch.from_numpy(g['model_in_%d' % it]).cuda())
+        _, rmax, _ = es.reduce()
+        assert np.array_equal(rmax.cpu().numpy(), g['rmax_%d' % it])

@@ -73,8 +73,6 @@ def parse_args():
     ap.add_argument('--cpu-seconds', type=float, default=20.,
                     help='target CPU time of the bounded oracle sample')
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    ap.add_argument('--no-variants', action='store_true',
-                    help='skip timing the FP16-slice variant of the screened form')
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-clocks', action='store_true', help='do not sample nvidia-smi clocks')
     ap.add_argument('--no-ref-gpu', action='store_true',
@@ -136,7 +134,7 @@ def dram_traffic(args, w, es, rows_per_launch):
     """DRAM bytes (read + write) of one likelihood launch from the committed
     ncu capture of the same workload (form, configuration, frames, rows per
     launch), or None when no capture matches."""
-    path = os.path.join(REPO, 'profiles', 'k_screen_ll2_config2_dram.json')
+    path = os.path.join(REPO, 'profiles', 'k_screen_config2_dram.json')
     try:
         with open(path) as f:
             caps = json.load(f)['captures']
@@ -564,11 +562,10 @@ def run_ours(args):
                'd2h_bytes_per_step': 16 * p + 4 * w['n'],
                'api': 'EMC.run_iteration (model host->device, model + argmax device->host)'}
 
-    # other forms on the same data, timed eagerly step by step: the plain form
-    # (FP64 slices and likelihoods, warp-per-frame kernel) and, for the
-    # screened form, its FP16-slice variant
-    plain = variant16 = None
-    if rank == 0 and (not args.no_plain or (es.form == 'screen' and es.slice_code == 0)):
+    # the plain form on the same data, timed eagerly step by step (FP64
+    # slices and likelihoods, warp-per-frame kernel)
+    plain = None
+    if rank == 0 and not args.no_plain:
         from rspi.device import EStep
         # the chosen form's likelihood matrix, slices, candidates and graph
         # pool are released first: the matrices need not fit at once
@@ -605,18 +602,10 @@ def run_ours(args):
             torch.cuda.empty_cache()
             return pms, cands
 
-        if not args.no_plain:
-            pms, _ = time_form(form='fp64', kernel='dynamic')
-            plain = {'form': 'fp64 slices + FP64 likelihood matrix, warp-per-frame kernel',
-                     'ms_per_step': pms, 'value': w['n'] * w['n_states'] / (pms * 1e-3),
-                     'speedup_of_chosen': pms / ms}
-        if es.form == 'screen' and es.slice_code == 0 and not args.no_variants:
-            pms, cands = time_form(form='screen', screen_slices='fp16')
-            variant16 = {'form': 'screened, FP16 slices (four rows per gather), same FP64 '
-                                 'rescoring; LL entries outside the candidates carry up to '
-                                 '2^-11 |L| storage error per photon',
-                         'ms_per_step': pms, 'value': w['n'] * w['n_states'] / (pms * 1e-3),
-                         'candidates_rescored': cands, 'timing': 'eager steps (no graph)'}
+        pms, _ = time_form(form='fp64', kernel='dynamic')
+        plain = {'form': 'fp64 slices + FP64 likelihood matrix, warp-per-frame kernel',
+                 'ms_per_step': pms, 'value': w['n'] * w['n_states'] / (pms * 1e-3),
+                 'speedup_of_chosen': pms / ms}
 
     if rank != 0:
         if world > 1:
@@ -659,7 +648,6 @@ def run_ours(args):
         'clocks': clk,
         'e2e': e2e,
         'plain': plain,
-        'fp16_slices': variant16,
         'form': {'likelihood': args.form, 'kernel': es.kernel,
                  'candidates_rescored': n_cand},
         'cpu_baseline': cpu,

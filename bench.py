@@ -66,6 +66,8 @@ def parse_args():
                     help='likelihood kernel (default: wide for the screened form, stream for FP64)')
     ap.add_argument('--screen-slices', default='fp32', choices=['fp32', 'fp16'],
                     help='screened form: FP32 slices (two rows per gather) or FP16 (four)')
+    ap.add_argument('--no-phaser-screen', action='store_true',
+                    help='pattern search: every candidate in FP64 (no FP32 screening pass)')
     ap.add_argument('--slice-gb', type=float, default=8.,
                     help='largest rotated-slice chunk (GB); smaller values give more launches')
     ap.add_argument('--no-plain', action='store_true',
@@ -491,6 +493,8 @@ def run_ours(args):
         rec = EMC(cfgfile, device=dev)
     if rec.estep.form != 'dense' and args.kernel and args.kernel != rec.estep.kernel:
         rec.estep.kernel = args.kernel
+    if args.no_phaser_screen:
+        rec.phaser.mstep.screen = False
     model0 = start_model(args.config, w)
     stream = torch.cuda.current_stream()
 
@@ -536,13 +540,19 @@ def run_ours(args):
         dist.barrier()
 
     n_cand = getattr(rec.estep, 'n_candidates', None)
+    ps = rec.phaser.mstep.stats.cpu().tolist()
+    phaser_form = {'screen': rec.phaser.mstep.screen, 'iterations_screened': ps[0],
+                   'iterations_fp64': ps[1], 'finalists': ps[2]}
     mem_gb = torch.cuda.max_memory_allocated(dev) / 1e9
 
     # e2e through the public API: host model in, host model + argmax out
     e2e = None
     if not args.no_e2e:
+        # the same iterations as the device-timed loop: from the start model,
+        # W untimed iterations, then K timed (the M-step's pattern search
+        # depends on the model, so each iteration's work differs)
         rec.model = model0.copy().reshape(rec._model_shape())
-        for _ in range(min(args.warmup, 1)):
+        for _ in range(args.warmup):
             rec.run_iteration(None)
         torch.cuda.synchronize()
         if world > 1:
@@ -602,8 +612,13 @@ def run_ours(args):
             torch.cuda.empty_cache()
             return pms, cands
 
+        # the plain form searches every pattern candidate in FP64 as well
+        screen0 = rec.phaser.mstep.screen
+        rec.phaser.mstep.screen = False
         pms, _ = time_form(form='fp64', kernel='dynamic')
-        plain = {'form': 'fp64 slices + FP64 likelihood matrix, warp-per-frame kernel',
+        rec.phaser.mstep.screen = screen0
+        plain = {'form': 'fp64 slices + FP64 likelihood matrix, warp-per-frame kernel, '
+                         'FP64 pattern search',
                  'ms_per_step': pms, 'value': w['n'] * w['n_states'] / (pms * 1e-3),
                  'speedup_of_chosen': pms / ms}
 
@@ -649,7 +664,7 @@ def run_ours(args):
         'e2e': e2e,
         'plain': plain,
         'form': {'likelihood': args.form, 'kernel': es.kernel,
-                 'candidates_rescored': n_cand},
+                 'candidates_rescored': n_cand, 'pattern_search': phaser_form},
         'cpu_baseline': cpu,
         'setup_s': {'generate': t_gen},
         'device_memory_gb': mem_gb,

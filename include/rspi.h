@@ -226,6 +226,22 @@ int rspi_wide_entry_fill(const unsigned short *entries16, const long long *row_o
                          long long n_data, int p_zero, int states_per_tile,
                          const long long *group_off, unsigned *wide, cudaStream_t stream);
 
+/* The same wide entries in the bank-class layout: a photon at tile column
+ * sel (byte offset sel * 4 * states_per_tile) has shared-memory bank class
+ * sel mod C, C = 32 / states_per_tile, and goes to a lane l with
+ * l mod C == its class (the k-th photon of class c: lane c + C (k mod 32/C),
+ * slot k / (32/C)); the other slots hold the lane's zero column.  Every
+ * gather instruction of the likelihood kernels then touches distinct bank
+ * classes.  A frame takes ceil(max_c n_c / (4 * 32/C)) groups (n_c: its
+ * photons of class c); the photons of a frame are summed in another order
+ * than with rspi_wide_entry_fill, within the same FP32 error bound. */
+int rspi_wide_entry_groups_banked(const unsigned short *entries16, const long long *row_off16,
+                                  long long n_data, int p_zero, int states_per_tile,
+                                  int *groups, cudaStream_t stream);
+int rspi_wide_entry_fill_banked(const unsigned short *entries16, const long long *row_off16,
+                                long long n_data, int p_zero, int states_per_tile,
+                                const long long *group_off, unsigned *wide, cudaStream_t stream);
+
 /* The same likelihoods as rspi_screen_loglike2 (1 or 2 states per tile) from
  * the wide entries built for that tile size: one 16-byte load per four
  * photons of a lane and no per-photon index arithmetic. */
@@ -387,6 +403,30 @@ int rspi_maxlp_pattern(double *fconv, const int *pixels, const int *hist_row,
                        const int *nstate, long long n_modes, const double *ref_params,
                        long long size, int rescale_mode, const double *rescale,
                        int num_iter, double *rescale_out, cudaStream_t stream);
+
+/* rspi_maxlp_pattern with an FP32 screening pass per iteration: every
+ * candidate is first evaluated in FP32 with a rigorous bound on its distance
+ * from the FP64 value; only the candidates that can still be the argmax
+ * (the finalists) are evaluated in FP64, in the same order and with the same
+ * roundings as rspi_maxlp_pattern, so the chosen candidates, and fconv and
+ * rescale_out, are bit-identical to it.  Iterations the bound cannot settle
+ * (more than 384 finalists, more than 1024 populated states, counts >= 2^24,
+ * values out of the FP32 range) run the FP64 pass.  stats (device, 3
+ * counters, NULL for none; the caller zeroes them) accumulates [iterations
+ * settled by the screen, iterations that ran the FP64 pass, finalists]. */
+int rspi_maxlp_pattern_screened(double *fconv, const int *pixels, const int *hist_row,
+                                long long n_pix, const int *hist, long long n_ref,
+                                const int *nstate, long long n_modes, const double *ref_params,
+                                long long size, int rescale_mode, const double *rescale,
+                                int num_iter, double *rescale_out, unsigned long long *stats,
+                                cudaStream_t stream);
+
+/* The error of the FP32 screen's log2 (lg2.approx.f32) over every float in
+ * [lo, hi] (0 < lo <= hi): out[0] (device double) = the largest
+ * |lg2(x) - log2(x)| / (2^-21 + 2^-22 |lg2(x)|), the bound the screened
+ * pattern search uses (it needs out[0] <= 1 on [2^-100, 2^100]); out[1] =
+ * the largest absolute error. */
+int rspi_log2_error_max(float lo, float hi, double *out, cudaStream_t stream);
 
 /* Polar grid search of the per-pixel MaxLP negative log-likelihood (the
  * judge beside the L-BFGS update of rspi_nll; no reference counterpart):

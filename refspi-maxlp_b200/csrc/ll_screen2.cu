@@ -400,6 +400,87 @@ __global__ void k_wide_fill(const unsigned short *__restrict__ ent16,
     }
 }
 
+// Bank-class layout of the wide entries.  A lane's shared gather at byte
+// offset sel * B (B = 4, 8 bytes per pixel) falls in bank class sel mod C,
+// C = 128 / B (the 32 four-byte banks taken B/4 at a time).  Here lane l only
+// ever holds photons of class l mod C (and its zero column p_zero + l, of the
+// same class since p_zero % 32 == 0), so the 32 addresses of every gather
+// instruction fall in distinct bank classes, two lanes per class when C = 16,
+// and the gather needs the minimum number of shared-memory wavefronts.  The
+// k-th photon of class c goes to lane c + C (k mod 32/C), slot k / (32/C);
+// a frame takes ceil(max_c n_c / (4 * 32/C)) groups.
+constexpr int BANK_WARPS = 8;
+
+__device__ __forceinline__ unsigned entry16_at(const unsigned short *__restrict__ ent16,
+                                               long long rr, int lane) {
+    return ent16[(rr >> 1) * 64 + lane * 2 + (rr & 1)];
+}
+
+__global__ void __launch_bounds__(BANK_WARPS * 32)
+k_wide_groups_banked(const unsigned short *__restrict__ ent16,
+                     const long long *__restrict__ row_off16, long long n, int p_zero,
+                     int classes, int *__restrict__ groups) {
+    __shared__ int cnt[BANK_WARPS][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int per = 32 / classes;
+    for (long long d = warp; d < n; d += nwarp) {
+        cnt[w][lane] = 0;
+        __syncwarp();
+        const long long r0 = row_off16[d], nr = row_off16[d + 1] - r0;
+        for (long long r = 0; r < nr; ++r) {
+            const unsigned e = entry16_at(ent16, r0 + r, lane);
+            const int key = e < (unsigned)p_zero ? (int)(e % (unsigned)classes) : classes;
+            const unsigned m = __match_any_sync(RSPI_FULL_MASK, key);
+            if (key < classes && lane == __ffs(m) - 1) cnt[w][key] += __popc(m);
+            __syncwarp();
+        }
+        int mx = lane < classes ? cnt[w][lane] : 0;
+        mx = warp_max_int(mx);
+        if (lane == 0) groups[d] = (mx + 4 * per - 1) / (4 * per);
+        __syncwarp();
+    }
+}
+
+__global__ void __launch_bounds__(BANK_WARPS * 32)
+k_wide_fill_banked(const unsigned short *__restrict__ ent16,
+                   const long long *__restrict__ row_off16, long long n, int p_zero, int classes,
+                   unsigned scale, const long long *__restrict__ goff,
+                   unsigned *__restrict__ out) {
+    __shared__ int base[BANK_WARPS][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int per = 32 / classes;
+    const unsigned lt = (1u << lane) - 1u;
+    for (long long d = warp; d < n; d += nwarp) {
+        const long long g0 = goff[d], ng = goff[d + 1] - g0;
+        // every slot of the frame starts as the lane's zero column
+        const unsigned pad = (unsigned)(p_zero + lane) * scale;
+        for (long long g = 0; g < ng; ++g)
+            reinterpret_cast<uint4 *>(out)[(g0 + g) * 32 + lane] = make_uint4(pad, pad, pad, pad);
+        base[w][lane] = 0;
+        __syncwarp();
+        const long long r0 = row_off16[d], nr = row_off16[d + 1] - r0;
+        for (long long r = 0; r < nr; ++r) {
+            const unsigned e = entry16_at(ent16, r0 + r, lane);
+            const int key = e < (unsigned)p_zero ? (int)(e % (unsigned)classes) : classes;
+            const unsigned m = __match_any_sync(RSPI_FULL_MASK, key);
+            if (key < classes) {
+                const int k = base[w][key] + __popc(m & lt);
+                const int slot_lane = key + classes * (k % per);
+                const long long slot = k / per;
+                if ((slot >> 2) < ng)
+                    out[((g0 + (slot >> 2)) * 32 + slot_lane) * 4 + (slot & 3)] = e * scale;
+            }
+            __syncwarp();
+            if (key < classes && lane == __ffs(m) - 1) base[w][key] += __popc(m);
+            __syncwarp();
+        }
+    }
+}
+
 template <int T>
 __device__ __forceinline__ Contrib<T> gather_pair(const unsigned char *sl, unsigned a,
                                                   unsigned b) {
@@ -795,6 +876,33 @@ extern "C" int rspi_wide_entry_fill(const unsigned short *entries16, const long 
         return RSPI_ERR_ARG;
     k_wide_fill<<<rspi_blocks(n_data * 32, 256), 256, 0, stream>>>(
         entries16, row_off16, n_data, p_zero, states_per_tile, group_off, wide);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_wide_entry_groups_banked(const unsigned short *entries16,
+                                             const long long *row_off16, long long n_data,
+                                             int p_zero, int states_per_tile, int *groups,
+                                             cudaStream_t stream) {
+    if (!entries16 || !row_off16 || !groups || n_data <= 0 || p_zero < 0 || p_zero % 32 ||
+        p_zero + 32 > 65536 || (states_per_tile != 1 && states_per_tile != 2))
+        return RSPI_ERR_ARG;
+    k_wide_groups_banked<<<rspi_blocks(n_data * 32, BANK_WARPS * 32), BANK_WARPS * 32, 0,
+                           stream>>>(entries16, row_off16, n_data, p_zero, 32 / states_per_tile,
+                                     groups);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_wide_entry_fill_banked(const unsigned short *entries16,
+                                           const long long *row_off16, long long n_data,
+                                           int p_zero, int states_per_tile,
+                                           const long long *group_off, unsigned *wide,
+                                           cudaStream_t stream) {
+    if (!entries16 || !row_off16 || !group_off || !wide || n_data <= 0 || p_zero < 0 ||
+        p_zero % 32 || p_zero + 32 > 65536 || (states_per_tile != 1 && states_per_tile != 2))
+        return RSPI_ERR_ARG;
+    k_wide_fill_banked<<<rspi_blocks(n_data * 32, BANK_WARPS * 32), BANK_WARPS * 32, 0,
+                         stream>>>(entries16, row_off16, n_data, p_zero, 32 / states_per_tile,
+                                   4u * (unsigned)states_per_tile, group_off, wide);
     RSPI_RETURN_LAUNCH();
 }
 

@@ -205,13 +205,143 @@ __device__ int load_populated(int s_begin, const int *__restrict__ hrow, long lo
     return s0 < n_ref ? s0 : (int)n_ref;
 }
 
-__global__ void __launch_bounds__(PT_THREADS)
+// One candidate of the 33 x 33 pattern around f (maxLP.py:45-48,168-170):
+// its value, the frame mean of |f_c + r_d|^2 (|f_c + rbar|^2 + var) and its
+// rescale (the ring pass: mean photons / that mean, maxLP.py:216-228;
+// the main pass: the ring's mean rescale).  Explicit roundings, so the plain
+// and the screened search compute the same bits.
+struct Cand {
+    double fr, fi, mw, rho;
+};
+
+__device__ __forceinline__ Cand cand_at(int c, double2 f, double step, const PixelConsts &pc,
+                                        bool ring, double kmean, double rescale) {
+    const double px = -8. + 0.5 * (c / 33), py = -8. + 0.5 * (c % 33);
+    Cand o;
+    o.fr = xadd(f.x, xmul(px, step));
+    o.fi = xadd(f.y, xmul(py, step));
+    const double er = xadd(o.fr, pc.ar), ei = xadd(o.fi, pc.ai);
+    o.mw = fma(er, er, fma(ei, ei, pc.var));
+    o.rho = ring ? kmean / o.mw : rescale;
+    return o;
+}
+
+// acc + k log(rho |f_c + r|^2): one populated state's term (maxLP.py:181-197).
+__device__ __forceinline__ double term64(double acc, double kk, const Cand &c, double rr,
+                                         double ri) {
+    const double re = xadd(c.fr, rr), im = xadd(c.fi, ri);
+    return fma(kk, log(xmul(c.rho, fma(re, re, xmul(im, im)))), acc);
+}
+
+// The candidate's value: frame mean of the log term minus the mean rescaled
+// intensity.
+__device__ __forceinline__ double cand_q(double acc, double dn, const Cand &c) {
+    return xsub(acc / dn, xmul(c.rho, c.mw));
+}
+
+__device__ __forceinline__ float lg2_approx(float x) {
+    float y;
+    asm("lg2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Error of lg2.approx.f32 for x in [2^-100, 2^100]:
+//   |lg2(x) - log2(x)| <= LG2_EA + LG2_ER |lg2(x)|,
+// checked over every float of that range by rspi_log2_error_max.
+constexpr double LG2_EA = 0x1p-21;
+constexpr double LG2_ER = 0x1p-22;
+constexpr double U32 = 0x1p-24;                    // FP32 unit roundoff
+constexpr double LN2 = 0x1.62e42fefa39efp-1;       // the double nearest ln 2
+constexpr int PT_CHUNK = 8;                        // FP32 terms per FP64 add
+constexpr double G_CHUNK = 8.01 * U32;             // gamma_8 (+ the FP64 adds)
+constexpr int FIN_CAP = PT_THREADS;                // finalists: one per thread
+
+__device__ __forceinline__ double block_max_d(double v, double *scratch) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(RSPI_FULL_MASK, v, o));
+    __syncthreads();
+    if (lane == 0) scratch[wid] = v;
+    __syncthreads();
+    double m = -INFINITY;
+    for (int w = 0; w < nw; ++w) m = fmax(m, scratch[w]);
+    __syncthreads();
+    return m;
+}
+
+// Exclusive prefix of v in thread order, and the block total in *total.
+__device__ __forceinline__ int block_scan(int v, int *wsum, int *total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int nw = (blockDim.x + 31) >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(RSPI_FULL_MASK, x, o);
+        if (lane >= o) x += y;
+    }
+    __syncthreads();
+    if (lane == 31) wsum[wid] = x;
+    __syncthreads();
+    int before = 0, tot = 0;
+    for (int w = 0; w < nw; ++w) {
+        if (w < wid) before += wsum[w];
+        tot += wsum[w];
+    }
+    __syncthreads();
+    *total = tot;
+    return before + x - v;
+}
+
+// One FP32 screening term for a candidate held as hi + lo parts (x: real,
+// y: imaginary) against a populated state r = (re hi, re lo, im hi, im lo),
+// everything scaled by the pixel's power of two.
+__device__ __forceinline__ void screen_term(float xh, float xl, float yh, float yl,
+                                            const float4 r, float kj, float &gmin, float &a32,
+                                            float &b32) {
+    const float re = __fadd_rn(__fadd_rn(xh, r.x), __fadd_rn(xl, r.y));
+    const float im = __fadd_rn(__fadd_rn(yh, r.z), __fadd_rn(yl, r.w));
+    const float g = fmaf(re, re, __fmul_rn(im, im));
+    gmin = fminf(gmin, g);
+    const float l = lg2_approx(g);
+    a32 = fmaf(kj, l, a32);
+    b32 = fmaf(kj, fabsf(l), b32);
+}
+
+// Per-pixel pattern search (maxLP.py:154-179, 304-340): one CTA per phaser
+// pixel (x mode), every thread PT_CPT candidates, the populated reference
+// states of the pixel in shared memory.
+//
+// SCREEN: each iteration first evaluates every candidate in FP32 (hi + lo
+// differences, lg2.approx, chunked sums) with a rigorous bound E_c on its
+// distance from the FP64 value; only the finalists, the candidates whose
+// upper end q32 + E reaches the best lower end max(q32 - E), are evaluated
+// in FP64, each by one thread in the plain search's order.  The FP64 argmax
+// is always a finalist and every other candidate's FP64 value is strictly
+// below it, so the chosen candidate is the plain search's.  A pixel falls
+// back to the plain FP64 iteration when it has more than one chunk of
+// populated states, counts >= 2^24, no candidate with a finite bound, or
+// more than FIN_CAP finalists.
+//
+// Bound, per term (u = 2^-24; A = |f_c|_inf + max_s |r_s|_inf, scaled):
+//   re, im from hi + lo parts: error <= 2u |re| + 6 u^2 A, so while
+//   |f_c + r|^2 >= max(2^-24 A^2, 2^-100) (checked through the minimum g):
+//   |ln g32 - ln g| <= 6.5 u, i.e. 9.5 u in log2;
+//   lg2: LG2_EA + LG2_ER |l|; chunk sums: gamma_8 sum k |l|.
+//   E_c = ln2 (K (LG2_EA + 9.5u) + (LG2_ER + g8)(1 + g8) sum k|l|) / n
+//         + 2^-40 (FP64 rounding of both evaluations).
+template <bool SCREEN>
+__global__ void __launch_bounds__(PT_THREADS, 2)
 k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
           const int *__restrict__ hist_row, long long n_pix, const int *__restrict__ hist,
           long long n_ref, const int *__restrict__ nstate, long long n_modes,
           const double *__restrict__ ref_params, int size, int ring,
-          const double *__restrict__ rescale_ptr, int num_iter, double *__restrict__ rescale_out) {
+          const double *__restrict__ rescale_ptr, int num_iter, double *__restrict__ rescale_out,
+          unsigned long long *__restrict__ stats) {
     __shared__ double fr_re[POP_CAP], fr_im[POP_CAP], fk[POP_CAP];
+    __shared__ float4 r32[SCREEN ? POP_CAP : 1];
+    __shared__ float k32[SCREEN ? POP_CAP : 1];
+    __shared__ int fin[SCREEN ? FIN_CAP : 1];
     __shared__ double scratch[32];
     __shared__ int iscratch[32];
     __shared__ int wsum[32];
@@ -249,8 +379,8 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
         if (ns > 0) {
             const double2 r = fref_value(pc.qx, pc.qy, pc.qrad, ref_params[3 * s],
                                          ref_params[3 * s + 1], ref_params[3 * s + 2]);
-            ar += ns * r.x;
-            ai += ns * r.y;
+            ar = fma((double)ns, r.x, ar);
+            ai = fma((double)ns, r.y, ai);
         }
     }
     pc.ar = block_sum(ar, scratch) / dn;
@@ -262,8 +392,8 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
         if (ns > 0) {
             const double2 r = fref_value(pc.qx, pc.qy, pc.qrad, ref_params[3 * s],
                                          ref_params[3 * s + 1], ref_params[3 * s + 2]);
-            const double er = r.x - pc.ar, ei = r.y - pc.ai;
-            vv += ns * (er * er + ei * ei);
+            const double er = xsub(r.x, pc.ar), ei = xsub(r.y, pc.ai);
+            vv = fma((double)ns, fma(er, er, xmul(ei, ei)), vv);
         }
     }
     pc.var = block_sum(vv, scratch) / dn;
@@ -278,52 +408,191 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
     double step = hypot(f.x, f.y) / 4.;
     const double shrink = 33. / 5.;  // sqrt(1089) / 5, maxLP.py:177
 
+    // FP32 copies of the populated states, scaled by 2^-sexp so that the
+    // largest of |f|_inf and max |r|_inf lies in [1/2, 1)
+    bool screen = false;
+    int sexp = 0;
+    double sc = 1., rinf_s = 0.;
+    if (SCREEN && one_chunk && !(ring && pc.ksum == 0.)) {
+        double rl = 0.;
+        int bad = 0;
+        for (int j = threadIdx.x; j < npop; j += blockDim.x) {
+            rl = fmax(rl, fmax(fabs(fr_re[j]), fabs(fr_im[j])));
+            bad |= !(fk[j] < 16777216.);
+        }
+        bad = __syncthreads_or(bad);
+        rl = block_max_d(rl, scratch);
+        const double top = fmax(rl, fmax(fabs(f.x), fabs(f.y)));
+        if (!bad && top > 0x1p-1000 && top < 0x1p1000) {
+            frexp(top, &sexp);
+            sc = ldexp(1., -sexp);
+            rinf_s = rl * sc;
+            for (int j = threadIdx.x; j < npop; j += blockDim.x) {
+                const double xr = fr_re[j] * sc, xi = fr_im[j] * sc;
+                const float hr = (float)xr, hi = (float)xi;
+                r32[j] = make_float4(hr, (float)(xr - (double)hr), hi, (float)(xi - (double)hi));
+                k32[j] = (float)fk[j];
+            }
+            __syncthreads();
+            screen = true;
+        }
+    }
+
     for (int it = 0; it < num_iter; ++it) {
-        double fcr[PT_CPT], fci[PT_CPT], rho[PT_CPT], acc[PT_CPT];
+        Cand cd[PT_CPT];
 #pragma unroll
         for (int k = 0; k < PT_CPT; ++k) {
             const int c = threadIdx.x + k * PT_THREADS;
-            const int cc = c < NCAND ? c : 0;
-            const double px = -8. + 0.5 * (cc / 33), py = -8. + 0.5 * (cc % 33);
-            fcr[k] = xadd(f.x, xmul(px, step));
-            fci[k] = xadd(f.y, xmul(py, step));
-            const double er = fcr[k] + pc.ar, ei = fci[k] + pc.ai;
-            const double mw = er * er + ei * ei + pc.var;
-            rho[k] = ring ? kmean / mw : rescale;
-            acc[k] = 0.;
+            cd[k] = cand_at(c < NCAND ? c : 0, f, step, pc, ring, kmean, rescale);
         }
-        int s_next = 0;
-        do {
-            if (!one_chunk)
-                s_next = load_populated(s_next, hrow, n_ref, ref_params, pc, fr_re, fr_im, fk,
-                                        &npop, wsum);
-            else
-                s_next = (int)n_ref;
-            for (int j = 0; j < npop; ++j) {
-                const double rr = fr_re[j], ri = fr_im[j], kk = fk[j];
-#pragma unroll
-                for (int k = 0; k < PT_CPT; ++k) {
-                    const double re = fcr[k] + rr, im = fci[k] + ri;
-                    acc[k] = fma(kk, log(rho[k] * (re * re + im * im)), acc[k]);
-                }
-            }
-            if (!one_chunk) __syncthreads();
-        } while (s_next < n_ref);
-
         double best = -INFINITY;
         int bidx = 0x7fffffff;
+        bool searched = false;
+        if (SCREEN && screen) {
+            float xh[PT_CPT], xl[PT_CPT], yh[PT_CPT], yl[PT_CPT], gmin[PT_CPT];
+            double a64[PT_CPT], b64[PT_CPT];
 #pragma unroll
-        for (int k = 0; k < PT_CPT; ++k) {
-            const int c = threadIdx.x + k * PT_THREADS;
-            if (c >= NCAND) continue;
-            const double er = fcr[k] + pc.ar, ei = fci[k] + pc.ai;
-            const double mw = er * er + ei * ei + pc.var;
-            double q = acc[k] / dn - rho[k] * mw;
-            if (ring && pc.ksum == 0.) q = NAN;  // 0 * log(0) in every frame
-            if (argmax_better(q, c, best, bidx)) {
-                best = q;
-                bidx = c;
+            for (int k = 0; k < PT_CPT; ++k) {
+                const double xs = cd[k].fr * sc, ys = cd[k].fi * sc;
+                xh[k] = (float)xs;
+                xl[k] = (float)(xs - (double)xh[k]);
+                yh[k] = (float)ys;
+                yl[k] = (float)(ys - (double)yh[k]);
+                gmin[k] = INFINITY;
+                a64[k] = 0.;
+                b64[k] = 0.;
             }
+            int j = 0;
+            for (; j + PT_CHUNK <= npop; j += PT_CHUNK) {
+                float a32[PT_CPT], b32[PT_CPT];
+#pragma unroll
+                for (int k = 0; k < PT_CPT; ++k) a32[k] = b32[k] = 0.f;
+#pragma unroll 2
+                for (int jj = 0; jj < PT_CHUNK; ++jj) {
+                    const float4 r = r32[j + jj];
+                    const float kj = k32[j + jj];
+#pragma unroll
+                    for (int k = 0; k < PT_CPT; ++k)
+                        screen_term(xh[k], xl[k], yh[k], yl[k], r, kj, gmin[k], a32[k], b32[k]);
+                }
+#pragma unroll
+                for (int k = 0; k < PT_CPT; ++k) {
+                    a64[k] += (double)a32[k];
+                    b64[k] += (double)b32[k];
+                }
+            }
+            {
+                float a32[PT_CPT], b32[PT_CPT];
+#pragma unroll
+                for (int k = 0; k < PT_CPT; ++k) a32[k] = b32[k] = 0.f;
+                for (; j < npop; ++j) {
+                    const float4 r = r32[j];
+                    const float kj = k32[j];
+#pragma unroll
+                    for (int k = 0; k < PT_CPT; ++k)
+                        screen_term(xh[k], xl[k], yh[k], yl[k], r, kj, gmin[k], a32[k], b32[k]);
+                }
+#pragma unroll
+                for (int k = 0; k < PT_CPT; ++k) {
+                    a64[k] += (double)a32[k];
+                    b64[k] += (double)b32[k];
+                }
+            }
+            // each candidate's interval [lo, hi] around its FP64 value
+            double lo[PT_CPT], up[PT_CPT];
+            const double ksum = pc.ksum, e2 = 2. * (double)sexp;
+#pragma unroll
+            for (int k = 0; k < PT_CPT; ++k) {
+                const int c = threadIdx.x + k * PT_THREADS;
+                lo[k] = -INFINITY;
+                up[k] = -INFINITY;
+                if (c >= NCAND) continue;
+                const double xs = cd[k].fr * sc, ys = cd[k].fi * sc;
+                const double amax = fmax(fabs(xs), fabs(ys)) + rinf_s;
+                const double thr = fmax(0x1p-24 * amax * amax, 0x1p-100);
+                const double rho = cd[k].rho, mwv = cd[k].mw;
+                bool safe = isfinite(a64[k]) && isfinite(b64[k]) && (double)gmin[k] >= thr &&
+                            amax >= 0x1p-38 && amax <= 0x1p60 && rho > 0. && rho < INFINITY &&
+                            isfinite(mwv);
+                if (safe) {
+                    const double lr = log(rho);
+                    const double q = (ksum * lr + LN2 * (a64[k] + e2 * ksum)) / dn - rho * mwv;
+                    const double b2 = ksum * (LG2_EA + 9.5 * U32) +
+                                      (LG2_ER + G_CHUNK) * (1. + G_CHUNK) * b64[k];
+                    const double fm = 0x1p-40 * ((ksum * (fabs(lr) + LN2 * fabs(e2) + 1.) +
+                                                  LN2 * 1.01 * b64[k]) / dn +
+                                                 fabs(rho * mwv));
+                    const double e = 1.001 * LN2 * b2 / dn + fm;
+                    safe = isfinite(q) && isfinite(e);
+                    lo[k] = q - e;
+                    up[k] = q + e;
+                }
+                if (!safe) {
+                    lo[k] = -INFINITY;
+                    up[k] = INFINITY;
+                }
+            }
+            double tl = -INFINITY;
+#pragma unroll
+            for (int k = 0; k < PT_CPT; ++k) tl = fmax(tl, lo[k]);
+            tl = block_max_d(tl, scratch);
+            int mine = 0;
+#pragma unroll
+            for (int k = 0; k < PT_CPT; ++k) mine += (threadIdx.x + k * PT_THREADS < NCAND) && up[k] >= tl;
+            int nfin = 0;
+            int pos = block_scan(mine, wsum, &nfin);
+            if (tl > -INFINITY && nfin <= FIN_CAP) {
+#pragma unroll
+                for (int k = 0; k < PT_CPT; ++k) {
+                    const int c = threadIdx.x + k * PT_THREADS;
+                    if (c < NCAND && up[k] >= tl) fin[pos++] = c;
+                }
+                __syncthreads();
+                if (threadIdx.x < nfin) {
+                    const int c = fin[threadIdx.x];
+                    const Cand cc = cand_at(c, f, step, pc, ring, kmean, rescale);
+                    double acc = 0.;
+                    for (int s = 0; s < npop; ++s) acc = term64(acc, fk[s], cc, fr_re[s], fr_im[s]);
+                    best = cand_q(acc, dn, cc);
+                    bidx = c;
+                }
+                searched = true;
+                if (stats && threadIdx.x == 0) {
+                    atomicAdd(&stats[0], 1ull);
+                    atomicAdd(&stats[2], (unsigned long long)nfin);
+                }
+            }
+        }
+        if (!searched) {
+            double acc[PT_CPT];
+#pragma unroll
+            for (int k = 0; k < PT_CPT; ++k) acc[k] = 0.;
+            int s_next = 0;
+            do {
+                if (!one_chunk)
+                    s_next = load_populated(s_next, hrow, n_ref, ref_params, pc, fr_re, fr_im, fk,
+                                            &npop, wsum);
+                else
+                    s_next = (int)n_ref;
+                for (int j = 0; j < npop; ++j) {
+                    const double rr = fr_re[j], ri = fr_im[j], kk = fk[j];
+#pragma unroll
+                    for (int k = 0; k < PT_CPT; ++k) acc[k] = term64(acc[k], kk, cd[k], rr, ri);
+                }
+                if (!one_chunk) __syncthreads();
+            } while (s_next < n_ref);
+#pragma unroll
+            for (int k = 0; k < PT_CPT; ++k) {
+                const int c = threadIdx.x + k * PT_THREADS;
+                if (c >= NCAND) continue;
+                double q = cand_q(acc[k], dn, cd[k]);
+                if (ring && pc.ksum == 0.) q = NAN;  // 0 * log(0) in every frame
+                if (argmax_better(q, c, best, bidx)) {
+                    best = q;
+                    bidx = c;
+                }
+            }
+            if (SCREEN && stats && threadIdx.x == 0) atomicAdd(&stats[1], 1ull);
         }
         block_argmax(best, bidx, scratch, iscratch);
         const double px = -8. + 0.5 * (bidx / 33), py = -8. + 0.5 * (bidx % 33);
@@ -335,10 +604,36 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
     }
     if (threadIdx.x == 0) {
         fconv[t] = f;
-        if (rescale_out) {
-            const double er = f.x + pc.ar, ei = f.y + pc.ai;
-            rescale_out[mode * n_pix + ip] = kmean / (er * er + ei * ei + pc.var);
+        if (rescale_out) {   // maxLP.py:328, with the candidates' explicit roundings
+            const double er = xadd(f.x, pc.ar), ei = xadd(f.y, pc.ai);
+            rescale_out[mode * n_pix + ip] = kmean / fma(er, er, fma(ei, ei, pc.var));
         }
+    }
+}
+
+// Every float x in [lo, hi] (positive): the largest |lg2.approx(x) - log2(x)|
+// / (LG2_EA + LG2_ER |lg2.approx(x)|) into out[0] and the largest absolute
+// error into out[1], both as the bit patterns of non-negative doubles.
+__global__ void k_log2_error(unsigned lo_bits, unsigned long long count,
+                             unsigned long long *__restrict__ out) {
+    double worst = 0., wabs = 0.;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+         i < count; i += stride) {
+        const float x = __uint_as_float(lo_bits + (unsigned)i);
+        const float y = lg2_approx(x);
+        const double e = fabs((double)y - log2((double)x));
+        worst = fmax(worst, e / (LG2_EA + LG2_ER * fabs((double)y)));
+        wabs = fmax(wabs, e);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        worst = fmax(worst, __shfl_xor_sync(RSPI_FULL_MASK, worst, o));
+        wabs = fmax(wabs, __shfl_xor_sync(RSPI_FULL_MASK, wabs, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(&out[0], (unsigned long long)__double_as_longlong(worst));
+        atomicMax(&out[1], (unsigned long long)__double_as_longlong(wabs));
     }
 }
 
@@ -519,10 +814,40 @@ extern "C" int rspi_maxlp_pattern(double *fconv, const int *pixels, const int *h
         (rescale_mode == 1 && !rescale) || (rescale_mode != 0 && rescale_mode != 1))
         return RSPI_ERR_ARG;
     const dim3 grid((unsigned)n_pix, (unsigned)n_modes);
-    k_pattern<<<grid, PT_THREADS, 0, stream>>>((double2 *)fconv, pixels, hist_row, n_pix, hist,
-                                               n_ref, nstate, n_modes, ref_params, (int)size,
-                                               rescale_mode == 0, rescale, num_iter,
-                                               rescale_out);
+    k_pattern<false><<<grid, PT_THREADS, 0, stream>>>(
+        (double2 *)fconv, pixels, hist_row, n_pix, hist, n_ref, nstate, n_modes, ref_params,
+        (int)size, rescale_mode == 0, rescale, num_iter, rescale_out, nullptr);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_maxlp_pattern_screened(double *fconv, const int *pixels, const int *hist_row,
+                                           long long n_pix, const int *hist, long long n_ref,
+                                           const int *nstate, long long n_modes,
+                                           const double *ref_params, long long size,
+                                           int rescale_mode, const double *rescale, int num_iter,
+                                           double *rescale_out, unsigned long long *stats,
+                                           cudaStream_t stream) {
+    if (n_pix == 0) return RSPI_OK;
+    if (!fconv || !pixels || !hist_row || !hist || !nstate || !ref_params || n_ref <= 0 ||
+        n_modes <= 0 || n_modes > 65535 || size <= 1 || size > 46340 || n_pix < 0 ||
+        n_pix > 0x7fffffffLL || n_ref * n_modes > 0x7fffffffLL || num_iter < 0 ||
+        (rescale_mode == 1 && !rescale) || (rescale_mode != 0 && rescale_mode != 1))
+        return RSPI_ERR_ARG;
+    const dim3 grid((unsigned)n_pix, (unsigned)n_modes);
+    k_pattern<true><<<grid, PT_THREADS, 0, stream>>>(
+        (double2 *)fconv, pixels, hist_row, n_pix, hist, n_ref, nstate, n_modes, ref_params,
+        (int)size, rescale_mode == 0, rescale, num_iter, rescale_out, stats);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_log2_error_max(float lo, float hi, double *out, cudaStream_t stream) {
+    if (!out || !(lo > 0.f) || !(hi >= lo) || !(hi < INFINITY)) return RSPI_ERR_ARG;
+    unsigned lb, hb;
+    memcpy(&lb, &lo, 4);
+    memcpy(&hb, &hi, 4);
+    cudaMemsetAsync(out, 0, 2 * sizeof(double), stream);
+    k_log2_error<<<rspi_sm_count() * 8, 256, 0, stream>>>(
+        lb, (unsigned long long)(hb - lb) + 1ull, (unsigned long long *)out);
     RSPI_RETURN_LAUNCH();
 }
 

@@ -20,7 +20,9 @@ densely, likelihood as a tensor-core GEMM, ``dense_gemm`` = ``auto`` /
 ``screen_slices`` (``fp32``, or ``fp16``: half-precision slices, four
 likelihood rows per gather, a wider candidate threshold), ``screen_delta``
 (default 20 nats), ``states_per_tile``, ``warps_per_cta``, ``phaser_iter``
-(default 10, maxLP.py:320,335), ``slice_budget_gb`` (rotated slices are built
+(default 10, maxLP.py:320,335), ``phaser_screen`` (default true: FP32
+screening of the pattern-search candidates, FP64 for the finalists, same
+chosen candidates as false), ``slice_budget_gb`` (rotated slices are built
 in chunks of at most this size, default 8), ``cuda_graph`` (capture the whole
 device iteration once and replay it, default true), ``autotune`` (pick the
 likelihood kernel's tile shape by timing, default false).
@@ -75,7 +77,8 @@ class EMC():
 
         self._parse_data()
         self.phaser = MaxLPhaser(self.photons_file, size=self.size, dataset=self.dset,
-                                 num_iter=self.phaser_iter, num_modes=self.num_modes)
+                                 num_iter=self.phaser_iter, num_modes=self.num_modes,
+                                 screen=self.phaser_screen)
         self._init_model()
 
         self.estep = EStep(self.dset.photons, self.size, self.num_rot, self.shiftx,
@@ -118,6 +121,7 @@ class EMC():
         self.states_per_tile = config.getint('emc', 'states_per_tile', fallback=0) or None
         self.warps_per_cta = config.getint('emc', 'warps_per_cta', fallback=32)
         self.phaser_iter = config.getint('emc', 'phaser_iter', fallback=10)
+        self.phaser_screen = config.getboolean('emc', 'phaser_screen', fallback=True)
         self.slice_budget_gb = config.getfloat('emc', 'slice_budget_gb', fallback=8.)
         self.use_graph = config.getboolean('emc', 'cuda_graph', fallback=True)
         self.dense_gemm = config.get('emc', 'dense_gemm', fallback='auto')

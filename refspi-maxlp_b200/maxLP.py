@@ -22,7 +22,7 @@ from rspi.device import MStep  # noqa: E402
 class MaxLPhaser():
     '''Reconstruction of object from holographic data using maximum likelihood and pattern search'''
     def __init__(self, data_fname, size=185, num_data=-1, dataset=None, device=None,
-                 num_iter=10, num_modes=1):
+                 num_iter=10, num_modes=1, screen=True):
         self.size = size
         self.num_iter = num_iter
         self.num_modes = int(num_modes)
@@ -39,7 +39,8 @@ class MaxLPhaser():
         self._gen_pattern(8)
         self.counts = dataset.photons.counts
         self.mean_count = dataset.photons.mean_count
-        self.mstep = MStep(dataset.photons, size, num_iter, n_modes=self.num_modes)
+        self.mstep = MStep(dataset.photons, size, num_iter, n_modes=self.num_modes,
+                           screen=screen)
 
     def _gen_pattern(self, nmax):
         '''33x33 candidate offsets (maxLP.py:45-48)'''

@@ -217,7 +217,8 @@ class EStep:
     def __init__(self, photons, size, num_rot, shiftx, shifty, sphere_dia, probmask, bg,
                  form='fp64', states_per_tile=None, warps=32, n_ctas=0,
                  slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel=None,
-                 n_modes=1, dense_gemm='auto', dense_rescore=True, screen_slices='fp32'):
+                 n_modes=1, dense_gemm='auto', dense_rescore=True, screen_slices='fp32',
+                 bank_layout=True):
         if form not in ('fp64', 'screen', 'dense'):
             raise ValueError('form must be fp64, screen or dense')
         if kernel is None:   # default likelihood kernel of each form
@@ -292,13 +293,10 @@ class EStep:
             self.prefetch_words = 4 if wpf <= 5 else (8 if wpf <= 10 else 12)
         if kernel == 'wide16' and self.tile != 4:
             raise ValueError('the FP16-slice kernel takes 4 states per tile')
+        self.bank_layout = bool(bank_layout)
         self.wide = self._wide_entries() if (form == 'screen' and kernel in ('wide', 'wide16')) \
             else None
-        if kernel == 'wide16':
-            # FP16 storage error <= 2^-11 |L| per value: 8192 more FP32 rounding
-            # steps (2^-24) per photon in the candidate threshold's eps_d
-            self.row_off_eps = self.ll16['row_off'] + 8192 * torch.arange(
-                n + 1, dtype=_i64, device=dev)
+        self._eps_key, self.row_off_eps = None, None
         self.warps, self.n_ctas = int(warps), int(n_ctas)
         esz = {0: 4, 1: 8, 2: 2}[self.slice_code]
         rows = max(self.tile, (slice_budget_bytes // (self.p_row * esz)) // self.tile * self.tile)
@@ -414,15 +412,42 @@ class EStep:
         group, rows of a frame padded to a multiple of four."""
         l16, n, dev, s = self.ll16, self.ph.num_data, self.device, cur_stream()
         groups = torch.empty(n, dtype=_i32, device=dev)
-        call('rspi_wide_entry_groups', ptr(l16['row_off']), n, ptr(groups), s)
+        bt, pz = self._wide_bytes_tile(), self.p_row - 32
+        if self.bank_layout:
+            call('rspi_wide_entry_groups_banked', ptr(l16['entries']), ptr(l16['row_off']), n,
+                 pz, bt, ptr(groups), s)
+        else:
+            call('rspi_wide_entry_groups', ptr(l16['row_off']), n, ptr(groups), s)
         goff = torch.empty(n + 1, dtype=_i64, device=dev)
         call('rspi_scan_rows', ptr(groups), n, ptr(goff), s)
         total = int(goff[-1].item())
         wide = torch.empty(max(1, total) * 128, dtype=torch.int32, device=dev)
-        call('rspi_wide_entry_fill', ptr(l16['entries']), ptr(l16['row_off']), n,
-             self.p_row - 32, self._wide_bytes_tile(), ptr(goff), ptr(wide), s)
-        return dict(entries=wide, group_off=goff, total_groups=total,
-                    tile=self._wide_bytes_tile())
+        fill = 'rspi_wide_entry_fill_banked' if self.bank_layout else 'rspi_wide_entry_fill'
+        call(fill, ptr(l16['entries']), ptr(l16['row_off']), n, pz, bt, ptr(goff), ptr(wide), s)
+        return dict(entries=wide, group_off=goff, total_groups=total, tile=bt,
+                    banked=self.bank_layout)
+
+    def _eps_rows(self):
+        """Prefix sums of each frame's FP32 summation length for the
+        candidate threshold's eps_d (the 'rows' of 2^-24 (rows + 8) photons
+        lmax): the frame's 16-bit entry rows, or its groups in the bank-class
+        layout when that is longer (a lane then adds one group's pair sum per
+        step); with FP16 slices 8192 more per photon (storage error <=
+        2^-11 |L| per value)."""
+        key = (self.kernel, None if self.wide is None else self.wide['entries'].data_ptr())
+        if key != self._eps_key:
+            ro = self.ll16['row_off']
+            rows = ro[1:] - ro[:-1]
+            if self.kernel in ('wide', 'wide16') and self.wide is not None and \
+                    self.wide['banked']:
+                go = self.wide['group_off']
+                rows = torch.maximum(rows, go[1:] - go[:-1])
+            if self.kernel == 'wide16':
+                rows = rows + 8192
+            self.row_off_eps = torch.cat([torch.zeros(1, dtype=_i64, device=self.device),
+                                          torch.cumsum(rows, 0)])
+            self._eps_key = key
+        return self.row_off_eps
 
     def _alloc_row_scratch(self):
         """Global rows for FP64 rescoring when a row exceeds shared memory
@@ -516,8 +541,9 @@ class EStep:
                  ptr(self.ph.scales), ptr(self.wide['entries']), ptr(self.wide['group_off']), n,
                  r0, r1, ptr(self.prob[r0]), n, self.warps, self.n_ctas, cur_stream())
         elif self.kernel == 'wide' and self.form == 'screen':
-            if self.wide is None or self.wide['tile'] != self.tile:
-                self.wide = self._wide_entries()   # kernel or tile changed after set-up
+            if self.wide is None or self.wide['tile'] != self.tile or \
+                    self.wide['banked'] != self.bank_layout:
+                self.wide = self._wide_entries()   # kernel, tile or layout changed
             call('rspi_screen_loglike4', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
                  ptr(self.ph.scales), ptr(self.wide['entries']), ptr(self.wide['group_off']), n,
                  r0, r1, ptr(self.prob[r0]), n, self.tile, self.warps, self.n_ctas,
@@ -573,8 +599,7 @@ class EStep:
              ptr(self.rmax32), None, s)
         while True:
             dense = self.form == 'dense'
-            rows_eq = self.eq_row_off if dense else (
-                self.row_off_eps if self.kernel == 'wide16' else self.ll16['row_off'])
+            rows_eq = self.eq_row_off if dense else self._eps_rows()
             call('rspi_screen_candidates', ptr(self.prob), self.n_rows, n, ptr(self.max32),
                  ptr(self.rmax32), ptr(self.ll['frame_sel_photons']), ptr(rows_eq),
                  ptr(self.lmax_eps if dense else self.lmax),
@@ -662,10 +687,17 @@ class MStep:
     With ``n_modes`` > 1 the model is ``n_modes`` stacked complex128 images
     and frames carry a reference state ``m*n_ref + s``: each mode is searched
     over the frames assigned to it, with its own ring rescale, in the same
-    launches."""
+    launches.
 
-    def __init__(self, photons, size, num_iter=10, n_modes=1):
+    ``screen`` (default): each pattern iteration evaluates every candidate in
+    FP32 with a rigorous error bound and only the finalists in FP64; the
+    chosen candidates are bit-identical to ``screen=False`` (every candidate
+    in FP64).  ``stats`` (device int64[3]) counts the iterations the screen
+    settled, the iterations that ran the FP64 pass, and the finalists."""
+
+    def __init__(self, photons, size, num_iter=10, n_modes=1, screen=True):
         self.lib = load()
+        self.screen = bool(screen)
         self.ph = photons
         self.device = dev = photons.device
         self.size = int(size)
@@ -686,6 +718,17 @@ class MStep:
         self.frot = torch.empty(photons.num_data, dtype=_i32, device=dev)
         self.hist = None
         self.nstate = None
+        self.stats = torch.zeros(3, dtype=torch.int64, device=dev)
+
+    def _pattern(self, fconv, pixels, rows, n_pix, hist, n_ref, mode, rescale, rescale_out, s):
+        if self.screen:
+            call('rspi_maxlp_pattern_screened', ptr(fconv), ptr(pixels), ptr(rows), n_pix,
+                 ptr(hist), n_ref, ptr(self.nstate), self.n_modes, ptr(self._ref_params),
+                 self.size, mode, rescale, self.num_iter, rescale_out, ptr(self.stats), s)
+        else:
+            call('rspi_maxlp_pattern', ptr(fconv), ptr(pixels), ptr(rows), n_pix, ptr(hist),
+                 n_ref, ptr(self.nstate), self.n_modes, ptr(self._ref_params), self.size, mode,
+                 rescale, self.num_iter, rescale_out, s)
 
     def frame_params_from_rmax(self, rmax, num_rot, n_ref):
         """fstate / frot / nstate from the E-step argmax (emc.py:218-224);
@@ -742,16 +785,15 @@ class MStep:
         hist = self.histogram(n_ref * nm, rot_cs)
         s = cur_stream()
         ph = self.ph
-        call('rspi_maxlp_pattern', ptr(fconv), ptr(self.ring), ptr(self.ring_rows), self.n_ring, ptr(hist), n_ref,
-            ptr(self.nstate), nm, ptr(ref_params), self.size, 0, None,
-            self.num_iter, ptr(self.rescales), s)
+        self._ref_params = ref_params
+        self._pattern(fconv, self.ring, self.ring_rows, self.n_ring, hist, n_ref, 0, None,
+                      ptr(self.rescales), s)
         if self.n_ring > 0:
             for m in range(nm):
                 call('rspi_mean', ptr(self.rescales[m * self.n_ring:]), self.n_ring,
                      ptr(self.rescale[m:]), s)
         else:
             self.rescale.fill_(float('nan'))   # np.mean of an empty ring
-        call('rspi_maxlp_pattern', ptr(fconv), ptr(self.main), ptr(self.main_rows), self.n_main, ptr(hist), n_ref,
-            ptr(self.nstate), nm, ptr(ref_params), self.size, 1, ptr(self.rescale),
-            self.num_iter, None, s)
+        self._pattern(fconv, self.main, self.main_rows, self.n_main, hist, n_ref, 1,
+                      ptr(self.rescale), None, s)
         return fconv

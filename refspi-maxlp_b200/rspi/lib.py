@@ -12,6 +12,7 @@ P = ctypes.c_void_p
 L = ctypes.c_longlong
 I = ctypes.c_int
 D = ctypes.c_double
+F = ctypes.c_float
 
 # name: (restype, argtypes) -- mirrors include/rspi.h
 SIGNATURES = {
@@ -31,6 +32,8 @@ SIGNATURES = {
     'rspi_maxlp_frame_params': (I, [P, L, L, L, P, P, P, P, P]),
     'rspi_maxlp_histogram': (I, [P, P, P, P, P, P, P, L, P, P, P, L, P, L, L, P, P, P]),
     'rspi_maxlp_pattern': (I, [P, P, P, L, P, L, P, L, P, L, I, P, I, P, P]),
+    'rspi_maxlp_pattern_screened': (I, [P, P, P, L, P, L, P, L, P, L, I, P, I, P, P, P]),
+    'rspi_log2_error_max': (I, [F, F, P, P]),
     'rspi_mean': (I, [P, L, P, P]),
     'rspi_ll16_entry_rows': (I, [P] * 8 + [L, L, I, P, P, P]),
     'rspi_ll16_entry_fill': (I, [P] * 8 + [L, L, I, P, P, P]),
@@ -47,6 +50,8 @@ SIGNATURES = {
     'rspi_screen_loglike4h': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, P]),
     'rspi_wide_entry_groups': (I, [P, L, P, P]),
     'rspi_wide_entry_fill': (I, [P, P, L, I, I, P, P, P]),
+    'rspi_wide_entry_groups_banked': (I, [P, P, L, I, I, P, P]),
+    'rspi_wide_entry_fill_banked': (I, [P, P, L, I, I, P, P, P]),
     'rspi_entries16_check': (I, [P, L, P, P]),
     'rspi_loglike_stream': (I, [I, P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
     'rspi_posterior_pairs': (I, [P, L, L, P, D, P, P, P, L, P, P, P, P, P]),
@@ -100,6 +105,7 @@ KERNELS_PER_CALL = {
     'rspi_ll_entry_fill': 1, 'rspi_holo_slices': 1, 'rspi_vscale_init': 1,
     'rspi_rot_log_slices': 1, 'rspi_loglike': 1, 'rspi_frame_reduce': 1,
     'rspi_maxlp_frame_params': 1, 'rspi_maxlp_histogram': 1, 'rspi_maxlp_pattern': 1,
+    'rspi_maxlp_pattern_screened': 1, 'rspi_log2_error_max': 1,
     'rspi_mean': 1, 'rspi_ll16_entry_rows': 1, 'rspi_ll16_entry_fill': 1,
     'rspi_screen_loglike': 1, 'rspi_screen_candidates': 3, 'rspi_rescore': 5,
     'rspi_loglike_stream': 1, 'rspi_posterior_pairs': 3, 'rspi_screen_loglike2': 1,
@@ -107,7 +113,8 @@ KERNELS_PER_CALL = {
     'rspi_dense_frames': 1, 'rspi_rot_log_split': 1, 'rspi_dense_loglike': 1,
     'rspi_maxlp_grid': 2, 'rspi_dense_frames_u8': 1, 'rspi_rot_log_fixed': 1,
     'rspi_dense_loglike_i8': 1, 'rspi_screen_loglike3': 1, 'rspi_screen_loglike4': 1,
-    'rspi_wide_entry_groups': 1, 'rspi_wide_entry_fill': 1, 'rspi_screen_loglike4h': 1,
+    'rspi_wide_entry_groups': 1, 'rspi_wide_entry_fill': 1,
+    'rspi_wide_entry_groups_banked': 1, 'rspi_wide_entry_fill_banked': 1, 'rspi_screen_loglike4h': 1,
 }
 launch_count = 0
 

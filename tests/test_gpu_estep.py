@@ -268,7 +268,8 @@ def test_random_shapes_vs_oracle(size, n, seed, kw, form):
 @pytest.mark.parametrize('tile,warps', [(1, 1), (2, 4), (2, 32), (1, 7), (2, 3)])
 @pytest.mark.parametrize('name,ds,need_scaling', CASES, ids=[c[0] for c in CASES])
 def test_frame_kernel_matches_stream_kernel(name, ds, need_scaling, tile, warps):
-    """The frame-at-a-time and wide-entry screening kernels give the interleaved kernel's
+    """The frame-at-a-time and wide-entry screening kernels (wide entries in
+    the bank-class and in the plain layout) give the interleaved kernel's
     FP32 likelihoods (other summation order: within 1e-6 relative of the
     largest term) on every case, empty and heavy frames included, and the
     same FP64-rescored argmax / maximum / log-sum-exp."""
@@ -279,18 +280,18 @@ def test_frame_kernel_matches_stream_kernel(name, ds, need_scaling, tile, warps)
     rng = np.random.default_rng(size)
     model = torch.from_numpy(rng.random(size * size) + 1j * rng.random(size * size)).cuda()
     out = {}
-    for kernel in ('stream', 'frame', 'wide'):
+    for kernel, banked in (('stream', True), ('frame', True), ('wide', True), ('wide', False)):
         ph = _photons(ds, need_scaling)
         es = _estep(ph, size, num_rot, sx, sy, dia, ds['bg'], form='screen', kernel=kernel,
-                    states_per_tile=tile, warps=warps)
+                    states_per_tile=tile, warps=warps, bank_layout=banked)
         es.run(model)
         maxll, rmax, logz = es.reduce()
         torch.cuda.synchronize()
-        out[kernel] = (es.prob.cpu().numpy().astype(np.float64), maxll.cpu().numpy(),
-                       rmax.cpu().numpy(), logz.cpu().numpy())
-    a = out['stream']
+        out[kernel, banked] = (es.prob.cpu().numpy().astype(np.float64), maxll.cpu().numpy(),
+                               rmax.cpu().numpy(), logz.cpu().numpy())
+    a = out['stream', True]
     scale = np.abs(a[0]).max(0, keepdims=True) + 1.
-    for b in (out['frame'], out['wide']):
+    for b in (out['frame', True], out['wide', True], out['wide', False]):
         assert np.all(np.abs(a[0] - b[0]) <= 1e-6 * scale)
         assert np.array_equal(a[2], b[2])
         np.testing.assert_allclose(a[1], b[1], rtol=1e-14)
@@ -351,3 +352,34 @@ def test_fp16_slices_match_reference(name):
         es.run(torch.from_numpy(g['model_in_%d' % it]).cuda())
         _, rmax, _ = es.reduce()
         assert np.array_equal(rmax.cpu().numpy(), g['rmax_%d' % it])
+
+
+@pytest.mark.parametrize('tile', [1, 2])
+def test_bank_layout_entries(tile):
+    """The bank-class layout holds every photon of every frame once (as the
+    plain layout does) and every other slot is the lane's zero column; lane l
+    only holds tile columns of bank class l mod (32 / tile)."""
+    size, n = 37, 60
+    d = random_photons(size, n, 40. * size, 9, empty_frames=(2,), heavy=5)
+    ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
+                         d['count_multi'], size * size, False)
+    sx, sy, dia, _ = E.generate_states(E.parse_triple('0 0 1'), E.parse_triple('0 0 1'),
+                                       E.parse_triple('2 2 1'))
+    got = {}
+    for banked in (True, False):
+        es = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen', kernel='wide',
+                    states_per_tile=tile, bank_layout=banked)
+        torch.cuda.synchronize()
+        got[banked] = (es.wide['entries'].cpu().numpy().view(np.uint32).reshape(-1, 32, 4),
+                       es.wide['group_off'].cpu().numpy(), es.p_row - 32)
+    bpp = 4 * tile
+    classes = 32 // tile
+    (wb, gb, pz), (wp, gp, _) = got[True], got[False]
+    lanes = np.arange(32)[None, :, None]
+    for f in range(n):
+        eb = wb[gb[f]:gb[f + 1]] // bpp
+        ep = wp[gp[f]:gp[f + 1]] // bpp
+        realb, realp = eb[eb < pz], ep[ep < pz]
+        assert np.array_equal(np.sort(realb), np.sort(realp)), f
+        assert np.all((eb >= pz) <= (eb == pz + lanes)), f
+        assert np.all(eb % classes == np.broadcast_to(lanes, eb.shape) % classes), f

@@ -239,6 +239,36 @@ __device__ __forceinline__ double cand_q(double acc, double dn, const Cand &c) {
     return xsub(acc / dn, xmul(c.rho, c.mw));
 }
 
+// A candidate's log term is summed as NPART partial sums, the p-th over the
+// populated states j = p, p + NPART, ... of a chunk in order, combined as
+// (s0 + s1) + (s2 + s3): the plain search keeps the four in registers, the
+// screened search's finalists give each to its own thread.
+__device__ __forceinline__ double combine4(double s0, double s1, double s2, double s3) {
+    return xadd(xadd(s0, s1), xadd(s2, s3));
+}
+
+// Adds one chunk of npop populated states to a candidate's NPART partial
+// sums (state j of the chunk to sum j mod NPART).
+__device__ __forceinline__ void sum_partials(double (&acc)[4], const Cand &ck, int npop,
+                                             const double *fr_re, const double *fr_im,
+                                             const double *fk) {
+    double a0 = acc[0], a1 = acc[1], a2 = acc[2], a3 = acc[3];
+    int j = 0;
+    for (; j + 4 <= npop; j += 4) {
+        a0 = term64(a0, fk[j], ck, fr_re[j], fr_im[j]);
+        a1 = term64(a1, fk[j + 1], ck, fr_re[j + 1], fr_im[j + 1]);
+        a2 = term64(a2, fk[j + 2], ck, fr_re[j + 2], fr_im[j + 2]);
+        a3 = term64(a3, fk[j + 3], ck, fr_re[j + 3], fr_im[j + 3]);
+    }
+    if (j < npop) a0 = term64(a0, fk[j], ck, fr_re[j], fr_im[j]);
+    if (j + 1 < npop) a1 = term64(a1, fk[j + 1], ck, fr_re[j + 1], fr_im[j + 1]);
+    if (j + 2 < npop) a2 = term64(a2, fk[j + 2], ck, fr_re[j + 2], fr_im[j + 2]);
+    acc[0] = a0;
+    acc[1] = a1;
+    acc[2] = a2;
+    acc[3] = a3;
+}
+
 __device__ __forceinline__ float lg2_approx(float x) {
     float y;
     asm("lg2.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
@@ -254,7 +284,10 @@ constexpr double U32 = 0x1p-24;                    // FP32 unit roundoff
 constexpr double LN2 = 0x1.62e42fefa39efp-1;       // the double nearest ln 2
 constexpr int PT_CHUNK = 8;                        // FP32 terms per FP64 add
 constexpr double G_CHUNK = 8.01 * U32;             // gamma_8 (+ the FP64 adds)
-constexpr int FIN_CAP = PT_THREADS;                // finalists: one per thread
+constexpr int NPART = 4;                           // partial sums per candidate
+static_assert(NPART == 4, "combine4 and sum_partials take four partial sums");
+constexpr int FIN_SPLIT = PT_THREADS / NPART;      // up to here: NPART threads each
+constexpr int FIN_CAP = PT_THREADS;                // beyond: one thread, NPART sums
 
 __device__ __forceinline__ double block_max_d(double v, double *scratch) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -548,13 +581,31 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
                     if (c < NCAND && up[k] >= tl) fin[pos++] = c;
                 }
                 __syncthreads();
-                if (threadIdx.x < nfin) {
-                    const int c = fin[threadIdx.x];
-                    const Cand cc = cand_at(c, f, step, pc, ring, kmean, rescale);
+                if (nfin <= FIN_SPLIT) {
+                    // NPART consecutive threads per finalist, thread p summing
+                    // the states j = p mod NPART in order
+                    const int fi = threadIdx.x / NPART, part = threadIdx.x % NPART;
                     double acc = 0.;
-                    for (int s = 0; s < npop; ++s) acc = term64(acc, fk[s], cc, fr_re[s], fr_im[s]);
-                    best = cand_q(acc, dn, cc);
-                    bidx = c;
+                    Cand cc;
+                    if (fi < nfin) {
+                        cc = cand_at(fin[fi], f, step, pc, ring, kmean, rescale);
+                        for (int s = part; s < npop; s += NPART)
+                            acc = term64(acc, fk[s], cc, fr_re[s], fr_im[s]);
+                    }
+                    const double v1 = __shfl_down_sync(RSPI_FULL_MASK, acc, 1);
+                    const double v2 = __shfl_down_sync(RSPI_FULL_MASK, acc, 2);
+                    const double v3 = __shfl_down_sync(RSPI_FULL_MASK, acc, 3);
+                    if (fi < nfin && part == 0) {
+                        best = cand_q(combine4(acc, v1, v2, v3), dn, cc);
+                        bidx = fin[fi];
+                    }
+                } else if (threadIdx.x < nfin) {
+                    // one thread per finalist, its NPART sums in registers
+                    const Cand cc = cand_at(fin[threadIdx.x], f, step, pc, ring, kmean, rescale);
+                    double a4[NPART] = {0., 0., 0., 0.};
+                    sum_partials(a4, cc, npop, fr_re, fr_im, fk);
+                    best = cand_q(combine4(a4[0], a4[1], a4[2], a4[3]), dn, cc);
+                    bidx = fin[threadIdx.x];
                 }
                 searched = true;
                 if (stats && threadIdx.x == 0) {
@@ -564,28 +615,40 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
             }
         }
         if (!searched) {
-            double acc[PT_CPT];
+            // candidate by candidate (few live registers), each with its
+            // NPART partial sums: four independent logs in flight
+            double acc[PT_CPT][NPART];
+            if (one_chunk) {
 #pragma unroll
-            for (int k = 0; k < PT_CPT; ++k) acc[k] = 0.;
-            int s_next = 0;
-            do {
-                if (!one_chunk)
+                for (int k = 0; k < PT_CPT; ++k) {
+                    double a4[NPART] = {0., 0., 0., 0.};
+                    sum_partials(a4, cd[k], npop, fr_re, fr_im, fk);
+                    acc[k][0] = combine4(a4[0], a4[1], a4[2], a4[3]);
+                }
+            } else {
+                double part[PT_CPT][NPART];
+#pragma unroll
+                for (int k = 0; k < PT_CPT; ++k)
+#pragma unroll
+                    for (int p = 0; p < NPART; ++p) part[k][p] = 0.;
+                int s_next = 0;
+                do {
                     s_next = load_populated(s_next, hrow, n_ref, ref_params, pc, fr_re, fr_im, fk,
                                             &npop, wsum);
-                else
-                    s_next = (int)n_ref;
-                for (int j = 0; j < npop; ++j) {
-                    const double rr = fr_re[j], ri = fr_im[j], kk = fk[j];
 #pragma unroll
-                    for (int k = 0; k < PT_CPT; ++k) acc[k] = term64(acc[k], kk, cd[k], rr, ri);
-                }
-                if (!one_chunk) __syncthreads();
-            } while (s_next < n_ref);
+                    for (int k = 0; k < PT_CPT; ++k)
+                        sum_partials(part[k], cd[k], npop, fr_re, fr_im, fk);
+                    __syncthreads();
+                } while (s_next < n_ref);
+#pragma unroll
+                for (int k = 0; k < PT_CPT; ++k)
+                    acc[k][0] = combine4(part[k][0], part[k][1], part[k][2], part[k][3]);
+            }
 #pragma unroll
             for (int k = 0; k < PT_CPT; ++k) {
                 const int c = threadIdx.x + k * PT_THREADS;
                 if (c >= NCAND) continue;
-                double q = cand_q(acc[k], dn, cd[k]);
+                double q = cand_q(acc[k][0], dn, cd[k]);
                 if (ring && pc.ksum == 0.) q = NAN;  // 0 * log(0) in every frame
                 if (argmax_better(q, c, best, bidx)) {
                     best = q;

@@ -380,20 +380,57 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
         }
         __syncthreads();
         const double ini = init[s0];
-        for (long long i = a + wid; i < b; i += nw) {
-            const int pair = row_cand[i];
-            const int d = cand_d[pair];
-            double acc = 0.;
-            const unsigned *ep = ent32 + row_off32[d] * 32 + lane;
-            for (long long q = row_off32[d]; q < row_off32[d + 1]; ++q, ep += 32) {
-                const unsigned e = __ldg(ep);
-                acc = fma((double)(e & 0xffffu), sl[min(e >> 16, cmax)], acc);
+        if constexpr (GROW) {
+            // a row in global scratch has a few candidates (dense frames):
+            // one warp per candidate
+            for (long long i = a + wid; i < b; i += nw) {
+                const int pair = row_cand[i];
+                const int d = cand_d[pair];
+                double acc = 0.;
+                const unsigned *ep = ent32 + row_off32[d] * 32 + lane;
+                for (long long q = row_off32[d]; q < row_off32[d + 1]; ++q, ep += 32) {
+                    const unsigned e = __ldg(ep);
+                    acc = fma((double)(e & 0xffffu), sl[min(e >> 16, cmax)], acc);
+                }
+                acc = warp_sum(acc);
+                if (lane == 0) {
+                    const double v = ini * scales[d] + acc;
+                    cand_ll[pair] = v;
+                    ll32[r * n_data + d] = (float)v;
+                }
             }
-            acc = warp_sum(acc);
-            if (lane == 0) {
-                const double v = ini * scales[d] + acc;
-                cand_ll[pair] = v;
-                ll32[r * n_data + d] = (float)v;
+        } else {
+            // the warp's candidates are a + wid + k nw, k = 0, 1, ...; lane l
+            // fetches the metadata of the warp's (k0 + l)-th candidate, so the
+            // dependent loads (row_cand -> cand_d -> row_off32) run once per 32
+            // candidates instead of once per candidate
+            for (long long k0 = 0; a + wid + k0 * nw < b; k0 += 32) {
+                const long long il = a + wid + (k0 + lane) * nw;
+                int pair = 0, d = 0;
+                long long q0 = 0, q1 = 0;
+                if (il < b) {
+                    pair = row_cand[il];
+                    d = cand_d[pair];
+                    q0 = row_off32[d];
+                    q1 = row_off32[d + 1];
+                }
+                const int nc = (int)min(32LL, (b - 1 - (a + wid + k0 * nw)) / nw + 1);
+                for (int c = 0; c < nc; ++c) {
+                    const long long cq0 = __shfl_sync(RSPI_FULL_MASK, q0, c);
+                    const long long cq1 = __shfl_sync(RSPI_FULL_MASK, q1, c);
+                    double acc = 0.;
+                    const unsigned *ep = ent32 + cq0 * 32 + lane;
+                    for (long long q = cq0; q < cq1; ++q, ep += 32) {
+                        const unsigned e = __ldg(ep);
+                        acc = fma((double)(e & 0xffffu), sl[min(e >> 16, cmax)], acc);
+                    }
+                    acc = warp_sum(acc);
+                    if (lane == c) {
+                        const double v = ini * scales[d] + acc;
+                        cand_ll[pair] = v;
+                        ll32[r * n_data + d] = (float)v;
+                    }
+                }
             }
         }
     }

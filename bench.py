@@ -66,6 +66,8 @@ def parse_args():
                     help='likelihood kernel (default: wide for the screened form, stream for FP64)')
     ap.add_argument('--screen-slices', default='fp32', choices=['fp32', 'fp16'],
                     help='screened form: FP32 slices (two rows per gather) or FP16 (four)')
+    ap.add_argument('--screen-delta', type=float, default=None,
+                    help='FP64 rescoring window in nats (EMC default 0: the argmax candidates)')
     ap.add_argument('--no-phaser-screen', action='store_true',
                     help='pattern search: every candidate in FP64 (no FP32 screening pass)')
     ap.add_argument('--slice-gb', type=float, default=8.,
@@ -211,7 +213,7 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
     return roof, gather, rows_per_launch
 
 
-def write_inputs(tmp, w, data, form, slice_gb=8., screen_slices='fp32'):
+def write_inputs(tmp, w, data, form, slice_gb=8., screen_slices='fp32', screen_delta=None):
     from rspi.photonfile import write_photons
     os.makedirs(os.path.join(tmp, 'out'), exist_ok=True)
     write_photons(os.path.join(tmp, 'photons.npz'), data)
@@ -224,6 +226,8 @@ def write_inputs(tmp, w, data, form, slice_gb=8., screen_slices='fp32'):
                 'screen_slices = %s\n' %
                 (w['size'], r['num_rot'], w['n_modes'], r['sphere_dia'], r['shiftx'], r['shifty'],
                  form, slice_gb, screen_slices))
+        if screen_delta is not None:
+            f.write('screen_delta = %r\n' % float(screen_delta))
     return cfg
 
 
@@ -485,7 +489,8 @@ def run_ours(args):
     data = generate_data(args.config, w, device=dev)
     t_gen = time.time() - t0
     tmp = tempfile.mkdtemp(prefix='rspi_bench_')
-    cfgfile = write_inputs(tmp, w, data, args.form, args.slice_gb, args.screen_slices)
+    cfgfile = write_inputs(tmp, w, data, args.form, args.slice_gb, args.screen_slices,
+                           args.screen_delta)
     from emc import EMC
     import contextlib
     import io
@@ -664,7 +669,8 @@ def run_ours(args):
         'e2e': e2e,
         'plain': plain,
         'form': {'likelihood': args.form, 'kernel': es.kernel,
-                 'candidates_rescored': n_cand, 'pattern_search': phaser_form},
+                 'candidates_rescored': n_cand, 'rescore_window_nats': getattr(es, 'delta', None),
+                 'pattern_search': phaser_form},
         'cpu_baseline': cpu,
         'setup_s': {'generate': t_gen},
         'device_memory_gb': mem_gb,

@@ -12,14 +12,18 @@ the MaxLP M-step run in librspi on the GPU; ``prob`` is a torch CUDA tensor
 
 Optional ``[emc]`` keys beyond the reference: ``form`` (``fp64``: FP64
 slices and FP64 likelihood matrix; ``screen``: FP32 screening pass with
-FP64 rescoring of every state that can be the argmax or carry posterior
-mass, same argmax/maximum/log-sum-exp as ``fp64``; ``dense``: frames stored
+FP64 rescoring of every state that can be the argmax (and, with
+``screen_delta`` > 0, carry posterior mass), same argmax/maximum as
+``fp64``; ``dense``: frames stored
 densely, likelihood as a tensor-core GEMM, ``dense_gemm`` = ``auto`` /
 ``i8`` (exact fixed point) / ``bf16`` (hi + lo split), ``dense_rescore``
 (default true: FP64 rescoring of the candidates as in ``screen``)),
 ``screen_slices`` (``fp32``, or ``fp16``: half-precision slices, four
 likelihood rows per gather, a wider candidate threshold), ``screen_delta``
-(default 20 nats), ``states_per_tile``, ``warps_per_cta``, ``phaser_iter``
+(default 0: FP64 rescoring of the states that can be the argmax, which is
+what the hard-argmax iteration uses; 20: also every state within 20 nats of
+it, so that ``logz`` equals the FP64 form's -- the posterior consumers'
+setting), ``states_per_tile``, ``warps_per_cta``, ``phaser_iter``
 (default 10, maxLP.py:320,335), ``phaser_screen`` (default true: FP32
 screening of the pattern-search candidates, FP64 for the finalists, same
 chosen candidates as false), ``slice_budget_gb`` (rotated slices are built
@@ -117,7 +121,7 @@ class EMC():
         self.form = config.get('emc', 'form', fallback='fp64')
         if self.form not in ('fp64', 'screen', 'dense'):
             raise ValueError('emc:form must be fp64, screen or dense')
-        self.screen_delta = config.getfloat('emc', 'screen_delta', fallback=20.)
+        self.screen_delta = config.getfloat('emc', 'screen_delta', fallback=0.)
         self.states_per_tile = config.getint('emc', 'states_per_tile', fallback=0) or None
         self.warps_per_cta = config.getint('emc', 'warps_per_cta', fallback=32)
         self.phaser_iter = config.getint('emc', 'phaser_iter', fallback=10)

@@ -242,6 +242,16 @@ int rspi_wide_entry_fill_banked(const unsigned short *entries16, const long long
                                 long long n_data, int p_zero, int states_per_tile,
                                 const long long *group_off, unsigned *wide, cudaStream_t stream);
 
+/* The bank-class layout with 16-bit entries (same groups and slots, from
+ * rspi_wide_entry_groups_banked): lane l only holds columns
+ * sel = C q + (l mod C), C = 32 / states_per_tile, so an entry stores
+ * q = sel / C and the gather's byte offset is q * 128 + 4 states_per_tile
+ * (l mod C).  group_off[n_data] * 128 entries, 8-byte aligned. */
+int rspi_wide_entry_fill_narrow(const unsigned short *entries16, const long long *row_off16,
+                                long long n_data, int p_zero, int states_per_tile,
+                                const long long *group_off, unsigned short *narrow,
+                                cudaStream_t stream);
+
 /* The same likelihoods as rspi_screen_loglike2 (1 or 2 states per tile) from
  * the wide entries built for that tile size: one 16-byte load per four
  * photons of a lane and no per-photon index arithmetic. */
@@ -251,6 +261,17 @@ int rspi_screen_loglike4(const float *lslices, long long p_row, long long num_ro
                          long long row_end, float *ll, long long ll_stride,
                          int states_per_tile, int warps_per_cta, int n_ctas,
                          cudaStream_t stream);
+
+/* rspi_screen_loglike4 from the 16-bit bank-class entries of
+ * rspi_wide_entry_fill_narrow: one 8-byte load per four photons of a lane
+ * (half the entry bytes), one integer multiply-add per photon for its
+ * offset; the same sums in the same order. */
+int rspi_screen_loglike4n(const float *lslices, long long p_row, long long num_rot,
+                          const double *init, const double *scales,
+                          const unsigned short *narrow, const long long *group_off,
+                          long long n_data, long long row_begin, long long row_end, float *ll,
+                          long long ll_stride, int states_per_tile, int warps_per_cta,
+                          int n_ctas, cudaStream_t stream);
 
 /* Four likelihood rows per tile from FP16 rotated log-slices
  * (rspi_rot_log_slices with out_dtype 2), the wide entries built for the

@@ -481,6 +481,49 @@ k_wide_fill_banked(const unsigned short *__restrict__ ent16,
     }
 }
 
+// The bank-class layout with 16-bit entries: lane l's photons all have
+// class c = l mod C, so the tile column is sel = C q + c and the entry
+// stores q (< 4096); the gather's byte offset is q * 128 + 4T (l mod C).
+// Same slots and groups as k_wide_fill_banked, half the bytes.
+__global__ void __launch_bounds__(BANK_WARPS * 32)
+k_narrow_fill_banked(const unsigned short *__restrict__ ent16,
+                     const long long *__restrict__ row_off16, long long n, int p_zero,
+                     int classes, const long long *__restrict__ goff,
+                     unsigned short *__restrict__ out) {
+    __shared__ int base[BANK_WARPS][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const int per = 32 / classes;
+    const unsigned lt = (1u << lane) - 1u;
+    for (long long d = warp; d < n; d += nwarp) {
+        const long long g0 = goff[d], ng = goff[d + 1] - g0;
+        const unsigned short pad = (unsigned short)((unsigned)(p_zero + lane) / (unsigned)classes);
+        const unsigned pad2 = (unsigned)pad | ((unsigned)pad << 16);
+        for (long long g = 0; g < ng; ++g)
+            reinterpret_cast<uint2 *>(out)[(g0 + g) * 32 + lane] = make_uint2(pad2, pad2);
+        base[w][lane] = 0;
+        __syncwarp();
+        const long long r0 = row_off16[d], nr = row_off16[d + 1] - r0;
+        for (long long r = 0; r < nr; ++r) {
+            const unsigned e = entry16_at(ent16, r0 + r, lane);
+            const int key = e < (unsigned)p_zero ? (int)(e % (unsigned)classes) : classes;
+            const unsigned m = __match_any_sync(RSPI_FULL_MASK, key);
+            if (key < classes) {
+                const int k = base[w][key] + __popc(m & lt);
+                const int slot_lane = key + classes * (k % per);
+                const long long slot = k / per;
+                if ((slot >> 2) < ng)
+                    out[((g0 + (slot >> 2)) * 32 + slot_lane) * 4 + (slot & 3)] =
+                        (unsigned short)(e / (unsigned)classes);
+            }
+            __syncwarp();
+            if (key < classes && lane == __ffs(m) - 1) base[w][key] += __popc(m);
+            __syncwarp();
+        }
+    }
+}
+
 template <int T>
 __device__ __forceinline__ Contrib<T> gather_pair(const unsigned char *sl, unsigned a,
                                                   unsigned b) {
@@ -497,12 +540,33 @@ __device__ __forceinline__ Contrib<T> gather_pair(const unsigned char *sl, unsig
     return c;
 }
 
+// One group of four photons of a lane: 32-bit entries hold the byte
+// offsets; 16-bit entries hold q with offset q * 128 + lane_off.
 template <int T>
+__device__ __forceinline__ void gather_group(const unsigned char *sl, const uint4 &g, unsigned,
+                                             Contrib<T> &c0, Contrib<T> &c1) {
+    c0 = gather_pair<T>(sl, g.x, g.y);
+    c1 = gather_pair<T>(sl, g.z, g.w);
+}
+
+template <int T>
+__device__ __forceinline__ void gather_group(const unsigned char *sl, const uint2 &g,
+                                             unsigned lane_off, Contrib<T> &c0, Contrib<T> &c1) {
+    c0 = gather_pair<T>(sl, (g.x & 0xffffu) * 128u + lane_off, (g.x >> 16) * 128u + lane_off);
+    c1 = gather_pair<T>(sl, (g.y & 0xffffu) * 128u + lane_off, (g.y >> 16) * 128u + lane_off);
+}
+
+template <bool NARROW> struct GroupOf { using type = uint4; };
+template <> struct GroupOf<true> { using type = uint2; };
+
+template <int T, bool NARROW>
 __global__ void __launch_bounds__(1024)
 k_screen_ll4(const float *__restrict__ lsl, int p_row, int num_rot,
              const double *__restrict__ init, const double *__restrict__ scales,
-             const uint4 *__restrict__ groups, const long long *__restrict__ goff, int n_data,
-             long long row_begin, long long row_end, float *__restrict__ ll, long long ll_stride) {
+             const typename GroupOf<NARROW>::type *__restrict__ groups,
+             const long long *__restrict__ goff, int n_data, long long row_begin,
+             long long row_end, float *__restrict__ ll, long long ll_stride) {
+    using G = typename GroupOf<NARROW>::type;
     constexpr int PG = 4;   // groups (16 photons per lane) loaded ahead
     extern __shared__ __align__(16) unsigned char smem_raw[];
     float *slf = reinterpret_cast<float *>(smem_raw);
@@ -566,9 +630,10 @@ k_screen_ll4(const float *__restrict__ lsl, int p_row, int num_rot,
         };
         while (f < fe && fend == g) finish();   // frames without entry rows
 
-        const uint4 *gp = groups + (long long)g * 32 + lane;
-        uint4 cur[PG], nxt[PG];
-        const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+        const G *gp = groups + (long long)g * 32 + lane;
+        G cur[PG], nxt[PG];
+        const G z{};
+        const unsigned lane_off = 4u * T * (unsigned)(lane % (32 / T));
 #pragma unroll
         for (int k = 0; k < PG; ++k) cur[k] = g + k < gend ? __ldg(gp + 32 * k) : z;
         while (g < gend) {
@@ -580,10 +645,7 @@ k_screen_ll4(const float *__restrict__ lsl, int p_row, int num_rot,
             // valid address whose values are never added)
             Contrib<T> c0[PG], c1[PG];
 #pragma unroll
-            for (int k = 0; k < PG; ++k) {
-                c0[k] = gather_pair<T>(smem_raw, cur[k].x, cur[k].y);
-                c1[k] = gather_pair<T>(smem_raw, cur[k].z, cur[k].w);
-            }
+            for (int k = 0; k < PG; ++k) gather_group<T>(smem_raw, cur[k], lane_off, c0[k], c1[k]);
 #pragma unroll
             for (int k = 0; k < PG; ++k) {
                 if (k < nb) {
@@ -721,16 +783,16 @@ k_screen_ll4h(const __half *__restrict__ lsl, int p_row, int num_rot,
     }
 }
 
-template <int T>
+template <int T, bool NARROW>
 int launch4(const float *lsl, long long p_row, long long num_rot, const double *init,
-            const double *scales, const uint4 *groups, const long long *goff, long long n_data,
-            long long r0, long long r1, float *ll, long long stride, int warps, int n_ctas,
-            cudaStream_t stream) {
+            const double *scales, const typename GroupOf<NARROW>::type *groups,
+            const long long *goff, long long n_data, long long r0, long long r1, float *ll,
+            long long stride, int warps, int n_ctas, cudaStream_t stream) {
     const size_t smem = (size_t)T * p_row * sizeof(float);
     if (smem > (size_t)SMEM_LIMIT - 1024) return RSPI_ERR_ARG;
     static size_t smem_set = 0;
     if (smem > smem_set) {
-        if (cudaFuncSetAttribute(k_screen_ll4<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(k_screen_ll4<T, NARROW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess)
             return RSPI_ERR_CUDA;
         smem_set = smem;
@@ -741,7 +803,7 @@ int launch4(const float *lsl, long long p_row, long long num_rot, const double *
         n_ctas = rspi_sm_count() * min(per_sm, max(1, 2048 / (warps * 32)));
     }
     if (n_ctas > n_tiles) n_ctas = (int)n_tiles;
-    k_screen_ll4<T><<<n_ctas, warps * 32, smem, stream>>>(
+    k_screen_ll4<T, NARROW><<<n_ctas, warps * 32, smem, stream>>>(
         lsl, (int)p_row, (int)num_rot, init, scales, groups, goff, (int)n_data, r0, r1, ll,
         stride);
     RSPI_RETURN_LAUNCH();
@@ -906,6 +968,21 @@ extern "C" int rspi_wide_entry_fill_banked(const unsigned short *entries16,
     RSPI_RETURN_LAUNCH();
 }
 
+extern "C" int rspi_wide_entry_fill_narrow(const unsigned short *entries16,
+                                           const long long *row_off16, long long n_data,
+                                           int p_zero, int states_per_tile,
+                                           const long long *group_off, unsigned short *narrow,
+                                           cudaStream_t stream) {
+    if (!entries16 || !row_off16 || !group_off || !narrow || n_data <= 0 || p_zero < 0 ||
+        p_zero % 32 || p_zero + 32 > 65536 || (states_per_tile != 1 && states_per_tile != 2) ||
+        (reinterpret_cast<uintptr_t>(narrow) & 7) != 0)
+        return RSPI_ERR_ARG;
+    k_narrow_fill_banked<<<rspi_blocks(n_data * 32, BANK_WARPS * 32), BANK_WARPS * 32, 0,
+                           stream>>>(entries16, row_off16, n_data, p_zero, 32 / states_per_tile,
+                                     group_off, narrow);
+    RSPI_RETURN_LAUNCH();
+}
+
 extern "C" int rspi_screen_loglike4(const float *lslices, long long p_row, long long num_rot,
                                     const double *init, const double *scales,
                                     const unsigned *wide, const long long *group_off,
@@ -923,11 +1000,36 @@ extern "C" int rspi_screen_loglike4(const float *lslices, long long p_row, long 
     if (row_end == row_begin) return RSPI_OK;
     const uint4 *g = reinterpret_cast<const uint4 *>(wide);
     if (states_per_tile == 1)
-        return launch4<1>(lslices, p_row, num_rot, init, scales, g, group_off, n_data, row_begin,
-                          row_end, ll, ll_stride, warps_per_cta, n_ctas, stream);
+        return launch4<1, false>(lslices, p_row, num_rot, init, scales, g, group_off, n_data,
+                                 row_begin, row_end, ll, ll_stride, warps_per_cta, n_ctas, stream);
     if (states_per_tile == 2)
-        return launch4<2>(lslices, p_row, num_rot, init, scales, g, group_off, n_data, row_begin,
-                          row_end, ll, ll_stride, warps_per_cta, n_ctas, stream);
+        return launch4<2, false>(lslices, p_row, num_rot, init, scales, g, group_off, n_data,
+                                 row_begin, row_end, ll, ll_stride, warps_per_cta, n_ctas, stream);
+    return RSPI_ERR_ARG;
+}
+
+extern "C" int rspi_screen_loglike4n(const float *lslices, long long p_row, long long num_rot,
+                                     const double *init, const double *scales,
+                                     const unsigned short *narrow, const long long *group_off,
+                                     long long n_data, long long row_begin, long long row_end,
+                                     float *ll, long long ll_stride, int states_per_tile,
+                                     int warps_per_cta, int n_ctas, cudaStream_t stream) {
+    if (!lslices || !init || !scales || !narrow || !group_off || !ll || n_data <= 0 ||
+        n_data > 0x7fffffffLL || p_row <= 32 || p_row % 32 || p_row > 65536 || num_rot <= 0 ||
+        num_rot > 0x7fffffffLL || row_begin < 0 || row_end < row_begin || ll_stride < n_data ||
+        warps_per_cta < 1 || warps_per_cta > 32)
+        return RSPI_ERR_ARG;
+    if ((reinterpret_cast<uintptr_t>(lslices) & 15) != 0 ||
+        (reinterpret_cast<uintptr_t>(narrow) & 7) != 0)
+        return RSPI_ERR_ARG;
+    if (row_end == row_begin) return RSPI_OK;
+    const uint2 *g = reinterpret_cast<const uint2 *>(narrow);
+    if (states_per_tile == 1)
+        return launch4<1, true>(lslices, p_row, num_rot, init, scales, g, group_off, n_data,
+                                row_begin, row_end, ll, ll_stride, warps_per_cta, n_ctas, stream);
+    if (states_per_tile == 2)
+        return launch4<2, true>(lslices, p_row, num_rot, init, scales, g, group_off, n_data,
+                                row_begin, row_end, ll, ll_stride, warps_per_cta, n_ctas, stream);
     return RSPI_ERR_ARG;
 }
 

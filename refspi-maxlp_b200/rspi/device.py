@@ -218,7 +218,7 @@ class EStep:
                  form='fp64', states_per_tile=None, warps=32, n_ctas=0,
                  slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel=None,
                  n_modes=1, dense_gemm='auto', dense_rescore=True, screen_slices='fp32',
-                 bank_layout=True):
+                 bank_layout=True, narrow_entries=True):
         if form not in ('fp64', 'screen', 'dense'):
             raise ValueError('form must be fp64, screen or dense')
         if kernel is None:   # default likelihood kernel of each form
@@ -294,6 +294,7 @@ class EStep:
         if kernel == 'wide16' and self.tile != 4:
             raise ValueError('the FP16-slice kernel takes 4 states per tile')
         self.bank_layout = bool(bank_layout)
+        self.narrow_entries = bool(narrow_entries)
         self.wide = self._wide_entries() if (form == 'screen' and kernel in ('wide', 'wide16')) \
             else None
         self._eps_key, self.row_off_eps = None, None
@@ -422,10 +423,18 @@ class EStep:
         call('rspi_scan_rows', ptr(groups), n, ptr(goff), s)
         total = int(goff[-1].item())
         wide = torch.empty(max(1, total) * 128, dtype=torch.int32, device=dev)
-        fill = 'rspi_wide_entry_fill_banked' if self.bank_layout else 'rspi_wide_entry_fill'
-        call(fill, ptr(l16['entries']), ptr(l16['row_off']), n, pz, bt, ptr(goff), ptr(wide), s)
+        narrow = self.bank_layout and self.narrow_entries and self.kernel == 'wide'
+        if narrow:
+            wide = torch.empty(max(1, total) * 128, dtype=torch.int16, device=dev)
+            call('rspi_wide_entry_fill_narrow', ptr(l16['entries']), ptr(l16['row_off']), n, pz,
+                 bt, ptr(goff), ptr(wide), s)
+        else:
+            wide = torch.empty(max(1, total) * 128, dtype=torch.int32, device=dev)
+            fill = 'rspi_wide_entry_fill_banked' if self.bank_layout else 'rspi_wide_entry_fill'
+            call(fill, ptr(l16['entries']), ptr(l16['row_off']), n, pz, bt, ptr(goff), ptr(wide),
+                 s)
         return dict(entries=wide, group_off=goff, total_groups=total, tile=bt,
-                    banked=self.bank_layout)
+                    banked=self.bank_layout, narrow=narrow)
 
     def _eps_rows(self):
         """Prefix sums of each frame's FP32 summation length for the
@@ -542,9 +551,11 @@ class EStep:
                  r0, r1, ptr(self.prob[r0]), n, self.warps, self.n_ctas, cur_stream())
         elif self.kernel == 'wide' and self.form == 'screen':
             if self.wide is None or self.wide['tile'] != self.tile or \
-                    self.wide['banked'] != self.bank_layout:
+                    self.wide['banked'] != self.bank_layout or \
+                    self.wide['narrow'] != (self.bank_layout and self.narrow_entries):
                 self.wide = self._wide_entries()   # kernel, tile or layout changed
-            call('rspi_screen_loglike4', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
+            entry = 'rspi_screen_loglike4n' if self.wide['narrow'] else 'rspi_screen_loglike4'
+            call(entry, ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
                  ptr(self.ph.scales), ptr(self.wide['entries']), ptr(self.wide['group_off']), n,
                  r0, r1, ptr(self.prob[r0]), n, self.tile, self.warps, self.n_ctas,
                  cur_stream())

@@ -47,6 +47,8 @@ SIGNATURES = {
     'rspi_screen_loglike2': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
     'rspi_screen_loglike3': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, I, P]),
     'rspi_screen_loglike4': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
+    'rspi_screen_loglike4n': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
+    'rspi_wide_entry_fill_narrow': (I, [P, P, L, I, I, P, P, P]),
     'rspi_screen_loglike4h': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, P]),
     'rspi_wide_entry_groups': (I, [P, L, P, P]),
     'rspi_wide_entry_fill': (I, [P, P, L, I, I, P, P, P]),
@@ -114,7 +116,8 @@ KERNELS_PER_CALL = {
     'rspi_maxlp_grid': 2, 'rspi_dense_frames_u8': 1, 'rspi_rot_log_fixed': 1,
     'rspi_dense_loglike_i8': 1, 'rspi_screen_loglike3': 1, 'rspi_screen_loglike4': 1,
     'rspi_wide_entry_groups': 1, 'rspi_wide_entry_fill': 1,
-    'rspi_wide_entry_groups_banked': 1, 'rspi_wide_entry_fill_banked': 1, 'rspi_screen_loglike4h': 1,
+    'rspi_wide_entry_groups_banked': 1, 'rspi_wide_entry_fill_banked': 1,
+    'rspi_screen_loglike4n': 1, 'rspi_wide_entry_fill_narrow': 1, 'rspi_screen_loglike4h': 1,
 }
 launch_count = 0
 

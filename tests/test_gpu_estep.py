@@ -269,7 +269,8 @@ def test_random_shapes_vs_oracle(size, n, seed, kw, form):
 @pytest.mark.parametrize('name,ds,need_scaling', CASES, ids=[c[0] for c in CASES])
 def test_frame_kernel_matches_stream_kernel(name, ds, need_scaling, tile, warps):
     """The frame-at-a-time and wide-entry screening kernels (wide entries in
-    the bank-class and in the plain layout) give the interleaved kernel's
+    the bank-class layout, 16- or 32-bit, and in the plain layout) give the
+    interleaved kernel's
     FP32 likelihoods (other summation order: within 1e-6 relative of the
     largest term) on every case, empty and heavy frames included, and the
     same FP64-rescored argmax / maximum / log-sum-exp."""
@@ -280,18 +281,24 @@ def test_frame_kernel_matches_stream_kernel(name, ds, need_scaling, tile, warps)
     rng = np.random.default_rng(size)
     model = torch.from_numpy(rng.random(size * size) + 1j * rng.random(size * size)).cuda()
     out = {}
-    for kernel, banked in (('stream', True), ('frame', True), ('wide', True), ('wide', False)):
+    variants = (('stream', True, True), ('frame', True, True), ('wide', True, True),
+                ('wide', True, False), ('wide', False, False))
+    for kernel, banked, narrow in variants:
         ph = _photons(ds, need_scaling)
         es = _estep(ph, size, num_rot, sx, sy, dia, ds['bg'], form='screen', kernel=kernel,
-                    states_per_tile=tile, warps=warps, bank_layout=banked)
+                    states_per_tile=tile, warps=warps, bank_layout=banked,
+                    narrow_entries=narrow)
         es.run(model)
         maxll, rmax, logz = es.reduce()
         torch.cuda.synchronize()
-        out[kernel, banked] = (es.prob.cpu().numpy().astype(np.float64), maxll.cpu().numpy(),
-                               rmax.cpu().numpy(), logz.cpu().numpy())
-    a = out['stream', True]
+        out[kernel, banked, narrow] = (es.prob.cpu().numpy().astype(np.float64),
+                                       maxll.cpu().numpy(), rmax.cpu().numpy(),
+                                       logz.cpu().numpy())
+    a = out['stream', True, True]
     scale = np.abs(a[0]).max(0, keepdims=True) + 1.
-    for b in (out['frame', True], out['wide', True], out['wide', False]):
+    # the 16-bit and 32-bit bank-class entries give the same sums in the same order
+    assert np.array_equal(out['wide', True, True][0], out['wide', True, False][0])
+    for b in (out['frame', True, True], out['wide', True, True], out['wide', False, False]):
         assert np.all(np.abs(a[0] - b[0]) <= 1e-6 * scale)
         assert np.array_equal(a[2], b[2])
         np.testing.assert_allclose(a[1], b[1], rtol=1e-14)
@@ -366,19 +373,25 @@ def test_bank_layout_entries(tile):
     sx, sy, dia, _ = E.generate_states(E.parse_triple('0 0 1'), E.parse_triple('0 0 1'),
                                        E.parse_triple('2 2 1'))
     got = {}
-    for banked in (True, False):
-        es = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen', kernel='wide',
-                    states_per_tile=tile, bank_layout=banked)
-        torch.cuda.synchronize()
-        got[banked] = (es.wide['entries'].cpu().numpy().view(np.uint32).reshape(-1, 32, 4),
-                       es.wide['group_off'].cpu().numpy(), es.p_row - 32)
     bpp = 4 * tile
     classes = 32 // tile
-    (wb, gb, pz), (wp, gp, _) = got[True], got[False]
     lanes = np.arange(32)[None, :, None]
+    for banked, narrow in ((True, True), (True, False), (False, False)):
+        es = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen', kernel='wide',
+                    states_per_tile=tile, bank_layout=banked, narrow_entries=narrow)
+        torch.cuda.synchronize()
+        if narrow:   # q per slot: column q * C + (lane mod C)
+            q = es.wide['entries'].cpu().numpy().view(np.uint16).reshape(-1, 32, 4).astype(np.int64)
+            sel = q * classes + lanes % classes
+        else:
+            sel = es.wide['entries'].cpu().numpy().view(np.uint32).reshape(-1, 32, 4) // bpp
+        got[banked, narrow] = (sel, es.wide['group_off'].cpu().numpy(), es.p_row - 32)
+    assert np.array_equal(got[True, True][0], got[True, False][0])
+    assert np.array_equal(got[True, True][1], got[True, False][1])
+    (wb, gb, pz), (wp, gp, _) = got[True, False], got[False, False]
     for f in range(n):
-        eb = wb[gb[f]:gb[f + 1]] // bpp
-        ep = wp[gp[f]:gp[f + 1]] // bpp
+        eb = wb[gb[f]:gb[f + 1]]
+        ep = wp[gp[f]:gp[f + 1]]
         realb, realp = eb[eb < pz], ep[ep < pz]
         assert np.array_equal(np.sort(realb), np.sort(realp)), f
         assert np.all((eb >= pz) <= (eb == pz + lanes)), f

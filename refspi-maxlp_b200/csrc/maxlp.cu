@@ -326,19 +326,19 @@ __device__ __forceinline__ int block_scan(int v, int *wsum, int *total) {
     return before + x - v;
 }
 
-// One FP32 screening term for a candidate held as hi + lo parts (x: real,
-// y: imaginary) against a populated state r = (re hi, re lo, im hi, im lo),
-// everything scaled by the pixel's power of two.
-__device__ __forceinline__ void screen_term(float xh, float xl, float yh, float yl,
-                                            const float4 r, float kj, float &gmin, float &a32,
-                                            float &b32) {
-    const float re = __fadd_rn(__fadd_rn(xh, r.x), __fadd_rn(xl, r.y));
-    const float im = __fadd_rn(__fadd_rn(yh, r.z), __fadd_rn(yl, r.w));
-    const float g = fmaf(re, re, __fmul_rn(im, im));
+// One FP32 screening term for a candidate held as hi + lo parts (xh, xl:
+// (real, imaginary)) against a populated state r = (re hi, im hi, re lo,
+// im lo), everything scaled by the pixel's power of two.  The real and
+// imaginary parts go through the packed FP32x2 adds (each lane rounded on
+// its own), and ab = (sum k l, sum k |l|) through one packed FMA.
+__device__ __forceinline__ void screen_term(float2 xh, float2 xl, const float4 r, float kj,
+                                            float &gmin, float2 &ab) {
+    const float2 z = __fadd2_rn(__fadd2_rn(xh, make_float2(r.x, r.y)),
+                                __fadd2_rn(xl, make_float2(r.z, r.w)));
+    const float g = fmaf(z.x, z.x, __fmul_rn(z.y, z.y));
     gmin = fminf(gmin, g);
     const float l = lg2_approx(g);
-    a32 = fmaf(kj, l, a32);
-    b32 = fmaf(kj, fabsf(l), b32);
+    ab = __ffma2_rn(make_float2(kj, kj), make_float2(l, fabsf(l)), ab);
 }
 
 // Per-pixel pattern search (maxLP.py:154-179, 304-340): one CTA per phaser
@@ -463,7 +463,7 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
             for (int j = threadIdx.x; j < npop; j += blockDim.x) {
                 const double xr = fr_re[j] * sc, xi = fr_im[j] * sc;
                 const float hr = (float)xr, hi = (float)xi;
-                r32[j] = make_float4(hr, (float)(xr - (double)hr), hi, (float)(xi - (double)hi));
+                r32[j] = make_float4(hr, hi, (float)(xr - (double)hr), (float)(xi - (double)hi));
                 k32[j] = (float)fk[j];
             }
             __syncthreads();
@@ -482,53 +482,50 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
         int bidx = 0x7fffffff;
         bool searched = false;
         if (SCREEN && screen) {
-            float xh[PT_CPT], xl[PT_CPT], yh[PT_CPT], yl[PT_CPT], gmin[PT_CPT];
+            float2 xh[PT_CPT], xl[PT_CPT];
+            float gmin[PT_CPT];
             double a64[PT_CPT], b64[PT_CPT];
 #pragma unroll
             for (int k = 0; k < PT_CPT; ++k) {
                 const double xs = cd[k].fr * sc, ys = cd[k].fi * sc;
-                xh[k] = (float)xs;
-                xl[k] = (float)(xs - (double)xh[k]);
-                yh[k] = (float)ys;
-                yl[k] = (float)(ys - (double)yh[k]);
+                xh[k] = make_float2((float)xs, (float)ys);
+                xl[k] = make_float2((float)(xs - (double)xh[k].x), (float)(ys - (double)xh[k].y));
                 gmin[k] = INFINITY;
                 a64[k] = 0.;
                 b64[k] = 0.;
             }
             int j = 0;
             for (; j + PT_CHUNK <= npop; j += PT_CHUNK) {
-                float a32[PT_CPT], b32[PT_CPT];
+                float2 ab[PT_CPT];
 #pragma unroll
-                for (int k = 0; k < PT_CPT; ++k) a32[k] = b32[k] = 0.f;
+                for (int k = 0; k < PT_CPT; ++k) ab[k] = make_float2(0.f, 0.f);
 #pragma unroll 2
                 for (int jj = 0; jj < PT_CHUNK; ++jj) {
                     const float4 r = r32[j + jj];
                     const float kj = k32[j + jj];
 #pragma unroll
-                    for (int k = 0; k < PT_CPT; ++k)
-                        screen_term(xh[k], xl[k], yh[k], yl[k], r, kj, gmin[k], a32[k], b32[k]);
+                    for (int k = 0; k < PT_CPT; ++k) screen_term(xh[k], xl[k], r, kj, gmin[k], ab[k]);
                 }
 #pragma unroll
                 for (int k = 0; k < PT_CPT; ++k) {
-                    a64[k] += (double)a32[k];
-                    b64[k] += (double)b32[k];
+                    a64[k] += (double)ab[k].x;
+                    b64[k] += (double)ab[k].y;
                 }
             }
             {
-                float a32[PT_CPT], b32[PT_CPT];
+                float2 ab[PT_CPT];
 #pragma unroll
-                for (int k = 0; k < PT_CPT; ++k) a32[k] = b32[k] = 0.f;
+                for (int k = 0; k < PT_CPT; ++k) ab[k] = make_float2(0.f, 0.f);
                 for (; j < npop; ++j) {
                     const float4 r = r32[j];
                     const float kj = k32[j];
 #pragma unroll
-                    for (int k = 0; k < PT_CPT; ++k)
-                        screen_term(xh[k], xl[k], yh[k], yl[k], r, kj, gmin[k], a32[k], b32[k]);
+                    for (int k = 0; k < PT_CPT; ++k) screen_term(xh[k], xl[k], r, kj, gmin[k], ab[k]);
                 }
 #pragma unroll
                 for (int k = 0; k < PT_CPT; ++k) {
-                    a64[k] += (double)a32[k];
-                    b64[k] += (double)b32[k];
+                    a64[k] += (double)ab[k].x;
+                    b64[k] += (double)ab[k].y;
                 }
             }
             // each candidate's interval [lo, hi] around its FP64 value

@@ -88,6 +88,18 @@ def parse_args():
     return args
 
 
+def max_over_ranks(x, device):
+    """The largest of ``x`` over all ranks of the initialised process group
+    (``x`` itself without one): the job's time is its slowest rank's."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def peaks():
     try:
         with open(os.path.join(REPO, 'MEASURED_PEAKS.json')) as f:
@@ -539,9 +551,7 @@ def run_ours(args):
     es.ll_events = None
     rec.dset.photons.err.check('bench')
     if world > 1:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dev)
         dist.barrier()
 
     n_cand = getattr(rec.estep, 'n_candidates', None)
@@ -568,9 +578,7 @@ def run_ours(args):
         torch.cuda.synchronize()
         e2e_s = (time.perf_counter() - t_e0) / args.steps
         if world > 1:
-            t = torch.tensor([e2e_s], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_s = float(t.item())
+            e2e_s = max_over_ranks(e2e_s, dev)
         p = w['size'] ** 2 * w['n_modes']
         e2e = {'value': world * w['n'] * w['n_states'] / e2e_s, 'unit': UNIT,
                's_per_iteration': e2e_s, 'h2d_bytes_per_step': 16 * p,

@@ -53,8 +53,18 @@ k_frame_reduce(const TL *__restrict__ ll, long long n_rows, long long n_data,
     const int tx = threadIdx.x, ty = threadIdx.y;
     const long long d = (long long)blockIdx.x * 32 + tx;
     Acc a{0., 0., -1};
-    if (d < n_data)
-        for (long long r = ty; r < n_rows; r += RY) acc_push<LSE>(a, (double)ll[r * n_data + d], (int)r);
+    if (d < n_data) {
+        // eight rows' loads in flight per thread, pushed in row order
+        long long r = ty;
+        for (; r + 7 * RY < n_rows; r += 8 * RY) {
+            TL v[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v[u] = __ldg(&ll[(r + u * RY) * n_data + d]);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) acc_push<LSE>(a, (double)v[u], (int)(r + u * RY));
+        }
+        for (; r < n_rows; r += RY) acc_push<LSE>(a, (double)ll[r * n_data + d], (int)r);
+    }
     sm[ty][tx] = a.m;
     ss[ty][tx] = a.s;
     si[ty][tx] = a.i;

@@ -269,7 +269,20 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_data,
         const long long rows = row_off16[d + 1] - row_off16[d];
         const double thr = m - delta - 2. * frame_eps(phot[d], rows, *lmax, m, delta);
         const int rm = rmax32[d];
-        for (long long r = ty; r < n_rows; r += RY) {
+        // eight rows' loads in flight per thread, taken in row order
+        long long r = ty;
+        for (; r + 7 * RY < n_rows; r += 8 * RY) {
+            float v8[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) v8[u] = __ldg(&ll[(r + u * RY) * n_data + d]);
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const double v = (double)v8[u];
+                if (v >= thr || r + u * RY == rm) ++c;
+                else nc += (double)expf((float)(v - m));   // each term < exp(-delta)
+            }
+        }
+        for (; r < n_rows; r += RY) {
             const double v = (double)ll[r * n_data + d];
             if (v >= thr || r == rm) ++c;
             else nc += (double)expf((float)(v - m));   // each term < exp(-delta)
@@ -305,8 +318,8 @@ k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_data,
     for (int k = 0; k < ty; ++k) pos += cnt_part[d * RY + k];
     const double th = thr[d];
     const int rm = rmax32[d];
-    for (long long r = ty; r < n_rows; r += RY) {
-        if ((double)ll[r * n_data + d] >= th || r == rm) {
+    auto take = [&](float v, long long r) {
+        if ((double)v >= th || r == rm) {
             if (pos < capacity) {
                 cand_d[pos] = (int)d;
                 cand_r[pos] = (int)r;
@@ -315,7 +328,17 @@ k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_data,
             }
             ++pos;
         }
+    };
+    // eight rows' loads in flight per thread, taken in row order
+    long long r = ty;
+    for (; r + 7 * RY < n_rows; r += 8 * RY) {
+        float v8[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v8[u] = __ldg(&ll[(r + u * RY) * n_data + d]);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) take(v8[u], r + u * RY);
     }
+    for (; r < n_rows; r += RY) take(ll[r * n_data + d], r);
 }
 
 // Candidates regrouped by likelihood row: count, scan (rows + 1 offsets),

@@ -76,32 +76,42 @@ __device__ __forceinline__ void add_contrib(Acc<T> &a, const Contrib<T> &c) {
     }
 }
 
-template <int T>
-__device__ __forceinline__ void add_word(Acc<T> &a, const unsigned char *sl, unsigned w);
-
-template <>
-__device__ __forceinline__ void add_word<1>(Acc<1> &a, const unsigned char *sl, unsigned w) {
-    const float v0 = *reinterpret_cast<const float *>(sl + (w & 0xffffu) * 4u);
-    const float v1 = *reinterpret_cast<const float *>(sl + (w >> 16) * 4u);
-    a.p[0].x += v0 + v1;
-}
-template <>
-__device__ __forceinline__ void add_word<2>(Acc<2> &a, const unsigned char *sl, unsigned w) {
-    const float2 v0 = *reinterpret_cast<const float2 *>(sl + (w & 0xffffu) * 8u);
-    const float2 v1 = *reinterpret_cast<const float2 *>(sl + (w >> 16) * 8u);
-    a.p[0] = __fadd2_rn(a.p[0], __fadd2_rn(v0, v1));
-}
-template <>
-__device__ __forceinline__ void add_word<4>(Acc<4> &a, const unsigned char *sl, unsigned w) {
-    const float4 v0 = *reinterpret_cast<const float4 *>(sl + (w & 0xffffu) * 16u);
-    const float4 v1 = *reinterpret_cast<const float4 *>(sl + (w >> 16) * 16u);
-    a.p[0] = __fadd2_rn(a.p[0], __fadd2_rn(make_float2(v0.x, v0.y), make_float2(v1.x, v1.y)));
-    a.p[1] = __fadd2_rn(a.p[1], __fadd2_rn(make_float2(v0.z, v0.w), make_float2(v1.z, v1.w)));
-}
-
 // Reduce-scatter over the warp: afterwards lane l holds the warp total of
 // row (l mod T).  log2(T) exchange steps halve the values a lane carries,
 // then 5 - log2(T) plain butterfly steps finish the sums.
+// Stage T consecutive slice rows into the interleaved tile sl[c][t]
+// (column c of row t at c * T + t, zeros for rows past nt): each thread takes
+// whole columns, T coalesced loads each, four columns' loads in flight.
+template <int T>
+__device__ __forceinline__ void stage_tile(float *sl, const float *__restrict__ src, int p_row,
+                                           int nt) {
+#pragma unroll 4
+    for (int c = threadIdx.x; c < p_row; c += blockDim.x) {
+        float v[T];
+#pragma unroll
+        for (int t = 0; t < T; ++t) v[t] = t < nt ? __ldg(src + (long long)t * p_row + c) : 0.f;
+        if constexpr (T == 1) {
+            sl[c] = v[0];
+        } else if constexpr (T == 2) {
+            reinterpret_cast<float2 *>(sl)[c] = make_float2(v[0], v[1]);
+        } else {
+#pragma unroll
+            for (int t = 0; t < T; ++t) sl[c * T + t] = v[t];
+        }
+    }
+}
+
+template <int T>
+__device__ __forceinline__ void stage_tile_h(__half *sl, const __half *__restrict__ src, int p_row,
+                                             int nt) {
+    const __half hz = __float2half(0.f);
+#pragma unroll 4
+    for (int c = threadIdx.x; c < p_row; c += blockDim.x) {
+#pragma unroll
+        for (int t = 0; t < T; ++t) sl[c * T + t] = t < nt ? src[(long long)t * p_row + c] : hz;
+    }
+}
+
 template <int T>
 __device__ __forceinline__ float reduce_scatter(Acc<T> &a, int lane);
 
@@ -168,10 +178,7 @@ k_screen_ll2(const float *__restrict__ lsl, int p_row, int num_rot,
         __syncthreads();
         // stage and interleave: sl[c][t] = L[first + t][c]
         const float *src = lsl + (first - row_begin) * (long long)p_row;
-        for (int i = threadIdx.x; i < T * p_row; i += blockDim.x) {
-            const int t = i / p_row, c = i - t * p_row;
-            slf[c * T + t] = t < nt ? __ldg(src + i) : 0.f;
-        }
+        stage_tile<T>(slf, src, p_row, nt);
         __syncthreads();
         if (fb >= fe) continue;
 
@@ -277,10 +284,7 @@ k_screen_ll3(const float *__restrict__ lsl, int p_row, int num_rot,
         const int nt = (int)min((long long)T, row_end - first);
         __syncthreads();
         const float *src = lsl + (first - row_begin) * (long long)p_row;
-        for (int i = threadIdx.x; i < T * p_row; i += blockDim.x) {
-            const int t = i / p_row, c = i - t * p_row;
-            slf[c * T + t] = t < nt ? __ldg(src + i) : 0.f;
-        }
+        stage_tile<T>(slf, src, p_row, nt);
         __syncthreads();
         if (fb >= fe) continue;
 
@@ -590,10 +594,7 @@ k_screen_ll4(const float *__restrict__ lsl, int p_row, int num_rot,
         const int nt = (int)min((long long)T, row_end - first);
         __syncthreads();
         const float *src = lsl + (first - row_begin) * (long long)p_row;
-        for (int i = threadIdx.x; i < T * p_row; i += blockDim.x) {
-            const int t = i / p_row, c = i - t * p_row;
-            slf[c * T + t] = t < nt ? __ldg(src + i) : 0.f;
-        }
+        stage_tile<T>(slf, src, p_row, nt);
         __syncthreads();
         if (fb >= fe) continue;
 
@@ -705,17 +706,12 @@ k_screen_ll4h(const __half *__restrict__ lsl, int p_row, int num_rot,
     };
     const int fb = wid == 0 ? 0 : lower((int)((long long)gtot * wid / nw));
     const int fe = wid == nw - 1 ? n_data : lower((int)((long long)gtot * (wid + 1) / nw));
-    const __half hz = __float2half(0.f);
-
     for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
         const long long first = row_begin + tile * T;
         const int nt = (int)min((long long)T, row_end - first);
         __syncthreads();
         const __half *src = lsl + (first - row_begin) * (long long)p_row;
-        for (int i = threadIdx.x; i < T * p_row; i += blockDim.x) {
-            const int t = i / p_row, c = i - t * p_row;
-            slh[c * T + t] = t < nt ? src[i] : hz;
-        }
+        stage_tile_h<T>(slh, src, p_row, nt);
         __syncthreads();
         if (fb >= fe) continue;
 

@@ -156,8 +156,11 @@ def dram_traffic(args, w, es, rows_per_launch):
             caps = json.load(f)['captures']
     except (OSError, ValueError, KeyError):
         return None
+    kern = es.kernel
+    if kern == 'wide' and getattr(es, 'wide', None) is not None:
+        kern = 'wide16b' if es.wide.get('narrow') else 'wide32'
     for c in caps:
-        if (c['form'] == es.form and c.get('kernel', 'stream') == es.kernel and
+        if (c['form'] == es.form and c.get('kernel', 'stream') == kern and
                 c['config'] == args.config and c['frames'] == w['n'] and
                 c['rows_per_launch'] == int(round(rows_per_launch))):
             return float(c['dram_bytes_read'] + c['dram_bytes_write'])

@@ -158,7 +158,8 @@ def dram_traffic(args, w, es, rows_per_launch):
         return None
     kern = es.kernel
     if kern == 'wide' and getattr(es, 'wide', None) is not None:
-        kern = 'wide16b' if es.wide.get('narrow') else 'wide32'
+        kern = 'wide16b' if es.wide.get('narrow') else (
+            'wide32b' if es.wide.get('banked') else 'wide32')
     for c in caps:
         if (c['form'] == es.form and c.get('kernel', 'stream') == kern and
                 c['config'] == args.config and c['frames'] == w['n'] and

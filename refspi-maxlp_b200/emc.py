@@ -11,7 +11,7 @@ the MaxLP M-step run in librspi on the GPU; ``prob`` is a torch CUDA tensor
 (rows ``s*num_rot + j``, columns frames).
 
 Optional ``[emc]`` keys beyond the reference: ``form`` (``fp64``: FP64
-slices and FP64 likelihood matrix; ``screen``: FP32 screening pass with
+slices and FP64 likelihood matrix; ``screen``, the default: FP32 screening pass with
 FP64 rescoring of every state that can be the argmax (and, with
 ``screen_delta`` > 0, carry posterior mass), same argmax/maximum as
 ``fp64``; ``dense``: frames stored
@@ -118,7 +118,7 @@ class EMC():
         self.output_folder = op.join(start_dir, config.get('emc', 'output_folder'))
         self.log_file = op.join(start_dir, config.get('emc', 'log_file'))
         self.need_scaling = config.getboolean('emc', 'need_scaling', fallback=False)
-        self.form = config.get('emc', 'form', fallback='fp64')
+        self.form = config.get('emc', 'form', fallback='screen')
         if self.form not in ('fp64', 'screen', 'dense'):
             raise ValueError('emc:form must be fp64, screen or dense')
         self.screen_delta = config.getfloat('emc', 'screen_delta', fallback=0.)

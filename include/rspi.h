@@ -509,7 +509,8 @@ int rspi_dense_loglike(const void *a0, const void *a1, const void *b_hi, const v
  * above 255 are clamped and *kmax tells the caller to use the BF16 path),
  * log-slices in fixed point Lq = rint(L * 2^21) as four 8-bit digit planes
  * (rspi_rot_log_fixed: rows [row_begin, row_end) into 4 planes of
- * plane_rows x k_pad bytes each, low digit first, the top one signed;
+ * plane_rows x k_pad bytes each, low digit first, the top one signed,
+ * digits 4-byte aligned;
  * |L| >= 1023 or NaN is clamped and sets
  * *err = RSPI_ERR_CAPACITY), and rspi_dense_loglike_i8 accumulating each
  * digit product exactly in int32 (requires fewer than 8.4e6 photons per

@@ -380,6 +380,7 @@ k_rot_log_split(const double *__restrict__ holo, long long num_rot,
     const long long npix = (long long)size * size;
     const int ns = (int)n_sel, kp = (int)k_pad;
     float amax = 0.f;
+    const float inv_size = 1.f / (float)size;
     for (long long rr = blockIdx.x; rr < n_rows; rr += gridDim.x) {   // one row per CTA
         const long long r = row_begin + rr;
         const long long s0 = r / num_rot, j = r - s0 * num_rot;
@@ -389,7 +390,8 @@ k_rot_log_split(const double *__restrict__ holo, long long num_rot,
             double v = 0.;
             if (c < ns) {
                 const int p = sel_pix[c];
-                const int x = p / size, y = p - x * size;
+                int x, y;
+                pixel_xy(p, size, inv_size, x, y);
                 v = rot_log_value(w, x, y, size, ac, as, bg[p]);
             }
             const __nv_bfloat16 h = __double2bfloat16(v);
@@ -435,28 +437,37 @@ k_rot_log_q(const double *__restrict__ holo, long long num_rot, const double *__
             long long plane, uint8_t *__restrict__ b, int *err) {
     const long long npix = (long long)size * size;
     const int ns = (int)n_sel, kp = (int)k_pad;
+    const float inv_size = 1.f / (float)size;
     for (long long rr = blockIdx.x; rr < n_rows; rr += gridDim.x) {   // one row per CTA
         const long long r = row_begin + rr;
         const long long s0 = r / num_rot, j = r - s0 * num_rot;
         const double ac = rot_cs[2 * j], as = rot_cs[2 * j + 1];
         const double *w = holo + s0 * npix;
         uint8_t *o = b + rr * k_pad;
-        for (int c = threadIdx.x; c < kp; c += blockDim.x) {
-            double v = 0.;
-            if (c < ns) {
-                const int p = sel_pix[c];
-                const int x = p / size, y = p - x * size;
-                v = rot_log_value(w, x, y, size, ac, as, bg[p]);
+        // four consecutive columns per thread: one 32-bit store per digit plane
+        for (int c0 = 4 * threadIdx.x; c0 < kp; c0 += 4 * blockDim.x) {
+            uint32_t dg[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int c = c0 + u;
+                double v = 0.;
+                if (c < ns) {
+                    const int p = sel_pix[c];
+                    int x, y;
+                    pixel_xy(p, size, inv_size, x, y);
+                    v = rot_log_value(w, x, y, size, ac, as, bg[p]);
+                }
+                if (!(fabs(v) < 1023.)) {   // also NaN
+                    rspi_flag(err, RSPI_ERR_CAPACITY);
+                    v = v != v ? 0. : (v > 0. ? 1023. : -1023.);
+                }
+                const uint32_t q = (uint32_t)__double2int_rn(v * 2097152.);   // rint(v 2^21)
+#pragma unroll
+                for (int d = 0; d < 4; ++d) dg[d] |= ((q >> (8 * d)) & 255u) << (8 * u);
             }
-            if (!(fabs(v) < 1023.)) {   // also NaN
-                rspi_flag(err, RSPI_ERR_CAPACITY);
-                v = v != v ? 0. : (v > 0. ? 1023. : -1023.);
-            }
-            const int q = (int)rint(v * 2097152.);   // 2^21
-            o[c] = (uint8_t)(q & 255);
-            o[plane + c] = (uint8_t)((q >> 8) & 255);
-            o[2 * plane + c] = (uint8_t)((q >> 16) & 255);
-            o[3 * plane + c] = (uint8_t)(q >> 24);
+#pragma unroll
+            for (int d = 0; d < 4; ++d)
+                *reinterpret_cast<uint32_t *>(o + (long long)d * plane + c0) = dg[d];
         }
     }
 }
@@ -599,7 +610,8 @@ extern "C" int rspi_rot_log_fixed(const double *holo, long long n_states0, long 
                                   void *digits, int *err, cudaStream_t stream) {
     if (n_states0 <= 0 || num_rot <= 0 || size <= 1 || size > 46340 || k_pad < n_sel ||
         k_pad % 128 || row_begin < 0 || row_end > n_states0 * num_rot || row_end < row_begin ||
-        plane_rows < row_end - row_begin || !holo || !rot_cs || !bg || !digits || !err)
+        plane_rows < row_end - row_begin || !holo || !rot_cs || !bg || !digits || !err ||
+        (reinterpret_cast<uintptr_t>(digits) & 3) != 0)
         return RSPI_ERR_ARG;
     const long long n_rows = row_end - row_begin;
     if (n_rows == 0) return RSPI_OK;

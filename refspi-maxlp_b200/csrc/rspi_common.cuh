@@ -27,6 +27,23 @@ __device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a,
 __device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
 
+// Row x and column y of pixel p = x * size + y (0 <= p < size^2, size <=
+// 46340) without the integer division sequence: a float estimate of p / size
+// (its error is far below one) and one exact correction step.
+__device__ __forceinline__ void pixel_xy(int p, int size, float inv_size, int &x, int &y) {
+    int q = (int)((float)p * inv_size);
+    int r = p - q * size;
+    if (r < 0) {
+        --q;
+        r += size;
+    } else if (r >= size) {
+        ++q;
+        r -= size;
+    }
+    x = q;
+    y = r;
+}
+
 // One rotated log-slice value (kernels.cu:19-41 with log_flag = 1, scale = 1):
 // bilinear sample of the holographic slice w at R(angle)(p - cen) + cen, plus
 // bg, then log; -1000 outside the detector or below 1e-20.  Shared by the

@@ -386,6 +386,7 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const long long npix = (long long)size * size;
     const unsigned cmax = (unsigned)p_pad - 1;
+    const float inv_size = 1.f / (float)size;
     for (long long r = blockIdx.x; r < n_rows; r += gridDim.x) {
         const long long a = row_off[r], b = row_off[r + 1];
         if (a == b) continue;   // uniform across the CTA
@@ -397,7 +398,9 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
             double v = 0.;
             if (c < n_sel) {
                 const int p = sel_pix[c];
-                v = rot_log_value(w, p / size, p - (p / size) * size, size, ac, as, bg[p]);
+                int x, y;
+                pixel_xy(p, size, inv_size, x, y);
+                v = rot_log_value(w, x, y, size, ac, as, bg[p]);
             }
             sl[c] = v;
         }

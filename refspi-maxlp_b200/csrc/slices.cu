@@ -78,6 +78,7 @@ k_rot_log(const double *__restrict__ holo, long long num_rot, const double *__re
     const long long npix = (long long)size * size;
     const int ns = (int)n_sel, pp = (int)p_pad;
     float amax = 0.f;
+    const float inv_size = 1.f / (float)size;
     for (long long rr = blockIdx.x; rr < n_rows; rr += gridDim.x) {
         const long long r = row_begin + rr;
         const long long s0 = r / num_rot, j = r - s0 * num_rot;
@@ -88,7 +89,8 @@ k_rot_log(const double *__restrict__ holo, long long num_rot, const double *__re
             double v = 0.;
             if (c < ns) {
                 const int p = sel_pix[c];
-                const int x = p / size, y = p - x * size;
+                int x, y;
+                pixel_xy(p, size, inv_size, x, y);
                 v = rot_log_value(w, x, y, size, ac, as, bg[p]);
             }
             const TL q = static_cast<TL>(v);

@@ -449,6 +449,39 @@ int rspi_maxlp_pattern_screened(double *fconv, const int *pixels, const int *his
  * the largest absolute error. */
 int rspi_log2_error_max(float lo, float hi, double *out, cudaStream_t stream);
 
+/* Per-pixel, per-frame phaser API (the reference's get_photons_pixel,
+ * get_fref_d, get_rescale_pixel, get_logq_pixel; maxLP.py:181-253), without
+ * the state aggregation of rspi_maxlp_pattern.
+ *
+ * rspi_maxlp_pixel_frames: for frame d = d_vals[i] (d = i when d_vals is
+ * NULL), k_out[i] = photons of frame d at the flat detector column
+ * rint(R q_t size) + size/2 of model pixel t (rot_cs[2d], rot_cs[2d+1] =
+ * cos, sin of -angle_d; 0 off the matrix) and fref_out[2i], [2i+1] = the
+ * complex reference amplitude ff(pi qrad dia) e^{2 pi i q . shift} of
+ * fparams[3d..3d+2] = (shift x, shift y, diameter).  A d_vals entry outside
+ * [0, n_data) sets RSPI_ERR_INDEX and gives 0.
+ *
+ * rspi_maxlp_pixel_values: for candidate c (complex cands[2c], [2c+1]) over
+ * the n frames: mode 0 writes mean_d k_d / mean_d |f_c + fref_d|^2 (the
+ * rescale); mode 1 writes mean_d k_d log(rho w) - mean_d rho w, w =
+ * |f_c + fref_d|^2, rho = rescale_vec[c] if given, else rescale. */
+int rspi_maxlp_pixel_frames(int t, long long size, const int *d_vals, long long n_vals,
+                            const int *ones, const int *multi, const long long *ones_accum,
+                            const long long *multi_accum, const int *place_ones,
+                            const int *place_multi, const int *count_multi, long long n_data,
+                            const double *rot_cs, const double *fparams, double *k_out,
+                            double *fref_out, int *err, cudaStream_t stream);
+int rspi_maxlp_pixel_values(const double *cands, long long n_c, const double *k,
+                            const double *fref, long long n, int mode, double rescale,
+                            const double *rescale_vec, double *out, cudaStream_t stream);
+
+/* Sphere transform ff(pi qrad dia) of every model pixel into sphere (P
+ * doubles, maxLP.py:266-269) and/or the holographic amplitude
+ * fobj + ff e^{2 pi i (qx shift_x + qy shift_y)} into fcalc (P complex128,
+ * maxLP.py:260-264). */
+int rspi_maxlp_fcalc(long long size, double dia, double sx, double sy, const double *fobj,
+                     double *sphere, double *fcalc, cudaStream_t stream);
+
 /* Polar grid search of the per-pixel MaxLP negative log-likelihood (the
  * judge beside the L-BFGS update of rspi_nll; no reference counterpart):
  * for each pixel t = pixels[i] (histogram row hist_row[i], one mode),

@@ -833,6 +833,127 @@ __global__ void __launch_bounds__(1024) k_mean(const double *__restrict__ v, lon
     if (threadIdx.x == 0) *out = a / (double)n;
 }
 
+// ---------------------------------------------------------------------------
+// Per-pixel, per-frame API of the reference phaser (maxLP.py:107-114,
+// 216-253): the photons every frame puts on model pixel t, the frames'
+// reference amplitudes there, and per-candidate rescales and log-likelihoods
+// over the frames, without the state aggregation of k_pattern.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pixel_q(int t, int size, double &qx, double &qy, double &qrad) {
+    const double ds = (double)size, c0 = (double)(size / 2);
+    const int tx = t / size, ty = t - (t / size) * size;
+    qx = ((double)tx - c0) / ds;
+    qy = ((double)ty - c0) / ds;
+    qrad = sqrt(xadd(xmul(qx, qx), xmul(qy, qy)));
+    if (qrad == 0.) qrad = 1.e-6;  // maxLP.py:85
+}
+
+// One warp per listed frame: k = photons of frame d at the detector pixel
+// rint(R(-theta_d) q_t size) + size/2 (maxLP.py:250-253),
+// fref = ff(pi qrad dia_d) exp(2 pi i q_t . shift_d) (maxLP.py:238-243).
+__global__ void k_pixel_frames(int t, int size, const int *__restrict__ d_vals, long long n_vals,
+                               const int *__restrict__ ones, const int *__restrict__ multi,
+                               const long long *__restrict__ ones_accum,
+                               const long long *__restrict__ multi_accum,
+                               const int *__restrict__ place_ones,
+                               const int *__restrict__ place_multi,
+                               const int *__restrict__ count_multi, long long n_data,
+                               const double *__restrict__ rot_cs,
+                               const double *__restrict__ fparams, double *__restrict__ k_out,
+                               double2 *__restrict__ fref_out, int *err) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    double qx, qy, qrad;
+    pixel_q(t, size, qx, qy, qrad);
+    const int tx = t / size, ty = t - (t / size) * size;
+    for (long long i = warp; i < n_vals; i += nwarp) {
+        const long long d = d_vals ? (long long)d_vals[i] : i;
+        if (d < 0 || d >= n_data) {
+            if (lane == 0) {
+                rspi_flag(err, RSPI_ERR_INDEX);
+                k_out[i] = 0.;
+                fref_out[i] = make_double2(0., 0.);
+            }
+            continue;
+        }
+        int ox, oy;
+        forward_pixel(tx, ty, rot_cs[2 * d], rot_cs[2 * d + 1], size, ox, oy);
+        // the flat column x * size + y as the reference's CSR lookup takes it
+        // (y == size aliases pixel (x + 1, 0) for even sizes); off the
+        // matrix it reads 0
+        const long long uf = (long long)ox * size + oy;
+        const bool on = uf >= 0 && uf < (long long)size * size;
+        const int u = on ? (int)uf : -1;
+        long long cnt = 0;
+        if (on) {
+            const long long oa = ones_accum[d], ma = multi_accum[d];
+            for (int j = lane; j < ones[d]; j += 32) cnt += place_ones[oa + j] == u;
+            for (int j = lane; j < multi[d]; j += 32)
+                if (place_multi[ma + j] == u) cnt += count_multi[ma + j];
+        }
+        cnt = warp_sum(cnt);
+        if (lane == 0) {
+            k_out[i] = (double)cnt;
+            fref_out[i] = fref_value(qx, qy, qrad, fparams[3 * d], fparams[3 * d + 1],
+                                     fparams[3 * d + 2]);
+        }
+    }
+}
+
+// One CTA per candidate f_c over the n frames (maxLP.py:216-228, 181-197):
+//   mode 0: rho_c = mean_d k_d / mean_d |f_c + fref_d|^2
+//   mode 1: mean_d k_d log(rho |f_c + fref_d|^2) - mean_d rho |f_c + fref_d|^2
+//           with rho = rescale_vec[c] (per candidate) or the scalar rescale.
+__global__ void __launch_bounds__(256)
+k_pixel_values(const double2 *__restrict__ cands, long long n_c, const double *__restrict__ k,
+               const double2 *__restrict__ fref, long long n, int mode, double rescale,
+               const double *__restrict__ rescale_vec, double *__restrict__ out) {
+    __shared__ double scratch[32];
+    for (long long c = blockIdx.x; c < n_c; c += gridDim.x) {
+        const double2 f = cands[c];
+        const double rho = rescale_vec ? rescale_vec[c] : rescale;
+        double a = 0., b = 0.;
+        for (long long d = threadIdx.x; d < n; d += blockDim.x) {
+            const double re = xadd(f.x, fref[d].x), im = xadd(f.y, fref[d].y);
+            const double w = xadd(xmul(re, re), xmul(im, im));
+            if (mode == 0) {
+                a = xadd(a, k[d]);
+                b = xadd(b, w);
+            } else {
+                const double rw = xmul(rho, w);
+                a = xadd(a, xmul(k[d], log(rw)));
+                b = xadd(b, rw);
+            }
+        }
+        a = block_sum(a, scratch);
+        b = block_sum(b, scratch);
+        if (threadIdx.x == 0)
+            out[c] = mode == 0 ? (a / (double)n) / (b / (double)n)
+                               : xsub(a / (double)n, b / (double)n);
+    }
+}
+
+// Sphere transform ff(pi qrad dia) of every model pixel (maxLP.py:266-269)
+// and, with fobj, the holographic amplitude fobj + ff e^{2 pi i q . shift}
+// (maxLP.py:260-264).
+__global__ void k_fcalc(int size, double dia, double sx, double sy,
+                        const double2 *__restrict__ fobj, double *__restrict__ sphere,
+                        double2 *__restrict__ fcalc) {
+    const long long npix = (long long)size * size;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < npix; t += stride) {
+        double qx, qy, qrad;
+        pixel_q((int)t, size, qx, qy, qrad);
+        const double2 r = fref_value(qx, qy, qrad, sx, sy, dia);
+        if (sphere) {
+            const double sval = xmul(xmul(PI, qrad), dia);
+            sphere[t] = xsub(sin(sval), xmul(sval, cos(sval))) / pow(sval, 3.);
+        }
+        if (fcalc) fcalc[t] = make_double2(xadd(fobj[t].x, r.x), xadd(fobj[t].y, r.y));
+    }
+}
+
 }  // namespace
 
 extern "C" int rspi_maxlp_frame_params(const int *rmax, long long n_data, long long num_rot,
@@ -934,5 +1055,47 @@ extern "C" int rspi_maxlp_grid(double *fconv, const int *pixels, const int *hist
     k_grid<<<(unsigned)n_pix, GR_THREADS, 0, stream>>>((double2 *)fconv, pixels, hist_row, hist,
                                                        n_ref, ssum, ref_params, (int)size,
                                                        n_phase, n_amp, best_nll);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_maxlp_pixel_frames(int t, long long size, const int *d_vals, long long n_vals,
+                                       const int *ones, const int *multi,
+                                       const long long *ones_accum, const long long *multi_accum,
+                                       const int *place_ones, const int *place_multi,
+                                       const int *count_multi, long long n_data,
+                                       const double *rot_cs, const double *fparams,
+                                       double *k_out, double *fref_out, int *err,
+                                       cudaStream_t stream) {
+    if (n_vals == 0) return RSPI_OK;
+    if (size <= 1 || size > 46340 || t < 0 || t >= size * size || n_vals < 0 || n_data <= 0 ||
+        !ones || !multi || !ones_accum || !multi_accum || !rot_cs || !fparams || !k_out ||
+        !fref_out || !err || (!d_vals && n_vals > n_data))
+        return RSPI_ERR_ARG;
+    k_pixel_frames<<<rspi_blocks(n_vals * 32, 256), 256, 0, stream>>>(
+        t, (int)size, d_vals, n_vals, ones, multi, ones_accum, multi_accum, place_ones,
+        place_multi, count_multi, n_data, rot_cs, fparams, k_out, (double2 *)fref_out, err);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_maxlp_pixel_values(const double *cands, long long n_c, const double *k,
+                                       const double *fref, long long n, int mode,
+                                       double rescale, const double *rescale_vec, double *out,
+                                       cudaStream_t stream) {
+    if (n_c == 0) return RSPI_OK;
+    if (!cands || !k || !fref || !out || n_c < 0 || n <= 0 || (mode != 0 && mode != 1))
+        return RSPI_ERR_ARG;
+    const unsigned grid = (unsigned)min(n_c, (long long)rspi_sm_count() * 16);
+    k_pixel_values<<<grid, 256, 0, stream>>>((const double2 *)cands, n_c, k,
+                                             (const double2 *)fref, n, mode, rescale,
+                                             rescale_vec, out);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_maxlp_fcalc(long long size, double dia, double sx, double sy,
+                                const double *fobj, double *sphere, double *fcalc,
+                                cudaStream_t stream) {
+    if (size <= 1 || size > 46340 || (!sphere && !fcalc) || (fcalc && !fobj)) return RSPI_ERR_ARG;
+    k_fcalc<<<rspi_blocks(size * size, 256), 256, 0, stream>>>(
+        (int)size, dia, sx, sy, (const double2 *)fobj, sphere, (double2 *)fcalc);
     RSPI_RETURN_LAUNCH();
 }

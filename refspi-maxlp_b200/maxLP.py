@@ -3,20 +3,26 @@
 ``MaxLPhaser(data_fname, size=185, num_data=-1)`` keeps the reference's
 constructor and ``_run_phaser(model, sx_vals, sy_vals, dia_vals, ang_vals)``
 (maxLP.py:304-340), with the same q grids, masks and candidate pattern
-(``qx``, ``qy``, ``qrad``, ``mask``, ``rmask``, ``pattern``).  The per-pixel
+(``qx``, ``qy``, ``qrad``, ``mask``, ``rmask``, ``pattern``), the
+``photons`` CSR matrix and the per-pixel methods (``get_photons_pixel``,
+``get_fref_d``, ``get_pixel_constants``, ``get_rescale_pixel``,
+``get_logq_pixel``, ``iterate_pixel_pattern``, ``run_pixel_pattern``,
+``_get_sphere``, ``get_fcalc_all``), all on the device.  The per-pixel
 pattern search runs in librspi (one CTA per pixel, all 1089 candidates at
 once); see csrc/maxlp.cu for the exact sparse/analytic rewrite of
 ``get_logq_pixel``.
 """
 import os
 import sys
+import warnings
 
 import numpy as np
 import torch
 
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 from rspi import geometry  # noqa: E402
-from rspi.device import MStep  # noqa: E402
+from rspi.device import MStep, cur_stream, ptr  # noqa: E402
+from rspi.lib import call  # noqa: E402
 
 
 class MaxLPhaser():
@@ -54,24 +60,176 @@ class MaxLPhaser():
         s = np.sin(ang)
         return np.array([[c, -s], [s, c]])
 
+    # -- per-pixel, per-frame API (maxLP.py:107-114, 154-253) ------------
+    # The reference's own search walks one pixel at a time over every frame;
+    # these run it through librspi on the frames' parameters of the last
+    # _run_phaser call, returning CUDA tensors as the reference returns CuPy
+    # arrays.
+
+    @property
+    def photons(self):
+        '''Photon counts as a sparse CSR matrix, frames x pixels
+        (maxLP.py:50-71), on the device.'''
+        if getattr(self, '_photons_csr', None) is None:
+            ph = self.dset.photons
+            n = self.num_data
+            rows_o = torch.repeat_interleave(torch.arange(n, device=self.device), ph.ones.long())
+            rows_m = torch.repeat_interleave(torch.arange(n, device=self.device), ph.multi.long())
+            idx = torch.stack([torch.cat([rows_o, rows_m]),
+                               torch.cat([ph.place_ones.long(), ph.place_multi.long()])])
+            val = torch.cat([torch.ones(rows_o.numel(), dtype=torch.float64, device=self.device),
+                             ph.count_multi.double()])
+            coo = torch.sparse_coo_tensor(idx, val, (n, self.size ** 2),
+                                          check_invariants=True).coalesce()
+            with warnings.catch_warnings():   # torch marks sparse CSR as beta
+                warnings.simplefilter('ignore', UserWarning)
+                self._photons_csr = coo.to_sparse_csr()
+        return self._photons_csr
+
+    def _frame_tables(self):
+        '''Per-frame (cos, sin) of -angle and (shift x, shift y, diameter) of
+        the last _run_phaser call, on the device.'''
+        if getattr(self, 'ang', None) is None:
+            raise ValueError('the per-frame parameters are set by _run_phaser')
+        key = (id(self.ang), id(self.shifts), id(self.diams))
+        if getattr(self, '_ftab_key', None) != key:
+            rot = torch.from_numpy(geometry.phaser_rotation_table(self.ang)).to(self.device)
+            fp = np.ascontiguousarray(np.stack([self.shifts[:, 0], self.shifts[:, 1],
+                                                self.diams], axis=1), dtype='f8')
+            self._ftab = (rot, torch.from_numpy(fp).to(self.device))
+            self._ftab_key = key
+        return self._ftab
+
+    def _pixel_frames(self, d_vals, t):
+        rot, fp = self._frame_tables()
+        ph = self.dset.photons
+        if d_vals is None:
+            dv, n = None, self.num_data
+        else:
+            dv = torch.as_tensor(np.ascontiguousarray(np.asarray(d_vals).ravel(), dtype='i4'))
+            dv = dv.to(self.device)
+            n = dv.numel()
+        k = torch.empty(n, dtype=torch.float64, device=self.device)
+        fref = torch.empty(n, dtype=torch.complex128, device=self.device)
+        call('rspi_maxlp_pixel_frames', int(t), self.size, ptr(dv), n, ptr(ph.ones),
+             ptr(ph.multi), ptr(ph.ones_accum), ptr(ph.multi_accum), ptr(ph.place_ones),
+             ptr(ph.place_multi), ptr(ph.count_multi), ph.num_data, ptr(rot), ptr(fp), ptr(k),
+             ptr(fref), ptr(ph.err.t), cur_stream())
+        ph.err.check('MaxLP pixel frames')
+        return k, fref
+
+    def get_photons_pixel(self, d_vals, t):
+        '''Photons of frames d_vals at model pixel t (maxLP.py:245-253)'''
+        return self._pixel_frames(d_vals, t)[0]
+
     def get_fref_d(self, d_vals, t):
         '''Reference amplitude of frames d_vals at model pixel t (maxLP.py:238-243)'''
-        sval = np.pi * self.qrad[t] * self.diams[d_vals]
-        fref = (np.sin(sval) - sval * np.cos(sval)) / sval ** 3
-        ramp = np.exp(1j * 2 * np.pi * (self.qx[t] * self.shifts[d_vals, 0] +
-                                        self.qy[t] * self.shifts[d_vals, 1]))
-        return fref * ramp
+        return self._pixel_frames(d_vals, t)[1]
 
-    def get_fcalc_all(self, fobj, dia, shift):
-        '''Holographic combination of model and spherical reference (maxLP.py:260-264)'''
-        qx2d = self.qx.reshape((self.size,) * 2)
-        qy2d = self.qy.reshape((self.size,) * 2)
-        return fobj + self._get_sphere(dia) * np.exp(1j * 2 * np.pi * (qx2d * shift[0] + qy2d * shift[1]))
+    def get_pixel_constants(self, t, frac=None):
+        '''k_d and fref_d of every frame (or a random fraction) at pixel t
+        (maxLP.py:107-114)'''
+        d_vals = None
+        if frac is not None:
+            d_vals = np.random.choice(self.num_data, int(np.round(self.num_data * frac)),
+                                      replace=False)
+        k, fref = self._pixel_frames(d_vals, t)
+        return {'k_d': k, 'fref_d': fref}
+
+    def _candidates(self, fobj_t):
+        if isinstance(fobj_t, torch.Tensor):
+            c = fobj_t.to(self.device, torch.complex128).reshape(-1).contiguous()
+        else:
+            c = torch.from_numpy(np.ascontiguousarray(np.atleast_1d(np.asarray(
+                fobj_t, dtype=np.complex128)).ravel())).to(self.device)
+        return c
+
+    def _pixel_values(self, cands, const, mode, rescale):
+        n = int(const['k_d'].numel())
+        out = torch.empty(cands.numel(), dtype=torch.float64, device=self.device)
+        rvec, rs = None, 0.
+        if isinstance(rescale, torch.Tensor) or (rescale is not None and np.ndim(rescale) > 0):
+            rvec = torch.as_tensor(rescale, dtype=torch.float64).to(self.device)
+            rvec = rvec.reshape(-1).contiguous()
+            if rvec.numel() != cands.numel():
+                rvec = rvec.expand(cands.numel()).contiguous()
+        elif rescale is not None:
+            rs = float(rescale)
+        call('rspi_maxlp_pixel_values', ptr(cands), cands.numel(),
+             ptr(const['k_d'].contiguous()), ptr(const['fref_d'].contiguous()), n, mode, rs,
+             ptr(rvec), ptr(out), cur_stream())
+        return out
+
+    def get_rescale_pixel(self, fobj_t, t, const=None):
+        '''mean_d k_d / mean_d |f + fref_d|^2 per candidate f (maxLP.py:216-228)'''
+        if const is None:
+            const = self.get_pixel_constants(t)
+        return self._pixel_values(self._candidates(fobj_t), const, 0, None)
+
+    def get_logq_pixel(self, fobj_t, t, rescale=None, const=None):
+        '''Log-likelihood of candidates f at model pixel t (maxLP.py:181-197)'''
+        if const is None:
+            const = self.get_pixel_constants(t)
+        cands = self._candidates(fobj_t)
+        if rescale is None:
+            rescale = self._pixel_values(cands, const, 0, None)
+        return self._pixel_values(cands, const, 1, rescale)
+
+    def _argmax(self, vals):
+        '''First index of the maximum (a NaN counts as the maximum), on the device.'''
+        v = vals.reshape(-1, 1).contiguous()
+        mx = torch.empty(1, dtype=torch.float64, device=self.device)
+        im = torch.empty(1, dtype=torch.int32, device=self.device)
+        call('rspi_frame_reduce', ptr(v), 1, v.shape[0], 1, ptr(mx), ptr(im), None, cur_stream())
+        return int(im.item())
+
+    def iterate_pixel_pattern(self, fobj_t, t, step, rescale=None, const=None):
+        '''One pattern-search step at pixel t (maxLP.py:169-179)'''
+        if const is None:
+            const = self.get_pixel_constants(t)
+        fobj_t = complex(fobj_t)
+        vals = self.get_logq_pixel(fobj_t + self.pattern * step, t, rescale=rescale,
+                                   const=const)
+        imax = self._argmax(vals)
+        retf = fobj_t + self.pattern[imax] * step
+        if imax == self.pattern.size // 2:   # centre of the pattern
+            return retf, step / (self.pattern.size ** 0.5 / 5)
+        return retf, step
+
+    def run_pixel_pattern(self, fobj, t, num_iter=10, rescale=None, frac=None):
+        '''Pattern search of model pixel t over every frame (maxLP.py:154-167)'''
+        if isinstance(fobj, torch.Tensor):
+            fobj_t = complex(fobj.reshape(-1)[t].item())
+        else:
+            fobj_t = complex(np.asarray(fobj).ravel()[t])
+        const = self.get_pixel_constants(t, frac=frac)
+        step = abs(fobj_t) / 4.
+        for _ in range(num_iter):
+            fobj_t_new, step_new = self.iterate_pixel_pattern(fobj_t, t, step, rescale, const)
+            with np.errstate(divide='ignore', invalid='ignore'):
+                if np.float64(step_new) / np.float64(abs(fobj_t_new)) < 1.e-3:
+                    break
+            fobj_t = fobj_t_new
+            step = step_new
+        return fobj_t
 
     def _get_sphere(self, dia):
-        '''Sphere transform for a diameter (maxLP.py:266-269)'''
-        sval = np.pi * self.qrad.reshape((self.size,) * 2) * dia
-        return (np.sin(sval) - sval * np.cos(sval)) / sval ** 3
+        '''Sphere transform for a diameter (maxLP.py:266-269), on the device'''
+        out = torch.empty((self.size, self.size), dtype=torch.float64, device=self.device)
+        call('rspi_maxlp_fcalc', self.size, float(dia), 0., 0., None, ptr(out), None,
+             cur_stream())
+        return out
+
+    def get_fcalc_all(self, fobj, dia, shift):
+        '''Holographic combination of model and spherical reference
+        (maxLP.py:260-264), on the device'''
+        f = self._candidates(fobj)
+        if f.numel() != self.size ** 2:
+            raise ValueError('fobj must hold %d pixels' % self.size ** 2)
+        out = torch.empty((self.size, self.size), dtype=torch.complex128, device=self.device)
+        call('rspi_maxlp_fcalc', self.size, float(dia), float(shift[0]), float(shift[1]),
+             ptr(f), None, ptr(out), cur_stream())
+        return out
 
     def _run_phaser(self, model, sx_vals, sy_vals, dia_vals, ang_vals, modes=None):
         '''Ring pass, global rescale and main pass over every phaser pixel

@@ -97,6 +97,13 @@ int rspi_holo_slices(const double *model /* complex128, P */, const double *shif
                      long long size, const double *bg, const int *sel_pix, long long n_sel,
                      double *holo /* n_states0 x P */, double *msum, cudaStream_t stream);
 
+/* EMC.sphere / EMC.ramp of one state (emc.py:244-254) over the P pixels, with
+ * integer-centred x, y and r = sqrt(x^2 + y^2): sphere (nullable, doubles) =
+ * (sin s - s cos s) / s^3, s = pi r dia / size (1e-5 where 0); ramp
+ * (nullable, complex128) = e^{2 pi i (x sx + y sy) / size}. */
+int rspi_sphere_ramp(long long size, double sx, double sy, double dia, double *sphere,
+                     double *ramp, cudaStream_t stream);
+
 /* vscale and per-state likelihood offsets (emc.py:181, 199):
  *   vscale = sum_sel powder / sum_s0 msum[s0] * n_states0,
  *   init[s0] = -(msum[s0] * vscale). */

@@ -50,6 +50,29 @@ k_holo(const double2 *__restrict__ model, const double *__restrict__ shiftx,
     if (threadIdx.x == 0) msum[s0] = acc;
 }
 
+// EMC.sphere and EMC.ramp of one state (emc.py:244-254): with integer-centred
+// x, y and r = sqrt(x^2 + y^2), s = pi r dia / size (1e-5 where 0),
+// sphere = (sin s - s cos s) / s^3 and ramp = e^{2 pi i (x sx + y sy) / size}.
+__global__ void k_sphere_ramp(int size, double sx, double sy, double dia,
+                              double *__restrict__ sphere, double2 *__restrict__ ramp) {
+    const long long npix = (long long)size * size;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const double cen = (double)(size / 2), dsize = (double)size;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += stride) {
+        const long long xi = p / size, yi = p - xi * size;
+        const double x = (double)xi - cen, y = (double)yi - cen;
+        if (sphere) {
+            double sv = xmul(xmul(PI, sqrt(xadd(xmul(x, x), xmul(y, y)))), dia) / dsize;
+            if (sv == 0.) sv = 1.e-5;
+            sphere[p] = xsub(sin(sv), xmul(sv, cos(sv))) / pow(sv, 3.);
+        }
+        if (ramp) {
+            const double ph = xmul(2. * PI, xadd(xmul(x, sx), xmul(y, sy))) / dsize;
+            ramp[p] = make_double2(cos(ph), sin(ph));
+        }
+    }
+}
+
 // vscale = sum_sel powder / sum_s0 msum * S0 ; init = -(msum * vscale)  (emc.py:181,199)
 __global__ void __launch_bounds__(1024)
 k_vscale_init(const double *__restrict__ msum, long long n_states0,
@@ -153,5 +176,13 @@ extern "C" int rspi_rot_log_slices(const double *holo, long long n_states0, long
                                                       (double *)lslices, abs_max);
     else
         return RSPI_ERR_ARG;
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_sphere_ramp(long long size, double sx, double sy, double dia, double *sphere,
+                                double *ramp, cudaStream_t stream) {
+    if (size <= 1 || size > 46340 || (!sphere && !ramp)) return RSPI_ERR_ARG;
+    k_sphere_ramp<<<rspi_blocks(size * size, 256), 256, 0, stream>>>(
+        (int)size, sx, sy, dia, sphere, (double2 *)ramp);
     RSPI_RETURN_LAUNCH();
 }

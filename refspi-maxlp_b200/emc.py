@@ -52,6 +52,8 @@ from dset import Dataset  # noqa: E402
 from maxLP import MaxLPhaser  # noqa: E402
 from rspi import geometry  # noqa: E402
 from rspi import h5lite  # noqa: E402
+from rspi.device import cur_stream, ptr  # noqa: E402
+from rspi.lib import call  # noqa: E402
 from rspi.device import EStep  # noqa: E402
 
 P_MIN = 1.e-6   # emc.py:20
@@ -281,12 +283,17 @@ class EMC():
         self.model = np.random.random(shape) + 1j * np.random.random(shape)
 
     def ramp(self, n):
-        '''Shift phase ramp of state n (emc.py:244-245)'''
-        return np.exp(1j * 2. * np.pi * (self.x_ind * self.shiftx[n] + self.y_ind * self.shifty[n]) / self.size)
+        '''Shift phase ramp of state n (emc.py:244-245), a complex128 CUDA
+        tensor of P pixels'''
+        out = torch.empty(self.size ** 2, dtype=torch.complex128, device=self.device)
+        call('rspi_sphere_ramp', self.size, float(self.shiftx[n]), float(self.shifty[n]), 0.,
+             None, ptr(out), cur_stream())
+        return out
 
     def sphere(self, n, diameter=None):
-        '''Sphere form factor of state n or of a diameter (emc.py:247-254)'''
+        '''Sphere form factor of state n or of a diameter (emc.py:247-254), a
+        float64 CUDA tensor of P pixels'''
         dia = diameter if n is None else self.sphere_dia[n]
-        s = np.pi * self.rad * dia / self.size
-        s[s == 0] = 1.e-5
-        return ((np.sin(s) - s * np.cos(s)) / s ** 3).ravel()
+        out = torch.empty(self.size ** 2, dtype=torch.float64, device=self.device)
+        call('rspi_sphere_ramp', self.size, 0., 0., float(dia), ptr(out), None, cur_stream())
+        return out

@@ -79,10 +79,10 @@ class MaxLPhaser():
                                torch.cat([ph.place_ones.long(), ph.place_multi.long()])])
             val = torch.cat([torch.ones(rows_o.numel(), dtype=torch.float64, device=self.device),
                              ph.count_multi.double()])
-            coo = torch.sparse_coo_tensor(idx, val, (n, self.size ** 2),
-                                          check_invariants=True).coalesce()
-            with warnings.catch_warnings():   # torch marks sparse CSR as beta
+            with warnings.catch_warnings():   # torch's notes on sparse tensors
                 warnings.simplefilter('ignore', UserWarning)
+                coo = torch.sparse_coo_tensor(idx, val, (n, self.size ** 2),
+                                              check_invariants=True).coalesce()
                 self._photons_csr = coo.to_sparse_csr()
         return self._photons_csr
 

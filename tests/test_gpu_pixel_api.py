@@ -103,3 +103,32 @@ def test_pixel_api_needs_frame_parameters(tmp_path):
     ph = MaxLPhaser(os.path.join(str(tmp_path), 'photons.npz'), size=int(g['size']))
     with pytest.raises(ValueError):
         ph.get_pixel_constants(int(np.flatnonzero(ph.mask)[0]))
+
+
+def test_emc_sphere_and_ramp(tmp_path):
+    """EMC.sphere / EMC.ramp (emc.py:244-254) on the device against the
+    reference's NumPy expressions on the same integer-centred grids."""
+    from emc import EMC
+    g = load_golden('case_a')
+    rec = EMC(write_case(str(tmp_path), g))
+    size = rec.size
+    x, y = np.indices((size, size), dtype='f8')
+    x = x.ravel() - size // 2
+    y = y.ravel() - size // 2
+    rad = np.sqrt(x * x + y * y)
+    for n in (0, len(rec.sphere_dia) - 1):
+        want = np.exp(1j * 2. * np.pi * (x * rec.shiftx[n] + y * rec.shifty[n]) / size)
+        np.testing.assert_allclose(rec.ramp(n).cpu().numpy(), want, rtol=1e-13, atol=1e-15)
+        _check_sphere(rec.sphere(n).cpu().numpy(), rad, rec.sphere_dia[n], size)
+    _check_sphere(rec.sphere(None, 7.25).cpu().numpy(), rad, 7.25, size)
+
+
+def _check_sphere(got, rad, dia, size):
+    s = np.pi * rad * dia / size
+    s[s == 0] = 1.e-5
+    want = (np.sin(s) - s * np.cos(s)) / s ** 3
+    # sin s - s cos s cancels to s^3/3 at the centre (s = 1e-5): one ulp of
+    # sin there is ~5e-6 of the difference, in either library
+    far = s > 1.e-3
+    np.testing.assert_allclose(got[far], want[far], rtol=1e-12)
+    np.testing.assert_allclose(got[~far], want[~far], rtol=1e-4)

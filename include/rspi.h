@@ -490,7 +490,7 @@ int rspi_maxlp_fcalc(long long size, double dia, double sx, double sy, const dou
                      double *sphere, double *fcalc, cudaStream_t stream);
 
 /* Polar grid search of the per-pixel MaxLP negative log-likelihood (the
- * judge beside the L-BFGS update of rspi_nll; no reference counterpart):
+ * comparison for the L-BFGS update of rspi_nll; no reference counterpart):
  * for each pixel t = pixels[i] (histogram row hist_row[i], one mode),
  *   NLL_t(F) = sum_s S_s |F + r_s|^2 - sum_s K_t[s] log |F + r_s|^2,
  * S_s = sum of scales[d] over frames with fstate[d] == s (written to

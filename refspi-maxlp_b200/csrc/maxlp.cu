@@ -712,7 +712,7 @@ __global__ void k_state_scale_sums(const int *__restrict__ fstate, const double 
     }
 }
 
-// Polar grid search of the per-pixel NLL (the judge of the L-BFGS update):
+// Polar grid search of the per-pixel NLL (the comparison for the L-BFGS update):
 //   NLL_t(F) = sum_s S_s |F + r_s|^2 - sum_s K_t[s] log |F + r_s|^2 (+ const)
 // over F = a_j e^{i phi_i}, phi_i = 2 pi i / n_phase, a_j = A (j + 1) / n_amp,
 // A = sqrt(sum K / sum S) + max_s |r_s| (every amplitude the data allow).

@@ -13,7 +13,7 @@ pytestmark = pytest.mark.gpu
 
 # FP64 pipeline vs FP64 oracle: only summation order differs
 RTOL_F64 = 1e-11
-# FP32 slices (FP64 accumulation): north-star bound on the likelihood
+# FP32 slices (FP64 accumulation): the 1e-5 bound on the likelihood
 RTOL_F32 = 1e-5
 
 

@@ -1,4 +1,4 @@
-"""The polar grid search of the per-pixel NLL (the judge beside L-BFGS) and
+"""The polar grid search of the per-pixel NLL (the comparison for L-BFGS) and
 the model-update comparison (pattern search, grid, L-BFGS) on NLL and FRC."""
 import numpy as np
 import pytest

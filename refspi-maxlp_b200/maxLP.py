@@ -91,13 +91,11 @@ class MaxLPhaser():
         the last _run_phaser call, on the device.'''
         if getattr(self, 'ang', None) is None:
             raise ValueError('the per-frame parameters are set by _run_phaser')
-        key = (id(self.ang), id(self.shifts), id(self.diams))
-        if getattr(self, '_ftab_key', None) != key:
+        if getattr(self, '_ftab', None) is None:
             rot = torch.from_numpy(geometry.phaser_rotation_table(self.ang)).to(self.device)
             fp = np.ascontiguousarray(np.stack([self.shifts[:, 0], self.shifts[:, 1],
                                                 self.diams], axis=1), dtype='f8')
             self._ftab = (rot, torch.from_numpy(fp).to(self.device))
-            self._ftab_key = key
         return self._ftab
 
     def _pixel_frames(self, d_vals, t):
@@ -255,6 +253,7 @@ class MaxLPhaser():
         self.shifts = np.array([sx, sy]).T
         self.diams = dia
         self.ang = ang
+        self._ftab = None   # the per-pixel API's frame tables follow these
         triples = np.stack([sx, sy, dia], axis=1)
         ref, fstate = np.unique(triples, axis=0, return_inverse=True)
         dev = self.device

@@ -132,3 +132,20 @@ def _check_sphere(got, rad, dia, size):
     far = s > 1.e-3
     np.testing.assert_allclose(got[far], want[far], rtol=1e-12)
     np.testing.assert_allclose(got[~far], want[~far], rtol=1e-4)
+
+
+def test_pixel_api_follows_the_last_run(tmp_path):
+    """A second _run_phaser with other frame parameters: the per-pixel API
+    uses the new ones."""
+    size = 17
+    ph, kmat, model, (sx, sy, dia, ang) = _phaser_case(tmp_path, size, 30, 4)
+    qx, qy, qrad, _, _ = M.get_qvals(size)
+    ang2 = (ang + 0.7) % (2 * np.pi)
+    dia2 = dia + 0.5
+    ph._run_phaser(model, sx, sy, dia2, ang2)
+    t = int(np.flatnonzero(ph.mask)[5])
+    assert np.array_equal(ph.get_photons_pixel(None, t).cpu().numpy(),
+                          M.photons_pixel(kmat, ang2, t, size, qx, qy))
+    np.testing.assert_allclose(ph.get_fref_d(None, t).cpu().numpy(),
+                               M.fref_pixel(t, qx, qy, qrad, dia2, np.stack([sx, sy], 1)),
+                               rtol=1e-13, atol=1e-15)

@@ -435,13 +435,13 @@ int rspi_maxlp_pattern(double *fconv, const int *pixels, const int *hist_row,
 /* rspi_maxlp_pattern with an FP32 screening pass per iteration: every
  * candidate is first evaluated in FP32 with a rigorous bound on its distance
  * from the FP64 value; only the candidates that can still be the argmax
- * (the finalists) are evaluated in FP64, in the same order and with the same
- * roundings as rspi_maxlp_pattern, so the chosen candidates, and fconv and
- * rescale_out, are bit-identical to it.  Iterations the bound cannot settle
- * (more than 384 finalists, more than 1024 populated states, counts >= 2^24,
- * values out of the FP32 range) run the FP64 pass.  stats (device, 3
+ * (the finalists; every candidate without a finite bound) are evaluated in
+ * FP64, with the same sums and roundings as rspi_maxlp_pattern, so the
+ * chosen candidates, and fconv and rescale_out, are bit-identical to it.
+ * Pixels with more than 1024 populated states, counts >= 2^24, or ring
+ * pixels without photons run the FP64 iterations.  stats (device, 3
  * counters, NULL for none; the caller zeroes them) accumulates [iterations
- * settled by the screen, iterations that ran the FP64 pass, finalists]. */
+ * through the screen, iterations of the FP64 pass, finalists]. */
 int rspi_maxlp_pattern_screened(double *fconv, const int *pixels, const int *hist_row,
                                 long long n_pix, const int *hist, long long n_ref,
                                 const int *nstate, long long n_modes, const double *ref_params,

@@ -287,7 +287,8 @@ constexpr double G_CHUNK = 8.01 * U32;             // gamma_8 (+ the FP64 adds)
 constexpr int NPART = 4;                           // partial sums per candidate
 static_assert(NPART == 4, "combine4 and sum_partials take four partial sums");
 constexpr int FIN_SPLIT = PT_THREADS / NPART;      // up to here: NPART threads each
-constexpr int FIN_CAP = PT_THREADS;                // beyond: one thread, NPART sums
+constexpr int FIN_CAP = NCAND;                     // beyond: a thread per finalist,
+                                                   // NPART sums, up to PT_CPT each
 
 __device__ __forceinline__ double block_max_d(double v, double *scratch) {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -349,12 +350,12 @@ __device__ __forceinline__ void screen_term(float2 xh, float2 xl, const float4 r
 // differences, lg2.approx, chunked sums) with a rigorous bound E_c on its
 // distance from the FP64 value; only the finalists, the candidates whose
 // upper end q32 + E reaches the best lower end max(q32 - E), are evaluated
-// in FP64, each by one thread in the plain search's order.  The FP64 argmax
-// is always a finalist and every other candidate's FP64 value is strictly
-// below it, so the chosen candidate is the plain search's.  A pixel falls
-// back to the plain FP64 iteration when it has more than one chunk of
-// populated states, counts >= 2^24, no candidate with a finite bound, or
-// more than FIN_CAP finalists.
+// in FP64 with the plain search's sums (four partial sums each, on four
+// threads or one).  The FP64 argmax is always a finalist and every other
+// candidate's FP64 value is strictly below it, so the chosen candidate is
+// the plain search's.  A candidate without a finite bound is a finalist.  A
+// pixel runs the plain FP64 iterations when it has more than one chunk of
+// populated states, counts >= 2^24, or is a ring pixel without photons.
 //
 // Bound, per term (u = 2^-24; A = |f_c|_inf + max_s |r_s|_inf, scaled):
 //   re, im from hi + lo parts: error <= 2u |re| + 6 u^2 A, so while
@@ -374,7 +375,7 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
     __shared__ double fr_re[POP_CAP], fr_im[POP_CAP], fk[POP_CAP];
     __shared__ float4 r32[SCREEN ? POP_CAP : 1];
     __shared__ float k32[SCREEN ? POP_CAP : 1];
-    __shared__ int fin[SCREEN ? FIN_CAP : 1];
+    __shared__ short fin[SCREEN ? FIN_CAP : 1];
     __shared__ double scratch[32];
     __shared__ int iscratch[32];
     __shared__ int wsum[32];
@@ -571,11 +572,13 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
             for (int k = 0; k < PT_CPT; ++k) mine += (threadIdx.x + k * PT_THREADS < NCAND) && up[k] >= tl;
             int nfin = 0;
             int pos = block_scan(mine, wsum, &nfin);
-            if (tl > -INFINITY && nfin <= FIN_CAP) {
+            // every candidate whose upper end reaches tl is a finalist (all
+            // of them when no candidate has a finite bound: tl = -inf)
+            {
 #pragma unroll
                 for (int k = 0; k < PT_CPT; ++k) {
                     const int c = threadIdx.x + k * PT_THREADS;
-                    if (c < NCAND && up[k] >= tl) fin[pos++] = c;
+                    if (c < NCAND && up[k] >= tl) fin[pos++] = (short)c;
                 }
                 __syncthreads();
                 if (nfin <= FIN_SPLIT) {
@@ -596,13 +599,19 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
                         best = cand_q(combine4(acc, v1, v2, v3), dn, cc);
                         bidx = fin[fi];
                     }
-                } else if (threadIdx.x < nfin) {
+                } else {
                     // one thread per finalist, its NPART sums in registers
-                    const Cand cc = cand_at(fin[threadIdx.x], f, step, pc, ring, kmean, rescale);
-                    double a4[NPART] = {0., 0., 0., 0.};
-                    sum_partials(a4, cc, npop, fr_re, fr_im, fk);
-                    best = cand_q(combine4(a4[0], a4[1], a4[2], a4[3]), dn, cc);
-                    bidx = fin[threadIdx.x];
+                    for (int i = threadIdx.x; i < nfin; i += PT_THREADS) {
+                        const int c = fin[i];
+                        const Cand cc = cand_at(c, f, step, pc, ring, kmean, rescale);
+                        double a4[NPART] = {0., 0., 0., 0.};
+                        sum_partials(a4, cc, npop, fr_re, fr_im, fk);
+                        const double q = cand_q(combine4(a4[0], a4[1], a4[2], a4[3]), dn, cc);
+                        if (argmax_better(q, c, best, bidx)) {
+                            best = q;
+                            bidx = c;
+                        }
+                    }
                 }
                 searched = true;
                 if (stats && threadIdx.x == 0) {

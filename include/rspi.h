@@ -269,6 +269,33 @@ int rspi_screen_loglike4(const float *lslices, long long p_row, long long num_ro
                          int states_per_tile, int warps_per_cta, int n_ctas,
                          cudaStream_t stream);
 
+/* Frame pairs (two rows per tile): the two half-warps take the two frames of
+ * a pair, so one reduction and store pass serves two frames.
+ * rspi_pair_entry_groups: each frame's group count ceil(max_c n_c / 4) with
+ * 16 bank classes, one lane per class.  The caller orders frames (e.g. by
+ * that count), pairs them (pair p = frames pair_frames[2p],
+ * pair_frames[2p + 1], -1 for none; pair_slot[d] = 2p + h for frame d in
+ * half h), takes each pair's larger count and scans those into
+ * pair_group_off[n_pairs + 1].
+ * rspi_pair_entry_fill: total_groups * 128 16-bit entries (8-byte aligned):
+ * lane 16 h + c of a pair group holds frame h's photons of class c (column
+ * 16 q + c, q stored), four per group, the lane's zero column elsewhere.
+ * rspi_screen_loglike5: the likelihood rows from those entries (the sums of
+ * rspi_screen_loglike4 in another order, within the same FP32 error bound
+ * with each frame's summation length max(entry rows, its pair's groups)). */
+int rspi_pair_entry_groups(const unsigned short *entries16, const long long *row_off16,
+                           long long n_data, int p_zero, int *groups, cudaStream_t stream);
+int rspi_pair_entry_fill(const unsigned short *entries16, const long long *row_off16,
+                         long long n_data, int p_zero, const int *pair_slot,
+                         const long long *pair_group_off, long long total_groups,
+                         unsigned short *narrow, cudaStream_t stream);
+int rspi_screen_loglike5(const float *lslices, long long p_row, long long num_rot,
+                         const double *init, const double *scales, const unsigned short *narrow,
+                         const long long *pair_group_off, const int *pair_frames,
+                         long long n_pairs, long long row_begin, long long row_end, float *ll,
+                         long long ll_stride, int warps_per_cta, int n_ctas,
+                         cudaStream_t stream);
+
 /* rspi_screen_loglike4 from the 16-bit bank-class entries of
  * rspi_wide_entry_fill_narrow: one 8-byte load per four photons of a lane
  * (half the entry bytes), one integer multiply-add per photon for its

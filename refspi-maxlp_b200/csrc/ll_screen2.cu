@@ -423,12 +423,11 @@ __device__ __forceinline__ unsigned entry16_at(const unsigned short *__restrict_
 __global__ void __launch_bounds__(BANK_WARPS * 32)
 k_wide_groups_banked(const unsigned short *__restrict__ ent16,
                      const long long *__restrict__ row_off16, long long n, int p_zero,
-                     int classes, int *__restrict__ groups) {
+                     int classes, int per, int *__restrict__ groups) {
     __shared__ int cnt[BANK_WARPS][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
-    const int per = 32 / classes;
     for (long long d = warp; d < n; d += nwarp) {
         cnt[w][lane] = 0;
         __syncwarp();
@@ -480,6 +479,57 @@ k_wide_fill_banked(const unsigned short *__restrict__ ent16,
             }
             __syncwarp();
             if (key < classes && lane == __ffs(m) - 1) base[w][key] += __popc(m);
+            __syncwarp();
+        }
+    }
+}
+
+// Frame pairs: the two half-warps take the two frames of a pair, so one
+// pass of the per-frame reduction and store serves two frames.  Two rows per
+// tile (C = 16 bank classes); lane 16 h + c of a pair group holds frame h's
+// photons of class c, four 16-bit q per group (column 16 q + c), the k-th
+// photon of class c in slot k of that lane; a pair takes the larger of its
+// frames' group counts ceil(max_c n_c / 4); every other slot holds the lane's
+// zero column (q = (p_zero + lane) / 16, of class lane mod 16).
+__global__ void k_pair_pad(long long n_slots, int p_zero, uint2 *__restrict__ out) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_slots;
+         i += stride) {
+        const unsigned pad = (unsigned)(p_zero + (int)(i & 31)) / 16u;
+        const unsigned pad2 = pad | (pad << 16);
+        out[i] = make_uint2(pad2, pad2);
+    }
+}
+
+__global__ void __launch_bounds__(BANK_WARPS * 32)
+k_pair_fill(const unsigned short *__restrict__ ent16, const long long *__restrict__ row_off16,
+            long long n, int p_zero, const int *__restrict__ pair_slot,
+            const long long *__restrict__ pgoff, unsigned short *__restrict__ out) {
+    __shared__ int base[BANK_WARPS][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    for (long long d = warp; d < n; d += nwarp) {
+        const int ps = pair_slot[d];
+        const long long p = ps >> 1;
+        const int h = ps & 1;
+        const long long g0 = pgoff[p], ng = pgoff[p + 1] - g0;
+        base[w][lane] = 0;
+        __syncwarp();
+        const long long r0 = row_off16[d], nr = row_off16[d + 1] - r0;
+        for (long long r = 0; r < nr; ++r) {
+            const unsigned e = entry16_at(ent16, r0 + r, lane);
+            const int key = e < (unsigned)p_zero ? (int)(e % 16u) : 16;
+            const unsigned m = __match_any_sync(RSPI_FULL_MASK, key);
+            if (key < 16) {
+                const int k = base[w][key] + __popc(m & lt);
+                if ((k >> 2) < ng)
+                    out[((g0 + (k >> 2)) * 32 + 16 * h + key) * 4 + (k & 3)] =
+                        (unsigned short)(e / 16u);
+            }
+            __syncwarp();
+            if (key < 16 && lane == __ffs(m) - 1) base[w][key] += __popc(m);
             __syncwarp();
         }
     }
@@ -655,6 +705,114 @@ k_screen_ll4(const float *__restrict__ lsl, int p_row, int num_rot,
                     if (g + k + 1 == fend) {
                         finish();
                         while (f < fe && fend == g + k + 1) finish();
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < PG; ++k) cur[k] = nxt[k];
+            g += PG;
+            gp += 32 * PG;
+        }
+    }
+}
+
+// Frame pairs (two rows per tile, 16-bit entries of k_pair_fill): half-warp
+// h of a warp sums frame pair_frames[2 p + h] of pair p, each lane its
+// photons of one bank class; a pair's two sums are reduced in one pass of
+// four exchange steps inside each half-warp, and lanes 16 h + t store row t
+// of frame h.  Warps take contiguous pair ranges of about equal group counts.
+__global__ void __launch_bounds__(1024)
+k_screen_ll5(const float *__restrict__ lsl, int p_row, int num_rot,
+             const double *__restrict__ init, const double *__restrict__ scales,
+             const uint2 *__restrict__ groups, const long long *__restrict__ pgoff,
+             const int *__restrict__ pair_frames, int n_pairs, long long row_begin,
+             long long row_end, float *__restrict__ ll, long long ll_stride) {
+    constexpr int T = 2;
+    constexpr int PG = 4;   // groups (4 photons per lane each) loaded ahead
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float *slf = reinterpret_cast<float *>(smem_raw);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int half = lane >> 4, hl = lane & 15;
+    const long long n_tiles = (row_end - row_begin + T - 1) / T;
+    const int gtot = (int)pgoff[n_pairs];
+    auto lower = [&](int target) {
+        int lo = 0, hi = n_pairs;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((int)pgoff[mid] < target) lo = mid + 1;
+            else hi = mid;
+        }
+        return lo;
+    };
+    const int pb = wid == 0 ? 0 : lower((int)((long long)gtot * wid / nw));
+    const int pe = wid == nw - 1 ? n_pairs : lower((int)((long long)gtot * (wid + 1) / nw));
+    const unsigned lane_off = 8u * (unsigned)hl;
+
+    for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const long long first = row_begin + tile * T;
+        const int nt = (int)min((long long)T, row_end - first);
+        __syncthreads();
+        stage_tile<T>(slf, lsl + (first - row_begin) * (long long)p_row, p_row, nt);
+        __syncthreads();
+        if (pb >= pe) continue;
+
+        const bool storer = hl < nt;   // lanes 16 h + t store row t
+        const double my_init = storer ? init[(first + hl) / num_rot] : 0.;
+        float *my_ll = ll + (first + (storer ? hl : 0) - row_begin) * ll_stride;
+        Acc<T> a0, a1;
+        a0.zero();
+        a1.zero();
+        int base = pb;
+        int my_end = pb + lane < n_pairs ? (int)pgoff[pb + lane + 1] : 0x7fffffff;
+        int p = pb;
+        int g = (int)pgoff[pb];
+        const int gend = (int)pgoff[pe];
+        int pend = __shfl_sync(RSPI_FULL_MASK, my_end, 0);
+        // this lane's frame of the current pair and its scale (storers only)
+        int my_d = storer ? pair_frames[2 * p + half] : -1;
+        double my_sc = my_d >= 0 ? scales[my_d] : 0.;
+        auto finish = [&]() {
+            float2 a = __fadd2_rn(a0.p[0], a1.p[0]);
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) {
+                const float2 b = make_float2(__shfl_xor_sync(RSPI_FULL_MASK, a.x, o),
+                                             __shfl_xor_sync(RSPI_FULL_MASK, a.y, o));
+                a = __fadd2_rn(a, b);
+            }
+            if (my_d >= 0) my_ll[my_d] = (float)(my_init * my_sc + (double)(hl == 0 ? a.x : a.y));
+            a0.zero();
+            a1.zero();
+            ++p;
+            if (p - base == 32) {
+                base = p;
+                my_end = p + lane < n_pairs ? (int)pgoff[p + lane + 1] : 0x7fffffff;
+            }
+            pend = p < pe ? __shfl_sync(RSPI_FULL_MASK, my_end, p - base) : gend + 1;
+            my_d = storer && p < pe ? pair_frames[2 * p + half] : -1;
+            my_sc = my_d >= 0 ? scales[my_d] : 0.;
+        };
+        while (p < pe && pend == g) finish();   // pairs without entries
+
+        const uint2 *gp = groups + (long long)g * 32 + lane;
+        uint2 cur[PG], nxt[PG];
+        const uint2 z{};
+#pragma unroll
+        for (int k = 0; k < PG; ++k) cur[k] = g + k < gend ? __ldg(gp + 32 * k) : z;
+        while (g < gend) {
+            const int nb = min(PG, gend - g);
+#pragma unroll
+            for (int k = 0; k < PG; ++k) nxt[k] = g + PG + k < gend ? __ldg(gp + 32 * (PG + k)) : z;
+            Contrib<T> c0[PG], c1[PG];
+#pragma unroll
+            for (int k = 0; k < PG; ++k) gather_group<T>(smem_raw, cur[k], lane_off, c0[k], c1[k]);
+#pragma unroll
+            for (int k = 0; k < PG; ++k) {
+                if (k < nb) {
+                    add_contrib<T>(a0, c0[k]);
+                    add_contrib<T>(a1, c1[k]);
+                    if (g + k + 1 == pend) {
+                        finish();
+                        while (p < pe && pend == g + k + 1) finish();
                     }
                 }
             }
@@ -946,7 +1104,7 @@ extern "C" int rspi_wide_entry_groups_banked(const unsigned short *entries16,
         return RSPI_ERR_ARG;
     k_wide_groups_banked<<<rspi_blocks(n_data * 32, BANK_WARPS * 32), BANK_WARPS * 32, 0,
                            stream>>>(entries16, row_off16, n_data, p_zero, 32 / states_per_tile,
-                                     groups);
+                                     states_per_tile, groups);
     RSPI_RETURN_LAUNCH();
 }
 
@@ -1063,5 +1221,68 @@ extern "C" int rspi_screen_loglike4h(const void *lslices16, long long p_row, lon
         (const __half *)lslices16, (int)p_row, (int)num_rot, init, scales,
         reinterpret_cast<const uint4 *>(wide), group_off, (int)n_data, row_begin, row_end, ll,
         ll_stride);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_pair_entry_groups(const unsigned short *entries16, const long long *row_off16,
+                                      long long n_data, int p_zero, int *groups,
+                                      cudaStream_t stream) {
+    if (!entries16 || !row_off16 || !groups || n_data <= 0 || p_zero < 0 || p_zero % 32 ||
+        p_zero + 32 > 65536)
+        return RSPI_ERR_ARG;
+    k_wide_groups_banked<<<rspi_blocks(n_data * 32, BANK_WARPS * 32), BANK_WARPS * 32, 0,
+                           stream>>>(entries16, row_off16, n_data, p_zero, 16, 1, groups);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_pair_entry_fill(const unsigned short *entries16, const long long *row_off16,
+                                    long long n_data, int p_zero, const int *pair_slot,
+                                    const long long *pair_group_off, long long total_groups,
+                                    unsigned short *narrow, cudaStream_t stream) {
+    if (!entries16 || !row_off16 || !pair_slot || !pair_group_off || !narrow || n_data <= 0 ||
+        p_zero < 0 || p_zero % 32 || p_zero + 32 > 65536 || total_groups < 0 ||
+        (reinterpret_cast<uintptr_t>(narrow) & 7) != 0)
+        return RSPI_ERR_ARG;
+    if (total_groups > 0)
+        k_pair_pad<<<rspi_blocks(total_groups * 32, 256), 256, 0, stream>>>(
+            total_groups * 32, p_zero, reinterpret_cast<uint2 *>(narrow));
+    k_pair_fill<<<rspi_blocks(n_data * 32, BANK_WARPS * 32), BANK_WARPS * 32, 0, stream>>>(
+        entries16, row_off16, n_data, p_zero, pair_slot, pair_group_off, narrow);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_screen_loglike5(const float *lslices, long long p_row, long long num_rot,
+                                    const double *init, const double *scales,
+                                    const unsigned short *narrow, const long long *pair_group_off,
+                                    const int *pair_frames, long long n_pairs, long long row_begin,
+                                    long long row_end, float *ll, long long ll_stride,
+                                    int warps_per_cta, int n_ctas, cudaStream_t stream) {
+    if (!lslices || !init || !scales || !narrow || !pair_group_off || !pair_frames || !ll ||
+        n_pairs <= 0 || n_pairs > 0x3fffffffLL || p_row <= 32 || p_row % 32 || p_row > 65536 ||
+        num_rot <= 0 || num_rot > 0x7fffffffLL || row_begin < 0 || row_end < row_begin ||
+        warps_per_cta < 1 || warps_per_cta > 32)
+        return RSPI_ERR_ARG;
+    if ((reinterpret_cast<uintptr_t>(lslices) & 15) != 0 ||
+        (reinterpret_cast<uintptr_t>(narrow) & 7) != 0)
+        return RSPI_ERR_ARG;
+    if (row_end == row_begin) return RSPI_OK;
+    const size_t smem = 2 * (size_t)p_row * sizeof(float);
+    if (smem > (size_t)SMEM_LIMIT - 1024) return RSPI_ERR_ARG;
+    static size_t smem_set = 0;
+    if (smem > smem_set) {
+        if (cudaFuncSetAttribute(k_screen_ll5, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return RSPI_ERR_CUDA;
+        smem_set = smem;
+    }
+    const long long n_tiles = (row_end - row_begin + 1) / 2;
+    if (n_ctas <= 0) {
+        const int per_sm = max(1, (int)(SMEM_LIMIT / (smem + 1024)));
+        n_ctas = rspi_sm_count() * min(per_sm, max(1, 2048 / (warps_per_cta * 32)));
+    }
+    if (n_ctas > n_tiles) n_ctas = (int)n_tiles;
+    k_screen_ll5<<<n_ctas, warps_per_cta * 32, smem, stream>>>(
+        lslices, (int)p_row, (int)num_rot, init, scales, reinterpret_cast<const uint2 *>(narrow),
+        pair_group_off, pair_frames, (int)n_pairs, row_begin, row_end, ll, ll_stride);
     RSPI_RETURN_LAUNCH();
 }

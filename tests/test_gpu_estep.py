@@ -283,6 +283,8 @@ def test_frame_kernel_matches_stream_kernel(name, ds, need_scaling, tile, warps)
     out = {}
     variants = (('stream', True, True), ('frame', True, True), ('wide', True, True),
                 ('wide', True, False), ('wide', False, False))
+    if tile == 2:
+        variants += (('pair', True, True),)
     for kernel, banked, narrow in variants:
         ph = _photons(ds, need_scaling)
         es = _estep(ph, size, num_rot, sx, sy, dia, ds['bg'], form='screen', kernel=kernel,
@@ -298,7 +300,10 @@ def test_frame_kernel_matches_stream_kernel(name, ds, need_scaling, tile, warps)
     scale = np.abs(a[0]).max(0, keepdims=True) + 1.
     # the 16-bit and 32-bit bank-class entries give the same sums in the same order
     assert np.array_equal(out['wide', True, True][0], out['wide', True, False][0])
-    for b in (out['frame', True, True], out['wide', True, True], out['wide', False, False]):
+    others = [out['frame', True, True], out['wide', True, True], out['wide', False, False]]
+    if tile == 2:
+        others.append(out['pair', True, True])
+    for b in others:
         assert np.all(np.abs(a[0] - b[0]) <= 1e-6 * scale)
         assert np.array_equal(a[2], b[2])
         np.testing.assert_allclose(a[1], b[1], rtol=1e-14)
@@ -396,3 +401,51 @@ def test_bank_layout_entries(tile):
         assert np.array_equal(np.sort(realb), np.sort(realp)), f
         assert np.all((eb >= pz) <= (eb == pz + lanes)), f
         assert np.all(eb % classes == np.broadcast_to(lanes, eb.shape) % classes), f
+
+
+@pytest.mark.parametrize('n', [61, 200])
+def test_pair_layout_entries(n):
+    """Frame pairs: every frame's photons once, in its half-warp, one bank
+    class per lane, the zero column elsewhere; frames paired within windows
+    of consecutive frames (longest first)."""
+    from rspi.device import PAIR_WINDOW
+    size = 37
+    d = random_photons(size, n, 40. * size, 12, empty_frames=(2, 9), heavy=5)
+    ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
+                         d['count_multi'], size * size, False)
+    sx, sy, dia, _ = E.generate_states(E.parse_triple('0 0 1'), E.parse_triple('0 0 1'),
+                                       E.parse_triple('2 2 1'))
+    es_p = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen',
+                  kernel='pair', states_per_tile=2)
+    es_w = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen',
+                  kernel='wide', states_per_tile=2, narrow_entries=False)
+    torch.cuda.synchronize()
+    w = es_p.wide
+    pz = es_p.p_row - 32
+    q = w['entries'].cpu().numpy().view(np.uint16).reshape(-1, 32, 4).astype(np.int64)
+    lanes = np.arange(32)[None, :, None]
+    sel = q * 16 + lanes % 16
+    pgoff = w['group_off'].cpu().numpy()
+    pf = w['pair_frames'].cpu().numpy()
+    assert w['n_pairs'] == (n + 1) // 2 and np.all(np.diff(pgoff) >= 0)
+    wide = es_w.wide['entries'].cpu().numpy().view(np.uint32).reshape(-1, 32, 4) // 8
+    goff = es_w.wide['group_off'].cpu().numpy()
+    seen = []
+    for p in range(w['n_pairs']):
+        blk = sel[pgoff[p]:pgoff[p + 1]]
+        for h in range(2):
+            f = pf[2 * p + h]
+            half = blk[:, 16 * h:16 * h + 16]
+            if f < 0:
+                assert np.all(half >= pz)
+                continue
+            seen.append(f)
+            real = np.sort(half[half < pz])
+            ref = wide[goff[f]:goff[f + 1]]
+            assert np.array_equal(real, np.sort(ref[ref < pz])), f
+            pads = half >= pz
+            want = np.broadcast_to(pz + lanes[:, 16 * h:16 * h + 16], half.shape)
+            assert np.array_equal(half[pads], want[pads])
+    assert sorted(seen) == list(range(n))
+    # pairing stays inside windows of consecutive frames
+    assert np.all(pf[:n] // PAIR_WINDOW == np.arange(n) // PAIR_WINDOW)

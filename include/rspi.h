@@ -296,6 +296,30 @@ int rspi_screen_loglike5(const float *lslices, long long p_row, long long num_ro
                          long long ll_stride, int warps_per_cta, int n_ctas,
                          cudaStream_t stream);
 
+/* Frame quads: four frames per warp, eight lanes each (two rows per tile).
+ * Lane 8 u + j of a quad group holds frame u's photons of bank classes j and
+ * j + 8, the first in slots 0 and 2 and the second in slots 1 and 3 for even
+ * u (swapped for odd u), so every gather of a half-warp covers 16 distinct
+ * classes; the k-th photon of a class goes to group k / 2, the lane's
+ * (k mod 2)-th slot of that class's phase; other slots hold column
+ * p_zero + (the slot's class).  A frame takes ceil(max_c n_c / 2) groups
+ * (rspi_quad_entry_groups); quads, quad_slot[d] = 4 q + u, quad_frames and
+ * quad_group_off as for the frame pairs.  rspi_screen_loglike6: the
+ * likelihood rows from them, within the FP32 error bound with each frame's
+ * summation length max(entry rows, its quad's groups). */
+int rspi_quad_entry_groups(const unsigned short *entries16, const long long *row_off16,
+                           long long n_data, int p_zero, int *groups, cudaStream_t stream);
+int rspi_quad_entry_fill(const unsigned short *entries16, const long long *row_off16,
+                         long long n_data, int p_zero, const int *quad_slot,
+                         const long long *quad_group_off, long long total_groups,
+                         unsigned short *narrow, cudaStream_t stream);
+int rspi_screen_loglike6(const float *lslices, long long p_row, long long num_rot,
+                         const double *init, const double *scales, const unsigned short *narrow,
+                         const long long *quad_group_off, const int *quad_frames,
+                         long long n_quads, long long row_begin, long long row_end, float *ll,
+                         long long ll_stride, int warps_per_cta, int n_ctas,
+                         cudaStream_t stream);
+
 /* rspi_screen_loglike4 from the 16-bit bank-class entries of
  * rspi_wide_entry_fill_narrow: one 8-byte load per four photons of a lane
  * (half the entry bytes), one integer multiply-add per photon for its

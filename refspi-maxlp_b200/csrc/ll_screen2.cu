@@ -423,7 +423,7 @@ __device__ __forceinline__ unsigned entry16_at(const unsigned short *__restrict_
 __global__ void __launch_bounds__(BANK_WARPS * 32)
 k_wide_groups_banked(const unsigned short *__restrict__ ent16,
                      const long long *__restrict__ row_off16, long long n, int p_zero,
-                     int classes, int per, int *__restrict__ groups) {
+                     int classes, int slots, int *__restrict__ groups) {
     __shared__ int cnt[BANK_WARPS][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -441,7 +441,7 @@ k_wide_groups_banked(const unsigned short *__restrict__ ent16,
         }
         int mx = lane < classes ? cnt[w][lane] : 0;
         mx = warp_max_int(mx);
-        if (lane == 0) groups[d] = (mx + 4 * per - 1) / (4 * per);
+        if (lane == 0) groups[d] = (mx + slots - 1) / slots;
         __syncwarp();
     }
 }
@@ -526,6 +526,59 @@ k_pair_fill(const unsigned short *__restrict__ ent16, const long long *__restric
                 const int k = base[w][key] + __popc(m & lt);
                 if ((k >> 2) < ng)
                     out[((g0 + (k >> 2)) * 32 + 16 * h + key) * 4 + (k & 3)] =
+                        (unsigned short)(e / 16u);
+            }
+            __syncwarp();
+            if (key < 16 && lane == __ffs(m) - 1) base[w][key] += __popc(m);
+            __syncwarp();
+        }
+    }
+}
+
+// Frame quads: eight lanes per frame, four frames per warp.  Sub-frame u of
+// a quad takes lanes 8 u + j (j < 8); lane j holds the frame's photons of
+// bank classes j and j + 8, the one in slots 0 and 2 of a group (phase 0)
+// and the other in slots 1 and 3 (phase 1), with the phases swapped on odd
+// u: every shared gather of a half-warp then touches 16 distinct bank
+// classes.  The k-th photon of class c goes to group k / 2, slot
+// 2 (k mod 2) + phase; a quad takes the largest of its frames' group counts
+// ceil(max_c n_c / 2); every other slot holds column p_zero + class (q =
+// p_zero / 16), a zero column of the slot's class.
+__global__ void k_quad_pad(long long n_slots, int p_zero, uint2 *__restrict__ out) {
+    const unsigned pad = (unsigned)p_zero / 16u;
+    const unsigned pad2 = pad | (pad << 16);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_slots;
+         i += stride)
+        out[i] = make_uint2(pad2, pad2);
+}
+
+__global__ void __launch_bounds__(BANK_WARPS * 32)
+k_quad_fill(const unsigned short *__restrict__ ent16, const long long *__restrict__ row_off16,
+            long long n, int p_zero, const int *__restrict__ quad_slot,
+            const long long *__restrict__ qgoff, unsigned short *__restrict__ out) {
+    __shared__ int base[BANK_WARPS][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    for (long long d = warp; d < n; d += nwarp) {
+        const int qs = quad_slot[d];
+        const long long qd = qs >> 2;
+        const int u = qs & 3;
+        const long long g0 = qgoff[qd], ng = qgoff[qd + 1] - g0;
+        base[w][lane] = 0;
+        __syncwarp();
+        const long long r0 = row_off16[d], nr = row_off16[d + 1] - r0;
+        for (long long r = 0; r < nr; ++r) {
+            const unsigned e = entry16_at(ent16, r0 + r, lane);
+            const int key = e < (unsigned)p_zero ? (int)(e % 16u) : 16;
+            const unsigned m = __match_any_sync(RSPI_FULL_MASK, key);
+            if (key < 16) {
+                const int k = base[w][key] + __popc(m & lt);
+                const int phase = (key >> 3) ^ (u & 1);
+                if ((k >> 1) < ng)
+                    out[((g0 + (k >> 1)) * 32 + 8 * u + (key & 7)) * 4 + 2 * (k & 1) + phase] =
                         (unsigned short)(e / 16u);
             }
             __syncwarp();
@@ -824,6 +877,119 @@ k_screen_ll5(const float *__restrict__ lsl, int p_row, int num_rot,
     }
 }
 
+// Frame quads (two rows per tile, 16-bit entries of k_quad_fill): lanes
+// 8 u .. 8 u + 7 sum frame quad_frames[4 q + u] of quad q; one pass of three
+// exchange steps inside each group of eight lanes reduces all four frames,
+// and lanes 8 u + t store row t of frame u.
+__global__ void __launch_bounds__(1024)
+k_screen_ll6(const float *__restrict__ lsl, int p_row, int num_rot,
+             const double *__restrict__ init, const double *__restrict__ scales,
+             const uint2 *__restrict__ groups, const long long *__restrict__ qgoff,
+             const int *__restrict__ quad_frames, int n_quads, long long row_begin,
+             long long row_end, float *__restrict__ ll, long long ll_stride) {
+    constexpr int T = 2;
+    constexpr int PG = 4;   // groups (4 photons per lane each) loaded ahead
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float *slf = reinterpret_cast<float *>(smem_raw);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int u = lane >> 3, j = lane & 7;
+    const long long n_tiles = (row_end - row_begin + T - 1) / T;
+    const int gtot = (int)qgoff[n_quads];
+    auto lower = [&](int target) {
+        int lo = 0, hi = n_quads;
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if ((int)qgoff[mid] < target) lo = mid + 1;
+            else hi = mid;
+        }
+        return lo;
+    };
+    const int qb = wid == 0 ? 0 : lower((int)((long long)gtot * wid / nw));
+    const int qe = wid == nw - 1 ? n_quads : lower((int)((long long)gtot * (wid + 1) / nw));
+    // byte offsets of the lane's two classes: phase 0 in slots 0, 2, phase 1 in 1, 3
+    const unsigned off0 = 8u * (unsigned)(j + 8 * (u & 1));
+    const unsigned off1 = 8u * (unsigned)(j + 8 * (1 - (u & 1)));
+
+    for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+        const long long first = row_begin + tile * T;
+        const int nt = (int)min((long long)T, row_end - first);
+        __syncthreads();
+        stage_tile<T>(slf, lsl + (first - row_begin) * (long long)p_row, p_row, nt);
+        __syncthreads();
+        if (qb >= qe) continue;
+
+        const bool storer = j < nt;   // lanes 8 u + t store row t
+        const double my_init = storer ? init[(first + j) / num_rot] : 0.;
+        float *my_ll = ll + (first + (storer ? j : 0) - row_begin) * ll_stride;
+        Acc<T> a0, a1;
+        a0.zero();
+        a1.zero();
+        int base = qb;
+        int my_end = qb + lane < n_quads ? (int)qgoff[qb + lane + 1] : 0x7fffffff;
+        int q = qb;
+        int g = (int)qgoff[qb];
+        const int gend = (int)qgoff[qe];
+        int qend = __shfl_sync(RSPI_FULL_MASK, my_end, 0);
+        int my_d = storer ? quad_frames[4 * q + u] : -1;
+        double my_sc = my_d >= 0 ? scales[my_d] : 0.;
+        auto finish = [&]() {
+            float2 a = __fadd2_rn(a0.p[0], a1.p[0]);
+#pragma unroll
+            for (int o = 4; o > 0; o >>= 1) {
+                const float2 b = make_float2(__shfl_xor_sync(RSPI_FULL_MASK, a.x, o),
+                                             __shfl_xor_sync(RSPI_FULL_MASK, a.y, o));
+                a = __fadd2_rn(a, b);
+            }
+            if (my_d >= 0) my_ll[my_d] = (float)(my_init * my_sc + (double)(j == 0 ? a.x : a.y));
+            a0.zero();
+            a1.zero();
+            ++q;
+            if (q - base == 32) {
+                base = q;
+                my_end = q + lane < n_quads ? (int)qgoff[q + lane + 1] : 0x7fffffff;
+            }
+            qend = q < qe ? __shfl_sync(RSPI_FULL_MASK, my_end, q - base) : gend + 1;
+            my_d = storer && q < qe ? quad_frames[4 * q + u] : -1;
+            my_sc = my_d >= 0 ? scales[my_d] : 0.;
+        };
+        while (q < qe && qend == g) finish();   // quads without entries
+
+        const uint2 *gp = groups + (long long)g * 32 + lane;
+        uint2 cur[PG], nxt[PG];
+        const uint2 z{};
+#pragma unroll
+        for (int k = 0; k < PG; ++k) cur[k] = g + k < gend ? __ldg(gp + 32 * k) : z;
+        while (g < gend) {
+            const int nb = min(PG, gend - g);
+#pragma unroll
+            for (int k = 0; k < PG; ++k) nxt[k] = g + PG + k < gend ? __ldg(gp + 32 * (PG + k)) : z;
+            Contrib<T> c0[PG], c1[PG];
+#pragma unroll
+            for (int k = 0; k < PG; ++k) {
+                c0[k] = gather_pair<T>(smem_raw, (cur[k].x & 0xffffu) * 128u + off0,
+                                       (cur[k].x >> 16) * 128u + off1);
+                c1[k] = gather_pair<T>(smem_raw, (cur[k].y & 0xffffu) * 128u + off0,
+                                       (cur[k].y >> 16) * 128u + off1);
+            }
+#pragma unroll
+            for (int k = 0; k < PG; ++k) {
+                if (k < nb) {
+                    add_contrib<T>(a0, c0[k]);
+                    add_contrib<T>(a1, c1[k]);
+                    if (g + k + 1 == qend) {
+                        finish();
+                        while (q < qe && qend == g + k + 1) finish();
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < PG; ++k) cur[k] = nxt[k];
+            g += PG;
+            gp += 32 * PG;
+        }
+    }
+}
+
 // FP16 slices, four rows per tile: the interleaved tile holds sl[c][0..3] as
 // halves (8 bytes per pixel), so one 8-byte gather brings four rows' values
 // of a photon -- twice the rows per shared-memory wavefront of the FP32
@@ -1104,7 +1270,7 @@ extern "C" int rspi_wide_entry_groups_banked(const unsigned short *entries16,
         return RSPI_ERR_ARG;
     k_wide_groups_banked<<<rspi_blocks(n_data * 32, BANK_WARPS * 32), BANK_WARPS * 32, 0,
                            stream>>>(entries16, row_off16, n_data, p_zero, 32 / states_per_tile,
-                                     states_per_tile, groups);
+                                     4 * states_per_tile, groups);
     RSPI_RETURN_LAUNCH();
 }
 
@@ -1231,7 +1397,7 @@ extern "C" int rspi_pair_entry_groups(const unsigned short *entries16, const lon
         p_zero + 32 > 65536)
         return RSPI_ERR_ARG;
     k_wide_groups_banked<<<rspi_blocks(n_data * 32, BANK_WARPS * 32), BANK_WARPS * 32, 0,
-                           stream>>>(entries16, row_off16, n_data, p_zero, 16, 1, groups);
+                           stream>>>(entries16, row_off16, n_data, p_zero, 16, 4, groups);
     RSPI_RETURN_LAUNCH();
 }
 
@@ -1284,5 +1450,68 @@ extern "C" int rspi_screen_loglike5(const float *lslices, long long p_row, long 
     k_screen_ll5<<<n_ctas, warps_per_cta * 32, smem, stream>>>(
         lslices, (int)p_row, (int)num_rot, init, scales, reinterpret_cast<const uint2 *>(narrow),
         pair_group_off, pair_frames, (int)n_pairs, row_begin, row_end, ll, ll_stride);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_quad_entry_groups(const unsigned short *entries16, const long long *row_off16,
+                                      long long n_data, int p_zero, int *groups,
+                                      cudaStream_t stream) {
+    if (!entries16 || !row_off16 || !groups || n_data <= 0 || p_zero < 0 || p_zero % 32 ||
+        p_zero + 32 > 65536)
+        return RSPI_ERR_ARG;
+    k_wide_groups_banked<<<rspi_blocks(n_data * 32, BANK_WARPS * 32), BANK_WARPS * 32, 0,
+                           stream>>>(entries16, row_off16, n_data, p_zero, 16, 2, groups);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_quad_entry_fill(const unsigned short *entries16, const long long *row_off16,
+                                    long long n_data, int p_zero, const int *quad_slot,
+                                    const long long *quad_group_off, long long total_groups,
+                                    unsigned short *narrow, cudaStream_t stream) {
+    if (!entries16 || !row_off16 || !quad_slot || !quad_group_off || !narrow || n_data <= 0 ||
+        p_zero < 0 || p_zero % 32 || p_zero + 32 > 65536 || total_groups < 0 ||
+        (reinterpret_cast<uintptr_t>(narrow) & 7) != 0)
+        return RSPI_ERR_ARG;
+    if (total_groups > 0)
+        k_quad_pad<<<rspi_blocks(total_groups * 32, 256), 256, 0, stream>>>(
+            total_groups * 32, p_zero, reinterpret_cast<uint2 *>(narrow));
+    k_quad_fill<<<rspi_blocks(n_data * 32, BANK_WARPS * 32), BANK_WARPS * 32, 0, stream>>>(
+        entries16, row_off16, n_data, p_zero, quad_slot, quad_group_off, narrow);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_screen_loglike6(const float *lslices, long long p_row, long long num_rot,
+                                    const double *init, const double *scales,
+                                    const unsigned short *narrow, const long long *quad_group_off,
+                                    const int *quad_frames, long long n_quads, long long row_begin,
+                                    long long row_end, float *ll, long long ll_stride,
+                                    int warps_per_cta, int n_ctas, cudaStream_t stream) {
+    if (!lslices || !init || !scales || !narrow || !quad_group_off || !quad_frames || !ll ||
+        n_quads <= 0 || n_quads > 0x1fffffffLL || p_row <= 32 || p_row % 32 || p_row > 65536 ||
+        num_rot <= 0 || num_rot > 0x7fffffffLL || row_begin < 0 || row_end < row_begin ||
+        warps_per_cta < 1 || warps_per_cta > 32)
+        return RSPI_ERR_ARG;
+    if ((reinterpret_cast<uintptr_t>(lslices) & 15) != 0 ||
+        (reinterpret_cast<uintptr_t>(narrow) & 7) != 0)
+        return RSPI_ERR_ARG;
+    if (row_end == row_begin) return RSPI_OK;
+    const size_t smem = 2 * (size_t)p_row * sizeof(float);
+    if (smem > (size_t)SMEM_LIMIT - 1024) return RSPI_ERR_ARG;
+    static size_t smem_set = 0;
+    if (smem > smem_set) {
+        if (cudaFuncSetAttribute(k_screen_ll6, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return RSPI_ERR_CUDA;
+        smem_set = smem;
+    }
+    const long long n_tiles = (row_end - row_begin + 1) / 2;
+    if (n_ctas <= 0) {
+        const int per_sm = max(1, (int)(SMEM_LIMIT / (smem + 1024)));
+        n_ctas = rspi_sm_count() * min(per_sm, max(1, 2048 / (warps_per_cta * 32)));
+    }
+    if (n_ctas > n_tiles) n_ctas = (int)n_tiles;
+    k_screen_ll6<<<n_ctas, warps_per_cta * 32, smem, stream>>>(
+        lslices, (int)p_row, (int)num_rot, init, scales, reinterpret_cast<const uint2 *>(narrow),
+        quad_group_off, quad_frames, (int)n_quads, row_begin, row_end, ll, ll_stride);
     RSPI_RETURN_LAUNCH();
 }

@@ -61,7 +61,7 @@ def tune(es, sample_tiles=2, repeats=2, use_cache=True, verbose=False):
     screen2 = es.form == 'screen' and es.kernel == 'stream'
     if es.form == 'screen' and es.kernel in ('frame', 'wide'):
         tiles = (1, 2)
-    elif es.form == 'screen' and es.kernel == 'pair':
+    elif es.form == 'screen' and es.kernel in ('pair', 'quad'):
         tiles = (2,)   # the frame-pair kernel: warps per CTA only
     else:
         tiles = (1, 2, 4) if screen2 else TILES

@@ -224,14 +224,14 @@ class EStep:
             raise ValueError('form must be fp64, screen or dense')
         auto_kernel = kernel is None
         if kernel is None:   # default likelihood kernel of each form (the screened
-            # form's frame-pair kernel is chosen below when a two-row tile fits)
+            # form's frame-quad kernel is chosen below when a two-row tile fits)
             kernel = 'wide' if form == 'screen' else 'stream'
         if screen_slices not in ('fp32', 'fp16'):
             raise ValueError('screen_slices must be fp32 or fp16')
         if form == 'screen' and screen_slices == 'fp16':
             kernel = 'wide16'   # the FP16-slice kernel: four rows per tile
-        if kernel not in ('stream', 'frame', 'wide', 'wide16', 'pair', 'dynamic'):
-            raise ValueError('kernel must be stream, frame, wide, pair or dynamic')
+        if kernel not in ('stream', 'frame', 'wide', 'wide16', 'pair', 'quad', 'dynamic'):
+            raise ValueError('kernel must be stream, frame, wide, pair, quad or dynamic')
         self.kernel = kernel
         self.lib = load()
         self.form = form
@@ -276,16 +276,16 @@ class EStep:
         tmax = self.lib.rspi_loglike_max_tile(self.p_row, self.slice_code)
         if auto_kernel and form == 'screen' and kernel == 'wide' and tmax >= 2 and \
                 states_per_tile in (None, 2):
-            kernel = self.kernel = 'pair'
+            kernel = self.kernel = 'quad'
         if kernel == 'wide16':
             tmax = 4 if self.p_row * 8 <= 226 * 1024 else 0
         if form == 'screen' and kernel == 'stream':
             tmax = 4 if tmax >= 4 else (2 if tmax >= 2 else tmax)   # interleaved: 1, 2 or 4
         if form == 'screen' and kernel in ('frame', 'wide'):
             tmax = min(tmax, 2)                                     # 1 or 2 rows per tile
-        if kernel == 'pair':
+        if kernel in ('pair', 'quad'):
             tmax = 2 if tmax >= 2 else 0                            # two rows per tile
-        if form != 'screen' and kernel in ('frame', 'wide', 'wide16', 'pair'):
+        if form != 'screen' and kernel in ('frame', 'wide', 'wide16', 'pair', 'quad'):
             raise ValueError('the %s kernel is a screened-form kernel' % kernel)
         if tmax == 0:
             raise ValueError('a %d-pixel likelihood slice does not fit in shared memory' % self.n_sel)
@@ -301,12 +301,12 @@ class EStep:
             self.prefetch_words = 4 if wpf <= 5 else (8 if wpf <= 10 else 12)
         if kernel == 'wide16' and self.tile != 4:
             raise ValueError('the FP16-slice kernel takes 4 states per tile')
-        if kernel == 'pair' and self.tile != 2:
-            raise ValueError('the frame-pair kernel takes 2 states per tile')
+        if kernel in ('pair', 'quad') and self.tile != 2:
+            raise ValueError('the multi-frame kernels take 2 states per tile')
         self.bank_layout = bool(bank_layout)
         self.narrow_entries = bool(narrow_entries)
         self.wide = self._wide_entries() if (form == 'screen' and
-                                             kernel in ('wide', 'wide16', 'pair')) else None
+                                             kernel in ('wide', 'wide16', 'pair', 'quad')) else None
         self._eps_key, self.row_off_eps = None, None
         self.warps, self.n_ctas = int(warps), int(n_ctas)
         esz = {0: 4, 1: 8, 2: 2}[self.slice_code]
@@ -418,42 +418,45 @@ class EStep:
         return 2 if self.kernel == 'wide16' else self.tile
 
     def _pair_entries(self):
-        """Frame pairs for the frame-pair kernel: within each window of
-        PAIR_WINDOW consecutive frames, frames sorted by their half-warp group
-        count (longest first) and taken two at a time, so that a warp's
-        likelihood stores stay within a few sectors of each row; the 16-bit
-        bank-class entries of both frames of a pair in one group range
-        (lanes 16 h + class for frame h)."""
+        """Frame groups for the multi-frame kernels (``pair``: two frames per
+        warp, 16 lanes each; ``quad``: four, 8 lanes each): within each window
+        of PAIR_WINDOW consecutive frames, frames sorted by their group count
+        (longest first) and taken F at a time, so that a warp's likelihood
+        stores stay within a few sectors of each row; the 16-bit bank-class
+        entries of the F frames of a group in one group range."""
         l16, n, dev, s = self.ll16, self.ph.num_data, self.device, cur_stream()
+        nf = 4 if self.kernel == 'quad' else 2
+        fn = 'quad' if nf == 4 else 'pair'
         pz = self.p_row - 32
         ng = torch.empty(n, dtype=_i32, device=dev)
-        call('rspi_pair_entry_groups', ptr(l16['entries']), ptr(l16['row_off']), n, pz, ptr(ng), s)
+        call('rspi_%s_entry_groups' % fn, ptr(l16['entries']), ptr(l16['row_off']), n, pz, ptr(ng),
+             s)
         gmax = int(ng.max().item())
         win = torch.arange(n, device=dev, dtype=_i64) // PAIR_WINDOW
         order = torch.argsort(win * (gmax + 1) + (gmax - ng.to(_i64)), stable=True).to(_i32)
-        n_pairs = (n + 1) // 2
-        pair_frames = torch.full((2 * n_pairs,), -1, dtype=_i32, device=dev)
-        pair_frames[:n] = order
-        pair_slot = torch.empty(n, dtype=_i32, device=dev)
-        pair_slot[order.long()] = torch.arange(n, dtype=_i32, device=dev)
-        ngp = torch.zeros(2 * n_pairs, dtype=_i32, device=dev)
-        ngp[:n] = ng[order.long()]
-        png = ngp.view(n_pairs, 2).amax(1).contiguous()
-        pgoff = torch.empty(n_pairs + 1, dtype=_i64, device=dev)
-        call('rspi_scan_rows', ptr(png), n_pairs, ptr(pgoff), s)
-        total = int(pgoff[-1].item())
+        n_sets = (n + nf - 1) // nf
+        set_frames = torch.full((nf * n_sets,), -1, dtype=_i32, device=dev)
+        set_frames[:n] = order
+        set_slot = torch.empty(n, dtype=_i32, device=dev)
+        set_slot[order.long()] = torch.arange(n, dtype=_i32, device=dev)
+        ngs = torch.zeros(nf * n_sets, dtype=_i32, device=dev)
+        ngs[:n] = ng[order.long()]
+        sng = ngs.view(n_sets, nf).amax(1).contiguous()
+        soff = torch.empty(n_sets + 1, dtype=_i64, device=dev)
+        call('rspi_scan_rows', ptr(sng), n_sets, ptr(soff), s)
+        total = int(soff[-1].item())
         narrow = torch.empty(max(1, total) * 128, dtype=torch.int16, device=dev)
-        call('rspi_pair_entry_fill', ptr(l16['entries']), ptr(l16['row_off']), n, pz,
-             ptr(pair_slot), ptr(pgoff), total, ptr(narrow), s)
-        return dict(entries=narrow, group_off=pgoff, total_groups=total, tile=2, banked=True,
-                    narrow=True, pairs=True, pair_frames=pair_frames, n_pairs=n_pairs,
-                    frame_groups=png[(pair_slot >> 1).long()])
+        call('rspi_%s_entry_fill' % fn, ptr(l16['entries']), ptr(l16['row_off']), n, pz,
+             ptr(set_slot), ptr(soff), total, ptr(narrow), s)
+        return dict(entries=narrow, group_off=soff, total_groups=total, tile=2, banked=True,
+                    narrow=True, pairs=True, frames_per=nf, pair_frames=set_frames,
+                    n_pairs=n_sets, frame_groups=sng[(set_slot // nf).long()])
 
     def _wide_entries(self):
         """32-bit entries holding each photon's byte offset in the
         interleaved tile (sel * 4 * tile), four rows of a lane per 16-byte
         group, rows of a frame padded to a multiple of four."""
-        if self.kernel == 'pair':
+        if self.kernel in ('pair', 'quad'):
             return self._pair_entries()
         l16, n, dev, s = self.ll16, self.ph.num_data, self.device, cur_stream()
         groups = torch.empty(n, dtype=_i32, device=dev)
@@ -491,7 +494,8 @@ class EStep:
         if key != self._eps_key:
             ro = self.ll16['row_off']
             rows = ro[1:] - ro[:-1]
-            if self.kernel == 'pair' and self.wide is not None and self.wide.get('pairs'):
+            if self.kernel in ('pair', 'quad') and self.wide is not None and \
+                    self.wide.get('pairs'):
                 rows = torch.maximum(rows, self.wide['frame_groups'].to(_i64))
             elif self.kernel in ('wide', 'wide16') and self.wide is not None and \
                     self.wide['banked']:
@@ -595,10 +599,11 @@ class EStep:
             call('rspi_screen_loglike4h', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
                  ptr(self.ph.scales), ptr(self.wide['entries']), ptr(self.wide['group_off']), n,
                  r0, r1, ptr(self.prob[r0]), n, self.warps, self.n_ctas, cur_stream())
-        elif self.kernel == 'pair' and self.form == 'screen':
-            if self.wide is None or not self.wide.get('pairs'):
+        elif self.kernel in ('pair', 'quad') and self.form == 'screen':
+            nf = 4 if self.kernel == 'quad' else 2
+            if self.wide is None or self.wide.get('frames_per') != nf:
                 self.wide = self._pair_entries()
-            call('rspi_screen_loglike5', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
+            call('rspi_screen_loglike6' if nf == 4 else 'rspi_screen_loglike5', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
                  ptr(self.ph.scales), ptr(self.wide['entries']), ptr(self.wide['group_off']),
                  ptr(self.wide['pair_frames']), self.wide['n_pairs'], r0, r1, ptr(self.prob[r0]), n,
                  self.warps, self.n_ctas, cur_stream())

@@ -284,7 +284,7 @@ def test_frame_kernel_matches_stream_kernel(name, ds, need_scaling, tile, warps)
     variants = (('stream', True, True), ('frame', True, True), ('wide', True, True),
                 ('wide', True, False), ('wide', False, False))
     if tile == 2:
-        variants += (('pair', True, True),)
+        variants += (('pair', True, True), ('quad', True, True))
     for kernel, banked, narrow in variants:
         ph = _photons(ds, need_scaling)
         es = _estep(ph, size, num_rot, sx, sy, dia, ds['bg'], form='screen', kernel=kernel,
@@ -302,7 +302,7 @@ def test_frame_kernel_matches_stream_kernel(name, ds, need_scaling, tile, warps)
     assert np.array_equal(out['wide', True, True][0], out['wide', True, False][0])
     others = [out['frame', True, True], out['wide', True, True], out['wide', False, False]]
     if tile == 2:
-        others.append(out['pair', True, True])
+        others += [out['pair', True, True], out['quad', True, True]]
     for b in others:
         assert np.all(np.abs(a[0] - b[0]) <= 1e-6 * scale)
         assert np.array_equal(a[2], b[2])
@@ -449,3 +449,56 @@ def test_pair_layout_entries(n):
     assert sorted(seen) == list(range(n))
     # pairing stays inside windows of consecutive frames
     assert np.all(pf[:n] // PAIR_WINDOW == np.arange(n) // PAIR_WINDOW)
+
+
+@pytest.mark.parametrize('n', [61, 300])
+def test_quad_layout_entries(n):
+    """Frame quads: every frame's photons once, in its eight lanes; lane j of
+    sub-frame u holds classes j and j + 8 in alternating slots (phases
+    swapped on odd u), so each half-warp gather covers 16 distinct classes;
+    zero columns of the slot's class elsewhere."""
+    from rspi.device import PAIR_WINDOW
+    size = 37
+    d = random_photons(size, n, 40. * size, 13, empty_frames=(2, 9), heavy=5)
+    ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
+                         d['count_multi'], size * size, False)
+    sx, sy, dia, _ = E.generate_states(E.parse_triple('0 0 1'), E.parse_triple('0 0 1'),
+                                       E.parse_triple('2 2 1'))
+    es_q = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen',
+                  kernel='quad', states_per_tile=2)
+    es_w = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen',
+                  kernel='wide', states_per_tile=2, narrow_entries=False)
+    torch.cuda.synchronize()
+    w = es_q.wide
+    pz = es_q.p_row - 32
+    q = w['entries'].cpu().numpy().view(np.uint16).reshape(-1, 32, 4).astype(np.int64)
+    lane = np.arange(32)[:, None]
+    slot = np.arange(4)[None, :]
+    u, j = lane // 8, lane % 8
+    cls = j + 8 * ((slot % 2) ^ (u % 2))                      # (32, 4)
+    sel = q * 16 + cls[None]
+    for hw in range(2):                                       # conflict-free half-warps
+        for sl in range(4):
+            assert len(set(cls[16 * hw:16 * hw + 16, sl])) == 16
+    goff = w['group_off'].cpu().numpy()
+    qf = w['pair_frames'].cpu().numpy()
+    assert w['frames_per'] == 4 and w['n_pairs'] == (n + 3) // 4
+    wide = es_w.wide['entries'].cpu().numpy().view(np.uint32).reshape(-1, 32, 4) // 8
+    woff = es_w.wide['group_off'].cpu().numpy()
+    seen = []
+    for qd in range(w['n_pairs']):
+        blk = sel[goff[qd]:goff[qd + 1]]
+        for uu in range(4):
+            f = qf[4 * qd + uu]
+            part = blk[:, 8 * uu:8 * uu + 8]
+            if f < 0:
+                assert np.all(part >= pz)
+                continue
+            seen.append(f)
+            ref = wide[woff[f]:woff[f + 1]]
+            assert np.array_equal(np.sort(part[part < pz]), np.sort(ref[ref < pz])), f
+            pads = part >= pz
+            want = np.broadcast_to(pz + cls[8 * uu:8 * uu + 8][None], part.shape)
+            assert np.array_equal(part[pads], want[pads])
+    assert sorted(seen) == list(range(n))
+    assert np.all(qf[:n] // PAIR_WINDOW == np.arange(n) // PAIR_WINDOW)

@@ -62,8 +62,10 @@ def parse_args():
     ap.add_argument('--frames', type=int, default=None, help='override frame count (testing)')
     ap.add_argument('--form', default=None, choices=['fp64', 'screen', 'dense'],
                     help='likelihood form (default: dense for config 5, screen otherwise)')
-    ap.add_argument('--kernel', default=None, choices=['stream', 'frame', 'wide', 'pair', 'quad', 'dynamic'],
+    ap.add_argument('--kernel', default=None, choices=['stream', 'frame', 'wide', 'pair', 'quad', 'quad4', 'dynamic'],
                     help='likelihood kernel (default: wide for the screened form, stream for FP64)')
+    ap.add_argument('--warps', type=int, default=None,
+                    help='warps per CTA of the likelihood kernel (default: the EStep default, 32)')
     ap.add_argument('--screen-slices', default='fp32', choices=['fp32', 'fp16'],
                     help='screened form: FP32 slices (two rows per gather) or FP16 (four)')
     ap.add_argument('--screen-delta', type=float, default=None,
@@ -214,7 +216,8 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
     gather_peak = sm_count * lanes * clk_mhz * 1e6
     gather_rate = gathers / (ll_launch_ms * 1e-3)
     names = {'stream': 'k_screen_ll2', 'frame': 'k_screen_ll3', 'wide': 'k_screen_ll4',
-             'wide16': 'k_screen_ll4h', 'pair': 'k_screen_ll5', 'quad': 'k_screen_ll6'}
+             'wide16': 'k_screen_ll4h', 'pair': 'k_screen_ll5', 'quad': 'k_screen_ll6',
+             'quad4': 'k_screen_ll7'}
     roof = dict({'kernel': ('%s (%s screening likelihood, row a7)' %
                             (names.get(es.kernel, es.kernel), 'FP16' if es.slice_code == 2 else 'FP32')
                             if es.form == 'screen' else 'k_ll_stream / k_loglike (FP64 likelihood, row a7)'),
@@ -514,6 +517,8 @@ def run_ours(args):
         rec = EMC(cfgfile, device=dev)
     if rec.estep.form != 'dense' and args.kernel and args.kernel != rec.estep.kernel:
         rec.estep.kernel = args.kernel
+    if args.warps:
+        rec.estep.warps = args.warps
     if args.no_phaser_screen:
         rec.phaser.mstep.screen = False
     model0 = start_model(args.config, w)

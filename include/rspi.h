@@ -320,6 +320,40 @@ int rspi_screen_loglike6(const float *lslices, long long p_row, long long num_ro
                          long long ll_stride, int warps_per_cta, int n_ctas,
                          cudaStream_t stream);
 
+/* Frame quads with four rows per tile: one 16-byte gather brings a photon's
+ * value in all four rows.  The likelihood columns [0, p_zero) are cut into
+ * n_parts (1-4) parts of part_w columns (part_w % 8 == 0, n_parts * part_w
+ * >= p_zero), each staged with 8 zero columns after it.  Lane 8 u + j of a
+ * group holds frame u's photons of part h whose local column (column -
+ * h part_w) is = j (mod 8), as q = local / 8, four per group; the k-th
+ * photon of (h, j) goes to group k / 4, slot k mod 4; other slots hold
+ * q = part_w / 8.
+ * rspi_quad4_entry_groups: groups[d * n_parts + h] = ceil(max_j n_hj / 4).
+ * The caller forms quads (quad_slot[d] = 4 q + u, quad_frames), takes per
+ * (quad, part) the largest count of its frames and scans them part-major
+ * into group_off[n_parts * n_quads + 1] (range h * n_quads + q).
+ * rspi_quad4_entry_fill: total_groups * 128 16-bit entries (8-byte aligned).
+ * rspi_screen_loglike7: the likelihood rows from them.  With several parts
+ * the running FP32 sum of each (CTA, row, frame slot) sits in part_sums
+ * (rspi_quad4_part_sums_floats(n_quads, part_sums_ctas) floats; at most
+ * part_sums_ctas CTAs run) and the parts' sums are added in FP64 before the
+ * final FP32 rounding: within the FP32 error bound with each frame's
+ * summation length max(entry rows, its quad's largest part group count). */
+int rspi_quad4_entry_groups(const unsigned short *entries16, const long long *row_off16,
+                            long long n_data, int p_zero, int n_parts, int part_w, int *groups,
+                            cudaStream_t stream);
+int rspi_quad4_entry_fill(const unsigned short *entries16, const long long *row_off16,
+                          long long n_data, int p_zero, int n_parts, int part_w,
+                          const int *quad_slot, const long long *group_off, long long n_quads,
+                          long long total_groups, unsigned short *narrow, cudaStream_t stream);
+long long rspi_quad4_part_sums_floats(long long n_quads, int n_ctas);
+int rspi_screen_loglike7(const float *lslices, long long p_row, long long num_rot,
+                         const double *init, const double *scales, const unsigned short *narrow,
+                         const long long *group_off, const int *quad_frames, long long n_quads,
+                         int n_parts, int part_w, long long row_begin, long long row_end,
+                         float *ll, long long ll_stride, float *part_sums, int part_sums_ctas,
+                         int warps_per_cta, int n_ctas, cudaStream_t stream);
+
 /* rspi_screen_loglike4 from the 16-bit bank-class entries of
  * rspi_wide_entry_fill_narrow: one 8-byte load per four photons of a lane
  * (half the entry bytes), one integer multiply-add per photon for its

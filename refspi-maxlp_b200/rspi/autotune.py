@@ -63,6 +63,8 @@ def tune(es, sample_tiles=2, repeats=2, use_cache=True, verbose=False):
         tiles = (1, 2)
     elif es.form == 'screen' and es.kernel in ('pair', 'quad'):
         tiles = (2,)   # the frame-pair kernel: warps per CTA only
+    elif es.form == 'screen' and es.kernel == 'quad4':
+        tiles = (4,)   # the four-row frame-quad kernel: warps per CTA only
     else:
         tiles = (1, 2, 4) if screen2 else TILES
     cands = [(t, w) for t in tiles if t <= tmax for w in WARPS

@@ -24,6 +24,8 @@ _i32 = torch.int32
 _i64 = torch.int64
 INT32_MAX = 2 ** 31 - 1
 PAIR_WINDOW = 256   # frames sorted by length for pairing within such windows
+QUAD4_SMEM = 227 * 1024 - 1024   # shared bytes of the four-row tile (kernel limit)
+QUAD4_MAX_PARTS = 4              # column parts of the four-row tile
 
 
 def ptr(t):
@@ -219,7 +221,7 @@ class EStep:
                  form='fp64', states_per_tile=None, warps=32, n_ctas=0,
                  slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel=None,
                  n_modes=1, dense_gemm='auto', dense_rescore=True, screen_slices='fp32',
-                 bank_layout=True, narrow_entries=True):
+                 bank_layout=True, narrow_entries=True, screen_parts=None):
         if form not in ('fp64', 'screen', 'dense'):
             raise ValueError('form must be fp64, screen or dense')
         auto_kernel = kernel is None
@@ -230,8 +232,9 @@ class EStep:
             raise ValueError('screen_slices must be fp32 or fp16')
         if form == 'screen' and screen_slices == 'fp16':
             kernel = 'wide16'   # the FP16-slice kernel: four rows per tile
-        if kernel not in ('stream', 'frame', 'wide', 'wide16', 'pair', 'quad', 'dynamic'):
-            raise ValueError('kernel must be stream, frame, wide, pair, quad or dynamic')
+        if kernel not in ('stream', 'frame', 'wide', 'wide16', 'pair', 'quad', 'quad4', 'dynamic'):
+            raise ValueError('kernel must be stream, frame, wide, pair, quad, quad4 or dynamic')
+        self.screen_parts = None if screen_parts is None else int(screen_parts)
         self.kernel = kernel
         self.lib = load()
         self.form = form
@@ -285,7 +288,9 @@ class EStep:
             tmax = min(tmax, 2)                                     # 1 or 2 rows per tile
         if kernel in ('pair', 'quad'):
             tmax = 2 if tmax >= 2 else 0                            # two rows per tile
-        if form != 'screen' and kernel in ('frame', 'wide', 'wide16', 'pair', 'quad'):
+        if kernel == 'quad4':
+            tmax = 4                                                # four rows, column parts
+        if form != 'screen' and kernel in ('frame', 'wide', 'wide16', 'pair', 'quad', 'quad4'):
             raise ValueError('the %s kernel is a screened-form kernel' % kernel)
         if tmax == 0:
             raise ValueError('a %d-pixel likelihood slice does not fit in shared memory' % self.n_sel)
@@ -303,12 +308,15 @@ class EStep:
             raise ValueError('the FP16-slice kernel takes 4 states per tile')
         if kernel in ('pair', 'quad') and self.tile != 2:
             raise ValueError('the multi-frame kernels take 2 states per tile')
+        if kernel == 'quad4' and self.tile != 4:
+            raise ValueError('the four-row frame-quad kernel takes 4 states per tile')
         self.bank_layout = bool(bank_layout)
         self.narrow_entries = bool(narrow_entries)
-        self.wide = self._wide_entries() if (form == 'screen' and
-                                             kernel in ('wide', 'wide16', 'pair', 'quad')) else None
-        self._eps_key, self.row_off_eps = None, None
         self.warps, self.n_ctas = int(warps), int(n_ctas)
+        self.wide = self._wide_entries() if (form == 'screen' and
+                                             kernel in ('wide', 'wide16', 'pair', 'quad',
+                                                        'quad4')) else None
+        self._eps_key, self.row_off_eps = None, None
         esz = {0: 4, 1: 8, 2: 2}[self.slice_code]
         rows = max(self.tile, (slice_budget_bytes // (self.p_row * esz)) // self.tile * self.tile)
         self.chunk_rows = int(min(self.n_rows, rows))
@@ -452,12 +460,71 @@ class EStep:
                     narrow=True, pairs=True, frames_per=nf, pair_frames=set_frames,
                     n_pairs=n_sets, frame_groups=sng[(set_slot // nf).long()])
 
+    def _quad4_parts(self):
+        """(parts, columns per part) of the four-row tile: the fewest column
+        parts whose four FP32 rows (16 bytes a column, plus 8 zero columns)
+        fit in shared memory, or ``screen_parts`` parts."""
+        pz = self.p_row - 32
+        cap = (QUAD4_SMEM // 16 - 8) // 8 * 8
+        parts = self.screen_parts or max(1, -(-pz // cap))
+        part_w = max(8, (-(-pz // parts) + 7) // 8 * 8)
+        if parts > QUAD4_MAX_PARTS or part_w > cap:
+            raise ValueError('%d likelihood pixels need more than %d column parts of the '
+                             'four-row tile' % (self.n_sel, QUAD4_MAX_PARTS))
+        return parts, part_w
+
+    def _quad4_entries(self):
+        """Entries of the four-row frame-quad kernel: frames ordered and taken
+        four at a time as for ``quad``; per (quad, column part) the largest of
+        its frames' group counts, group ranges part-major; lane j of a
+        sub-frame holds the photons of local column class j (mod 8); one
+        FP32 running sum per (CTA, row, frame slot) when there are several
+        parts."""
+        l16, n, dev, s = self.ll16, self.ph.num_data, self.device, cur_stream()
+        pz = self.p_row - 32
+        parts, part_w = self._quad4_parts()
+        ng = torch.empty(n * parts, dtype=_i32, device=dev)
+        call('rspi_quad4_entry_groups', ptr(l16['entries']), ptr(l16['row_off']), n, pz, parts,
+             part_w, ptr(ng), s)
+        ngp = ng.view(n, parts).to(_i64)
+        tot = ngp.sum(1)
+        gmax = int(tot.max().item())
+        win = torch.arange(n, device=dev, dtype=_i64) // PAIR_WINDOW
+        order = torch.argsort(win * (gmax + 1) + (gmax - tot), stable=True).to(_i32)
+        nq = (n + 3) // 4
+        set_frames = torch.full((4 * nq,), -1, dtype=_i32, device=dev)
+        set_frames[:n] = order
+        set_slot = torch.empty(n, dtype=_i32, device=dev)
+        set_slot[order.long()] = torch.arange(n, dtype=_i32, device=dev)
+        ngs = torch.zeros((4 * nq, parts), dtype=_i64, device=dev)
+        ngs[:n] = ngp[order.long()]
+        sng = ngs.view(nq, 4, parts).amax(1)                       # (quad, part)
+        flat = sng.t().contiguous().view(-1).to(_i32)             # part-major
+        soff = torch.empty(parts * nq + 1, dtype=_i64, device=dev)
+        call('rspi_scan_rows', ptr(flat), parts * nq, ptr(soff), s)
+        total = int(soff[-1].item())
+        narrow = torch.empty(max(1, total) * 128, dtype=torch.int16, device=dev)
+        call('rspi_quad4_entry_fill', ptr(l16['entries']), ptr(l16['row_off']), n, pz, parts,
+             part_w, ptr(set_slot), ptr(soff), nq, total, ptr(narrow), s)
+        ps, ps_ctas = None, 0
+        if parts > 1:
+            ps_ctas = self.n_ctas if self.n_ctas > 0 else \
+                torch.cuda.get_device_properties(dev).multi_processor_count
+            nfl = self.lib.rspi_quad4_part_sums_floats(nq, ps_ctas)
+            ps = torch.empty(nfl, dtype=torch.float32, device=dev)
+        return dict(entries=narrow, group_off=soff, total_groups=total, tile=4, banked=True,
+                    narrow=True, pairs=True, frames_per=4, quad4=True, pair_frames=set_frames,
+                    n_pairs=nq, frame_groups=sng.amax(1)[(set_slot // 4).long()],
+                    n_parts=parts, part_w=part_w, part_sums=ps, part_sums_ctas=ps_ctas)
+
     def _wide_entries(self):
         """32-bit entries holding each photon's byte offset in the
         interleaved tile (sel * 4 * tile), four rows of a lane per 16-byte
         group, rows of a frame padded to a multiple of four."""
         if self.kernel in ('pair', 'quad'):
             return self._pair_entries()
+        if self.kernel == 'quad4':
+            return self._quad4_entries()
         l16, n, dev, s = self.ll16, self.ph.num_data, self.device, cur_stream()
         groups = torch.empty(n, dtype=_i32, device=dev)
         bt, pz = self._wide_bytes_tile(), self.p_row - 32
@@ -494,7 +561,7 @@ class EStep:
         if key != self._eps_key:
             ro = self.ll16['row_off']
             rows = ro[1:] - ro[:-1]
-            if self.kernel in ('pair', 'quad') and self.wide is not None and \
+            if self.kernel in ('pair', 'quad', 'quad4') and self.wide is not None and \
                     self.wide.get('pairs'):
                 rows = torch.maximum(rows, self.wide['frame_groups'].to(_i64))
             elif self.kernel in ('wide', 'wide16') and self.wide is not None and \
@@ -599,9 +666,19 @@ class EStep:
             call('rspi_screen_loglike4h', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
                  ptr(self.ph.scales), ptr(self.wide['entries']), ptr(self.wide['group_off']), n,
                  r0, r1, ptr(self.prob[r0]), n, self.warps, self.n_ctas, cur_stream())
+        elif self.kernel == 'quad4' and self.form == 'screen':
+            w = self.wide
+            if w is None or not w.get('quad4') or (w['n_parts'] > 1 and self.n_ctas > 0 and
+                                                    self.n_ctas != w['part_sums_ctas']):
+                w = self.wide = self._quad4_entries()
+            call('rspi_screen_loglike7', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
+                 ptr(self.ph.scales), ptr(w['entries']), ptr(w['group_off']),
+                 ptr(w['pair_frames']), w['n_pairs'], w['n_parts'], w['part_w'], r0, r1,
+                 ptr(self.prob[r0]), n, ptr(w['part_sums']), w['part_sums_ctas'], self.warps,
+                 self.n_ctas, cur_stream())
         elif self.kernel in ('pair', 'quad') and self.form == 'screen':
             nf = 4 if self.kernel == 'quad' else 2
-            if self.wide is None or self.wide.get('frames_per') != nf:
+            if self.wide is None or self.wide.get('frames_per') != nf or self.wide.get('quad4'):
                 self.wide = self._pair_entries()
             call('rspi_screen_loglike6' if nf == 4 else 'rspi_screen_loglike5', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
                  ptr(self.ph.scales), ptr(self.wide['entries']), ptr(self.wide['group_off']),

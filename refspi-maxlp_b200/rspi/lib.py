@@ -44,6 +44,10 @@ SIGNATURES = {
     'rspi_quad_entry_groups': (I, [P, P, L, I, P, P]),
     'rspi_quad_entry_fill': (I, [P, P, L, I, P, P, L, P, P]),
     'rspi_screen_loglike6': (I, [P, L, L, P, P, P, P, P, L, L, L, P, L, I, I, P]),
+    'rspi_quad4_entry_groups': (I, [P, P, L, I, I, I, P, P]),
+    'rspi_quad4_entry_fill': (I, [P, P, L, I, I, I, P, P, L, L, P, P]),
+    'rspi_quad4_part_sums_floats': (L, [L, I]),
+    'rspi_screen_loglike7': (I, [P, L, L, P, P, P, P, P, L, I, I, L, L, P, L, P, I, I, I, P]),
     'rspi_mean': (I, [P, L, P, P]),
     'rspi_ll16_entry_rows': (I, [P] * 8 + [L, L, I, P, P, P]),
     'rspi_ll16_entry_fill': (I, [P] * 8 + [L, L, I, P, P, P]),
@@ -121,7 +125,8 @@ KERNELS_PER_CALL = {
     'rspi_maxlp_pixel_frames': 1, 'rspi_maxlp_pixel_values': 1, 'rspi_maxlp_fcalc': 1,
     'rspi_sphere_ramp': 1, 'rspi_pair_entry_groups': 1, 'rspi_pair_entry_fill': 2,
     'rspi_screen_loglike5': 1, 'rspi_quad_entry_groups': 1, 'rspi_quad_entry_fill': 2,
-    'rspi_screen_loglike6': 1,
+    'rspi_screen_loglike6': 1, 'rspi_quad4_entry_groups': 1, 'rspi_quad4_entry_fill': 2,
+    'rspi_screen_loglike7': 1, 'rspi_quad4_part_sums_floats': 0,
     'rspi_mean': 1, 'rspi_ll16_entry_rows': 1, 'rspi_ll16_entry_fill': 1,
     'rspi_screen_loglike': 1, 'rspi_screen_candidates': 3, 'rspi_rescore': 5,
     'rspi_loglike_stream': 1, 'rspi_posterior_pairs': 3, 'rspi_screen_loglike2': 1,

@@ -63,7 +63,7 @@ def test_bindings_match_header_argument_counts():
     with open(os.path.join(REPO, 'include', 'rspi.h')) as f:
         h = re.sub(r'/\*.*?\*/', '', f.read(), flags=re.S)
     seen = 0
-    for m in re.finditer(r'\b(?:int|const char \*)\s*(rspi_\w+)\s*\(([^)]*)\)\s*;', h):
+    for m in re.finditer(r'\b(?:int|long long|const char \*)\s*(rspi_\w+)\s*\(([^)]*)\)\s*;', h):
         name, args = m.group(1), m.group(2).strip()
         n = 0 if args in ('', 'void') else len(args.split(','))
         assert name in SIGNATURES, name

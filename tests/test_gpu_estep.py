@@ -502,3 +502,101 @@ def test_quad_layout_entries(n):
             assert np.array_equal(part[pads], want[pads])
     assert sorted(seen) == list(range(n))
     assert np.all(qf[:n] // PAIR_WINDOW == np.arange(n) // PAIR_WINDOW)
+
+
+@pytest.mark.parametrize('parts,warps', [(None, 32), (2, 24), (3, 7), (4, 32)])
+@pytest.mark.parametrize('name,ds,need_scaling', CASES, ids=[c[0] for c in CASES])
+def test_quad4_kernel_matches_stream_kernel(name, ds, need_scaling, parts, warps):
+    """The four-row frame-quad kernel (column parts staged one after
+    another, running sums per frame slot between parts) gives the
+    interleaved kernel's FP32 likelihoods within 1e-6 of the largest term,
+    and the same FP64-rescored argmax / maximum / log-sum-exp, on every case
+    (empty, heavy and single-frame data included)."""
+    size = int(round(np.sqrt(ds['num_pix'])))
+    num_rot = 5
+    sx, sy, dia, _ = E.generate_states(E.parse_triple('-1 1 3'), E.parse_triple('0 0 1'),
+                                       E.parse_triple('2 3 2'))
+    rng = np.random.default_rng(size)
+    model = torch.from_numpy(rng.random(size * size) + 1j * rng.random(size * size)).cuda()
+    out = {}
+    for kernel, tile, kw in (('stream', 2, {}), ('quad4', 4, dict(screen_parts=parts))):
+        ph = _photons(ds, need_scaling)
+        es = _estep(ph, size, num_rot, sx, sy, dia, ds['bg'], form='screen', kernel=kernel,
+                    states_per_tile=tile, warps=warps, **kw)
+        es.run(model)
+        maxll, rmax, logz = es.reduce()
+        torch.cuda.synchronize()
+        out[kernel] = (es.prob.cpu().numpy().astype(np.float64), maxll.cpu().numpy(),
+                       rmax.cpu().numpy(), logz.cpu().numpy())
+        if kernel == 'quad4':
+            assert es.wide['n_parts'] == (parts or 1)
+    a, b = out['stream'], out['quad4']
+    scale = np.abs(a[0]).max(0, keepdims=True) + 1.
+    assert np.all(np.abs(a[0] - b[0]) <= 1e-6 * scale)
+    assert np.array_equal(a[2], b[2])
+    np.testing.assert_allclose(a[1], b[1], rtol=1e-14)
+    np.testing.assert_allclose(a[3], b[3], rtol=1e-12)
+
+
+@pytest.mark.parametrize('n,parts', [(61, 1), (300, 2), (45, 3)])
+def test_quad4_layout_entries(n, parts):
+    """Four-row frame quads: every frame's photons once per column part, in
+    its eight lanes, lane j holding local columns = j (mod 8) as q = local / 8;
+    the pad q = part_w / 8 (zero columns) elsewhere; group ranges part-major
+    with each (quad, part) as long as its longest frame needs; frames taken
+    within windows of consecutive frames."""
+    from rspi.device import PAIR_WINDOW
+    size = 37
+    d = random_photons(size, n, 40. * size, 14, empty_frames=(2, 9), heavy=5)
+    ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
+                         d['count_multi'], size * size, False)
+    sx, sy, dia, _ = E.generate_states(E.parse_triple('0 0 1'), E.parse_triple('0 0 1'),
+                                       E.parse_triple('2 2 1'))
+    es_q = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen',
+                  kernel='quad4', states_per_tile=4, screen_parts=parts)
+    es_w = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen',
+                  kernel='wide', states_per_tile=2, narrow_entries=False)
+    torch.cuda.synchronize()
+    w = es_q.wide
+    pz = es_q.p_row - 32
+    pw, nq = w['part_w'], w['n_pairs']
+    assert w['n_parts'] == parts and pw % 8 == 0 and parts * pw >= pz
+    q = w['entries'].cpu().numpy().view(np.uint16).reshape(-1, 32, 4).astype(np.int64)
+    j = (np.arange(32) % 8)[None, :, None]
+    local = q * 8 + j                                          # local column of each slot
+    goff = w['group_off'].cpu().numpy()
+    qf = w['pair_frames'].cpu().numpy()
+    assert nq == (n + 3) // 4 and goff.size == parts * nq + 1 and np.all(np.diff(goff) >= 0)
+    wide = es_w.wide['entries'].cpu().numpy().view(np.uint32).reshape(-1, 32, 4) // 8
+    woff = es_w.wide['group_off'].cpu().numpy()
+    seen = []
+    for qd in range(nq):
+        for uu in range(4):
+            f = qf[4 * qd + uu]
+            got = []
+            for h in range(parts):
+                blk = local[goff[h * nq + qd]:goff[h * nq + qd + 1], 8 * uu:8 * uu + 8]
+                real = blk < pw
+                assert np.all(blk[~real] == pw + np.broadcast_to(np.arange(8)[None, :, None],
+                                                                blk.shape)[~real])
+                if f < 0:
+                    assert not real.any()
+                got.append(blk[real] + h * pw)
+            if f < 0:
+                continue
+            seen.append(f)
+            ref = wide[woff[f]:woff[f + 1]]
+            assert np.array_equal(np.sort(np.concatenate(got)), np.sort(ref[ref < pz])), f
+    assert sorted(seen) == list(range(n))
+    assert np.all(qf[:n] // PAIR_WINDOW == np.arange(n) // PAIR_WINDOW)
+    # each (quad, part) range is as long as its longest frame needs
+    for h in range(parts):
+        for qd in range(nq):
+            fr = [f for f in qf[4 * qd:4 * qd + 4] if f >= 0]
+            need = 0
+            for f in fr:
+                ref = wide[woff[f]:woff[f + 1]]
+                cols = ref[(ref < pz) & (ref // pw == h)] % pw
+                if cols.size:
+                    need = max(need, -(-np.bincount(cols % 8, minlength=8).max() // 4))
+            assert goff[h * nq + qd + 1] - goff[h * nq + qd] == need

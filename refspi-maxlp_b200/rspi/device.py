@@ -26,6 +26,7 @@ INT32_MAX = 2 ** 31 - 1
 PAIR_WINDOW = 256   # frames sorted by length for pairing within such windows
 QUAD4_SMEM = 227 * 1024 - 1024   # shared bytes of the four-row tile (kernel limit)
 QUAD4_MAX_PARTS = 4              # column parts of the four-row tile
+QUAD4_COLS = (QUAD4_SMEM // 16 - 8) // 8 * 8   # most columns of one part
 
 
 def ptr(t):
@@ -226,7 +227,7 @@ class EStep:
             raise ValueError('form must be fp64, screen or dense')
         auto_kernel = kernel is None
         if kernel is None:   # default likelihood kernel of each form (the screened
-            # form's frame-quad kernel is chosen below when a two-row tile fits)
+            # form's four-row frame-quad kernel is chosen below)
             kernel = 'wide' if form == 'screen' else 'stream'
         if screen_slices not in ('fp32', 'fp16'):
             raise ValueError('screen_slices must be fp32 or fp16')
@@ -277,9 +278,11 @@ class EStep:
         self.slice_torch = {0: torch.float32, 1: _f64, 2: torch.float16}[self.slice_code]
         self.prob_torch = torch.float32 if self.prob_code == 0 else _f64
         tmax = self.lib.rspi_loglike_max_tile(self.p_row, self.slice_code)
-        if auto_kernel and form == 'screen' and kernel == 'wide' and tmax >= 2 and \
-                states_per_tile in (None, 2):
-            kernel = self.kernel = 'quad'
+        if auto_kernel and form == 'screen' and kernel == 'wide':
+            if states_per_tile in (None, 4) and self.p_row - 32 <= QUAD4_MAX_PARTS * QUAD4_COLS:
+                kernel = self.kernel = 'quad4'
+            elif tmax >= 2 and states_per_tile in (None, 2):
+                kernel = self.kernel = 'quad'
         if kernel == 'wide16':
             tmax = 4 if self.p_row * 8 <= 226 * 1024 else 0
         if form == 'screen' and kernel == 'stream':
@@ -464,8 +467,7 @@ class EStep:
         """(parts, columns per part) of the four-row tile: the fewest column
         parts whose four FP32 rows (16 bytes a column, plus 8 zero columns)
         fit in shared memory, or ``screen_parts`` parts."""
-        pz = self.p_row - 32
-        cap = (QUAD4_SMEM // 16 - 8) // 8 * 8
+        pz, cap = self.p_row - 32, QUAD4_COLS
         parts = self.screen_parts or max(1, -(-pz // cap))
         part_w = max(8, (-(-pz // parts) + 7) // 8 * 8)
         if parts > QUAD4_MAX_PARTS or part_w > cap:

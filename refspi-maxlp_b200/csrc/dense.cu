@@ -370,7 +370,7 @@ __global__ void k_dense_frames(const unsigned short *__restrict__ frames, long l
 }
 
 // Rotated log-slices split into BF16 hi + lo parts (same values as
-// k_rot_log: rot_log_value in FP64), zero beyond n_sel.
+// k_rot_log_js: rot_log_value in FP64), zero beyond n_sel.
 __global__ void __launch_bounds__(256)
 k_rot_log_split(const double *__restrict__ holo, long long num_rot,
                 const double *__restrict__ rot_cs, int size, const double *__restrict__ bg,

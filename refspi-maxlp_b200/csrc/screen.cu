@@ -363,7 +363,7 @@ __global__ void k_row_scatter(const int *__restrict__ cand_r, const long long *_
 }
 
 // One CTA per likelihood row with candidates: the row's FP64 rotated slice
-// is computed into shared memory with rot_log_value (as k_rot_log does),
+// is computed into shared memory with rot_log_value (as k_rot_log_js does),
 // then each warp rescores candidate frames exactly as the FP64 form sums
 // them (per lane over the frame's packed rows, fma(count, L, acc), then the
 // warp reduction), so every value equals the FP64 form's.  A row longer than

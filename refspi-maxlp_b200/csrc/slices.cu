@@ -89,40 +89,79 @@ k_vscale_init(const double *__restrict__ msum, long long n_states0,
     for (long long s = threadIdx.x; s < n_states0; s += blockDim.x) init[s] = -(msum[s] * vs);
 }
 
-// One CTA per likelihood row (grid-stride over rows): the row's state,
-// rotation and slice pointer are computed once, the threads walk the row's
-// columns; no per-element 64-bit division.
+// Rotated log-slices (row s0 * num_rot + j of every state s0 and rotation
+// j; zeros past n_sel), rotation-major: a CTA takes one rotation j and up to
+// RL_STATES consecutive states.  The rotated position of each likelihood
+// column (pixel row/column, the FP64 rotation, floors and the in-detector
+// test) depends on (j, column) only, so it is computed once per column and
+// reused for every state; each state then costs its four bilinear loads,
+// the same FP64 interpolation and log as rot_log_value (identical values)
+// and one store.
+constexpr int RL_STATES = 8;
+
 template <typename TL>
 __global__ void __launch_bounds__(256)
-k_rot_log(const double *__restrict__ holo, long long num_rot, const double *__restrict__ rot_cs,
-          int size, const double *__restrict__ bg, const int *__restrict__ sel_pix,
-          long long n_sel, long long p_pad, long long row_begin, long long n_rows,
-          TL *__restrict__ out, float *__restrict__ abs_max) {
+k_rot_log_js(const double *__restrict__ holo, int num_rot, const double *__restrict__ rot_cs,
+             int size, const double *__restrict__ bg, const int *__restrict__ sel_pix, int n_sel,
+             int p_pad, long long row_begin, long long row_end, long long s_lo, int n_groups,
+             TL *__restrict__ out, float *__restrict__ abs_max) {
+    const int j = (int)(blockIdx.x % (unsigned)num_rot);
+    const long long s_first = s_lo + (long long)(blockIdx.x / (unsigned)num_rot) * RL_STATES;
     const long long npix = (long long)size * size;
-    const int ns = (int)n_sel, pp = (int)p_pad;
-    float amax = 0.f;
+    const double ac = rot_cs[2 * j], as = rot_cs[2 * j + 1];
+    const int cen = size / 2;
     const float inv_size = 1.f / (float)size;
-    for (long long rr = blockIdx.x; rr < n_rows; rr += gridDim.x) {
-        const long long r = row_begin + rr;
-        const long long s0 = r / num_rot, j = r - s0 * num_rot;
-        const double ac = rot_cs[2 * j], as = rot_cs[2 * j + 1];
-        const double *w = holo + s0 * npix;
-        TL *o = out + rr * p_pad;
-        for (int c = threadIdx.x; c < pp; c += blockDim.x) {
-            double v = 0.;
-            if (c < ns) {
+    // this CTA's states whose row s0 * num_rot + j lies in [row_begin, row_end)
+    long long sb = s_first, se = s_first + RL_STATES;
+    while (sb < se && sb * num_rot + j < row_begin) ++sb;
+    while (se > sb && (se - 1) * num_rot + j >= row_end) --se;
+    float amax = 0.f;
+    if (sb < se) {
+        for (int c = threadIdx.x; c < p_pad; c += blockDim.x) {
+            bool in = false;
+            long long base = 0;
+            double fx = 0., fy = 0., cx = 0., cy = 0., b = 0.;
+            if (c < n_sel) {
                 const int p = sel_pix[c];
                 int x, y;
                 pixel_xy(p, size, inv_size, x, y);
-                v = rot_log_value(w, x, y, size, ac, as, bg[p]);
+                const double xc = (double)(x - cen), yc = (double)(y - cen);
+                const double tx = xadd(xsub(xmul(xc, ac), xmul(yc, as)), (double)cen);
+                const double ty = xadd(xadd(xmul(xc, as), xmul(yc, ac)), (double)cen);
+                const double fxl = floor(tx), fyl = floor(ty);
+                in = !(fxl < 0. || fxl > size - 2 || fyl < 0. || fyl > size - 2);
+                if (in) {
+                    base = (long long)(int)fxl * size + (int)fyl;
+                    fx = tx - fxl;
+                    fy = ty - fyl;
+                    cx = 1. - fx;
+                    cy = 1. - fy;
+                }
+                b = bg[p];
             }
-            const TL q = static_cast<TL>(v);
-            o[c] = q;
-            amax = fmaxf(amax, fabsf(static_cast<float>(q)));
+            for (long long s0 = sb; s0 < se; ++s0) {
+                double v = 0.;
+                if (c < n_sel) {
+                    if (in) {
+                        const double *r0 = holo + s0 * npix + base;
+                        const double *r1 = r0 + size;
+                        double t = xmul(xmul(r0[0], cx), cy);
+                        t = xadd(t, xmul(xmul(r1[0], fx), cy));
+                        t = xadd(t, xmul(xmul(r0[1], cx), fy));
+                        t = xadd(t, xmul(xmul(r1[1], fx), fy));
+                        t = xadd(t, b);
+                        v = t < 1.e-20 ? -1000. : log(t);
+                    } else {
+                        v = -1000.;
+                    }
+                }
+                const TL q = static_cast<TL>(v);
+                out[(s0 * num_rot + j - row_begin) * (long long)p_pad + c] = q;
+                amax = fmaxf(amax, fabsf(static_cast<float>(q)));
+            }
         }
     }
     if (abs_max) {
-        // non-negative floats order like their bit patterns
         amax = __int_as_float(warp_max_int(__float_as_int(amax)));
         if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int *>(abs_max), __float_as_int(amax));
     }
@@ -161,19 +200,24 @@ extern "C" int rspi_rot_log_slices(const double *holo, long long n_states0, long
         return RSPI_ERR_ARG;
     const long long n_rows = row_end - row_begin;
     if (n_rows == 0) return RSPI_OK;
-    const unsigned blocks = (unsigned)std::min<long long>(n_rows, (long long)rspi_sm_count() * 64);
+    // rotation-major CTAs: one rotation, RL_STATES consecutive states
+    const long long s_lo = row_begin / num_rot, s_hi = (row_end - 1) / num_rot;
+    const long long n_groups = (s_hi - s_lo) / RL_STATES + 1;
+    if (n_groups * num_rot > 0x7fffffffLL || p_pad > 0x7fffffffLL || n_sel > p_pad)
+        return RSPI_ERR_ARG;
+    const unsigned blocks = (unsigned)(n_groups * num_rot);
     if (out_dtype == 0)
-        k_rot_log<float><<<blocks, 256, 0, stream>>>(holo, num_rot, rot_cs, (int)size, bg, sel_pix,
-                                                     n_sel, p_pad, row_begin, n_rows,
-                                                     (float *)lslices, abs_max);
+        k_rot_log_js<float><<<blocks, 256, 0, stream>>>(
+            holo, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, (int)p_pad,
+            row_begin, row_end, s_lo, (int)n_groups, (float *)lslices, abs_max);
     else if (out_dtype == 2)
-        k_rot_log<__half><<<blocks, 256, 0, stream>>>(holo, num_rot, rot_cs, (int)size, bg,
-                                                      sel_pix, n_sel, p_pad, row_begin, n_rows,
-                                                      (__half *)lslices, abs_max);
+        k_rot_log_js<__half><<<blocks, 256, 0, stream>>>(
+            holo, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, (int)p_pad,
+            row_begin, row_end, s_lo, (int)n_groups, (__half *)lslices, abs_max);
     else if (out_dtype == 1)
-        k_rot_log<double><<<blocks, 256, 0, stream>>>(holo, num_rot, rot_cs, (int)size, bg,
-                                                      sel_pix, n_sel, p_pad, row_begin, n_rows,
-                                                      (double *)lslices, abs_max);
+        k_rot_log_js<double><<<blocks, 256, 0, stream>>>(
+            holo, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, (int)p_pad,
+            row_begin, row_end, s_lo, (int)n_groups, (double *)lslices, abs_max);
     else
         return RSPI_ERR_ARG;
     RSPI_RETURN_LAUNCH();

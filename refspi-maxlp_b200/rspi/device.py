@@ -29,6 +29,21 @@ QUAD4_MAX_PARTS = 4              # column parts of the four-row tile
 QUAD4_COLS = (QUAD4_SMEM // 16 - 8) // 8 * 8   # most columns of one part
 
 
+def quad4_parts(p_row, parts=None):
+    """(parts, columns per part) of the four-row frame-quad tile for a slice
+    row of ``p_row`` columns (the last 32 zero): the fewest parts (or
+    ``parts``) of a multiple of 8 columns covering the ``p_row - 32``
+    likelihood columns whose four FP32 rows, 16 bytes a column plus 8 zero
+    columns, fit the kernel's shared memory."""
+    pz = int(p_row) - 32
+    parts = int(parts) if parts else max(1, -(-pz // QUAD4_COLS))
+    part_w = max(8, (-(-pz // parts) + 7) // 8 * 8)
+    if parts < 1 or parts > QUAD4_MAX_PARTS or part_w > QUAD4_COLS:
+        raise ValueError('%d likelihood columns need more than %d column parts of the '
+                         'four-row tile' % (pz, QUAD4_MAX_PARTS))
+    return parts, part_w
+
+
 def ptr(t):
     return ctypes.c_void_p(0 if t is None else t.data_ptr())
 
@@ -464,16 +479,9 @@ class EStep:
                     n_pairs=n_sets, frame_groups=sng[(set_slot // nf).long()])
 
     def _quad4_parts(self):
-        """(parts, columns per part) of the four-row tile: the fewest column
-        parts whose four FP32 rows (16 bytes a column, plus 8 zero columns)
-        fit in shared memory, or ``screen_parts`` parts."""
-        pz, cap = self.p_row - 32, QUAD4_COLS
-        parts = self.screen_parts or max(1, -(-pz // cap))
-        part_w = max(8, (-(-pz // parts) + 7) // 8 * 8)
-        if parts > QUAD4_MAX_PARTS or part_w > cap:
-            raise ValueError('%d likelihood pixels need more than %d column parts of the '
-                             'four-row tile' % (self.n_sel, QUAD4_MAX_PARTS))
-        return parts, part_w
+        """Column parts of the four-row tile (``quad4_parts``), or
+        ``screen_parts`` parts."""
+        return quad4_parts(self.p_row, self.screen_parts)
 
     def _quad4_entries(self):
         """Entries of the four-row frame-quad kernel: frames ordered and taken

@@ -127,6 +127,20 @@ int rspi_rot_log_slices(const double *holo, long long n_states0, long long num_r
                         long long row_begin, long long row_end, void *lslices,
                         int out_dtype, float *abs_max, cudaStream_t stream);
 
+/* The same slices from a paired copy of the holographic slices:
+ * rspi_holo_pairs writes holo_pairs[2 i], holo_pairs[2 i + 1] = holo[i],
+ * holo[i + 1] (0 past the end; 16-byte aligned, 2 * n_states0 * size^2
+ * doubles), so each row of a bilinear 2 x 2 neighbourhood is one 16-byte
+ * load; rspi_rot_log_slices_pairs takes it in place of holo and gives
+ * bit-identical output. */
+int rspi_holo_pairs(const double *holo, long long n_states0, long long size,
+                    double *holo_pairs, cudaStream_t stream);
+int rspi_rot_log_slices_pairs(const double *holo_pairs, long long n_states0, long long num_rot,
+                              const double *rot_cs, long long size, const double *bg,
+                              const int *sel_pix, long long n_sel, long long p_pad,
+                              long long row_begin, long long row_end, void *lslices,
+                              int out_dtype, float *abs_max, cudaStream_t stream);
+
 /* ------------------------------------------------------------------------ a7
  * Log-likelihood of frames x states, replacing calc_prob_all
  * (kernels.cu:116-137) launched once per (state, rotation) at emc.py:194-199:

@@ -96,12 +96,24 @@ k_vscale_init(const double *__restrict__ msum, long long n_states0,
 // test) depends on (j, column) only, so it is computed once per column and
 // reused for every state; each state then costs its four bilinear loads,
 // the same FP64 interpolation and log as rot_log_value (identical values)
-// and one store.
+// and one store.  With PAIRS the four neighbours come as two 16-byte loads
+// from the paired copy hp[p] = (w[p], w[p + 1]) of the holographic slices.
 constexpr int RL_STATES = 8;
 
-template <typename TL>
+// hp[i] = (holo[i], holo[i + 1]) over the whole state-major array (0 past
+// its end); only pairs of a pixel and its right neighbour in the same row
+// are read.
+__global__ void k_holo_pairs(const double *__restrict__ holo, long long total,
+                             double2 *__restrict__ hp) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
+        hp[i] = make_double2(holo[i], i + 1 < total ? holo[i + 1] : 0.);
+}
+
+template <typename TL, bool PAIRS>
 __global__ void __launch_bounds__(256)
-k_rot_log_js(const double *__restrict__ holo, int num_rot, const double *__restrict__ rot_cs,
+k_rot_log_js(const double *__restrict__ holo, const double2 *__restrict__ hp, int num_rot,
+             const double *__restrict__ rot_cs,
              int size, const double *__restrict__ bg, const int *__restrict__ sel_pix, int n_sel,
              int p_pad, long long row_begin, long long row_end, long long s_lo, int n_groups,
              TL *__restrict__ out, float *__restrict__ abs_max) {
@@ -143,12 +155,24 @@ k_rot_log_js(const double *__restrict__ holo, int num_rot, const double *__restr
                 double v = 0.;
                 if (c < n_sel) {
                     if (in) {
-                        const double *r0 = holo + s0 * npix + base;
-                        const double *r1 = r0 + size;
-                        double t = xmul(xmul(r0[0], cx), cy);
-                        t = xadd(t, xmul(xmul(r1[0], fx), cy));
-                        t = xadd(t, xmul(xmul(r0[1], cx), fy));
-                        t = xadd(t, xmul(xmul(r1[1], fx), fy));
+                        double w00, w01, w10, w11;   // w[ix + a][iy + b] as w_ab
+                        if constexpr (PAIRS) {
+                            const double2 a = hp[s0 * npix + base], b2 = hp[s0 * npix + base + size];
+                            w00 = a.x;
+                            w01 = a.y;
+                            w10 = b2.x;
+                            w11 = b2.y;
+                        } else {
+                            const double *r0 = holo + s0 * npix + base;
+                            w00 = r0[0];
+                            w01 = r0[1];
+                            w10 = r0[size];
+                            w11 = r0[size + 1];
+                        }
+                        double t = xmul(xmul(w00, cx), cy);
+                        t = xadd(t, xmul(xmul(w10, fx), cy));
+                        t = xadd(t, xmul(xmul(w01, cx), fy));
+                        t = xadd(t, xmul(xmul(w11, fx), fy));
                         t = xadd(t, b);
                         v = t < 1.e-20 ? -1000. : log(t);
                     } else {
@@ -189,15 +213,17 @@ extern "C" int rspi_vscale_init(const double *msum, long long n_states0, const d
     RSPI_RETURN_LAUNCH();
 }
 
-extern "C" int rspi_rot_log_slices(const double *holo, long long n_states0, long long num_rot,
-                                   const double *rot_cs, long long size, const double *bg,
-                                   const int *sel_pix, long long n_sel, long long p_pad,
-                                   long long row_begin, long long row_end, void *lslices,
-                                   int out_dtype, float *abs_max, cudaStream_t stream) {
+template <bool PAIRS>
+static int rot_log_launch(const double *holo, const double2 *hp, long long n_states0,
+                          long long num_rot, const double *rot_cs, long long size,
+                          const double *bg, const int *sel_pix, long long n_sel, long long p_pad,
+                          long long row_begin, long long row_end, void *lslices, int out_dtype,
+                          float *abs_max, cudaStream_t stream) {
     if (n_states0 <= 0 || num_rot <= 0 || size <= 1 || size > 46340 || p_pad < n_sel ||
         p_pad % 32 || row_begin < 0 || row_end > n_states0 * num_rot || row_end < row_begin ||
-        !holo || !rot_cs || !bg || !lslices)
+        !(PAIRS ? (const void *)hp : (const void *)holo) || !rot_cs || !bg || !lslices)
         return RSPI_ERR_ARG;
+    if (PAIRS && (reinterpret_cast<uintptr_t>(hp) & 15) != 0) return RSPI_ERR_ARG;
     const long long n_rows = row_end - row_begin;
     if (n_rows == 0) return RSPI_OK;
     // rotation-major CTAs: one rotation, RL_STATES consecutive states
@@ -207,20 +233,52 @@ extern "C" int rspi_rot_log_slices(const double *holo, long long n_states0, long
         return RSPI_ERR_ARG;
     const unsigned blocks = (unsigned)(n_groups * num_rot);
     if (out_dtype == 0)
-        k_rot_log_js<float><<<blocks, 256, 0, stream>>>(
-            holo, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, (int)p_pad,
+        k_rot_log_js<float, PAIRS><<<blocks, 256, 0, stream>>>(
+            holo, hp, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, (int)p_pad,
             row_begin, row_end, s_lo, (int)n_groups, (float *)lslices, abs_max);
     else if (out_dtype == 2)
-        k_rot_log_js<__half><<<blocks, 256, 0, stream>>>(
-            holo, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, (int)p_pad,
+        k_rot_log_js<__half, PAIRS><<<blocks, 256, 0, stream>>>(
+            holo, hp, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, (int)p_pad,
             row_begin, row_end, s_lo, (int)n_groups, (__half *)lslices, abs_max);
     else if (out_dtype == 1)
-        k_rot_log_js<double><<<blocks, 256, 0, stream>>>(
-            holo, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, (int)p_pad,
+        k_rot_log_js<double, PAIRS><<<blocks, 256, 0, stream>>>(
+            holo, hp, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, (int)p_pad,
             row_begin, row_end, s_lo, (int)n_groups, (double *)lslices, abs_max);
     else
         return RSPI_ERR_ARG;
     RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_rot_log_slices(const double *holo, long long n_states0, long long num_rot,
+                                   const double *rot_cs, long long size, const double *bg,
+                                   const int *sel_pix, long long n_sel, long long p_pad,
+                                   long long row_begin, long long row_end, void *lslices,
+                                   int out_dtype, float *abs_max, cudaStream_t stream) {
+    return rot_log_launch<false>(holo, nullptr, n_states0, num_rot, rot_cs, size, bg, sel_pix,
+                                 n_sel, p_pad, row_begin, row_end, lslices, out_dtype, abs_max,
+                                 stream);
+}
+
+extern "C" int rspi_holo_pairs(const double *holo, long long n_states0, long long size,
+                               double *holo_pairs, cudaStream_t stream) {
+    if (!holo || !holo_pairs || n_states0 <= 0 || size <= 1 || size > 46340 ||
+        (reinterpret_cast<uintptr_t>(holo_pairs) & 15) != 0)
+        return RSPI_ERR_ARG;
+    const long long total = n_states0 * size * size;
+    k_holo_pairs<<<rspi_blocks(total, 256), 256, 0, stream>>>(
+        holo, total, reinterpret_cast<double2 *>(holo_pairs));
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_rot_log_slices_pairs(const double *holo_pairs, long long n_states0,
+                                         long long num_rot, const double *rot_cs, long long size,
+                                         const double *bg, const int *sel_pix, long long n_sel,
+                                         long long p_pad, long long row_begin, long long row_end,
+                                         void *lslices, int out_dtype, float *abs_max,
+                                         cudaStream_t stream) {
+    return rot_log_launch<true>(nullptr, reinterpret_cast<const double2 *>(holo_pairs),
+                                n_states0, num_rot, rot_cs, size, bg, sel_pix, n_sel, p_pad,
+                                row_begin, row_end, lslices, out_dtype, abs_max, stream);
 }
 
 extern "C" int rspi_sphere_ramp(long long size, double sx, double sy, double dia, double *sphere,

@@ -339,6 +339,9 @@ class EStep:
         rows = max(self.tile, (slice_budget_bytes // (self.p_row * esz)) // self.tile * self.tile)
         self.chunk_rows = int(min(self.n_rows, rows))
         self.holo = torch.empty((self.n_states0, self.size ** 2), dtype=_f64, device=dev)
+        # (w[p], w[p + 1]) pairs: the slice kernel's bilinear rows as 16-byte loads
+        self.holo_pairs = torch.empty((self.n_states0, self.size ** 2, 2), dtype=_f64,
+                                      device=dev)
         self.msum = torch.empty(self.n_states0, dtype=_f64, device=dev)
         self.vscale = torch.empty(1, dtype=_f64, device=dev)
         self.init = torch.empty(self.n_states0, dtype=_f64, device=dev)
@@ -619,6 +622,9 @@ class EStep:
                  self.n_sel, ptr(self.holo[g0]), ptr(self.msum[g0:]), s)
         call('rspi_vscale_init', ptr(self.msum), self.n_states0, ptr(self.ph.powder),
              ptr(self.sel_pix), self.n_sel, ptr(self.vscale), ptr(self.init), s)
+        if self.form != 'dense':
+            call('rspi_holo_pairs', ptr(self.holo), self.n_states0, self.size,
+                 ptr(self.holo_pairs), s)
         if self.form != 'fp64':
             # the FP16 bound needs |L| >= 2^-14 (below it the absolute error
             # 2^-25 is covered by 2^-11 * 2^-14)
@@ -642,7 +648,7 @@ class EStep:
                  cur_stream())
             return self.lsl_hi
         out = self.lsl if out is None else out
-        call('rspi_rot_log_slices', ptr(self.holo), self.n_states0, self.num_rot,
+        call('rspi_rot_log_slices_pairs', ptr(self.holo_pairs), self.n_states0, self.num_rot,
              ptr(self.rot_cs), self.size, ptr(self.bg), ptr(self.sel_pix), self.n_sel,
              self.p_row, r0, r1, ptr(out), self.slice_code,
              ptr(self.lmax) if self.form == 'screen' else None, cur_stream())

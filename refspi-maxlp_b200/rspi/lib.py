@@ -26,6 +26,8 @@ SIGNATURES = {
     'rspi_holo_slices': (I, [P, P, P, P, L, L, P, P, L, P, P, P]),
     'rspi_vscale_init': (I, [P, L, P, P, L, P, P, P]),
     'rspi_rot_log_slices': (I, [P, L, L, P, L, P, P, L, L, L, L, P, I, P, P]),
+    'rspi_holo_pairs': (I, [P, L, L, P, P]),
+    'rspi_rot_log_slices_pairs': (I, [P, L, L, P, L, P, P, L, L, L, L, P, I, P, P]),
     'rspi_loglike': (I, [P, I, L, L, P, P, P, P, P, L, L, L, P, I, L, I, I, I, P]),
     'rspi_loglike_max_tile': (I, [L, I]),
     'rspi_frame_reduce': (I, [P, I, L, L, P, P, P, P]),
@@ -119,7 +121,8 @@ def check(code, what):
 KERNELS_PER_CALL = {
     'rspi_photon_offsets': 4, 'rspi_powder': 2, 'rspi_ll_entry_rows': 1, 'rspi_scan_rows': 1,
     'rspi_ll_entry_fill': 1, 'rspi_holo_slices': 1, 'rspi_vscale_init': 1,
-    'rspi_rot_log_slices': 1, 'rspi_loglike': 1, 'rspi_frame_reduce': 1,
+    'rspi_rot_log_slices': 1, 'rspi_holo_pairs': 1, 'rspi_rot_log_slices_pairs': 1,
+    'rspi_loglike': 1, 'rspi_frame_reduce': 1,
     'rspi_maxlp_frame_params': 1, 'rspi_maxlp_histogram': 1, 'rspi_maxlp_pattern': 1,
     'rspi_maxlp_pattern_screened': 1, 'rspi_log2_error_max': 1,
     'rspi_maxlp_pixel_frames': 1, 'rspi_maxlp_pixel_values': 1, 'rspi_maxlp_fcalc': 1,

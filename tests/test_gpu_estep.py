@@ -600,3 +600,30 @@ def test_quad4_layout_entries(n, parts):
                 if cols.size:
                     need = max(need, -(-np.bincount(cols % 8, minlength=8).max() // 4))
             assert goff[h * nq + qd + 1] - goff[h * nq + qd] == need
+
+
+@pytest.mark.parametrize('dtype,code', [(torch.float32, 0), (torch.float64, 1), (torch.float16, 2)])
+def test_paired_holo_slices_bit_identical(dtype, code):
+    """rspi_rot_log_slices_pairs (two 16-byte loads per bilinear sample from
+    the paired copy) gives the bits of rspi_rot_log_slices on row ranges
+    that start and end inside a state's rotations, and the same abs_max."""
+    from rspi.device import cur_stream, ptr
+    from rspi.lib import call
+    g = load_golden('case_b')
+    _, es = _golden_estep(g, form='screen')
+    es.slices(torch.from_numpy(g['model_in_1']).cuda())
+    n = es.n_rows
+    for r0, r1 in ((0, n), (3, n - 5), (es.num_rot + 1, min(n, 3 * es.num_rot + 2)), (7, 8)):
+        outs = []
+        for fn, src in (('rspi_rot_log_slices', es.holo), ('rspi_rot_log_slices_pairs',
+                                                            es.holo_pairs)):
+            out = torch.full((r1 - r0, es.p_row), 7., dtype=dtype, device='cuda')
+            amax = torch.zeros(1, dtype=torch.float32, device='cuda')
+            call(fn, ptr(src), es.n_states0, es.num_rot, ptr(es.rot_cs), es.size, ptr(es.bg),
+                 ptr(es.sel_pix), es.n_sel, es.p_row, r0, r1, ptr(out), code, ptr(amax),
+                 cur_stream())
+            torch.cuda.synchronize()
+            outs.append((out.cpu().numpy(), float(amax.item())))
+        a, b = outs
+        assert np.array_equal(a[0].view(np.uint8), b[0].view(np.uint8)), (r0, r1)
+        assert a[1] == b[1] and a[1] > 0.

@@ -208,13 +208,24 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
     ent_bytes = total_rows * 32 * (2 if es.form == 'screen' else 4)
     alg_bytes = rows_per_launch * (es.p_row * esz + w['n'] * osz) + ent_bytes + 8 * w['n']
     achieved = alg_bytes / (ll_launch_ms * 1e-3) / 1e9
-    # on-chip gather roofline: one shared-memory value per entry slot per likelihood row
-    gathers = rows_per_launch * total_rows * 32
+    # on-chip gather roofline.  Screened form: one shared-memory value per
+    # photon (count-expanded, on likelihood pixels) per likelihood row; the
+    # padded entry slots the kernel gathers (its conflict-free layout) as
+    # slots_frac.  FP64 form: one value per (pixel, count) entry slot.
+    slots = total_rows * 32
+    if es.wide is not None and 'total_groups' in es.wide:
+        slots = es.wide['total_groups'] * 128
+    if es.form == 'screen':
+        work = int(es.ll['frame_sel_photons'].sum().item())
+    else:
+        work = total_rows * 32
+    gathers = rows_per_launch * work
     clk_mhz = (clk or {}).get('sm_mhz') or 1965.
     # values a shared-memory wavefront (128 B per clock) carries
     lanes = {0: 32, 1: 16, 2: 64}[es.slice_code]
     gather_peak = sm_count * lanes * clk_mhz * 1e6
     gather_rate = gathers / (ll_launch_ms * 1e-3)
+    slots_rate = rows_per_launch * slots / (ll_launch_ms * 1e-3)
     names = {'stream': 'k_screen_ll2', 'frame': 'k_screen_ll3', 'wide': 'k_screen_ll4',
              'wide16': 'k_screen_ll4h', 'pair': 'k_screen_ll5', 'quad': 'k_screen_ll6',
              'quad4': 'k_screen_ll7'}
@@ -225,10 +236,14 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
                  'frac': achieved / pk['hbm_gbs'],
                  'traffic': dram_traffic(args, w, es, rows_per_launch),
                  'peak_source': pk['source'] + ' (HBM copy)'}, **common)
-    gather = {'achieved': gather_rate, 'peak': gather_peak, 'unit': 'gathers/s',
-              'frac': gather_rate / gather_peak,
-              'note': 'shared-memory gather limit: %d SMs x %d lanes/clk x %.0f MHz'
-              % (sm_count, lanes, clk_mhz)}
+    gather = {'achieved': gather_rate, 'peak': gather_peak, 'unit': 'values/s',
+              'frac': gather_rate / gather_peak, 'slots_frac': slots_rate / gather_peak,
+              'slot_efficiency': work / max(1, slots),
+              'note': ('%s per likelihood row against the shared-memory value rate %d SMs x '
+                       '%d values/clk x %.0f MHz; slots_frac: the entry slots the kernel '
+                       'gathers, padding included'
+                       % ('photons' if es.form == 'screen' else 'entry slots', sm_count, lanes,
+                          clk_mhz))}
     return roof, gather, rows_per_launch
 
 

@@ -487,8 +487,9 @@ class EStep:
         return quad4_parts(self.p_row, self.screen_parts)
 
     def _quad4_entries(self):
-        """Entries of the four-row frame-quad kernel: frames ordered and taken
-        four at a time as for ``quad``; per (quad, column part) the largest of
+        """Entries of the four-row frame-quad kernel: frames ordered within
+        each window of PAIR_WINDOW by decreasing group counts, part 0 first,
+        and taken four at a time; per (quad, column part) the largest of
         its frames' group counts, group ranges part-major; lane j of a
         sub-frame holds the photons of local column class j (mod 8); one
         FP32 running sum per (CTA, row, frame slot) when there are several
@@ -500,10 +501,12 @@ class EStep:
         call('rspi_quad4_entry_groups', ptr(l16['entries']), ptr(l16['row_off']), n, pz, parts,
              part_w, ptr(ng), s)
         ngp = ng.view(n, parts).to(_i64)
-        tot = ngp.sum(1)
-        gmax = int(tot.max().item())
-        win = torch.arange(n, device=dev, dtype=_i64) // PAIR_WINDOW
-        order = torch.argsort(win * (gmax + 1) + (gmax - tot), stable=True).to(_i32)
+        # within each window, frames in decreasing (part 0, part 1, ...) group
+        # counts: a quad's frames then need alike counts in every part
+        order = torch.arange(n, device=dev, dtype=_i64)
+        for h in reversed(range(parts)):
+            order = order[torch.argsort(-ngp[order, h], stable=True)]
+        order = order[torch.argsort(order // PAIR_WINDOW, stable=True)].to(_i32)
         nq = (n + 3) // 4
         set_frames = torch.full((4 * nq,), -1, dtype=_i32, device=dev)
         set_frames[:n] = order

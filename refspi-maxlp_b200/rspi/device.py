@@ -24,6 +24,7 @@ _i32 = torch.int32
 _i64 = torch.int64
 INT32_MAX = 2 ** 31 - 1
 PAIR_WINDOW = 256   # frames sorted by length for pairing within such windows
+QUAD4_WINDOW = 512   # frames ordered by group counts within such windows (four-row quads)
 QUAD4_SMEM = 227 * 1024 - 1024   # shared bytes of the four-row tile (kernel limit)
 QUAD4_MAX_PARTS = 4              # column parts of the four-row tile
 QUAD4_COLS = (QUAD4_SMEM // 16 - 8) // 8 * 8   # most columns of one part
@@ -488,7 +489,7 @@ class EStep:
 
     def _quad4_entries(self):
         """Entries of the four-row frame-quad kernel: frames ordered within
-        each window of PAIR_WINDOW by decreasing group counts, part 0 first,
+        each window of QUAD4_WINDOW by decreasing group counts, part 0 first,
         and taken four at a time; per (quad, column part) the largest of
         its frames' group counts, group ranges part-major; lane j of a
         sub-frame holds the photons of local column class j (mod 8); one
@@ -506,7 +507,7 @@ class EStep:
         order = torch.arange(n, device=dev, dtype=_i64)
         for h in reversed(range(parts)):
             order = order[torch.argsort(-ngp[order, h], stable=True)]
-        order = order[torch.argsort(order // PAIR_WINDOW, stable=True)].to(_i32)
+        order = order[torch.argsort(order // QUAD4_WINDOW, stable=True)].to(_i32)
         nq = (n + 3) // 4
         set_frames = torch.full((4 * nq,), -1, dtype=_i32, device=dev)
         set_frames[:n] = order

@@ -545,7 +545,7 @@ def test_quad4_layout_entries(n, parts):
     the pad q = part_w / 8 (zero columns) elsewhere; group ranges part-major
     with each (quad, part) as long as its longest frame needs; frames taken
     within windows of consecutive frames."""
-    from rspi.device import PAIR_WINDOW
+    from rspi.device import QUAD4_WINDOW
     size = 37
     d = random_photons(size, n, 40. * size, 14, empty_frames=(2, 9), heavy=5)
     ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
@@ -588,7 +588,7 @@ def test_quad4_layout_entries(n, parts):
             ref = wide[woff[f]:woff[f + 1]]
             assert np.array_equal(np.sort(np.concatenate(got)), np.sort(ref[ref < pz])), f
     assert sorted(seen) == list(range(n))
-    assert np.all(qf[:n] // PAIR_WINDOW == np.arange(n) // PAIR_WINDOW)
+    assert np.all(qf[:n] // QUAD4_WINDOW == np.arange(n) // QUAD4_WINDOW)
     # each (quad, part) range is as long as its longest frame needs
     for h in range(parts):
         for qd in range(nq):

@@ -62,12 +62,10 @@ def parse_args():
     ap.add_argument('--frames', type=int, default=None, help='override frame count (testing)')
     ap.add_argument('--form', default=None, choices=['fp64', 'screen', 'dense'],
                     help='likelihood form (default: dense for config 5, screen otherwise)')
-    ap.add_argument('--kernel', default=None, choices=['stream', 'frame', 'wide', 'pair', 'quad', 'quad4', 'dynamic'],
-                    help='likelihood kernel (default: wide for the screened form, stream for FP64)')
+    ap.add_argument('--kernel', default=None, choices=['stream', 'quad4', 'dynamic'],
+                    help='likelihood kernel (default: the EStep default of the form)')
     ap.add_argument('--warps', type=int, default=None,
                     help='warps per CTA of the likelihood kernel (default: the EStep default, 32)')
-    ap.add_argument('--screen-slices', default='fp32', choices=['fp32', 'fp16'],
-                    help='screened form: FP32 slices (two rows per gather) or FP16 (four)')
     ap.add_argument('--screen-delta', type=float, default=None,
                     help='FP64 rescoring window in nats (EMC default 0: the argmax candidates)')
     ap.add_argument('--no-phaser-screen', action='store_true',
@@ -159,9 +157,6 @@ def dram_traffic(args, w, es, rows_per_launch):
     except (OSError, ValueError, KeyError):
         return None
     kern = es.kernel
-    if kern == 'wide' and getattr(es, 'wide', None) is not None:
-        kern = 'wide16b' if es.wide.get('narrow') else (
-            'wide32b' if es.wide.get('banked') else 'wide32')
     for c in caps:
         if (c['form'] == es.form and c.get('kernel', 'stream') == kern and
                 c['config'] == args.config and c['frames'] == w['n'] and
@@ -201,7 +196,7 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
                      'flops_per_launch': flops, 'algorithmic_bytes_per_launch': bytes_alg}, **common)
         return roof, None, rows_per_launch
     total_rows = es.ll16['total_rows'] if es.form == 'screen' else es.ll['total_rows']
-    esz = {0: 4, 1: 8, 2: 2}[es.slice_code]
+    esz = {0: 4, 1: 8}[es.slice_code]
     osz = 4 if es.prob_code == 0 else 8
     # algorithmic bytes per launch = its slices in + its LL rows out + the
     # packed photon entries once
@@ -222,15 +217,13 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
     gathers = rows_per_launch * work
     clk_mhz = (clk or {}).get('sm_mhz') or 1965.
     # values a shared-memory wavefront (128 B per clock) carries
-    lanes = {0: 32, 1: 16, 2: 64}[es.slice_code]
+    lanes = {0: 32, 1: 16}[es.slice_code]
     gather_peak = sm_count * lanes * clk_mhz * 1e6
     gather_rate = gathers / (ll_launch_ms * 1e-3)
     slots_rate = rows_per_launch * slots / (ll_launch_ms * 1e-3)
-    names = {'stream': 'k_screen_ll2', 'frame': 'k_screen_ll3', 'wide': 'k_screen_ll4',
-             'wide16': 'k_screen_ll4h', 'pair': 'k_screen_ll5', 'quad': 'k_screen_ll6',
-             'quad4': 'k_screen_ll7'}
-    roof = dict({'kernel': ('%s (%s screening likelihood, row a7)' %
-                            (names.get(es.kernel, es.kernel), 'FP16' if es.slice_code == 2 else 'FP32')
+    names = {'stream': 'k_ll_stream<FormScreen>', 'quad4': 'k_screen_ll7'}
+    roof = dict({'kernel': ('%s (FP32 screening likelihood, row a7)' %
+                            names.get(es.kernel, es.kernel)
                             if es.form == 'screen' else 'k_ll_stream / k_loglike (FP64 likelihood, row a7)'),
                  'bound': 'hbm', 'achieved': achieved, 'peak': pk['hbm_gbs'], 'unit': 'GB/s',
                  'frac': achieved / pk['hbm_gbs'],
@@ -247,7 +240,7 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
     return roof, gather, rows_per_launch
 
 
-def write_inputs(tmp, w, data, form, slice_gb=8., screen_slices='fp32', screen_delta=None):
+def write_inputs(tmp, w, data, form, slice_gb=8., screen_delta=None):
     from rspi.photonfile import write_photons
     os.makedirs(os.path.join(tmp, 'out'), exist_ok=True)
     write_photons(os.path.join(tmp, 'photons.npz'), data)
@@ -256,10 +249,9 @@ def write_inputs(tmp, w, data, form, slice_gb=8., screen_slices='fp32', screen_d
     with open(cfg, 'w') as f:
         f.write('[emc]\nsize = %d\nin_photons_file = photons.npz\noutput_folder = out/\n'
                 'log_file = out/EMC.log\nneed_scaling = True\nnum_rot = %d\nnum_modes = %d\n'
-                'sphere_dia = %s\nshiftx = %s\nshifty = %s\nform = %s\nslice_budget_gb = %g\n'
-                'screen_slices = %s\n' %
+                'sphere_dia = %s\nshiftx = %s\nshifty = %s\nform = %s\nslice_budget_gb = %g\n' %
                 (w['size'], r['num_rot'], w['n_modes'], r['sphere_dia'], r['shiftx'], r['shifty'],
-                 form, slice_gb, screen_slices))
+                 form, slice_gb))
         if screen_delta is not None:
             f.write('screen_delta = %r\n' % float(screen_delta))
     return cfg
@@ -505,6 +497,61 @@ def reference_gpu(args, w, data, model):
         return {'unavailable': '%s: %s' % (type(exc).__name__, exc)}
 
 
+def parity_block(rec, es, w, model0, dev, EStep):
+    """One EMC iteration of the chosen (screened) form and of the plain FP64
+    form from the same start model, compared over the whole likelihood
+    matrix (every row x frame), the argmax, the per-frame maximum and
+    log-sum-exp, and the model after the M-step (emc.py:134-157).  Returns
+    the errors relative to FP64, or the reason the comparison was skipped."""
+    import torch
+    free, _ = torch.cuda.mem_get_info(dev)
+    need = es.n_rows * w['n'] * 8 + es.chunk_rows * es.p_row * 8 + (1 << 30)
+    if need > 0.9 * free:
+        return {'skipped': 'the FP64 likelihood matrix (%.1f GB) does not fit beside the '
+                           'chosen form\'s' % (es.n_rows * w['n'] * 8 / 1e9)}
+    m_c = torch.from_numpy(model0).to(dev)
+    es.run(m_c)
+    maxll, rmax, logz = es.reduce()
+    rec.phaser.run_from_rmax(m_c, rmax, w['num_rot'], rec.state_vals, rec.phaser_rot)
+    screen0 = rec.phaser.mstep.screen
+    rec.phaser.mstep.screen = False
+    pe = EStep(rec.dset.photons, w['size'], w['num_rot'], rec.shiftx, rec.shifty,
+               rec.sphere_dia, rec.probmask, rec.dset.bg.cpu().numpy(), n_modes=w['n_modes'],
+               form='fp64', kernel='dynamic')
+    m_p = torch.from_numpy(model0).to(dev)
+    pe.run(m_p)
+    maxll64, rmax64, logz64 = pe.reduce()
+    rec.phaser.run_from_rmax(m_p, rmax64, w['num_rot'], rec.state_vals, rec.phaser_rot)
+    rec.phaser.mstep.screen = screen0
+    torch.cuda.synchronize()
+    rec.dset.photons.err.check('parity iteration')
+    # every entry of the FP32 matrix against FP64, in row chunks
+    worst, nan_mismatch = 0., 0
+    step = max(1, (1 << 28) // max(1, w['n']))
+    for r0 in range(0, es.n_rows, step):
+        a = es.prob[r0:r0 + step].double()
+        b = pe.prob[r0:r0 + step]
+        nan_mismatch += int((a.isnan() != b.isnan()).sum().item())
+        ok = ~b.isnan()
+        if bool(ok.any()):
+            worst = max(worst, float(((a - b).abs()[ok] / b.abs()[ok]).max().item()))
+
+    def rel(x, y):
+        return float(((x - y).abs() / y.abs().clamp_min(1e-300)).max().item())
+    out = {'entries': es.n_rows * w['n'], 'll_rel_err_max': worst,
+           'nan_mismatches': nan_mismatch,
+           'argmax_identical': bool(torch.equal(rmax, rmax64)),
+           'maxll_rel_err': rel(maxll, maxll64), 'logz_rel_err': rel(logz, logz64),
+           'model_rel_err': rel(m_c, m_p),
+           'candidates_rescored': getattr(es, 'n_candidates', None),
+           'note': 'one iteration of each form from the start model; FP32 screened '
+                   'likelihoods and FP64-rescored argmax/max/log-sum-exp vs the FP64 form, '
+                   'model after the M-step vs the FP64 pattern search'}
+    del pe
+    torch.cuda.empty_cache()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -523,8 +570,7 @@ def run_ours(args):
     data = generate_data(args.config, w, device=dev)
     t_gen = time.time() - t0
     tmp = tempfile.mkdtemp(prefix='rspi_bench_')
-    cfgfile = write_inputs(tmp, w, data, args.form, args.slice_gb, args.screen_slices,
-                           args.screen_delta)
+    cfgfile = write_inputs(tmp, w, data, args.form, args.slice_gb, args.screen_delta)
     from emc import EMC
     import contextlib
     import io
@@ -609,14 +655,19 @@ def run_ours(args):
                'd2h_bytes_per_step': 16 * p + 4 * w['n'],
                'api': 'EMC.run_iteration (model host->device, model + argmax device->host)'}
 
-    # the plain form on the same data, timed eagerly step by step (FP64
-    # slices and likelihoods, warp-per-frame kernel)
-    plain = None
+    # the plain form on the same data (FP64 slices and likelihoods,
+    # warp-per-frame kernel, FP64 pattern search): first one iteration of each
+    # form from the start model, compared entry by entry (the parity block),
+    # then the plain form timed eagerly step by step
+    plain, parity = None, None
     if rank == 0 and not args.no_plain:
         from rspi.device import EStep
+        rec._graph = None
+        pe = None
+        if es.form == 'screen':
+            parity = parity_block(rec, es, w, model0, dev, EStep)
         # the chosen form's likelihood matrix, slices, candidates and graph
         # pool are released first: the matrices need not fit at once
-        rec._graph = None
         rec.prob = None
         for name in ('prob', 'lsl', 'cand_d', 'cand_r', 'cand_ll', 'row_cand'):
             setattr(es, name, None)
@@ -700,6 +751,7 @@ def run_ours(args):
         'clocks': clk,
         'e2e': e2e,
         'plain': plain,
+        'parity': parity,
         'form': {'likelihood': args.form, 'kernel': es.kernel,
                  'candidates_rescored': n_cand, 'rescore_window_nats': getattr(es, 'delta', None),
                  'pattern_search': phaser_form},

@@ -35,7 +35,8 @@ extern "C" {
 #define RSPI_ERR_CUDA (-3)     /* launch failed */
 #define RSPI_ERR_TIMEOUT (-4)  /* a bounded device-side wait ran out */
 #define RSPI_ERR_CAPACITY (-5) /* a value does not fit the packed layout */
-#define RSPI_ERR_TOO_LARGE (-6) /* larger than the fixed scratch of a no-allocation entry */
+#define RSPI_ERR_TOO_LARGE (-6) /* larger than the fixed scratch of a no-allocation entry
+                                 * point (rspi_screen_candidates_noalloc only) */
 
 /* Library version and build target, e.g. "rspi 0.1 sm_100a". */
 const char *rspi_version(void);
@@ -160,8 +161,10 @@ int rspi_loglike(const void *lslices, int slice_dtype, long long p_pad, long lon
                  int n_ctas, cudaStream_t stream);
 
 /* Streaming variant of rspi_loglike (form 1: 32-bit entries, FP64 slices and
- * output, bit-identical to rspi_loglike) and of rspi_screen_loglike (form 0:
- * 16-bit entries, FP32 slices and output).  Each warp owns a contiguous range
+ * output, bit-identical to rspi_loglike) and a plain screening kernel (form 0:
+ * the 16-bit entries of rspi_ll16_entry_fill, two rows per 32-bit word, FP32
+ * slices, FP32 sums and output: LL32[r][d] = float(init[r/num_rot]*scales[d]
+ * + FP32 sum of the frame's FP32 slice values)).  Each warp owns a contiguous range
  * of frames holding an equal share of the entry words and streams it with a
  * prefetch across frame boundaries; frames are processed in index order
  * (no frame_order).  row_off are the entry-row offsets of that form. */
@@ -198,142 +201,6 @@ int rspi_ll16_entry_fill(const int *ones, const int *multi, const long long *one
                          const long long *row_off, unsigned short *entries,
                          cudaStream_t stream);
 
-/* FP32 screening likelihood: LL32[r][d] = float(init[r/num_rot]*scales[d] +
- * FP32 sum of the frame's FP32 slice values).  Slices of rows
- * [row_begin, row_end) are read from lslices (p_row floats per row). */
-int rspi_screen_loglike(const float *lslices, long long p_row, long long num_rot,
-                        const double *init, const double *scales,
-                        const unsigned short *entries, const long long *row_off,
-                        const int *frame_order, long long n_data, long long row_begin,
-                        long long row_end, float *ll, long long ll_stride, int states_per_tile,
-                        int warps_per_cta, int n_ctas, cudaStream_t stream);
-
-/* Interleaved screening likelihood (the chosen kernel): same inputs and
- * output as rspi_screen_loglike (frames in index order, no frame_order);
- * the tile's T in {1, 2, 4} rows are staged as sl[c*T + t] so one vector
- * gather serves all T rows.  Requires every entry index < p_row (check once
- * with rspi_entries16_check). */
-int rspi_screen_loglike2(const float *lslices, long long p_row, long long num_rot,
-                         const double *init, const double *scales,
-                         const unsigned short *entries, const long long *row_off,
-                         long long n_data, long long row_begin, long long row_end, float *ll,
-                         long long ll_stride, int states_per_tile, int warps_per_cta,
-                         int n_ctas, cudaStream_t stream);
-
-/* The same likelihoods as rspi_screen_loglike2 for 1 or 2 states per tile,
- * frame at a time: each warp sums one frame after another, the frame's
- * first prefetch_words (4, 8 or 12) words having been loaded during the
- * previous frame, without per-word frame-boundary tests (words past a
- * frame's end read the lane's zero column).  Same arguments plus
- * prefetch_words; same error bound for the screening threshold. */
-int rspi_screen_loglike3(const float *lslices, long long p_row, long long num_rot,
-                         const double *init, const double *scales,
-                         const unsigned short *entries, const long long *row_off,
-                         long long n_data, long long row_begin, long long row_end, float *ll,
-                         long long ll_stride, int states_per_tile, int prefetch_words,
-                         int warps_per_cta, int n_ctas, cudaStream_t stream);
-
-/* Wide entries for rspi_screen_loglike4: per frame the 16-bit entry rows
- * (rspi_ll16_entry_fill layout) padded to a multiple of four with the
- * lane's zero column, as 32-bit byte offsets sel * 4 * states_per_tile of
- * the interleaved tile, four rows of a lane in one 16-byte group:
- * wide[((group_off[d] + g) * 32 + lane) * 4 + k] holds row 4g + k.
- * rspi_wide_entry_groups writes each frame's group count; the caller scans
- * it (rspi_scan_rows) into group_off[n_data + 1] and allocates
- * group_off[n_data] * 128 entries. */
-int rspi_wide_entry_groups(const long long *row_off16, long long n_data, int *groups,
-                           cudaStream_t stream);
-int rspi_wide_entry_fill(const unsigned short *entries16, const long long *row_off16,
-                         long long n_data, int p_zero, int states_per_tile,
-                         const long long *group_off, unsigned *wide, cudaStream_t stream);
-
-/* The same wide entries in the bank-class layout: a photon at tile column
- * sel (byte offset sel * 4 * states_per_tile) has shared-memory bank class
- * sel mod C, C = 32 / states_per_tile, and goes to a lane l with
- * l mod C == its class (the k-th photon of class c: lane c + C (k mod 32/C),
- * slot k / (32/C)); the other slots hold the lane's zero column.  Every
- * gather instruction of the likelihood kernels then touches distinct bank
- * classes.  A frame takes ceil(max_c n_c / (4 * 32/C)) groups (n_c: its
- * photons of class c); the photons of a frame are summed in another order
- * than with rspi_wide_entry_fill, within the same FP32 error bound. */
-int rspi_wide_entry_groups_banked(const unsigned short *entries16, const long long *row_off16,
-                                  long long n_data, int p_zero, int states_per_tile,
-                                  int *groups, cudaStream_t stream);
-int rspi_wide_entry_fill_banked(const unsigned short *entries16, const long long *row_off16,
-                                long long n_data, int p_zero, int states_per_tile,
-                                const long long *group_off, unsigned *wide, cudaStream_t stream);
-
-/* The bank-class layout with 16-bit entries (same groups and slots, from
- * rspi_wide_entry_groups_banked): lane l only holds columns
- * sel = C q + (l mod C), C = 32 / states_per_tile, so an entry stores
- * q = sel / C and the gather's byte offset is q * 128 + 4 states_per_tile
- * (l mod C).  group_off[n_data] * 128 entries, 8-byte aligned. */
-int rspi_wide_entry_fill_narrow(const unsigned short *entries16, const long long *row_off16,
-                                long long n_data, int p_zero, int states_per_tile,
-                                const long long *group_off, unsigned short *narrow,
-                                cudaStream_t stream);
-
-/* The same likelihoods as rspi_screen_loglike2 (1 or 2 states per tile) from
- * the wide entries built for that tile size: one 16-byte load per four
- * photons of a lane and no per-photon index arithmetic. */
-int rspi_screen_loglike4(const float *lslices, long long p_row, long long num_rot,
-                         const double *init, const double *scales, const unsigned *wide,
-                         const long long *group_off, long long n_data, long long row_begin,
-                         long long row_end, float *ll, long long ll_stride,
-                         int states_per_tile, int warps_per_cta, int n_ctas,
-                         cudaStream_t stream);
-
-/* Frame pairs (two rows per tile): the two half-warps take the two frames of
- * a pair, so one reduction and store pass serves two frames.
- * rspi_pair_entry_groups: each frame's group count ceil(max_c n_c / 4) with
- * 16 bank classes, one lane per class.  The caller orders frames (e.g. by
- * that count), pairs them (pair p = frames pair_frames[2p],
- * pair_frames[2p + 1], -1 for none; pair_slot[d] = 2p + h for frame d in
- * half h), takes each pair's larger count and scans those into
- * pair_group_off[n_pairs + 1].
- * rspi_pair_entry_fill: total_groups * 128 16-bit entries (8-byte aligned):
- * lane 16 h + c of a pair group holds frame h's photons of class c (column
- * 16 q + c, q stored), four per group, the lane's zero column elsewhere.
- * rspi_screen_loglike5: the likelihood rows from those entries (the sums of
- * rspi_screen_loglike4 in another order, within the same FP32 error bound
- * with each frame's summation length max(entry rows, its pair's groups)). */
-int rspi_pair_entry_groups(const unsigned short *entries16, const long long *row_off16,
-                           long long n_data, int p_zero, int *groups, cudaStream_t stream);
-int rspi_pair_entry_fill(const unsigned short *entries16, const long long *row_off16,
-                         long long n_data, int p_zero, const int *pair_slot,
-                         const long long *pair_group_off, long long total_groups,
-                         unsigned short *narrow, cudaStream_t stream);
-int rspi_screen_loglike5(const float *lslices, long long p_row, long long num_rot,
-                         const double *init, const double *scales, const unsigned short *narrow,
-                         const long long *pair_group_off, const int *pair_frames,
-                         long long n_pairs, long long row_begin, long long row_end, float *ll,
-                         long long ll_stride, int warps_per_cta, int n_ctas,
-                         cudaStream_t stream);
-
-/* Frame quads: four frames per warp, eight lanes each (two rows per tile).
- * Lane 8 u + j of a quad group holds frame u's photons of bank classes j and
- * j + 8, the first in slots 0 and 2 and the second in slots 1 and 3 for even
- * u (swapped for odd u), so every gather of a half-warp covers 16 distinct
- * classes; the k-th photon of a class goes to group k / 2, the lane's
- * (k mod 2)-th slot of that class's phase; other slots hold column
- * p_zero + (the slot's class).  A frame takes ceil(max_c n_c / 2) groups
- * (rspi_quad_entry_groups); quads, quad_slot[d] = 4 q + u, quad_frames and
- * quad_group_off as for the frame pairs.  rspi_screen_loglike6: the
- * likelihood rows from them, within the FP32 error bound with each frame's
- * summation length max(entry rows, its quad's groups). */
-int rspi_quad_entry_groups(const unsigned short *entries16, const long long *row_off16,
-                           long long n_data, int p_zero, int *groups, cudaStream_t stream);
-int rspi_quad_entry_fill(const unsigned short *entries16, const long long *row_off16,
-                         long long n_data, int p_zero, const int *quad_slot,
-                         const long long *quad_group_off, long long total_groups,
-                         unsigned short *narrow, cudaStream_t stream);
-int rspi_screen_loglike6(const float *lslices, long long p_row, long long num_rot,
-                         const double *init, const double *scales, const unsigned short *narrow,
-                         const long long *quad_group_off, const int *quad_frames,
-                         long long n_quads, long long row_begin, long long row_end, float *ll,
-                         long long ll_stride, int warps_per_cta, int n_ctas,
-                         cudaStream_t stream);
-
 /* Frame quads with four rows per tile: one 16-byte gather brings a photon's
  * value in all four rows.  The likelihood columns [0, p_zero) are cut into
  * n_parts (1-4) parts of part_w columns (part_w % 8 == 0, n_parts * part_w
@@ -367,28 +234,6 @@ int rspi_screen_loglike7(const float *lslices, long long p_row, long long num_ro
                          int n_parts, int part_w, long long row_begin, long long row_end,
                          float *ll, long long ll_stride, float *part_sums, int part_sums_ctas,
                          int warps_per_cta, int n_ctas, cudaStream_t stream);
-
-/* rspi_screen_loglike4 from the 16-bit bank-class entries of
- * rspi_wide_entry_fill_narrow: one 8-byte load per four photons of a lane
- * (half the entry bytes), one integer multiply-add per photon for its
- * offset; the same sums in the same order. */
-int rspi_screen_loglike4n(const float *lslices, long long p_row, long long num_rot,
-                          const double *init, const double *scales,
-                          const unsigned short *narrow, const long long *group_off,
-                          long long n_data, long long row_begin, long long row_end, float *ll,
-                          long long ll_stride, int states_per_tile, int warps_per_cta,
-                          int n_ctas, cudaStream_t stream);
-
-/* Four likelihood rows per tile from FP16 rotated log-slices
- * (rspi_rot_log_slices with out_dtype 2), the wide entries built for the
- * FP32 two-row tile (offset sel * 8).  FP16 storage adds up to 2^-11 |L| per
- * value; the caller's candidate threshold covers it by passing row offsets
- * row_off16[d] + 8192 d to rspi_screen_candidates. */
-int rspi_screen_loglike4h(const void *lslices16, long long p_row, long long num_rot,
-                          const double *init, const double *scales, const unsigned *wide,
-                          const long long *group_off, long long n_data, long long row_begin,
-                          long long row_end, float *ll, long long ll_stride, int warps_per_cta,
-                          int n_ctas, cudaStream_t stream);
 
 /* *max_index = largest value in a 16-bit entry array. */
 int rspi_entries16_check(const unsigned short *entries, long long n_entries,
@@ -635,8 +480,10 @@ int rspi_rot_log_split(const double *holo, long long n_states0, long long num_ro
  * with FP32 accumulation in tensor memory: b_hi/b_lo hold n_brows slice rows
  * starting at row_begin; a1 may be NULL (counts below 256).  prob points at
  * row row_begin (row stride ld >= n_frames, frames contiguous, FP32).  All
- * matrix bases 16-byte aligned.  A device wait that exceeds its bound sets
- * *err = RSPI_ERR_TIMEOUT and leaves the tile's likelihoods unwritten. */
+ * matrix bases 16-byte aligned.  One call covers at most 65535 * 128 rows
+ * (more is RSPI_ERR_ARG; split the range).  A device wait that exceeds its
+ * bound sets *err = RSPI_ERR_TIMEOUT and leaves the tile's likelihoods
+ * unwritten. */
 int rspi_dense_loglike(const void *a0, const void *a1, const void *b_hi, const void *b_lo,
                        long long k_pad, long long n_frames, long long n_brows,
                        long long num_rot, long long row_begin, long long row_end,

@@ -17,7 +17,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT_DIR = os.path.join(os.path.dirname(HERE), '_ref')
 LIB = os.path.join(OUT_DIR, 'libref_kernels_gpu.so')
-DEFAULT_REF = '/root/reference'
+DEFAULT_REF = os.environ.get('RSPI_REFERENCE_ROOT', '/root/reference')
 
 
 def build(ref_root=DEFAULT_REF, quiet=False):

@@ -516,16 +516,14 @@ int launch_dense(const DenseMaps &maps, int n_digits, long long k_pad, long long
     const int stage_bytes = (n_digits + b_parts) * DN_TILE_BYTES;
     const int stages = min(8, DN_SMEM_BUDGET / stage_bytes);
     const int smem = stages * stage_bytes + 1024;
-    static bool attr = false;
-    if (!attr) {
-        if (cudaFuncSetAttribute(k_dense_ll<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 DN_SMEM_BUDGET + 1024) != cudaSuccess)
-            return RSPI_ERR_CUDA;
-        attr = true;
-    }
+    static RspiSmemOptIn optin;
+    if (!rspi_smem_optin((const void *)k_dense_ll<KIND>, DN_SMEM_BUDGET + 1024, optin))
+        return RSPI_ERR_CUDA;
+    // a launch covers at most 65535 row tiles of 128 rows: larger row ranges
+    // are the caller's to split (bad argument)
+    if ((n_rows + DN_BN - 1) / DN_BN > 65535) return RSPI_ERR_ARG;
     const dim3 grid((unsigned)((n_frames + DN_BM - 1) / DN_BM),
                     (unsigned)((n_rows + DN_BN - 1) / DN_BN));
-    if (grid.y > 65535) return RSPI_ERR_TOO_LARGE;
     const int n_kb = (int)(k_pad / (KIND == KIND_I8 ? 128 : DN_BK));
     k_dense_ll<KIND><<<grid, 128, smem, stream>>>(maps, n_digits, stages, n_kb, n_frames,
                                                   row_begin, row_end, num_rot, init, scales,

@@ -168,13 +168,8 @@ int launch(const void *lsl, long long p_row, long long num_rot, const double *in
            int n_ctas, cudaStream_t stream) {
     const size_t smem = (size_t)T * p_row * sizeof(typename F::TL);
     if (smem > (size_t)SMEM_LIMIT - 1024) return RSPI_ERR_ARG;
-    static size_t smem_set = 0;
-    if (smem > smem_set) {
-        if (cudaFuncSetAttribute(k_ll_stream<F, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem) != cudaSuccess)
-            return RSPI_ERR_CUDA;
-        smem_set = smem;
-    }
+    static RspiSmemOptIn optin;
+    if (!rspi_smem_optin((const void *)k_ll_stream<F, T>, smem, optin)) return RSPI_ERR_CUDA;
     const long long n_tiles = (r1 - r0 + T - 1) / T;
     warps = min(warps, max_threads<T>() / 32);
     if (n_ctas <= 0) {

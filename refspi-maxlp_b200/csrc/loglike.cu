@@ -103,13 +103,8 @@ int launch_t(const void *lsl, long long p_pad, long long num_rot, const double *
     const size_t smem = (size_t)T * p_pad * sizeof(TL);
     if (smem > (size_t)SMEM_LIMIT - 1024) return RSPI_ERR_ARG;
     auto kern = k_loglike<TL, TO, T>;
-    static size_t smem_set = 0;   // set once, so launches can be graph-captured
-    if (smem > smem_set) {
-        if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
-            return RSPI_ERR_CUDA;
-        smem_set = smem;
-    }
+    static RspiSmemOptIn optin;   // once per device, so launches can be graph-captured
+    if (!rspi_smem_optin((const void *)kern, smem, optin)) return RSPI_ERR_CUDA;
     const long long n_tiles = (row_end - row_begin + T - 1) / T;
     if (n_ctas <= 0) {
         const int per_sm = max(1, (int)((SMEM_LIMIT) / (smem + 1024)));

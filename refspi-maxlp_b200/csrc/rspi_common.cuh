@@ -4,6 +4,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "rspi.h"
 
 #define RSPI_FULL_MASK 0xffffffffu
@@ -127,15 +129,52 @@ __device__ __forceinline__ double block_sum(double v, double *scratch) {
     return t;
 }
 
+// Per-device host state: the library may drive several GPUs from one process,
+// so every cached device property and kernel attribute is kept per device.
+constexpr int RSPI_MAX_DEVICES = 64;
+
+static inline int rspi_device() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return dev;
+}
+
+// SM count of the current device (cached per device).
 static inline int rspi_sm_count() {
-    static int count = 0;
-    if (count == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
-        if (count <= 0) count = 148;
+    static std::atomic<int> count[RSPI_MAX_DEVICES];
+    const int dev = rspi_device();
+    int c = (dev >= 0 && dev < RSPI_MAX_DEVICES) ? count[dev].load(std::memory_order_relaxed) : 0;
+    if (c <= 0) {
+        cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev);
+        if (c <= 0) c = 148;
+        if (dev >= 0 && dev < RSPI_MAX_DEVICES) count[dev].store(c, std::memory_order_relaxed);
     }
-    return count;
+    return c;
+}
+
+// Dynamic shared-memory opt-in of one kernel, applied on each device the
+// first time a launch there needs more than the default: one static
+// RspiSmemOptIn per kernel instance.  Concurrent first calls on one device
+// both apply the same attribute, which is harmless.  Returns false when the
+// attribute cannot be set.
+struct RspiSmemOptIn {
+    std::atomic<size_t> done[RSPI_MAX_DEVICES];
+};
+
+static inline bool rspi_smem_optin(const void *kernel, size_t smem, RspiSmemOptIn &st) {
+    const int dev = rspi_device();
+    const bool cached = dev >= 0 && dev < RSPI_MAX_DEVICES;
+    if (cached && st.done[dev].load(std::memory_order_acquire) >= smem) return true;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return false;
+    if (cached) {
+        size_t prev = st.done[dev].load(std::memory_order_relaxed);
+        while (prev < smem &&
+               !st.done[dev].compare_exchange_weak(prev, smem, std::memory_order_release))
+            ;
+    }
+    return true;
 }
 
 static inline unsigned rspi_blocks(long long work, int threads, int cap_per_sm = 8) {

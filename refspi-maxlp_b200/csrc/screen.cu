@@ -1,9 +1,9 @@
 // Screened likelihood (rows a7-a9, the chosen form).
 //
-// 1. FP32 screening pass: rotated log-slices stored in FP32, photons stored
-//    as 16-bit sel indices with counts expanded (a pixel with k photons is k
-//    entries), two rows per 32-bit word: one warp load brings 64 photons and
-//    every shared-memory gather is bank-conflict free.  Sums are FP32.
+// 1. FP32 screening pass (ll_sets.cu, ll_quad4.cu, ll_stream.cu): rotated
+//    log-slices stored in FP32, photons as 16-bit sel indices with counts
+//    expanded (a pixel with k photons is k entries, built here).  Sums are
+//    FP32.
 // 2. Per frame, every state whose screened value is within
 //    delta + 2 * eps_d of the frame's screened maximum becomes a candidate,
 //    where eps_d bounds |LL32 - LL64| (storage rounding of the slices,
@@ -137,105 +137,6 @@ k_entry16_fill(const int *__restrict__ ones, const int *__restrict__ multi,
         }
         __syncwarp();
     }
-}
-
-// ---------------------------------------------------------------------------
-// FP32 screening likelihood
-// ---------------------------------------------------------------------------
-template <int T>
-__global__ void __launch_bounds__(1024)
-k_screen_ll(const float *__restrict__ lsl, long long p_row, long long num_rot,
-            const double *__restrict__ init, const double *__restrict__ scales,
-            const unsigned int *__restrict__ ent, const long long *__restrict__ row_off,
-            const int *__restrict__ frame_order, long long n_data, long long row_begin,
-            long long row_end, float *__restrict__ ll, long long ll_stride) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    float *sl = reinterpret_cast<float *>(smem_raw);
-    __shared__ int next_frame;
-    const int lane = threadIdx.x & 31;
-    const long long n_tiles = (row_end - row_begin + T - 1) / T;
-    const unsigned cmax = (unsigned)p_row - 1;
-    for (long long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
-        const long long first = row_begin + tile * T;
-        const int nt = (int)min((long long)T, row_end - first);
-        {
-            const long long nvec = (long long)nt * p_row / 4;
-            const float4 *src = reinterpret_cast<const float4 *>(lsl + (first - row_begin) * p_row);
-            float4 *dst = reinterpret_cast<float4 *>(sl);
-            for (long long i = threadIdx.x; i < nvec; i += blockDim.x) dst[i] = src[i];
-            const long long nzero = (long long)(T - nt) * p_row / 4;
-            for (long long i = threadIdx.x; i < nzero; i += blockDim.x)
-                dst[nvec + i] = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-        if (threadIdx.x == 0) next_frame = 0;
-        __syncthreads();
-        while (true) {
-            int k = 0;
-            if (lane == 0) k = atomicAdd(&next_frame, 1);
-            k = __shfl_sync(RSPI_FULL_MASK, k, 0);
-            if (k >= n_data) break;
-            const int d = frame_order ? frame_order[k] : k;
-            const long long p0 = row_off[d] >> 1, p1 = row_off[d + 1] >> 1;
-            float acc[T];
-#pragma unroll
-            for (int t = 0; t < T; ++t) acc[t] = 0.f;
-            const unsigned int *ep = ent + p0 * 32 + lane;
-            long long q = p0;
-            for (; q + 4 <= p1; q += 4, ep += 128) {
-                unsigned wv[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) wv[u] = __ldg(ep + 32 * u);
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const unsigned c0 = min(wv[u] & 0xffffu, cmax), c1 = min(wv[u] >> 16, cmax);
-#pragma unroll
-                    for (int t = 0; t < T; ++t) acc[t] += sl[t * p_row + c0] + sl[t * p_row + c1];
-                }
-            }
-            for (; q < p1; ++q, ep += 32) {
-                const unsigned wv = __ldg(ep);
-                const unsigned c0 = min(wv & 0xffffu, cmax), c1 = min(wv >> 16, cmax);
-#pragma unroll
-                for (int t = 0; t < T; ++t) acc[t] += sl[t * p_row + c0] + sl[t * p_row + c1];
-            }
-#pragma unroll
-            for (int t = 0; t < T; ++t) acc[t] = warp_sum(acc[t]);
-            if (lane < nt) {
-                float v = 0.f;
-#pragma unroll
-                for (int t = 0; t < T; ++t)
-                    if (t == lane) v = (float)(init[(first + t) / num_rot] * scales[d] + (double)acc[t]);
-                ll[(first + lane - row_begin) * ll_stride + d] = v;
-            }
-        }
-        __syncthreads();
-    }
-}
-
-template <int T>
-int launch_screen(const float *lsl, long long p_row, long long num_rot, const double *init,
-                  const double *scales, const unsigned *ent, const long long *row_off,
-                  const int *order, long long n_data, long long r0, long long r1, float *ll,
-                  long long stride, int warps, int n_ctas, cudaStream_t stream) {
-    const size_t smem = (size_t)T * p_row * sizeof(float);
-    if (smem > (size_t)SMEM_LIMIT - 1024) return RSPI_ERR_ARG;
-    static size_t smem_set = 0;
-    if (smem > smem_set) {
-        if (cudaFuncSetAttribute(k_screen_ll<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem) != cudaSuccess)
-            return RSPI_ERR_CUDA;
-        smem_set = smem;
-    }
-    const long long n_tiles = (r1 - r0 + T - 1) / T;
-    if (n_ctas <= 0) {
-        const int per_sm = max(1, (int)(SMEM_LIMIT / (smem + 1024)));
-        n_ctas = rspi_sm_count() * min(per_sm, max(1, 2048 / (warps * 32)));
-    }
-    if (n_ctas > n_tiles) n_ctas = (int)n_tiles;
-    k_screen_ll<T><<<n_ctas, warps * 32, smem, stream>>>(lsl, p_row, num_rot, init, scales, ent,
-                                                         row_off, order, n_data, r0, r1, ll,
-                                                         stride);
-    RSPI_RETURN_LAUNCH();
 }
 
 // ---------------------------------------------------------------------------
@@ -563,41 +464,6 @@ extern "C" int rspi_ll16_entry_fill(const int *ones, const int *multi,
     RSPI_RETURN_LAUNCH();
 }
 
-extern "C" int rspi_screen_loglike(const float *lslices, long long p_row, long long num_rot,
-                                   const double *init, const double *scales,
-                                   const unsigned short *entries, const long long *row_off,
-                                   const int *frame_order, long long n_data, long long row_begin,
-                                   long long row_end, float *ll, long long ll_stride,
-                                   int states_per_tile, int warps_per_cta, int n_ctas,
-                                   cudaStream_t stream) {
-    if (!lslices || !init || !scales || !entries || !row_off || !ll || n_data <= 0 ||
-        n_data > 0x7fffffffLL || p_row <= 32 || p_row % 32 || p_row > 65536 || num_rot <= 0 ||
-        row_begin < 0 || row_end < row_begin || ll_stride < n_data || warps_per_cta < 1 ||
-        warps_per_cta > 32)
-        return RSPI_ERR_ARG;
-    if ((reinterpret_cast<uintptr_t>(lslices) & 15) != 0 ||
-        (reinterpret_cast<uintptr_t>(entries) & 3) != 0)
-        return RSPI_ERR_ARG;
-    if (row_end == row_begin) return RSPI_OK;
-    const unsigned *ent = reinterpret_cast<const unsigned *>(entries);
-#define RSPI_SC(TT)                                                                            \
-    case TT:                                                                                   \
-        return launch_screen<TT>(lslices, p_row, num_rot, init, scales, ent, row_off,          \
-                                 frame_order, n_data, row_begin, row_end, ll, ll_stride,       \
-                                 warps_per_cta, n_ctas, stream);
-    switch (states_per_tile) {
-        RSPI_SC(1)
-        RSPI_SC(2)
-        RSPI_SC(3)
-        RSPI_SC(4)
-        RSPI_SC(6)
-        RSPI_SC(8)
-        default:
-            return RSPI_ERR_ARG;
-    }
-#undef RSPI_SC
-}
-
 extern "C" int rspi_screen_candidates(const float *ll, long long n_rows, long long n_data,
                                       const double *max32, const int *rmax32,
                                       const long long *frame_photons,
@@ -640,14 +506,9 @@ extern "C" int rspi_rescore(const int *cand_d, const int *cand_r, const long lon
     const size_t smem = (size_t)p_pad * sizeof(double);
     const bool grow = smem > (size_t)SMEM_LIMIT - 1024;
     if (grow && (!row_scratch || scratch_rows < 1)) return RSPI_ERR_ARG;
-    static size_t smem_set = 0;
-    if (!grow && smem > smem_set) {
-        if (cudaFuncSetAttribute(k_rescore_rows<false>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem) != cudaSuccess)
-            return RSPI_ERR_CUDA;
-        smem_set = smem;
-    }
+    static RspiSmemOptIn optin;
+    if (!grow && !rspi_smem_optin((const void *)k_rescore_rows<false>, smem, optin))
+        return RSPI_ERR_CUDA;
     const long long *total = cand_off + n_data;
     cudaMemsetAsync(row_cnt, 0, sizeof(int) * n_rows, stream);
     k_row_count<<<rspi_sm_count() * 8, 256, 0, stream>>>(cand_r, total, capacity, row_cnt);
@@ -700,22 +561,29 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 
 static __device__ __align__(256) int g_cand_scratch[NOALLOC_MAX_FRAMES * RY];
 
+// The array's device address on the current device, looked up once per
+// device and cached for the life of the process's primary context (a
+// cudaDeviceReset invalidates it; this library is not meant to outlive one).
+// Two host threads making the first call on one device at once both look
+// the address up and store the same value; the store is atomic.
 int *cand_scratch_address(int *status) {
-    static int *addr[NOALLOC_MAX_DEVICES] = {};
+    static std::atomic<int *> addr[NOALLOC_MAX_DEVICES];
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
         *status = RSPI_ERR_CUDA;
         return nullptr;
     }
-    if (addr[dev] == nullptr) {
+    int *cached = addr[dev].load(std::memory_order_acquire);
+    if (cached == nullptr) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_cand_scratch) != cudaSuccess || p == nullptr) {
             *status = RSPI_ERR_CUDA;
             return nullptr;
         }
-        addr[dev] = static_cast<int *>(p);
+        cached = static_cast<int *>(p);
+        addr[dev].store(cached, std::memory_order_release);
     }
-    return addr[dev];
+    return cached;
 }
 
 }  // namespace

@@ -18,8 +18,7 @@ FP64 rescoring of every state that can be the argmax (and, with
 densely, likelihood as a tensor-core GEMM, ``dense_gemm`` = ``auto`` /
 ``i8`` (exact fixed point) / ``bf16`` (hi + lo split), ``dense_rescore``
 (default true: FP64 rescoring of the candidates as in ``screen``)),
-``screen_slices`` (``fp32``, or ``fp16``: half-precision slices, four
-likelihood rows per gather, a wider candidate threshold), ``screen_delta``
+``screen_delta``
 (default 0: FP64 rescoring of the states that can be the argmax, which is
 what the hard-argmax iteration uses; 20: also every state within 20 nats of
 it, so that ``logz`` equals the FP64 form's -- the posterior consumers'
@@ -57,6 +56,7 @@ from rspi.lib import call  # noqa: E402
 from rspi.device import EStep  # noqa: E402
 
 P_MIN = 1.e-6   # emc.py:20
+RSPI_ERR_CAPACITY = -5   # include/rspi.h
 
 
 class EMC():
@@ -94,7 +94,7 @@ class EMC():
                            delta=self.screen_delta,
                            slice_budget_bytes=int(self.slice_budget_gb * (1 << 30)),
                            n_modes=self.num_modes, dense_gemm=self.dense_gemm,
-                           dense_rescore=self.dense_rescore, screen_slices=self.screen_slices)
+                           dense_rescore=self.dense_rescore)
         self.prob = self.estep.prob
         self.state_vals = torch.from_numpy(self._state_values).to(self.device)
         self.phaser_rot = torch.from_numpy(geometry.phaser_rotation_table(
@@ -132,7 +132,6 @@ class EMC():
         self.use_graph = config.getboolean('emc', 'cuda_graph', fallback=True)
         self.dense_gemm = config.get('emc', 'dense_gemm', fallback='auto')
         self.dense_rescore = config.getboolean('emc', 'dense_rescore', fallback=True)
-        self.screen_slices = config.get('emc', 'screen_slices', fallback='fp32')
         self.autotune = config.getboolean('emc', 'autotune', fallback=False)
 
     def _generate_states(self, config):
@@ -179,18 +178,18 @@ class EMC():
         self._host_rmax.copy_(self.estep.rmax, non_blocking=True)
         self._host_model.copy_(self._dmodel, non_blocking=True)
         torch.cuda.current_stream(self.device).synchronize()
-        try:
-            self.dset.photons.err.check('EMC iteration')
-        except Exception:
-            if self._graph is None:
-                raise
-            # a capacity limit was hit inside the graph: redo the iteration eagerly
+        err = self.dset.photons.err
+        if self._graph is not None and int(err.t.item()) == RSPI_ERR_CAPACITY:
+            # the candidate buffers sized by the eager iteration were too
+            # small inside the graph: redo the iteration eagerly (which grows
+            # them) and capture again next time; any other error is raised
+            err.t.zero_()
             self._graph = None
             self._dmodel.copy_(torch.from_numpy(np.asarray(self.model, dtype=np.complex128).ravel()))
             self._device_step()
             self._host_rmax.copy_(self.estep.rmax)
             self._host_model.copy_(self._dmodel)
-            self.dset.photons.err.check('EMC iteration')
+        err.check('EMC iteration')
         self.rmax = self._host_rmax.numpy().copy()
         self.model = self._host_model.numpy().copy().reshape(self._model_shape())
         self.save_output(self.model, iternum)

@@ -24,7 +24,7 @@ from emc import EMC  # noqa: E402
 
 
 def main(argv=None):
-    '''Parses command line arguments and launches EMC reconstruction'''
+    '''Command-line entry point: read the options, build the EMC reconstructor and run it'''
     parser = argparse.ArgumentParser(description='In-plane rotation EMC')
     parser.add_argument('num_iter', type=int, help='Number of iterations')
     parser.add_argument('-c', '--config_file', default='emc_config.ini',

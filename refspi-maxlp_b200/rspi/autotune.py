@@ -58,17 +58,12 @@ def tune(es, sample_tiles=2, repeats=2, use_cache=True, verbose=False):
         es.tile, es.warps = t, w
         return (t, w, table[key]['ms_per_row']), None
     tmax = es.lib.rspi_loglike_max_tile(es.p_row, es.slice_code)
-    screen2 = es.form == 'screen' and es.kernel == 'stream'
-    if es.form == 'screen' and es.kernel in ('frame', 'wide'):
-        tiles = (1, 2)
-    elif es.form == 'screen' and es.kernel in ('pair', 'quad'):
-        tiles = (2,)   # the frame-pair kernel: warps per CTA only
-    elif es.form == 'screen' and es.kernel == 'quad4':
+    if es.form == 'screen' and es.kernel == 'quad4':
         tiles = (4,)   # the four-row frame-quad kernel: warps per CTA only
     else:
-        tiles = (1, 2, 4) if screen2 else TILES
+        tiles = TILES
     cands = [(t, w) for t in tiles if t <= tmax for w in WARPS
-             if screen2 or es.form == 'screen' or not (t > 2 and w > 16)]
+             if es.form == 'screen' or not (t > 2 and w > 16)]
     sms = torch.cuda.get_device_properties(es.device).multi_processor_count
     rows = min(es.n_rows, es.chunk_rows, sms * sample_tiles * max(t for t, _ in cands))
     es.rot_slices(0, rows)

@@ -23,7 +23,6 @@ _f64 = torch.float64
 _i32 = torch.int32
 _i64 = torch.int64
 INT32_MAX = 2 ** 31 - 1
-PAIR_WINDOW = 256   # frames sorted by length for pairing within such windows
 QUAD4_WINDOW = 512   # frames ordered by group counts within such windows (four-row quads)
 QUAD4_SMEM = 227 * 1024 - 1024   # shared bytes of the four-row tile (kernel limit)
 QUAD4_MAX_PARTS = 4              # column parts of the four-row tile
@@ -237,20 +236,15 @@ class EStep:
     def __init__(self, photons, size, num_rot, shiftx, shifty, sphere_dia, probmask, bg,
                  form='fp64', states_per_tile=None, warps=32, n_ctas=0,
                  slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel=None,
-                 n_modes=1, dense_gemm='auto', dense_rescore=True, screen_slices='fp32',
-                 bank_layout=True, narrow_entries=True, screen_parts=None):
+                 n_modes=1, dense_gemm='auto', dense_rescore=True, screen_parts=None):
         if form not in ('fp64', 'screen', 'dense'):
             raise ValueError('form must be fp64, screen or dense')
-        auto_kernel = kernel is None
-        if kernel is None:   # default likelihood kernel of each form (the screened
-            # form's four-row frame-quad kernel is chosen below)
-            kernel = 'wide' if form == 'screen' else 'stream'
-        if screen_slices not in ('fp32', 'fp16'):
-            raise ValueError('screen_slices must be fp32 or fp16')
-        if form == 'screen' and screen_slices == 'fp16':
-            kernel = 'wide16'   # the FP16-slice kernel: four rows per tile
-        if kernel not in ('stream', 'frame', 'wide', 'wide16', 'pair', 'quad', 'quad4', 'dynamic'):
-            raise ValueError('kernel must be stream, frame, wide, pair, quad, quad4 or dynamic')
+        if kernel is None:   # default likelihood kernel of each form
+            kernel = 'quad4' if form == 'screen' else 'stream'
+        kernels = {'fp64': ('stream', 'dynamic'), 'screen': ('stream', 'quad4'),
+                   'dense': ('stream', 'tcgen05')}[form]
+        if kernel not in kernels:
+            raise ValueError('the %s form takes the kernels %s' % (form, ', '.join(kernels)))
         self.screen_parts = None if screen_parts is None else int(screen_parts)
         self.kernel = kernel
         self.lib = load()
@@ -284,57 +278,31 @@ class EStep:
         if form == 'fp64':
             self.slice_code, self.prob_code, self.p_row = 1, 1, self.p_pad
         else:
-            # FP32 slices (code 0), or FP16 slices (code 2) for the four-row kernel
-            self.slice_code, self.prob_code = (2 if kernel == 'wide16' else 0), 0
-            self.p_row = self.p_pad + 32           # 32 zero columns for padding slots
+            # FP32 slices; 32 zero columns after the likelihood columns for
+            # the padding slots of the 16-bit entries
+            self.slice_code, self.prob_code = 0, 0
+            self.p_row = self.p_pad + 32
             if self.p_row > 65536:
                 raise ValueError('screened form needs at most 65504 likelihood pixels')
             self.ll16 = photons.ll16_entries(self.pix2sel, self.p_row - 32)
             self.delta = float(delta)
-        self.slice_torch = {0: torch.float32, 1: _f64, 2: torch.float16}[self.slice_code]
+        self.slice_torch = {0: torch.float32, 1: _f64}[self.slice_code]
         self.prob_torch = torch.float32 if self.prob_code == 0 else _f64
-        tmax = self.lib.rspi_loglike_max_tile(self.p_row, self.slice_code)
-        if auto_kernel and form == 'screen' and kernel == 'wide':
-            if states_per_tile in (None, 4) and self.p_row - 32 <= QUAD4_MAX_PARTS * QUAD4_COLS:
-                kernel = self.kernel = 'quad4'
-            elif tmax >= 2 and states_per_tile in (None, 2):
-                kernel = self.kernel = 'quad'
-        if kernel == 'wide16':
-            tmax = 4 if self.p_row * 8 <= 226 * 1024 else 0
-        if form == 'screen' and kernel == 'stream':
-            tmax = 4 if tmax >= 4 else (2 if tmax >= 2 else tmax)   # interleaved: 1, 2 or 4
-        if form == 'screen' and kernel in ('frame', 'wide'):
-            tmax = min(tmax, 2)                                     # 1 or 2 rows per tile
-        if kernel in ('pair', 'quad'):
-            tmax = 2 if tmax >= 2 else 0                            # two rows per tile
         if kernel == 'quad4':
-            tmax = 4                                                # four rows, column parts
-        if form != 'screen' and kernel in ('frame', 'wide', 'wide16', 'pair', 'quad', 'quad4'):
-            raise ValueError('the %s kernel is a screened-form kernel' % kernel)
+            tmax = 4                 # four rows per tile over column parts
+            if self.p_row - 32 > QUAD4_MAX_PARTS * QUAD4_COLS:
+                raise ValueError('%d likelihood columns exceed the four-row tile' % self.n_sel)
+        else:
+            tmax = self.lib.rspi_loglike_max_tile(self.p_row, self.slice_code)
         if tmax == 0:
             raise ValueError('a %d-pixel likelihood slice does not fit in shared memory' % self.n_sel)
         self.tile = int(states_per_tile or tmax)
         if self.tile > tmax:
             raise ValueError('states_per_tile %d exceeds the shared-memory limit %d' % (self.tile, tmax))
-        if form == 'screen' and kernel == 'stream' and self.tile not in (1, 2, 4):
-            raise ValueError('the interleaved screening kernel takes 1, 2 or 4 states per tile')
-        if form == 'screen':
-            # words (two 16-bit entry rows) per frame decide how many of a
-            # frame's words the frame-at-a-time kernel prefetches
-            wpf = self.ll16['total_rows'] / 2. / max(1, photons.num_data)
-            self.prefetch_words = 4 if wpf <= 5 else (8 if wpf <= 10 else 12)
-        if kernel == 'wide16' and self.tile != 4:
-            raise ValueError('the FP16-slice kernel takes 4 states per tile')
-        if kernel in ('pair', 'quad') and self.tile != 2:
-            raise ValueError('the multi-frame kernels take 2 states per tile')
         if kernel == 'quad4' and self.tile != 4:
             raise ValueError('the four-row frame-quad kernel takes 4 states per tile')
-        self.bank_layout = bool(bank_layout)
-        self.narrow_entries = bool(narrow_entries)
         self.warps, self.n_ctas = int(warps), int(n_ctas)
-        self.wide = self._wide_entries() if (form == 'screen' and
-                                             kernel in ('wide', 'wide16', 'pair', 'quad',
-                                                        'quad4')) else None
+        self.wide = self._quad4_entries() if kernel == 'quad4' else None
         self._eps_key, self.row_off_eps = None, None
         esz = {0: 4, 1: 8, 2: 2}[self.slice_code]
         rows = max(self.tile, (slice_budget_bytes // (self.p_row * esz)) // self.tile * self.tile)
@@ -442,46 +410,6 @@ class EStep:
         self.check_capacity = True
         self.ll_events = None
 
-    def _wide_bytes_tile(self):
-        """Tile whose entries the kernel reads: offsets sel * 8 serve both the
-        FP32 two-row and the FP16 four-row tiles."""
-        return 2 if self.kernel == 'wide16' else self.tile
-
-    def _pair_entries(self):
-        """Frame groups for the multi-frame kernels (``pair``: two frames per
-        warp, 16 lanes each; ``quad``: four, 8 lanes each): within each window
-        of PAIR_WINDOW consecutive frames, frames sorted by their group count
-        (longest first) and taken F at a time, so that a warp's likelihood
-        stores stay within a few sectors of each row; the 16-bit bank-class
-        entries of the F frames of a group in one group range."""
-        l16, n, dev, s = self.ll16, self.ph.num_data, self.device, cur_stream()
-        nf = 4 if self.kernel == 'quad' else 2
-        fn = 'quad' if nf == 4 else 'pair'
-        pz = self.p_row - 32
-        ng = torch.empty(n, dtype=_i32, device=dev)
-        call('rspi_%s_entry_groups' % fn, ptr(l16['entries']), ptr(l16['row_off']), n, pz, ptr(ng),
-             s)
-        gmax = int(ng.max().item())
-        win = torch.arange(n, device=dev, dtype=_i64) // PAIR_WINDOW
-        order = torch.argsort(win * (gmax + 1) + (gmax - ng.to(_i64)), stable=True).to(_i32)
-        n_sets = (n + nf - 1) // nf
-        set_frames = torch.full((nf * n_sets,), -1, dtype=_i32, device=dev)
-        set_frames[:n] = order
-        set_slot = torch.empty(n, dtype=_i32, device=dev)
-        set_slot[order.long()] = torch.arange(n, dtype=_i32, device=dev)
-        ngs = torch.zeros(nf * n_sets, dtype=_i32, device=dev)
-        ngs[:n] = ng[order.long()]
-        sng = ngs.view(n_sets, nf).amax(1).contiguous()
-        soff = torch.empty(n_sets + 1, dtype=_i64, device=dev)
-        call('rspi_scan_rows', ptr(sng), n_sets, ptr(soff), s)
-        total = int(soff[-1].item())
-        narrow = torch.empty(max(1, total) * 128, dtype=torch.int16, device=dev)
-        call('rspi_%s_entry_fill' % fn, ptr(l16['entries']), ptr(l16['row_off']), n, pz,
-             ptr(set_slot), ptr(soff), total, ptr(narrow), s)
-        return dict(entries=narrow, group_off=soff, total_groups=total, tile=2, banked=True,
-                    narrow=True, pairs=True, frames_per=nf, pair_frames=set_frames,
-                    n_pairs=n_sets, frame_groups=sng[(set_slot // nf).long()])
-
     def _quad4_parts(self):
         """Column parts of the four-row tile (``quad4_parts``), or
         ``screen_parts`` parts."""
@@ -534,59 +462,17 @@ class EStep:
                     n_pairs=nq, frame_groups=sng.amax(1)[(set_slot // 4).long()],
                     n_parts=parts, part_w=part_w, part_sums=ps, part_sums_ctas=ps_ctas)
 
-    def _wide_entries(self):
-        """32-bit entries holding each photon's byte offset in the
-        interleaved tile (sel * 4 * tile), four rows of a lane per 16-byte
-        group, rows of a frame padded to a multiple of four."""
-        if self.kernel in ('pair', 'quad'):
-            return self._pair_entries()
-        if self.kernel == 'quad4':
-            return self._quad4_entries()
-        l16, n, dev, s = self.ll16, self.ph.num_data, self.device, cur_stream()
-        groups = torch.empty(n, dtype=_i32, device=dev)
-        bt, pz = self._wide_bytes_tile(), self.p_row - 32
-        if self.bank_layout:
-            call('rspi_wide_entry_groups_banked', ptr(l16['entries']), ptr(l16['row_off']), n,
-                 pz, bt, ptr(groups), s)
-        else:
-            call('rspi_wide_entry_groups', ptr(l16['row_off']), n, ptr(groups), s)
-        goff = torch.empty(n + 1, dtype=_i64, device=dev)
-        call('rspi_scan_rows', ptr(groups), n, ptr(goff), s)
-        total = int(goff[-1].item())
-        wide = torch.empty(max(1, total) * 128, dtype=torch.int32, device=dev)
-        narrow = self.bank_layout and self.narrow_entries and self.kernel == 'wide'
-        if narrow:
-            wide = torch.empty(max(1, total) * 128, dtype=torch.int16, device=dev)
-            call('rspi_wide_entry_fill_narrow', ptr(l16['entries']), ptr(l16['row_off']), n, pz,
-                 bt, ptr(goff), ptr(wide), s)
-        else:
-            wide = torch.empty(max(1, total) * 128, dtype=torch.int32, device=dev)
-            fill = 'rspi_wide_entry_fill_banked' if self.bank_layout else 'rspi_wide_entry_fill'
-            call(fill, ptr(l16['entries']), ptr(l16['row_off']), n, pz, bt, ptr(goff), ptr(wide),
-                 s)
-        return dict(entries=wide, group_off=goff, total_groups=total, tile=bt,
-                    banked=self.bank_layout, narrow=narrow)
-
     def _eps_rows(self):
         """Prefix sums of each frame's FP32 summation length for the
         candidate threshold's eps_d (the 'rows' of 2^-24 (rows + 8) photons
-        lmax): the frame's 16-bit entry rows, or its groups in the bank-class
-        layout when that is longer (a lane then adds one group's pair sum per
-        step); with FP16 slices 8192 more per photon (storage error <=
-        2^-11 |L| per value)."""
+        lmax): the frame's 16-bit entry rows, or the summation length of the
+        kernel's entry layout when that is longer."""
         key = (self.kernel, None if self.wide is None else self.wide['entries'].data_ptr())
         if key != self._eps_key:
             ro = self.ll16['row_off']
             rows = ro[1:] - ro[:-1]
-            if self.kernel in ('pair', 'quad', 'quad4') and self.wide is not None and \
-                    self.wide.get('pairs'):
+            if self.wide is not None:
                 rows = torch.maximum(rows, self.wide['frame_groups'].to(_i64))
-            elif self.kernel in ('wide', 'wide16') and self.wide is not None and \
-                    self.wide['banked']:
-                go = self.wide['group_off']
-                rows = torch.maximum(rows, go[1:] - go[:-1])
-            if self.kernel == 'wide16':
-                rows = rows + 8192
             self.row_off_eps = torch.cat([torch.zeros(1, dtype=_i64, device=self.device),
                                           torch.cumsum(rows, 0)])
             self._eps_key = key
@@ -630,12 +516,7 @@ class EStep:
             call('rspi_holo_pairs', ptr(self.holo), self.n_states0, self.size,
                  ptr(self.holo_pairs), s)
         if self.form != 'fp64':
-            # the FP16 bound needs |L| >= 2^-14 (below it the absolute error
-            # 2^-25 is covered by 2^-11 * 2^-14)
-            if self.kernel == 'wide16':
-                self.lmax.fill_(2. ** -14)
-            else:
-                self.lmax.zero_()
+            self.lmax.zero_()
 
     def rot_slices(self, r0, r1, out=None):
         """a6: rotated log-slices of rows [r0, r1) into ``out`` (or the chunk buffer)."""
@@ -682,10 +563,6 @@ class EStep:
                  ptr(self.lsl_lo), self.k_pad, n, self.chunk_rows, self.num_rot, r0, r1,
                  ptr(self.init), ptr(self.ph.scales), ptr(self.prob[r0]), n, ptr(self.ph.err.t),
                  cur_stream())
-        elif self.kernel == 'wide16' and self.form == 'screen':
-            call('rspi_screen_loglike4h', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
-                 ptr(self.ph.scales), ptr(self.wide['entries']), ptr(self.wide['group_off']), n,
-                 r0, r1, ptr(self.prob[r0]), n, self.warps, self.n_ctas, cur_stream())
         elif self.kernel == 'quad4' and self.form == 'screen':
             w = self.wide
             if w is None or not w.get('quad4') or (w['n_parts'] > 1 and self.n_ctas > 0 and
@@ -696,33 +573,9 @@ class EStep:
                  ptr(w['pair_frames']), w['n_pairs'], w['n_parts'], w['part_w'], r0, r1,
                  ptr(self.prob[r0]), n, ptr(w['part_sums']), w['part_sums_ctas'], self.warps,
                  self.n_ctas, cur_stream())
-        elif self.kernel in ('pair', 'quad') and self.form == 'screen':
-            nf = 4 if self.kernel == 'quad' else 2
-            if self.wide is None or self.wide.get('frames_per') != nf or self.wide.get('quad4'):
-                self.wide = self._pair_entries()
-            call('rspi_screen_loglike6' if nf == 4 else 'rspi_screen_loglike5', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
-                 ptr(self.ph.scales), ptr(self.wide['entries']), ptr(self.wide['group_off']),
-                 ptr(self.wide['pair_frames']), self.wide['n_pairs'], r0, r1, ptr(self.prob[r0]), n,
-                 self.warps, self.n_ctas, cur_stream())
-        elif self.kernel == 'wide' and self.form == 'screen':
-            if self.wide is None or self.wide.get('pairs') or self.wide['tile'] != self.tile or \
-                    self.wide['banked'] != self.bank_layout or \
-                    self.wide['narrow'] != (self.bank_layout and self.narrow_entries):
-                self.wide = self._wide_entries()   # kernel, tile or layout changed
-            entry = 'rspi_screen_loglike4n' if self.wide['narrow'] else 'rspi_screen_loglike4'
-            call(entry, ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
-                 ptr(self.ph.scales), ptr(self.wide['entries']), ptr(self.wide['group_off']), n,
-                 r0, r1, ptr(self.prob[r0]), n, self.tile, self.warps, self.n_ctas,
-                 cur_stream())
-        elif self.kernel == 'frame' and self.form == 'screen':
-            l16 = self.ll16
-            call('rspi_screen_loglike3', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
-                 ptr(self.ph.scales), ptr(l16['entries']), ptr(l16['row_off']), n, r0, r1,
-                 ptr(self.prob[r0]), n, self.tile, self.prefetch_words, self.warps, self.n_ctas,
-                 cur_stream())
         elif self.kernel == 'stream' and self.form == 'screen':
             l16 = self.ll16
-            call('rspi_screen_loglike2', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
+            call('rspi_loglike_stream', 0, ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
                  ptr(self.ph.scales), ptr(l16['entries']), ptr(l16['row_off']), n, r0, r1,
                  ptr(self.prob[r0]), n, self.tile, self.warps, self.n_ctas, cur_stream())
         elif self.kernel == 'stream':
@@ -731,18 +584,12 @@ class EStep:
                  ptr(self.init), ptr(self.ph.scales), ptr(ent['entries']), ptr(ent['row_off']),
                  n, r0, r1, ptr(self.prob[r0]), n, self.tile, self.warps, self.n_ctas,
                  cur_stream())
-        elif self.form == 'fp64':
+        else:
             ll = self.ll
             call('rspi_loglike', ptr(lsl), self.slice_code, self.p_row, self.num_rot,
                  ptr(self.init), ptr(self.ph.scales), ptr(ll['entries']), ptr(ll['row_off']),
                  ptr(ll['order']), n, r0, r1, ptr(self.prob[r0]), self.prob_code, n, self.tile,
                  self.warps, self.n_ctas, cur_stream())
-        else:
-            l16 = self.ll16
-            call('rspi_screen_loglike', ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
-                 ptr(self.ph.scales), ptr(l16['entries']), ptr(l16['row_off']),
-                 ptr(l16['order']), n, r0, r1, ptr(self.prob[r0]), n, self.tile, self.warps,
-                 self.n_ctas, cur_stream())
 
     def run(self, model):
         """Full likelihood matrix ``prob`` for ``model`` (a4-a7)."""

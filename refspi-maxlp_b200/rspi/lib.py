@@ -40,12 +40,6 @@ SIGNATURES = {
     'rspi_maxlp_pixel_values': (I, [P, L, P, P, L, I, D, P, P, P]),
     'rspi_maxlp_fcalc': (I, [L, D, D, D, P, P, P, P]),
     'rspi_sphere_ramp': (I, [L, D, D, D, P, P, P]),
-    'rspi_pair_entry_groups': (I, [P, P, L, I, P, P]),
-    'rspi_pair_entry_fill': (I, [P, P, L, I, P, P, L, P, P]),
-    'rspi_screen_loglike5': (I, [P, L, L, P, P, P, P, P, L, L, L, P, L, I, I, P]),
-    'rspi_quad_entry_groups': (I, [P, P, L, I, P, P]),
-    'rspi_quad_entry_fill': (I, [P, P, L, I, P, P, L, P, P]),
-    'rspi_screen_loglike6': (I, [P, L, L, P, P, P, P, P, L, L, L, P, L, I, I, P]),
     'rspi_quad4_entry_groups': (I, [P, P, L, I, I, I, P, P]),
     'rspi_quad4_entry_fill': (I, [P, P, L, I, I, I, P, P, L, L, P, P]),
     'rspi_quad4_part_sums_floats': (L, [L, I]),
@@ -53,23 +47,12 @@ SIGNATURES = {
     'rspi_mean': (I, [P, L, P, P]),
     'rspi_ll16_entry_rows': (I, [P] * 8 + [L, L, I, P, P, P]),
     'rspi_ll16_entry_fill': (I, [P] * 8 + [L, L, I, P, P, P]),
-    'rspi_screen_loglike': (I, [P, L, L, P, P, P, P, P, L, L, L, P, L, I, I, I, P]),
     'rspi_screen_candidates': (I, [P, L, L, P, P, P, P, P, D, P, P, P, P, P, L, P, P, P, P]),
     'rspi_rescore': (I, [P, P, P, L, L, L, P, L, P, L, P, P, L, L, P, P, P, P, P, P, P, P, P,
                          P, P, P, P, P, P, L, P]),
     'rspi_screen_candidates_noalloc': (I, [P, L, L, P, P, P, P, P, D, P, P, P, P, L, P, P, P,
                                            P]),
     'rspi_nll': (I, [I, I] + [P] * 7 + [L, P, L, P, L] + [P] * 18),
-    'rspi_screen_loglike2': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
-    'rspi_screen_loglike3': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, I, P]),
-    'rspi_screen_loglike4': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
-    'rspi_screen_loglike4n': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
-    'rspi_wide_entry_fill_narrow': (I, [P, P, L, I, I, P, P, P]),
-    'rspi_screen_loglike4h': (I, [P, L, L, P, P, P, P, L, L, L, P, L, I, I, P]),
-    'rspi_wide_entry_groups': (I, [P, L, P, P]),
-    'rspi_wide_entry_fill': (I, [P, P, L, I, I, P, P, P]),
-    'rspi_wide_entry_groups_banked': (I, [P, P, L, I, I, P, P]),
-    'rspi_wide_entry_fill_banked': (I, [P, P, L, I, I, P, P, P]),
     'rspi_entries16_check': (I, [P, L, P, P]),
     'rspi_loglike_stream': (I, [I, P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
     'rspi_posterior_pairs': (I, [P, L, L, P, D, P, P, P, L, P, P, P, P, P]),
@@ -126,20 +109,14 @@ KERNELS_PER_CALL = {
     'rspi_maxlp_frame_params': 1, 'rspi_maxlp_histogram': 1, 'rspi_maxlp_pattern': 1,
     'rspi_maxlp_pattern_screened': 1, 'rspi_log2_error_max': 1,
     'rspi_maxlp_pixel_frames': 1, 'rspi_maxlp_pixel_values': 1, 'rspi_maxlp_fcalc': 1,
-    'rspi_sphere_ramp': 1, 'rspi_pair_entry_groups': 1, 'rspi_pair_entry_fill': 2,
-    'rspi_screen_loglike5': 1, 'rspi_quad_entry_groups': 1, 'rspi_quad_entry_fill': 2,
-    'rspi_screen_loglike6': 1, 'rspi_quad4_entry_groups': 1, 'rspi_quad4_entry_fill': 2,
+    'rspi_sphere_ramp': 1, 'rspi_quad4_entry_groups': 1, 'rspi_quad4_entry_fill': 2,
     'rspi_screen_loglike7': 1, 'rspi_quad4_part_sums_floats': 0,
-    'rspi_mean': 1, 'rspi_ll16_entry_rows': 1, 'rspi_ll16_entry_fill': 1,
-    'rspi_screen_loglike': 1, 'rspi_screen_candidates': 3, 'rspi_rescore': 5,
-    'rspi_loglike_stream': 1, 'rspi_posterior_pairs': 3, 'rspi_screen_loglike2': 1,
+    'rspi_mean': 1, 'rspi_ll16_entry_rows': 1, 'rspi_ll16_entry_fill': 1, 'rspi_screen_candidates': 3, 'rspi_rescore': 5,
+    'rspi_loglike_stream': 1, 'rspi_posterior_pairs': 3,
     'rspi_entries16_check': 1, 'rspi_nll': 2, 'rspi_screen_candidates_noalloc': 3, 'rspi_merge_coverage': 1, 'rspi_merge': 2,
     'rspi_dense_frames': 1, 'rspi_rot_log_split': 1, 'rspi_dense_loglike': 1,
     'rspi_maxlp_grid': 2, 'rspi_dense_frames_u8': 1, 'rspi_rot_log_fixed': 1,
-    'rspi_dense_loglike_i8': 1, 'rspi_screen_loglike3': 1, 'rspi_screen_loglike4': 1,
-    'rspi_wide_entry_groups': 1, 'rspi_wide_entry_fill': 1,
-    'rspi_wide_entry_groups_banked': 1, 'rspi_wide_entry_fill_banked': 1,
-    'rspi_screen_loglike4n': 1, 'rspi_wide_entry_fill_narrow': 1, 'rspi_screen_loglike4h': 1,
+    'rspi_dense_loglike_i8': 1,
 }
 launch_count = 0
 

@@ -86,6 +86,21 @@ def test_ll_entry_lists_bit_exact(name, ds, need_scaling):
     assert np.all(np.diff(rows[order]) <= 0)
 
 
+def frame_photons16(es):
+    """Each frame's sorted likelihood-column indices, one per photon (counts
+    expanded), read from the 16-bit entry rows of ``es``."""
+    l16 = es.ll16
+    ent = l16['entries'].cpu().numpy().view(np.uint16).astype(np.int64)
+    off = l16['row_off'].cpu().numpy()
+    pz = es.p_row - 32
+    out = []
+    for d in range(off.size - 1):
+        rows = [ent[(r >> 1) * 64 + 2 * np.arange(32) + (r & 1)] for r in range(off[d], off[d + 1])]
+        v = np.concatenate(rows) if rows else np.zeros(0, np.int64)
+        out.append(np.sort(v[v < pz]))
+    return out
+
+
 def _golden_estep(g, **kw):
     ds = golden_dataset(g)
     size, num_rot = int(g['size']), int(g['num_rot'])
@@ -194,21 +209,24 @@ def test_screen_candidates_cover_posterior_mass():
     np.testing.assert_allclose(cl, want[cr, cd], rtol=RTOL_F64)
 
 
-@pytest.mark.parametrize('kernel', ['stream', 'dynamic'])
-@pytest.mark.parametrize('form', ['fp64', 'screen'])
+@pytest.mark.parametrize('form,kernel', [('fp64', 'stream'), ('fp64', 'dynamic'),
+                                         ('screen', 'stream')])
 @pytest.mark.parametrize('tile,warps', [(1, 1), (2, 4), (3, 32), (1, 7), (8, 16), (4, 32)])
 def test_tiling_does_not_change_results(tile, warps, form, kernel):
     g = load_golden('case_a')
-    if form == 'screen' and kernel == 'stream' and tile not in (1, 2, 4):
-        with pytest.raises(ValueError):
-            _golden_estep(g, states_per_tile=tile, warps=warps, form=form, kernel=kernel)
-        return
-    _, ref = _golden_estep(g, form=form)
+    _, ref = _golden_estep(g, form=form, kernel=kernel)
     ref.run(torch.from_numpy(g['model_in_1']).cuda())
     _, es = _golden_estep(g, states_per_tile=tile, warps=warps, form=form, kernel=kernel)
     es.run(torch.from_numpy(g['model_in_1']).cuda())
     rtol = 1e-14 if form == 'fp64' else 1e-6
     np.testing.assert_allclose(es.prob.cpu().numpy(), ref.prob.cpu().numpy(), rtol=rtol)
+
+
+def test_kernel_choice_is_checked():
+    g = load_golden('case_a')
+    for form, kernel in (('screen', 'dynamic'), ('fp64', 'quad4'), ('screen', 'wide')):
+        with pytest.raises(ValueError):
+            _golden_estep(g, form=form, kernel=kernel)
 
 
 @pytest.mark.parametrize('name', GOLDEN_CASES)
@@ -265,54 +283,9 @@ def test_random_shapes_vs_oracle(size, n, seed, kw, form):
     assert np.array_equal(rmax.cpu().numpy(), want_rmax)
 
 
-@pytest.mark.parametrize('tile,warps', [(1, 1), (2, 4), (2, 32), (1, 7), (2, 3)])
-@pytest.mark.parametrize('name,ds,need_scaling', CASES, ids=[c[0] for c in CASES])
-def test_frame_kernel_matches_stream_kernel(name, ds, need_scaling, tile, warps):
-    """The frame-at-a-time and wide-entry screening kernels (wide entries in
-    the bank-class layout, 16- or 32-bit, and in the plain layout) give the
-    interleaved kernel's
-    FP32 likelihoods (other summation order: within 1e-6 relative of the
-    largest term) on every case, empty and heavy frames included, and the
-    same FP64-rescored argmax / maximum / log-sum-exp."""
-    size = int(round(np.sqrt(ds['num_pix'])))
-    num_rot = 5
-    sx, sy, dia, _ = E.generate_states(E.parse_triple('-1 1 3'), E.parse_triple('0 0 1'),
-                                       E.parse_triple('2 3 2'))
-    rng = np.random.default_rng(size)
-    model = torch.from_numpy(rng.random(size * size) + 1j * rng.random(size * size)).cuda()
-    out = {}
-    variants = (('stream', True, True), ('frame', True, True), ('wide', True, True),
-                ('wide', True, False), ('wide', False, False))
-    if tile == 2:
-        variants += (('pair', True, True), ('quad', True, True))
-    for kernel, banked, narrow in variants:
-        ph = _photons(ds, need_scaling)
-        es = _estep(ph, size, num_rot, sx, sy, dia, ds['bg'], form='screen', kernel=kernel,
-                    states_per_tile=tile, warps=warps, bank_layout=banked,
-                    narrow_entries=narrow)
-        es.run(model)
-        maxll, rmax, logz = es.reduce()
-        torch.cuda.synchronize()
-        out[kernel, banked, narrow] = (es.prob.cpu().numpy().astype(np.float64),
-                                       maxll.cpu().numpy(), rmax.cpu().numpy(),
-                                       logz.cpu().numpy())
-    a = out['stream', True, True]
-    scale = np.abs(a[0]).max(0, keepdims=True) + 1.
-    # the 16-bit and 32-bit bank-class entries give the same sums in the same order
-    assert np.array_equal(out['wide', True, True][0], out['wide', True, False][0])
-    others = [out['frame', True, True], out['wide', True, True], out['wide', False, False]]
-    if tile == 2:
-        others += [out['pair', True, True], out['quad', True, True]]
-    for b in others:
-        assert np.all(np.abs(a[0] - b[0]) <= 1e-6 * scale)
-        assert np.array_equal(a[2], b[2])
-        np.testing.assert_allclose(a[1], b[1], rtol=1e-14)
-        np.testing.assert_allclose(a[3], b[3], rtol=1e-12)
-
-
-@pytest.mark.parametrize('kernel', ['frame', 'wide'])
+@pytest.mark.parametrize('kernel', ['stream', 'quad4'])
 @pytest.mark.parametrize('name', GOLDEN_CASES)
-def test_frame_kernel_screened_form_matches_reference(name, kernel):
+def test_screen_kernels_match_reference(name, kernel):
     g = load_golden(name)
     _, es = _golden_estep(g, form='screen', kernel=kernel)
     for it in (1, 2):
@@ -322,186 +295,6 @@ def test_frame_kernel_screened_form_matches_reference(name, kernel):
         assert (np.abs(screened - want) / np.abs(want)).max() <= RTOL_F32
         _, rmax, _ = es.reduce()
         assert np.array_equal(rmax.cpu().numpy(), g['rmax_%d' % it])
-
-
-@pytest.mark.parametrize('name,ds,need_scaling', CASES, ids=[c[0] for c in CASES])
-def test_fp16_slices_same_rescored_results(name, ds, need_scaling):
-    """FP16 slices (four rows per gather): the screening values within their
-    stated bound of the FP32 ones, and after FP64 rescoring the same argmax,
-    maximum and log-sum-exp as the FP32-slice screened form."""
-    size = int(round(np.sqrt(ds['num_pix'])))
-    num_rot = 5
-    sx, sy, dia, _ = E.generate_states(E.parse_triple('-1 1 3'), E.parse_triple('0 0 1'),
-                                       E.parse_triple('2 3 2'))
-    rng = np.random.default_rng(size + 1)
-    model = torch.from_numpy(rng.random(size * size) + 1j * rng.random(size * size)).cuda()
-    out = {}
-    for sl in ('fp32', 'fp16'):
-        ph = _photons(ds, need_scaling)
-        es = _estep(ph, size, num_rot, sx, sy, dia, ds['bg'], form='screen', screen_slices=sl)
-        es.run(model)
-        maxll, rmax, logz = es.reduce()
-        torch.cuda.synchronize()
-        out[sl] = (es.prob.cpu().numpy().astype(np.float64), maxll.cpu().numpy(),
-                   rmax.cpu().numpy(), logz.cpu().numpy(), float(es.lmax.item()))
-        if sl == 'fp16':
-            assert es.tile == 4 and es.kernel == 'wide16'
-            phot = es.ll['frame_sel_photons'].cpu().numpy().astype(np.float64)
-    a, b = out['fp32'], out['fp16']
-    # FP16 storage: |dL| <= 2^-11 lmax per photon, plus FP32 sums
-    bound = 2. ** -11 * b[4] * phot[None, :] + 1e-5 * (np.abs(a[0]) + 1.)
-    assert np.all(np.abs(a[0] - b[0]) <= bound)
-    assert np.array_equal(a[2], b[2])
-    np.testing.assert_allclose(a[1], b[1], rtol=1e-14)
-    np.testing.assert_allclose(a[3], b[3], rtol=1e-9)
-
-
-@pytest.mark.parametrize('name', GOLDEN_CASES)
-def test_fp16_slices_match_reference(name):
-    g = load_golden(name)
-    _, es = _golden_estep(g, form='screen', screen_slices='fp16')
-    for it in (1, 2):
-        es.run(torch.from_numpy(g['model_in_%d' % it]).cuda())
-        _, rmax, _ = es.reduce()
-        assert np.array_equal(rmax.cpu().numpy(), g['rmax_%d' % it])
-
-
-@pytest.mark.parametrize('tile', [1, 2])
-def test_bank_layout_entries(tile):
-    """The bank-class layout holds every photon of every frame once (as the
-    plain layout does) and every other slot is the lane's zero column; lane l
-    only holds tile columns of bank class l mod (32 / tile)."""
-    size, n = 37, 60
-    d = random_photons(size, n, 40. * size, 9, empty_frames=(2,), heavy=5)
-    ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
-                         d['count_multi'], size * size, False)
-    sx, sy, dia, _ = E.generate_states(E.parse_triple('0 0 1'), E.parse_triple('0 0 1'),
-                                       E.parse_triple('2 2 1'))
-    got = {}
-    bpp = 4 * tile
-    classes = 32 // tile
-    lanes = np.arange(32)[None, :, None]
-    for banked, narrow in ((True, True), (True, False), (False, False)):
-        es = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen', kernel='wide',
-                    states_per_tile=tile, bank_layout=banked, narrow_entries=narrow)
-        torch.cuda.synchronize()
-        if narrow:   # q per slot: column q * C + (lane mod C)
-            q = es.wide['entries'].cpu().numpy().view(np.uint16).reshape(-1, 32, 4).astype(np.int64)
-            sel = q * classes + lanes % classes
-        else:
-            sel = es.wide['entries'].cpu().numpy().view(np.uint32).reshape(-1, 32, 4) // bpp
-        got[banked, narrow] = (sel, es.wide['group_off'].cpu().numpy(), es.p_row - 32)
-    assert np.array_equal(got[True, True][0], got[True, False][0])
-    assert np.array_equal(got[True, True][1], got[True, False][1])
-    (wb, gb, pz), (wp, gp, _) = got[True, False], got[False, False]
-    for f in range(n):
-        eb = wb[gb[f]:gb[f + 1]]
-        ep = wp[gp[f]:gp[f + 1]]
-        realb, realp = eb[eb < pz], ep[ep < pz]
-        assert np.array_equal(np.sort(realb), np.sort(realp)), f
-        assert np.all((eb >= pz) <= (eb == pz + lanes)), f
-        assert np.all(eb % classes == np.broadcast_to(lanes, eb.shape) % classes), f
-
-
-@pytest.mark.parametrize('n', [61, 200])
-def test_pair_layout_entries(n):
-    """Frame pairs: every frame's photons once, in its half-warp, one bank
-    class per lane, the zero column elsewhere; frames paired within windows
-    of consecutive frames (longest first)."""
-    from rspi.device import PAIR_WINDOW
-    size = 37
-    d = random_photons(size, n, 40. * size, 12, empty_frames=(2, 9), heavy=5)
-    ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
-                         d['count_multi'], size * size, False)
-    sx, sy, dia, _ = E.generate_states(E.parse_triple('0 0 1'), E.parse_triple('0 0 1'),
-                                       E.parse_triple('2 2 1'))
-    es_p = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen',
-                  kernel='pair', states_per_tile=2)
-    es_w = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen',
-                  kernel='wide', states_per_tile=2, narrow_entries=False)
-    torch.cuda.synchronize()
-    w = es_p.wide
-    pz = es_p.p_row - 32
-    q = w['entries'].cpu().numpy().view(np.uint16).reshape(-1, 32, 4).astype(np.int64)
-    lanes = np.arange(32)[None, :, None]
-    sel = q * 16 + lanes % 16
-    pgoff = w['group_off'].cpu().numpy()
-    pf = w['pair_frames'].cpu().numpy()
-    assert w['n_pairs'] == (n + 1) // 2 and np.all(np.diff(pgoff) >= 0)
-    wide = es_w.wide['entries'].cpu().numpy().view(np.uint32).reshape(-1, 32, 4) // 8
-    goff = es_w.wide['group_off'].cpu().numpy()
-    seen = []
-    for p in range(w['n_pairs']):
-        blk = sel[pgoff[p]:pgoff[p + 1]]
-        for h in range(2):
-            f = pf[2 * p + h]
-            half = blk[:, 16 * h:16 * h + 16]
-            if f < 0:
-                assert np.all(half >= pz)
-                continue
-            seen.append(f)
-            real = np.sort(half[half < pz])
-            ref = wide[goff[f]:goff[f + 1]]
-            assert np.array_equal(real, np.sort(ref[ref < pz])), f
-            pads = half >= pz
-            want = np.broadcast_to(pz + lanes[:, 16 * h:16 * h + 16], half.shape)
-            assert np.array_equal(half[pads], want[pads])
-    assert sorted(seen) == list(range(n))
-    # pairing stays inside windows of consecutive frames
-    assert np.all(pf[:n] // PAIR_WINDOW == np.arange(n) // PAIR_WINDOW)
-
-
-@pytest.mark.parametrize('n', [61, 300])
-def test_quad_layout_entries(n):
-    """Frame quads: every frame's photons once, in its eight lanes; lane j of
-    sub-frame u holds classes j and j + 8 in alternating slots (phases
-    swapped on odd u), so each half-warp gather covers 16 distinct classes;
-    zero columns of the slot's class elsewhere."""
-    from rspi.device import PAIR_WINDOW
-    size = 37
-    d = random_photons(size, n, 40. * size, 13, empty_frames=(2, 9), heavy=5)
-    ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
-                         d['count_multi'], size * size, False)
-    sx, sy, dia, _ = E.generate_states(E.parse_triple('0 0 1'), E.parse_triple('0 0 1'),
-                                       E.parse_triple('2 2 1'))
-    es_q = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen',
-                  kernel='quad', states_per_tile=2)
-    es_w = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen',
-                  kernel='wide', states_per_tile=2, narrow_entries=False)
-    torch.cuda.synchronize()
-    w = es_q.wide
-    pz = es_q.p_row - 32
-    q = w['entries'].cpu().numpy().view(np.uint16).reshape(-1, 32, 4).astype(np.int64)
-    lane = np.arange(32)[:, None]
-    slot = np.arange(4)[None, :]
-    u, j = lane // 8, lane % 8
-    cls = j + 8 * ((slot % 2) ^ (u % 2))                      # (32, 4)
-    sel = q * 16 + cls[None]
-    for hw in range(2):                                       # conflict-free half-warps
-        for sl in range(4):
-            assert len(set(cls[16 * hw:16 * hw + 16, sl])) == 16
-    goff = w['group_off'].cpu().numpy()
-    qf = w['pair_frames'].cpu().numpy()
-    assert w['frames_per'] == 4 and w['n_pairs'] == (n + 3) // 4
-    wide = es_w.wide['entries'].cpu().numpy().view(np.uint32).reshape(-1, 32, 4) // 8
-    woff = es_w.wide['group_off'].cpu().numpy()
-    seen = []
-    for qd in range(w['n_pairs']):
-        blk = sel[goff[qd]:goff[qd + 1]]
-        for uu in range(4):
-            f = qf[4 * qd + uu]
-            part = blk[:, 8 * uu:8 * uu + 8]
-            if f < 0:
-                assert np.all(part >= pz)
-                continue
-            seen.append(f)
-            ref = wide[woff[f]:woff[f + 1]]
-            assert np.array_equal(np.sort(part[part < pz]), np.sort(ref[ref < pz])), f
-            pads = part >= pz
-            want = np.broadcast_to(pz + cls[8 * uu:8 * uu + 8][None], part.shape)
-            assert np.array_equal(part[pads], want[pads])
-    assert sorted(seen) == list(range(n))
-    assert np.all(qf[:n] // PAIR_WINDOW == np.arange(n) // PAIR_WINDOW)
 
 
 @pytest.mark.parametrize('parts,warps', [(None, 32), (2, 24), (3, 7), (4, 32)])
@@ -554,8 +347,6 @@ def test_quad4_layout_entries(n, parts):
                                        E.parse_triple('2 2 1'))
     es_q = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen',
                   kernel='quad4', states_per_tile=4, screen_parts=parts)
-    es_w = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen',
-                  kernel='wide', states_per_tile=2, narrow_entries=False)
     torch.cuda.synchronize()
     w = es_q.wide
     pz = es_q.p_row - 32
@@ -567,8 +358,7 @@ def test_quad4_layout_entries(n, parts):
     goff = w['group_off'].cpu().numpy()
     qf = w['pair_frames'].cpu().numpy()
     assert nq == (n + 3) // 4 and goff.size == parts * nq + 1 and np.all(np.diff(goff) >= 0)
-    wide = es_w.wide['entries'].cpu().numpy().view(np.uint32).reshape(-1, 32, 4) // 8
-    woff = es_w.wide['group_off'].cpu().numpy()
+    photons = frame_photons16(es_q)
     seen = []
     for qd in range(nq):
         for uu in range(4):
@@ -585,8 +375,7 @@ def test_quad4_layout_entries(n, parts):
             if f < 0:
                 continue
             seen.append(f)
-            ref = wide[woff[f]:woff[f + 1]]
-            assert np.array_equal(np.sort(np.concatenate(got)), np.sort(ref[ref < pz])), f
+            assert np.array_equal(np.sort(np.concatenate(got)), photons[f]), f
     assert sorted(seen) == list(range(n))
     assert np.all(qf[:n] // QUAD4_WINDOW == np.arange(n) // QUAD4_WINDOW)
     # each (quad, part) range is as long as its longest frame needs
@@ -595,14 +384,14 @@ def test_quad4_layout_entries(n, parts):
             fr = [f for f in qf[4 * qd:4 * qd + 4] if f >= 0]
             need = 0
             for f in fr:
-                ref = wide[woff[f]:woff[f + 1]]
-                cols = ref[(ref < pz) & (ref // pw == h)] % pw
+                ref = photons[f]
+                cols = ref[ref // pw == h] % pw
                 if cols.size:
                     need = max(need, -(-np.bincount(cols % 8, minlength=8).max() // 4))
             assert goff[h * nq + qd + 1] - goff[h * nq + qd] == need
 
 
-@pytest.mark.parametrize('dtype,code', [(torch.float32, 0), (torch.float64, 1), (torch.float16, 2)])
+@pytest.mark.parametrize('dtype,code', [(torch.float32, 0), (torch.float64, 1)])
 def test_paired_holo_slices_bit_identical(dtype, code):
     """rspi_rot_log_slices_pairs (two 16-byte loads per bilinear sample from
     the paired copy) gives the bits of rspi_rot_log_slices on row ranges

@@ -62,7 +62,7 @@ def parse_args():
     ap.add_argument('--frames', type=int, default=None, help='override frame count (testing)')
     ap.add_argument('--form', default=None, choices=['fp64', 'screen', 'dense'],
                     help='likelihood form (default: dense for config 5, screen otherwise)')
-    ap.add_argument('--kernel', default=None, choices=['stream', 'quad4', 'dynamic'],
+    ap.add_argument('--kernel', default=None, choices=['stream', 'quad4', 'sets', 'dynamic'],
                     help='likelihood kernel (default: the EStep default of the form)')
     ap.add_argument('--warps', type=int, default=None,
                     help='warps per CTA of the likelihood kernel (default: the EStep default, 32)')
@@ -221,7 +221,8 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
     gather_peak = sm_count * lanes * clk_mhz * 1e6
     gather_rate = gathers / (ll_launch_ms * 1e-3)
     slots_rate = rows_per_launch * slots / (ll_launch_ms * 1e-3)
-    names = {'stream': 'k_ll_stream<FormScreen>', 'quad4': 'k_screen_ll7'}
+    names = {'stream': 'k_ll_stream<FormScreen>', 'quad4': 'k_screen_ll7',
+             'sets': 'k_screen_sets'}
     roof = dict({'kernel': ('%s (FP32 screening likelihood, row a7)' %
                             names.get(es.kernel, es.kernel)
                             if es.form == 'screen' else 'k_ll_stream / k_loglike (FP64 likelihood, row a7)'),
@@ -528,8 +529,10 @@ def parity_block(rec, es, w, model0, dev, EStep):
     # every entry of the FP32 matrix against FP64, in row chunks
     worst, nan_mismatch = 0., 0
     step = max(1, (1 << 28) // max(1, w['n']))
+    cof = None if es.col_of_frame is None else es.col_of_frame.long()
     for r0 in range(0, es.n_rows, step):
-        a = es.prob[r0:r0 + step].double()
+        a = es.prob[r0:r0 + step]
+        a = (a if cof is None else a.index_select(1, cof)).double()
         b = pe.prob[r0:r0 + step]
         nan_mismatch += int((a.isnan() != b.isnan()).sum().item())
         ok = ~b.isnan()
@@ -668,7 +671,6 @@ def run_ours(args):
             parity = parity_block(rec, es, w, model0, dev, EStep)
         # the chosen form's likelihood matrix, slices, candidates and graph
         # pool are released first: the matrices need not fit at once
-        rec.prob = None
         for name in ('prob', 'lsl', 'cand_d', 'cand_r', 'cand_ll', 'row_cand'):
             setattr(es, name, None)
         torch.cuda.empty_cache()

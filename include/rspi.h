@@ -235,6 +235,86 @@ int rspi_screen_loglike7(const float *lslices, long long p_row, long long num_ro
                          float *ll, long long ll_stride, float *part_sums, int part_sums_ctas,
                          int warps_per_cta, int n_ctas, cudaStream_t stream);
 
+/* Frame sets (the chosen screening kernel).  Frames are taken 32 at a time:
+ * set s holds frames set_frames[32 s + l] (l = lane, -1 for none) and writes
+ * them to likelihood column 32 s + l (the caller orders frames, e.g. by
+ * photon count, so a set's frames need alike work; the likelihood matrix
+ * then has n_sets * 32 columns in that order).  Lane 8 p + f of a set is
+ * frame f of quarter warp p.  The likelihood columns [0, p_zero) are cut
+ * into n_parts (1-4) parts of part_w columns (part_w % 8 == 0,
+ * n_parts * part_w >= p_zero), each staged in shared memory as four FP32
+ * rows per column with 8 zero columns after it.
+ * rspi_sets_counts: counts[d * 32 + 8 h + c] = frame d's photons in part h of
+ * local column class c (local column mod 8), from the 16-bit entries of
+ * rspi_ll16_entry_fill (p_zero = their zero column).
+ * rspi_sets_steps: groups[h * n_sets + s] = ceil(D / 4), D = the most steps
+ * any quarter warp of set s needs in part h: max(largest frame count,
+ * largest class total over its eight frames) (Koenig's edge-colouring bound).
+ * The caller scans the groups part-major into group_off[n_parts*n_sets + 1].
+ * rspi_sets_fill: group_off[last] * 128 16-bit entries (8-byte aligned,
+ * prefilled by the caller with any value <= part_w + 7): entry
+ * ((g * 32 + lane) * 4 + k) is the local column the lane reads at step
+ * 4 (g - g0) + k of its (set, part) range [g0, g1).  At every step the eight
+ * lanes of a quarter warp read eight distinct classes (a Birkhoff-von
+ * Neumann decomposition of the padded count matrix), real photons first,
+ * the zero column part_w + class otherwise.  A schedule that cannot be
+ * built sets *err = RSPI_ERR_CAPACITY. */
+int rspi_sets_counts(const unsigned short *entries16, const long long *row_off16,
+                     long long n_data, int p_zero, int n_parts, int part_w, int *counts,
+                     cudaStream_t stream);
+int rspi_sets_steps(const int *counts, const int *set_frames, long long n_sets, int n_parts,
+                    int *groups, cudaStream_t stream);
+int rspi_sets_fill(const unsigned short *entries16, const long long *row_off16, int p_zero,
+                   int n_parts, int part_w, const int *counts, const int *set_frames,
+                   long long n_sets, const long long *group_off, unsigned short *entries,
+                   int *err, cudaStream_t stream);
+
+/* Rotated log-slices (as rspi_rot_log_slices, FP32, identical values) in the
+ * layout of rspi_screen_loglike_sets: rows taken four at a time from
+ * row_begin, columns cut into parts:
+ * out[(((r - row_begin) / 4 * n_parts + h) * part_w + c) * 4 + (r - row_begin) % 4]
+ * is row r at column h * part_w + c (zero past n_sel); rows of a partial
+ * last tile beyond row_end are not written.  holo_pairs as for
+ * rspi_rot_log_slices_pairs; out 16-byte aligned. */
+int rspi_rot_log_slices_sets(const double *holo_pairs, long long n_states0, long long num_rot,
+                             const double *rot_cs, long long size, const double *bg,
+                             const int *sel_pix, long long n_sel, int n_parts, int part_w,
+                             long long row_begin, long long row_end, float *out,
+                             float *abs_max, cudaStream_t stream);
+
+/* FP32 screening likelihood of rows [row_begin, row_end) from those slices
+ * (one bulk copy per tile part into shared memory) and the set entries: lane l
+ * of set s sums its frame's photons in the four rows (two alternating FP32
+ * accumulators over the groups, each group's four photons as a depth-two
+ * tree: at most ceil(G/2) + 3 roundings per value and part, G = the set's
+ * groups in the part); the parts are added in FP64 before the final
+ * rounding, the running sum of parts before the last kept in part_sums
+ * (rspi_sets_part_sums_floats(n_sets, part_sums_ctas) floats, 16-byte
+ * aligned; at most part_sums_ctas CTAs run).  LL32 of row r, frame
+ * set_frames[c] goes to ll[(r - row_begin) * ll_stride + c] (ll_stride >=
+ * n_sets * 32), and frame_max[c] (zero before the first launch of a pass)
+ * takes the unsigned maximum of an order-preserving (value, row) key, read
+ * and reset by rspi_frame_max_finalize.  A bulk copy that does not complete
+ * within 1 s sets *err = RSPI_ERR_TIMEOUT and the kernel returns.  Requires
+ * every entry <= part_w + 7 (check with rspi_entries16_check). */
+long long rspi_sets_part_sums_floats(long long n_sets, int n_ctas);
+int rspi_screen_loglike_sets(const float *lslices_sets, long long num_rot, const double *init,
+                             const double *scales, const unsigned short *entries,
+                             const long long *group_off, const int *set_frames,
+                             long long n_sets, int n_parts, int part_w, long long row_begin,
+                             long long row_end, float *ll, long long ll_stride,
+                             float *part_sums, int part_sums_ctas,
+                             unsigned long long *frame_max, int warps_per_cta, int n_ctas,
+                             int *err, cudaStream_t stream);
+
+/* Per-frame screened maximum and first-index argmax (NumPy's rules: the
+ * first NaN wins) from the keys of rspi_screen_loglike_sets: for every
+ * column c with frame d = frame_of_col[c] >= 0, max32[d] and rmax32[d]; the
+ * keys are reset to zero for the next pass (replaces rspi_frame_reduce's
+ * pass over the FP32 matrix, emc.py:207-216). */
+int rspi_frame_max_finalize(unsigned long long *frame_max, const int *frame_of_col,
+                            long long n_cols, double *max32, int *rmax32, cudaStream_t stream);
+
 /* *max_index = largest value in a 16-bit entry array. */
 int rspi_entries16_check(const unsigned short *entries, long long n_entries,
                          unsigned *max_index, cudaStream_t stream);
@@ -271,6 +351,17 @@ int rspi_screen_candidates_noalloc(const float *ll, long long n_rows, long long 
                                    long long capacity, int *cand_d, int *cand_r, int *err,
                                    cudaStream_t stream);
 
+/* rspi_screen_candidates over a likelihood matrix whose n_cols columns hold
+ * frames in another order: column c holds frame frame_of_col[c] (-1: none);
+ * the outputs are per frame as in rspi_screen_candidates. */
+int rspi_screen_candidates_cols(const float *ll, long long n_rows, long long n_cols,
+                                const int *frame_of_col, long long n_data, const double *max32,
+                                const int *rmax32, const long long *frame_photons,
+                                const long long *row_off16, const float *lmax, double delta,
+                                int *cnt_part, int *cand_n, double *noncand, double *thr,
+                                long long *cand_off, long long capacity, int *cand_d,
+                                int *cand_r, int *err, cudaStream_t stream);
+
 /* FP64 rescoring of every candidate, in the summation order of rspi_loglike
  * (so the values equal the FP64 form's), written to cand_ll and into ll32;
  * then per frame the first-index argmax, maximum and
@@ -291,6 +382,19 @@ int rspi_rescore(const int *cand_d, const int *cand_r, const long long *cand_off
                  int *row_cand, double *cand_ll, float *ll32, const double *max32,
                  const double *noncand, double *maxll, int *rmax, double *logz,
                  double *row_scratch, long long scratch_rows, cudaStream_t stream);
+
+/* rspi_rescore for a likelihood matrix with n_cols columns in which frame d
+ * is column col_of_frame[d]. */
+int rspi_rescore_cols(const int *cand_d, const int *cand_r, const long long *cand_off,
+                      long long n_data, long long capacity, long long n_rows, const double *holo,
+                      long long num_rot, const double *rot_cs, long long size, const double *bg,
+                      const int *sel_pix, long long n_sel, long long p_pad, const double *init,
+                      const double *scales, const unsigned int *entries32,
+                      const long long *row_off32, int *row_cnt, long long *row_cand_off,
+                      int *row_cand, double *cand_ll, float *ll32, long long n_cols,
+                      const int *col_of_frame, const double *max32, const double *noncand,
+                      double *maxll, int *rmax, double *logz, double *row_scratch,
+                      long long scratch_rows, cudaStream_t stream);
 
 /* ------------------------------------------------------------------- a8, a9
  * Per-frame reduction over all states of LL (n_rows x n_data, FP64 or FP32):

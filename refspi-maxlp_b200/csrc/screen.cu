@@ -153,7 +153,8 @@ __device__ __forceinline__ double frame_eps(long long phot, long long rows, floa
 }
 
 __global__ void __launch_bounds__(32 * RY)
-k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_data,
+k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_x, long long stride,
+             const int *__restrict__ frame_of_col,
              const double *__restrict__ max32, const int *__restrict__ rmax32,
              const long long *__restrict__ phot,
              const long long *__restrict__ row_off16, const float *__restrict__ lmax, double delta,
@@ -162,10 +163,13 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_data,
     __shared__ int sc[RY][33];
     __shared__ double sn[RY][33];
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const long long d = (long long)blockIdx.x * 32 + tx;
+    // thread column x of the likelihood matrix holds frame d (x itself
+    // unless the columns are a permutation of the frames)
+    const long long x = (long long)blockIdx.x * 32 + tx;
+    const long long d = x >= n_x ? -1 : (frame_of_col ? (long long)frame_of_col[x] : x);
     int c = 0;
     double nc = 0.;
-    if (d < n_data) {
+    if (d >= 0) {
         const double m = max32[d];
         const long long rows = row_off16[d + 1] - row_off16[d];
         const double thr = m - delta - 2. * frame_eps(phot[d], rows, *lmax, m, delta);
@@ -175,7 +179,7 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_data,
         for (; r + 7 * RY < n_rows; r += 8 * RY) {
             float v8[8];
 #pragma unroll
-            for (int u = 0; u < 8; ++u) v8[u] = __ldg(&ll[(r + u * RY) * n_data + d]);
+            for (int u = 0; u < 8; ++u) v8[u] = __ldg(&ll[(r + u * RY) * stride + x]);
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
                 const double v = (double)v8[u];
@@ -184,7 +188,7 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_data,
             }
         }
         for (; r < n_rows; r += RY) {
-            const double v = (double)ll[r * n_data + d];
+            const double v = (double)ll[r * stride + x];
             if (v >= thr || r == rm) ++c;
             else nc += (double)expf((float)(v - m));   // each term < exp(-delta)
         }
@@ -194,7 +198,7 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_data,
     sc[ty][tx] = c;
     sn[ty][tx] = nc;
     __syncthreads();
-    if (ty == 0 && d < n_data) {
+    if (ty == 0 && d >= 0) {
         int tot = 0;
         double s = 0.;
         for (int k = 0; k < RY; ++k) {
@@ -207,14 +211,16 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_data,
 }
 
 __global__ void __launch_bounds__(32 * RY)
-k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_data,
+k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_x, long long stride,
+            const int *__restrict__ frame_of_col,
             const double *__restrict__ thr, const int *__restrict__ rmax32,
             const int *__restrict__ cnt_part,
             const long long *__restrict__ cand_off, long long capacity,
             int *__restrict__ cand_d, int *__restrict__ cand_r, int *err) {
     const int tx = threadIdx.x, ty = threadIdx.y;
-    const long long d = (long long)blockIdx.x * 32 + tx;
-    if (d >= n_data) return;
+    const long long x = (long long)blockIdx.x * 32 + tx;
+    const long long d = x >= n_x ? -1 : (frame_of_col ? (long long)frame_of_col[x] : x);
+    if (d < 0) return;
     long long pos = cand_off[d];
     for (int k = 0; k < ty; ++k) pos += cnt_part[d * RY + k];
     const double th = thr[d];
@@ -235,11 +241,11 @@ k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_data,
     for (; r + 7 * RY < n_rows; r += 8 * RY) {
         float v8[8];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) v8[u] = __ldg(&ll[(r + u * RY) * n_data + d]);
+        for (int u = 0; u < 8; ++u) v8[u] = __ldg(&ll[(r + u * RY) * stride + x]);
 #pragma unroll
         for (int u = 0; u < 8; ++u) take(v8[u], r + u * RY);
     }
-    for (; r < n_rows; r += RY) take(ll[r * n_data + d], r);
+    for (; r < n_rows; r += RY) take(ll[r * stride + x], r);
 }
 
 // Candidates regrouped by likelihood row: count, scan (rows + 1 offsets),
@@ -279,8 +285,8 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
                const double *__restrict__ bg, const int *__restrict__ sel_pix, long long n_sel,
                long long p_pad, const double *__restrict__ init, const double *__restrict__ scales,
                const unsigned int *__restrict__ ent32, const long long *__restrict__ row_off32,
-               double *__restrict__ cand_ll, float *__restrict__ ll32, long long n_data,
-               double *row_scratch) {
+               double *__restrict__ cand_ll, float *__restrict__ ll32, long long ll_stride,
+               const int *__restrict__ col_of_frame, double *row_scratch) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *sl = GROW ? row_scratch + (long long)blockIdx.x * p_pad
                       : reinterpret_cast<double *>(smem_raw);
@@ -323,7 +329,7 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
                 if (lane == 0) {
                     const double v = ini * scales[d] + acc;
                     cand_ll[pair] = v;
-                    ll32[r * n_data + d] = (float)v;
+                    ll32[r * ll_stride + (col_of_frame ? col_of_frame[d] : d)] = (float)v;
                 }
             }
         } else {
@@ -355,7 +361,7 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
                     if (lane == c) {
                         const double v = ini * scales[d] + acc;
                         cand_ll[pair] = v;
-                        ll32[r * n_data + d] = (float)v;
+                        ll32[r * ll_stride + (col_of_frame ? col_of_frame[d] : d)] = (float)v;
                     }
                 }
             }
@@ -464,6 +470,36 @@ extern "C" int rspi_ll16_entry_fill(const int *ones, const int *multi,
     RSPI_RETURN_LAUNCH();
 }
 
+namespace {
+
+// Candidate selection over a likelihood matrix with n_x columns of stride
+// `stride`; column x holds frame frame_of_col[x] (-1: none), or frame x when
+// frame_of_col is null.
+int candidates_launch(const float *ll, long long n_rows, long long n_x, long long stride,
+                      const int *frame_of_col, long long n_data, const double *max32,
+                      const int *rmax32, const long long *frame_photons,
+                      const long long *row_off16, const float *lmax, double delta,
+                      int *cnt_part, int *cand_n, double *noncand, double *thr,
+                      long long *cand_off, long long capacity, int *cand_d, int *cand_r,
+                      int *err, cudaStream_t stream) {
+    if (!ll || !max32 || !rmax32 || !frame_photons || !row_off16 || !lmax || !cnt_part ||
+        !cand_n || !noncand || !thr || !cand_off || !cand_d || !cand_r || n_rows <= 0 ||
+        n_data <= 0 || n_x <= 0 || stride < n_x || n_rows > 0x7fffffffLL || capacity < 0 ||
+        capacity > 0x7fffffffLL || !(delta >= 0.))
+        return RSPI_ERR_ARG;
+    const dim3 block(32, RY);
+    const unsigned grid = (unsigned)((n_x + 31) / 32);
+    k_cand_count<<<grid, block, 0, stream>>>(ll, n_rows, n_x, stride, frame_of_col, max32,
+                                             rmax32, frame_photons, row_off16, lmax, delta,
+                                             cnt_part, cand_n, noncand, thr);
+    k_scan_counts<<<1, 1024, 0, stream>>>(cand_n, n_data, cand_off);
+    k_cand_fill<<<grid, block, 0, stream>>>(ll, n_rows, n_x, stride, frame_of_col, thr, rmax32,
+                                            cnt_part, cand_off, capacity, cand_d, cand_r, err);
+    RSPI_RETURN_LAUNCH();
+}
+
+}  // namespace
+
 extern "C" int rspi_screen_candidates(const float *ll, long long n_rows, long long n_data,
                                       const double *max32, const int *rmax32,
                                       const long long *frame_photons,
@@ -471,22 +507,27 @@ extern "C" int rspi_screen_candidates(const float *ll, long long n_rows, long lo
                                       int *cnt_part, int *cand_n, double *noncand, double *thr,
                                       long long *cand_off, long long capacity, int *cand_d,
                                       int *cand_r, int *err, cudaStream_t stream) {
-    if (!ll || !max32 || !rmax32 || !frame_photons || !row_off16 || !lmax || !cnt_part || !cand_n ||
-        !noncand || !thr || !cand_off || !cand_d || !cand_r || n_rows <= 0 || n_data <= 0 ||
-        n_rows > 0x7fffffffLL || capacity < 0 || capacity > 0x7fffffffLL || !(delta >= 0.))
-        return RSPI_ERR_ARG;
-    const dim3 block(32, RY);
-    const unsigned grid = (unsigned)((n_data + 31) / 32);
-    k_cand_count<<<grid, block, 0, stream>>>(ll, n_rows, n_data, max32, rmax32, frame_photons,
-                                             row_off16, lmax, delta, cnt_part, cand_n, noncand,
-                                             thr);
-    k_scan_counts<<<1, 1024, 0, stream>>>(cand_n, n_data, cand_off);
-    k_cand_fill<<<grid, block, 0, stream>>>(ll, n_rows, n_data, thr, rmax32, cnt_part, cand_off,
-                                            capacity, cand_d, cand_r, err);
-    RSPI_RETURN_LAUNCH();
+    return candidates_launch(ll, n_rows, n_data, n_data, nullptr, n_data, max32, rmax32,
+                             frame_photons, row_off16, lmax, delta, cnt_part, cand_n, noncand,
+                             thr, cand_off, capacity, cand_d, cand_r, err, stream);
 }
 
-extern "C" int rspi_rescore(const int *cand_d, const int *cand_r, const long long *cand_off,
+extern "C" int rspi_screen_candidates_cols(const float *ll, long long n_rows, long long n_cols,
+                                           const int *frame_of_col, long long n_data,
+                                           const double *max32, const int *rmax32,
+                                           const long long *frame_photons,
+                                           const long long *row_off16, const float *lmax,
+                                           double delta, int *cnt_part, int *cand_n,
+                                           double *noncand, double *thr, long long *cand_off,
+                                           long long capacity, int *cand_d, int *cand_r,
+                                           int *err, cudaStream_t stream) {
+    if (!frame_of_col) return RSPI_ERR_ARG;
+    return candidates_launch(ll, n_rows, n_cols, n_cols, frame_of_col, n_data, max32, rmax32,
+                             frame_photons, row_off16, lmax, delta, cnt_part, cand_n, noncand,
+                             thr, cand_off, capacity, cand_d, cand_r, err, stream);
+}
+
+static int rescore_launch(const int *cand_d, const int *cand_r, const long long *cand_off,
                             long long n_data, long long capacity, long long n_rows,
                             const double *holo, long long num_rot, const double *rot_cs,
                             long long size, const double *bg, const int *sel_pix, long long n_sel,
@@ -495,12 +536,13 @@ extern "C" int rspi_rescore(const int *cand_d, const int *cand_r, const long lon
                             int *row_cnt, long long *row_cand_off, int *row_cand,
                             double *cand_ll, float *ll32, const double *max32,
                             const double *noncand, double *maxll, int *rmax, double *logz,
-                            double *row_scratch, long long scratch_rows, cudaStream_t stream) {
+                            double *row_scratch, long long scratch_rows,
+                            const int *col_of_frame, long long ll_stride, cudaStream_t stream) {
     if (!cand_d || !cand_r || !cand_off || !holo || !rot_cs || !bg || !sel_pix || !init ||
         !scales || !entries32 || !row_off32 || !row_cnt || !row_cand_off || !row_cand ||
         !cand_ll || !ll32 || !max32 || !noncand || !maxll || !rmax || !logz || n_data <= 0 ||
         capacity < 0 || capacity > 0x7fffffffLL || n_rows <= 0 || n_rows > 0x7fffffffLL ||
-        size <= 1 || size > 46340 ||
+        size <= 1 || size > 46340 || ll_stride < n_data ||
         p_pad < n_sel || p_pad % 32 || p_pad > 65536)
         return RSPI_ERR_ARG;
     const size_t smem = (size_t)p_pad * sizeof(double);
@@ -521,19 +563,56 @@ extern "C" int rspi_rescore(const int *cand_d, const int *cand_r, const long lon
         const unsigned grid = (unsigned)min(scratch_rows, n_rows);
         k_rescore_rows<true><<<grid, 1024, 0, stream>>>(
             row_cand_off, row_cand, n_rows, cand_d, holo, num_rot, rot_cs, (int)size, bg,
-            sel_pix, n_sel, p_pad, init, scales, entries32, row_off32, cand_ll, ll32, n_data,
-            row_scratch);
+            sel_pix, n_sel, p_pad, init, scales, entries32, row_off32, cand_ll, ll32, ll_stride,
+            col_of_frame, row_scratch);
     } else {
         const int per_sm = max(1, (int)(SMEM_LIMIT / (smem + 1024)));
         const unsigned grid = (unsigned)min((long long)rspi_sm_count() * min(per_sm, 2), n_rows);
         k_rescore_rows<false><<<grid, 1024 / min(per_sm, 2), smem, stream>>>(
             row_cand_off, row_cand, n_rows, cand_d, holo, num_rot, rot_cs, (int)size, bg,
-            sel_pix, n_sel, p_pad, init, scales, entries32, row_off32, cand_ll, ll32, n_data,
-            nullptr);
+            sel_pix, n_sel, p_pad, init, scales, entries32, row_off32, cand_ll, ll32, ll_stride,
+            col_of_frame, nullptr);
     }
     k_cand_finalize<<<rspi_blocks(n_data * 32, 256), 256, 0, stream>>>(
         cand_off, cand_r, cand_ll, max32, noncand, n_data, capacity, maxll, rmax, logz);
     RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_rescore(const int *cand_d, const int *cand_r, const long long *cand_off,
+                            long long n_data, long long capacity, long long n_rows,
+                            const double *holo, long long num_rot, const double *rot_cs,
+                            long long size, const double *bg, const int *sel_pix, long long n_sel,
+                            long long p_pad, const double *init, const double *scales,
+                            const unsigned int *entries32, const long long *row_off32,
+                            int *row_cnt, long long *row_cand_off, int *row_cand,
+                            double *cand_ll, float *ll32, const double *max32,
+                            const double *noncand, double *maxll, int *rmax, double *logz,
+                            double *row_scratch, long long scratch_rows, cudaStream_t stream) {
+    return rescore_launch(cand_d, cand_r, cand_off, n_data, capacity, n_rows, holo, num_rot,
+                          rot_cs, size, bg, sel_pix, n_sel, p_pad, init, scales, entries32,
+                          row_off32, row_cnt, row_cand_off, row_cand, cand_ll, ll32, max32,
+                          noncand, maxll, rmax, logz, row_scratch, scratch_rows, nullptr, n_data,
+                          stream);
+}
+
+extern "C" int rspi_rescore_cols(const int *cand_d, const int *cand_r, const long long *cand_off,
+                                 long long n_data, long long capacity, long long n_rows,
+                                 const double *holo, long long num_rot, const double *rot_cs,
+                                 long long size, const double *bg, const int *sel_pix,
+                                 long long n_sel, long long p_pad, const double *init,
+                                 const double *scales, const unsigned int *entries32,
+                                 const long long *row_off32, int *row_cnt,
+                                 long long *row_cand_off, int *row_cand, double *cand_ll,
+                                 float *ll32, long long n_cols, const int *col_of_frame,
+                                 const double *max32, const double *noncand, double *maxll,
+                                 int *rmax, double *logz, double *row_scratch,
+                                 long long scratch_rows, cudaStream_t stream) {
+    if (!col_of_frame) return RSPI_ERR_ARG;
+    return rescore_launch(cand_d, cand_r, cand_off, n_data, capacity, n_rows, holo, num_rot,
+                          rot_cs, size, bg, sel_pix, n_sel, p_pad, init, scales, entries32,
+                          row_off32, row_cnt, row_cand_off, row_cand, cand_ll, ll32, max32,
+                          noncand, maxll, rmax, logz, row_scratch, scratch_rows, col_of_frame,
+                          n_cols, stream);
 }
 
 // ---------------------------------------------------------------------------
@@ -606,11 +685,11 @@ extern "C" int rspi_screen_candidates_noalloc(const float *ll, long long n_rows,
     if (scratch == nullptr) return status;
     const dim3 block(32, RY);
     const unsigned grid = (unsigned)((n_data + 31) / 32);
-    k_cand_count<<<grid, block, 0, stream>>>(ll, n_rows, n_data, max32, rmax32, frame_photons,
-                                             row_off16, lmax, delta, scratch, cand_n, noncand,
-                                             thr);
+    k_cand_count<<<grid, block, 0, stream>>>(ll, n_rows, n_data, n_data, nullptr, max32, rmax32,
+                                             frame_photons, row_off16, lmax, delta, scratch,
+                                             cand_n, noncand, thr);
     k_scan_counts<<<1, 1024, 0, stream>>>(cand_n, n_data, cand_off);
-    k_cand_fill<<<grid, block, 0, stream>>>(ll, n_rows, n_data, thr, rmax32, scratch, cand_off,
-                                            capacity, cand_d, cand_r, err);
+    k_cand_fill<<<grid, block, 0, stream>>>(ll, n_rows, n_data, n_data, nullptr, thr, rmax32,
+                                            scratch, cand_off, capacity, cand_d, cand_r, err);
     RSPI_RETURN_LAUNCH();
 }

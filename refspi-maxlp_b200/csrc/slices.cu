@@ -191,6 +191,115 @@ k_rot_log_js(const double *__restrict__ holo, const double2 *__restrict__ hp, in
     }
 }
 
+// Rotated log-slices in the layout of the frame-set screening kernel: rows
+// taken four at a time from row_begin (tile q = (r - row_begin) / 4, lane
+// (r - row_begin) mod 4) and columns cut into n_parts parts of part_w, so
+// that one tile's part is one contiguous run of float4 columns:
+// out[((q * n_parts + h) * part_w + c') * 4 + lane] holds column
+// h * part_w + c' (zero past n_sel).  A CTA takes four consecutive rotations
+// j0..j0+3 and up to RL_STATES consecutive states; per column the four
+// rotated positions are computed once and reused for every state, and with
+// num_rot and row_begin multiples of four a state's four rotations are one
+// tile's four rows, stored as one 16-byte write.  Values are those of
+// rot_log_value (same operations, identical bits).
+__global__ void __launch_bounds__(256)
+k_rot_log_sets(const double2 *__restrict__ hp, int num_rot, const double *__restrict__ rot_cs,
+               int size, const double *__restrict__ bg, const int *__restrict__ sel_pix, int n_sel,
+               int n_parts, int part_w, long long row_begin, long long row_end, long long s_lo,
+               float *__restrict__ out, float *__restrict__ abs_max) {
+    const int n_jb = (num_rot + 3) / 4;
+    const int j0 = (int)(blockIdx.x % (unsigned)n_jb) * 4;
+    const long long s_first = s_lo + (long long)(blockIdx.x / (unsigned)n_jb) * RL_STATES;
+    const long long npix = (long long)size * size;
+    const long long n_rows = row_end - row_begin;
+    const int cen = size / 2;
+    const float inv_size = 1.f / (float)size;
+    // this CTA's states with a row s0 * num_rot + j0 + q in [row_begin, row_end)
+    long long sb = s_first, se = s_first + RL_STATES;
+    while (sb < se && sb * num_rot + min(j0 + 3, num_rot - 1) < row_begin) ++sb;
+    while (se > sb && (se - 1) * num_rot + j0 >= row_end) --se;
+    double ac[4], as[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = min(j0 + q, num_rot - 1);
+        ac[q] = rot_cs[2 * j];
+        as[q] = rot_cs[2 * j + 1];
+    }
+    const int n_cols = n_parts * part_w;
+    float amax = 0.f;
+    if (sb < se) {
+        for (int c = threadIdx.x; c < n_cols; c += blockDim.x) {
+            const int h = c / part_w, cl = c - h * part_w;
+            bool in[4] = {false, false, false, false};
+            int base[4] = {0, 0, 0, 0};
+            double fx[4] = {0., 0., 0., 0.}, fy[4] = {0., 0., 0., 0.};
+            double b = 0.;
+            if (c < n_sel) {
+                const int p = sel_pix[c];
+                int x, y;
+                pixel_xy(p, size, inv_size, x, y);
+                const double xc = (double)(x - cen), yc = (double)(y - cen);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const double tx = xadd(xsub(xmul(xc, ac[q]), xmul(yc, as[q])), (double)cen);
+                    const double ty = xadd(xadd(xmul(xc, as[q]), xmul(yc, ac[q])), (double)cen);
+                    const double fxl = floor(tx), fyl = floor(ty);
+                    in[q] = !(fxl < 0. || fxl > size - 2 || fyl < 0. || fyl > size - 2);
+                    if (in[q]) {
+                        base[q] = (int)fxl * size + (int)fyl;
+                        fx[q] = tx - fxl;
+                        fy[q] = ty - fyl;
+                    }
+                }
+                b = bg[p];
+            }
+            for (long long s0 = sb; s0 < se; ++s0) {
+                float v[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    double val = 0.;
+                    if (c < n_sel) {
+                        if (in[q]) {
+                            const double2 a = hp[s0 * npix + base[q]];
+                            const double2 b2 = hp[s0 * npix + base[q] + size];
+                            const double cx = 1. - fx[q], cy = 1. - fy[q];
+                            double t = xmul(xmul(a.x, cx), cy);
+                            t = xadd(t, xmul(xmul(b2.x, fx[q]), cy));
+                            t = xadd(t, xmul(xmul(a.y, cx), fy[q]));
+                            t = xadd(t, xmul(xmul(b2.y, fx[q]), fy[q]));
+                            t = xadd(t, b);
+                            val = t < 1.e-20 ? -1000. : log(t);
+                        } else {
+                            val = -1000.;
+                        }
+                    }
+                    v[q] = (float)val;
+                }
+                const long long r0 = s0 * num_rot + j0 - row_begin;
+                if (j0 + 3 < num_rot && (r0 & 3) == 0 && r0 >= 0 && r0 + 3 < n_rows) {
+                    reinterpret_cast<float4 *>(out)[((r0 >> 2) * n_parts + h) * part_w + cl] =
+                        make_float4(v[0], v[1], v[2], v[3]);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) amax = fmaxf(amax, fabsf(v[q]));
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const long long r = r0 + q;
+                        if (j0 + q >= num_rot || r < 0 || r >= n_rows) continue;
+                        out[(((r >> 2) * n_parts + h) * part_w + cl) * 4 + (r & 3)] = v[q];
+                        amax = fmaxf(amax, fabsf(v[q]));
+                    }
+                }
+            }
+        }
+    }
+    if (abs_max) {
+        amax = __int_as_float(warp_max_int(__float_as_int(amax)));
+        if ((threadIdx.x & 31) == 0)
+            atomicMax(reinterpret_cast<int *>(abs_max), __float_as_int(amax));
+    }
+}
+
 }  // namespace
 
 extern "C" int rspi_holo_slices(const double *model, const double *shiftx, const double *shifty,
@@ -286,5 +395,30 @@ extern "C" int rspi_sphere_ramp(long long size, double sx, double sy, double dia
     if (size <= 1 || size > 46340 || (!sphere && !ramp)) return RSPI_ERR_ARG;
     k_sphere_ramp<<<rspi_blocks(size * size, 256), 256, 0, stream>>>(
         (int)size, sx, sy, dia, sphere, (double2 *)ramp);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_rot_log_slices_sets(const double *holo_pairs, long long n_states0,
+                                        long long num_rot, const double *rot_cs, long long size,
+                                        const double *bg, const int *sel_pix, long long n_sel,
+                                        int n_parts, int part_w, long long row_begin,
+                                        long long row_end, float *out, float *abs_max,
+                                        cudaStream_t stream) {
+    if (!holo_pairs || !rot_cs || !bg || !out || n_states0 <= 0 || num_rot <= 0 ||
+        num_rot > 0x7fffffffLL || size <= 1 || size > 46340 || n_sel < 0 || n_parts < 1 ||
+        part_w < 1 || (long long)n_parts * part_w < n_sel ||
+        (long long)n_parts * part_w > 0x7fffffffLL || row_begin < 0 || row_end < row_begin ||
+        row_end > n_states0 * num_rot || (n_sel > 0 && !sel_pix) ||
+        (reinterpret_cast<uintptr_t>(holo_pairs) & 15) != 0 ||
+        (reinterpret_cast<uintptr_t>(out) & 15) != 0)
+        return RSPI_ERR_ARG;
+    if (row_end == row_begin) return RSPI_OK;
+    const long long s_lo = row_begin / num_rot, s_hi = (row_end - 1) / num_rot;
+    const long long n_groups = (s_hi - s_lo) / RL_STATES + 1;
+    const long long n_jb = (num_rot + 3) / 4;
+    if (n_groups * n_jb > 0x7fffffffLL) return RSPI_ERR_ARG;
+    k_rot_log_sets<<<(unsigned)(n_groups * n_jb), 256, 0, stream>>>(
+        reinterpret_cast<const double2 *>(holo_pairs), (int)num_rot, rot_cs, (int)size, bg,
+        sel_pix, (int)n_sel, n_parts, part_w, row_begin, row_end, s_lo, out, abs_max);
     RSPI_RETURN_LAUNCH();
 }

@@ -95,7 +95,6 @@ class EMC():
                            slice_budget_bytes=int(self.slice_budget_gb * (1 << 30)),
                            n_modes=self.num_modes, dense_gemm=self.dense_gemm,
                            dense_rescore=self.dense_rescore)
-        self.prob = self.estep.prob
         self.state_vals = torch.from_numpy(self._state_values).to(self.device)
         self.phaser_rot = torch.from_numpy(geometry.phaser_rotation_table(
             np.arange(self.num_rot) * np.pi / self.num_rot)).to(self.device)
@@ -233,6 +232,14 @@ class EMC():
             raise ValueError('frame ranges are not supported: all frames are processed')
         self.estep.run(dmodel)
         return self.prob
+
+    @property
+    def prob(self):
+        '''Likelihood of every frame (columns) in every state (rows
+        ``s*num_rot + j``), emc.py's ``prob``; a device tensor in frame order
+        (a reordered copy when the likelihood kernel keeps frames in set
+        order)'''
+        return self.estep.frame_prob()
 
     def _get_rmax(self):
         '''First-index argmax per frame (emc.py:207-216; one rank)'''

@@ -241,7 +241,7 @@ class EStep:
             raise ValueError('form must be fp64, screen or dense')
         if kernel is None:   # default likelihood kernel of each form
             kernel = 'quad4' if form == 'screen' else 'stream'
-        kernels = {'fp64': ('stream', 'dynamic'), 'screen': ('stream', 'quad4'),
+        kernels = {'fp64': ('stream', 'dynamic'), 'screen': ('stream', 'quad4', 'sets'),
                    'dense': ('stream', 'tcgen05')}[form]
         if kernel not in kernels:
             raise ValueError('the %s form takes the kernels %s' % (form, ', '.join(kernels)))
@@ -271,6 +271,7 @@ class EStep:
         self.rot_cs = t(geometry.emc_rotation_table(self.num_rot))
         self.bg = t(np.asarray(bg, dtype='f8').ravel())
         self.ll = photons.ll_entries(self.pix2sel, self.p_pad)
+        self.col_of_frame, self.frame_of_col, self.n_cols = None, None, n
         if form == 'dense':
             self._init_dense(photons, slice_budget_bytes, delta, cand_per_frame, dense_gemm,
                              dense_rescore)
@@ -288,7 +289,7 @@ class EStep:
             self.delta = float(delta)
         self.slice_torch = {0: torch.float32, 1: _f64}[self.slice_code]
         self.prob_torch = torch.float32 if self.prob_code == 0 else _f64
-        if kernel == 'quad4':
+        if kernel in ('quad4', 'sets'):
             tmax = 4                 # four rows per tile over column parts
             if self.p_row - 32 > QUAD4_MAX_PARTS * QUAD4_COLS:
                 raise ValueError('%d likelihood columns exceed the four-row tile' % self.n_sel)
@@ -299,13 +300,27 @@ class EStep:
         self.tile = int(states_per_tile or tmax)
         if self.tile > tmax:
             raise ValueError('states_per_tile %d exceeds the shared-memory limit %d' % (self.tile, tmax))
-        if kernel == 'quad4' and self.tile != 4:
-            raise ValueError('the four-row frame-quad kernel takes 4 states per tile')
+        if kernel in ('quad4', 'sets') and self.tile != 4:
+            raise ValueError('the four-row %s kernel takes 4 states per tile' % kernel)
         self.warps, self.n_ctas = int(warps), int(n_ctas)
-        self.wide = self._quad4_entries() if kernel == 'quad4' else None
+        # column order of the likelihood matrix: frame order, except for the
+        # frame-set kernel (column 32 s + l = frame set_frames[32 s + l])
+        self.wide = None
+        if kernel == 'quad4':
+            self.wide = self._quad4_entries()
+        elif kernel == 'sets':
+            self.wide = self._sets_entries()
+            self.col_of_frame = self.wide['col_of_frame']
+            self.frame_of_col = self.wide['set_frames']
+            self.n_cols = self.wide['n_sets'] * 32
+            self.frame_max = torch.zeros(self.n_cols, dtype=_i64, device=dev)
         self._eps_key, self.row_off_eps = None, None
         esz = {0: 4, 1: 8, 2: 2}[self.slice_code]
-        rows = max(self.tile, (slice_budget_bytes // (self.p_row * esz)) // self.tile * self.tile)
+        # slice bytes per likelihood row (the frame-set layout holds the
+        # column parts without the 32 zero columns)
+        row_bytes = (self.wide['n_parts'] * self.wide['part_w'] * 4 if kernel == 'sets'
+                     else self.p_row * esz)
+        rows = max(self.tile, (slice_budget_bytes // row_bytes) // self.tile * self.tile)
         self.chunk_rows = int(min(self.n_rows, rows))
         self.holo = torch.empty((self.n_states0, self.size ** 2), dtype=_f64, device=dev)
         # (w[p], w[p + 1]) pairs: the slice kernel's bilinear rows as 16-byte loads
@@ -314,8 +329,15 @@ class EStep:
         self.msum = torch.empty(self.n_states0, dtype=_f64, device=dev)
         self.vscale = torch.empty(1, dtype=_f64, device=dev)
         self.init = torch.empty(self.n_states0, dtype=_f64, device=dev)
-        self.lsl = torch.empty((self.chunk_rows, self.p_row), dtype=self.slice_torch, device=dev)
-        self.prob = torch.empty((self.n_rows, n), dtype=self.prob_torch, device=dev)
+        if kernel == 'sets':
+            # tiles of four rows x parts x part_w float4 columns
+            tiles = (self.chunk_rows + 3) // 4
+            self.lsl = torch.empty(tiles * self.wide['n_parts'] * self.wide['part_w'] * 4,
+                                   dtype=torch.float32, device=dev)
+        else:
+            self.lsl = torch.empty((self.chunk_rows, self.p_row), dtype=self.slice_torch,
+                                   device=dev)
+        self.prob = torch.empty((self.n_rows, self.n_cols), dtype=self.prob_torch, device=dev)
         self.maxll = torch.empty(n, dtype=_f64, device=dev)
         self.rmax = torch.empty(n, dtype=_i32, device=dev)
         self.logz = torch.empty(n, dtype=_f64, device=dev)
@@ -462,6 +484,64 @@ class EStep:
                     n_pairs=nq, frame_groups=sng.amax(1)[(set_slot // 4).long()],
                     n_parts=parts, part_w=part_w, part_sums=ps, part_sums_ctas=ps_ctas)
 
+    def _sets_entries(self):
+        """Entries of the frame-set kernel: frames in decreasing order of
+        their likelihood-pixel photons, taken 32 at a time; lane 8 p + f of
+        set s is the frame of rank 32 s + p + 4 f, so the four quarter warps
+        of a set get alike frames.  Per (set, column part) a step schedule
+        in which a quarter warp's eight lanes read eight distinct bank
+        classes (rspi_sets_steps / rspi_sets_fill); one FP32 running sum per
+        (CTA, column) between parts when there are several."""
+        l16, n, dev, s = self.ll16, self.ph.num_data, self.device, cur_stream()
+        pz = self.p_row - 32
+        parts, part_w = self._quad4_parts()
+        counts = torch.empty(n * 32, dtype=_i32, device=dev)
+        call('rspi_sets_counts', ptr(l16['entries']), ptr(l16['row_off']), n, pz, parts, part_w,
+             ptr(counts), s)
+        tot = self.ll['frame_sel_photons']
+        order = torch.argsort(-tot, stable=True)
+        n_sets = (n + 31) // 32
+        k = torch.arange(n_sets * 32, device=dev, dtype=_i64)
+        lane = k % 32
+        src = (k - lane) + (lane // 8) + 4 * (lane % 8)
+        set_frames = torch.where(src < n, order[src.clamp(max=n - 1)],
+                                 torch.full_like(src, -1)).to(_i32)
+        col_of_frame = torch.empty(n, dtype=_i32, device=dev)
+        real = set_frames >= 0
+        col_of_frame[set_frames[real].long()] = k[real].to(_i32)
+        groups = torch.empty(parts * n_sets, dtype=_i32, device=dev)
+        call('rspi_sets_steps', ptr(counts), ptr(set_frames), n_sets, parts, ptr(groups), s)
+        goff = torch.empty(parts * n_sets + 1, dtype=_i64, device=dev)
+        call('rspi_scan_rows', ptr(groups), parts * n_sets, ptr(goff), s)
+        total = int(goff[-1].item())
+        # every slot starts at the zero column part_w (class 0), a valid index
+        entries = torch.full((max(1, total) * 128,), part_w, dtype=torch.int16, device=dev)
+        call('rspi_sets_fill', ptr(l16['entries']), ptr(l16['row_off']), pz, parts, part_w,
+             ptr(counts), ptr(set_frames), n_sets, ptr(goff), ptr(entries), ptr(self.ph.err.t),
+             s)
+        self.ph.err.check('frame-set entries')
+        mx = torch.zeros(1, dtype=_i32, device=dev)
+        call('rspi_entries16_check', ptr(entries), max(1, total) * 128, ptr(mx), s)
+        if int(mx.item()) > part_w + 7:
+            raise RuntimeError('frame-set entry %d outside the staged part' % int(mx.item()))
+        # each frame's FP32 summation length for the candidate threshold:
+        # ceil(G / 2) accumulator steps of its set's largest part (the +3 of
+        # the group tree and the final add are within the threshold's +8)
+        g = groups.view(parts, n_sets).to(_i64)
+        per_set = ((g + 1) // 2).amax(0)
+        frame_groups = torch.zeros(n, dtype=_i64, device=dev)
+        frame_groups[set_frames[real].long()] = per_set[(k[real] // 32)]
+        ps, ps_ctas = None, 0
+        if parts > 1:
+            ps_ctas = self.n_ctas if self.n_ctas > 0 else \
+                torch.cuda.get_device_properties(dev).multi_processor_count
+            ps = torch.empty(self.lib.rspi_sets_part_sums_floats(n_sets, ps_ctas),
+                             dtype=torch.float32, device=dev)
+        return dict(entries=entries, group_off=goff, total_groups=total, tile=4, sets=True,
+                    set_frames=set_frames, col_of_frame=col_of_frame, n_sets=n_sets,
+                    frame_groups=frame_groups, n_parts=parts, part_w=part_w, part_sums=ps,
+                    part_sums_ctas=ps_ctas, counts=counts)
+
     def _eps_rows(self):
         """Prefix sums of each frame's FP32 summation length for the
         candidate threshold's eps_d (the 'rows' of 2^-24 (rows + 8) photons
@@ -517,6 +597,8 @@ class EStep:
                  ptr(self.holo_pairs), s)
         if self.form != 'fp64':
             self.lmax.zero_()
+        if self.col_of_frame is not None:
+            self.frame_max.zero_()
 
     def rot_slices(self, r0, r1, out=None):
         """a6: rotated log-slices of rows [r0, r1) into ``out`` (or the chunk buffer)."""
@@ -533,6 +615,12 @@ class EStep:
                  cur_stream())
             return self.lsl_hi
         out = self.lsl if out is None else out
+        if self.kernel == 'sets':
+            w = self.wide
+            call('rspi_rot_log_slices_sets', ptr(self.holo_pairs), self.n_states0, self.num_rot,
+                 ptr(self.rot_cs), self.size, ptr(self.bg), ptr(self.sel_pix), self.n_sel,
+                 w['n_parts'], w['part_w'], r0, r1, ptr(out), ptr(self.lmax), cur_stream())
+            return out
         call('rspi_rot_log_slices_pairs', ptr(self.holo_pairs), self.n_states0, self.num_rot,
              ptr(self.rot_cs), self.size, ptr(self.bg), ptr(self.sel_pix), self.n_sel,
              self.p_row, r0, r1, ptr(out), self.slice_code,
@@ -573,6 +661,15 @@ class EStep:
                  ptr(w['pair_frames']), w['n_pairs'], w['n_parts'], w['part_w'], r0, r1,
                  ptr(self.prob[r0]), n, ptr(w['part_sums']), w['part_sums_ctas'], self.warps,
                  self.n_ctas, cur_stream())
+        elif self.kernel == 'sets':
+            w = self.wide
+            if w['n_parts'] > 1 and self.n_ctas > 0 and self.n_ctas != w['part_sums_ctas']:
+                w = self.wide = self._sets_entries()
+            call('rspi_screen_loglike_sets', ptr(lsl), self.num_rot, ptr(self.init),
+                 ptr(self.ph.scales), ptr(w['entries']), ptr(w['group_off']),
+                 ptr(w['set_frames']), w['n_sets'], w['n_parts'], w['part_w'], r0, r1,
+                 ptr(self.prob[r0]), self.n_cols, ptr(w['part_sums']), w['part_sums_ctas'],
+                 ptr(self.frame_max), self.warps, self.n_ctas, ptr(self.ph.err.t), cur_stream())
         elif self.kernel == 'stream' and self.form == 'screen':
             l16 = self.ll16
             call('rspi_loglike_stream', 0, ptr(lsl), self.p_row, self.num_rot, ptr(self.init),
@@ -608,17 +705,28 @@ class EStep:
             call('rspi_frame_reduce', ptr(self.prob), self.prob_code, self.n_rows, n,
                  ptr(self.maxll), ptr(self.rmax), ptr(self.logz), s)
             return self.maxll, self.rmax, self.logz
-        call('rspi_frame_reduce', ptr(self.prob), 0, self.n_rows, n, ptr(self.max32),
-             ptr(self.rmax32), None, s)
+        cols = self.col_of_frame is not None
+        if cols:
+            # the screening kernel already folded each column's maximum into
+            # its key
+            call('rspi_frame_max_finalize', ptr(self.frame_max), ptr(self.frame_of_col),
+                 self.n_cols, ptr(self.max32), ptr(self.rmax32), s)
+        else:
+            call('rspi_frame_reduce', ptr(self.prob), 0, self.n_rows, n, ptr(self.max32),
+                 ptr(self.rmax32), None, s)
         while True:
             dense = self.form == 'dense'
             rows_eq = self.eq_row_off if dense else self._eps_rows()
-            call('rspi_screen_candidates', ptr(self.prob), self.n_rows, n, ptr(self.max32),
-                 ptr(self.rmax32), ptr(self.ll['frame_sel_photons']), ptr(rows_eq),
-                 ptr(self.lmax_eps if dense else self.lmax),
-                 self.delta, ptr(self.cnt_part), ptr(self.cand_n), ptr(self.noncand),
-                 ptr(self.thr), ptr(self.cand_off), self.capacity, ptr(self.cand_d),
-                 ptr(self.cand_r), ptr(self.ph.err.t), s)
+            tail = (ptr(self.rmax32), ptr(self.ll['frame_sel_photons']), ptr(rows_eq),
+                    ptr(self.lmax_eps if dense else self.lmax), self.delta, ptr(self.cnt_part),
+                    ptr(self.cand_n), ptr(self.noncand), ptr(self.thr), ptr(self.cand_off),
+                    self.capacity, ptr(self.cand_d), ptr(self.cand_r), ptr(self.ph.err.t), s)
+            if cols:
+                call('rspi_screen_candidates_cols', ptr(self.prob), self.n_rows, self.n_cols,
+                     ptr(self.frame_of_col), n, ptr(self.max32), *tail)
+            else:
+                call('rspi_screen_candidates', ptr(self.prob), self.n_rows, n, ptr(self.max32),
+                     *tail)
             if self.check_capacity:
                 total = int(self.cand_off[n].item())
                 if total > self.capacity:
@@ -631,14 +739,27 @@ class EStep:
                     continue
                 self.n_candidates = total
             break
-        call('rspi_rescore', ptr(self.cand_d), ptr(self.cand_r), ptr(self.cand_off), n,
-             self.capacity, self.n_rows, ptr(self.holo), self.num_rot, ptr(self.rot_cs),
-             self.size, ptr(self.bg), ptr(self.sel_pix), self.n_sel, self.p_pad, ptr(self.init),
-             ptr(self.ph.scales), ptr(self.ll['entries']), ptr(self.ll['row_off']),
-             ptr(self.row_cnt), ptr(self.row_cand_off), ptr(self.row_cand), ptr(self.cand_ll),
-             ptr(self.prob), ptr(self.max32), ptr(self.noncand), ptr(self.maxll),
-             ptr(self.rmax), ptr(self.logz), ptr(self.row_scratch), self.scratch_rows, s)
+        head = (ptr(self.cand_d), ptr(self.cand_r), ptr(self.cand_off), n, self.capacity,
+                self.n_rows, ptr(self.holo), self.num_rot, ptr(self.rot_cs), self.size,
+                ptr(self.bg), ptr(self.sel_pix), self.n_sel, self.p_pad, ptr(self.init),
+                ptr(self.ph.scales), ptr(self.ll['entries']), ptr(self.ll['row_off']),
+                ptr(self.row_cnt), ptr(self.row_cand_off), ptr(self.row_cand), ptr(self.cand_ll),
+                ptr(self.prob))
+        tail = (ptr(self.max32), ptr(self.noncand), ptr(self.maxll), ptr(self.rmax),
+                ptr(self.logz), ptr(self.row_scratch), self.scratch_rows, s)
+        if cols:
+            call('rspi_rescore_cols', *head, self.n_cols, ptr(self.col_of_frame), *tail)
+        else:
+            call('rspi_rescore', *head, *tail)
         return self.maxll, self.rmax, self.logz
+
+    def frame_prob(self):
+        """The likelihood matrix with frames in their own order (rows x
+        frames, the layout of emc.py's ``prob``): ``prob`` itself, or for the
+        frame-set kernel, whose columns are in set order, a reordered copy."""
+        if self.col_of_frame is None:
+            return self.prob
+        return self.prob.index_select(1, self.col_of_frame.long())
 
 
 class Merge:

@@ -54,6 +54,18 @@ SIGNATURES = {
                                            P]),
     'rspi_nll': (I, [I, I] + [P] * 7 + [L, P, L, P, L] + [P] * 18),
     'rspi_entries16_check': (I, [P, L, P, P]),
+    'rspi_sets_counts': (I, [P, P, L, I, I, I, P, P]),
+    'rspi_sets_steps': (I, [P, P, L, I, P, P]),
+    'rspi_sets_fill': (I, [P, P, I, I, I, P, P, L, P, P, P, P]),
+    'rspi_rot_log_slices_sets': (I, [P, L, L, P, L, P, P, L, I, I, L, L, P, P, P]),
+    'rspi_sets_part_sums_floats': (L, [L, I]),
+    'rspi_screen_loglike_sets': (I, [P, L, P, P, P, P, P, L, I, I, L, L, P, L, P, I, P, I, I,
+                                     P, P]),
+    'rspi_frame_max_finalize': (I, [P, P, L, P, P, P]),
+    'rspi_screen_candidates_cols': (I, [P, L, L, P, L, P, P, P, P, P, D, P, P, P, P, P, L, P, P,
+                                        P, P]),
+    'rspi_rescore_cols': (I, [P, P, P, L, L, L, P, L, P, L, P, P, L, L, P, P, P, P, P, P, P, P,
+                              P, L, P, P, P, P, P, P, P, L, P]),
     'rspi_loglike_stream': (I, [I, P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
     'rspi_posterior_pairs': (I, [P, L, L, P, D, P, P, P, L, P, P, P, P, P]),
     'rspi_merge_coverage': (I, [L, P, L, P, P]),
@@ -113,7 +125,10 @@ KERNELS_PER_CALL = {
     'rspi_screen_loglike7': 1, 'rspi_quad4_part_sums_floats': 0,
     'rspi_mean': 1, 'rspi_ll16_entry_rows': 1, 'rspi_ll16_entry_fill': 1, 'rspi_screen_candidates': 3, 'rspi_rescore': 5,
     'rspi_loglike_stream': 1, 'rspi_posterior_pairs': 3,
-    'rspi_entries16_check': 1, 'rspi_nll': 2, 'rspi_screen_candidates_noalloc': 3, 'rspi_merge_coverage': 1, 'rspi_merge': 2,
+    'rspi_entries16_check': 1, 'rspi_sets_counts': 1, 'rspi_sets_steps': 1,
+    'rspi_sets_fill': 1, 'rspi_rot_log_slices_sets': 1, 'rspi_sets_part_sums_floats': 0,
+    'rspi_screen_loglike_sets': 1, 'rspi_frame_max_finalize': 1,
+    'rspi_screen_candidates_cols': 3, 'rspi_rescore_cols': 5, 'rspi_nll': 2, 'rspi_screen_candidates_noalloc': 3, 'rspi_merge_coverage': 1, 'rspi_merge': 2,
     'rspi_dense_frames': 1, 'rspi_rot_log_split': 1, 'rspi_dense_loglike': 1,
     'rspi_maxlp_grid': 2, 'rspi_dense_frames_u8': 1, 'rspi_rot_log_fixed': 1,
     'rspi_dense_loglike_i8': 1,

@@ -1,8 +1,9 @@
 """Parity of the default screened form at the benchmark geometries.
 
 The golden and random cases are small detectors.  These tests run the
-default E-step (the screened form with its default kernel, the column-part
-split and frame ordering it chooses on its own) on data generated like the
+screened E-step (its default kernel and the four-row quad kernel, with the
+column-part split and frame ordering they choose on their own) on data
+generated like the
 benchmark's, at the 185x185 production geometry (24,912 likelihood pixels,
 the full 9 x 9 x 5 state grid x 180 rotations) and at the 101x101 small
 geometry (7 x 7 x 5 x 180), with more frames than one frame-ordering window:
@@ -46,15 +47,16 @@ def _setup(cfg, n_frames):
     return ds, ph, size, r['num_rot'], sx, sy, dia, model
 
 
+@pytest.mark.parametrize('kernel', [None, 'quad4'])
 @pytest.mark.parametrize('cfg,n_frames,parts', [(2, 700, 2), (1, 600, 1)])
-def test_default_screened_form_at_config_geometry(cfg, n_frames, parts):
+def test_screened_form_at_config_geometry(cfg, n_frames, parts, kernel):
     from rspi.device import EStep
     ds, ph, size, num_rot, sx, sy, dia, model = _setup(cfg, n_frames)
     _, pm = E.generate_masks(size)
-    es = EStep(ph, size, num_rot, sx, sy, dia, pm, ds['bg'], form='screen')
+    es = EStep(ph, size, num_rot, sx, sy, dia, pm, ds['bg'], form='screen', kernel=kernel)
     ref = EStep(ph, size, num_rot, sx, sy, dia, pm, ds['bg'], form='fp64')
-    # the kernel and column split the defaults pick at this geometry
-    assert es.kernel == 'quad4' and es.wide['n_parts'] == parts
+    # the column split the kernel picks at this geometry
+    assert es.wide['n_parts'] == parts
     dm = torch.from_numpy(model).cuda()
     es.run(dm)
     maxll, rmax, logz = es.reduce()
@@ -68,8 +70,8 @@ def test_default_screened_form_at_config_geometry(cfg, n_frames, parts):
     want, _, _ = E.calc_prob(model, ds, sx, sy, dia, size, num_rot, pm,
                              E.get_scales(ds, True), states=states)
     rows = np.concatenate([np.arange(s * num_rot, (s + 1) * num_rot) for s in states])
-    got32 = es.prob[torch.from_numpy(rows).cuda()].double().cpu().numpy()
-    got64 = ref.prob[torch.from_numpy(rows).cuda()].cpu().numpy()
+    got32 = es.frame_prob()[torch.from_numpy(rows).cuda()].double().cpu().numpy()
+    got64 = ref.frame_prob()[torch.from_numpy(rows).cuda()].cpu().numpy()
     assert np.max(np.abs(got32 - want) / np.abs(want)) <= RTOL_F32
     assert np.max(np.abs(got64 - want) / np.abs(want)) <= RTOL_F64
 
@@ -86,7 +88,7 @@ def test_default_screened_form_at_config_geometry(cfg, n_frames, parts):
     on_sub = sub_best >= full_best
     assert np.array_equal(rows[np.argmax(want, 0)][on_sub], r64[on_sub])
     # the whole FP32 matrix against the FP64 form's, every entry
-    a = es.prob.double()
-    b = ref.prob
+    a = es.frame_prob().double()
+    b = ref.frame_prob()
     rel = ((a - b).abs() / b.abs()).max().item()
     assert rel <= RTOL_F32, rel

@@ -174,7 +174,7 @@ def test_dense_estep_matches_oracle(name, gemm):
     torch.cuda.synchronize()
     want, _, _ = E.calc_prob(g['model_in_1'], ds, sx, sy, dia, size, num_rot, pm,
                              E.get_scales(ds, bool(g['need_scaling'])))
-    got = es.prob.cpu().numpy().astype(np.float64)
+    got = es.frame_prob().cpu().numpy().astype(np.float64)
     kmat = E.sparse_frames(ds, pm < 1)
     lsl = np.concatenate([E.log_slices_for_state(g['model_in_1'], sx[s], sy[s], dia[s], size,
                                                  ds['bg'], num_rot, pm < 1) for s in range(sx.size)])

@@ -155,7 +155,7 @@ def test_loglike_fp64_matches_reference(name, it):
     g = load_golden(name)
     _, es = _golden_estep(g)
     es.run(torch.from_numpy(g['model_in_%d' % it]).cuda())
-    prob = es.prob.cpu().numpy()
+    prob = es.frame_prob().cpu().numpy()
     np.testing.assert_allclose(prob, g['prob_%d' % it], rtol=RTOL_F64, atol=0)
     maxll, rmax, logz = es.reduce()
     assert np.array_equal(rmax.cpu().numpy(), g['rmax_%d' % it])
@@ -175,7 +175,7 @@ def test_screened_form_matches_fp64(name, it):
     model = torch.from_numpy(g['model_in_%d' % it]).cuda()
     es.run(model)
     ref.run(model)
-    screened = es.prob.cpu().numpy().astype(np.float64)
+    screened = es.frame_prob().cpu().numpy().astype(np.float64)
     want = g['prob_%d' % it]
     assert (np.abs(screened - want) / np.abs(want)).max() <= RTOL_F32
     maxll, rmax, logz = es.reduce()
@@ -219,7 +219,7 @@ def test_tiling_does_not_change_results(tile, warps, form, kernel):
     _, es = _golden_estep(g, states_per_tile=tile, warps=warps, form=form, kernel=kernel)
     es.run(torch.from_numpy(g['model_in_1']).cuda())
     rtol = 1e-14 if form == 'fp64' else 1e-6
-    np.testing.assert_allclose(es.prob.cpu().numpy(), ref.prob.cpu().numpy(), rtol=rtol)
+    np.testing.assert_allclose(es.frame_prob().cpu().numpy(), ref.frame_prob().cpu().numpy(), rtol=rtol)
 
 
 def test_kernel_choice_is_checked():
@@ -239,7 +239,7 @@ def test_stream_kernel_bit_identical_to_dynamic(name):
     m = torch.from_numpy(g['model_in_2']).cuda()
     a.run(m)
     b.run(m)
-    assert torch.equal(a.prob, b.prob)
+    assert torch.equal(a.frame_prob(), b.frame_prob())
 
 
 def test_chunked_slices_match_single_pass():
@@ -249,7 +249,7 @@ def test_chunked_slices_match_single_pass():
     _, es = _golden_estep(g, states_per_tile=2, slice_budget_bytes=7 * 32 * 8 * 2)
     assert es.chunk_rows < es.n_rows
     es.run(torch.from_numpy(g['model_in_1']).cuda())
-    np.testing.assert_allclose(es.prob.cpu().numpy(), ref.prob.cpu().numpy(), rtol=1e-14)
+    np.testing.assert_allclose(es.frame_prob().cpu().numpy(), ref.frame_prob().cpu().numpy(), rtol=1e-14)
 
 
 @pytest.mark.parametrize('form', ['fp64', 'screen'])
@@ -272,7 +272,7 @@ def test_random_shapes_vs_oracle(size, n, seed, kw, form):
     _, pm = E.generate_masks(size)
     with np.errstate(invalid='ignore', divide='ignore'):
         want, _, _ = E.calc_prob(model, ds, sx, sy, dia, size, num_rot, pm, E.get_scales(ds, True))
-    got = es.prob.cpu().numpy().astype(np.float64)
+    got = es.frame_prob().cpu().numpy().astype(np.float64)
     if np.isnan(want).all():
         assert np.isnan(got).all()
     else:
@@ -290,7 +290,7 @@ def test_screen_kernels_match_reference(name, kernel):
     _, es = _golden_estep(g, form='screen', kernel=kernel)
     for it in (1, 2):
         es.run(torch.from_numpy(g['model_in_%d' % it]).cuda())
-        screened = es.prob.cpu().numpy().astype(np.float64)
+        screened = es.frame_prob().cpu().numpy().astype(np.float64)
         want = g['prob_%d' % it]
         assert (np.abs(screened - want) / np.abs(want)).max() <= RTOL_F32
         _, rmax, _ = es.reduce()
@@ -319,7 +319,7 @@ def test_quad4_kernel_matches_stream_kernel(name, ds, need_scaling, parts, warps
         es.run(model)
         maxll, rmax, logz = es.reduce()
         torch.cuda.synchronize()
-        out[kernel] = (es.prob.cpu().numpy().astype(np.float64), maxll.cpu().numpy(),
+        out[kernel] = (es.frame_prob().cpu().numpy().astype(np.float64), maxll.cpu().numpy(),
                        rmax.cpu().numpy(), logz.cpu().numpy())
         if kernel == 'quad4':
             assert es.wide['n_parts'] == (parts or 1)
@@ -416,3 +416,157 @@ def test_paired_holo_slices_bit_identical(dtype, code):
         a, b = outs
         assert np.array_equal(a[0].view(np.uint8), b[0].view(np.uint8)), (r0, r1)
         assert a[1] == b[1] and a[1] > 0.
+
+
+@pytest.mark.parametrize('parts,warps', [(None, 32), (2, 16), (3, 7), (4, 32)])
+@pytest.mark.parametrize('name,ds,need_scaling', CASES, ids=[c[0] for c in CASES])
+def test_sets_kernel_matches_stream_kernel(name, ds, need_scaling, parts, warps):
+    """The frame-set kernel (column parts copied in by TMA one after another,
+    one lane per frame, running sums per column between parts, the
+    likelihood columns in set order) gives the plain streaming kernel's FP32
+    likelihoods within 1e-6 of the largest term, and the same FP64-rescored
+    argmax / maximum / log-sum-exp, on every case (empty, heavy and
+    single-frame data included)."""
+    size = int(round(np.sqrt(ds['num_pix'])))
+    num_rot = 5
+    sx, sy, dia, _ = E.generate_states(E.parse_triple('-1 1 3'), E.parse_triple('0 0 1'),
+                                       E.parse_triple('2 3 2'))
+    rng = np.random.default_rng(size)
+    model = torch.from_numpy(rng.random(size * size) + 1j * rng.random(size * size)).cuda()
+    out = {}
+    for kernel, tile, kw in (('stream', 2, {}), ('sets', 4, dict(screen_parts=parts))):
+        ph = _photons(ds, need_scaling)
+        es = _estep(ph, size, num_rot, sx, sy, dia, ds['bg'], form='screen', kernel=kernel,
+                    states_per_tile=tile, warps=warps, **kw)
+        es.run(model)
+        maxll, rmax, logz = es.reduce()
+        torch.cuda.synchronize()
+        ph.err.check('sets kernel')
+        out[kernel] = (es.frame_prob().cpu().numpy().astype(np.float64), maxll.cpu().numpy(),
+                       rmax.cpu().numpy(), logz.cpu().numpy())
+        if kernel == 'sets':
+            assert es.wide['n_parts'] == (parts or 1)
+    a, b = out['stream'], out['sets']
+    scale = np.abs(a[0]).max(0, keepdims=True) + 1.
+    assert np.all(np.abs(a[0] - b[0]) <= 1e-6 * scale)
+    assert np.array_equal(a[2], b[2])
+    np.testing.assert_allclose(a[1], b[1], rtol=1e-14)
+    np.testing.assert_allclose(a[3], b[3], rtol=1e-12)
+
+
+@pytest.mark.parametrize('n,parts', [(61, 1), (300, 2), (45, 3), (33, 4)])
+def test_sets_layout_entries(n, parts):
+    """Frame sets: every frame's photons of each column part once, in its own
+    lane; at every step the eight lanes of each quarter warp read eight
+    distinct bank classes (column mod 8); other slots hold the zero column of
+    the slot's class; each (set, part) range has ceil(D / 4) groups, D the
+    fewest steps any schedule needs (largest frame or class total of a
+    quarter warp); frames in decreasing photon order, rank 32 s + p + 4 f in
+    lane 8 p + f; column of frame d = its slot."""
+    size = 37
+    d = random_photons(size, n, 40. * size, 15, empty_frames=(2, 9), heavy=5)
+    ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
+                         d['count_multi'], size * size, False)
+    sx, sy, dia, _ = E.generate_states(E.parse_triple('0 0 1'), E.parse_triple('0 0 1'),
+                                       E.parse_triple('2 2 1'))
+    es = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen',
+                kernel='sets', screen_parts=parts)
+    torch.cuda.synchronize()
+    w = es.wide
+    pw, ns = w['part_w'], w['n_sets']
+    assert w['n_parts'] == parts and pw % 8 == 0 and parts * pw >= es.p_row - 32
+    ent = w['entries'].cpu().numpy().view(np.uint16).reshape(-1, 32, 4).astype(np.int64)
+    goff = w['group_off'].cpu().numpy()
+    sf = w['set_frames'].cpu().numpy()
+    cof = es.col_of_frame.cpu().numpy()
+    assert goff.size == parts * ns + 1 and np.all(np.diff(goff) >= 0)
+    photons = frame_photons16(es)
+    tot = np.array([p.size for p in photons])
+    order = np.argsort(-tot, kind='stable')
+    k = np.arange(ns * 32)
+    src = (k - k % 32) + (k % 32) // 8 + 4 * (k % 8)
+    want_sf = np.where(src < n, order[np.minimum(src, n - 1)], -1)
+    assert np.array_equal(sf, want_sf)
+    assert np.array_equal(cof[sf[sf >= 0]], k[sf >= 0])
+    for s in range(ns):
+        for h in range(parts):
+            blk = ent[goff[h * ns + s]:goff[h * ns + s + 1]]          # (G, 32, 4)
+            steps = blk.transpose(0, 2, 1).reshape(-1, 32)           # (4G, 32)
+            assert np.all(steps <= pw + 7)
+            for q in range(4):
+                cls = steps[:, 8 * q:8 * q + 8] % 8
+                assert all(len(set(row)) == 8 for row in cls), (s, h, q)
+            need = 0
+            for q in range(4):
+                m = np.zeros((8, 8), np.int64)
+                for f in range(8):
+                    fr = sf[32 * s + 8 * q + f]
+                    if fr >= 0:
+                        loc = photons[fr][photons[fr] // pw == h] % pw
+                        m[f] = np.bincount(loc % 8, minlength=8)
+                need = max(need, m.sum(1).max(), m.sum(0).max())
+            assert blk.shape[0] == -(-need // 4), (s, h)
+            for lane in range(32):
+                fr = sf[32 * s + lane]
+                col = steps[:, lane]
+                real = col < pw
+                assert np.all(col[~real] == pw + (col[~real] % 8))
+                if fr < 0:
+                    assert not real.any()
+                    continue
+                ref = photons[fr][photons[fr] // pw == h] % pw
+                assert np.array_equal(np.sort(col[real]), np.sort(ref)), (s, h, lane)
+
+
+@pytest.mark.parametrize('num_rot,r0,r1', [(5, 0, None), (8, 0, None), (8, 4, 20), (5, 3, 22),
+                                           (6, 7, 8)])
+def test_sets_slice_layout_bit_identical(num_rot, r0, r1):
+    """rspi_rot_log_slices_sets writes the bits of the row-major FP32 slices
+    (rspi_rot_log_slices_pairs) in the tile-interleaved part layout, for
+    row ranges that start and end inside a state's rotations, with the same
+    abs_max."""
+    from rspi.device import cur_stream, ptr
+    from rspi.lib import call
+    g = load_golden('case_b')
+    ds = golden_dataset(g)
+    size = int(g['size'])
+    sx, sy, dia, _ = golden_states(g)
+    es = _estep(_photons(ds, bool(g['need_scaling'])), size, num_rot, sx, sy, dia, ds['bg'],
+                form='screen', kernel='sets', screen_parts=2)
+    es.slices(torch.from_numpy(g['model_in_1']).cuda())
+    r1 = es.n_rows if r1 is None else r1
+    parts, pw = es.wide['n_parts'], es.wide['part_w']
+    ref = torch.full((r1 - r0, es.p_row), 7., dtype=torch.float32, device='cuda')
+    amax_a = torch.zeros(1, dtype=torch.float32, device='cuda')
+    call('rspi_rot_log_slices_pairs', ptr(es.holo_pairs), es.n_states0, es.num_rot,
+         ptr(es.rot_cs), es.size, ptr(es.bg), ptr(es.sel_pix), es.n_sel, es.p_row, r0, r1,
+         ptr(ref), 0, ptr(amax_a), cur_stream())
+    tiles = (r1 - r0 + 3) // 4
+    out = torch.full((tiles * parts * pw * 4,), 7., dtype=torch.float32, device='cuda')
+    amax_b = torch.zeros(1, dtype=torch.float32, device='cuda')
+    call('rspi_rot_log_slices_sets', ptr(es.holo_pairs), es.n_states0, es.num_rot,
+         ptr(es.rot_cs), es.size, ptr(es.bg), ptr(es.sel_pix), es.n_sel, parts, pw, r0, r1,
+         ptr(out), ptr(amax_b), cur_stream())
+    torch.cuda.synchronize()
+    a = ref.cpu().numpy()
+    b = out.cpu().numpy().reshape(tiles, parts, pw, 4)
+    for r in range(r1 - r0):
+        row = b[r // 4, :, :, r % 4].reshape(-1)           # parts * pw columns
+        want = np.zeros(parts * pw, np.float32)
+        want[:es.n_sel] = a[r, :es.n_sel]
+        assert np.array_equal(row.view(np.uint32), want.view(np.uint32)), r
+    assert float(amax_a.item()) == float(amax_b.item()) > 0.
+
+
+def test_sets_fused_frame_maximum():
+    """The screened maximum and first-index argmax folded into the frame-set
+    kernel's stores equal those of the FP32 matrix it wrote."""
+    g = load_golden('case_b')
+    _, es = _golden_estep(g, form='screen', kernel='sets')
+    es.run(torch.from_numpy(g['model_in_2']).cuda())
+    m = es.frame_prob().cpu().numpy()   # before the rescoring refines candidates
+    es.reduce()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(es.rmax32.cpu().numpy(), np.argmax(m, 0))
+    np.testing.assert_array_equal(es.max32.cpu().numpy(), m.max(0).astype(np.float64))
+    assert not bool(es.frame_max.any())   # reset for the next pass

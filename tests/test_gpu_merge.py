@@ -50,7 +50,7 @@ def test_posterior_normalisation(name):
     _, es, mg = _setup(g, 'fp64')
     es.run(torch.from_numpy(g['model_in_2']).cuda())
     _, _, logz = es.reduce()
-    post = torch.exp(es.prob - logz[None, :]).cpu().numpy()
+    post = torch.exp(es.frame_prob() - logz[None, :]).cpu().numpy()
     want_logz, want = E.posterior(g['prob_2'])
     np.testing.assert_allclose(logz.cpu().numpy(), want_logz, rtol=1e-12)
     np.testing.assert_allclose(post, want, rtol=1e-9, atol=1e-300)

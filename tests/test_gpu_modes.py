@@ -60,7 +60,7 @@ def test_estep_two_modes_matches_oracle(form):
     assert es.n_rows == want.shape[0] == 2 * sx.size * num_rot
     np.testing.assert_allclose(float(es.vscale.item()), vs, rtol=RTOL_F64)
     if form == 'fp64':
-        np.testing.assert_allclose(es.prob.cpu().numpy(), want, rtol=RTOL_F64,
+        np.testing.assert_allclose(es.frame_prob().cpu().numpy(), want, rtol=RTOL_F64,
                                    atol=RTOL_F64 * np.abs(want).max())
     mx, am = E.get_rmax(want)
     assert np.array_equal(rmax.cpu().numpy(), am)            # argmax bit-exact

@@ -72,7 +72,7 @@ def test_product_estep_equals_reference_kernels(name, form):
     maxll, rmax, _ = es.reduce()
     torch.cuda.synchronize()
     if form == 'fp64':
-        np.testing.assert_allclose(es.prob.cpu().numpy(), want, rtol=1e-11,
+        np.testing.assert_allclose(es.frame_prob().cpu().numpy(), want, rtol=1e-11,
                                    atol=1e-11 * np.abs(want).max())
     assert np.array_equal(rmax.cpu().numpy(), want.argmax(0).astype('i4'))
     np.testing.assert_allclose(maxll.cpu().numpy(), want.max(0), rtol=1e-11)

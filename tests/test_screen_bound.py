@@ -102,3 +102,65 @@ def test_chain_fits_the_threshold_budget():
     for g in range(0, 200):
         for p in range(1, 5):
             assert g + 5 + max(0, p - 2) <= g + 8
+
+
+def _sets_lane_sum(slots):
+    """One lane of the frame-set kernel over its groups (four slots each,
+    zero-column slots hold 0): group trees (v0 + v1) + (v2 + v3) go
+    alternately into a0 and a1, then a0 + a1 -- float32."""
+    g = slots.reshape(-1, 4).astype(F)
+    a0, a1 = F(0.), F(0.)
+    for i in range(g.shape[0]):
+        t = F(F(g[i, 0] + g[i, 1]) + F(g[i, 2] + g[i, 3]))
+        if i % 2 == 0:
+            a0 = F(a0 + t)
+        else:
+            a1 = F(a1 + t)
+    return F(a0 + a1)
+
+
+def test_sets_summation_within_its_rounding_chain():
+    """k_screen_sets: per part a frame's photons sit in some of its lane's
+    4 G slots (G = the set's group count there); each value passes through at
+    most ceil(G / 2) + 3 FP32 roundings per part, parts after the first add
+    in FP64 (a stored running sum between parts when P > 2), so the chain
+    ceil(Gmax / 2) + 3 + max(0, P - 2) fits rows + 8 with rows = ceil(Gmax / 2)
+    (what the threshold is given for each frame)."""
+    rng = np.random.default_rng(20261)
+    scales = [
+        lambda r, n: r.normal(-8., 3., n),
+        lambda r, n: -r.uniform(0., 1000., n),
+        lambda r, n: np.where(r.random(n) < 0.5, 1e4, 1.) * r.normal(0., 1., n),
+        lambda r, n: np.full(n, 1. + 2. ** -20) * np.where(np.arange(n) % 2, 1., -1.),
+    ]
+    worst = 0.
+    for trial in range(400):
+        n = int(rng.integers(0, 500))
+        n_parts = int(rng.integers(1, 5))
+        values = scales[trial % len(scales)](rng, n).astype(F)
+        part_of = rng.integers(0, n_parts, n)
+        groups = []
+        run = 0.
+        for h in range(n_parts):
+            v = values[part_of == h]
+            g = -(-v.size // 4) + int(rng.integers(0, 4))      # the set may need more
+            groups.append(g)
+            slots = np.zeros(4 * g, dtype=F)
+            slots[rng.permutation(4 * g)[:v.size]] = v
+            s = float(_sets_lane_sum(slots))
+            if h == n_parts - 1:
+                run = run + s if h > 0 else s
+            elif h == 0:
+                run = float(F(s))
+            else:
+                run = float(F(run + s))
+        exact = math.fsum(float(x) for x in values)
+        gmax = max(groups) if groups else 0
+        rows = -(-gmax // 2)
+        chain = rows + 3 + max(0, n_parts - 2)
+        assert chain <= rows + 8
+        bound = U32 * chain * float(np.sum(np.abs(values.astype(np.float64))))
+        assert abs(run - exact) <= bound, (trial, n, n_parts)
+        if bound > 0:
+            worst = max(worst, abs(run - exact) / bound)
+    print('largest error / chain bound: %.3g' % worst)

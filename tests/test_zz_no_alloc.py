@@ -26,7 +26,7 @@ def _screened():
     ph = DevicePhotons(ds['ones'], ds['multi'], ds['place_ones'], ds['place_multi'],
                        ds['count_multi'], ds['num_pix'], bool(g['need_scaling']))
     _, pm = E.generate_masks(size)
-    es = EStep(ph, size, num_rot, sx, sy, dia, pm, ds['bg'], form='screen')
+    es = EStep(ph, size, num_rot, sx, sy, dia, pm, ds['bg'], form='screen', kernel='stream')
     es.run(torch.from_numpy(g['model_in_1']).cuda())
     call('rspi_frame_reduce', ptr(es.prob), 0, es.n_rows, ph.num_data, ptr(es.max32),
          ptr(es.rmax32), None, cur_stream())

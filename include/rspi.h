@@ -644,6 +644,40 @@ int rspi_nll(int precision, int want_grad, const int *ones, const int *multi,
              const double *scale, double *nll, double *gfre, double *gfim, double *gdia,
              double *gsx, double *gsy, double *gscale, int *err, cudaStream_t stream);
 
+/* ------------------------------------------------------------ model refinement
+ * Error reduction and difference map after the pattern search
+ * (MaxLPhaser.proj_fourier / proj_real / er / diffmap / _get_support /
+ * _improve_model, maxLP.py:271-298, 342-354).  Images are size x size
+ * complex128 (row-major pixel t = x*size + y, 2 <= size <= 1024), masks one
+ * byte per pixel (non-zero = true).  The centred transforms are NumPy's
+ * fftshift(fftn(ifftshift(.))) and fftshift(ifftn(ifftshift(.))) as
+ * line DFTs with the phase index reduced mod size in integer arithmetic.
+ * work holds 8 * size^2 doubles.
+ * rspi_cdft2: out = the centred forward (inverse = 0) or inverse (1) 2-D
+ *   transform of in.
+ * rspi_phase_support: minvsupp = !(G * |re(centred inverse of fconv *
+ *   expit((mrad - taper_radius) * taper_slope))| > threshold), G the
+ *   normalised Gaussian of `sigma` and half-width `radius` ('reflect'
+ *   edges) along axis 0 then axis 1 (the reference: 12, 0.5, 3, 12, 1.2e-4).
+ * rspi_phase_proj_fourier: out = x with the pixels of minvmask from fconv.
+ * rspi_phase_proj_real: out = centred forward transform of the real part of
+ *   the centred inverse transform of x, negatives and minvsupp pixels 0.
+ * rspi_phase_refine: x <- n_dm difference-map steps
+ *   x + proj_real(2 p - x) - p, p = proj_fourier(fconv, x), then n_er
+ *   error-reduction steps x <- proj_real(proj_fourier(fconv, x)). */
+int rspi_cdft2(const double *in, double *out, double *work, long long size, int inverse,
+               cudaStream_t stream);
+int rspi_phase_support(const double *fconv, long long size, double taper_radius,
+                       double taper_slope, double sigma, int radius, double threshold,
+                       unsigned char *minvsupp, double *work, cudaStream_t stream);
+int rspi_phase_proj_fourier(const double *fconv, const unsigned char *minvmask, const double *x,
+                            double *out, long long size, cudaStream_t stream);
+int rspi_phase_proj_real(const double *x, const unsigned char *minvsupp, double *out,
+                         double *work, long long size, cudaStream_t stream);
+int rspi_phase_refine(const double *fconv, const unsigned char *minvmask,
+                      const unsigned char *minvsupp, double *x, double *work, long long size,
+                      int n_dm, int n_er, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

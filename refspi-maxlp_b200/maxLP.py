@@ -22,6 +22,7 @@ import torch
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 from rspi import geometry  # noqa: E402
 from rspi.device import MStep, cur_stream, ptr  # noqa: E402
+from rspi import lib as rlib  # noqa: E402
 from rspi.lib import call  # noqa: E402
 
 
@@ -47,6 +48,16 @@ class MaxLPhaser():
         self.mean_count = dataset.photons.mean_count
         self.mstep = MStep(dataset.photons, size, num_iter, n_modes=self.num_modes,
                            screen=screen)
+        # model-refinement masks (maxLP.py:28-33): integer-centred radius, the
+        # pixels the Fourier projection takes from the data, the support
+        mx, my = np.indices((size,) * 2, dtype='f8')
+        self.mx_ind = torch.from_numpy(mx.ravel() - size // 2).to(self.device)
+        self.my_ind = torch.from_numpy(my.ravel() - size // 2).to(self.device)
+        self.mrad = torch.sqrt(self.mx_ind ** 2 + self.my_ind ** 2)
+        self.minvsuppmask = torch.ones((size,) * 2, dtype=torch.bool, device=self.device)
+        self.minvmask = self._get_invmask(4)
+        self.badpixmask = torch.ones(size ** 2, dtype=torch.bool, device=self.device)
+        self._phase_work = None
 
     def _gen_pattern(self, nmax):
         '''33x33 candidate offsets (maxLP.py:45-48)'''
@@ -269,6 +280,97 @@ class MaxLPhaser():
         self.mstep.run(fconv, ref_params, rot_cs)
         out = fconv.cpu().numpy().reshape(model.shape)
         self.dset.photons.err.check('MaxLP phaser')
+        return out
+
+    # -- model refinement: error reduction and difference map --------------
+    # (maxLP.py:271-298, 342-354) through librspi's centred transforms; the
+    # images are flat complex128 CUDA tensors of size**2 pixels.
+
+    def _get_invmask(self, r):
+        '''Pixels taken from the data by the Fourier projection: r <= mrad <
+        size//2 (maxLP.py:71-75)'''
+        self.minvmask = (self.mrad >= r) & (self.mrad < self.size // 2)
+        return self.minvmask
+
+    def _image(self, x):
+        t = torch.as_tensor(np.asarray(x) if not torch.is_tensor(x) else x)
+        t = t.to(self.device, torch.complex128).reshape(-1).contiguous()
+        if t.numel() != self.size ** 2:
+            raise ValueError('an image of %d pixels is required' % self.size ** 2)
+        return t
+
+    @staticmethod
+    def _bytes(mask):
+        return mask.reshape(-1).to(torch.uint8).contiguous()
+
+    def _work(self):
+        if self._phase_work is None:
+            self._phase_work = torch.empty(8 * self.size ** 2, dtype=torch.float64,
+                                           device=self.device)
+        return self._phase_work
+
+    def proj_fourier(self, fconv, x):
+        '''x with the data pixels (minvmask) replaced by fconv\'s
+        (maxLP.py:271-274)'''
+        fconv, x = self._image(fconv), self._image(x)
+        out = torch.empty_like(x)
+        call('rspi_phase_proj_fourier', ptr(fconv), ptr(self._bytes(self.minvmask)), ptr(x),
+             ptr(out), self.size, cur_stream())
+        return out
+
+    def proj_real(self, x):
+        '''Real-space projection (maxLP.py:276-280): real part of the centred
+        inverse transform, negatives and pixels outside the support set to 0,
+        transformed back'''
+        x = self._image(x)
+        out = torch.empty_like(x)
+        call('rspi_phase_proj_real', ptr(x), ptr(self._bytes(self.minvsuppmask)), ptr(out),
+             ptr(self._work()), self.size, cur_stream())
+        return out
+
+    def _refine(self, fconv, x, n_dm, n_er):
+        fconv = self._image(fconv)
+        out = self._image(x).clone()
+        call('rspi_phase_refine', ptr(fconv), ptr(self._bytes(self.minvmask)),
+             ptr(self._bytes(self.minvsuppmask)), ptr(out), ptr(self._work()), self.size,
+             int(n_dm), int(n_er), cur_stream())
+        rlib.launch_count += 5 * (int(n_dm) + int(n_er))
+        return out
+
+    def er(self, fconv, x):
+        '''One error-reduction step (maxLP.py:282-284)'''
+        return self._refine(fconv, x, 0, 1)
+
+    def diffmap(self, fconv, x):
+        '''One difference-map step (maxLP.py:286-289)'''
+        return self._refine(fconv, x, 1, 0)
+
+    def _get_support(self, fconv):
+        '''True outside the support (maxLP.py:292-298): fconv tapered by
+        expit((mrad - 12) / 2), centred inverse transform, |real part|
+        smoothed by a sigma-3 Gaussian, not above 1.2e-4'''
+        fconv = self._image(fconv)
+        supp = torch.empty(self.size ** 2, dtype=torch.uint8, device=self.device)
+        call('rspi_phase_support', ptr(fconv), self.size, 12., 0.5, 3., 12, 1.2e-4, ptr(supp),
+             ptr(self._work()), cur_stream())
+        return supp.bool().reshape((self.size,) * 2)
+
+    def _get_tot_mask(self, fconv):
+        '''Data mask without the pixels whose real part is at or below -0.2
+        (maxLP.py:299-302)'''
+        self.badpixmask = self._image(fconv).real > -0.2
+        return self.badpixmask & self.minvmask
+
+    def _improve_model(self, fconv, update_masks=True):
+        '''Support from fconv (with update_masks), then 10 difference-map and
+        5 error-reduction iterations starting from fconv (maxLP.py:342-354);
+        a complex128 CUDA tensor of size**2 pixels'''
+        print('Starting diffmap and er')
+        fconv = self._image(fconv)
+        if update_masks is True:
+            self.minvsuppmask = self._get_support(fconv)
+        out = self._refine(fconv, fconv, 10, 5)
+        print('Done...')
         return out
 
     def run_from_rmax(self, fconv, rmax, num_rot, state_values, rot_cs):

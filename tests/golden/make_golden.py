@@ -13,7 +13,10 @@ lists, config values, start model) and the reference outputs:
 * for iterations 1 and 2 of ``EMC.run_iteration``: ``prob``, ``rmax`` and
   the model after the MaxLP M-step;
 * MaxLPhaser pieces for a few pixels: photons, reference amplitudes,
-  per-candidate rescale and log-likelihood.
+  per-candidate rescale and log-likelihood;
+* the model refinement of MaxLPhaser._improve_model (support mask, one
+  difference-map and one error-reduction step, the refined model) on the
+  iteration-2 model, and in ``phase_a.npz`` on a compact 61x61 object.
 
 Run from the repository root: ``python tests/golden/make_golden.py``.
 Needs the reference tree (default ``/root/reference``).
@@ -76,6 +79,60 @@ def _write_inputs(tmp, name, c):
                  c['shiftx'], c['shifty']))
     os.makedirs(os.path.join(tmp, 'out'), exist_ok=True)
     return data, bg, cfg
+
+
+def _phase_outputs(ph, fconv, sink):
+    """The reference's ER / difference-map pieces on one model: the support
+    mask of _improve_model (maxLP.py:292-298), one diffmap and one er step
+    from the model itself (maxLP.py:282-289), and _improve_model's result
+    (10 difference-map + 5 error-reduction iterations, maxLP.py:342-354)."""
+    with contextlib.redirect_stdout(sink), contextlib.redirect_stderr(sink):
+        fout = np.asarray(ph._improve_model(fconv.copy())).ravel()
+        supp = np.asarray(ph.minvsuppmask).ravel()
+        dm1 = np.asarray(ph.diffmap(fconv.copy(), fconv.copy())).ravel()
+        er1 = np.asarray(ph.er(fconv.copy(), fconv.copy())).ravel()
+    return dict(phase_in=fconv.copy(), phase_supp=supp, phase_dm1=dm1, phase_er1=er1,
+                phase_out=fout, phase_invmask=np.asarray(ph.minvmask).ravel())
+
+
+def run_phase_case(size=61, seed=13):
+    """A model refinement case with a compact object: the Fourier transform
+    of a blob density of radius 8 px plus noise, so the support is a proper
+    subset of the image; run through a MaxLPhaser of the reference built on
+    a two-frame photons file of that size."""
+    rng = np.random.default_rng(seed)
+    # densities of ~1e-2, so that the support threshold 1.2e-4 of
+    # maxLP.py:296 cuts the smoothed object's tails
+    obj = 1e-2 * synth.make_object(size, 10, 8., rng)
+    f = synth.fourier(obj)
+    f = f + 0.05 * np.abs(f).mean() * (rng.standard_normal(f.shape) +
+                                       1j * rng.standard_normal(f.shape))
+    with tempfile.TemporaryDirectory() as tmp:
+        import h5py  # the stand-in
+        path = os.path.join(tmp, 'photons.h5')
+        with h5py.File(path, 'w') as fh:
+            fh['num_pix'] = np.array([size ** 2])
+            fh['ones'] = np.array([1, 1], dtype='i4')
+            fh['multi'] = np.array([0, 0], dtype='i4')
+            po = np.empty(2, dtype=object)
+            po[0], po[1] = np.array([0], 'i4'), np.array([1], 'i4')
+            pm = np.empty(2, dtype=object)
+            pm[0], pm[1] = np.zeros(0, 'i4'), np.zeros(0, 'i4')
+            fh['place_ones'] = po
+            fh['place_multi'] = pm
+            fh['count_multi'] = pm
+        cwd = os.getcwd()
+        os.chdir(REF)
+        try:
+            import maxLP as ref_maxlp
+            sink = io.StringIO()
+            with contextlib.redirect_stdout(sink), contextlib.redirect_stderr(sink):
+                ph = ref_maxlp.MaxLPhaser(path, size=size)
+            out = _phase_outputs(ph, f.ravel().astype(np.complex128), sink)
+        finally:
+            os.chdir(cwd)
+    out['size'] = np.array(size)
+    return out
 
 
 def run_case(name, c):
@@ -154,6 +211,8 @@ def run_case(name, c):
                        ph_rescale=np.array(rs_l), ph_logq=np.array(lq_l), ph_cand=np.array(cand_l),
                        ph_shifts=np.asarray(ph.shifts), ph_diams=np.asarray(ph.diams),
                        ph_ang=np.asarray(ph.ang))
+            # model refinement (maxLP.py:271-354) on the iteration-2 model
+            out.update(_phase_outputs(ph, np.asarray(out['model_out_2']).ravel(), sink))
         finally:
             os.chdir(cwd)
     out.update(model0=model0, size=np.array(c['size']), num_rot=np.array(c['num_rot']),
@@ -178,6 +237,9 @@ def main():
         path = os.path.join(HERE, name + '.npz')
         np.savez_compressed(path, **res)
         print(name, '->', path, '%.1f KB' % (os.path.getsize(path) / 1024))
+    path = os.path.join(HERE, 'phase_a.npz')
+    np.savez_compressed(path, **run_phase_case())
+    print('phase_a ->', path, '%.1f KB' % (os.path.getsize(path) / 1024))
 
 
 if __name__ == '__main__':

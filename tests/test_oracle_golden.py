@@ -97,3 +97,26 @@ def test_posterior_normalises():
     np.testing.assert_allclose(post.sum(0), 1., rtol=1e-12)
     np.testing.assert_allclose(logz, np.log(np.exp(prob - prob.max(0)).sum(0)) + prob.max(0),
                                rtol=1e-14)
+
+
+@pytest.mark.parametrize('name', ['case_a', 'case_b', 'phase_a'])
+def test_phase_oracle_matches_reference(name):
+    """The model-refinement restatement (oracle/phase_oracle.py) against the
+    reference's own MaxLPhaser._improve_model / diffmap / er / _get_support
+    run on the same inputs (tests/golden/make_golden.py)."""
+    import os
+    from conftest import GOLDEN
+    from oracle import phase_oracle as P
+    g = np.load(os.path.join(GOLDEN, name + '.npz'))
+    size = int(g['size'])
+    f = g['phase_in']
+    inv = P.get_invmask(size)
+    assert np.array_equal(inv, g['phase_invmask'])
+    supp = P.get_support(f, size)
+    assert np.array_equal(supp, g['phase_supp'])
+    np.testing.assert_array_equal(P.diffmap(f, f, inv, supp, size), g['phase_dm1'])
+    np.testing.assert_array_equal(P.er(f, f, inv, supp, size), g['phase_er1'])
+    out, _ = P.improve_model(f, size)
+    np.testing.assert_array_equal(out, g['phase_out'])
+    if name == 'phase_a':
+        assert 0.5 < supp.mean() < 0.99   # a proper support, not the whole image

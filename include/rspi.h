@@ -644,6 +644,30 @@ int rspi_nll(int precision, int want_grad, const int *ones, const int *multi,
              const double *scale, double *nll, double *gfre, double *gfim, double *gdia,
              double *gsx, double *gsy, double *gscale, int *err, cudaStream_t stream);
 
+/* The E-step side of the adjoint: negative log-likelihood through model
+ * slicing for frames in given orientations (rot_cs[2d], rot_cs[2d + 1]: the
+ * cos, sin of frame d's angle, as rspi_rot_log_slices uses them) with
+ * continuous dia, sx, sy and scale per frame:
+ *   NLL = sum_d [ vscale s_d sum_{q in sel} W_d(q)
+ *                 - sum_{p in sel} K_d(p) (log s_d + L_d(p)) ]
+ * W_d = |M + r_d|^2 + bg (slice_gen_holo, kernels.cu:58-75), L_d(p) the
+ * bilinear rotated log-slice (slice_gen, kernels.cu:19-41; -1000, with no
+ * gradient, outside the detector or below 1e-20): minus calc_prob_all's
+ * value (kernels.cu:116-137, emc.py:194-199) with K_d log s_d added.
+ * model complex128 size^2; sel_pix the n_sel likelihood pixels, pix2sel
+ * their inverse map (-1 elsewhere).  With want_grad: gre/gim (size^2) and
+ * gdia/gsx/gsy/gscale (n_frames) receive dNLL/d(Re M, Im M, dia, sx, sy, s).
+ * precision 0: FP32 terms, 1: FP64; sums FP64.  No counterpart in the
+ * reference, which has no gradient of its likelihood. */
+int rspi_emc_nll(int precision, int want_grad, const double *model, long long size,
+                 const double *bg, const int *sel_pix, long long n_sel, const int *pix2sel,
+                 const int *ones, const int *multi, const long long *ones_accum,
+                 const long long *multi_accum, const int *place_ones, const int *place_multi,
+                 const int *count_multi, long long n_frames, const double *rot_cs,
+                 const double *dia, const double *sx, const double *sy, const double *scale,
+                 double vscale, double *nll, double *gre, double *gim, double *gdia,
+                 double *gsx, double *gsy, double *gscale, int *err, cudaStream_t stream);
+
 /* ------------------------------------------------------------ model refinement
  * Error reduction and difference map after the pattern search
  * (MaxLPhaser.proj_fourier / proj_real / er / diffmap / _get_support /

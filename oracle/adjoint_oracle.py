@@ -18,10 +18,17 @@ maxLP.py:197 (up to the frame-independent k log(rescale) terms).
 ``nll_torch`` evaluates it densely in torch FP64 so that torch.autograd
 gives the reference gradient; ``photon_matrix`` builds k_dt with the
 oracle's exact rotation (maxlp_oracle.photon_pixels).
+
+The E-step side (``emc_nll_torch``): minus the reference likelihood
+calc_prob_all (emc.py:194-199, kernels.cu:116-137) of each frame in its
+chosen orientation, differentiable in the complex model and the continuous
+diameter, shift and scale, with the Poisson term K_d log s_d that the
+reference drops (constant over states) kept.
 """
 import numpy as np
 import torch
 
+from . import emc_oracle as E
 from . import maxlp_oracle as M
 
 
@@ -82,3 +89,71 @@ def grid_pixel(k_d, fref_d, s_d, n_phase=64, n_amp=32):
         nll = (s_d[:, None] * w).sum(0) - (k_d[:, None] * np.log(w)).sum(0)
     idx = int(np.argmin(nll))
     return cand[idx], nll[idx], idx
+
+
+# ---------------------------------------------------------------------------
+# EMC side: the likelihood through model slicing (kernels.cu:6-82,116-137)
+# ---------------------------------------------------------------------------
+def emc_nll_torch(m_re, m_im, dia, sx, sy, scale, vscale, kmat, angles, size, bg, sel):
+    """Dense FP64 EMC negative log-likelihood, differentiable in torch:
+
+        NLL = sum_d [ vscale s_d sum_{q in sel} W_d(q)
+                      - sum_{p in sel} K_d(p) (log s_d + L_d(p)) ]
+
+    W_d = |M + ff(pi rho dia_d / size) e^{2 pi i ((x-c) sx_d + (y-c) sy_d)/size}|^2 + bg
+    (holo_slice, kernels.cu:58-75) and L_d the bilinear rotated log-slice of
+    W_d plus bg (rotate_slice with log_flag, kernels.cu:19-41; -1000 where
+    invalid, a constant).  ``m_*`` (P,), the per-frame parameters (N,),
+    ``kmat`` a scipy CSR (N, P) of photons, ``angles`` (N,) fixed, ``sel``
+    (P,) bool.  The bilinear indices and weights depend on the fixed angles
+    only."""
+    size = int(size)
+    x, y = np.indices((size, size), dtype='f8')
+    cen = np.floor(size / 2.)
+    dx = torch.tensor((x - cen).ravel())
+    dy = torch.tensor((y - cen).ravel())
+    rho = torch.sqrt(dx * dx + dy * dy)
+    bg_t = torch.tensor(np.asarray(bg, dtype='f8').ravel())
+    sel_t = torch.tensor(np.asarray(sel, dtype=bool).ravel())
+    s = rho[None, :] * np.pi * dia[:, None] / size
+    s = torch.where(s == 0., torch.full_like(s, 1.e-5), s)
+    ff = (torch.sin(s) - s * torch.cos(s)) / (s * s * s)
+    ph = 2. * np.pi * (dx[None, :] * sx[:, None] + dy[None, :] * sy[:, None]) / size
+    zr = torch.cos(ph) * ff + m_re[None, :]
+    zi = torch.sin(ph) * ff + m_im[None, :]
+    w = zr * zr + zi * zi + bg_t[None, :]                          # (N, P)
+    total = (vscale * scale * w[:, sel_t].sum(1)).sum()
+    for d in range(w.shape[0]):
+        row = kmat.getrow(d)
+        pix = row.indices[np.asarray(sel, dtype=bool).ravel()[row.indices]]
+        k = torch.tensor(np.asarray(kmat[d, pix].toarray()).ravel() if pix.size else np.zeros(0))
+        if pix.size == 0:
+            continue
+        ix, iy, fx, fy, valid = E.rotation_geometry(float(angles[d]), size)
+        ix, iy, fx, fy, valid = ix[pix], iy[pix], fx[pix], fy[pix], valid[pix]
+        ixc, iyc = np.where(valid, ix, 0), np.where(valid, iy, 0)
+        cx, cy = 1. - fx, 1. - fy
+        wd = w[d]
+        b = (wd[torch.tensor(ixc * size + iyc)] * torch.tensor(cx * cy) +
+             wd[torch.tensor((ixc + 1) * size + iyc)] * torch.tensor(fx * cy) +
+             wd[torch.tensor(ixc * size + iyc + 1)] * torch.tensor(cx * fy) +
+             wd[torch.tensor((ixc + 1) * size + iyc + 1)] * torch.tensor(fx * fy))
+        b = b + bg_t[torch.tensor(pix)]
+        ok = torch.tensor(valid) & (b >= 1.e-20)
+        logv = torch.where(ok, torch.log(torch.where(ok, b, torch.ones_like(b))),
+                           torch.full_like(b, E.LOG_SENTINEL))
+        total = total - (k * (torch.log(scale[d]) + logv)).sum()
+    return total
+
+
+def emc_nll_and_grad(model, dia, sx, sy, scale, vscale, kmat, angles, size, bg, sel):
+    """EMC NLL and its gradient (dM as d/dRe + i d/dIm over every pixel;
+    per-frame d/ddia, d/dsx, d/dsy, d/dscale) in FP64 via torch.autograd."""
+    t = lambda a: torch.tensor(np.asarray(a, dtype=np.float64), requires_grad=True)  # noqa: E731
+    model = np.asarray(model, dtype=np.complex128).ravel()
+    mr, mi = t(model.real), t(model.imag)
+    dd, xx, yy, ss = t(dia), t(sx), t(sy), t(scale)
+    loss = emc_nll_torch(mr, mi, dd, xx, yy, ss, float(vscale), kmat, angles, size, bg, sel)
+    loss.backward()
+    g = lambda v: v.grad.numpy().copy()  # noqa: E731
+    return float(loss.detach()), g(mr) + 1j * g(mi), g(dd), g(xx), g(yy), g(ss)

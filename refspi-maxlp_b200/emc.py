@@ -28,7 +28,11 @@ screening of the pattern-search candidates, FP64 for the finalists, same
 chosen candidates as false), ``slice_budget_gb`` (rotated slices are built
 in chunks of at most this size, default 8), ``cuda_graph`` (capture the whole
 device iteration once and replay it, default true), ``autotune`` (pick the
-likelihood kernel's tile shape by timing, default false).
+likelihood kernel's tile shape by timing, default false), ``mstep``
+(``pattern``, the default: the MaxLP pattern search; ``grid``: the polar grid
+search of the pixel NLL; ``lbfgs``: L-BFGS on that NLL through its
+hand-written adjoint, ``lbfgs_steps`` iterations, default 50;
+``grid+lbfgs``: the grid, then L-BFGS).
 
 ``num_modes`` (emc.py:59, parsed but unused by the reference) reconstructs
 that many models at once: the (shift, diameter) grid is repeated per mode,
@@ -132,6 +136,12 @@ class EMC():
         self.dense_gemm = config.get('emc', 'dense_gemm', fallback='auto')
         self.dense_rescore = config.getboolean('emc', 'dense_rescore', fallback=True)
         self.autotune = config.getboolean('emc', 'autotune', fallback=False)
+        self.mstep_kind = config.get('emc', 'mstep', fallback='pattern')
+        if self.mstep_kind not in ('pattern', 'grid', 'lbfgs', 'grid+lbfgs'):
+            raise ValueError('emc:mstep must be pattern, grid, lbfgs or grid+lbfgs')
+        if self.mstep_kind != 'pattern' and self.num_modes != 1:
+            raise ValueError('emc:mstep %s takes one mode' % self.mstep_kind)
+        self.lbfgs_steps = config.getint('emc', 'lbfgs_steps', fallback=50)
 
     def _generate_states(self, config):
         '''emc.py:67-87'''
@@ -195,10 +205,41 @@ class EMC():
 
     def _device_step(self):
         '''One iteration on device buffers: E-step, reduction, M-step.'''
+        self._estep_part()
+        self._mstep_part()
+
+    def _estep_part(self):
         self.estep.run(self._dmodel)
         self.estep.reduce()
-        self.phaser.run_from_rmax(self._dmodel, self.estep.rmax, self.num_rot, self.state_vals,
-                                  self.phaser_rot)
+
+    def _mstep_part(self):
+        '''The M-step on the E-step's argmax: the MaxLP pattern search
+        (maxLP.py:304-340, ``mstep = pattern``), or after its ring pass and
+        global rescale (maxLP.py:317-330) the polar grid search of the pixel
+        NLL (``grid``), L-BFGS on that NLL through its hand-written adjoint
+        (``lbfgs``, ``lbfgs_steps`` iterations), or the grid then L-BFGS
+        (``grid+lbfgs``) over the main phaser pixels.'''
+        if self.mstep_kind == 'pattern':
+            self.phaser.run_from_rmax(self._dmodel, self.estep.rmax, self.num_rot,
+                                      self.state_vals, self.phaser_rot)
+            return
+        from rspi.adjoint import NLLProblem, lbfgs_update
+        ms = self.phaser.mstep
+        n_ref = self.state_vals.shape[0]
+        ms.frame_params_from_rmax(self.estep.rmax, self.num_rot, n_ref)
+        ms.run(self._dmodel, self.state_vals, self.phaser_rot, main=False)
+        scale = self.dset.photons.scales * ms.rescale[0]
+        if 'grid' in self.mstep_kind:
+            ms.grid(self._dmodel, self.state_vals, self.phaser_rot, scale)
+        if 'lbfgs' in self.mstep_kind:
+            vals = self.state_vals[ms.fstate.long()]
+            ang = (ms.frot.double() * np.pi / self.num_rot).cpu().numpy()
+            prob = NLLProblem(self.dset.photons, self.size, ang, precision='fp32')
+            out, self.mstep_nll, _ = lbfgs_update(
+                prob, self._dmodel.cpu().numpy(), vals[:, 2].cpu().numpy(),
+                vals[:, 0].cpu().numpy(), vals[:, 1].cpu().numpy(), scale.cpu().numpy(),
+                steps=self.lbfgs_steps)
+            self._dmodel.copy_(torch.from_numpy(out))
 
     def device_step(self):
         '''The iteration on the device model buffer ``_dmodel``: eager the
@@ -207,8 +248,13 @@ class EMC():
         if not self.use_graph:
             self._device_step()
             return
+        # the graph holds the whole iteration, or with an adjoint-driven
+        # M-step (host-side L-BFGS line searches) the E-step only
+        part = self._device_step if self.mstep_kind == 'pattern' else self._estep_part
         if self._graph is not None:
             self._graph.replay()
+            if part is not self._device_step:
+                self._mstep_part()
             return
         self._device_step()
         torch.cuda.current_stream(self.device).synchronize()
@@ -219,7 +265,7 @@ class EMC():
         side.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(side):
             with torch.cuda.graph(graph, stream=side):
-                self._device_step()
+                part()
         torch.cuda.current_stream(self.device).wait_stream(side)
         self.estep.check_capacity = True
         self._dmodel.copy_(model_after)   # capture does not execute: keep the eager result

@@ -1,5 +1,6 @@
-"""Differentiable MaxLP negative log-likelihood (row a16) and an L-BFGS
-update that stands beside the pattern/grid search.
+"""Differentiable negative log-likelihoods (row a16): the MaxLP pixel NLL
+with an L-BFGS update that stands beside the pattern/grid search, and the
+E-step NLL through model slicing (``EMCNLLProblem`` / ``EMCNLL``).
 
 ``NLLProblem`` fixes the data (photons, frame orientations) and evaluates
 
@@ -120,3 +121,73 @@ def lbfgs_update(problem, model, dia, sx, sy, scale, steps=50, params=False, his
     out[problem.pixels] = (fre.detach() + 1j * fim.detach()).cpu().numpy()
     return out, final, (fd.detach().cpu().numpy(), fx.detach().cpu().numpy(),
                         fy.detach().cpu().numpy(), fs.detach().cpu().numpy())
+
+
+# ---------------------------------------------------------------------------
+# E-step side: the likelihood through model slicing (rspi_emc_nll)
+# ---------------------------------------------------------------------------
+class EMCNLLProblem:
+    """Fixed data of the E-step NLL: photons, frame orientations, the
+    likelihood pixels, background and vscale (kernels.cu:6-82,116-137)."""
+
+    def __init__(self, photons, size, rot_cs, probmask, bg, vscale, precision='fp32'):
+        if precision not in ('fp32', 'fp64'):
+            raise ValueError('precision must be fp32 or fp64')
+        self.ph = photons
+        self.size = int(size)
+        self.device = dev = photons.device
+        self.prec = 0 if precision == 'fp32' else 1
+        rc = torch.as_tensor(np.asarray(rot_cs, dtype='f8') if not torch.is_tensor(rot_cs)
+                             else rot_cs)
+        self.rot_cs = rc.to(dev, _f64).reshape(-1).contiguous()
+        if self.rot_cs.numel() != 2 * photons.num_data:
+            raise ValueError('one (cos, sin) pair per frame is required')
+        sel, pix2sel, _ = geometry.sel_pixels(probmask)
+        t = lambda a, dt=_f64: torch.as_tensor(np.ascontiguousarray(a)).to(dev, dt)  # noqa: E731
+        self.sel_pix = t(sel if sel.size else np.zeros(1, 'i4'), torch.int32)
+        self.n_sel = int(sel.size)
+        self.pix2sel = t(pix2sel, torch.int32)
+        self.bg = t(np.asarray(bg, dtype='f8').ravel())
+        self.vscale = float(vscale)
+        self.out = torch.empty(1, dtype=_f64, device=dev)
+
+    def evaluate(self, mre, mim, dia, sx, sy, scale, grad=False):
+        """NLL and, with ``grad``, (dRe M, dIm M, d dia, d sx, d sy, d scale)."""
+        n, npix = self.ph.num_data, self.size ** 2
+        c = lambda v: v.detach().to(self.device, _f64).contiguous()  # noqa: E731
+        model = torch.complex(c(mre), c(mim)).contiguous()
+        dia, sx, sy, scale = c(dia), c(sx), c(sy), c(scale)
+        g = ([torch.empty(npix, dtype=_f64, device=self.device) for _ in range(2)] +
+             [torch.empty(n, dtype=_f64, device=self.device) for _ in range(4)]) if grad \
+            else [None] * 6
+        ph = self.ph
+        call('rspi_emc_nll', self.prec, int(grad), ptr(model), self.size, ptr(self.bg),
+             ptr(self.sel_pix), self.n_sel, ptr(self.pix2sel), ptr(ph.ones), ptr(ph.multi),
+             ptr(ph.ones_accum), ptr(ph.multi_accum), ptr(ph.place_ones), ptr(ph.place_multi),
+             ptr(ph.count_multi), n, ptr(self.rot_cs), ptr(dia), ptr(sx), ptr(sy), ptr(scale),
+             self.vscale, ptr(self.out), *[ptr(x) for x in g], ptr(ph.err.t), cur_stream())
+        if grad:
+            return self.out.clone(), g
+        return self.out.clone()
+
+
+class EMCNLL(torch.autograd.Function):
+    """E-step NLL with the hand-written adjoint as its backward (the slices
+    are recomputed in backward; nothing frames x states is kept)."""
+
+    @staticmethod
+    def forward(ctx, mre, mim, dia, sx, sy, scale, problem):
+        ctx.save_for_backward(mre, mim, dia, sx, sy, scale)
+        ctx.problem = problem
+        return problem.evaluate(mre, mim, dia, sx, sy, scale, grad=False).reshape(())
+
+    @staticmethod
+    def backward(ctx, gout):
+        mre, mim, dia, sx, sy, scale = ctx.saved_tensors
+        _, g = ctx.problem.evaluate(mre, mim, dia, sx, sy, scale, grad=True)
+        outs = [x * gout for x in g]
+        return tuple(o.to(v.dtype) for o, v in zip(outs, (mre, mim, dia, sx, sy, scale))) + (None,)
+
+
+def emc_nll(problem, mre, mim, dia, sx, sy, scale):
+    return EMCNLL.apply(mre, mim, dia, sx, sy, scale, problem)

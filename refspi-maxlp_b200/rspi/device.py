@@ -908,8 +908,9 @@ class MStep:
              cur_stream())
         return best[:self.n_main]
 
-    def run(self, fconv, ref_params, rot_cs):
-        """Update ``fconv`` (complex128 device tensor, ``n_modes`` x P) in place."""
+    def run(self, fconv, ref_params, rot_cs, main=True):
+        """Update ``fconv`` (complex128 device tensor, ``n_modes`` x P) in place:
+        the ring pass and the global rescale, then (``main``) the main pass."""
         n_ref = int(ref_params.shape[0])
         nm = self.n_modes
         if fconv.numel() != nm * self.size ** 2:
@@ -928,6 +929,7 @@ class MStep:
                      ptr(self.rescale[m:]), s)
         else:
             self.rescale.fill_(float('nan'))   # np.mean of an empty ring
-        self._pattern(fconv, self.main, self.main_rows, self.n_main, hist, n_ref, 1,
-                      ptr(self.rescale), None, s)
+        if main:
+            self._pattern(fconv, self.main, self.main_rows, self.n_main, hist, n_ref, 1,
+                          ptr(self.rescale), None, s)
         return fconv

@@ -54,6 +54,8 @@ SIGNATURES = {
                                            P]),
     'rspi_nll': (I, [I, I] + [P] * 7 + [L, P, L, P, L] + [P] * 18),
     'rspi_entries16_check': (I, [P, L, P, P]),
+    'rspi_emc_nll': (I, [I, I, P, L, P, P, L, P, P, P, P, P, P, P, P, L, P, P, P, P, P, D, P,
+                         P, P, P, P, P, P, P, P]),
     'rspi_cdft2': (I, [P, P, P, L, I, P]),
     'rspi_phase_support': (I, [P, L, D, D, D, I, D, P, P, P]),
     'rspi_phase_proj_fourier': (I, [P, P, P, P, L, P]),
@@ -130,7 +132,7 @@ KERNELS_PER_CALL = {
     'rspi_screen_loglike7': 1, 'rspi_quad4_part_sums_floats': 0,
     'rspi_mean': 1, 'rspi_ll16_entry_rows': 1, 'rspi_ll16_entry_fill': 1, 'rspi_screen_candidates': 3, 'rspi_rescore': 5,
     'rspi_loglike_stream': 1, 'rspi_posterior_pairs': 3,
-    'rspi_entries16_check': 1, 'rspi_cdft2': 2, 'rspi_phase_support': 5,
+    'rspi_entries16_check': 1, 'rspi_emc_nll': 2, 'rspi_cdft2': 2, 'rspi_phase_support': 5,
     'rspi_phase_proj_fourier': 1, 'rspi_phase_proj_real': 4, 'rspi_sets_counts': 1, 'rspi_sets_steps': 1,
     'rspi_sets_fill': 1, 'rspi_rot_log_slices_sets': 1, 'rspi_sets_part_sums_floats': 0,
     'rspi_screen_loglike_sets': 1, 'rspi_frame_max_finalize': 1,

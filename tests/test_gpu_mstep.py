@@ -168,3 +168,41 @@ def test_recon_cli_writes_log_and_outputs(tmp_path):
     np.testing.assert_array_equal(out['shifts'], np.array([sxv, syv]).T)
     assert os.path.exists(os.path.join(str(tmp_path), 'out', 'model_000.npy'))
     assert rec.rmax.shape == (len(g['ones']),)
+
+
+@pytest.mark.parametrize('kind', ['grid', 'lbfgs', 'grid+lbfgs'])
+def test_emc_adjoint_driven_mstep(tmp_path, kind):
+    """[emc] mstep = grid / lbfgs / grid+lbfgs: the E-step (replayed from its
+    CUDA graph after the first iteration) gives the reference's argmax, the
+    M-step keeps the ring pass of the pattern search and then lowers the
+    pixel NLL of the main pixels below the pattern search's; iterations run
+    through EMC.run_iteration."""
+    from emc import EMC
+    from rspi.adjoint import NLLProblem
+    g = load_golden('case_b')
+    cfg = write_case(str(tmp_path), g=g, extra='mstep = %s\nlbfgs_steps = 20\n' % kind)
+    rec = EMC(cfg)
+    assert rec.mstep_kind == kind
+    rec.model = g['model_in_1'].copy()
+    rec.run_iteration(1)
+    assert np.array_equal(rec.rmax, g['rmax_1'])
+    ms = rec.phaser.mstep
+    rho = float(ms.rescale[0])
+    # the pattern search's model from the same start, for comparison
+    ref = EMC(write_case(str(tmp_path / 'p'), g=g))
+    ref.model = g['model_in_1'].copy()
+    ref.run_iteration(1)
+    num_rot = int(g['num_rot'])
+    vals = rec.state_vals[ms.fstate.long()]
+    ang = (ms.frot.double() * np.pi / num_rot).cpu().numpy()
+    prob = NLLProblem(rec.dset.photons, rec.size, ang, precision='fp64')
+    scale = rec.dset.photons.scales * rho
+
+    def nll(m):
+        fre, fim = prob.model_pixels(m)
+        return float(prob.evaluate(fre, fim, vals[:, 2], vals[:, 0], vals[:, 1], scale))
+    assert nll(rec.model) < nll(ref.model)
+    # a second iteration replays the E-step graph and runs the M-step eagerly
+    rec.run_iteration(2)
+    assert rec._graph is not None
+    assert np.all(np.isfinite(rec.model))

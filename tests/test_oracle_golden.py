@@ -120,3 +120,29 @@ def test_phase_oracle_matches_reference(name):
     np.testing.assert_array_equal(out, g['phase_out'])
     if name == 'phase_a':
         assert 0.5 < supp.mean() < 0.99   # a proper support, not the whole image
+
+
+@pytest.mark.parametrize('name', GOLDEN_CASES)
+def test_emc_nll_oracle_matches_reference_likelihood(name):
+    """The differentiable E-step NLL restatement at grid values equals minus
+    the reference's likelihood of each frame in its argmax state, plus the
+    Poisson term K_d log s_d (oracle/adjoint_oracle.emc_nll_torch)."""
+    import torch
+    from oracle import adjoint_oracle as A
+    g = load_golden(name)
+    ds = golden_dataset(g)
+    size, num_rot = int(g['size']), int(g['num_rot'])
+    sx, sy, dia, _ = golden_states(g)
+    _, pm = E.generate_masks(size)
+    scales = E.get_scales(ds, bool(g['need_scaling']))
+    model = g['model_in_1']
+    rmax = g['rmax_1']
+    s0, j = rmax // num_rot, rmax % num_rot
+    _, vscale = E.msum_vscale(model, sx, sy, dia, size, ds['bg'], pm, E.get_powder(ds))
+    t = lambda a: torch.tensor(np.asarray(a, dtype='f8'))  # noqa: E731
+    val = float(A.emc_nll_torch(t(model.real), t(model.imag), t(dia[s0]), t(sx[s0]), t(sy[s0]),
+                                t(scales), vscale, E.sparse_frames(ds), j * np.pi / num_rot,
+                                size, ds['bg'], pm < 1))
+    k_tot = np.asarray(E.sparse_frames(ds, pm < 1).sum(1)).ravel()
+    want = -np.sum(g['prob_1'][rmax, np.arange(rmax.size)] + k_tot * np.log(scales))
+    np.testing.assert_allclose(val, want, rtol=1e-12)

@@ -14,6 +14,8 @@ lists, config values, start model) and the reference outputs:
   the model after the MaxLP M-step;
 * MaxLPhaser pieces for a few pixels: photons, reference amplitudes,
   per-candidate rescale and log-likelihood;
+* the posterior-weighted merge of the iteration-1 likelihoods through the
+  reference's own merge_all and slice_merge kernels;
 * the model refinement of MaxLPhaser._improve_model (support mask, one
   difference-map and one error-reduction step, the refined model) on the
   iteration-2 model, and in ``phase_a.npz`` on a compact 61x61 object.
@@ -79,6 +81,43 @@ def _write_inputs(tmp, name, c):
                  c['shiftx'], c['shifty']))
     os.makedirs(os.path.join(tmp, 'out'), exist_ok=True)
     return data, bg, cfg
+
+
+def _merge_outputs(rec, prob, size, num_rot, ds):
+    import cupy as cp   # the stand-in
+    m = prob.max(0)
+    e = np.exp(prob - m)
+    post = e / e.sum(0)
+    post = np.where(post >= ref_p_min(), post, 0.)
+    n_rows, ndata = post.shape
+    n0 = n_rows // num_rot
+    scales = np.asarray(rec.scales, dtype='f8')
+    num = np.zeros((n0, size * size)).view(cp.ndarray)
+    den = np.zeros((n0, size * size)).view(cp.ndarray)
+    mw = np.zeros(size * size).view(cp.ndarray)
+    bsz = int(np.ceil(size / 32.))
+    ones = np.ones(size * size)
+    args = (np.asarray(ds.ones, dtype='i4'), np.asarray(ds.multi, dtype='i4'),
+            np.asarray(ds.ones_accum, dtype='i8'), np.asarray(ds.multi_accum, dtype='i8'),
+            np.asarray(ds.place_ones, dtype='i4'), np.asarray(ds.place_multi, dtype='i4'),
+            np.asarray(ds.count_multi, dtype='i4'))
+    for r in range(n_rows):
+        w = float(post[r] @ scales)
+        if w == 0.:
+            continue
+        s0, j = divmod(r, num_rot)
+        view = np.zeros(size * size).view(cp.ndarray)
+        rec.k_merge_all((int(np.ceil(ndata / 32.)),), (32,),
+                        (np.ascontiguousarray(post[r]), ndata) + args + (view,))
+        rec.k_slice_merge((bsz,) * 2, (32,) * 2, (view, j * np.pi / num_rot, size, num[s0], mw))
+        rec.k_slice_merge((bsz,) * 2, (32,) * 2,
+                          (np.ascontiguousarray(ones * w), j * np.pi / num_rot, size, den[s0], mw))
+    return dict(merge_post=post, merge_num=np.asarray(num), merge_den=np.asarray(den))
+
+
+def ref_p_min():
+    import emc as ref_emc
+    return ref_emc.P_MIN
 
 
 def _phase_outputs(ph, fconv, sink):
@@ -189,6 +228,14 @@ def run_case(name, c):
                 resc = [line for line in sink.getvalue().splitlines()
                         if line.startswith('Estimated rescale:')]
                 out['rescale_%d' % it] = np.array(float(resc[-1].split(':')[1]))
+
+            # posterior-weighted merge with the reference's own merge_all and
+            # slice_merge kernels (kernels.cu:84-152, loaded by emc.py:104,107
+            # but not launched on its run path) on the iteration-1
+            # likelihoods: posteriors normalised per frame, those below P_MIN
+            # dropped, the data-space sums of each row back-rotated into its
+            # (shift, diameter) state, and the weights sum_d P scale_d likewise
+            out.update(_merge_outputs(rec, out['prob_1'], size, c['num_rot'], ds))
 
             # phaser pieces on the state left by iteration 2
             import cupy as cp   # the stand-in

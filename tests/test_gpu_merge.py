@@ -1,6 +1,7 @@
 """Posterior normalisation and merge on the GPU (rows a9, a10) vs the FP64
-oracle (build-defined equations; the reference ships merge_all / slice_merge
-but never launches them, so these are pinned by the oracle only)."""
+oracle and vs the reference's own merge_all / slice_merge kernels
+(kernels.cu:84-152, which emc.py loads but never launches) run on the
+golden posteriors (merge_num / merge_den of tests/golden/case_*.npz)."""
 import numpy as np
 import pytest
 import torch
@@ -42,6 +43,9 @@ def test_merge_matches_oracle(name, form):
     np.testing.assert_allclose(mg.den.cpu().numpy(), den, rtol=RTOL, atol=1e-12)
     np.testing.assert_allclose(intens, want, rtol=1e-9, atol=1e-12)
     assert np.all(intens[den == 0] == 0)
+    # the reference kernels' merge of the same posteriors
+    np.testing.assert_allclose(mg.num.cpu().numpy(), g['merge_num'], rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(mg.den.cpu().numpy(), g['merge_den'], rtol=1e-9, atol=1e-12)
 
 
 @pytest.mark.parametrize('name', GOLDEN_CASES)

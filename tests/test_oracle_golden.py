@@ -146,3 +146,21 @@ def test_emc_nll_oracle_matches_reference_likelihood(name):
     k_tot = np.asarray(E.sparse_frames(ds, pm < 1).sum(1)).ravel()
     want = -np.sum(g['prob_1'][rmax, np.arange(rmax.size)] + k_tot * np.log(scales))
     np.testing.assert_allclose(val, want, rtol=1e-12)
+
+
+@pytest.mark.parametrize('name', GOLDEN_CASES)
+def test_merge_oracle_matches_reference_kernels(name):
+    """oracle/emc_oracle.merge (num, den) against the reference's own
+    merge_all + slice_merge kernels (kernels.cu:84-152) on the same
+    posteriors (tests/golden/make_golden.py), and the oracle's posterior
+    against the goldens' normalisation."""
+    g = load_golden(name)
+    ds = golden_dataset(g)
+    size, num_rot = int(g['size']), int(g['num_rot'])
+    n0 = g['prob_1'].shape[0] // num_rot
+    _, post = E.posterior(g['prob_1'])
+    np.testing.assert_allclose(np.where(post >= E.P_MIN, post, 0.), g['merge_post'],
+                               rtol=1e-12, atol=1e-15)
+    _, num, den = E.merge(g['merge_post'], ds, g['scales'], n0, num_rot, size)
+    np.testing.assert_allclose(num, g['merge_num'], rtol=1e-13, atol=1e-15)
+    np.testing.assert_allclose(den, g['merge_den'], rtol=1e-13, atol=1e-15)

@@ -68,6 +68,11 @@ def parse_args():
                     help='warps per CTA of the likelihood kernel (default: the EStep default, 32)')
     ap.add_argument('--screen-delta', type=float, default=None,
                     help='FP64 rescoring window in nats (EMC default 0: the argmax candidates)')
+    ap.add_argument('--mstep', default=None, choices=['pattern', 'grid', 'lbfgs', 'grid+lbfgs'],
+                    help='M-step: the MaxLP pattern search (default), or the pixel-NLL grid / '
+                         'L-BFGS through the adjoint after its ring pass')
+    ap.add_argument('--no-autotune', action='store_true',
+                    help='keep the likelihood kernel\'s default tiling')
     ap.add_argument('--no-phaser-screen', action='store_true',
                     help='pattern search: every candidate in FP64 (no FP32 screening pass)')
     ap.add_argument('--slice-gb', type=float, default=8.,
@@ -241,7 +246,8 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
     return roof, gather, rows_per_launch
 
 
-def write_inputs(tmp, w, data, form, slice_gb=8., screen_delta=None):
+def write_inputs(tmp, w, data, form, slice_gb=8., screen_delta=None, kernel=None, mstep=None,
+                 autotune=True):
     from rspi.photonfile import write_photons
     os.makedirs(os.path.join(tmp, 'out'), exist_ok=True)
     write_photons(os.path.join(tmp, 'photons.npz'), data)
@@ -255,6 +261,11 @@ def write_inputs(tmp, w, data, form, slice_gb=8., screen_delta=None):
                  form, slice_gb))
         if screen_delta is not None:
             f.write('screen_delta = %r\n' % float(screen_delta))
+        if kernel:
+            f.write('kernel = %s\n' % kernel)
+        if mstep:
+            f.write('mstep = %s\n' % mstep)
+        f.write('autotune = %s\n' % bool(autotune))
     return cfg
 
 
@@ -573,16 +584,16 @@ def run_ours(args):
     data = generate_data(args.config, w, device=dev)
     t_gen = time.time() - t0
     tmp = tempfile.mkdtemp(prefix='rspi_bench_')
-    cfgfile = write_inputs(tmp, w, data, args.form, args.slice_gb, args.screen_delta)
+    cfgfile = write_inputs(tmp, w, data, args.form, args.slice_gb, args.screen_delta,
+                           args.kernel if args.form != 'dense' else None, args.mstep,
+                           not args.no_autotune and not args.warps)
     from emc import EMC
     import contextlib
     import io
     with contextlib.redirect_stdout(io.StringIO()):
         rec = EMC(cfgfile, device=dev)
-    if rec.estep.form != 'dense' and args.kernel and args.kernel != rec.estep.kernel:
-        rec.estep.kernel = args.kernel
     if args.warps:
-        rec.estep.warps = args.warps
+        rec.estep.configure(warps=args.warps)
     if args.no_phaser_screen:
         rec.phaser.mstep.screen = False
     model0 = start_model(args.config, w)
@@ -754,6 +765,10 @@ def run_ours(args):
         'e2e': e2e,
         'plain': plain,
         'parity': parity,
+        'tiling': {'warps_per_cta': es.warps, 'column_parts': es.parts(),
+                   'rows_per_tile': es.tile, 'autotuned': bool(getattr(rec, 'tuning', None)),
+                   'tuned_ms_per_row': (rec.tuning[1] if getattr(rec, 'tuning', None)
+                                        else None)},
         'form': {'likelihood': args.form, 'kernel': es.kernel,
                  'candidates_rescored': n_cand, 'rescore_window_nats': getattr(es, 'delta', None),
                  'pattern_search': phaser_form},

@@ -18,7 +18,9 @@ FP64 rescoring of every state that can be the argmax (and, with
 densely, likelihood as a tensor-core GEMM, ``dense_gemm`` = ``auto`` /
 ``i8`` (exact fixed point) / ``bf16`` (hi + lo split), ``dense_rescore``
 (default true: FP64 rescoring of the candidates as in ``screen``)),
-``screen_delta``
+``kernel`` (the likelihood kernel: ``sets`` or ``quad4`` (four-row
+tiles) or ``stream`` for the screened form, ``stream`` or ``dynamic`` for
+``fp64``; default: the form's default), ``screen_delta``
 (default 0: FP64 rescoring of the states that can be the argmax, which is
 what the hard-argmax iteration uses; 20: also every state within 20 nats of
 it, so that ``logz`` equals the FP64 form's -- the posterior consumers'
@@ -28,7 +30,8 @@ screening of the pattern-search candidates, FP64 for the finalists, same
 chosen candidates as false), ``slice_budget_gb`` (rotated slices are built
 in chunks of at most this size, default 8), ``cuda_graph`` (capture the whole
 device iteration once and replay it, default true), ``autotune`` (pick the
-likelihood kernel's tile shape by timing, default false), ``mstep``
+likelihood kernel's tiling by timing it on the first iteration's slices,
+cached per geometry, default true), ``mstep``
 (``pattern``, the default: the MaxLP pattern search; ``grid``: the polar grid
 search of the pixel NLL; ``lbfgs``: L-BFGS on that NLL through its
 hand-written adjoint, ``lbfgs_steps`` iterations, default 50;
@@ -98,14 +101,12 @@ class EMC():
                            delta=self.screen_delta,
                            slice_budget_bytes=int(self.slice_budget_gb * (1 << 30)),
                            n_modes=self.num_modes, dense_gemm=self.dense_gemm,
-                           dense_rescore=self.dense_rescore)
+                           dense_rescore=self.dense_rescore, kernel=self.kernel)
         self.state_vals = torch.from_numpy(self._state_values).to(self.device)
         self.phaser_rot = torch.from_numpy(geometry.phaser_rotation_table(
             np.arange(self.num_rot) * np.pi / self.num_rot)).to(self.device)
         self.rmax = None
-        if self.autotune:
-            from rspi import autotune
-            autotune.tune(self.estep)
+        self._tuned = not self.autotune or self.form == 'dense'
         npix = self.size ** 2 * self.num_modes
         self._dmodel = torch.empty(npix, dtype=torch.complex128, device=self.device)
         self._host_model = torch.empty(npix, dtype=torch.complex128, pin_memory=True)
@@ -135,7 +136,8 @@ class EMC():
         self.use_graph = config.getboolean('emc', 'cuda_graph', fallback=True)
         self.dense_gemm = config.get('emc', 'dense_gemm', fallback='auto')
         self.dense_rescore = config.getboolean('emc', 'dense_rescore', fallback=True)
-        self.autotune = config.getboolean('emc', 'autotune', fallback=False)
+        self.autotune = config.getboolean('emc', 'autotune', fallback=True)
+        self.kernel = config.get('emc', 'kernel', fallback=None) or None
         self.mstep_kind = config.get('emc', 'mstep', fallback='pattern')
         if self.mstep_kind not in ('pattern', 'grid', 'lbfgs', 'grid+lbfgs'):
             raise ValueError('emc:mstep must be pattern, grid, lbfgs or grid+lbfgs')
@@ -245,6 +247,12 @@ class EMC():
         '''The iteration on the device model buffer ``_dmodel``: eager the
         first time (which sizes every buffer and checks capacities), then
         captured once into a CUDA graph and replayed.'''
+        if not self._tuned:
+            # the likelihood kernel's tiling, timed on this model's slices
+            from rspi import autotune
+            self.estep.slices(self._dmodel)
+            self.tuning = autotune.tune(self.estep)[:2]
+            self._tuned = True
         if not self.use_graph:
             self._device_step()
             return

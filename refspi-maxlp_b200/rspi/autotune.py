@@ -1,29 +1,54 @@
-"""Tile autotuner for the likelihood kernel (states per CTA x warps per CTA).
+"""Autotuner of the likelihood kernel's tiling.
 
-For a given E-step (its form, kernel, slice row length and entry stream) the
-tuner times the E-step's likelihood kernel over a sample of likelihood rows
-for every (states_per_tile, warps_per_cta) that fits in shared memory, with CUDA
-events on the launching stream, and keeps the fastest.  Results are cached
-in a JSON file keyed by device name, form, slice row length, frame count and
-entry rows, so later runs of the same geometry skip the search.
+For an E-step (its form, kernel, geometry and photon entries) the tuner
+times the likelihood kernel on a sample of likelihood rows -- two tiles per
+SM of the largest tile -- for every candidate tiling of that kernel, with
+CUDA events on the launching stream, and keeps the fastest:
+
+* ``sets`` and ``quad4`` (four rows per tile over column parts): warps per
+  CTA and the number of column parts (the fewest that fit shared memory, or
+  one more);
+* ``stream`` / ``dynamic`` (the streaming and warp-per-frame kernels): rows
+  per tile and warps per CTA.
+
+The FP64-rescored argmax, maximum and log-sum-exp do not depend on the
+tiling (every tiling keeps the screened FP32 values within the threshold's
+error bound).  Results are cached in a JSON file keyed by GPU name, form,
+kernel, detector geometry (slice row length, states), frame count and photon
+entries, so later runs of the same geometry skip the search; the cache path
+is ``$RSPI_AUTOTUNE_CACHE`` or ``~/.cache/rspi_autotune.json``.
 """
 import json
 import os
 
 import torch
 
+from .device import QUAD4_MAX_PARTS, quad4_parts
 
 CACHE = os.environ.get('RSPI_AUTOTUNE_CACHE',
                        os.path.join(os.path.expanduser('~'), '.cache', 'rspi_autotune.json'))
 TILES = (1, 2, 3, 4, 6, 8)
 WARPS = (8, 16, 32)
+WARPS_FOUR_ROW = (16, 24, 32)
 
 
-def _key(es):
+def key(es):
     name = torch.cuda.get_device_name(es.device)
     ent = es.ll if es.form == 'fp64' else es.ll16
-    return '%s|%s|%s|%d|%d|%d' % (name, es.form, es.kernel, es.p_row, es.ph.num_data,
-                                  ent['total_rows'])
+    return '%s|%s|%s|%d|%d|%d|%d' % (name, es.form, es.kernel, es.p_row, es.n_rows,
+                                     es.ph.num_data, ent['total_rows'])
+
+
+def candidates(es):
+    """The tilings the tuner tries for ``es``: dicts of EStep.configure
+    arguments."""
+    if es.kernel in ('sets', 'quad4'):
+        p0 = quad4_parts(es.p_row)[0]
+        parts = [p for p in (p0, p0 + 1) if p <= QUAD4_MAX_PARTS]
+        return [dict(warps=w, screen_parts=p) for p in parts for w in WARPS_FOUR_ROW]
+    tmax = es.lib.rspi_loglike_max_tile(es.p_row, es.slice_code)
+    return [dict(tile=t, warps=w) for t in TILES if t <= tmax for w in WARPS
+            if es.form == 'screen' or not (t > 2 and w > 16)]
 
 
 def _load():
@@ -45,51 +70,48 @@ def _save(table):
         pass
 
 
-def tune(es, sample_tiles=2, repeats=2, use_cache=True, verbose=False):
-    """Pick (states_per_tile, warps) for ``es`` and set them on it.
-
-    The sample covers ``sample_tiles`` tiles per SM of the largest tile size,
-    so every candidate runs on the same rows.  Returns (tile, warps, ms
-    per row) and a table of all timings."""
-    key = _key(es)
-    table = _load() if use_cache else {}
-    if key in table:
-        t, w = table[key]['tile'], table[key]['warps']
-        es.tile, es.warps = t, w
-        return (t, w, table[key]['ms_per_row']), None
-    tmax = es.lib.rspi_loglike_max_tile(es.p_row, es.slice_code)
-    if es.form == 'screen' and es.kernel == 'quad4':
-        tiles = (4,)   # the four-row frame-quad kernel: warps per CTA only
-    else:
-        tiles = TILES
-    cands = [(t, w) for t in tiles if t <= tmax for w in WARPS
-             if es.form == 'screen' or not (t > 2 and w > 16)]
+def _time(es, cfg, repeats):
+    """Milliseconds per likelihood row of ``es`` under tiling ``cfg`` on a
+    sample of rows (slices rebuilt in that tiling's layout)."""
+    es.configure(**cfg)
     sms = torch.cuda.get_device_properties(es.device).multi_processor_count
-    rows = min(es.n_rows, es.chunk_rows, sms * sample_tiles * max(t for t, _ in cands))
+    rows = min(es.n_rows, es.chunk_rows, sms * 2 * max(4, es.tile))
     es.rot_slices(0, rows)
     n = es.ph.num_data
     stream = torch.cuda.current_stream()
+    es._loglike_launch(0, rows, es.lsl, n)          # warm-up
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(repeats):
+        es._loglike_launch(0, rows, es.lsl, n)
+    b.record(stream)
+    b.synchronize()
+    return a.elapsed_time(b) / repeats / rows
+
+
+def tune(es, repeats=3, use_cache=True, verbose=False):
+    """Pick the fastest tiling for ``es`` and set it.  Returns (the chosen
+    tiling, ms per row, all timings or None when taken from the cache).
+    A model must have been sliced (``es.slices``) before: the timing reuses
+    the E-step's slices of that model."""
+    k = key(es)
+    table = _load() if use_cache else {}
+    if k in table:
+        cfg = table[k]['config']
+        es.configure(**cfg)
+        return cfg, table[k]['ms_per_row'], None
     results = []
-    for t, w in cands:
-        def run():
-            es.tile, es.warps = t, w
-            es._loglike_launch(0, rows, es.lsl, n)
-        run()
-        a = torch.cuda.Event(enable_timing=True)
-        b = torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(repeats):
-            run()
-        b.record(stream)
-        b.synchronize()
-        ms = a.elapsed_time(b) / repeats / rows
-        results.append((ms, t, w))
+    for cfg in candidates(es):
+        ms = _time(es, cfg, repeats)
+        results.append((ms, cfg))
         if verbose:
-            print('tile %d warps %2d: %.4f us/row' % (t, w, ms * 1e3))
-    ms, t, w = min(results)
-    es.tile, es.warps = t, w
-    table[key] = {'tile': t, 'warps': w, 'ms_per_row': ms,
-                  'all': [[r[1], r[2], r[0]] for r in results]}
+            print('%s: %.5f us/row' % (cfg, ms * 1e3))
+    ms, cfg = min(results, key=lambda r: r[0])
+    es.configure(**cfg)
+    es.ph.err.check('autotune')
+    table[k] = {'config': cfg, 'ms_per_row': ms,
+                'all': [[c, m] for m, c in results]}
     if use_cache:
         _save(table)
-    return (t, w, ms), results
+    return cfg, ms, results

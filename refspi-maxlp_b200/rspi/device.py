@@ -432,6 +432,39 @@ class EStep:
         self.check_capacity = True
         self.ll_events = None
 
+    def parts(self):
+        """Column parts of the four-row kernels' tile (None for the others)."""
+        return None if self.wide is None else int(self.wide['n_parts'])
+
+    def configure(self, warps=None, screen_parts=None, tile=None):
+        """Change the likelihood kernel's tiling -- warps per CTA, the column
+        parts of the four-row kernels, the rows per tile of the streaming
+        kernels -- rebuilding the entries and buffers that depend on it.
+        The FP64-rescored results do not depend on the tiling."""
+        if warps is not None:
+            self.warps = int(warps)
+        if tile is not None and int(tile) != self.tile:
+            if self.kernel in ('quad4', 'sets'):
+                raise ValueError('the four-row kernels take 4 states per tile')
+            tmax = self.lib.rspi_loglike_max_tile(self.p_row, self.slice_code)
+            if not 1 <= int(tile) <= tmax:
+                raise ValueError('states_per_tile %d outside 1..%d' % (int(tile), tmax))
+            self.tile = int(tile)
+        if screen_parts is not None and self.kernel in ('quad4', 'sets') and \
+                int(screen_parts) != self.parts():
+            self.screen_parts = int(screen_parts)
+            if self.kernel == 'quad4':
+                self.wide = self._quad4_entries()
+            else:
+                self.wide = self._sets_entries()
+                self.col_of_frame = self.wide['col_of_frame']
+                self.frame_of_col = self.wide['set_frames']
+                need = ((self.chunk_rows + 3) // 4) * self.wide['n_parts'] * \
+                    self.wide['part_w'] * 4
+                if self.lsl.numel() < need:
+                    self.lsl = torch.empty(need, dtype=torch.float32, device=self.device)
+            self._eps_key = None
+
     def _quad4_parts(self):
         """Column parts of the four-row tile (``quad4_parts``), or
         ``screen_parts`` parts."""

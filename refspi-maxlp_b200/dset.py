@@ -10,6 +10,12 @@ prefix sums, counts and powder are computed by librspi kernels.  A photons
 file may also hold dense uint16 counts ``frames`` (N, num_pix) for the
 dense likelihood form; a file with only ``frames`` gets its sparse lists
 derived from them.
+
+With ``shard=True`` inside an initialised torch.distributed group of several
+ranks, the dataset holds this rank's frames only (a contiguous block of the
+file's frames, or the whole of ``photons_file.format(rank=rank)`` when the
+name contains ``{rank}``); ``num_data`` counts them and ``num_data_global``
+all frames, and the mean count, scales and powder are the whole dataset's.
 """
 import os
 import sys
@@ -19,6 +25,8 @@ import torch
 
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 from rspi.device import DevicePhotons  # noqa: E402
+from rspi.shard import shard_photons  # noqa: E402
+from rspi.shard import world as shard_world  # noqa: E402
 from rspi.photonfile import PhotonsFile, sparse_from_dense  # noqa: E402
 
 
@@ -65,19 +73,32 @@ class Dataset():
         need_scaling (bool, optional): Whether scaling will be used
         device (optional): CUDA device (default: current)
     '''
-    def __init__(self, photons_file, num_pix, need_scaling=False, device=None, num_data=-1):
+    def __init__(self, photons_file, num_pix, need_scaling=False, device=None, num_data=-1,
+                 shard=False):
         self.powder = None
         self.photons_file = photons_file
         self.num_pix = num_pix
+        rank, size = shard_world() if shard else (0, 1)
+        pre_sharded = size > 1 and '{rank}' in photons_file
+        if pre_sharded:
+            # one file per rank (frames already split)
+            photons_file = photons_file.format(rank=rank)
         host = read_photons(photons_file, num_pix)
         if 0 <= num_data < host['num_data']:
             host = _first_frames(host, num_data)
-        self.num_data = host['num_data']
         before = torch.cuda.memory_allocated() if torch.cuda.is_available() else 0
-        self.photons = DevicePhotons(host['ones'], host['multi'], host['place_ones'],
-                                     host['place_multi'], host['count_multi'], num_pix,
-                                     need_scaling, device, frames=host.get('frames'))
+        if size > 1:
+            # this rank's frames, with the dataset-wide mean count and powder
+            self.photons = shard_photons(host, num_pix, need_scaling, device,
+                                         pre_sharded=pre_sharded)
+            self.num_data_global = self.photons.num_data_global
+        else:
+            self.photons = DevicePhotons(host['ones'], host['multi'], host['place_ones'],
+                                         host['place_multi'], host['count_multi'], num_pix,
+                                         need_scaling, device, frames=host.get('frames'))
+            self.num_data_global = self.photons.num_data
         ph = self.photons
+        self.num_data = ph.num_data
         self.device = ph.device
         self.ones, self.multi = ph.ones, ph.multi
         self.ones_accum, self.multi_accum = ph.ones_accum, ph.multi_accum

@@ -44,6 +44,15 @@ mode as well as a state, and MaxLP updates each mode from the frames that
 chose it.  ``model`` is then a (num_modes, size**2) array and
 ``output_%03d.h5`` holds ``model`` as (num_modes, size, size) plus each
 frame's mode in ``modes``.
+
+Several GPUs: run one process per GPU inside an initialised
+torch.distributed group (NCCL).  The reference splits states over MPI ranks
+(emc.py:143,171,207-216); here each rank takes a contiguous block of the
+frames (or its own file when ``in_photons_file`` contains ``{rank}``),
+computes every state for them with no exchange, and the M-step sums the
+pixel histograms over ranks and splits the pattern search by pixels
+(rspi/shard.py): model and argmax are those of one GPU, bit for bit.  Rank
+0 writes the output files; ``prob`` holds the rank's own frames.
 """
 import configparser
 import os.path as op
@@ -58,6 +67,7 @@ from dset import Dataset  # noqa: E402
 from maxLP import MaxLPhaser  # noqa: E402
 from rspi import geometry  # noqa: E402
 from rspi import h5lite  # noqa: E402
+from rspi import shard  # noqa: E402
 from rspi.device import cur_stream, ptr  # noqa: E402
 from rspi.lib import call  # noqa: E402
 from rspi.device import EStep  # noqa: E402
@@ -76,8 +86,9 @@ class EMC():
     '''
     def __init__(self, config_file, num_streams=4, device=None):
         self.num_streams = num_streams
-        self.rank = 0
-        self.num_proc = 1
+        # several ranks of an initialised torch.distributed group split the
+        # frames (rspi/shard.py); one rank is the reference's one-process run
+        self.rank, self.num_proc = shard.world()
         self.device = torch.device('cuda', torch.cuda.current_device()) if device is None \
             else torch.device(device)
         self.mem_size = torch.cuda.get_device_properties(self.device).total_memory
@@ -92,6 +103,10 @@ class EMC():
         self.phaser = MaxLPhaser(self.photons_file, size=self.size, dataset=self.dset,
                                  num_iter=self.phaser_iter, num_modes=self.num_modes,
                                  screen=self.phaser_screen)
+        if self.num_proc > 1:
+            if self.mstep_kind != 'pattern':
+                raise ValueError('emc:mstep %s runs on one GPU' % self.mstep_kind)
+            self.phaser.mstep.shard = shard.ShardedMStep(self.phaser.mstep)
         self._init_model()
 
         self.estep = EStep(self.dset.photons, self.size, self.num_rot, self.shiftx,
@@ -165,7 +180,7 @@ class EMC():
         '''emc.py:109-118'''
         stime = time.time()
         self.dset = Dataset(self.photons_file, self.size ** 2, self.need_scaling,
-                            device=self.device)
+                            device=self.device, shard=self.num_proc > 1)
         self.powder = self.dset.get_powder()
         etime = time.time()
         print('%d frames with %.3f photons/frame (%.3f s) (%.2f MB)' %
@@ -201,9 +216,16 @@ class EMC():
             self._host_rmax.copy_(self.estep.rmax)
             self._host_model.copy_(self._dmodel)
         err.check('EMC iteration')
-        self.rmax = self._host_rmax.numpy().copy()
+        if self.num_proc > 1:
+            # every rank's argmax, in frame order (the model is the same on
+            # every rank)
+            self.rmax = shard.gather_frames(self.estep.rmax, self.dset.num_data_global).cpu() \
+                .numpy().astype('i4')
+        else:
+            self.rmax = self._host_rmax.numpy().copy()
         self.model = self._host_model.numpy().copy().reshape(self._model_shape())
-        self.save_output(self.model, iternum)
+        if self.rank == 0:
+            self.save_output(self.model, iternum)
 
     def _device_step(self):
         '''One iteration on device buffers: E-step, reduction, M-step.'''
@@ -256,9 +278,11 @@ class EMC():
         if not self.use_graph:
             self._device_step()
             return
-        # the graph holds the whole iteration, or with an adjoint-driven
-        # M-step (host-side L-BFGS line searches) the E-step only
-        part = self._device_step if self.mstep_kind == 'pattern' else self._estep_part
+        # the graph holds the whole iteration, or the E-step only with an
+        # adjoint-driven M-step (host-side L-BFGS line searches) or with
+        # frames split over ranks (collectives in the M-step)
+        part = self._device_step if self.mstep_kind == 'pattern' and self.num_proc == 1 \
+            else self._estep_part
         if self._graph is not None:
             self._graph.replay()
             if part is not self._device_step:
@@ -338,9 +362,14 @@ class EMC():
         h5lite.write_datasets(op.join(self.output_folder, 'output_%.3d.h5' % iternum), out)
 
     def _random_model(self):
-        '''emc.py:241-242 (one such model per mode)'''
+        '''emc.py:241-242 (one such model per mode; with several ranks rank
+        0's, so that every rank starts from the same model)'''
         shape = self._model_shape()
         self.model = np.random.random(shape) + 1j * np.random.random(shape)
+        if self.num_proc > 1:
+            m = torch.from_numpy(np.ascontiguousarray(self.model).ravel()).to(self.device)
+            torch.distributed.broadcast(torch.view_as_real(m), 0)
+            self.model = m.cpu().numpy().reshape(shape)
 
     def ramp(self, n):
         '''Shift phase ramp of state n (emc.py:244-245), a complex128 CUDA

@@ -886,6 +886,7 @@ class MStep:
         self.hist = None
         self.nstate = None
         self.stats = torch.zeros(3, dtype=torch.int64, device=dev)
+        self.shard = None   # rspi.shard.ShardedMStep when frames are split over ranks
 
     def _pattern(self, fconv, pixels, rows, n_pix, hist, n_ref, mode, rescale, rescale_out, s):
         if self.screen:
@@ -923,6 +924,9 @@ class MStep:
             ptr(ph.place_ones), ptr(ph.place_multi), ptr(ph.count_multi), ph.num_data,
             ptr(self.fstate), ptr(self.frot), ptr(rot_cs), self.size, ptr(self.mask_idx),
             self.n_hist_rows, n_cols, ptr(hist), ptr(ph.err.t), cur_stream())
+        if self.shard is not None:
+            # sums over every rank's frames: the histogram of the whole dataset
+            self.shard.reduce_histogram(hist, self.nstate)
         return hist
 
     def grid(self, fconv, ref_params, rot_cs, scales, n_phase=64, n_amp=32):
@@ -931,6 +935,9 @@ class MStep:
         values of the chosen points (without the F-independent term)."""
         if self.n_modes != 1:
             raise ValueError('the grid search takes one mode')
+        if self.shard is not None:
+            raise ValueError('the grid search runs on one GPU (its per-state scale sums are '
+                             'frame-local)')
         n_ref = int(ref_params.shape[0])
         hist = self.histogram(n_ref, rot_cs)
         ssum = torch.empty(n_ref, dtype=_f64, device=self.device)
@@ -962,7 +969,13 @@ class MStep:
                      ptr(self.rescale[m:]), s)
         else:
             self.rescale.fill_(float('nan'))   # np.mean of an empty ring
-        if main:
+        if main and self.shard is None:
             self._pattern(fconv, self.main, self.main_rows, self.n_main, hist, n_ref, 1,
                           ptr(self.rescale), None, s)
+        elif main:
+            # this rank's block of the main pixels, then every rank's updates
+            lo, hi = self.shard.main_block()
+            self._pattern(fconv, self.main[lo:], self.main_rows[lo:], hi - lo, hist, n_ref, 1,
+                          ptr(self.rescale), None, s)
+            self.shard.gather_main(fconv, self.main[lo:hi])
         return fconv

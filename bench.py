@@ -26,8 +26,12 @@ with torch in place of CuPy), also on a bounded sample.
 L-BFGS against the polar grid search on NLL and FRC); ``--config 4`` and
 ``--config 5`` run the multi-mode and the dense high-fluence workloads.
 
-Multi-GPU: the path runs as independent replicas (one full workload per
-rank, no collective on the data path); value = sum over ranks, time = max.
+Multi-GPU (torchrun, one process per GPU, NCCL): one job whose frames are
+split over the ranks -- each rank draws its own ``--frames`` frames of the
+same object (weak scaling), the E-step needs no exchange, the M-step sums
+the pixel histograms over ranks and splits the pattern search by pixels
+(rspi/shard.py); value = all ranks' frames x states / the slowest rank's
+time.
 """
 import argparse
 import json
@@ -135,13 +139,15 @@ def workload_name(cfg_id, w):
              w['n_states']))
 
 
-def generate_data(cfg_id, w, device='cpu'):
-    """The configuration's seeded synthetic photons (``w['n']`` frames)."""
+def generate_data(cfg_id, w, device='cpu', rank=0):
+    """The configuration's seeded synthetic photons (``w['n']`` frames;
+    rank r > 0 of a multi-GPU job draws its own frames of the same object)."""
     from rspi import synth
     c = w['cfg']
     return synth.generate(c['size'], w['n'], c['mean_count'], c['n_blobs'], c['obj_radius'],
                           c['fluence_sigma'], c['dia'], c['shift_max'], seed=20260000 + cfg_id,
-                          device=device, **synth.config_extras(cfg_id))
+                          device=device, frame_seed=None if rank == 0 else 7919 * rank,
+                          **synth.config_extras(cfg_id))
 
 
 def start_model(cfg_id, w):
@@ -247,14 +253,17 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
 
 
 def write_inputs(tmp, w, data, form, slice_gb=8., screen_delta=None, kernel=None, mstep=None,
-                 autotune=True):
+                 autotune=True, rank=None):
     from rspi.photonfile import write_photons
     os.makedirs(os.path.join(tmp, 'out'), exist_ok=True)
-    write_photons(os.path.join(tmp, 'photons.npz'), data)
+    name = 'photons.npz' if rank is None else 'photons_%d.npz' % rank
+    write_photons(os.path.join(tmp, name), data)
     cfg = os.path.join(tmp, 'config.ini')
     r = w['recon']
     with open(cfg, 'w') as f:
-        f.write('[emc]\nsize = %d\nin_photons_file = photons.npz\noutput_folder = out/\n'
+        f.write('[emc]\nsize = %d\nin_photons_file = ' +
+                ('photons.npz' if rank is None else 'photons_{rank}.npz') +
+                '\noutput_folder = out/\n'
                 'log_file = out/EMC.log\nneed_scaling = True\nnum_rot = %d\nnum_modes = %d\n'
                 'sphere_dia = %s\nshiftx = %s\nshifty = %s\nform = %s\nslice_budget_gb = %g\n' %
                 (w['size'], r['num_rot'], w['n_modes'], r['sphere_dia'], r['shiftx'], r['shifty'],
@@ -581,12 +590,15 @@ def run_ours(args):
     dev = torch.device('cuda', local)
     w = workload(args.config, args.frames)
     t0 = time.time()
-    data = generate_data(args.config, w, device=dev)
+    data = generate_data(args.config, w, device=dev, rank=rank)
     t_gen = time.time() - t0
     tmp = tempfile.mkdtemp(prefix='rspi_bench_')
+    # several ranks: each its own frames (photons_{rank}.npz), one job split
+    # by frames (rspi/shard.py)
     cfgfile = write_inputs(tmp, w, data, args.form, args.slice_gb, args.screen_delta,
                            args.kernel if args.form != 'dense' else None, args.mstep,
-                           not args.no_autotune and not args.warps)
+                           not args.no_autotune and not args.warps,
+                           rank=rank if world > 1 else None)
     from emc import EMC
     import contextlib
     import io
@@ -674,7 +686,7 @@ def run_ours(args):
     # form from the start model, compared entry by entry (the parity block),
     # then the plain form timed eagerly step by step
     plain, parity = None, None
-    if rank == 0 and not args.no_plain:
+    if world == 1 and not args.no_plain:
         from rspi.device import EStep
         rec._graph = None
         pe = None
@@ -754,7 +766,10 @@ def run_ours(args):
         'data': 'synthetic (seeded generator with the configuration\'s shapes)',
         'config': {'workload': workload_name(args.config, w),
                    'frames': w['n'], 'states_per_frame': w['n_states'],
-                   'form': args.form, 'parallelism': 'replicas' if world > 1 else 'single',
+                   'form': args.form,
+                   'parallelism': ('frame shards: %d ranks x %d frames, histogram all-reduce '
+                                   'and pixel-split pattern search' % (world, w['n'])
+                                   if world > 1 else 'single'),
                    'l2': 'inputs larger than L2 (slices %.1f GB, likelihoods %.1f GB per step)' %
                    (es.n_rows * es.p_row * esz / 1e9, es.n_rows * w['n'] * osz / 1e9)},
         'gpu_launches': launches,

@@ -143,7 +143,8 @@ def _rotate_bilinear(img, angle, size):
 def generate(size, num_data, mean_count, n_blobs=20, obj_radius=12.,
              fluence_sigma=0.3, dia=(6., 8.), shift_max=3., seed=0,
              device='cpu', chunk=256, dense=False, n_modes=1, mode_weights=None,
-             displace=(2., 4.), displace_frac=0.15, count_lognormal=None, bg_level=0.):
+             displace=(2., 4.), displace_frac=0.15, count_lognormal=None, bg_level=0.,
+             frame_seed=None):
     """Generate one dataset; returns a dict in the photons-file layout.
 
     Keys: ``num_pix``, ``ones``, ``multi`` (int32, N), ``place_ones``,
@@ -152,10 +153,15 @@ def generate(size, num_data, mean_count, n_blobs=20, obj_radius=12.,
     ``true_diameters``, ``scale``, ``solution``, and ``fsample``/``rel_scale``.
     With ``n_modes`` > 1, ``solution``/``fsample`` hold one row per
     conformation and ``true_modes`` each frame's.  With ``dense=True`` a
-    dense uint16 ``frames`` (N, size^2) is added.
+    dense uint16 ``frames`` (N, size^2) is added.  ``frame_seed`` draws
+    other frames (parameters and photons) of the same object.
     """
     ss = np.random.SeedSequence(seed)
     r_obj, r_par, r_poi = [np.random.default_rng(s) for s in ss.spawn(3)]
+    if frame_seed is not None:
+        # the same object, other frames (parameters and photon draws)
+        r_par, r_poi = [np.random.default_rng(s)
+                        for s in np.random.SeedSequence([seed, frame_seed]).spawn(2)]
     blobs = [make_blobs(size, n_blobs, obj_radius, r_obj)]
     for _ in range(1, n_modes):
         blobs.append(displaced_blobs(blobs[0], displace_frac, displace, r_obj))

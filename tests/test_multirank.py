@@ -1,7 +1,7 @@
 """The multi-rank host logic of bench.py on CPU (gloo, world size 2): the
 job time is the maximum over ranks, and under torchrun the reference arm
-runs on rank 0 only.  The path itself runs as independent replicas (no
-collective on the data path), so these are its only collectives."""
+runs on rank 0 only.  The collectives of the frame-sharded iteration itself
+are tested in test_shard.py (CPU) and test_gpu_shard.py."""
 import os
 import socket
 import subprocess

@@ -353,14 +353,19 @@ int rspi_screen_candidates_noalloc(const float *ll, long long n_rows, long long 
 
 /* rspi_screen_candidates over a likelihood matrix whose n_cols columns hold
  * frames in another order: column c holds frame frame_of_col[c] (-1: none);
- * the outputs are per frame as in rspi_screen_candidates. */
+ * the outputs are per frame as in rspi_screen_candidates.  With cand_slot
+ * (n_data * 32 ints of scratch) the matrix is read once: the counting pass
+ * records each thread's candidate row when it has one, a compaction writes
+ * those frames' lists, and only frames where one thread (rows r = t mod 32)
+ * met two or more candidates are scanned again -- the same lists in the
+ * same order as without it. */
 int rspi_screen_candidates_cols(const float *ll, long long n_rows, long long n_cols,
                                 const int *frame_of_col, long long n_data, const double *max32,
                                 const int *rmax32, const long long *frame_photons,
                                 const long long *row_off16, const float *lmax, double delta,
                                 int *cnt_part, int *cand_n, double *noncand, double *thr,
                                 long long *cand_off, long long capacity, int *cand_d,
-                                int *cand_r, int *err, cudaStream_t stream);
+                                int *cand_r, int *cand_slot, int *err, cudaStream_t stream);
 
 /* FP64 rescoring of every candidate, in the summation order of rspi_loglike
  * (so the values equal the FP64 form's), written to cand_ll and into ll32;

@@ -159,7 +159,8 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_x, long
              const long long *__restrict__ phot,
              const long long *__restrict__ row_off16, const float *__restrict__ lmax, double delta,
              int *__restrict__ cnt_part /* n_data x RY */, int *__restrict__ cand_n,
-             double *__restrict__ noncand, double *__restrict__ thr_out) {
+             double *__restrict__ noncand, double *__restrict__ thr_out,
+             int *__restrict__ cand_slot /* n_data x RY, or null */) {
     __shared__ int sc[RY][33];
     __shared__ double sn[RY][33];
     const int tx = threadIdx.x, ty = threadIdx.y;
@@ -167,7 +168,7 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_x, long
     // unless the columns are a permutation of the frames)
     const long long x = (long long)blockIdx.x * 32 + tx;
     const long long d = x >= n_x ? -1 : (frame_of_col ? (long long)frame_of_col[x] : x);
-    int c = 0;
+    int c = 0, first = -1;
     double nc = 0.;
     if (d >= 0) {
         const double m = max32[d];
@@ -183,16 +184,24 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_x, long
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
                 const double v = (double)v8[u];
-                if (v >= thr || r + u * RY == rm) ++c;
-                else nc += (double)expf((float)(v - m));   // each term < exp(-delta)
+                if (v >= thr || r + u * RY == rm) {
+                    if (c++ == 0) first = (int)(r + u * RY);
+                } else {
+                    nc += (double)expf((float)(v - m));   // each term < exp(-delta)
+                }
             }
         }
         for (; r < n_rows; r += RY) {
             const double v = (double)ll[r * stride + x];
-            if (v >= thr || r == rm) ++c;
-            else nc += (double)expf((float)(v - m));   // each term < exp(-delta)
+            if (v >= thr || r == rm) {
+                if (c++ == 0) first = (int)r;
+            } else {
+                nc += (double)expf((float)(v - m));   // each term < exp(-delta)
+            }
         }
         cnt_part[d * RY + ty] = c;
+        // the thread's candidate row when it has exactly one (-2: more)
+        if (cand_slot) cand_slot[d * RY + ty] = c > 1 ? -2 : first;
         if (ty == 0) thr_out[d] = thr;
     }
     sc[ty][tx] = c;
@@ -212,7 +221,7 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_x, long
 
 __global__ void __launch_bounds__(32 * RY)
 k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_x, long long stride,
-            const int *__restrict__ frame_of_col,
+            const int *__restrict__ frame_of_col, const int *__restrict__ cand_slot,
             const double *__restrict__ thr, const int *__restrict__ rmax32,
             const int *__restrict__ cnt_part,
             const long long *__restrict__ cand_off, long long capacity,
@@ -220,6 +229,16 @@ k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_x, long 
     const int tx = threadIdx.x, ty = threadIdx.y;
     const long long x = (long long)blockIdx.x * 32 + tx;
     const long long d = x >= n_x ? -1 : (frame_of_col ? (long long)frame_of_col[x] : x);
+    if (cand_slot) {
+        // only frames in which some thread had two or more candidates are
+        // filled here (k_cand_compact took the others)
+        __shared__ int over[32];
+        if (ty == 0) over[tx] = 0;
+        __syncthreads();
+        if (d >= 0 && cand_slot[d * RY + ty] == -2) over[tx] = 1;
+        __syncthreads();
+        if (!over[tx]) return;
+    }
     if (d < 0) return;
     long long pos = cand_off[d];
     for (int k = 0; k < ty; ++k) pos += cnt_part[d * RY + k];
@@ -246,6 +265,38 @@ k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_x, long 
         for (int u = 0; u < 8; ++u) take(v8[u], r + u * RY);
     }
     for (; r < n_rows; r += RY) take(ll[r * stride + x], r);
+}
+
+// One warp per frame whose threads of k_cand_count each found at most one
+// candidate: the recorded rows written in the order k_cand_fill writes them
+// (thread ty's rows, ty ascending), so both paths give the same list.
+__global__ void k_cand_compact(const int *__restrict__ cand_slot, const int *__restrict__ cnt_part,
+                               const long long *__restrict__ cand_off, long long n_data,
+                               long long capacity, int *__restrict__ cand_d,
+                               int *__restrict__ cand_r, int *err) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long d = warp; d < n_data; d += nwarp) {
+        const int slot = cand_slot[d * RY + lane];
+        if (__any_sync(RSPI_FULL_MASK, slot == -2)) continue;   // k_cand_fill's frame
+        const int c = cnt_part[d * RY + lane];
+        int pre = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(RSPI_FULL_MASK, pre, o);
+            if (lane >= o) pre += v;
+        }
+        if (c == 1) {
+            const long long pos = cand_off[d] + pre - 1;
+            if (pos < capacity) {
+                cand_d[pos] = (int)d;
+                cand_r[pos] = slot;
+            } else {
+                rspi_flag(err, RSPI_ERR_CAPACITY);
+            }
+        }
+    }
 }
 
 // Candidates regrouped by likelihood row: count, scan (rows + 1 offsets),
@@ -481,7 +532,7 @@ int candidates_launch(const float *ll, long long n_rows, long long n_x, long lon
                       const long long *row_off16, const float *lmax, double delta,
                       int *cnt_part, int *cand_n, double *noncand, double *thr,
                       long long *cand_off, long long capacity, int *cand_d, int *cand_r,
-                      int *err, cudaStream_t stream) {
+                      int *err, cudaStream_t stream, int *cand_slot = nullptr) {
     if (!ll || !max32 || !rmax32 || !frame_photons || !row_off16 || !lmax || !cnt_part ||
         !cand_n || !noncand || !thr || !cand_off || !cand_d || !cand_r || n_rows <= 0 ||
         n_data <= 0 || n_x <= 0 || stride < n_x || n_rows > 0x7fffffffLL || capacity < 0 ||
@@ -491,10 +542,14 @@ int candidates_launch(const float *ll, long long n_rows, long long n_x, long lon
     const unsigned grid = (unsigned)((n_x + 31) / 32);
     k_cand_count<<<grid, block, 0, stream>>>(ll, n_rows, n_x, stride, frame_of_col, max32,
                                              rmax32, frame_photons, row_off16, lmax, delta,
-                                             cnt_part, cand_n, noncand, thr);
+                                             cnt_part, cand_n, noncand, thr, cand_slot);
     k_scan_counts<<<1, 1024, 0, stream>>>(cand_n, n_data, cand_off);
-    k_cand_fill<<<grid, block, 0, stream>>>(ll, n_rows, n_x, stride, frame_of_col, thr, rmax32,
-                                            cnt_part, cand_off, capacity, cand_d, cand_r, err);
+    if (cand_slot)
+        k_cand_compact<<<rspi_blocks(n_data * 32, 256), 256, 0, stream>>>(
+            cand_slot, cnt_part, cand_off, n_data, capacity, cand_d, cand_r, err);
+    k_cand_fill<<<grid, block, 0, stream>>>(ll, n_rows, n_x, stride, frame_of_col, cand_slot,
+                                            thr, rmax32, cnt_part, cand_off, capacity, cand_d,
+                                            cand_r, err);
     RSPI_RETURN_LAUNCH();
 }
 
@@ -520,11 +575,11 @@ extern "C" int rspi_screen_candidates_cols(const float *ll, long long n_rows, lo
                                            double delta, int *cnt_part, int *cand_n,
                                            double *noncand, double *thr, long long *cand_off,
                                            long long capacity, int *cand_d, int *cand_r,
-                                           int *err, cudaStream_t stream) {
+                                           int *cand_slot, int *err, cudaStream_t stream) {
     if (!frame_of_col) return RSPI_ERR_ARG;
     return candidates_launch(ll, n_rows, n_cols, n_cols, frame_of_col, n_data, max32, rmax32,
                              frame_photons, row_off16, lmax, delta, cnt_part, cand_n, noncand,
-                             thr, cand_off, capacity, cand_d, cand_r, err, stream);
+                             thr, cand_off, capacity, cand_d, cand_r, err, stream, cand_slot);
 }
 
 static int rescore_launch(const int *cand_d, const int *cand_r, const long long *cand_off,
@@ -687,9 +742,10 @@ extern "C" int rspi_screen_candidates_noalloc(const float *ll, long long n_rows,
     const unsigned grid = (unsigned)((n_data + 31) / 32);
     k_cand_count<<<grid, block, 0, stream>>>(ll, n_rows, n_data, n_data, nullptr, max32, rmax32,
                                              frame_photons, row_off16, lmax, delta, scratch,
-                                             cand_n, noncand, thr);
+                                             cand_n, noncand, thr, nullptr);
     k_scan_counts<<<1, 1024, 0, stream>>>(cand_n, n_data, cand_off);
-    k_cand_fill<<<grid, block, 0, stream>>>(ll, n_rows, n_data, n_data, nullptr, thr, rmax32,
-                                            scratch, cand_off, capacity, cand_d, cand_r, err);
+    k_cand_fill<<<grid, block, 0, stream>>>(ll, n_rows, n_data, n_data, nullptr, nullptr, thr,
+                                            rmax32, scratch, cand_off, capacity, cand_d, cand_r,
+                                            err);
     RSPI_RETURN_LAUNCH();
 }

@@ -314,6 +314,7 @@ class EStep:
             self.frame_of_col = self.wide['set_frames']
             self.n_cols = self.wide['n_sets'] * 32
             self.frame_max = torch.zeros(self.n_cols, dtype=_i64, device=dev)
+            self.cand_slot = torch.empty(n * 32, dtype=_i32, device=dev)
         self._eps_key, self.row_off_eps = None, None
         esz = {0: 4, 1: 8, 2: 2}[self.slice_code]
         # slice bytes per likelihood row (the frame-set layout holds the
@@ -756,7 +757,8 @@ class EStep:
                     self.capacity, ptr(self.cand_d), ptr(self.cand_r), ptr(self.ph.err.t), s)
             if cols:
                 call('rspi_screen_candidates_cols', ptr(self.prob), self.n_rows, self.n_cols,
-                     ptr(self.frame_of_col), n, ptr(self.max32), *tail)
+                     ptr(self.frame_of_col), n, ptr(self.max32), *tail[:-2],
+                     ptr(self.cand_slot), *tail[-2:])
             else:
                 call('rspi_screen_candidates', ptr(self.prob), self.n_rows, n, ptr(self.max32),
                      *tail)

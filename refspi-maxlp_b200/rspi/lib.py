@@ -70,7 +70,7 @@ SIGNATURES = {
                                      P, P]),
     'rspi_frame_max_finalize': (I, [P, P, L, P, P, P]),
     'rspi_screen_candidates_cols': (I, [P, L, L, P, L, P, P, P, P, P, D, P, P, P, P, P, L, P, P,
-                                        P, P]),
+                                        P, P, P]),
     'rspi_rescore_cols': (I, [P, P, P, L, L, L, P, L, P, L, P, P, L, L, P, P, P, P, P, P, P, P,
                               P, L, P, P, P, P, P, P, P, L, P]),
     'rspi_loglike_stream': (I, [I, P, L, L, P, P, P, P, L, L, L, P, L, I, I, I, P]),
@@ -136,7 +136,7 @@ KERNELS_PER_CALL = {
     'rspi_phase_proj_fourier': 1, 'rspi_phase_proj_real': 4, 'rspi_sets_counts': 1, 'rspi_sets_steps': 1,
     'rspi_sets_fill': 1, 'rspi_rot_log_slices_sets': 1, 'rspi_sets_part_sums_floats': 0,
     'rspi_screen_loglike_sets': 1, 'rspi_frame_max_finalize': 1,
-    'rspi_screen_candidates_cols': 3, 'rspi_rescore_cols': 5, 'rspi_nll': 2, 'rspi_screen_candidates_noalloc': 3, 'rspi_merge_coverage': 1, 'rspi_merge': 2,
+    'rspi_screen_candidates_cols': 4, 'rspi_rescore_cols': 5, 'rspi_nll': 2, 'rspi_screen_candidates_noalloc': 3, 'rspi_merge_coverage': 1, 'rspi_merge': 2,
     'rspi_dense_frames': 1, 'rspi_rot_log_split': 1, 'rspi_dense_loglike': 1,
     'rspi_maxlp_grid': 2, 'rspi_dense_frames_u8': 1, 'rspi_rot_log_fixed': 1,
     'rspi_dense_loglike_i8': 1,

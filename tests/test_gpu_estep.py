@@ -570,3 +570,38 @@ def test_sets_fused_frame_maximum():
     np.testing.assert_array_equal(es.rmax32.cpu().numpy(), np.argmax(m, 0))
     np.testing.assert_array_equal(es.max32.cpu().numpy(), m.max(0).astype(np.float64))
     assert not bool(es.frame_max.any())   # reset for the next pass
+
+
+@pytest.mark.parametrize('delta', [0., 20., 400.])
+def test_one_pass_candidates_equal_two_pass(delta):
+    """The one-pass candidate selection (counting pass records each thread's
+    single candidate, compaction, a second scan only for frames where a
+    thread met several) gives the two-pass lists, in the same order, for
+    windows from the argmax alone to hundreds of candidates per frame."""
+    from rspi.device import cur_stream, ptr
+    from rspi.lib import call
+    g = load_golden('case_b')
+    _, es = _golden_estep(g, form='screen', kernel='sets', delta=delta)
+    es.run(torch.from_numpy(g['model_in_1']).cuda())
+    es.reduce()                      # sizes the candidate buffers
+    n = es.ph.num_data
+    outs = []
+    for slot in (es.cand_slot, None):
+        cand_n = torch.empty(n, dtype=torch.int32, device='cuda')
+        off = torch.empty(n + 1, dtype=torch.int64, device='cuda')
+        cd = torch.full((es.capacity,), -7, dtype=torch.int32, device='cuda')
+        cr = torch.full((es.capacity,), -7, dtype=torch.int32, device='cuda')
+        call('rspi_screen_candidates_cols', ptr(es.prob), es.n_rows, es.n_cols,
+             ptr(es.frame_of_col), n, ptr(es.max32), ptr(es.rmax32),
+             ptr(es.ll['frame_sel_photons']), ptr(es._eps_rows()), ptr(es.lmax), es.delta,
+             ptr(es.cnt_part), ptr(cand_n), ptr(es.noncand), ptr(es.thr), ptr(off),
+             es.capacity, ptr(cd), ptr(cr), ptr(slot), ptr(es.ph.err.t), cur_stream())
+        torch.cuda.synchronize()
+        es.ph.err.check('candidates')
+        total = int(off[n])
+        outs.append((off.cpu().numpy(), cd[:total].cpu().numpy(), cr[:total].cpu().numpy()))
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+    if delta >= 20.:
+        # some frames took the second scan
+        assert (np.diff(outs[0][0]) > 32).any() or delta == 20.

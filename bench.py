@@ -75,6 +75,8 @@ def parse_args():
     ap.add_argument('--mstep', default=None, choices=['pattern', 'grid', 'lbfgs', 'grid+lbfgs'],
                     help='M-step: the MaxLP pattern search (default), or the pixel-NLL grid / '
                          'L-BFGS through the adjoint after its ring pass')
+    ap.add_argument('--slice-math', default=None, choices=['fp64', 'fp32'],
+                    help='arithmetic of the frame-set kernel\'s log-slices')
     ap.add_argument('--no-autotune', action='store_true',
                     help='keep the likelihood kernel\'s default tiling')
     ap.add_argument('--no-phaser-screen', action='store_true',
@@ -253,7 +255,7 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
 
 
 def write_inputs(tmp, w, data, form, slice_gb=8., screen_delta=None, kernel=None, mstep=None,
-                 autotune=True, rank=None):
+                 autotune=True, rank=None, slice_math=None):
     from rspi.photonfile import write_photons
     os.makedirs(os.path.join(tmp, 'out'), exist_ok=True)
     name = 'photons.npz' if rank is None else 'photons_%d.npz' % rank
@@ -274,6 +276,8 @@ def write_inputs(tmp, w, data, form, slice_gb=8., screen_delta=None, kernel=None
             f.write('kernel = %s\n' % kernel)
         if mstep:
             f.write('mstep = %s\n' % mstep)
+        if slice_math:
+            f.write('slice_math = %s\n' % slice_math)
         f.write('autotune = %s\n' % bool(autotune))
     return cfg
 
@@ -598,7 +602,7 @@ def run_ours(args):
     cfgfile = write_inputs(tmp, w, data, args.form, args.slice_gb, args.screen_delta,
                            args.kernel if args.form != 'dense' else None, args.mstep,
                            not args.no_autotune and not args.warps,
-                           rank=rank if world > 1 else None)
+                           rank=rank if world > 1 else None, slice_math=args.slice_math)
     from emc import EMC
     import contextlib
     import io

@@ -269,18 +269,25 @@ int rspi_sets_fill(const unsigned short *entries16, const long long *row_off16, 
                    long long n_sets, const long long *group_off, unsigned short *entries,
                    int *err, cudaStream_t stream);
 
-/* Rotated log-slices (as rspi_rot_log_slices, FP32, identical values) in the
- * layout of rspi_screen_loglike_sets: rows taken four at a time from
- * row_begin, columns cut into parts:
+/* Rotated log-slices in the layout of rspi_screen_loglike_sets: rows taken
+ * four at a time from row_begin, columns cut into parts:
  * out[(((r - row_begin) / 4 * n_parts + h) * part_w + c) * 4 + (r - row_begin) % 4]
  * is row r at column h * part_w + c (zero past n_sel); rows of a partial
  * last tile beyond row_end are not written.  holo_pairs as for
- * rspi_rot_log_slices_pairs; out 16-byte aligned. */
-int rspi_rot_log_slices_sets(const double *holo_pairs, long long n_states0, long long num_rot,
-                             const double *rot_cs, long long size, const double *bg,
-                             const int *sel_pix, long long n_sel, int n_parts, int part_w,
-                             long long row_begin, long long row_end, float *out,
-                             float *abs_max, cudaStream_t stream);
+ * rspi_rot_log_slices_pairs; out 16-byte aligned.  holo_pairs32 NULL: the
+ * values of rspi_rot_log_slices rounded to FP32 (identical bits).
+ * holo_pairs32 given (the same pairs in FP32, rspi_holo_pairs32): the
+ * interpolation and the log in FP32, |L32 - L| <= 2^-24 (10 + 2 |L|), with
+ * values at or below 2e-20 (and the in-detector test) in FP64 so the -1000
+ * sentinel falls where the reference's does; the caller's candidate
+ * threshold must cover the extra error (rows + 12 with abs_max >= 1). */
+int rspi_holo_pairs32(const double *holo, long long n_states0, long long size,
+                      float *holo_pairs32, cudaStream_t stream);
+int rspi_rot_log_slices_sets(const double *holo_pairs, const float *holo_pairs32,
+                             long long n_states0, long long num_rot, const double *rot_cs,
+                             long long size, const double *bg, const int *sel_pix,
+                             long long n_sel, int n_parts, int part_w, long long row_begin,
+                             long long row_end, float *out, float *abs_max, cudaStream_t stream);
 
 /* FP32 screening likelihood of rows [row_begin, row_end) from those slices
  * (one bulk copy per tile part into shared memory) and the set entries: lane l

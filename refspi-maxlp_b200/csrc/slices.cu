@@ -110,6 +110,14 @@ __global__ void k_holo_pairs(const double *__restrict__ holo, long long total,
         hp[i] = make_double2(holo[i], i + 1 < total ? holo[i + 1] : 0.);
 }
 
+// The same pairs rounded to FP32, for the frame-set slices' FP32 arithmetic.
+__global__ void k_holo_pairs32(const double *__restrict__ holo, long long total,
+                               float2 *__restrict__ hp) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
+        hp[i] = make_float2((float)holo[i], i + 1 < total ? (float)holo[i + 1] : 0.f);
+}
+
 template <typename TL, bool PAIRS>
 __global__ void __launch_bounds__(256)
 k_rot_log_js(const double *__restrict__ holo, const double2 *__restrict__ hp, int num_rot,
@@ -202,11 +210,23 @@ k_rot_log_js(const double *__restrict__ holo, const double2 *__restrict__ hp, in
 // num_rot and row_begin multiples of four a state's four rotations are one
 // tile's four rows, stored as one 16-byte write.  Values are those of
 // rot_log_value (same operations, identical bits).
+//
+// With MATH32 the value of each (state, rotation) is computed in FP32 from
+// an FP32 copy of the pairs: bilinear interpolation of positive terms
+// (|relative error| <= 9 * 2^-24: the FP32 roundings of W, the weights and
+// bg, four products and four sums) and logf (at most 1 ulp, CUDA's
+// documented bound), so |L32 - L| <= 2^-24 (10 + 2 |L|); the rotated
+// positions, floors and the in-detector test stay FP64, and an
+// interpolated value at or below 2e-20 (or above 1e30) is computed in FP64
+// instead, so the -1000 sentinel is taken exactly where the reference takes
+// it.
+template <bool MATH32>
 __global__ void __launch_bounds__(256)
-k_rot_log_sets(const double2 *__restrict__ hp, int num_rot, const double *__restrict__ rot_cs,
-               int size, const double *__restrict__ bg, const int *__restrict__ sel_pix, int n_sel,
-               int n_parts, int part_w, long long row_begin, long long row_end, long long s_lo,
-               float *__restrict__ out, float *__restrict__ abs_max) {
+k_rot_log_sets(const double2 *__restrict__ hp, const float2 *__restrict__ hp32, int num_rot,
+               const double *__restrict__ rot_cs, int size, const double *__restrict__ bg,
+               const int *__restrict__ sel_pix, int n_sel, int n_parts, int part_w,
+               long long row_begin, long long row_end, long long s_lo, float *__restrict__ out,
+               float *__restrict__ abs_max) {
     const int n_jb = (num_rot + 3) / 4;
     const int j0 = (int)(blockIdx.x % (unsigned)n_jb) * 4;
     const long long s_first = s_lo + (long long)(blockIdx.x / (unsigned)n_jb) * RL_STATES;
@@ -258,22 +278,40 @@ k_rot_log_sets(const double2 *__restrict__ hp, int num_rot, const double *__rest
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     double val = 0.;
-                    if (c < n_sel) {
-                        if (in[q]) {
-                            const double2 a = hp[s0 * npix + base[q]];
-                            const double2 b2 = hp[s0 * npix + base[q] + size];
-                            const double cx = 1. - fx[q], cy = 1. - fy[q];
-                            double t = xmul(xmul(a.x, cx), cy);
-                            t = xadd(t, xmul(xmul(b2.x, fx[q]), cy));
-                            t = xadd(t, xmul(xmul(a.y, cx), fy[q]));
-                            t = xadd(t, xmul(xmul(b2.y, fx[q]), fy[q]));
-                            t = xadd(t, b);
-                            val = t < 1.e-20 ? -1000. : log(t);
-                        } else {
-                            val = -1000.;
+                    bool done = false;
+                    if (MATH32 && c < n_sel && in[q]) {
+                        const float2 a = hp32[s0 * npix + base[q]];
+                        const float2 b2 = hp32[s0 * npix + base[q] + size];
+                        const float fxf = (float)fx[q], fyf = (float)fy[q];
+                        const float cxf = (float)(1. - fx[q]), cyf = (float)(1. - fy[q]);
+                        float t = a.x * cxf * cyf;
+                        t += b2.x * fxf * cyf;
+                        t += a.y * cxf * fyf;
+                        t += b2.y * fxf * fyf;
+                        t += (float)b;
+                        if (t > 2.e-20f && t < 1.e30f) {
+                            v[q] = logf(t);
+                            done = true;
                         }
                     }
-                    v[q] = (float)val;
+                    if (!done) {
+                        if (c < n_sel) {
+                            if (in[q]) {
+                                const double2 a = hp[s0 * npix + base[q]];
+                                const double2 b2 = hp[s0 * npix + base[q] + size];
+                                const double cx = 1. - fx[q], cy = 1. - fy[q];
+                                double t = xmul(xmul(a.x, cx), cy);
+                                t = xadd(t, xmul(xmul(b2.x, fx[q]), cy));
+                                t = xadd(t, xmul(xmul(a.y, cx), fy[q]));
+                                t = xadd(t, xmul(xmul(b2.y, fx[q]), fy[q]));
+                                t = xadd(t, b);
+                                val = t < 1.e-20 ? -1000. : log(t);
+                            } else {
+                                val = -1000.;
+                            }
+                        }
+                        v[q] = (float)val;
+                    }
                 }
                 const long long r0 = s0 * num_rot + j0 - row_begin;
                 if (j0 + 3 < num_rot && (r0 & 3) == 0 && r0 >= 0 && r0 + 3 < n_rows) {
@@ -398,18 +436,30 @@ extern "C" int rspi_sphere_ramp(long long size, double sx, double sy, double dia
     RSPI_RETURN_LAUNCH();
 }
 
-extern "C" int rspi_rot_log_slices_sets(const double *holo_pairs, long long n_states0,
-                                        long long num_rot, const double *rot_cs, long long size,
-                                        const double *bg, const int *sel_pix, long long n_sel,
-                                        int n_parts, int part_w, long long row_begin,
-                                        long long row_end, float *out, float *abs_max,
-                                        cudaStream_t stream) {
+extern "C" int rspi_holo_pairs32(const double *holo, long long n_states0, long long size,
+                                 float *holo_pairs32, cudaStream_t stream) {
+    if (!holo || !holo_pairs32 || n_states0 <= 0 || size <= 1 || size > 46340 ||
+        (reinterpret_cast<uintptr_t>(holo_pairs32) & 7) != 0)
+        return RSPI_ERR_ARG;
+    const long long total = n_states0 * size * size;
+    k_holo_pairs32<<<rspi_blocks(total, 256), 256, 0, stream>>>(
+        holo, total, reinterpret_cast<float2 *>(holo_pairs32));
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_rot_log_slices_sets(const double *holo_pairs, const float *holo_pairs32,
+                                        long long n_states0, long long num_rot,
+                                        const double *rot_cs, long long size, const double *bg,
+                                        const int *sel_pix, long long n_sel, int n_parts,
+                                        int part_w, long long row_begin, long long row_end,
+                                        float *out, float *abs_max, cudaStream_t stream) {
     if (!holo_pairs || !rot_cs || !bg || !out || n_states0 <= 0 || num_rot <= 0 ||
         num_rot > 0x7fffffffLL || size <= 1 || size > 46340 || n_sel < 0 || n_parts < 1 ||
         part_w < 1 || (long long)n_parts * part_w < n_sel ||
         (long long)n_parts * part_w > 0x7fffffffLL || row_begin < 0 || row_end < row_begin ||
         row_end > n_states0 * num_rot || (n_sel > 0 && !sel_pix) ||
         (reinterpret_cast<uintptr_t>(holo_pairs) & 15) != 0 ||
+        (reinterpret_cast<uintptr_t>(holo_pairs32) & 7) != 0 ||
         (reinterpret_cast<uintptr_t>(out) & 15) != 0)
         return RSPI_ERR_ARG;
     if (row_end == row_begin) return RSPI_OK;
@@ -417,8 +467,15 @@ extern "C" int rspi_rot_log_slices_sets(const double *holo_pairs, long long n_st
     const long long n_groups = (s_hi - s_lo) / RL_STATES + 1;
     const long long n_jb = (num_rot + 3) / 4;
     if (n_groups * n_jb > 0x7fffffffLL) return RSPI_ERR_ARG;
-    k_rot_log_sets<<<(unsigned)(n_groups * n_jb), 256, 0, stream>>>(
-        reinterpret_cast<const double2 *>(holo_pairs), (int)num_rot, rot_cs, (int)size, bg,
-        sel_pix, (int)n_sel, n_parts, part_w, row_begin, row_end, s_lo, out, abs_max);
+    const double2 *hp = reinterpret_cast<const double2 *>(holo_pairs);
+    const float2 *hp32 = reinterpret_cast<const float2 *>(holo_pairs32);
+    if (hp32)
+        k_rot_log_sets<true><<<(unsigned)(n_groups * n_jb), 256, 0, stream>>>(
+            hp, hp32, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, n_parts, part_w,
+            row_begin, row_end, s_lo, out, abs_max);
+    else
+        k_rot_log_sets<false><<<(unsigned)(n_groups * n_jb), 256, 0, stream>>>(
+            hp, nullptr, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, n_parts,
+            part_w, row_begin, row_end, s_lo, out, abs_max);
     RSPI_RETURN_LAUNCH();
 }

@@ -20,7 +20,10 @@ densely, likelihood as a tensor-core GEMM, ``dense_gemm`` = ``auto`` /
 (default true: FP64 rescoring of the candidates as in ``screen``)),
 ``kernel`` (the likelihood kernel: ``sets`` or ``quad4`` (four-row
 tiles) or ``stream`` for the screened form, ``stream`` or ``dynamic`` for
-``fp64``; default: the form's default), ``screen_delta``
+``fp64``; default: the form's default), ``slice_math`` (``fp64``, the
+default, or ``fp32``: the frame-set kernel's log-slices interpolated and
+logged in FP32 within a bound the candidate threshold covers),
+``screen_delta``
 (default 0: FP64 rescoring of the states that can be the argmax, which is
 what the hard-argmax iteration uses; 20: also every state within 20 nats of
 it, so that ``logz`` equals the FP64 form's -- the posterior consumers'
@@ -116,7 +119,8 @@ class EMC():
                            delta=self.screen_delta,
                            slice_budget_bytes=int(self.slice_budget_gb * (1 << 30)),
                            n_modes=self.num_modes, dense_gemm=self.dense_gemm,
-                           dense_rescore=self.dense_rescore, kernel=self.kernel)
+                           dense_rescore=self.dense_rescore, kernel=self.kernel,
+                           slice_math=self.slice_math)
         self.state_vals = torch.from_numpy(self._state_values).to(self.device)
         self.phaser_rot = torch.from_numpy(geometry.phaser_rotation_table(
             np.arange(self.num_rot) * np.pi / self.num_rot)).to(self.device)
@@ -153,6 +157,7 @@ class EMC():
         self.dense_rescore = config.getboolean('emc', 'dense_rescore', fallback=True)
         self.autotune = config.getboolean('emc', 'autotune', fallback=True)
         self.kernel = config.get('emc', 'kernel', fallback=None) or None
+        self.slice_math = config.get('emc', 'slice_math', fallback='fp64')
         self.mstep_kind = config.get('emc', 'mstep', fallback='pattern')
         if self.mstep_kind not in ('pattern', 'grid', 'lbfgs', 'grid+lbfgs'):
             raise ValueError('emc:mstep must be pattern, grid, lbfgs or grid+lbfgs')

@@ -236,7 +236,8 @@ class EStep:
     def __init__(self, photons, size, num_rot, shiftx, shifty, sphere_dia, probmask, bg,
                  form='fp64', states_per_tile=None, warps=32, n_ctas=0,
                  slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel=None,
-                 n_modes=1, dense_gemm='auto', dense_rescore=True, screen_parts=None):
+                 n_modes=1, dense_gemm='auto', dense_rescore=True, screen_parts=None,
+                 slice_math='fp64'):
         if form not in ('fp64', 'screen', 'dense'):
             raise ValueError('form must be fp64, screen or dense')
         if kernel is None:   # default likelihood kernel of each form
@@ -246,6 +247,11 @@ class EStep:
         if kernel not in kernels:
             raise ValueError('the %s form takes the kernels %s' % (form, ', '.join(kernels)))
         self.screen_parts = None if screen_parts is None else int(screen_parts)
+        if slice_math not in ('fp64', 'fp32'):
+            raise ValueError('slice_math must be fp64 or fp32')
+        if slice_math == 'fp32' and kernel != 'sets':
+            raise ValueError('FP32 slice arithmetic is for the frame-set kernel')
+        self.slice_math = slice_math
         self.kernel = kernel
         self.lib = load()
         self.form = form
@@ -272,6 +278,7 @@ class EStep:
         self.bg = t(np.asarray(bg, dtype='f8').ravel())
         self.ll = photons.ll_entries(self.pix2sel, self.p_pad)
         self.col_of_frame, self.frame_of_col, self.n_cols = None, None, n
+        self.holo_pairs32 = None
         if form == 'dense':
             self._init_dense(photons, slice_budget_bytes, delta, cand_per_frame, dense_gemm,
                              dense_rescore)
@@ -315,6 +322,10 @@ class EStep:
             self.n_cols = self.wide['n_sets'] * 32
             self.frame_max = torch.zeros(self.n_cols, dtype=_i64, device=dev)
             self.cand_slot = torch.empty(n * 32, dtype=_i32, device=dev)
+        # FP32 copy of the pairs for the FP32 slice arithmetic
+        self.holo_pairs32 = torch.empty((self.n_states0, self.size ** 2, 2),
+                                        dtype=torch.float32, device=dev) \
+            if self.slice_math == 'fp32' else None
         self._eps_key, self.row_off_eps = None, None
         esz = {0: 4, 1: 8, 2: 2}[self.slice_code]
         # slice bytes per likelihood row (the frame-set layout holds the
@@ -587,6 +598,8 @@ class EStep:
             rows = ro[1:] - ro[:-1]
             if self.wide is not None:
                 rows = torch.maximum(rows, self.wide['frame_groups'].to(_i64))
+            if self.slice_math == 'fp32':
+                rows = rows + 12
             self.row_off_eps = torch.cat([torch.zeros(1, dtype=_i64, device=self.device),
                                           torch.cumsum(rows, 0)])
             self._eps_key = key
@@ -630,7 +643,12 @@ class EStep:
             call('rspi_holo_pairs', ptr(self.holo), self.n_states0, self.size,
                  ptr(self.holo_pairs), s)
         if self.form != 'fp64':
-            self.lmax.zero_()
+            # FP32 slice arithmetic: its per-value error bound 2^-24 (10 + 2|L|)
+            # is charged as 12 more summation steps of max(|L|, 1)
+            self.lmax.fill_(1. if self.slice_math == 'fp32' else 0.)
+        if self.holo_pairs32 is not None:
+            call('rspi_holo_pairs32', ptr(self.holo), self.n_states0, self.size,
+                 ptr(self.holo_pairs32), s)
         if self.col_of_frame is not None:
             self.frame_max.zero_()
 
@@ -651,7 +669,8 @@ class EStep:
         out = self.lsl if out is None else out
         if self.kernel == 'sets':
             w = self.wide
-            call('rspi_rot_log_slices_sets', ptr(self.holo_pairs), self.n_states0, self.num_rot,
+            call('rspi_rot_log_slices_sets', ptr(self.holo_pairs), ptr(self.holo_pairs32),
+                 self.n_states0, self.num_rot,
                  ptr(self.rot_cs), self.size, ptr(self.bg), ptr(self.sel_pix), self.n_sel,
                  w['n_parts'], w['part_w'], r0, r1, ptr(out), ptr(self.lmax), cur_stream())
             return out

@@ -544,7 +544,7 @@ def test_sets_slice_layout_bit_identical(num_rot, r0, r1):
     tiles = (r1 - r0 + 3) // 4
     out = torch.full((tiles * parts * pw * 4,), 7., dtype=torch.float32, device='cuda')
     amax_b = torch.zeros(1, dtype=torch.float32, device='cuda')
-    call('rspi_rot_log_slices_sets', ptr(es.holo_pairs), es.n_states0, es.num_rot,
+    call('rspi_rot_log_slices_sets', ptr(es.holo_pairs), None, es.n_states0, es.num_rot,
          ptr(es.rot_cs), es.size, ptr(es.bg), ptr(es.sel_pix), es.n_sel, parts, pw, r0, r1,
          ptr(out), ptr(amax_b), cur_stream())
     torch.cuda.synchronize()
@@ -605,3 +605,44 @@ def test_one_pass_candidates_equal_two_pass(delta):
     if delta >= 20.:
         # some frames took the second scan
         assert (np.diff(outs[0][0]) > 32).any() or delta == 20.
+
+
+@pytest.mark.parametrize('name,ds,need_scaling', CASES, ids=[c[0] for c in CASES])
+def test_sets_fp32_slice_arithmetic(name, ds, need_scaling):
+    """FP32 interpolation and log in the frame-set slices: every value within
+    2^-24 (10 + 2|L|) of the FP64 value (the sentinel exactly where FP64 has
+    it), the FP32 likelihoods within 1e-5 of the FP64 form's, and after
+    FP64 rescoring the same argmax, maximum and log-sum-exp."""
+    size = int(round(np.sqrt(ds['num_pix'])))
+    num_rot = 6
+    sx, sy, dia, _ = E.generate_states(E.parse_triple('-1 1 3'), E.parse_triple('0 1 2'),
+                                       E.parse_triple('2 3 2'))
+    rng = np.random.default_rng(size + 3)
+    model = torch.from_numpy(rng.random(size * size) + 1j * rng.random(size * size)).cuda()
+    out = {}
+    for math in ('fp64', 'fp32'):
+        ph = _photons(ds, need_scaling)
+        es = _estep(ph, size, num_rot, sx, sy, dia, ds['bg'], form='screen', kernel='sets',
+                    slice_math=math, screen_parts=2 if size > 20 else None)
+        es.run(model)
+        lsl = es.lsl.clone()
+        maxll, rmax, logz = es.reduce()
+        torch.cuda.synchronize()
+        out[math] = (lsl.cpu().numpy(), es.frame_prob().cpu().numpy().astype(np.float64),
+                     maxll.cpu().numpy(), rmax.cpu().numpy(), logz.cpu().numpy())
+    a, b = out['fp64'], out['fp32']
+    real = a[0] != 0
+    assert np.array_equal(a[0] == -1000., b[0] == -1000.)
+    assert np.all(np.abs(b[0] - a[0]) <= 2. ** -24 * (10. + 2. * np.abs(a[0])) * (1 + 1e-6))
+    assert real.any()
+    _, pm = E.generate_masks(size)
+    ref = _estep(_photons(ds, need_scaling), size, num_rot, sx, sy, dia, ds['bg'], form='fp64')
+    ref.run(model)
+    ref.reduce()
+    want = ref.frame_prob().cpu().numpy()
+    with np.errstate(invalid='ignore'):
+        rel = np.abs(b[1] - want) / np.abs(want)
+    assert np.nanmax(rel) <= RTOL_F32 or np.isnan(want).all()
+    assert np.array_equal(a[3], b[3])
+    np.testing.assert_allclose(a[2], b[2], rtol=1e-15)
+    np.testing.assert_allclose(a[4], b[4], rtol=1e-9)

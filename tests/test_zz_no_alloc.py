@@ -87,3 +87,54 @@ def test_noalloc_rejects_more_frames_than_its_scratch():
                                               null, null, null, null, 0, null, null, null, null)
     assert code == -6
     assert 'scratch' in lib.rspi_status_string(code).decode()
+
+
+def test_noalloc_at_its_frame_limit():
+    """65,536 frames, the most the fixed scratch holds: the last slots of the
+    library's array are written and read back, and the outputs equal the
+    allocating entry point's on a synthetic likelihood matrix."""
+    from rspi.device import call, cur_stream, ptr
+    n, rows = 65536, 9
+    g = torch.Generator(device='cuda')
+    g.manual_seed(5)
+    ll = (torch.randn((rows, n), generator=g, device='cuda') * 3. - 100.).float()
+    max32 = torch.empty(n, dtype=torch.float64, device='cuda')
+    rmax32 = torch.empty(n, dtype=torch.int32, device='cuda')
+    call('rspi_frame_reduce', ptr(ll), 0, rows, n, ptr(max32), ptr(rmax32), None, cur_stream())
+    phot = torch.randint(0, 300, (n,), generator=g, device='cuda', dtype=torch.int64)
+    row_off = torch.arange(n + 1, device='cuda', dtype=torch.int64) * 4
+    lmax = torch.ones(1, dtype=torch.float32, device='cuda')
+    cap = rows * n
+
+    def outputs():
+        return dict(cand_n=torch.full((n,), -7, dtype=torch.int32, device='cuda'),
+                    noncand=torch.full((n,), -7., dtype=torch.float64, device='cuda'),
+                    thr=torch.full((n,), -7., dtype=torch.float64, device='cuda'),
+                    cand_off=torch.full((n + 1,), -7, dtype=torch.int64, device='cuda'),
+                    cand_d=torch.full((cap,), -7, dtype=torch.int32, device='cuda'),
+                    cand_r=torch.full((cap,), -7, dtype=torch.int32, device='cuda'),
+                    err=torch.zeros(1, dtype=torch.int32, device='cuda'))
+    common = (ptr(ll), rows, n, ptr(max32), ptr(rmax32), ptr(phot), ptr(row_off), ptr(lmax),
+              2.0)
+    ref = outputs()
+    scratch = torch.empty(n * 32, dtype=torch.int32, device='cuda')
+    call('rspi_screen_candidates', *common, ptr(scratch), ptr(ref['cand_n']),
+         ptr(ref['noncand']), ptr(ref['thr']), ptr(ref['cand_off']), cap, ptr(ref['cand_d']),
+         ptr(ref['cand_r']), ptr(ref['err']), cur_stream())
+    torch.cuda.synchronize()
+    total = int(ref['cand_off'][n])
+    assert total > n and int(ref['err']) == 0
+    for _ in range(2):
+        out = outputs()
+        call('rspi_screen_candidates_noalloc', *common, ptr(out['cand_n']), ptr(out['noncand']),
+             ptr(out['thr']), ptr(out['cand_off']), cap, ptr(out['cand_d']), ptr(out['cand_r']),
+             ptr(out['err']), cur_stream())
+        torch.cuda.synchronize()
+        assert int(out['err']) == 0
+        for key in ('cand_n', 'cand_off'):
+            assert torch.equal(out[key], ref[key]), key
+        for key in ('cand_d', 'cand_r'):
+            assert torch.equal(out[key][:total], ref[key][:total]), key
+        for key in ('noncand', 'thr'):
+            np.testing.assert_allclose(out[key].cpu().numpy(), ref[key].cpu().numpy(),
+                                       rtol=1e-12, atol=0)

@@ -263,12 +263,11 @@ def write_inputs(tmp, w, data, form, slice_gb=8., screen_delta=None, kernel=None
     cfg = os.path.join(tmp, 'config.ini')
     r = w['recon']
     with open(cfg, 'w') as f:
-        f.write('[emc]\nsize = %d\nin_photons_file = ' +
-                ('photons.npz' if rank is None else 'photons_{rank}.npz') +
-                '\noutput_folder = out/\n'
+        f.write('[emc]\nsize = %d\nin_photons_file = %s\noutput_folder = out/\n'
                 'log_file = out/EMC.log\nneed_scaling = True\nnum_rot = %d\nnum_modes = %d\n'
                 'sphere_dia = %s\nshiftx = %s\nshifty = %s\nform = %s\nslice_budget_gb = %g\n' %
-                (w['size'], r['num_rot'], w['n_modes'], r['sphere_dia'], r['shiftx'], r['shifty'],
+                (w['size'], 'photons.npz' if rank is None else 'photons_{rank}.npz',
+                 r['num_rot'], w['n_modes'], r['sphere_dia'], r['shiftx'], r['shifty'],
                  form, slice_gb))
         if screen_delta is not None:
             f.write('screen_delta = %r\n' % float(screen_delta))

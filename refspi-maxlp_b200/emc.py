@@ -286,11 +286,11 @@ class EMC():
         # the graph holds the whole iteration, or the E-step only with an
         # adjoint-driven M-step (host-side L-BFGS line searches) or with
         # frames split over ranks (collectives in the M-step)
-        part = self._device_step if self.mstep_kind == 'pattern' and self.num_proc == 1 \
-            else self._estep_part
+        whole = self.mstep_kind == 'pattern' and self.num_proc == 1
+        part = self._device_step if whole else self._estep_part
         if self._graph is not None:
             self._graph.replay()
-            if part is not self._device_step:
+            if not whole:
                 self._mstep_part()
             return
         self._device_step()

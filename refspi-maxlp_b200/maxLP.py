@@ -164,9 +164,11 @@ class MaxLPhaser():
                 rvec = rvec.expand(cands.numel()).contiguous()
         elif rescale is not None:
             rs = float(rescale)
-        call('rspi_maxlp_pixel_values', ptr(cands), cands.numel(),
-             ptr(const['k_d'].contiguous()), ptr(const['fref_d'].contiguous()), n, mode, rs,
-             ptr(rvec), ptr(out), cur_stream())
+        # operands held in locals: a temporary passed straight to ptr() is
+        # freed before the launch and its block may be handed to the next one
+        k_d, fref_d = const['k_d'].contiguous(), const['fref_d'].contiguous()
+        call('rspi_maxlp_pixel_values', ptr(cands), cands.numel(), ptr(k_d), ptr(fref_d), n,
+             mode, rs, ptr(rvec), ptr(out), cur_stream())
         return out
 
     def get_rescale_pixel(self, fobj_t, t, const=None):
@@ -314,8 +316,9 @@ class MaxLPhaser():
         (maxLP.py:271-274)'''
         fconv, x = self._image(fconv), self._image(x)
         out = torch.empty_like(x)
-        call('rspi_phase_proj_fourier', ptr(fconv), ptr(self._bytes(self.minvmask)), ptr(x),
-             ptr(out), self.size, cur_stream())
+        inv = self._bytes(self.minvmask)
+        call('rspi_phase_proj_fourier', ptr(fconv), ptr(inv), ptr(x), ptr(out), self.size,
+             cur_stream())
         return out
 
     def proj_real(self, x):
@@ -324,16 +327,20 @@ class MaxLPhaser():
         transformed back'''
         x = self._image(x)
         out = torch.empty_like(x)
-        call('rspi_phase_proj_real', ptr(x), ptr(self._bytes(self.minvsuppmask)), ptr(out),
-             ptr(self._work()), self.size, cur_stream())
+        supp = self._bytes(self.minvsuppmask)
+        call('rspi_phase_proj_real', ptr(x), ptr(supp), ptr(out), ptr(self._work()), self.size,
+             cur_stream())
         return out
 
     def _refine(self, fconv, x, n_dm, n_er):
         fconv = self._image(fconv)
         out = self._image(x).clone()
-        call('rspi_phase_refine', ptr(fconv), ptr(self._bytes(self.minvmask)),
-             ptr(self._bytes(self.minvsuppmask)), ptr(out), ptr(self._work()), self.size,
-             int(n_dm), int(n_er), cur_stream())
+        # both masks held until the launch: a temporary handed straight to
+        # ptr() goes back to the allocator at once, and the second mask's copy
+        # could then land in the first one's block before the kernel reads it
+        inv, supp = self._bytes(self.minvmask), self._bytes(self.minvsuppmask)
+        call('rspi_phase_refine', ptr(fconv), ptr(inv), ptr(supp), ptr(out), ptr(self._work()),
+             self.size, int(n_dm), int(n_er), cur_stream())
         rlib.launch_count += 5 * (int(n_dm) + int(n_er))
         return out
 

@@ -18,9 +18,10 @@ FP64 rescoring of every state that can be the argmax (and, with
 densely, likelihood as a tensor-core GEMM, ``dense_gemm`` = ``auto`` /
 ``i8`` (exact fixed point) / ``bf16`` (hi + lo split), ``dense_rescore``
 (default true: FP64 rescoring of the candidates as in ``screen``)),
-``kernel`` (the likelihood kernel: ``sets`` or ``quad4`` (four-row
-tiles) or ``stream`` for the screened form, ``stream`` or ``dynamic`` for
-``fp64``; default: the form's default), ``slice_math`` (``fp64``, the
+``kernel`` (the likelihood kernel: ``sets`` (the screened form's
+default: one lane per frame, 32 frames per warp), ``quad4`` (four frames
+per warp) or ``stream`` for the screened form, ``stream`` (default) or
+``dynamic`` for ``fp64``), ``slice_math`` (``fp64``, the
 default, or ``fp32``: the frame-set kernel's log-slices interpolated and
 logged in FP32 within a bound the candidate threshold covers),
 ``screen_delta``

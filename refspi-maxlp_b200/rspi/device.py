@@ -231,6 +231,14 @@ class EStep:
     ``dense_rescore`` the candidates within delta + 2 eps of each frame's
     maximum are rescored in FP64 as in the screened form; without it the
     GEMM values are final (FP64 log-sum-exp over them).
+
+    ``kernel`` (the likelihood kernel): for the screened form ``sets`` (the
+    default: frames 32 at a time, one lane per frame, a bank-conflict-free
+    step schedule; likelihood columns in set order, ``frame_prob()`` gives
+    frame order), ``quad4`` (four frames per warp) or ``stream``; for the
+    FP64 form ``stream`` (default) or ``dynamic``.  ``slice_math='fp32'``
+    (frame-set kernel only) interpolates and logs the slices in FP32 within
+    a bound that the candidate threshold covers.
     """
 
     def __init__(self, photons, size, num_rot, shiftx, shifty, sphere_dia, probmask, bg,
@@ -241,7 +249,7 @@ class EStep:
         if form not in ('fp64', 'screen', 'dense'):
             raise ValueError('form must be fp64, screen or dense')
         if kernel is None:   # default likelihood kernel of each form
-            kernel = 'quad4' if form == 'screen' else 'stream'
+            kernel = 'sets' if form == 'screen' else 'stream'
         kernels = {'fp64': ('stream', 'dynamic'), 'screen': ('stream', 'quad4', 'sets'),
                    'dense': ('stream', 'tcgen05')}[form]
         if kernel not in kernels:

@@ -714,6 +714,51 @@ int rspi_phase_refine(const double *fconv, const unsigned char *minvmask,
                       const unsigned char *minvsupp, double *x, double *work, long long size,
                       int n_dm, int n_er, cudaStream_t stream);
 
+/* ------------------------------------------------------------ data simulator
+ * The per-frame loop of the reference's simulator (make_data.py:199-333),
+ * batched: frames frame0 .. frame0 + n_frames - 1 of a dataset.
+ * rspi_sim_views: view[f] (size^2 doubles per frame) = the holographic
+ *   intensity scale[f] * |M_f + rel_scale * ff * ramp|^2 (kernels.cu:44-82,
+ *   no background; ramp from shifts[2f], shifts[2f+1], ff from dia[f]) of the
+ *   frame's model M_f, times mask_value on the detector mask (0 where
+ *   r < 4 or r >= size/2; make_data.py:210-216 -- mask_value 2 for a
+ *   heterogeneous object, whose two masks are added), scaled to sum to
+ *   mean_count (make_data.py:316-318).  M_f by kind (make_data.py:294-309):
+ *   0 iso: model; 1 homo, 2 mix, 3 blur: model plus wobble_model times the
+ *   phase ramps e^{2 pi i w (qx + qy)} / e^{2 pi i w (qx - 3.7 qy)}
+ *   (w = wobble[f]; mix alternates by the parity of frame0 + f; mirrored
+ *   columns as np.fliplr).  model and wobble_model are complex128 size^2.
+ *   A frame whose masked intensity sums to zero sets RSPI_ERR_ARG.
+ * rspi_sim_counts: counts[f] (int32 size^2) ~ Poisson of the view rotated by
+ *   the frame's angle (rot_cs[2f], rot_cs[2f+1] = cos, sin; slice_gen's
+ *   bilinear rule, kernels.cu:6-42, pixels whose footprint leaves the
+ *   detector 0) plus bg (NULL: none) on the others; expected (NULL: not
+ *   written) receives the Poisson means.  Draws come from Philox4x32-10 with
+ *   key = seed and counter (pixel, frame), so they do not depend on how the
+ *   frames are batched.  n_frames <= 65535.  A mean that is negative, not
+ *   finite or above 1e9 sets RSPI_ERR_ARG.
+ * rspi_sim_poisson: out[i] ~ Poisson(lam[i]) from the same generator
+ *   (stream_id separates the draws of different calls).
+ * rspi_sim_sparse_counts: ones[f] / multi[f] = pixels of frame f with one /
+ *   with more than one photon.
+ * rspi_sim_sparse_fill: those pixels in ascending order at ones_off[f] /
+ *   multi_off[f] (exclusive prefix sums of ones / multi), with the counts of
+ *   the latter in count_multi (make_data.py:324-328). */
+int rspi_sim_views(const double *model, const double *wobble_model, int kind, long long frame0,
+                   long long n_frames, const double *wobble, const double *shifts,
+                   const double *dia, const double *scale, double rel_scale, double mean_count,
+                   double mask_value, int size, double *view, int *err, cudaStream_t stream);
+int rspi_sim_counts(const double *view, long long frame0, long long n_frames,
+                    const double *rot_cs, const double *bg, int size, unsigned long long seed,
+                    int *counts, double *expected, int *err, cudaStream_t stream);
+int rspi_sim_poisson(const double *lam, long long n, unsigned long long seed,
+                     unsigned long long stream_id, int *out, int *err, cudaStream_t stream);
+int rspi_sim_sparse_counts(const int *counts, long long n_frames, long long num_pix, int *ones,
+                           int *multi, cudaStream_t stream);
+int rspi_sim_sparse_fill(const int *counts, long long n_frames, long long num_pix,
+                         const long long *ones_off, const long long *multi_off, int *place_ones,
+                         int *place_multi, int *count_multi, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

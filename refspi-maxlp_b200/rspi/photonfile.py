@@ -85,3 +85,43 @@ class PhotonsFile:
         if key in self._raw:
             return self._raw[key]
         raise KeyError(key)
+
+
+def update_datasets(path, new, delete=()):
+    """Write the datasets ``new`` into the photons file ``path`` (HDF5 for
+    ``.h5``, else ``.npz``), keeping the file's other datasets except those
+    named in ``delete`` -- what the reference does with h5py's append mode
+    (make_data.py:156-167, 228-276).  Values of ``place_ones``,
+    ``place_multi`` and ``count_multi`` are flat arrays whose row lengths are
+    ``ones`` / ``multi`` (as for ``write_photons``)."""
+    raw = {}
+    if os.path.exists(path):
+        raw = dict(PhotonsFile(path)._raw)
+    gone = set(delete) | set(new)
+    raw = {k: v for k, v in raw.items() if k.split('@')[0] not in gone}
+    lens = {'place_ones': 'ones', 'place_multi': 'multi', 'count_multi': 'multi'}
+    for key, val in new.items():
+        if key in VLEN:
+            src = new.get(lens[key])
+            if src is None:
+                raise ValueError('%s needs %s in the same update' % (key, lens[key]))
+            raw[key + '@flat'] = np.asarray(val, dtype='i4')
+            raw[key + '@lens'] = np.asarray(src, dtype='i8')
+        else:
+            raw[key] = np.asarray(val)
+    if path.endswith('.h5'):
+        from . import h5lite
+        out = {}
+        for k, v in raw.items():
+            if k.endswith('@flat'):
+                name = k[:-5]
+                out[name] = ('vlen', np.asarray(v, dtype='<i4'), raw[name + '@lens'])
+            elif not k.endswith('@lens'):
+                out[k] = v
+        h5lite.write_datasets(path, out)
+        return path
+    tmp = path + '.tmp'
+    with open(tmp, 'wb') as fh:
+        np.savez(fh, **raw)
+    os.replace(tmp, path)
+    return path

@@ -295,9 +295,11 @@ int rspi_rot_log_slices_sets(const double *holo_pairs, const float *holo_pairs32
  * accumulators over the groups, each group's four photons as a depth-two
  * tree: at most ceil(G/2) + 3 roundings per value and part, G = the set's
  * groups in the part); the parts are added in FP64 before the final
- * rounding, the running sum of parts before the last kept in part_sums
- * (rspi_sets_part_sums_floats(n_sets, part_sums_ctas) floats, 16-byte
- * aligned; at most part_sums_ctas CTAs run).  LL32 of row r, frame
+ * rounding, the running sum of parts before the last kept in the SM's
+ * tensor memory for the first 512 sets (each CTA allocates all 512 TMEM
+ * columns and frees them before it ends; warps_per_cta >= 4) and in
+ * part_sums for the others (rspi_sets_part_sums_floats(n_sets,
+ * part_sums_ctas) floats, 16-byte aligned; at most part_sums_ctas CTAs run).  LL32 of row r, frame
  * set_frames[c] goes to ll[(r - row_begin) * ll_stride + c] (ll_stride >=
  * n_sets * 32), and frame_max[c] (zero before the first launch of a pass)
  * takes the unsigned maximum of an order-preserving (value, row) key, read

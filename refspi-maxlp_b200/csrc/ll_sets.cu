@@ -351,14 +351,50 @@ __device__ __forceinline__ float4 group_sum(const unsigned char *tile, uint2 e) 
     return f4_add(f4_add(v0, v1), f4_add(v2, v3));
 }
 
+// Tensor memory (TMEM, 128 lanes x 512 columns of 32 bits per SM) as the
+// store of the running part sums: warp w reaches lanes 32 (w % 4) .. + 31, so
+// set s lives in lane quarter s % 4, columns 4 (s / 4) .. + 3 (one float4 per
+// lane), for the first TMEM_SETS sets; later sets use the global scratch.
+constexpr int TMEM_COLS = 512;
+constexpr int TMEM_SETS = 4 * (TMEM_COLS / 4);
+
+__device__ __forceinline__ void tmem_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_store4(unsigned taddr, float4 v) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1, %2, %3, %4};" ::"r"(taddr),
+                 "r"(__float_as_uint(v.x)), "r"(__float_as_uint(v.y)), "r"(__float_as_uint(v.z)),
+                 "r"(__float_as_uint(v.w))
+                 : "memory");
+    asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ float4 tmem_load4(unsigned taddr) {
+    unsigned x, y, z, w;
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(x), "=r"(y), "=r"(z), "=r"(w)
+                 : "r"(taddr)
+                 : "memory");
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    return make_float4(__uint_as_float(x), __uint_as_float(y), __uint_as_float(z),
+                       __uint_as_float(w));
+}
+
 // Lane l of a set sums frame set_frames[32 s + l] over the set's groups of
 // the part: groups alternate between two accumulators, then a0 + a1.  Each
 // photon's value passes through at most ceil(G / 2) + 3 FP32 roundings in a
-// part (G = the set's group count there).  Parts before the last keep the
-// running FP32 sum of (row, column 32 s + l) in part_sums[cta][32 s + l];
-// the last part adds the parts in FP64 before the final rounding, stores
-// the four rows' likelihoods in column 32 s + l and folds them into the
-// column's argmax key (frame_max).
+// part (G = the set's group count there).  With several parts, the parts
+// before the last keep the running FP32 sum of (row, column 32 s + l) in
+// tensor memory (sets below TMEM_SETS; the others in
+// part_sums[cta][32 (s - TMEM_SETS) + l]); sets are then handed out by four
+// queues, queue q = s % 4 to the warps w with w % 4 = q, so that a set meets
+// its lane quarter in every part.  The last part adds the parts in FP64
+// before the final rounding, stores the four rows' likelihoods in column
+// 32 s + l and folds them into the column's argmax key (frame_max).
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 1)
 k_screen_sets(const float4 *__restrict__ lsl4, int num_rot, const double *__restrict__ init,
@@ -369,29 +405,49 @@ k_screen_sets(const float4 *__restrict__ lsl4, int num_rot, const double *__rest
               unsigned long long *__restrict__ frame_max, int *err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) unsigned long long mbar;
-    __shared__ int next_set;
+    __shared__ int next_set[4];
     __shared__ int abort_flag;
+    __shared__ unsigned tmem_slot;
     float4 *tile = reinterpret_cast<float4 *>(smem_raw);
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned bytes = (unsigned)part_w * 16u;
     const unsigned mbar_a = smem_u32(&mbar), tile_a = smem_u32(tile);
     const unsigned long long keep = policy_evict_last(), stream_out = policy_evict_first();
+    const bool split = n_parts > 1;   // running part sums (TMEM + scratch)
     if (threadIdx.x < 8) tile[part_w + threadIdx.x] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mbar_a) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         abort_flag = 0;
     }
+    if (split && warp == 0) {
+        // the whole tensor memory of the SM (one CTA per SM: 200 KB of
+        // shared memory each); freed by the same warp at the end
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_slot)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tmem_fence_before();
+    __syncthreads();
+    tmem_fence_after();
+    const unsigned tbase = split ? tmem_slot + ((unsigned)((warp & 3) * 32) << 16) : 0u;
+    const int queue = split ? (warp & 3) : 0, n_queues = split ? 4 : 1;
+    const int n_extra = n_sets > TMEM_SETS ? n_sets - TMEM_SETS : 0;
+    float4 *ps = split ? part_sums + (long long)blockIdx.x * n_extra * 32 : nullptr;
     unsigned phase = 0;
+    bool aborted = false;
     const long long n_tiles = (row_end - row_begin + 3) / 4;
-    float4 *ps = part_sums ? part_sums + (long long)blockIdx.x * n_sets * 32 : nullptr;
-    for (long long t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    for (long long t = blockIdx.x; t < n_tiles && !aborted; t += gridDim.x) {
         const long long first = row_begin + 4 * t;
         const int nt = (int)min(4LL, row_end - first);
         for (int h = 0; h < n_parts; ++h) {
+            tmem_fence_before();
             __syncthreads();   // every warp is done with the previous part
+            tmem_fence_after();
             if (threadIdx.x == 0) {
-                next_set = 0;
+                next_set[0] = next_set[1] = next_set[2] = next_set[3] = 0;
                 const float4 *src = lsl4 + (t * n_parts + h) * (long long)part_w;
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar_a),
@@ -444,7 +500,8 @@ k_screen_sets(const float4 *__restrict__ lsl4, int num_rot, const double *__rest
                             : "r"(mbar_a), "r"(phase ^ 1u)
                             : "memory");
                 }
-                return;
+                aborted = true;
+                break;
             }
             const bool last = h == n_parts - 1;
             double ini[4] = {0., 0., 0., 0.};
@@ -455,7 +512,7 @@ k_screen_sets(const float4 *__restrict__ lsl4, int num_rot, const double *__rest
             }
             while (true) {
                 int s = 0;
-                if (lane == 0) s = atomicAdd(&next_set, 1);
+                if (lane == 0) s = queue + n_queues * atomicAdd(&next_set[queue], 1);
                 s = __shfl_sync(RSPI_FULL_MASK, s, 0);
                 if (s >= n_sets) break;
                 const long long gi = (long long)h * n_sets + s;
@@ -476,24 +533,30 @@ k_screen_sets(const float4 *__restrict__ lsl4, int num_rot, const double *__rest
                 if (g < g1) a0 = f4_add(a0, group_sum(smem_raw, c0));
                 const float4 sum = f4_add(a0, a1);
                 const int col = s * 32 + lane;
+                // this set's running sum: TMEM columns 4 (s / 4) of the lane
+                // quarter, or the scratch
+                const bool in_tmem = s < TMEM_SETS;
+                const unsigned taddr = tbase + (unsigned)(4 * (s >> 2));
+                float4 *pp = in_tmem ? nullptr : ps + (long long)(s - TMEM_SETS) * 32 + lane;
                 if (!last) {
-                    if (h == 0) {
-                        st_f4_hint(ps + col, sum, keep);
-                    } else {
-                        const float4 pv = ld_f4_hint(ps + col, keep);
-                        st_f4_hint(ps + col,
-                                   make_float4((float)((double)pv.x + (double)sum.x),
-                                               (float)((double)pv.y + (double)sum.y),
-                                               (float)((double)pv.z + (double)sum.z),
-                                               (float)((double)pv.w + (double)sum.w)),
-                                   keep);
+                    float4 run = sum;
+                    if (h > 0) {
+                        const float4 pv = in_tmem ? tmem_load4(taddr) : ld_f4_hint(pp, keep);
+                        run = make_float4((float)((double)pv.x + (double)sum.x),
+                                          (float)((double)pv.y + (double)sum.y),
+                                          (float)((double)pv.z + (double)sum.z),
+                                          (float)((double)pv.w + (double)sum.w));
                     }
+                    if (in_tmem)
+                        tmem_store4(taddr, run);
+                    else
+                        st_f4_hint(pp, run, keep);
                     continue;
                 }
+                float4 pv = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (h > 0) pv = in_tmem ? tmem_load4(taddr) : ld_f4_hint(pp, stream_out);
                 const int d = set_frames[col];
                 if (d < 0) continue;
-                float4 pv = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (h > 0) pv = ld_f4_hint(ps + col, stream_out);
                 const double sc = scales[d];
                 const float pr[4] = {pv.x, pv.y, pv.z, pv.w};
                 const float sm[4] = {sum.x, sum.y, sum.z, sum.w};
@@ -511,6 +574,14 @@ k_screen_sets(const float4 *__restrict__ lsl4, int num_rot, const double *__rest
             }
         }
     }
+    // every warp is done with tensor memory; the allocating warp frees it
+    tmem_fence_before();
+    __syncthreads();
+    tmem_fence_after();
+    if (split && warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_slot),
+                     "r"(TMEM_COLS)
+                     : "memory");
 }
 
 // Per column: the screened maximum and first-index argmax row of its frame
@@ -580,7 +651,9 @@ extern "C" int rspi_sets_fill(const unsigned short *entries16, const long long *
 
 extern "C" long long rspi_sets_part_sums_floats(long long n_sets, int n_ctas) {
     if (n_sets <= 0 || n_ctas <= 0) return -1;
-    return (long long)n_ctas * n_sets * 32 * 4;
+    // the sets beyond the tensor-memory store (at least one set's room)
+    const long long extra = n_sets > TMEM_SETS ? n_sets - TMEM_SETS : 1;
+    return (long long)n_ctas * extra * 32 * 4;
 }
 
 extern "C" int rspi_screen_loglike_sets(const float *lslices_sets, long long num_rot,
@@ -598,7 +671,10 @@ extern "C" int rspi_screen_loglike_sets(const float *lslices_sets, long long num
         row_end > 0x7fffffffLL || n_parts < 1 || n_parts > SETS_MAX_PARTS || part_w < 8 ||
         part_w % 8 || ll_stride < n_sets * 32 || warps_per_cta < 1 || warps_per_cta > 32)
         return RSPI_ERR_ARG;
-    if (n_parts > 1 && (!part_sums || part_sums_ctas < 1)) return RSPI_ERR_ARG;
+    // several parts: the part sums' four lane quarters of tensor memory need
+    // a warp in each quarter
+    if (n_parts > 1 && (!part_sums || part_sums_ctas < 1 || warps_per_cta < 4))
+        return RSPI_ERR_ARG;
     if ((reinterpret_cast<uintptr_t>(lslices_sets) & 15) != 0 ||
         (reinterpret_cast<uintptr_t>(entries) & 7) != 0 ||
         (reinterpret_cast<uintptr_t>(part_sums) & 15) != 0 ||

@@ -21,9 +21,10 @@ densely, likelihood as a tensor-core GEMM, ``dense_gemm`` = ``auto`` /
 ``kernel`` (the likelihood kernel: ``sets`` (the screened form's
 default: one lane per frame, 32 frames per warp), ``quad4`` (four frames
 per warp) or ``stream`` for the screened form, ``stream`` (default) or
-``dynamic`` for ``fp64``), ``slice_math`` (``fp64``, the
-default, or ``fp32``: the frame-set kernel's log-slices interpolated and
-logged in FP32 within a bound the candidate threshold covers),
+``dynamic`` for ``fp64``), ``slice_math`` (``fp32``, the
+frame-set kernel's default: its log-slices interpolated and logged in FP32
+within a bound the candidate threshold covers; ``fp64``: computed in FP64,
+stored in FP32, the other kernels' only choice),
 ``screen_delta``
 (default 0: FP64 rescoring of the states that can be the argmax, which is
 what the hard-argmax iteration uses; 20: also every state within 20 nats of
@@ -158,7 +159,7 @@ class EMC():
         self.dense_rescore = config.getboolean('emc', 'dense_rescore', fallback=True)
         self.autotune = config.getboolean('emc', 'autotune', fallback=True)
         self.kernel = config.get('emc', 'kernel', fallback=None) or None
-        self.slice_math = config.get('emc', 'slice_math', fallback='fp64')
+        self.slice_math = config.get('emc', 'slice_math', fallback='').strip() or None
         self.mstep_kind = config.get('emc', 'mstep', fallback='pattern')
         if self.mstep_kind not in ('pattern', 'grid', 'lbfgs', 'grid+lbfgs'):
             raise ValueError('emc:mstep must be pattern, grid, lbfgs or grid+lbfgs')

@@ -236,16 +236,17 @@ class EStep:
     default: frames 32 at a time, one lane per frame, a bank-conflict-free
     step schedule; likelihood columns in set order, ``frame_prob()`` gives
     frame order), ``quad4`` (four frames per warp) or ``stream``; for the
-    FP64 form ``stream`` (default) or ``dynamic``.  ``slice_math='fp32'``
-    (frame-set kernel only) interpolates and logs the slices in FP32 within
-    a bound that the candidate threshold covers.
+    FP64 form ``stream`` (default) or ``dynamic``.  ``slice_math``: ``fp32``
+    (the frame-set kernel's default, for it only) interpolates and logs the
+    slices in FP32 within a bound that the candidate threshold covers;
+    ``fp64`` computes them in FP64 and stores them in FP32.
     """
 
     def __init__(self, photons, size, num_rot, shiftx, shifty, sphere_dia, probmask, bg,
                  form='fp64', states_per_tile=None, warps=32, n_ctas=0,
                  slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel=None,
                  n_modes=1, dense_gemm='auto', dense_rescore=True, screen_parts=None,
-                 slice_math='fp64'):
+                 slice_math=None):
         if form not in ('fp64', 'screen', 'dense'):
             raise ValueError('form must be fp64, screen or dense')
         if kernel is None:   # default likelihood kernel of each form
@@ -255,6 +256,8 @@ class EStep:
         if kernel not in kernels:
             raise ValueError('the %s form takes the kernels %s' % (form, ', '.join(kernels)))
         self.screen_parts = None if screen_parts is None else int(screen_parts)
+        if slice_math is None:
+            slice_math = 'fp32' if kernel == 'sets' else 'fp64'
         if slice_math not in ('fp64', 'fp32'):
             raise ValueError('slice_math must be fp64 or fp32')
         if slice_math == 'fp32' and kernel != 'sets':

@@ -128,8 +128,11 @@ def test_holo_msum_vscale(name):
 @pytest.mark.parametrize('name', GOLDEN_CASES)
 @pytest.mark.parametrize('form', ['fp64', 'screen'])
 def test_rotated_log_slices(name, form):
+    """Row-major rotated log-slices (the slice layout of the streaming
+    kernels; the frame-set layout holds the same values, checked by
+    test_sets_slice_layout_bit_identical) against the oracle."""
     g = load_golden(name)
-    ds, es = _golden_estep(g, form=form)
+    ds, es = _golden_estep(g, form=form, kernel='stream')
     size, num_rot = int(g['size']), int(g['num_rot'])
     sx, sy, dia, _ = golden_states(g)
     es.slices(torch.from_numpy(g['model0']).cuda())

@@ -790,8 +790,10 @@ def run_ours(args):
         'e2e': e2e,
         'plain': plain,
         'parity': parity,
-        'tiling': {'warps_per_cta': es.warps, 'column_parts': es.parts(),
-                   'rows_per_tile': es.tile, 'autotuned': bool(getattr(rec, 'tuning', None)),
+        'tiling': {'warps_per_cta': getattr(es, 'warps', None),
+                   'column_parts': es.parts() if es.form != 'dense' else None,
+                   'rows_per_tile': getattr(es, 'tile', None),
+                   'autotuned': bool(getattr(rec, 'tuning', None)),
                    'tuned_ms_per_row': (rec.tuning[1] if getattr(rec, 'tuning', None)
                                         else None)},
         'form': {'likelihood': args.form, 'kernel': es.kernel,

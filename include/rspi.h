@@ -254,11 +254,14 @@ int rspi_screen_loglike7(const float *lslices, long long p_row, long long num_ro
  * rspi_sets_fill: group_off[last] * 128 16-bit entries (8-byte aligned,
  * prefilled by the caller with any value <= part_w + 7): entry
  * ((g * 32 + lane) * 4 + k) is the local column the lane reads at step
- * 4 (g - g0) + k of its (set, part) range [g0, g1).  At every step the eight
- * lanes of a quarter warp read eight distinct classes (a Birkhoff-von
- * Neumann decomposition of the padded count matrix), real photons first,
- * the zero column part_w + class otherwise.  A schedule that cannot be
- * built sets *err = RSPI_ERR_CAPACITY. */
+ * 4 (g - g0) + k of its (set, part) range [g0, g1).  A quarter warp runs
+ * its own D_q steps (max of its largest frame count and largest class
+ * total), in each of which its eight lanes read eight distinct classes (a
+ * Birkhoff-von Neumann decomposition of the count matrix padded to a
+ * regular one), real photons first, the zero column part_w + class
+ * otherwise; from step D_q on all eight lanes hold 0xffff (idle: the
+ * kernel issues no load for them).  A schedule that cannot be built sets
+ * *err = RSPI_ERR_CAPACITY. */
 int rspi_sets_counts(const unsigned short *entries16, const long long *row_off16,
                      long long n_data, int p_zero, int n_parts, int part_w, int *counts,
                      cudaStream_t stream);
@@ -307,6 +310,11 @@ int rspi_rot_log_slices_sets(const double *holo_pairs, const float *holo_pairs32
  * within 1 s sets *err = RSPI_ERR_TIMEOUT and the kernel returns.  Requires
  * every entry <= part_w + 7 (check with rspi_entries16_check). */
 long long rspi_sets_part_sums_floats(long long n_sets, int n_ctas);
+/* *bad += the entries of entries[0, n) that are neither a staged column
+ * (< part_w + 8) nor the idle mark 0xffff (the check of rspi_sets_fill's
+ * output before the first launch). */
+int rspi_sets_entries_check(const unsigned short *entries, long long n, int part_w, int *bad,
+                            cudaStream_t stream);
 int rspi_screen_loglike_sets(const float *lslices_sets, long long num_rot, const double *init,
                              const double *scales, const unsigned short *entries,
                              const long long *group_off, const int *set_frames,

@@ -38,6 +38,7 @@ namespace {
 constexpr int SMEM_LIMIT = 227 * 1024;
 constexpr int SETS_MAX_PARTS = 4;
 constexpr int SETS_MAX_PERMS = 64;   // terms of one decomposition (each zeroes a cell)
+constexpr unsigned SETS_IDLE = 0xffffu;   // entry of a step in which the lane's quarter warp is idle
 constexpr int BUILD_WARPS = 4;
 constexpr long long WAIT_NS = 1000000000LL;   // bound of every mbarrier wait (1 s)
 
@@ -154,11 +155,15 @@ __device__ bool perfect_matching(const int (&m)[8][8], int (&col_of)[8]) {
 }
 
 // One warp per (set, part).  Lane 8 p of the warp decomposes quarter warp
-// p's padded count matrix into permutations (shared memory: packed classes
-// of the eight lanes, 3 bits each in 4-bit fields, the multiplicity and the
-// first step of each); then every lane places its frame's photons of the
-// part, the k-th photon of class c at the k-th step in which the lane reads
-// class c, and the zero column part_w + c at that class's remaining steps.
+// p's count matrix, padded to a regular matrix of its own step count D_p
+// (the larger of its fullest frame and its fullest class), into
+// permutations (shared memory: packed classes of the eight lanes, 3 bits
+// each in 4-bit fields, the multiplicity and the first step of each); then
+// every lane places its frame's photons of the part, the k-th photon of
+// class c at the k-th step in which the lane reads class c, the zero column
+// part_w + c at that class's remaining steps below D_p, and SETS_IDLE at
+// the set's steps from D_p on, where the whole quarter warp is idle (its
+// gathers are not issued, so they cost no shared-memory wavefront).
 __global__ void __launch_bounds__(BUILD_WARPS * 32)
 k_sets_fill(const unsigned short *__restrict__ ent16, const long long *__restrict__ row_off16,
             int p_zero, int n_parts, int part_w, const int *__restrict__ counts,
@@ -169,6 +174,7 @@ k_sets_fill(const unsigned short *__restrict__ ent16, const long long *__restric
     __shared__ int mult[BUILD_WARPS][4][SETS_MAX_PERMS];
     __shared__ int start[BUILD_WARPS][4][SETS_MAX_PERMS];
     __shared__ int n_perm[BUILD_WARPS][4];
+    __shared__ int n_step[BUILD_WARPS][4];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int p = lane >> 3, f = lane & 7;
     const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -191,18 +197,20 @@ k_sets_fill(const unsigned short *__restrict__ ent16, const long long *__restric
                     cols[c] += m[ff][c];
                 }
             }
-            bool ok = true;
-            for (int k = 0; k < 8; ++k) ok = ok && rows[k] <= steps && cols[k] <= steps;
-            // pad to a regular matrix: every row and column sums to `steps`
+            // this quarter warp's step count (Koenig: the fewest possible)
+            int dq = 0;
+            for (int k = 0; k < 8; ++k) dq = max(dq, max(rows[k], cols[k]));
+            bool ok = dq <= steps;
+            // pad to a regular matrix: every row and column sums to dq
             for (int ff = 0; ff < 8 && ok; ++ff)
                 for (int c = 0; c < 8; ++c) {
-                    const int t = min(steps - rows[ff], steps - cols[c]);
+                    const int t = min(dq - rows[ff], dq - cols[c]);
                     m[ff][c] += t;
                     rows[ff] += t;
                     cols[c] += t;
                 }
             int np = 0, done = 0;
-            while (ok && done < steps) {
+            while (ok && done < dq) {
                 int col_of[8];
                 if (np == SETS_MAX_PERMS || !perfect_matching(m, col_of)) {
                     ok = false;
@@ -224,11 +232,14 @@ k_sets_fill(const unsigned short *__restrict__ ent16, const long long *__restric
             if (!ok) {
                 rspi_flag(err, RSPI_ERR_CAPACITY);
                 np = 0;
+                done = 0;
             }
             n_perm[w][p] = np;
+            n_step[w][p] = done;
         }
         __syncwarp();
         const int np = n_perm[w][p];
+        const int dq = n_step[w][p];
         const int d = set_frames[s * 32 + lane];
         // per class: current permutation index and offset within its run
         int ic[8], oc[8];
@@ -269,6 +280,7 @@ k_sets_fill(const unsigned short *__restrict__ ent16, const long long *__restric
         for (int c = 0; c < 8 && np > 0; ++c)
             for (int st = next_step(c); st >= 0; st = next_step(c))
                 put(st, (unsigned)(part_w + c));
+        for (int st = dq; st < steps; ++st) put(st, SETS_IDLE);
         __syncwarp();
     }
 }
@@ -341,13 +353,22 @@ __device__ __forceinline__ float4 f4_add(float4 a, float4 b) {
     return make_float4(lo.x, lo.y, hi.x, hi.y);
 }
 
+// One step's value: the four rows at local column q, or zeros (no shared
+// load) at an idle step.
+__device__ __forceinline__ float4 step_value(const unsigned char *tile, unsigned q) {
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (q != SETS_IDLE) v = *reinterpret_cast<const float4 *>(tile + (q << 4));
+    return v;
+}
+
 // The four photons of one group of a lane, summed as a tree of depth two:
-// (v0 + v1) + (v2 + v3), four rows each.
+// (v0 + v1) + (v2 + v3), four rows each; idle steps add zeros, as the zero
+// columns do.
 __device__ __forceinline__ float4 group_sum(const unsigned char *tile, uint2 e) {
-    const float4 v0 = *reinterpret_cast<const float4 *>(tile + ((e.x & 0xffffu) << 4));
-    const float4 v1 = *reinterpret_cast<const float4 *>(tile + ((e.x >> 16) << 4));
-    const float4 v2 = *reinterpret_cast<const float4 *>(tile + ((e.y & 0xffffu) << 4));
-    const float4 v3 = *reinterpret_cast<const float4 *>(tile + ((e.y >> 16) << 4));
+    const float4 v0 = step_value(tile, e.x & 0xffffu);
+    const float4 v1 = step_value(tile, e.x >> 16);
+    const float4 v2 = step_value(tile, e.y & 0xffffu);
+    const float4 v3 = step_value(tile, e.y >> 16);
     return f4_add(f4_add(v0, v1), f4_add(v2, v3));
 }
 
@@ -584,6 +605,19 @@ k_screen_sets(const float4 *__restrict__ lsl4, int num_rot, const double *__rest
                      : "memory");
 }
 
+// bad += entries that are neither a staged column (< part_w + 8) nor idle.
+__global__ void k_sets_check(const unsigned short *__restrict__ e, long long n, int part_w,
+                             int *__restrict__ bad) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    int cnt = 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const unsigned v = e[i];
+        cnt += v >= (unsigned)(part_w + 8) && v != SETS_IDLE;
+    }
+    cnt = warp_sum(cnt);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(bad, cnt);
+}
+
 // Per column: the screened maximum and first-index argmax row of its frame
 // from the key, into frame order; the key is reset for the next pass.
 __global__ void k_frame_max_finalize(unsigned long long *__restrict__ frame_max,
@@ -646,6 +680,13 @@ extern "C" int rspi_sets_fill(const unsigned short *entries16, const long long *
     k_sets_fill<<<rspi_blocks(n_sets * n_parts * 32, BUILD_WARPS * 32), BUILD_WARPS * 32, 0,
                   stream>>>(entries16, row_off16, p_zero, n_parts, part_w, counts, set_frames,
                             n_sets, group_off, entries, err);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_sets_entries_check(const unsigned short *entries, long long n, int part_w,
+                                       int *bad, cudaStream_t stream) {
+    if (!entries || !bad || n <= 0 || part_w < 8 || part_w + 8 > 0xffff) return RSPI_ERR_ARG;
+    k_sets_check<<<rspi_blocks(n, 256), 256, 0, stream>>>(entries, n, part_w, bad);
     RSPI_RETURN_LAUNCH();
 }
 

@@ -576,10 +576,10 @@ class EStep:
              ptr(counts), ptr(set_frames), n_sets, ptr(goff), ptr(entries), ptr(self.ph.err.t),
              s)
         self.ph.err.check('frame-set entries')
-        mx = torch.zeros(1, dtype=_i32, device=dev)
-        call('rspi_entries16_check', ptr(entries), max(1, total) * 128, ptr(mx), s)
-        if int(mx.item()) > part_w + 7:
-            raise RuntimeError('frame-set entry %d outside the staged part' % int(mx.item()))
+        bad = torch.zeros(1, dtype=_i32, device=dev)
+        call('rspi_sets_entries_check', ptr(entries), max(1, total) * 128, part_w, ptr(bad), s)
+        if int(bad.item()) != 0:
+            raise RuntimeError('%d frame-set entries outside the staged part' % int(bad.item()))
         # each frame's FP32 summation length for the candidate threshold:
         # ceil(G / 2) accumulator steps of its set's largest part (the +3 of
         # the group tree and the final add are within the threshold's +8)

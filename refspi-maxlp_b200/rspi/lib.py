@@ -38,6 +38,7 @@ SIGNATURES = {
     'rspi_log2_error_max': (I, [F, F, P, P]),
     'rspi_maxlp_pixel_frames': (I, [I, L, P, L] + [P] * 7 + [L, P, P, P, P, P, P]),
     'rspi_maxlp_pixel_values': (I, [P, L, P, P, L, I, D, P, P, P]),
+    'rspi_sets_entries_check': (I, [P, L, I, P, P]),
     'rspi_sim_views': (I, [P, P, I, L, L, P, P, P, P, D, D, D, I, P, P, P]),
     'rspi_sim_counts': (I, [P, L, L, P, P, I, ctypes.c_ulonglong, P, P, P, P]),
     'rspi_sim_poisson': (I, [P, L, ctypes.c_ulonglong, ctypes.c_ulonglong, P, P, P]),
@@ -145,7 +146,7 @@ KERNELS_PER_CALL = {
     'rspi_screen_candidates_cols': 4, 'rspi_rescore_cols': 5, 'rspi_nll': 2, 'rspi_screen_candidates_noalloc': 3, 'rspi_merge_coverage': 1, 'rspi_merge': 2,
     'rspi_dense_frames': 1, 'rspi_rot_log_split': 1, 'rspi_dense_loglike': 1,
     'rspi_maxlp_grid': 2, 'rspi_dense_frames_u8': 1, 'rspi_rot_log_fixed': 1,
-    'rspi_dense_loglike_i8': 1, 'rspi_sim_views': 1, 'rspi_sim_counts': 1,
+    'rspi_dense_loglike_i8': 1, 'rspi_sets_entries_check': 1, 'rspi_sim_views': 1, 'rspi_sim_counts': 1,
     'rspi_sim_poisson': 1, 'rspi_sim_sparse_counts': 1, 'rspi_sim_sparse_fill': 1,
 }
 launch_count = 0

@@ -77,6 +77,9 @@ def parse_args():
                          'L-BFGS through the adjoint after its ring pass')
     ap.add_argument('--slice-math', default=None, choices=['fp64', 'fp32'],
                     help='arithmetic of the frame-set kernel\'s log-slices')
+    ap.add_argument('--merge', action='store_true',
+                    help='each iteration also merges the posterior-weighted intensities '
+                         '(row a10; rescoring window 20 nats)')
     ap.add_argument('--no-autotune', action='store_true',
                     help='keep the likelihood kernel\'s default tiling')
     ap.add_argument('--no-phaser-screen', action='store_true',
@@ -255,7 +258,7 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
 
 
 def write_inputs(tmp, w, data, form, slice_gb=8., screen_delta=None, kernel=None, mstep=None,
-                 autotune=True, rank=None, slice_math=None):
+                 autotune=True, rank=None, slice_math=None, merge=False):
     from rspi.photonfile import write_photons
     os.makedirs(os.path.join(tmp, 'out'), exist_ok=True)
     name = 'photons.npz' if rank is None else 'photons_%d.npz' % rank
@@ -277,6 +280,8 @@ def write_inputs(tmp, w, data, form, slice_gb=8., screen_delta=None, kernel=None
             f.write('mstep = %s\n' % mstep)
         if slice_math:
             f.write('slice_math = %s\n' % slice_math)
+        if merge:
+            f.write('merge = true\n')
         f.write('autotune = %s\n' % bool(autotune))
     return cfg
 
@@ -601,7 +606,8 @@ def run_ours(args):
     cfgfile = write_inputs(tmp, w, data, args.form, args.slice_gb, args.screen_delta,
                            args.kernel if args.form != 'dense' else None, args.mstep,
                            not args.no_autotune and not args.warps,
-                           rank=rank if world > 1 else None, slice_math=args.slice_math)
+                           rank=rank if world > 1 else None, slice_math=args.slice_math,
+                           merge=args.merge)
     from emc import EMC
     import contextlib
     import io
@@ -648,6 +654,22 @@ def run_ours(args):
     ll_ms = sum(a.elapsed_time(b) for a, b, _ in es.ll_events)
     ll_launches = len(es.ll_events)
     es.ll_events = None
+    merge_info = None
+    if rec.merger is not None:
+        # the merge alone (row a10): CUDA events around one more merge of the
+        # same E-step's posteriors
+        es.reduce()
+        m0 = torch.cuda.Event(enable_timing=True)
+        m1 = torch.cuda.Event(enable_timing=True)
+        m0.record(stream)
+        rec.merger.run()
+        m1.record(stream)
+        torch.cuda.synchronize()
+        n_pairs = int(es.cand_off[rec.dset.num_data].item()) if es.form != 'fp64' else None
+        merge_info = {'ms': m0.elapsed_time(m1), 'posterior_pairs': n_pairs,
+                      'p_min': rec.merger.p_min,
+                      'note': 'posterior-weighted intensities of every (shift, diameter) '
+                              'state, included in ms_per_step'}
     rec.dset.photons.err.check('bench')
     if world > 1:
         ms = max_over_ranks(ms, dev)
@@ -790,6 +812,7 @@ def run_ours(args):
         'e2e': e2e,
         'plain': plain,
         'parity': parity,
+        'merge': merge_info,
         'tiling': {'warps_per_cta': getattr(es, 'warps', None),
                    'column_parts': es.parts() if es.form != 'dense' else None,
                    'rows_per_tile': getattr(es, 'tile', None),

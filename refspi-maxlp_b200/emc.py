@@ -25,6 +25,10 @@ per warp) or ``stream`` for the screened form, ``stream`` (default) or
 frame-set kernel's default: its log-slices interpolated and logged in FP32
 within a bound the candidate threshold covers; ``fp64``: computed in FP64,
 stored in FP32, the other kernels' only choice),
+``merge`` (default false: true adds each iteration's posterior-weighted
+intensities of every (shift, diameter) state, the reference's unused
+``merge_all`` / ``slice_merge`` kernels (kernels.cu:84-152), to
+output_%03d.h5 as ``intens``; ``screen_delta`` then defaults to 20),
 ``screen_delta``
 (default 0: FP64 rescoring of the states that can be the argmax, which is
 what the hard-argmax iteration uses; 20: also every state within 20 nats of
@@ -123,6 +127,13 @@ class EMC():
                            n_modes=self.num_modes, dense_gemm=self.dense_gemm,
                            dense_rescore=self.dense_rescore, kernel=self.kernel,
                            slice_math=self.slice_math)
+        self.merger = None
+        self.intens = None
+        if self.merge_intens:
+            if self.num_proc > 1:
+                raise ValueError('emc:merge runs on one GPU')
+            from rspi.device import Merge
+            self.merger = Merge(self.estep, p_min=P_MIN)
         self.state_vals = torch.from_numpy(self._state_values).to(self.device)
         self.phaser_rot = torch.from_numpy(geometry.phaser_rotation_table(
             np.arange(self.num_rot) * np.pi / self.num_rot)).to(self.device)
@@ -148,7 +159,13 @@ class EMC():
         self.form = config.get('emc', 'form', fallback='screen')
         if self.form not in ('fp64', 'screen', 'dense'):
             raise ValueError('emc:form must be fp64, screen or dense')
-        self.screen_delta = config.getfloat('emc', 'screen_delta', fallback=0.)
+        # merge: the posterior-weighted intensities of every (shift, diameter)
+        # state (a10), written as output_%03d.h5's ``intens``; the posteriors
+        # above P_MIN need FP64 values within 13.8 nats of each maximum, so the
+        # rescoring window defaults to 20 nats then
+        self.merge_intens = config.getboolean('emc', 'merge', fallback=False)
+        self.screen_delta = config.getfloat('emc', 'screen_delta',
+                                            fallback=20. if self.merge_intens else 0.)
         self.states_per_tile = config.getint('emc', 'states_per_tile', fallback=0) or None
         self.warps_per_cta = config.getint('emc', 'warps_per_cta', fallback=32)
         self.phaser_iter = config.getint('emc', 'phaser_iter', fallback=10)
@@ -220,6 +237,8 @@ class EMC():
             self._graph = None
             self._dmodel.copy_(torch.from_numpy(np.asarray(self.model, dtype=np.complex128).ravel()))
             self._device_step()
+            if self.merger is not None:
+                self.intens = self.merger.run()
             self._host_rmax.copy_(self.estep.rmax)
             self._host_model.copy_(self._dmodel)
         err.check('EMC iteration')
@@ -232,7 +251,7 @@ class EMC():
             self.rmax = self._host_rmax.numpy().copy()
         self.model = self._host_model.numpy().copy().reshape(self._model_shape())
         if self.rank == 0:
-            self.save_output(self.model, iternum)
+            self.save_output(self.model, iternum, intens=self.intens)
 
     def _device_step(self):
         '''One iteration on device buffers: E-step, reduction, M-step.'''
@@ -275,7 +294,14 @@ class EMC():
     def device_step(self):
         '''The iteration on the device model buffer ``_dmodel``: eager the
         first time (which sizes every buffer and checks capacities), then
-        captured once into a CUDA graph and replayed.'''
+        captured once into a CUDA graph and replayed; with ``merge`` the
+        posterior-weighted intensities of the iteration's E-step follow
+        (eagerly: the merge sizes its pair buffers on the host).'''
+        self._iteration()
+        if self.merger is not None:
+            self.intens = self.merger.run()
+
+    def _iteration(self):
         if not self._tuned:
             # the likelihood kernel's tiling, timed on this model's slices
             from rspi import autotune

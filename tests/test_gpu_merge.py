@@ -73,3 +73,32 @@ def test_coverage_is_rotation_adjoint_of_ones():
         wts = np.zeros(size * size)
         E.slice_merge(np.ones(size * size), j * np.pi / num_rot, size, model, wts)
         np.testing.assert_allclose(cov[j].cpu().numpy(), model, rtol=1e-13, atol=1e-15)
+
+
+@pytest.mark.parametrize('graph', [False, True])
+def test_emc_merge_option_writes_intens(tmp_path, graph):
+    """[emc] merge = true: each iteration's posterior-weighted intensities
+    (from the E-step on the iteration's start model, the rescoring window
+    defaulting to 20 nats) equal the oracle's merge of the golden posteriors
+    and are written to output_%03d.h5 as intens; graph replays give the
+    eager values."""
+    import os
+    from emc import EMC
+    from helpers import write_case
+    from rspi import h5lite
+    g = load_golden('case_b')
+    cfg = write_case(str(tmp_path), g, extra='merge = true\ncuda_graph = %s\n' % graph)
+    rec = EMC(cfg)
+    assert rec.screen_delta == 20.
+    rec.model = g['model_in_1'].copy()
+    ds = golden_dataset(g)
+    size, num_rot = int(g['size']), int(g['num_rot'])
+    for it in (1, 2):
+        rec.run_iteration(it)
+        _, post = E.posterior(g['prob_%d' % it])
+        want, _, _ = E.merge(post, ds, E.get_scales(ds, bool(g['need_scaling'])),
+                             rec.estep.n_states0, num_rot, size)
+        got = rec.intens.cpu().numpy()
+        np.testing.assert_allclose(got, want, rtol=1e-9, atol=1e-12)
+        out = h5lite.read_datasets(os.path.join(str(tmp_path), 'out', 'output_%03d.h5' % it))
+        assert np.array_equal(out['intens'], got)

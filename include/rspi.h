@@ -247,10 +247,12 @@ int rspi_screen_loglike7(const float *lslices, long long p_row, long long num_ro
  * rspi_sets_counts: counts[d * 32 + 8 h + c] = frame d's photons in part h of
  * local column class c (local column mod 8), from the 16-bit entries of
  * rspi_ll16_entry_fill (p_zero = their zero column).
- * rspi_sets_steps: groups[h * n_sets + s] = ceil(D / 4), D = the most steps
- * any quarter warp of set s needs in part h: max(largest frame count,
- * largest class total over its eight frames) (Koenig's edge-colouring bound).
- * The caller scans the groups part-major into group_off[n_parts*n_sets + 1].
+ * rspi_sets_steps: quarter_groups[(h * n_sets + s) * 4 + p] (NULL: not
+ * written) = ceil(D_p / 4), D_p the fewest steps quarter warp p of set s
+ * needs in part h: max(largest frame count, largest class total over its
+ * eight frames) (Koenig's edge-colouring bound); groups[h * n_sets + s] =
+ * the largest of the four.  The caller scans the groups part-major into
+ * group_off[n_parts*n_sets + 1].
  * rspi_sets_fill: group_off[last] * 128 16-bit entries (8-byte aligned,
  * prefilled by the caller with any value <= part_w + 7): entry
  * ((g * 32 + lane) * 4 + k) is the local column the lane reads at step
@@ -259,14 +261,15 @@ int rspi_screen_loglike7(const float *lslices, long long p_row, long long num_ro
  * total), in each of which its eight lanes read eight distinct classes (a
  * Birkhoff-von Neumann decomposition of the count matrix padded to a
  * regular one), real photons first, the zero column part_w + class
- * otherwise; from step D_q on all eight lanes hold 0xffff (idle: the
- * kernel issues no load for them).  A schedule that cannot be built sets
+ * otherwise; from step D_q on each lane holds the zero column of its own
+ * class (rspi_screen_loglike_sets skips those groups of the quarter warp
+ * when given quarter_groups).  A schedule that cannot be built sets
  * *err = RSPI_ERR_CAPACITY. */
 int rspi_sets_counts(const unsigned short *entries16, const long long *row_off16,
                      long long n_data, int p_zero, int n_parts, int part_w, int *counts,
                      cudaStream_t stream);
 int rspi_sets_steps(const int *counts, const int *set_frames, long long n_sets, int n_parts,
-                    int *groups, cudaStream_t stream);
+                    int *groups, int *quarter_groups, cudaStream_t stream);
 int rspi_sets_fill(const unsigned short *entries16, const long long *row_off16, int p_zero,
                    int n_parts, int part_w, const int *counts, const int *set_frames,
                    long long n_sets, const long long *group_off, unsigned short *entries,
@@ -302,22 +305,26 @@ int rspi_rot_log_slices_sets(const double *holo_pairs, const float *holo_pairs32
  * tensor memory for the first 512 sets (each CTA allocates all 512 TMEM
  * columns and frees them before it ends; warps_per_cta >= 4) and in
  * part_sums for the others (rspi_sets_part_sums_floats(n_sets,
- * part_sums_ctas) floats, 16-byte aligned; at most part_sums_ctas CTAs run).  LL32 of row r, frame
- * set_frames[c] goes to ll[(r - row_begin) * ll_stride + c] (ll_stride >=
- * n_sets * 32), and frame_max[c] (zero before the first launch of a pass)
- * takes the unsigned maximum of an order-preserving (value, row) key, read
- * and reset by rspi_frame_max_finalize.  A bulk copy that does not complete
- * within 1 s sets *err = RSPI_ERR_TIMEOUT and the kernel returns.  Requires
- * every entry <= part_w + 7 (check with rspi_entries16_check). */
+ * part_sums_ctas) floats, 16-byte aligned; at most part_sums_ctas CTAs
+ * run).  With quarter_groups (rspi_sets_steps; NULL: every quarter warp
+ * runs its set's groups) a quarter warp stops gathering after its own
+ * groups.  LL32 of row r, frame set_frames[c] goes to
+ * ll[(r - row_begin) * ll_stride + c] (ll_stride >= n_sets * 32), and
+ * frame_max[c] (zero before the first launch of a pass) takes the unsigned
+ * maximum of an order-preserving (value, row) key, read and reset by
+ * rspi_frame_max_finalize.  A bulk copy that does not complete within 1 s
+ * sets *err = RSPI_ERR_TIMEOUT and the kernel returns.  Requires every entry
+ * <= part_w + 7 (check with rspi_sets_entries_check). */
 long long rspi_sets_part_sums_floats(long long n_sets, int n_ctas);
-/* *bad += the entries of entries[0, n) that are neither a staged column
- * (< part_w + 8) nor the idle mark 0xffff (the check of rspi_sets_fill's
- * output before the first launch). */
+/* *bad += the entries of entries[0, n) that are not a staged column
+ * (< part_w + 8): the check of rspi_sets_fill's output before the first
+ * launch. */
 int rspi_sets_entries_check(const unsigned short *entries, long long n, int part_w, int *bad,
                             cudaStream_t stream);
 int rspi_screen_loglike_sets(const float *lslices_sets, long long num_rot, const double *init,
                              const double *scales, const unsigned short *entries,
-                             const long long *group_off, const int *set_frames,
+                             const long long *group_off, const int *quarter_groups,
+                             const int *set_frames,
                              long long n_sets, int n_parts, int part_w, long long row_begin,
                              long long row_end, float *ll, long long ll_stride,
                              float *part_sums, int part_sums_ctas,

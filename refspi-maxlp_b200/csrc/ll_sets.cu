@@ -38,7 +38,6 @@ namespace {
 constexpr int SMEM_LIMIT = 227 * 1024;
 constexpr int SETS_MAX_PARTS = 4;
 constexpr int SETS_MAX_PERMS = 64;   // terms of one decomposition (each zeroes a cell)
-constexpr unsigned SETS_IDLE = 0xffffu;   // entry of a step in which the lane's quarter warp is idle
 constexpr int BUILD_WARPS = 4;
 constexpr long long WAIT_NS = 1000000000LL;   // bound of every mbarrier wait (1 s)
 
@@ -79,18 +78,21 @@ k_sets_counts(const unsigned short *__restrict__ ent16, const long long *__restr
     }
 }
 
-// groups[h * n_sets + s] = ceil(D / 4), D = the largest over the set's four
-// quarter warps of max(largest frame total, largest class total) in part h.
+// quarter_groups[(h * n_sets + s) * 4 + p] = ceil(D_p / 4), D_p = max(largest
+// frame total, largest class total) of quarter warp p of set s in part h;
+// groups[h * n_sets + s] = the largest of the four.
 __global__ void k_sets_steps(const int *__restrict__ counts, const int *__restrict__ set_frames,
-                             long long n_sets, int n_parts, int *__restrict__ groups) {
+                             long long n_sets, int n_parts, int *__restrict__ groups,
+                             int *__restrict__ quarter_groups) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n_sets * n_parts;
          i += stride) {
         const int h = (int)(i / n_sets);
         const long long s = i - (long long)h * n_sets;
-        int dmax = 0;
+        int gmax = 0;
         for (int p = 0; p < 4; ++p) {
             int col[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            int dq = 0;
             for (int f = 0; f < 8; ++f) {
                 const int d = set_frames[s * 32 + 8 * p + f];
                 if (d < 0) continue;
@@ -101,12 +103,15 @@ __global__ void k_sets_steps(const int *__restrict__ counts, const int *__restri
                     row += v;
                     col[c] += v;
                 }
-                dmax = max(dmax, row);
+                dq = max(dq, row);
             }
 #pragma unroll
-            for (int c = 0; c < 8; ++c) dmax = max(dmax, col[c]);
+            for (int c = 0; c < 8; ++c) dq = max(dq, col[c]);
+            const int gq = (dq + 3) / 4;
+            if (quarter_groups) quarter_groups[i * 4 + p] = gq;
+            gmax = max(gmax, gq);
         }
-        groups[i] = (dmax + 3) / 4;
+        groups[i] = gmax;
     }
 }
 
@@ -161,9 +166,9 @@ __device__ bool perfect_matching(const int (&m)[8][8], int (&col_of)[8]) {
 // each in 4-bit fields, the multiplicity and the first step of each); then
 // every lane places its frame's photons of the part, the k-th photon of
 // class c at the k-th step in which the lane reads class c, the zero column
-// part_w + c at that class's remaining steps below D_p, and SETS_IDLE at
-// the set's steps from D_p on, where the whole quarter warp is idle (its
-// gathers are not issued, so they cost no shared-memory wavefront).
+// part_w + c at that class's remaining steps below D_p, and from D_p on
+// (steps the kernel skips after group ceil(D_p / 4) of the quarter warp)
+// the zero column of its own class f.
 __global__ void __launch_bounds__(BUILD_WARPS * 32)
 k_sets_fill(const unsigned short *__restrict__ ent16, const long long *__restrict__ row_off16,
             int p_zero, int n_parts, int part_w, const int *__restrict__ counts,
@@ -280,7 +285,7 @@ k_sets_fill(const unsigned short *__restrict__ ent16, const long long *__restric
         for (int c = 0; c < 8 && np > 0; ++c)
             for (int st = next_step(c); st >= 0; st = next_step(c))
                 put(st, (unsigned)(part_w + c));
-        for (int st = dq; st < steps; ++st) put(st, SETS_IDLE);
+        for (int st = dq; st < steps; ++st) put(st, (unsigned)(part_w + f));
         __syncwarp();
     }
 }
@@ -353,22 +358,13 @@ __device__ __forceinline__ float4 f4_add(float4 a, float4 b) {
     return make_float4(lo.x, lo.y, hi.x, hi.y);
 }
 
-// One step's value: the four rows at local column q, or zeros (no shared
-// load) at an idle step.
-__device__ __forceinline__ float4 step_value(const unsigned char *tile, unsigned q) {
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (q != SETS_IDLE) v = *reinterpret_cast<const float4 *>(tile + (q << 4));
-    return v;
-}
-
 // The four photons of one group of a lane, summed as a tree of depth two:
-// (v0 + v1) + (v2 + v3), four rows each; idle steps add zeros, as the zero
-// columns do.
+// (v0 + v1) + (v2 + v3), four rows each.
 __device__ __forceinline__ float4 group_sum(const unsigned char *tile, uint2 e) {
-    const float4 v0 = step_value(tile, e.x & 0xffffu);
-    const float4 v1 = step_value(tile, e.x >> 16);
-    const float4 v2 = step_value(tile, e.y & 0xffffu);
-    const float4 v3 = step_value(tile, e.y >> 16);
+    const float4 v0 = *reinterpret_cast<const float4 *>(tile + ((e.x & 0xffffu) << 4));
+    const float4 v1 = *reinterpret_cast<const float4 *>(tile + ((e.x >> 16) << 4));
+    const float4 v2 = *reinterpret_cast<const float4 *>(tile + ((e.y & 0xffffu) << 4));
+    const float4 v3 = *reinterpret_cast<const float4 *>(tile + ((e.y >> 16) << 4));
     return f4_add(f4_add(v0, v1), f4_add(v2, v3));
 }
 
@@ -420,10 +416,11 @@ template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 1)
 k_screen_sets(const float4 *__restrict__ lsl4, int num_rot, const double *__restrict__ init,
               const double *__restrict__ scales, const uint2 *__restrict__ groups,
-              const long long *__restrict__ goff, const int *__restrict__ set_frames,
-              int n_sets, int n_parts, int part_w, long long row_begin, long long row_end,
-              float *__restrict__ ll, long long ll_stride, float4 *part_sums,
-              unsigned long long *__restrict__ frame_max, int *err) {
+              const long long *__restrict__ goff, const int *__restrict__ qgroups,
+              const int *__restrict__ set_frames, int n_sets, int n_parts, int part_w,
+              long long row_begin, long long row_end, float *__restrict__ ll,
+              long long ll_stride, float4 *part_sums, unsigned long long *__restrict__ frame_max,
+              int *err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) unsigned long long mbar;
     __shared__ int next_set[4];
@@ -538,20 +535,23 @@ k_screen_sets(const float4 *__restrict__ lsl4, int num_rot, const double *__rest
                 if (s >= n_sets) break;
                 const long long gi = (long long)h * n_sets + s;
                 const long long g0 = goff[gi], g1 = goff[gi + 1];
+                // this lane's quarter warp stops after its own groups: its
+                // later gathers are not issued (no shared-memory wavefront)
+                const long long ge = qgroups ? g0 + qgroups[gi * 4 + (lane >> 3)] : g1;
                 float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0;
                 const uint2 *gp = groups + g0 * 32 + lane;
                 long long g = g0;
-                uint2 c0 = g < g1 ? ld_entries(gp, keep) : make_uint2(0, 0);
-                uint2 c1 = g + 1 < g1 ? ld_entries(gp + 32, keep) : make_uint2(0, 0);
+                uint2 c0 = g < ge ? ld_entries(gp, keep) : make_uint2(0, 0);
+                uint2 c1 = g + 1 < ge ? ld_entries(gp + 32, keep) : make_uint2(0, 0);
                 for (; g + 1 < g1; g += 2, gp += 64) {
-                    const uint2 n0 = g + 2 < g1 ? ld_entries(gp + 64, keep) : make_uint2(0, 0);
-                    const uint2 n1 = g + 3 < g1 ? ld_entries(gp + 96, keep) : make_uint2(0, 0);
-                    a0 = f4_add(a0, group_sum(smem_raw, c0));
-                    a1 = f4_add(a1, group_sum(smem_raw, c1));
+                    const uint2 n0 = g + 2 < ge ? ld_entries(gp + 64, keep) : make_uint2(0, 0);
+                    const uint2 n1 = g + 3 < ge ? ld_entries(gp + 96, keep) : make_uint2(0, 0);
+                    if (g < ge) a0 = f4_add(a0, group_sum(smem_raw, c0));
+                    if (g + 1 < ge) a1 = f4_add(a1, group_sum(smem_raw, c1));
                     c0 = n0;
                     c1 = n1;
                 }
-                if (g < g1) a0 = f4_add(a0, group_sum(smem_raw, c0));
+                if (g < ge) a0 = f4_add(a0, group_sum(smem_raw, c0));
                 const float4 sum = f4_add(a0, a1);
                 const int col = s * 32 + lane;
                 // this set's running sum: TMEM columns 4 (s / 4) of the lane
@@ -605,15 +605,13 @@ k_screen_sets(const float4 *__restrict__ lsl4, int num_rot, const double *__rest
                      : "memory");
 }
 
-// bad += entries that are neither a staged column (< part_w + 8) nor idle.
+// bad += entries that are not a staged column (< part_w + 8).
 __global__ void k_sets_check(const unsigned short *__restrict__ e, long long n, int part_w,
                              int *__restrict__ bad) {
     const long long stride = (long long)gridDim.x * blockDim.x;
     int cnt = 0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const unsigned v = e[i];
-        cnt += v >= (unsigned)(part_w + 8) && v != SETS_IDLE;
-    }
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        cnt += (unsigned)e[i] >= (unsigned)(part_w + 8);
     cnt = warp_sum(cnt);
     if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(bad, cnt);
 }
@@ -658,12 +656,13 @@ extern "C" int rspi_sets_counts(const unsigned short *entries16, const long long
 }
 
 extern "C" int rspi_sets_steps(const int *counts, const int *set_frames, long long n_sets,
-                               int n_parts, int *groups, cudaStream_t stream) {
+                               int n_parts, int *groups, int *quarter_groups,
+                               cudaStream_t stream) {
     if (!counts || !set_frames || !groups || n_sets <= 0 || n_sets > 0x3ffffffLL ||
         n_parts < 1 || n_parts > SETS_MAX_PARTS)
         return RSPI_ERR_ARG;
-    k_sets_steps<<<rspi_blocks(n_sets * n_parts, 256), 256, 0, stream>>>(counts, set_frames,
-                                                                         n_sets, n_parts, groups);
+    k_sets_steps<<<rspi_blocks(n_sets * n_parts, 256), 256, 0, stream>>>(
+        counts, set_frames, n_sets, n_parts, groups, quarter_groups);
     RSPI_RETURN_LAUNCH();
 }
 
@@ -700,7 +699,8 @@ extern "C" long long rspi_sets_part_sums_floats(long long n_sets, int n_ctas) {
 extern "C" int rspi_screen_loglike_sets(const float *lslices_sets, long long num_rot,
                                         const double *init, const double *scales,
                                         const unsigned short *entries, const long long *group_off,
-                                        const int *set_frames, long long n_sets, int n_parts,
+                                        const int *quarter_groups, const int *set_frames,
+                                        long long n_sets, int n_parts,
                                         int part_w, long long row_begin, long long row_end,
                                         float *ll, long long ll_stride, float *part_sums,
                                         int part_sums_ctas, unsigned long long *frame_max,
@@ -735,15 +735,15 @@ extern "C" int rspi_screen_loglike_sets(const float *lslices_sets, long long num
         static RspiSmemOptIn optin;
         if (!rspi_smem_optin((const void *)k_screen_sets<512>, smem, optin)) return RSPI_ERR_CUDA;
         k_screen_sets<512><<<n_ctas, warps_per_cta * 32, smem, stream>>>(
-            src, (int)num_rot, init, scales, ent, group_off, set_frames, (int)n_sets, n_parts,
-            part_w, row_begin, row_end, ll, ll_stride, ps, frame_max, err);
+            src, (int)num_rot, init, scales, ent, group_off, quarter_groups, set_frames,
+            (int)n_sets, n_parts, part_w, row_begin, row_end, ll, ll_stride, ps, frame_max, err);
     } else {
         static RspiSmemOptIn optin;
         if (!rspi_smem_optin((const void *)k_screen_sets<1024>, smem, optin))
             return RSPI_ERR_CUDA;
         k_screen_sets<1024><<<n_ctas, warps_per_cta * 32, smem, stream>>>(
-            src, (int)num_rot, init, scales, ent, group_off, set_frames, (int)n_sets, n_parts,
-            part_w, row_begin, row_end, ll, ll_stride, ps, frame_max, err);
+            src, (int)num_rot, init, scales, ent, group_off, quarter_groups, set_frames,
+            (int)n_sets, n_parts, part_w, row_begin, row_end, ll, ll_stride, ps, frame_max, err);
     }
     RSPI_RETURN_LAUNCH();
 }

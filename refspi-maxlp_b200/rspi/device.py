@@ -566,7 +566,9 @@ class EStep:
         real = set_frames >= 0
         col_of_frame[set_frames[real].long()] = k[real].to(_i32)
         groups = torch.empty(parts * n_sets, dtype=_i32, device=dev)
-        call('rspi_sets_steps', ptr(counts), ptr(set_frames), n_sets, parts, ptr(groups), s)
+        qgroups = torch.empty(parts * n_sets * 4, dtype=_i32, device=dev)
+        call('rspi_sets_steps', ptr(counts), ptr(set_frames), n_sets, parts, ptr(groups),
+             ptr(qgroups), s)
         goff = torch.empty(parts * n_sets + 1, dtype=_i64, device=dev)
         call('rspi_scan_rows', ptr(groups), parts * n_sets, ptr(goff), s)
         total = int(goff[-1].item())
@@ -593,7 +595,8 @@ class EStep:
                 torch.cuda.get_device_properties(dev).multi_processor_count
             ps = torch.empty(self.lib.rspi_sets_part_sums_floats(n_sets, ps_ctas),
                              dtype=torch.float32, device=dev)
-        return dict(entries=entries, group_off=goff, total_groups=total, tile=4, sets=True,
+        return dict(entries=entries, group_off=goff, quarter_groups=qgroups,
+                    total_groups=total, tile=4, sets=True,
                     set_frames=set_frames, col_of_frame=col_of_frame, n_sets=n_sets,
                     frame_groups=frame_groups, n_parts=parts, part_w=part_w, part_sums=ps,
                     part_sums_ctas=ps_ctas, counts=counts)
@@ -731,7 +734,8 @@ class EStep:
                 w = self.wide = self._sets_entries()
             call('rspi_screen_loglike_sets', ptr(lsl), self.num_rot, ptr(self.init),
                  ptr(self.ph.scales), ptr(w['entries']), ptr(w['group_off']),
-                 ptr(w['set_frames']), w['n_sets'], w['n_parts'], w['part_w'], r0, r1,
+                 ptr(w['quarter_groups']), ptr(w['set_frames']), w['n_sets'], w['n_parts'],
+                 w['part_w'], r0, r1,
                  ptr(self.prob[r0]), self.n_cols, ptr(w['part_sums']), w['part_sums_ctas'],
                  ptr(self.frame_max), self.warps, self.n_ctas, ptr(self.ph.err.t), cur_stream())
         elif self.kernel == 'stream' and self.form == 'screen':

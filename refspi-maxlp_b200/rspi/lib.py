@@ -68,13 +68,13 @@ SIGNATURES = {
     'rspi_phase_proj_real': (I, [P, P, P, P, L, P]),
     'rspi_phase_refine': (I, [P, P, P, P, P, L, I, I, P]),
     'rspi_sets_counts': (I, [P, P, L, I, I, I, P, P]),
-    'rspi_sets_steps': (I, [P, P, L, I, P, P]),
+    'rspi_sets_steps': (I, [P, P, L, I, P, P, P]),
     'rspi_sets_fill': (I, [P, P, I, I, I, P, P, L, P, P, P, P]),
     'rspi_holo_pairs32': (I, [P, L, L, P, P]),
     'rspi_rot_log_slices_sets': (I, [P, P, L, L, P, L, P, P, L, I, I, L, L, P, P, P]),
     'rspi_sets_part_sums_floats': (L, [L, I]),
-    'rspi_screen_loglike_sets': (I, [P, L, P, P, P, P, P, L, I, I, L, L, P, L, P, I, P, I, I,
-                                     P, P]),
+    'rspi_screen_loglike_sets': (I, [P, L, P, P, P, P, P, P, L, I, I, L, L, P, L, P, I, P, I,
+                                     I, P, P]),
     'rspi_frame_max_finalize': (I, [P, P, L, P, P, P]),
     'rspi_screen_candidates_cols': (I, [P, L, L, P, L, P, P, P, P, P, D, P, P, P, P, P, L, P, P,
                                         P, P, P]),

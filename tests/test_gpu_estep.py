@@ -475,11 +475,12 @@ def test_sets_kernel_matches_stream_kernel(name, ds, need_scaling, parts, warps)
 @pytest.mark.parametrize('n,parts', [(61, 1), (300, 2), (45, 3), (33, 4)])
 def test_sets_layout_entries(n, parts):
     """Frame sets: every frame's photons of each column part once, in its own
-    lane; a quarter warp runs D_q steps, D_q the fewest any schedule needs
-    (its largest frame or class total), in which its eight lanes read eight
-    distinct bank classes (column mod 8), the slots without a photon holding
-    the zero column of the slot's class, and is idle (every lane 0xffff)
-    from step D_q on; each (set, part) range has ceil(max_q D_q / 4) groups;
+    lane, within its quarter warp's first D_q steps, D_q the fewest any
+    schedule needs (its largest frame or class total), in which the eight
+    lanes read eight distinct bank classes (column mod 8), the slots without
+    a photon holding the zero column of the slot's class; from step D_q on
+    lane 8 q + f holds zero column f; the quarter warp's own group count is
+    ceil(D_q / 4) and each (set, part) range has the largest of the four;
     frames in decreasing photon order, rank 32 s + p + 4 f in lane 8 p + f;
     column of frame d = its slot."""
     size = 37
@@ -511,8 +512,8 @@ def test_sets_layout_entries(n, parts):
         for h in range(parts):
             blk = ent[goff[h * ns + s]:goff[h * ns + s + 1]]          # (G, 32, 4)
             steps = blk.transpose(0, 2, 1).reshape(-1, 32)           # (4G, 32)
-            idle = steps == 0xffff
-            assert np.all((steps <= pw + 7) | idle)
+            assert np.all(steps <= pw + 7)
+            qg = w['quarter_groups'].cpu().numpy()[(h * ns + s) * 4:(h * ns + s) * 4 + 4]
             need = 0
             for q in range(4):
                 m = np.zeros((8, 8), np.int64)
@@ -523,18 +524,16 @@ def test_sets_layout_entries(n, parts):
                         m[f] = np.bincount(loc % 8, minlength=8)
                 dq = max(m.sum(1).max(), m.sum(0).max())
                 need = max(need, dq)
-                qi = idle[:, 8 * q:8 * q + 8]
-                # idle exactly from step dq on, all eight lanes together
-                assert not qi[:dq].any() and qi[dq:].all(), (s, h, q)
+                assert qg[q] == -(-dq // 4), (s, h, q)
                 cls = steps[:dq, 8 * q:8 * q + 8] % 8
                 assert all(len(set(row)) == 8 for row in cls), (s, h, q)
+                assert np.all(steps[dq:, 8 * q:8 * q + 8] == pw + np.arange(8)), (s, h, q)
             assert blk.shape[0] == -(-need // 4), (s, h)
             for lane in range(32):
                 fr = sf[32 * s + lane]
                 col = steps[:, lane]
                 real = col < pw
-                pad = ~real & (col != 0xffff)
-                assert np.all(col[pad] == pw + (col[pad] % 8))
+                assert np.all(col[~real] == pw + (col[~real] % 8))
                 if fr < 0:
                     assert not real.any()
                     continue

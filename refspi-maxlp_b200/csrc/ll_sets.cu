@@ -535,23 +535,25 @@ k_screen_sets(const float4 *__restrict__ lsl4, int num_rot, const double *__rest
                 if (s >= n_sets) break;
                 const long long gi = (long long)h * n_sets + s;
                 const long long g0 = goff[gi], g1 = goff[gi + 1];
-                // this lane's quarter warp stops after its own groups: its
-                // later gathers are not issued (no shared-memory wavefront)
-                const long long ge = qgroups ? g0 + qgroups[gi * 4 + (lane >> 3)] : g1;
+                // the set runs ng groups; this lane's quarter warp stops after
+                // its own nq (<= ng): its later gathers are not issued, so
+                // they take no shared-memory wavefront
+                const int ng = (int)(g1 - g0);
+                const int nq = qgroups ? qgroups[gi * 4 + (lane >> 3)] : ng;
                 float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0;
                 const uint2 *gp = groups + g0 * 32 + lane;
-                long long g = g0;
-                uint2 c0 = g < ge ? ld_entries(gp, keep) : make_uint2(0, 0);
-                uint2 c1 = g + 1 < ge ? ld_entries(gp + 32, keep) : make_uint2(0, 0);
-                for (; g + 1 < g1; g += 2, gp += 64) {
-                    const uint2 n0 = g + 2 < ge ? ld_entries(gp + 64, keep) : make_uint2(0, 0);
-                    const uint2 n1 = g + 3 < ge ? ld_entries(gp + 96, keep) : make_uint2(0, 0);
-                    if (g < ge) a0 = f4_add(a0, group_sum(smem_raw, c0));
-                    if (g + 1 < ge) a1 = f4_add(a1, group_sum(smem_raw, c1));
+                int k = 0;
+                uint2 c0 = 0 < nq ? ld_entries(gp, keep) : make_uint2(0, 0);
+                uint2 c1 = 1 < nq ? ld_entries(gp + 32, keep) : make_uint2(0, 0);
+                for (; k + 1 < ng; k += 2, gp += 64) {
+                    const uint2 n0 = k + 2 < nq ? ld_entries(gp + 64, keep) : make_uint2(0, 0);
+                    const uint2 n1 = k + 3 < nq ? ld_entries(gp + 96, keep) : make_uint2(0, 0);
+                    if (k < nq) a0 = f4_add(a0, group_sum(smem_raw, c0));
+                    if (k + 1 < nq) a1 = f4_add(a1, group_sum(smem_raw, c1));
                     c0 = n0;
                     c1 = n1;
                 }
-                if (g < ge) a0 = f4_add(a0, group_sum(smem_raw, c0));
+                if (k < nq) a0 = f4_add(a0, group_sum(smem_raw, c0));
                 const float4 sum = f4_add(a0, a1);
                 const int col = s * 32 + lane;
                 // this set's running sum: TMEM columns 4 (s / 4) of the lane

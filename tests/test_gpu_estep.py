@@ -669,3 +669,44 @@ def test_sets_fp32_slice_arithmetic(name, ds, need_scaling):
     assert np.array_equal(a[3], b[3])
     np.testing.assert_allclose(a[2], b[2], rtol=1e-15)
     np.testing.assert_allclose(a[4], b[4], rtol=1e-9)
+
+
+@pytest.mark.parametrize('parts', [2, 3])
+def test_sets_kernel_beyond_tensor_memory_sets(parts):
+    """More than 512 sets (16,384 frames): the running part sums of the
+    first 512 sets live in tensor memory, the others in the global scratch;
+    every FP32 likelihood within the screening bound eps_d of the FP64
+    form's, and the FP64-rescored argmax and maximum equal the FP64 form's,
+    for two and three column parts (the middle part reads and rewrites its
+    running sums)."""
+    size, n = 29, 16384 + 32 * 9 + 5          # 522 sets, the last one partial
+    d = random_photons(size, n, 150., 21, empty_frames=(3, n - 1))
+    ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
+                         d['count_multi'], size * size, True)
+    sx, sy, dia, _ = E.generate_states(E.parse_triple('-1 1 2'), E.parse_triple('0 0 1'),
+                                       E.parse_triple('2 2 1'))
+    num_rot = 4
+    rng = np.random.default_rng(7)
+    model = torch.from_numpy(rng.random(size * size) + 1j * rng.random(size * size)).cuda()
+    ref = _estep(_photons(ds, True), size, num_rot, sx, sy, dia, ds['bg'], form='fp64')
+    ref.run(model)
+    maxll64, rmax64, _ = ref.reduce()
+    want = ref.frame_prob().cpu().numpy()
+    ph = _photons(ds, True)
+    es = _estep(ph, size, num_rot, sx, sy, dia, ds['bg'], form='screen', kernel='sets',
+                screen_parts=parts)
+    assert es.wide['n_sets'] > 512 and es.wide['n_parts'] == parts
+    es.run(model)
+    maxll, rmax, _ = es.reduce()
+    torch.cuda.synchronize()
+    ph.err.check('sets kernel beyond the tensor-memory sets')
+    got = es.frame_prob().cpu().numpy().astype(np.float64)
+    rows = np.diff(es._eps_rows().cpu().numpy()).astype(np.float64)
+    phot = es.ll['frame_sel_photons'].cpu().numpy().astype(np.float64)
+    lmax = float(es.lmax.cpu().numpy().reshape(-1)[0])
+    eps = 2. ** -24 * ((rows + 8.) * phot * lmax + np.abs(want) + 1.)
+    err = np.abs(got - want)
+    worst = np.unravel_index(np.argmax(err / eps), err.shape)
+    assert np.all(err <= eps), (worst, err[worst], eps[worst])
+    assert np.array_equal(rmax.cpu().numpy(), rmax64.cpu().numpy())
+    np.testing.assert_allclose(maxll.cpu().numpy(), maxll64.cpu().numpy(), rtol=1e-14)

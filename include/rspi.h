@@ -280,16 +280,18 @@ int rspi_sets_fill(const unsigned short *entries16, const long long *row_off16, 
  * out[(((r - row_begin) / 4 * n_parts + h) * part_w + c) * 4 + (r - row_begin) % 4]
  * is row r at column h * part_w + c (zero past n_sel); rows of a partial
  * last tile beyond row_end are not written.  holo_pairs as for
- * rspi_rot_log_slices_pairs; out 16-byte aligned.  holo_pairs32 NULL: the
+ * rspi_rot_log_slices_pairs; out 16-byte aligned.  holo_quads32 NULL: the
  * values of rspi_rot_log_slices rounded to FP32 (identical bits).
- * holo_pairs32 given (the same pairs in FP32, rspi_holo_pairs32): the
- * interpolation and the log in FP32, |L32 - L| <= 2^-24 (10 + 2 |L|), with
- * values at or below 2e-20 (and the in-detector test) in FP64 so the -1000
- * sentinel falls where the reference's does; the caller's candidate
- * threshold must cover the extra error (rows + 12 with abs_max >= 1). */
-int rspi_holo_pairs32(const double *holo, long long n_states0, long long size,
-                      float *holo_pairs32, cudaStream_t stream);
-int rspi_rot_log_slices_sets(const double *holo_pairs, const float *holo_pairs32,
+ * holo_quads32 given (rspi_holo_quads32: per pixel i of every state the four
+ * bilinear corners W[i], W[i + 1], W[i + size], W[i + size + 1] in FP32,
+ * 16-byte aligned, 4 * n_states0 * size^2 floats): the interpolation and
+ * the log in FP32, |L32 - L| <= 2^-24 (10 + 2 |L|), with values at or below
+ * 2e-20 (and the in-detector test) in FP64 so the -1000 sentinel falls
+ * where the reference's does; the caller's candidate threshold must cover
+ * the extra error (rows + 12 with abs_max >= 1). */
+int rspi_holo_quads32(const double *holo, long long n_states0, long long size,
+                      float *holo_quads32, cudaStream_t stream);
+int rspi_rot_log_slices_sets(const double *holo_pairs, const float *holo_quads32,
                              long long n_states0, long long num_rot, const double *rot_cs,
                              long long size, const double *bg, const int *sel_pix,
                              long long n_sel, int n_parts, int part_w, long long row_begin,

@@ -110,12 +110,17 @@ __global__ void k_holo_pairs(const double *__restrict__ holo, long long total,
         hp[i] = make_double2(holo[i], i + 1 < total ? holo[i + 1] : 0.);
 }
 
-// The same pairs rounded to FP32, for the frame-set slices' FP32 arithmetic.
-__global__ void k_holo_pairs32(const double *__restrict__ holo, long long total,
-                               float2 *__restrict__ hp) {
+// The four bilinear corners of every pixel rounded to FP32, for the
+// frame-set slices' FP32 arithmetic: hq[i] = (W[i], W[i + 1], W[i + size],
+// W[i + size + 1]) (zero past the end; corners that wrap into the next row
+// or state belong to no in-detector footprint), one 16-byte load per value.
+__global__ void k_holo_quads32(const double *__restrict__ holo, long long total, int size,
+                               float4 *__restrict__ hq) {
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride)
-        hp[i] = make_float2((float)holo[i], i + 1 < total ? (float)holo[i + 1] : 0.f);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        auto at = [&](long long j) { return j < total ? (float)holo[j] : 0.f; };
+        hq[i] = make_float4(at(i), at(i + 1), at(i + size), at(i + size + 1));
+    }
 }
 
 template <typename TL, bool PAIRS>
@@ -211,15 +216,17 @@ k_rot_log_js(const double *__restrict__ holo, const double2 *__restrict__ hp, in
 // tile's four rows, stored as one 16-byte write.  Values are those of
 // rot_log_value (same operations, identical bits).
 //
-// With MATH32 the value of each (state, rotation) is computed in FP32 from
-// an FP32 copy of the pairs: bilinear interpolation of positive terms
-// (|relative error| <= 9 * 2^-24: the FP32 roundings of W, the weights and
-// bg, four products and four sums) and logf (at most 1 ulp, CUDA's
-// documented bound), so |L32 - L| <= 2^-24 (10 + 2 |L|); the rotated
+// k_rot_log_sets computes them in FP64 from the paired copy.
+// k_rot_log_sets32 computes the value of each (state, rotation) in FP32
+// from an FP32 copy of the four corners: bilinear interpolation of positive
+// terms (|relative error| <= 9 * 2^-24: the FP32 roundings of W, the
+// weights and bg, four products and four sums) and logf (at most 1 ulp,
+// CUDA's documented bound), so |L32 - L| <= 2^-24 (10 + 2 |L|); the rotated
 // positions, floors and the in-detector test stay FP64, and an
 // interpolated value at or below 2e-20 (or above 1e30) is computed in FP64
 // instead, so the -1000 sentinel is taken exactly where the reference takes
 // it.
+
 // FP64 value of one (state, rotation, column) for the FP32 path's rare
 // fallback: the operations of the FP64 path (and of rot_log_value), the
 // rotated position recomputed from (x, y) so that the FP32 path keeps no
@@ -248,11 +255,12 @@ __device__ __noinline__ float rot_log_fp64(const double2 *__restrict__ w2, int x
 // The FP32-arithmetic form of k_rot_log_sets (its values as described
 // there): per column only the four rotations' in-detector bits, corner
 // indices and FP32 weights stay live across the states, so that 1,024
-// threads fit an SM (64 registers): 6.17 ms instead of 8.17 ms (256 threads,
-// 108 registers) for the 72,900 rows x 24,928 columns of a 185^2 detector,
-// with identical values.
+// threads fit an SM (64 registers), and a value's four corners come in one
+// 16-byte load of the quad copy: 5.37 ms instead of 8.17 ms (256 threads,
+// 108 registers, two 8-byte pair loads) for the 72,900 rows x 24,928
+// columns of a 185^2 detector, with identical values.
 __global__ void __launch_bounds__(1024, 1)
-k_rot_log_sets32(const double2 *__restrict__ hp, const float2 *__restrict__ hp32, int num_rot,
+k_rot_log_sets32(const double2 *__restrict__ hp, const float4 *__restrict__ hq, int num_rot,
                  const double *__restrict__ rot_cs, int size, const double *__restrict__ bg,
                  const int *__restrict__ sel_pix, int n_sel, int n_parts, int part_w,
                  long long row_begin, long long row_end, long long s_lo,
@@ -309,12 +317,11 @@ k_rot_log_sets32(const double2 *__restrict__ hp, const float2 *__restrict__ hp32
                     if (!real) continue;
                     bool done = false;
                     if ((inmask >> q) & 1u) {
-                        const float2 a = hp32[s0 * npix + base[q]];
-                        const float2 b2 = hp32[s0 * npix + base[q] + size];
-                        float t = a.x * cxf[q] * cyf[q];
-                        t += b2.x * fxf[q] * cyf[q];
-                        t += a.y * cxf[q] * fyf[q];
-                        t += b2.y * fxf[q] * fyf[q];
+                        const float4 w = hq[s0 * npix + base[q]];   // corners 00, 01, 10, 11
+                        float t = w.x * cxf[q] * cyf[q];
+                        t += w.z * fxf[q] * cyf[q];
+                        t += w.y * cxf[q] * fyf[q];
+                        t += w.w * fxf[q] * fyf[q];
                         t += bf;
                         if (t > 2.e-20f && t < 1.e30f) {
                             v[q] = logf(t);
@@ -355,9 +362,8 @@ k_rot_log_sets32(const double2 *__restrict__ hp, const float2 *__restrict__ hp32
     }
 }
 
-template <bool MATH32>
 __global__ void __launch_bounds__(256)
-k_rot_log_sets(const double2 *__restrict__ hp, const float2 *__restrict__ hp32, int num_rot,
+k_rot_log_sets(const double2 *__restrict__ hp, int num_rot,
                const double *__restrict__ rot_cs, int size, const double *__restrict__ bg,
                const int *__restrict__ sel_pix, int n_sel, int n_parts, int part_w,
                long long row_begin, long long row_end, long long s_lo, float *__restrict__ out,
@@ -413,40 +419,22 @@ k_rot_log_sets(const double2 *__restrict__ hp, const float2 *__restrict__ hp32, 
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
                     double val = 0.;
-                    bool done = false;
-                    if (MATH32 && c < n_sel && in[q]) {
-                        const float2 a = hp32[s0 * npix + base[q]];
-                        const float2 b2 = hp32[s0 * npix + base[q] + size];
-                        const float fxf = (float)fx[q], fyf = (float)fy[q];
-                        const float cxf = (float)(1. - fx[q]), cyf = (float)(1. - fy[q]);
-                        float t = a.x * cxf * cyf;
-                        t += b2.x * fxf * cyf;
-                        t += a.y * cxf * fyf;
-                        t += b2.y * fxf * fyf;
-                        t += (float)b;
-                        if (t > 2.e-20f && t < 1.e30f) {
-                            v[q] = logf(t);
-                            done = true;
+                    if (c < n_sel) {
+                        if (in[q]) {
+                            const double2 a = hp[s0 * npix + base[q]];
+                            const double2 b2 = hp[s0 * npix + base[q] + size];
+                            const double cx = 1. - fx[q], cy = 1. - fy[q];
+                            double t = xmul(xmul(a.x, cx), cy);
+                            t = xadd(t, xmul(xmul(b2.x, fx[q]), cy));
+                            t = xadd(t, xmul(xmul(a.y, cx), fy[q]));
+                            t = xadd(t, xmul(xmul(b2.y, fx[q]), fy[q]));
+                            t = xadd(t, b);
+                            val = t < 1.e-20 ? -1000. : log(t);
+                        } else {
+                            val = -1000.;
                         }
                     }
-                    if (!done) {
-                        if (c < n_sel) {
-                            if (in[q]) {
-                                const double2 a = hp[s0 * npix + base[q]];
-                                const double2 b2 = hp[s0 * npix + base[q] + size];
-                                const double cx = 1. - fx[q], cy = 1. - fy[q];
-                                double t = xmul(xmul(a.x, cx), cy);
-                                t = xadd(t, xmul(xmul(b2.x, fx[q]), cy));
-                                t = xadd(t, xmul(xmul(a.y, cx), fy[q]));
-                                t = xadd(t, xmul(xmul(b2.y, fx[q]), fy[q]));
-                                t = xadd(t, b);
-                                val = t < 1.e-20 ? -1000. : log(t);
-                            } else {
-                                val = -1000.;
-                            }
-                        }
-                        v[q] = (float)val;
-                    }
+                    v[q] = (float)val;
                 }
                 const long long r0 = s0 * num_rot + j0 - row_begin;
                 if (j0 + 3 < num_rot && (r0 & 3) == 0 && r0 >= 0 && r0 + 3 < n_rows) {
@@ -571,18 +559,18 @@ extern "C" int rspi_sphere_ramp(long long size, double sx, double sy, double dia
     RSPI_RETURN_LAUNCH();
 }
 
-extern "C" int rspi_holo_pairs32(const double *holo, long long n_states0, long long size,
-                                 float *holo_pairs32, cudaStream_t stream) {
-    if (!holo || !holo_pairs32 || n_states0 <= 0 || size <= 1 || size > 46340 ||
-        (reinterpret_cast<uintptr_t>(holo_pairs32) & 7) != 0)
+extern "C" int rspi_holo_quads32(const double *holo, long long n_states0, long long size,
+                                 float *holo_quads32, cudaStream_t stream) {
+    if (!holo || !holo_quads32 || n_states0 <= 0 || size <= 1 || size > 46340 ||
+        (reinterpret_cast<uintptr_t>(holo_quads32) & 15) != 0)
         return RSPI_ERR_ARG;
     const long long total = n_states0 * size * size;
-    k_holo_pairs32<<<rspi_blocks(total, 256), 256, 0, stream>>>(
-        holo, total, reinterpret_cast<float2 *>(holo_pairs32));
+    k_holo_quads32<<<rspi_blocks(total, 256), 256, 0, stream>>>(
+        holo, total, (int)size, reinterpret_cast<float4 *>(holo_quads32));
     RSPI_RETURN_LAUNCH();
 }
 
-extern "C" int rspi_rot_log_slices_sets(const double *holo_pairs, const float *holo_pairs32,
+extern "C" int rspi_rot_log_slices_sets(const double *holo_pairs, const float *holo_quads32,
                                         long long n_states0, long long num_rot,
                                         const double *rot_cs, long long size, const double *bg,
                                         const int *sel_pix, long long n_sel, int n_parts,
@@ -594,7 +582,7 @@ extern "C" int rspi_rot_log_slices_sets(const double *holo_pairs, const float *h
         (long long)n_parts * part_w > 0x7fffffffLL || row_begin < 0 || row_end < row_begin ||
         row_end > n_states0 * num_rot || (n_sel > 0 && !sel_pix) ||
         (reinterpret_cast<uintptr_t>(holo_pairs) & 15) != 0 ||
-        (reinterpret_cast<uintptr_t>(holo_pairs32) & 7) != 0 ||
+        (reinterpret_cast<uintptr_t>(holo_quads32) & 15) != 0 ||
         (reinterpret_cast<uintptr_t>(out) & 15) != 0)
         return RSPI_ERR_ARG;
     if (row_end == row_begin) return RSPI_OK;
@@ -603,14 +591,14 @@ extern "C" int rspi_rot_log_slices_sets(const double *holo_pairs, const float *h
     const long long n_jb = (num_rot + 3) / 4;
     if (n_groups * n_jb > 0x7fffffffLL) return RSPI_ERR_ARG;
     const double2 *hp = reinterpret_cast<const double2 *>(holo_pairs);
-    const float2 *hp32 = reinterpret_cast<const float2 *>(holo_pairs32);
-    if (hp32)
+    const float4 *hq = reinterpret_cast<const float4 *>(holo_quads32);
+    if (hq)
         k_rot_log_sets32<<<(unsigned)(n_groups * n_jb), 1024, 0, stream>>>(
-            hp, hp32, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, n_parts, part_w,
+            hp, hq, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, n_parts, part_w,
             row_begin, row_end, s_lo, out, abs_max);
     else
-        k_rot_log_sets<false><<<(unsigned)(n_groups * n_jb), 256, 0, stream>>>(
-            hp, nullptr, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, n_parts,
-            part_w, row_begin, row_end, s_lo, out, abs_max);
+        k_rot_log_sets<<<(unsigned)(n_groups * n_jb), 256, 0, stream>>>(
+            hp, (int)num_rot, rot_cs, (int)size, bg, sel_pix, (int)n_sel, n_parts, part_w,
+            row_begin, row_end, s_lo, out, abs_max);
     RSPI_RETURN_LAUNCH();
 }

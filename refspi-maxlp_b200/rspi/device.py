@@ -289,7 +289,7 @@ class EStep:
         self.bg = t(np.asarray(bg, dtype='f8').ravel())
         self.ll = photons.ll_entries(self.pix2sel, self.p_pad)
         self.col_of_frame, self.frame_of_col, self.n_cols = None, None, n
-        self.holo_pairs32 = None
+        self.holo_quads32 = None
         if form == 'dense':
             self._init_dense(photons, slice_budget_bytes, delta, cand_per_frame, dense_gemm,
                              dense_rescore)
@@ -333,8 +333,8 @@ class EStep:
             self.n_cols = self.wide['n_sets'] * 32
             self.frame_max = torch.zeros(self.n_cols, dtype=_i64, device=dev)
             self.cand_slot = torch.empty(n * 32, dtype=_i32, device=dev)
-        # FP32 copy of the pairs for the FP32 slice arithmetic
-        self.holo_pairs32 = torch.empty((self.n_states0, self.size ** 2, 2),
+        # FP32 copy of the four bilinear corners for the FP32 slice arithmetic
+        self.holo_quads32 = torch.empty((self.n_states0, self.size ** 2, 4),
                                         dtype=torch.float32, device=dev) \
             if self.slice_math == 'fp32' else None
         self._eps_key, self.row_off_eps = None, None
@@ -660,9 +660,9 @@ class EStep:
             # FP32 slice arithmetic: its per-value error bound 2^-24 (10 + 2|L|)
             # is charged as 12 more summation steps of max(|L|, 1)
             self.lmax.fill_(1. if self.slice_math == 'fp32' else 0.)
-        if self.holo_pairs32 is not None:
-            call('rspi_holo_pairs32', ptr(self.holo), self.n_states0, self.size,
-                 ptr(self.holo_pairs32), s)
+        if self.holo_quads32 is not None:
+            call('rspi_holo_quads32', ptr(self.holo), self.n_states0, self.size,
+                 ptr(self.holo_quads32), s)
         if self.col_of_frame is not None:
             self.frame_max.zero_()
 
@@ -683,7 +683,7 @@ class EStep:
         out = self.lsl if out is None else out
         if self.kernel == 'sets':
             w = self.wide
-            call('rspi_rot_log_slices_sets', ptr(self.holo_pairs), ptr(self.holo_pairs32),
+            call('rspi_rot_log_slices_sets', ptr(self.holo_pairs), ptr(self.holo_quads32),
                  self.n_states0, self.num_rot,
                  ptr(self.rot_cs), self.size, ptr(self.bg), ptr(self.sel_pix), self.n_sel,
                  w['n_parts'], w['part_w'], r0, r1, ptr(out), ptr(self.lmax), cur_stream())

@@ -304,7 +304,8 @@ class DataGenerator():
             sys.stderr.write('\rWritten %d/%d frames (%d)' % (f0 + b, n, photons))
         etime = time.time()
         sys.stderr.write('\nTime taken (make_data): %f s\n' % (etime - stime))
-        out.update({k: np.concatenate(v).astype('i4') for k, v in lists.items()})
+        out.update({k: (np.concatenate(v) if v else np.zeros(0)).astype('i4')
+                    for k, v in lists.items()})
         delete = ['ones', 'multi', 'place_ones', 'place_multi', 'count_multi', 'num_pix',
                   'true_shifts', 'true_diameters', 'true_angles', 'bg', 'scale']
         if self.object_hetro:

@@ -279,3 +279,15 @@ def test_datagenerator_rejects_wobble_types_without_hetero(tmp_path):
     gen = DataGenerator(cfg)
     with pytest.raises(ValueError):
         gen.make_data()
+
+
+def test_datagenerator_without_frames(tmp_path):
+    """num_data = 0 writes the object and empty frame datasets."""
+    from make_data import DataGenerator
+    from rspi.photonfile import PhotonsFile
+    cfg = _config(str(tmp_path / 'sim.ini'), n=0)
+    gen = DataGenerator(cfg)
+    out = gen.make_data()
+    assert out['ones'].shape == (0,) and out['place_ones'].shape == (0,)
+    f = PhotonsFile(str(tmp_path / 'photons.h5'))
+    assert f['true_angles'].shape == (0,) and 'solution' in f

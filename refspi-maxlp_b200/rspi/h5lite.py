@@ -354,17 +354,25 @@ class _Writer:
         return addr
 
     def global_heap(self, objects):
-        """One collection holding every object; returns its address."""
-        body = b''
-        for i, o in enumerate(objects, start=1):
-            body += struct.pack('<HHIQ', i, 1, 0, len(o)) + _pad8(o)
-        size = 16 + len(body) + 16
-        size = max(size, 4096)
-        free = size - 16 - len(body)
-        body += struct.pack('<HHIQ', 0, 0, 0, free)
-        data = b'GCOL' + struct.pack('<B3xQ', 1, size) + body
-        data += b'\0' * (size - len(data))
-        return self.alloc(data)
+        """Global heap collections holding the objects in order (at most
+        65,535 per collection: the object index is 16 bits); returns each
+        object's (collection address, index)."""
+        refs = []
+        for c0 in range(0, len(objects), 65535):
+            chunk = objects[c0:c0 + 65535]
+            parts = []
+            for i, o in enumerate(chunk, start=1):
+                parts.append(struct.pack('<HHIQ', i, 1, 0, len(o)))
+                parts.append(_pad8(o))
+            body = b''.join(parts)
+            size = max(16 + len(body) + 16, 4096)
+            free = size - 16 - len(body)
+            data = b''.join([b'GCOL', struct.pack('<B3xQ', 1, size), body,
+                             struct.pack('<HHIQ', 0, 0, 0, free)])
+            data += b'\0' * (size - len(data))
+            addr = self.alloc(data)
+            refs.extend((addr, i) for i in range(1, len(chunk) + 1))
+        return refs
 
     def dataset(self, arr):
         if isinstance(arr, tuple) and arr[0] == 'vlen':
@@ -373,16 +381,15 @@ class _Writer:
             base = flat.dtype
             bounds = np.concatenate([[0], np.cumsum(lens)])
             objs = [flat[bounds[i]:bounds[i + 1]].tobytes() for i in range(len(lens))]
-            nonempty = [o for o in objs if o]
-            gaddr = self.global_heap(nonempty) if nonempty else UNDEF
-            raw = b''
-            k = 0
+            refs = iter(self.global_heap([o for o in objs if o]))
+            parts = []
             for i, o in enumerate(objs):
                 if o:
-                    k += 1
-                    raw += struct.pack('<IQI', int(lens[i]), gaddr, k)
+                    gaddr, k = next(refs)
+                    parts.append(struct.pack('<IQI', int(lens[i]), gaddr, k))
                 else:
-                    raw += struct.pack('<IQI', 0, 0, 0)
+                    parts.append(struct.pack('<IQI', 0, 0, 0))
+            raw = b''.join(parts)
             shape = (len(lens),)
             dtmsg = _dt_vlen(base)
         else:

@@ -96,3 +96,20 @@ def test_not_hdf5(tmp_path):
     p.write_bytes(b'not an hdf5 file at all')
     with pytest.raises(h5lite.H5FormatError):
         h5lite.read_datasets(str(p))
+
+
+def test_vlen_beyond_one_global_heap_collection(tmp_path):
+    """More than 65,535 non-empty variable-length rows (the 16-bit object
+    index of one global heap collection) go to several collections and read
+    back in order."""
+    from rspi import h5lite
+    n = 70000
+    rng = np.random.default_rng(4)
+    lens = rng.integers(0, 4, n)
+    flat = rng.integers(0, 1 << 20, int(lens.sum())).astype('<i4')
+    path = str(tmp_path / 'big.h5')
+    h5lite.write_datasets(path, {'place_ones': ('vlen', flat, lens), 'ones': lens.astype('i4')})
+    out = h5lite.read_datasets(path)
+    assert np.array_equal(out['place_ones@flat'], flat)
+    assert np.array_equal(out['place_ones@lens'], lens)
+    assert np.array_equal(out['ones'], lens)

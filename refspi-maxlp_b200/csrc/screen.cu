@@ -327,7 +327,10 @@ __global__ void k_row_scatter(const int *__restrict__ cand_r, const long long *_
 // warp reduction), so every value equals the FP64 form's.  A row longer than
 // shared memory holds (GROW: more than ~28,900 likelihood pixels) is built
 // in the CTA's slot of a global scratch array instead and gathered through
-// L1/L2; the arithmetic is the same.
+// L1/L2; the arithmetic is the same.  A row whose candidates read fewer
+// values than the row holds (a sparse frame or two, the usual case of the
+// argmax-only window) is not built: each value is computed with
+// rot_log_value where the sum reads it.
 template <bool GROW>
 __global__ void __launch_bounds__(1024)
 k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ row_cand,
@@ -345,6 +348,7 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
     const long long npix = (long long)size * size;
     const unsigned cmax = (unsigned)p_pad - 1;
     const float inv_size = 1.f / (float)size;
+    __shared__ long long s_work;
     for (long long r = blockIdx.x; r < n_rows; r += gridDim.x) {
         const long long a = row_off[r], b = row_off[r + 1];
         if (a == b) continue;   // uniform across the CTA
@@ -352,17 +356,44 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
         const double ac = rot_cs[2 * j], as = rot_cs[2 * j + 1];
         const double *w = holo + s0 * npix;
         __syncthreads();        // the previous row's readers are done
-        for (long long c = threadIdx.x; c < p_pad; c += blockDim.x) {
-            double v = 0.;
-            if (c < n_sel) {
-                const int p = sel_pix[c];
-                int x, y;
-                pixel_xy(p, size, inv_size, x, y);
-                v = rot_log_value(w, x, y, size, ac, as, bg[p]);
+        // the values the row's candidates read (their entry slots): when they
+        // are fewer than the row's, each is computed where it is read
+        // instead of building the row (same function, same sums: the same
+        // bits)
+        if (wid == 0) {
+            long long wk = 0;
+            for (long long i = a + lane; i < b; i += 32) {
+                const int d = cand_d[row_cand[i]];
+                wk += (row_off32[d + 1] - row_off32[d]) * 32;
             }
-            sl[c] = v;
+            wk = warp_sum(wk);
+            if (lane == 0) s_work = wk;
         }
         __syncthreads();
+        const bool direct = s_work < p_pad;
+        if (!direct) {
+            for (long long c = threadIdx.x; c < p_pad; c += blockDim.x) {
+                double v = 0.;
+                if (c < n_sel) {
+                    const int p = sel_pix[c];
+                    int x, y;
+                    pixel_xy(p, size, inv_size, x, y);
+                    v = rot_log_value(w, x, y, size, ac, as, bg[p]);
+                }
+                sl[c] = v;
+            }
+        }
+        __syncthreads();
+        // the likelihood-pixel value of entry column c (0 past n_sel, as
+        // the row holds it)
+        auto value = [&](unsigned c) -> double {
+            if (!direct) return sl[min(c, cmax)];
+            if (c >= (unsigned)n_sel) return 0.;
+            const int p = sel_pix[c];
+            int x, y;
+            pixel_xy(p, size, inv_size, x, y);
+            return rot_log_value(w, x, y, size, ac, as, bg[p]);
+        };
         const double ini = init[s0];
         if constexpr (GROW) {
             // a row in global scratch has a few candidates (dense frames):
@@ -374,7 +405,7 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
                 const unsigned *ep = ent32 + row_off32[d] * 32 + lane;
                 for (long long q = row_off32[d]; q < row_off32[d + 1]; ++q, ep += 32) {
                     const unsigned e = __ldg(ep);
-                    acc = fma((double)(e & 0xffffu), sl[min(e >> 16, cmax)], acc);
+                    acc = fma((double)(e & 0xffffu), value(e >> 16), acc);
                 }
                 acc = warp_sum(acc);
                 if (lane == 0) {
@@ -406,7 +437,7 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
                     const unsigned *ep = ent32 + cq0 * 32 + lane;
                     for (long long q = cq0; q < cq1; ++q, ep += 32) {
                         const unsigned e = __ldg(ep);
-                        acc = fma((double)(e & 0xffffu), sl[min(e >> 16, cmax)], acc);
+                        acc = fma((double)(e & 0xffffu), value(e >> 16), acc);
                     }
                     acc = warp_sum(acc);
                     if (lane == c) {

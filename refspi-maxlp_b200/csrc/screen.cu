@@ -327,10 +327,10 @@ __global__ void k_row_scatter(const int *__restrict__ cand_r, const long long *_
 // warp reduction), so every value equals the FP64 form's.  A row longer than
 // shared memory holds (GROW: more than ~28,900 likelihood pixels) is built
 // in the CTA's slot of a global scratch array instead and gathered through
-// L1/L2; the arithmetic is the same.  A row whose candidates read fewer
-// values than the row holds (a sparse frame or two, the usual case of the
-// argmax-only window) is not built: each value is computed with
-// rot_log_value where the sum reads it.
+// L1/L2; the arithmetic is the same.  A row whose candidates' warps read
+// fewer values each than the CTA's threads would build (a sparse frame or
+// two, the usual case of the argmax-only window) is not built: each value
+// is computed with rot_log_value where the sum reads it.
 template <bool GROW>
 __global__ void __launch_bounds__(1024)
 k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ row_cand,
@@ -356,10 +356,10 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
         const double ac = rot_cs[2 * j], as = rot_cs[2 * j + 1];
         const double *w = holo + s0 * npix;
         __syncthreads();        // the previous row's readers are done
-        // the values the row's candidates read (their entry slots): when they
-        // are fewer than the row's, each is computed where it is read
-        // instead of building the row (same function, same sums: the same
-        // bits)
+        // the values the row's candidates read (their entry slots): when
+        // their warps finish them sooner than the CTA builds the row (work
+        // per warp below the row per warp), each is computed where it is
+        // read instead (same function, same sums: the same bits)
         if (wid == 0) {
             long long wk = 0;
             for (long long i = a + lane; i < b; i += 32) {
@@ -370,7 +370,8 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
             if (lane == 0) s_work = wk;
         }
         __syncthreads();
-        const bool direct = s_work < p_pad;
+        const long long n_cand = b - a;
+        const bool direct = s_work * nw < p_pad * min(n_cand, (long long)nw);
         if (!direct) {
             for (long long c = threadIdx.x; c < p_pad; c += blockDim.x) {
                 double v = 0.;

@@ -327,10 +327,11 @@ __global__ void k_row_scatter(const int *__restrict__ cand_r, const long long *_
 // warp reduction), so every value equals the FP64 form's.  A row longer than
 // shared memory holds (GROW: more than ~28,900 likelihood pixels) is built
 // in the CTA's slot of a global scratch array instead and gathered through
-// L1/L2; the arithmetic is the same.  A row whose candidates' warps read
-// fewer values each than the CTA's threads would build (a sparse frame or
-// two, the usual case of the argmax-only window) is not built: each value
-// is computed with rot_log_value where the sum reads it.
+// L1/L2; the arithmetic is the same.  A shared-memory row whose
+// candidates' warps read fewer values each than the CTA's threads would
+// build (a sparse frame or two, the usual case of the argmax-only window)
+// is not built: each value is computed with rot_log_value where the sum
+// reads it.
 template <bool GROW>
 __global__ void __launch_bounds__(1024)
 k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ row_cand,
@@ -359,19 +360,25 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
         // the values the row's candidates read (their entry slots): when
         // their warps finish them sooner than the CTA builds the row (work
         // per warp below the row per warp), each is computed where it is
-        // read instead (same function, same sums: the same bits)
-        if (wid == 0) {
-            long long wk = 0;
-            for (long long i = a + lane; i < b; i += 32) {
-                const int d = cand_d[row_cand[i]];
-                wk += (row_off32[d + 1] - row_off32[d]) * 32;
+        // read instead (same function, same sums: the same bits).  Rows in
+        // global scratch (GROW) are always built: there the candidates of a
+        // row are one or two dense frames, and a row left to one warp keeps
+        // the SM at one warp in flight (measured slower on a 47,616-pixel
+        // row, 10,000 frames).
+        bool direct = false;
+        if constexpr (!GROW) {
+            if (wid == 0) {
+                long long wk = 0;
+                for (long long i = a + lane; i < b; i += 32) {
+                    const int d = cand_d[row_cand[i]];
+                    wk += (row_off32[d + 1] - row_off32[d]) * 32;
+                }
+                wk = warp_sum(wk);
+                if (lane == 0) s_work = wk;
             }
-            wk = warp_sum(wk);
-            if (lane == 0) s_work = wk;
+            __syncthreads();
+            direct = s_work * nw < p_pad * min(b - a, (long long)nw);
         }
-        __syncthreads();
-        const long long n_cand = b - a;
-        const bool direct = s_work * nw < p_pad * min(n_cand, (long long)nw);
         if (!direct) {
             for (long long c = threadIdx.x; c < p_pad; c += blockDim.x) {
                 double v = 0.;

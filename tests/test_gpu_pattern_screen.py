@@ -87,8 +87,24 @@ def test_screen_falls_back_beyond_one_chunk(tmp_path):
     size, n = 19, 1100
     path, params, rng = _random_case(tmp_path, size, n, 100000, 3)
     model = rng.random(size * size) + 1j * rng.random(size * size)
-    st = _check_same(_run_both(path, size, params, model))
+    res = _run_both(path, size, params, model)
+    st = _check_same(res)
     assert st[0] == 0 and st[1] > 0
+    # the chunked path against the oracle's phaser: the ring pass in full
+    # (its mean rescale enters every main pixel), a sample of main pixels.
+    # The main pass covers the ring pixels too, so only the sampled main
+    # pixels hold the same values in both.
+    from oracle import emc_oracle as E
+    from oracle import maxlp_oracle as M
+    d = random_photons(size, n, 30. * size, 3, empty_frames=(1,))
+    ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
+                         d['count_multi'], size * size)
+    _, _, _, mask, rmask = M.get_qvals(size)
+    main = np.flatnonzero(mask)[::9]
+    assert np.any(rmask[main])
+    want = M.run_phaser(model, E.sparse_frames(ds), *params, size, pixels=main)
+    got = np.asarray(res[False][0]).ravel()
+    np.testing.assert_allclose(got[main], want[main], rtol=1e-9, atol=1e-12)
 
 
 def test_screen_handles_zero_model(tmp_path):

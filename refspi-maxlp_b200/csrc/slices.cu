@@ -255,10 +255,12 @@ __device__ __noinline__ float rot_log_fp64(const double2 *__restrict__ w2, int x
 // The FP32-arithmetic form of k_rot_log_sets (its values as described
 // there): per column only the four rotations' in-detector bits, corner
 // indices and FP32 weights stay live across the states, so that 1,024
-// threads fit an SM (64 registers), and a value's four corners come in one
-// 16-byte load of the quad copy: 5.37 ms instead of 8.17 ms (256 threads,
-// 108 registers, two 8-byte pair loads) for the 72,900 rows x 24,928
-// columns of a 185^2 detector, with identical values.
+// threads fit an SM (64 registers), a value's four corners come in one
+// 16-byte load of the quad copy, and a state's four loads (one per rotation)
+// are all issued before any is used: 4.88 ms instead of 8.17 ms (256
+// threads, 108 registers, two 8-byte pair loads, one rotation's load in
+// flight at a time) for the 72,900 rows x 24,928 columns of a 185^2
+// detector, with identical values.
 __global__ void __launch_bounds__(1024, 1)
 k_rot_log_sets32(const double2 *__restrict__ hp, const float4 *__restrict__ hq, int num_rot,
                  const double *__restrict__ rot_cs, int size, const double *__restrict__ bg,
@@ -282,7 +284,8 @@ k_rot_log_sets32(const double2 *__restrict__ hp, const float4 *__restrict__ hq, 
             const int h = c / part_w, cl = c - h * part_w;
             unsigned inmask = 0;
             int base[4] = {0, 0, 0, 0};
-            float fxf[4], fyf[4], cxf[4], cyf[4];
+            float fxf[4] = {0.f, 0.f, 0.f, 0.f}, fyf[4] = {0.f, 0.f, 0.f, 0.f};
+            float cxf[4] = {0.f, 0.f, 0.f, 0.f}, cyf[4] = {0.f, 0.f, 0.f, 0.f};
             int x = 0, y = 0;
             double b = 0.;
             const bool real = c < n_sel;
@@ -310,28 +313,31 @@ k_rot_log_sets32(const double2 *__restrict__ hp, const float4 *__restrict__ hq, 
             }
             const float bf = (float)b;
             for (long long s0 = sb; s0 < se; ++s0) {
+                // the four rotations' corner loads first, all in flight at
+                // once (an out-of-detector or padding column reads corner 0,
+                // a valid address, with zero weights, and ignores it)
+                float4 w[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) w[q] = hq[s0 * npix + base[q]];   // 00, 01, 10, 11
                 float v[4];
+                unsigned slow = 0;
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    v[q] = 0.f;
-                    if (!real) continue;
-                    bool done = false;
-                    if ((inmask >> q) & 1u) {
-                        const float4 w = hq[s0 * npix + base[q]];   // corners 00, 01, 10, 11
-                        float t = w.x * cxf[q] * cyf[q];
-                        t += w.z * fxf[q] * cyf[q];
-                        t += w.y * cxf[q] * fyf[q];
-                        t += w.w * fxf[q] * fyf[q];
-                        t += bf;
-                        if (t > 2.e-20f && t < 1.e30f) {
-                            v[q] = logf(t);
-                            done = true;
-                        }
-                    } else {
-                        v[q] = -1000.f;
-                        done = true;
-                    }
-                    if (!done) {
+                    float t = w[q].x * cxf[q] * cyf[q];
+                    t += w[q].z * fxf[q] * cyf[q];
+                    t += w[q].y * cxf[q] * fyf[q];
+                    t += w[q].w * fxf[q] * fyf[q];
+                    t += bf;
+                    const bool in = (inmask >> q) & 1u;
+                    const bool ok = t > 2.e-20f && t < 1.e30f;
+                    v[q] = !real ? 0.f : !in ? -1000.f : ok ? logf(t) : 0.f;
+                    slow |= (unsigned)(real && in && !ok) << q;
+                }
+                if (slow) {
+                    // at or below 2e-20 (or above 1e30): the FP64 value
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        if (!((slow >> q) & 1u)) continue;
                         const int j = min(j0 + q, num_rot - 1);
                         v[q] = rot_log_fp64(hp + s0 * npix, x, y, size, rot_cs[2 * j],
                                             rot_cs[2 * j + 1], b);

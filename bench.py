@@ -77,6 +77,9 @@ def parse_args():
                          'L-BFGS through the adjoint after its ring pass')
     ap.add_argument('--slice-math', default=None, choices=['fp64', 'fp32'],
                     help='arithmetic of the frame-set kernel\'s log-slices')
+    ap.add_argument('--set-order', default=None, choices=['grouped', 'rank'],
+                    help='frames of the frame-set kernel\'s quarter warps: grouped by class '
+                         'totals (default) or in rank order')
     ap.add_argument('--merge', action='store_true',
                     help='each iteration also merges the posterior-weighted intensities '
                          '(row a10; rescoring window 20 nats)')
@@ -258,7 +261,7 @@ def roofline_blocks(args, w, es, ll_ms, ll_launches, ms, clk, pk, sm_count):
 
 
 def write_inputs(tmp, w, data, form, slice_gb=8., screen_delta=None, kernel=None, mstep=None,
-                 autotune=True, rank=None, slice_math=None, merge=False):
+                 autotune=True, rank=None, slice_math=None, merge=False, set_order=None):
     from rspi.photonfile import write_photons
     os.makedirs(os.path.join(tmp, 'out'), exist_ok=True)
     name = 'photons.npz' if rank is None else 'photons_%d.npz' % rank
@@ -282,6 +285,8 @@ def write_inputs(tmp, w, data, form, slice_gb=8., screen_delta=None, kernel=None
             f.write('slice_math = %s\n' % slice_math)
         if merge:
             f.write('merge = true\n')
+        if set_order:
+            f.write('set_order = %s\n' % set_order)
         f.write('autotune = %s\n' % bool(autotune))
     return cfg
 
@@ -607,7 +612,7 @@ def run_ours(args):
                            args.kernel if args.form != 'dense' else None, args.mstep,
                            not args.no_autotune and not args.warps,
                            rank=rank if world > 1 else None, slice_math=args.slice_math,
-                           merge=args.merge)
+                           merge=args.merge, set_order=args.set_order)
     from emc import EMC
     import contextlib
     import io
@@ -820,6 +825,7 @@ def run_ours(args):
                    'tuned_ms_per_row': (rec.tuning[1] if getattr(rec, 'tuning', None)
                                         else None)},
         'form': {'likelihood': args.form, 'kernel': es.kernel,
+                 'set_order': getattr(es, 'set_order', None) if es.kernel == 'sets' else None,
                  'candidates_rescored': n_cand, 'rescore_window_nats': getattr(es, 'delta', None),
                  'pattern_search': phaser_form},
         'cpu_baseline': cpu,

@@ -247,6 +247,18 @@ int rspi_screen_loglike7(const float *lslices, long long p_row, long long num_ro
  * rspi_sets_counts: counts[d * 32 + 8 h + c] = frame d's photons in part h of
  * local column class c (local column mod 8), from the 16-bit entries of
  * rspi_ll16_entry_fill (p_zero = their zero column).
+ * rspi_sets_group: set_frames[32 * ceil(n_data / 32)] from `order` (the
+ * frames by decreasing photon count, a permutation of [0, n_data)) and
+ * rspi_sets_counts' counts: per window of 256 consecutive ranks, quarters of
+ * eight frames built greedily (each from the longest frame left, adding the
+ * frame that keeps sum over parts of max(largest frame, largest class total)
+ * smallest), then up to `sweeps` sweeps over every pair of the window's
+ * quarters making the best cost-lowering exchange of one frame each, then
+ * the quarters in decreasing cost, four to a set (-1 for empty slots).
+ * Deterministic (integer costs, ties to the lower index).  An `order` entry
+ * outside [0, n_data) sets *err = RSPI_ERR_INDEX and is left out.  Replaces
+ * the rank-interleaved order (frame of rank 32 s + p + 4 f in lane 8 p + f)
+ * as the library's default.
  * rspi_sets_steps: quarter_groups[(h * n_sets + s) * 4 + p] (NULL: not
  * written) = ceil(D_p / 4), D_p the fewest steps quarter warp p of set s
  * needs in part h: max(largest frame count, largest class total over its
@@ -268,6 +280,8 @@ int rspi_screen_loglike7(const float *lslices, long long p_row, long long num_ro
 int rspi_sets_counts(const unsigned short *entries16, const long long *row_off16,
                      long long n_data, int p_zero, int n_parts, int part_w, int *counts,
                      cudaStream_t stream);
+int rspi_sets_group(const int *counts, const int *order, long long n_data, int n_parts,
+                    int sweeps, int *set_frames, int *err, cudaStream_t stream);
 int rspi_sets_steps(const int *counts, const int *set_frames, long long n_sets, int n_parts,
                     int *groups, int *quarter_groups, cudaStream_t stream);
 int rspi_sets_fill(const unsigned short *entries16, const long long *row_off16, int p_zero,

@@ -115,6 +115,203 @@ __global__ void k_sets_steps(const int *__restrict__ counts, const int *__restri
     }
 }
 
+// ---------------------------------------------------------------------------
+// frame grouping: which eight frames share a quarter warp
+// ---------------------------------------------------------------------------
+// A quarter warp's steps are max(largest frame, largest class total) per
+// part, and its gathers cost that many wavefronts whatever its photons.
+// With eight frames of alike length taken in rank order the class totals of
+// a 250-photon frame's quarter exceed their mean by ~12% (Poisson spread of
+// eight frames' photons over eight classes).  So frames are grouped per
+// window of GROUP_W frames of neighbouring ranks (sorted by photon count):
+//  1. greedy: each quarter starts from the longest frame left and takes, seven
+//     times, the frame that keeps sum over parts of max(largest frame,
+//     largest class total) smallest (ties: the lower rank);
+//  2. pair sweeps: for every pair of quarters (a < b) the best of the 64
+//     exchanges of one frame of a with one of b (an empty slot counts as a
+//     frame without photons) is made when it lowers the pair's total cost
+//     (ties: the lower exchange index), until a sweep changes nothing or
+//     `sweeps` are done;
+//  3. the window's quarters in decreasing cost (ties: lower index), four to a
+//     set, so a set's quarters need alike step counts.
+// Everything is integer and in a fixed order: the result is deterministic.
+constexpr int GROUP_W = 256;             // frames per window (a multiple of 32)
+constexpr int GROUP_Q = GROUP_W / 8;     // quarters per window
+constexpr int GROUP_STRIDE = SETS_MAX_PARTS * 8 + 1;
+constexpr unsigned long long GROUP_NONE = ~0ull;
+
+__device__ __forceinline__ unsigned long long block_min_u64(unsigned long long v,
+                                                            unsigned long long *red) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long u = __shfl_xor_sync(RSPI_FULL_MASK, v, o);
+        v = u < v ? u : v;
+    }
+    __syncthreads();
+    if (lane == 0) red[wid] = v;
+    __syncthreads();
+    unsigned long long m = GROUP_NONE;
+    for (int k = 0; k < nw; ++k) m = red[k] < m ? red[k] : m;
+    return m;
+}
+
+// cost of quarter q with slot `slot` holding local frame `f` instead (slot
+// -1: as it is): sum over parts of max(largest frame, largest class total)
+__device__ __forceinline__ int group_cost(short (*qf)[8], int q, int slot, int f,
+                                          int (*cnt)[GROUP_STRIDE], int (*len)[SETS_MAX_PARTS],
+                                          int n_parts) {
+    int cost = 0;
+    for (int p = 0; p < n_parts; ++p) {
+        int lane = 0, cls[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < 8; ++k) {
+            const int g = k == slot ? f : qf[q][k];
+            if (g < 0) continue;
+            lane = max(lane, len[g][p]);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) cls[c] += cnt[g][p * 8 + c];
+        }
+#pragma unroll
+        for (int c = 0; c < 8; ++c) lane = max(lane, cls[c]);
+        cost += lane;
+    }
+    return cost;
+}
+
+__global__ void __launch_bounds__(GROUP_W)
+k_sets_group(const int *__restrict__ counts, const int *__restrict__ order, long long n,
+             int n_parts, int sweeps, int *__restrict__ set_frames, int *err) {
+    __shared__ int cnt[GROUP_W][GROUP_STRIDE];
+    __shared__ int len[GROUP_W][SETS_MAX_PARTS];
+    __shared__ short qf[GROUP_Q][8];
+    __shared__ int qc[GROUP_Q];
+    __shared__ int S[SETS_MAX_PARTS * 8], L[SETS_MAX_PARTS];
+    __shared__ unsigned char used[GROUP_W];
+    __shared__ unsigned long long red[GROUP_W / 32];
+    __shared__ int changed;
+    const int t = threadIdx.x;
+    const long long w0 = (long long)blockIdx.x * GROUP_W;
+    const int m = (int)min((long long)GROUP_W, n - w0);
+    const int nq = (m + 7) / 8;
+    const int p8 = n_parts * 8;
+    // a frame index outside [0, n) is flagged and taken as a frame without
+    // photons (its slot is written as -1)
+    __shared__ int fid[GROUP_W];
+    if (t < m) {
+        const int d = order[w0 + t];
+        const bool ok = d >= 0 && d < n;
+        if (!ok) rspi_flag(err, RSPI_ERR_INDEX);
+        fid[t] = ok ? d : -1;
+    } else {
+        fid[t] = -1;
+    }
+    __syncthreads();
+    for (int i = t; i < GROUP_W * 32; i += blockDim.x) {
+        const int f = i >> 5, k = i & 31;
+        cnt[f][k] = (f < m && k < p8 && fid[f] >= 0) ? counts[(long long)fid[f] * 32 + k] : 0;
+    }
+    __syncthreads();
+    used[t] = t >= m;
+    for (int p = 0; p < SETS_MAX_PARTS; ++p) {
+        int s = 0;
+        for (int c = 0; c < 8; ++c) s += cnt[t][p * 8 + c];
+        len[t][p] = s;
+    }
+    for (int i = t; i < GROUP_Q * 8; i += blockDim.x) qf[i >> 3][i & 7] = -1;
+    __syncthreads();
+
+    // 1. greedy quarters
+    for (int q = 0; q < nq; ++q) {
+        const unsigned long long seed = block_min_u64(used[t] ? GROUP_NONE : (unsigned long long)t, red);
+        if (seed == GROUP_NONE) break;   // uniform; never before the last quarter
+        if (t == 0) {
+            const int f = (int)seed;
+            qf[q][0] = (short)f;
+            used[f] = 1;
+            for (int k = 0; k < p8; ++k) S[k] = cnt[f][k];
+            for (int p = 0; p < n_parts; ++p) L[p] = len[f][p];
+        }
+        __syncthreads();
+        for (int k = 1; k < 8; ++k) {
+            unsigned long long key = GROUP_NONE;
+            if (!used[t]) {
+                int cost = 0;
+                for (int p = 0; p < n_parts; ++p) {
+                    int v = max(L[p], len[t][p]);
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) v = max(v, S[p * 8 + c] + cnt[t][p * 8 + c]);
+                    cost += v;
+                }
+                key = ((unsigned long long)(unsigned)cost << 32) | (unsigned)t;
+            }
+            const unsigned long long best = block_min_u64(key, red);
+            if (best == GROUP_NONE) break;   // uniform: every thread saw the same minimum
+            if (t == 0) {
+                const int f = (int)(best & 0xffffffffu);
+                qf[q][k] = (short)f;
+                used[f] = 1;
+                for (int j = 0; j < p8; ++j) S[j] += cnt[f][j];
+                for (int p = 0; p < n_parts; ++p) L[p] = max(L[p], len[f][p]);
+            }
+            __syncthreads();
+        }
+    }
+    __syncthreads();
+    if (t < nq) qc[t] = group_cost(qf, t, -1, -1, cnt, len, n_parts);
+    __syncthreads();
+
+    // 2. pair sweeps
+    for (int sw = 0; sw < sweeps; ++sw) {
+        if (t == 0) changed = 0;
+        __syncthreads();
+        for (int a = 0; a < nq; ++a) {
+            for (int b = a + 1; b < nq; ++b) {
+                unsigned long long key = GROUP_NONE;
+                int ca = 0, cb = 0;
+                if (t < 64) {
+                    const int i = t >> 3, j = t & 7;
+                    const int fa = qf[a][i], fb = qf[b][j];
+                    if (fa >= 0 || fb >= 0) {
+                        ca = group_cost(qf, a, i, fb, cnt, len, n_parts);
+                        cb = group_cost(qf, b, j, fa, cnt, len, n_parts);
+                        const int delta = ca + cb - qc[a] - qc[b];
+                        // order-preserving map of the signed delta to 32 bits
+                        if (delta < 0)
+                            key = ((unsigned long long)((unsigned)delta ^ 0x80000000u) << 32) |
+                                  (unsigned)t;
+                    }
+                }
+                const unsigned long long best = block_min_u64(key, red);
+                if (best != GROUP_NONE && t == (int)(best & 0xffffffffu)) {
+                    const int i = t >> 3, j = t & 7;
+                    const short fa = qf[a][i];
+                    qf[a][i] = qf[b][j];
+                    qf[b][j] = fa;
+                    qc[a] = ca;
+                    qc[b] = cb;
+                    changed = 1;
+                }
+                __syncthreads();
+            }
+        }
+        if (!changed) break;   // uniform: read after the last pair's barrier
+        __syncthreads();
+    }
+
+    // 3. quarters in decreasing cost, four to a set
+    const long long set0 = w0 / 32;
+    const int ns = (nq + 3) / 4;
+    if (t < nq) {
+        int rank = 0;
+        for (int q = 0; q < nq; ++q) rank += qc[q] > qc[t] || (qc[q] == qc[t] && q < t);
+        for (int k = 0; k < 8; ++k) {
+            const int f = qf[t][k];
+            set_frames[set0 * 32 + rank * 8 + k] = f >= 0 ? fid[f] : -1;
+        }
+    }
+    for (int i = nq * 8 + t; i < ns * 32; i += blockDim.x) set_frames[set0 * 32 + i] = -1;
+}
+
 // Perfect matching of the support of m (8 x 8, m[f][c] > 0) by augmenting
 // paths (breadth-first from each row); col_of[f] receives row f's column.
 // False when none exists (never, for a regular matrix: Hall's condition).
@@ -654,6 +851,17 @@ extern "C" int rspi_sets_counts(const unsigned short *entries16, const long long
         return RSPI_ERR_ARG;
     k_sets_counts<<<rspi_blocks(n_data * 32, BUILD_WARPS * 32), BUILD_WARPS * 32, 0, stream>>>(
         entries16, row_off16, n_data, p_zero, n_parts, part_w, counts);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_sets_group(const int *counts, const int *order, long long n, int n_parts,
+                               int sweeps, int *set_frames, int *err, cudaStream_t stream) {
+    if (!counts || !order || !set_frames || !err || n <= 0 || n > 0x7fffffffLL ||
+        n_parts < 1 || n_parts > SETS_MAX_PARTS || sweeps < 0)
+        return RSPI_ERR_ARG;
+    const long long windows = (n + GROUP_W - 1) / GROUP_W;
+    k_sets_group<<<(unsigned)windows, GROUP_W, 0, stream>>>(counts, order, n, n_parts, sweeps,
+                                                           set_frames, err);
     RSPI_RETURN_LAUNCH();
 }
 

@@ -24,7 +24,10 @@ per warp) or ``stream`` for the screened form, ``stream`` (default) or
 ``dynamic`` for ``fp64``), ``slice_math`` (``fp32``, the
 frame-set kernel's default: its log-slices interpolated and logged in FP32
 within a bound the candidate threshold covers; ``fp64``: computed in FP64,
-stored in FP32, the other kernels' only choice),
+stored in FP32, the other kernels' only choice), ``set_order``
+(``grouped``, the default: each quarter warp's eight frames picked among
+256 of alike photon count so that their bank-class totals stay close to
+their mean; ``rank``: taken in rank order),
 ``merge`` (default false: true adds each iteration's posterior-weighted
 intensities of every (shift, diameter) state, the reference's unused
 ``merge_all`` / ``slice_merge`` kernels (kernels.cu:84-152), to
@@ -126,7 +129,7 @@ class EMC():
                            slice_budget_bytes=int(self.slice_budget_gb * (1 << 30)),
                            n_modes=self.num_modes, dense_gemm=self.dense_gemm,
                            dense_rescore=self.dense_rescore, kernel=self.kernel,
-                           slice_math=self.slice_math)
+                           slice_math=self.slice_math, set_order=self.set_order)
         self.merger = None
         self.intens = None
         if self.merge_intens:
@@ -177,6 +180,7 @@ class EMC():
         self.autotune = config.getboolean('emc', 'autotune', fallback=True)
         self.kernel = config.get('emc', 'kernel', fallback=None) or None
         self.slice_math = config.get('emc', 'slice_math', fallback='').strip() or None
+        self.set_order = config.get('emc', 'set_order', fallback='grouped').strip()
         self.mstep_kind = config.get('emc', 'mstep', fallback='pattern')
         if self.mstep_kind not in ('pattern', 'grid', 'lbfgs', 'grid+lbfgs'):
             raise ValueError('emc:mstep must be pattern, grid, lbfgs or grid+lbfgs')

@@ -27,6 +27,7 @@ QUAD4_WINDOW = 512   # frames ordered by group counts within such windows (four-
 QUAD4_SMEM = 227 * 1024 - 1024   # shared bytes of the four-row tile (kernel limit)
 QUAD4_MAX_PARTS = 4              # column parts of the four-row tile
 QUAD4_COLS = (QUAD4_SMEM // 16 - 8) // 8 * 8   # most columns of one part
+SETS_SWEEPS = 4                  # pair sweeps of the frame grouping (rspi_sets_group)
 
 
 def quad4_parts(p_row, parts=None):
@@ -239,14 +240,18 @@ class EStep:
     FP64 form ``stream`` (default) or ``dynamic``.  ``slice_math``: ``fp32``
     (the frame-set kernel's default, for it only) interpolates and logs the
     slices in FP32 within a bound that the candidate threshold covers;
-    ``fp64`` computes them in FP64 and stores them in FP32.
+    ``fp64`` computes them in FP64 and stores them in FP32.  ``set_order``
+    (frame-set kernel): ``grouped`` (default) picks each quarter warp's
+    eight frames among 256 of alike photon count so that their bank-class
+    totals stay close to their mean (``rspi_sets_group``); ``rank`` takes
+    them in rank order.
     """
 
     def __init__(self, photons, size, num_rot, shiftx, shifty, sphere_dia, probmask, bg,
                  form='fp64', states_per_tile=None, warps=32, n_ctas=0,
                  slice_budget_bytes=8 << 30, delta=20., cand_per_frame=None, kernel=None,
                  n_modes=1, dense_gemm='auto', dense_rescore=True, screen_parts=None,
-                 slice_math=None):
+                 slice_math=None, set_order='grouped'):
         if form not in ('fp64', 'screen', 'dense'):
             raise ValueError('form must be fp64, screen or dense')
         if kernel is None:   # default likelihood kernel of each form
@@ -263,6 +268,9 @@ class EStep:
         if slice_math == 'fp32' and kernel != 'sets':
             raise ValueError('FP32 slice arithmetic is for the frame-set kernel')
         self.slice_math = slice_math
+        if set_order not in ('grouped', 'rank'):
+            raise ValueError('set_order must be grouped or rank')
+        self.set_order = set_order
         self.kernel = kernel
         self.lib = load()
         self.form = form
@@ -542,9 +550,11 @@ class EStep:
 
     def _sets_entries(self):
         """Entries of the frame-set kernel: frames in decreasing order of
-        their likelihood-pixel photons, taken 32 at a time; lane 8 p + f of
-        set s is the frame of rank 32 s + p + 4 f, so the four quarter warps
-        of a set get alike frames.  Per (set, column part) a step schedule
+        their likelihood-pixel photons, grouped per 256 ranks into quarter
+        warps whose class totals stay close to their mean and quarters of
+        alike cost four to a set (``set_order='grouped'``), or lane 8 p + f
+        of set s the frame of rank 32 s + p + 4 f (``'rank'``).  Per (set,
+        column part) a step schedule
         in which a quarter warp's eight lanes read eight distinct bank
         classes (rspi_sets_steps / rspi_sets_fill); one FP32 running sum per
         (CTA, column) between parts when there are several."""
@@ -558,10 +568,16 @@ class EStep:
         order = torch.argsort(-tot, stable=True)
         n_sets = (n + 31) // 32
         k = torch.arange(n_sets * 32, device=dev, dtype=_i64)
-        lane = k % 32
-        src = (k - lane) + (lane // 8) + 4 * (lane % 8)
-        set_frames = torch.where(src < n, order[src.clamp(max=n - 1)],
-                                 torch.full_like(src, -1)).to(_i32)
+        if self.set_order == 'grouped':
+            set_frames = torch.empty(n_sets * 32, dtype=_i32, device=dev)
+            call('rspi_sets_group', ptr(counts), ptr(order.to(_i32)), n, parts, SETS_SWEEPS,
+                 ptr(set_frames), ptr(self.ph.err.t), s)
+            self.ph.err.check('frame grouping')
+        else:
+            lane = k % 32
+            src = (k - lane) + (lane // 8) + 4 * (lane % 8)
+            set_frames = torch.where(src < n, order[src.clamp(max=n - 1)],
+                                     torch.full_like(src, -1)).to(_i32)
         col_of_frame = torch.empty(n, dtype=_i32, device=dev)
         real = set_frames >= 0
         col_of_frame[set_frames[real].long()] = k[real].to(_i32)

@@ -68,6 +68,7 @@ SIGNATURES = {
     'rspi_phase_proj_real': (I, [P, P, P, P, L, P]),
     'rspi_phase_refine': (I, [P, P, P, P, P, L, I, I, P]),
     'rspi_sets_counts': (I, [P, P, L, I, I, I, P, P]),
+    'rspi_sets_group': (I, [P, P, L, I, I, P, P, P]),
     'rspi_sets_steps': (I, [P, P, L, I, P, P, P]),
     'rspi_sets_fill': (I, [P, P, I, I, I, P, P, L, P, P, P, P]),
     'rspi_holo_quads32': (I, [P, L, L, P, P]),
@@ -140,7 +141,7 @@ KERNELS_PER_CALL = {
     'rspi_mean': 1, 'rspi_ll16_entry_rows': 1, 'rspi_ll16_entry_fill': 1, 'rspi_screen_candidates': 3, 'rspi_rescore': 5,
     'rspi_loglike_stream': 1, 'rspi_posterior_pairs': 3,
     'rspi_entries16_check': 1, 'rspi_emc_nll': 2, 'rspi_cdft2': 2, 'rspi_phase_support': 5,
-    'rspi_phase_proj_fourier': 1, 'rspi_phase_proj_real': 4, 'rspi_sets_counts': 1, 'rspi_sets_steps': 1,
+    'rspi_phase_proj_fourier': 1, 'rspi_phase_proj_real': 4, 'rspi_sets_counts': 1, 'rspi_sets_group': 1, 'rspi_sets_steps': 1,
     'rspi_sets_fill': 1, 'rspi_rot_log_slices_sets': 1, 'rspi_holo_quads32': 1, 'rspi_sets_part_sums_floats': 0,
     'rspi_screen_loglike_sets': 1, 'rspi_frame_max_finalize': 1,
     'rspi_screen_candidates_cols': 4, 'rspi_rescore_cols': 5, 'rspi_nll': 2, 'rspi_screen_candidates_noalloc': 3, 'rspi_merge_coverage': 1, 'rspi_merge': 2,

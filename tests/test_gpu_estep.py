@@ -421,9 +421,10 @@ def test_paired_holo_slices_bit_identical(dtype, code):
         assert a[1] == b[1] and a[1] > 0.
 
 
+@pytest.mark.parametrize('set_order', ['grouped', 'rank'])
 @pytest.mark.parametrize('parts,warps', [(None, 32), (2, 16), (3, 7), (4, 32)])
 @pytest.mark.parametrize('name,ds,need_scaling', CASES, ids=[c[0] for c in CASES])
-def test_sets_kernel_matches_stream_kernel(name, ds, need_scaling, parts, warps):
+def test_sets_kernel_matches_stream_kernel(name, ds, need_scaling, parts, warps, set_order):
     """The frame-set kernel (column parts copied in by TMA one after another,
     one lane per frame, running sums per column between parts, the
     likelihood columns in set order) gives FP32 likelihoods within the
@@ -442,7 +443,8 @@ def test_sets_kernel_matches_stream_kernel(name, ds, need_scaling, parts, warps)
     ref.reduce()
     want = ref.frame_prob().cpu().numpy()
     out = {}
-    for kernel, tile, kw in (('stream', 2, {}), ('sets', 4, dict(screen_parts=parts))):
+    for kernel, tile, kw in (('stream', 2, {}),
+                             ('sets', 4, dict(screen_parts=parts, set_order=set_order))):
         ph = _photons(ds, need_scaling)
         es = _estep(ph, size, num_rot, sx, sy, dia, ds['bg'], form='screen', kernel=kernel,
                     states_per_tile=tile, warps=warps, **kw)
@@ -472,8 +474,9 @@ def test_sets_kernel_matches_stream_kernel(name, ds, need_scaling, parts, warps)
     np.testing.assert_allclose(a[3], b[3], rtol=1e-12)
 
 
+@pytest.mark.parametrize('set_order', ['grouped', 'rank'])
 @pytest.mark.parametrize('n,parts', [(61, 1), (300, 2), (45, 3), (33, 4)])
-def test_sets_layout_entries(n, parts):
+def test_sets_layout_entries(n, parts, set_order):
     """Frame sets: every frame's photons of each column part once, in its own
     lane, within its quarter warp's first D_q steps, D_q the fewest any
     schedule needs (its largest frame or class total), in which the eight
@@ -481,8 +484,9 @@ def test_sets_layout_entries(n, parts):
     a photon holding the zero column of the slot's class; from step D_q on
     lane 8 q + f holds zero column f; the quarter warp's own group count is
     ceil(D_q / 4) and each (set, part) range has the largest of the four;
-    frames in decreasing photon order, rank 32 s + p + 4 f in lane 8 p + f;
-    column of frame d = its slot."""
+    frames in decreasing photon order, grouped as the host restatement of
+    rspi_sets_group groups them (set_order 'grouped') or rank 32 s + p + 4 f
+    in lane 8 p + f ('rank'); column of frame d = its slot."""
     size = 37
     d = random_photons(size, n, 40. * size, 15, empty_frames=(2, 9), heavy=5)
     ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
@@ -490,7 +494,7 @@ def test_sets_layout_entries(n, parts):
     sx, sy, dia, _ = E.generate_states(E.parse_triple('0 0 1'), E.parse_triple('0 0 1'),
                                        E.parse_triple('2 2 1'))
     es = _estep(_photons(ds, False), size, 3, sx, sy, dia, ds['bg'], form='screen',
-                kernel='sets', screen_parts=parts)
+                kernel='sets', screen_parts=parts, set_order=set_order)
     torch.cuda.synchronize()
     w = es.wide
     pw, ns = w['part_w'], w['n_sets']
@@ -504,8 +508,18 @@ def test_sets_layout_entries(n, parts):
     tot = np.array([p.size for p in photons])
     order = np.argsort(-tot, kind='stable')
     k = np.arange(ns * 32)
-    src = (k - k % 32) + (k % 32) // 8 + 4 * (k % 8)
-    want_sf = np.where(src < n, order[np.minimum(src, n - 1)], -1)
+    if set_order == 'rank':
+        src = (k - k % 32) + (k % 32) // 8 + 4 * (k % 8)
+        want_sf = np.where(src < n, order[np.minimum(src, n - 1)], -1)
+    else:
+        from rspi.device import SETS_SWEEPS
+        from sets_group_ref import group_frames
+        cnt = np.zeros((n, 32), np.int64)
+        for fr, ph in enumerate(photons):
+            for h in range(parts):
+                cnt[fr, 8 * h:8 * h + 8] = np.bincount(ph[ph // pw == h] % pw % 8, minlength=8)
+        assert np.array_equal(cnt, w['counts'].cpu().numpy().reshape(n, 32))
+        want_sf = group_frames(cnt, order, parts, SETS_SWEEPS)
     assert np.array_equal(sf, want_sf)
     assert np.array_equal(cof[sf[sf >= 0]], k[sf >= 0])
     for s in range(ns):

@@ -438,6 +438,12 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
 
     const double kmean = pc.ksum / dn;
     const double rescale = ring ? 0. : rescale_ptr[mode];
+    // screen bound constants: the main pass's rho is the ring's mean rescale
+    // for every candidate, so its log is taken once per pixel; the bound
+    // multiplies by 1/dn (at most two ulps of q and e beyond the divisions,
+    // far inside its 2^-40 term)
+    const double inv_dn = 1. / dn;
+    const double lr_main = ring ? 0. : log(rescale);
     double2 f = fconv[t];
     double step = hypot(f.x, f.y) / 4.;
     const double shrink = 33. / 5.;  // sqrt(1089) / 5, maxLP.py:177
@@ -546,14 +552,14 @@ k_pattern(double2 *__restrict__ fconv, const int *__restrict__ pixels,
                             amax >= 0x1p-38 && amax <= 0x1p60 && rho > 0. && rho < INFINITY &&
                             isfinite(mwv);
                 if (safe) {
-                    const double lr = log(rho);
-                    const double q = (ksum * lr + LN2 * (a64[k] + e2 * ksum)) / dn - rho * mwv;
+                    const double lr = ring ? log(rho) : lr_main;
+                    const double q = (ksum * lr + LN2 * (a64[k] + e2 * ksum)) * inv_dn - rho * mwv;
                     const double b2 = ksum * (LG2_EA + 9.5 * U32) +
                                       (LG2_ER + G_CHUNK) * (1. + G_CHUNK) * b64[k];
                     const double fm = 0x1p-40 * ((ksum * (fabs(lr) + LN2 * fabs(e2) + 1.) +
-                                                  LN2 * 1.01 * b64[k]) / dn +
+                                                  LN2 * 1.01 * b64[k]) * inv_dn +
                                                  fabs(rho * mwv));
-                    const double e = 1.001 * LN2 * b2 / dn + fm;
+                    const double e = 1.001 * LN2 * b2 * inv_dn + fm;
                     safe = isfinite(q) && isfinite(e);
                     lo[k] = q - e;
                     up[k] = q + e;

@@ -18,7 +18,7 @@ def test_write_inputs_config(tmp_path, rank):
     w = bench.workload(1, 8)
     data = bench.generate_data(1, w)
     cfg = bench.write_inputs(str(tmp_path), w, data, 'screen', 2.5, 20., 'sets', 'pattern',
-                             False, rank=rank, slice_math='fp32')
+                             False, rank=rank, slice_math='fp32', set_order='rank')
     c = configparser.ConfigParser()
     c.read(cfg)
     e = c['emc']
@@ -30,6 +30,7 @@ def test_write_inputs_config(tmp_path, rank):
     assert e['form'] == 'screen' and float(e['slice_budget_gb']) == 2.5
     assert float(e['screen_delta']) == 20.
     assert e['kernel'] == 'sets' and e['mstep'] == 'pattern' and e['slice_math'] == 'fp32'
+    assert e['set_order'] == 'rank'
     assert e['autotune'] == 'False'
     if rank is None:
         assert e['in_photons_file'] == 'photons.npz'

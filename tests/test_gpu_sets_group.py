@@ -70,3 +70,26 @@ def test_grouping_flags_frames_outside_the_dataset():
     got, err = _gpu_group(c, order, 1, 1)
     assert err == -2   # RSPI_ERR_INDEX (include/rspi.h)
     assert 64 not in got and (got == -1).sum() == 1
+
+
+def test_emc_set_order_option_gives_the_same_iteration(tmp_path):
+    """[emc] set_order = grouped / rank: the screened likelihood columns are
+    grouped differently, the FP64-rescored argmax and the model after the
+    M-step are the same bits."""
+    import os
+    from emc import EMC
+    from helpers import load_golden, write_case
+    g = load_golden('case_b')
+    out = {}
+    for order in ('grouped', 'rank'):
+        cfg = write_case(os.path.join(str(tmp_path), order), g,
+                         extra='form = screen\nkernel = sets\nset_order = %s\n' % order)
+        rec = EMC(cfg)
+        assert rec.estep.set_order == order
+        rec.model = g['model_in_1'].copy()
+        rec.run_iteration(None)
+        out[order] = (rec.model.copy(), rec.rmax.copy())
+    a, b = out['grouped'], out['rank']
+    assert np.array_equal(a[1], b[1])
+    assert np.array_equal(np.ascontiguousarray(a[0]).view(np.uint8),
+                          np.ascontiguousarray(b[0]).view(np.uint8))

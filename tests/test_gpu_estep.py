@@ -639,6 +639,8 @@ def test_one_pass_candidates_equal_two_pass(delta):
         outs.append((off.cpu().numpy(), cd[:total].cpu().numpy(), cr[:total].cpu().numpy()))
     for a, b in zip(*outs):
         assert np.array_equal(a, b)
+    off, cd, _ = outs[0]
+    assert np.array_equal(cd, np.repeat(np.arange(n), np.diff(off)))
     if delta >= 20.:
         # some frames took the second scan
         assert (np.diff(outs[0][0]) > 32).any() or delta == 20.
@@ -724,3 +726,53 @@ def test_sets_kernel_beyond_tensor_memory_sets(parts):
     assert np.all(err <= eps), (worst, err[worst], eps[worst])
     assert np.array_equal(rmax.cpu().numpy(), rmax64.cpu().numpy())
     np.testing.assert_allclose(maxll.cpu().numpy(), maxll64.cpu().numpy(), rtol=1e-14)
+
+
+@pytest.mark.parametrize('delta', [0., 20.])
+def test_candidates_many_rows(delta):
+    """18 states x 180 rotations (3,240 likelihood rows), frames in set
+    order: the one-pass selection gives the second scan's lists, and the
+    rescored argmax and maximum equal the FP64 form's; the log-sum-exp too,
+    to 1e-12 with a 20-nat window, and within the FP32 error of the
+    non-candidates' terms (1e-7) with the argmax alone."""
+    from rspi.device import cur_stream, ptr
+    from rspi.lib import call
+    size, n, num_rot = 37, 300, 180
+    d = random_photons(size, n, 30. * size, 41, empty_frames=(3,), heavy=7)
+    ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
+                         d['count_multi'], size * size, True)
+    sx, sy, dia, _ = E.generate_states(E.parse_triple('-1 1 3'), E.parse_triple('-1 1 3'),
+                                       E.parse_triple('2 3 2'))
+    rng = np.random.default_rng(5)
+    model = torch.from_numpy(rng.random(size * size) + 1j * rng.random(size * size)).cuda()
+    es = _estep(_photons(ds, True), size, num_rot, sx, sy, dia, ds['bg'], form='screen',
+                kernel='sets', delta=delta)
+    ref = _estep(_photons(ds, True), size, num_rot, sx, sy, dia, ds['bg'], form='fp64')
+    assert es.n_rows == 3240
+    es.run(model)
+    ref.run(model)
+    maxll, rmax, logz = es.reduce()
+    ref.reduce()
+    torch.cuda.synchronize()
+    assert np.array_equal(rmax.cpu().numpy(), ref.rmax.cpu().numpy())
+    np.testing.assert_allclose(maxll.cpu().numpy(), ref.maxll.cpu().numpy(), rtol=1e-15)
+    np.testing.assert_allclose(logz.cpu().numpy(), ref.logz.cpu().numpy(),
+                               rtol=1e-12 if delta >= 20. else 1e-7)
+    outs = []
+    for slot in (es.cand_slot, None):
+        cand_n = torch.empty(n, dtype=torch.int32, device='cuda')
+        off = torch.empty(n + 1, dtype=torch.int64, device='cuda')
+        cd = torch.full((es.capacity,), -7, dtype=torch.int32, device='cuda')
+        cr = torch.full((es.capacity,), -7, dtype=torch.int32, device='cuda')
+        call('rspi_screen_candidates_cols', ptr(es.prob), es.n_rows, es.n_cols,
+             ptr(es.frame_of_col), n, ptr(es.max32), ptr(es.rmax32),
+             ptr(es.ll['frame_sel_photons']), ptr(es._eps_rows()), ptr(es.lmax), es.delta,
+             ptr(es.cnt_part), ptr(cand_n), ptr(es.noncand), ptr(es.thr), ptr(off),
+             es.capacity, ptr(cd), ptr(cr), ptr(slot), ptr(es.ph.err.t), cur_stream())
+        torch.cuda.synchronize()
+        es.ph.err.check('candidates')
+        total = int(off[n])
+        outs.append((off.cpu().numpy(), cd[:total].cpu().numpy(), cr[:total].cpu().numpy()))
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+    assert int(outs[0][0][-1]) >= n   # at least each frame's argmax

@@ -415,7 +415,7 @@ int rspi_screen_candidates_cols(const float *ll, long long n_rows, long long n_c
  * row_cand_off[n_rows + 1], row_cand[capacity]); one CTA computes a row's
  * FP64 rotated slice (p_pad values, as rspi_rot_log_slices) in shared
  * memory and rescores that row's candidate frames.  A row too long for
- * shared memory (p_pad * 8 bytes above 226 KB) is built in row_scratch
+ * shared memory (p_pad * 8 bytes above 220 KB) is built in row_scratch
  * instead (scratch_rows x p_pad doubles, one slot per CTA; required then,
  * ignored otherwise). */
 int rspi_rescore(const int *cand_d, const int *cand_r, const long long *cand_off,

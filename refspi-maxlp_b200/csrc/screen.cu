@@ -320,12 +320,86 @@ __global__ void k_row_scatter(const int *__restrict__ cand_r, const long long *_
     }
 }
 
+// A "direct" row: at most DIRECT_MAX candidates whose entry slots together
+// read no more values than the row holds.  Its candidates are evaluated by
+// k_rescore_direct, one warp per candidate anywhere on the GPU, each value
+// computed with rot_log_value where the sum reads it; k_rescore_rows skips
+// the row.  (With about one candidate per row, the argmax-only window's
+// usual case, a CTA per row kept one warp of the SM busy.)
+constexpr int DIRECT_MAX = 4;
+
+__device__ __forceinline__ bool row_direct(long long r, const long long *__restrict__ row_off,
+                                           const int *__restrict__ row_cand,
+                                           const int *__restrict__ cand_d,
+                                           const long long *__restrict__ row_off32,
+                                           long long p_pad) {
+    const long long a = row_off[r], b = row_off[r + 1];
+    if (a == b || b - a > DIRECT_MAX) return false;
+    long long wk = 0;
+    for (long long i = a; i < b; ++i) {
+        const int d = cand_d[row_cand[i]];
+        wk += (row_off32[d + 1] - row_off32[d]) * 32;
+    }
+    return wk <= p_pad;
+}
+
+// One warp per candidate pair of a direct row: the FP64 form's sum (per
+// lane over the frame's packed rows, fma(count, L, acc), then the warp
+// reduction) with each value from rot_log_value, the same bits as the row
+// kernel's.
+__global__ void __launch_bounds__(256)
+k_rescore_direct(const int *__restrict__ cand_d, const int *__restrict__ cand_r,
+                 const long long *__restrict__ total_ptr, long long capacity,
+                 const long long *__restrict__ row_off, const int *__restrict__ row_cand,
+                 const double *__restrict__ holo, long long num_rot,
+                 const double *__restrict__ rot_cs, int size, const double *__restrict__ bg,
+                 const int *__restrict__ sel_pix, long long n_sel, long long p_pad,
+                 const double *__restrict__ init, const double *__restrict__ scales,
+                 const unsigned int *__restrict__ ent32, const long long *__restrict__ row_off32,
+                 double *__restrict__ cand_ll, float *__restrict__ ll32, long long ll_stride,
+                 const int *__restrict__ col_of_frame) {
+    const long long total = min(*total_ptr, capacity);
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long npix = (long long)size * size;
+    const float inv_size = 1.f / (float)size;
+    for (long long i = warp; i < total; i += nwarp) {
+        const long long r = cand_r[i];
+        if (!row_direct(r, row_off, row_cand, cand_d, row_off32, p_pad)) continue;   // per warp
+        const int d = cand_d[i];
+        const long long s0 = r / num_rot, j = r - s0 * num_rot;
+        const double ac = rot_cs[2 * j], as = rot_cs[2 * j + 1];
+        const double *w = holo + s0 * npix;
+        double acc = 0.;
+        const unsigned *ep = ent32 + row_off32[d] * 32 + lane;
+        for (long long q = row_off32[d]; q < row_off32[d + 1]; ++q, ep += 32) {
+            const unsigned e = __ldg(ep);
+            const unsigned c = e >> 16;
+            double v = 0.;
+            if (c < (unsigned)n_sel) {
+                const int p = sel_pix[c];
+                int x, y;
+                pixel_xy(p, size, inv_size, x, y);
+                v = rot_log_value(w, x, y, size, ac, as, bg[p]);
+            }
+            acc = fma((double)(e & 0xffffu), v, acc);
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) {
+            const double v = init[s0] * scales[d] + acc;
+            cand_ll[i] = v;
+            ll32[r * ll_stride + (col_of_frame ? col_of_frame[d] : d)] = (float)v;
+        }
+    }
+}
+
 // One CTA per likelihood row with candidates: the row's FP64 rotated slice
 // is computed into shared memory with rot_log_value (as k_rot_log_js does),
 // then each warp rescores candidate frames exactly as the FP64 form sums
 // them (per lane over the frame's packed rows, fma(count, L, acc), then the
 // warp reduction), so every value equals the FP64 form's.  A row longer than
-// shared memory holds (GROW: more than ~28,900 likelihood pixels) is built
+// shared memory holds (GROW: more than ~28,100 likelihood pixels) is built
 // in the CTA's slot of a global scratch array instead and gathered through
 // L1/L2; the arithmetic is the same.  A shared-memory row whose
 // candidates' warps read fewer values each than the CTA's threads would
@@ -350,9 +424,32 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
     const unsigned cmax = (unsigned)p_pad - 1;
     const float inv_size = 1.f / (float)size;
     __shared__ long long s_work;
-    for (long long r = blockIdx.x; r < n_rows; r += gridDim.x) {
+    __shared__ int s_rows[1024], s_cnt[32];
+    const long long step = gridDim.x;
+    // the CTA's rows r = blockIdx.x + k gridDim.x, taken blockDim.x at a
+    // time: each thread tests one (empty rows and k_rescore_direct's rows
+    // are skipped) and the rows to build are listed in row order
+    for (long long base = blockIdx.x; base < n_rows; base += step * blockDim.x) {
+    const long long rt = base + (long long)threadIdx.x * step;
+    bool build = false;
+    if (rt < n_rows) {
+        build = row_off[rt] != row_off[rt + 1];
+        if (!GROW && build) build = !row_direct(rt, row_off, row_cand, cand_d, row_off32, p_pad);
+    }
+    __syncthreads();            // the previous list's readers are done
+    const unsigned bal = __ballot_sync(RSPI_FULL_MASK, build);
+    if (lane == 0) s_cnt[wid] = __popc(bal);
+    __syncthreads();
+    int before = 0, n_build = 0;
+    for (int k = 0; k < nw; ++k) {
+        if (k < wid) before += s_cnt[k];
+        n_build += s_cnt[k];
+    }
+    if (build) s_rows[before + __popc(bal & ((1u << lane) - 1u))] = (int)rt;
+    __syncthreads();
+    for (int kr = 0; kr < n_build; ++kr) {
+        const long long r = s_rows[kr];
         const long long a = row_off[r], b = row_off[r + 1];
-        if (a == b) continue;   // uniform across the CTA
         const long long s0 = r / num_rot, j = r - s0 * num_rot;
         const double ac = rot_cs[2 * j], as = rot_cs[2 * j + 1];
         const double *w = holo + s0 * npix;
@@ -456,6 +553,7 @@ k_rescore_rows(const long long *__restrict__ row_off, const int *__restrict__ ro
                 }
             }
         }
+    }
     }
 }
 
@@ -640,7 +738,7 @@ static int rescore_launch(const int *cand_d, const int *cand_r, const long long 
         p_pad < n_sel || p_pad % 32 || p_pad > 65536)
         return RSPI_ERR_ARG;
     const size_t smem = (size_t)p_pad * sizeof(double);
-    const bool grow = smem > (size_t)SMEM_LIMIT - 1024;
+    const bool grow = smem > (size_t)SMEM_LIMIT - 7 * 1024;   // 220 KB: with the static row list
     if (grow && (!row_scratch || scratch_rows < 1)) return RSPI_ERR_ARG;
     static RspiSmemOptIn optin;
     if (!grow && !rspi_smem_optin((const void *)k_rescore_rows<false>, smem, optin))
@@ -660,6 +758,10 @@ static int rescore_launch(const int *cand_d, const int *cand_r, const long long 
             sel_pix, n_sel, p_pad, init, scales, entries32, row_off32, cand_ll, ll32, ll_stride,
             col_of_frame, row_scratch);
     } else {
+        k_rescore_direct<<<rspi_sm_count() * 8, 256, 0, stream>>>(
+            cand_d, cand_r, total, capacity, row_cand_off, row_cand, holo, num_rot, rot_cs,
+            (int)size, bg, sel_pix, n_sel, p_pad, init, scales, entries32, row_off32, cand_ll,
+            ll32, ll_stride, col_of_frame);
         const int per_sm = max(1, (int)(SMEM_LIMIT / (smem + 1024)));
         const unsigned grid = (unsigned)min((long long)rspi_sm_count() * min(per_sm, 2), n_rows);
         k_rescore_rows<false><<<grid, 1024 / min(per_sm, 2), smem, stream>>>(

@@ -639,7 +639,7 @@ class EStep:
         """Global rows for FP64 rescoring when a row exceeds shared memory
         (one per SM; none otherwise)."""
         self.row_scratch, self.scratch_rows = None, 0
-        if self.p_pad * 8 > 226 * 1024:
+        if self.p_pad * 8 > 220 * 1024:
             sms = torch.cuda.get_device_properties(self.device).multi_processor_count
             self.scratch_rows = int(sms)
             self.row_scratch = torch.empty((sms, self.p_pad), dtype=_f64, device=self.device)

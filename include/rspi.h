@@ -504,6 +504,29 @@ int rspi_maxlp_histogram(const int *ones, const int *multi, const long long *one
                          long long size, const int *mask_idx, long long n_mask,
                          long long n_ref, int *hist, int *err, cudaStream_t stream);
 
+/* The same histogram from a table built once per rotation table (what the
+ * library's M-step uses).  rspi_maxlp_pixel_map lists, for each rotation j
+ * of rot_cs and detector pixel p, the phaser rows m whose pixel maps onto p
+ * (on an even detector a map onto column `size` of row x is listed under
+ * pixel (x + 1, 0), as rspi_maxlp_histogram aliases it): rows
+ * map_rows[map_off[j * size^2 + p] .. map_off[j * size^2 + p + 1]), in no
+ * particular order.  Scratch cnt: num_rot * size^2 ints; map_off:
+ * num_rot * size^2 + 1; map_rows: num_rot * n_mask (each pixel maps to one
+ * detector pixel per rotation at most).  rspi_maxlp_histogram_map adds each
+ * photon of frame d to the rows listed under its pixel for rotation
+ * frot[d]: the same integer sums as rspi_maxlp_histogram (hist zeroed by
+ * the caller; a rotation outside [0, num_rot) or a pixel outside the
+ * detector sets *err = RSPI_ERR_INDEX). */
+int rspi_maxlp_pixel_map(const double *rot_cs, long long num_rot, long long size,
+                         const int *mask_idx, int *cnt, long long *map_off, int *map_rows,
+                         cudaStream_t stream);
+int rspi_maxlp_histogram_map(const int *ones, const int *multi, const long long *ones_accum,
+                             const long long *multi_accum, const int *place_ones,
+                             const int *place_multi, const int *count_multi, long long n_data,
+                             const int *fstate, const int *frot, long long num_rot,
+                             long long size, const long long *map_off, const int *map_rows,
+                             long long n_ref, int *hist, int *err, cudaStream_t stream);
+
 /* Pattern search of a set of model pixels (maxLP.py:154-197): for each pixel
  * t = pixels[i] (its histogram row hist_row[i]) run <= num_iter iterations over
  * the 33x33 candidate grid.  rescale_mode 0: per-candidate rescale

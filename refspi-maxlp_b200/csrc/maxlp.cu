@@ -107,6 +107,97 @@ k_histogram(const int *__restrict__ ones, const int *__restrict__ multi,
     }
 }
 
+// The same histogram from a table built once per rotation table: for each
+// rotation j and detector pixel p, the phaser rows whose pixel's forward
+// map lands on p (the 3 x 3 search of scatter_photon finds exactly these,
+// since such pixels lie within 1/sqrt(2) px of p's inverse image).  A pixel
+// whose map lands on column `size` of row x (even sizes) is listed under
+// pixel (x + 1, 0), as scatter_photon aliases it.  Per photon the histogram
+// then reads its table range instead of nine forward maps.
+__device__ __forceinline__ long long map_key(int tx, int ty, double c, double s, int size) {
+    int ox, oy;
+    forward_pixel(tx, ty, c, s, size, ox, oy);
+    if (ox >= 0 && ox < size && oy >= 0 && oy < size) return (long long)ox * size + oy;
+    if ((size % 2) == 0 && oy == size && ox >= 0 && ox + 1 < size)
+        return (long long)(ox + 1) * size;
+    return -1;
+}
+
+__global__ void k_pixel_map_count(const double *__restrict__ rot_cs, long long num_rot, int size,
+                                  const int *__restrict__ mask_idx, int *__restrict__ cnt) {
+    const long long npix = (long long)size * size;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < num_rot * npix;
+         i += stride) {
+        const long long j = i / npix, t = i - j * npix;
+        if (mask_idx[t] < 0) continue;
+        const long long key = map_key((int)(t / size), (int)(t % size), rot_cs[2 * j],
+                                      rot_cs[2 * j + 1], size);
+        if (key >= 0) atomicAdd(&cnt[j * npix + key], 1);
+    }
+}
+
+__global__ void k_pixel_map_fill(const double *__restrict__ rot_cs, long long num_rot, int size,
+                                 const int *__restrict__ mask_idx,
+                                 const long long *__restrict__ off, int *__restrict__ cursor,
+                                 int *__restrict__ rows) {
+    const long long npix = (long long)size * size;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < num_rot * npix;
+         i += stride) {
+        const long long j = i / npix, t = i - j * npix;
+        const int m = mask_idx[t];
+        if (m < 0) continue;
+        const long long key = map_key((int)(t / size), (int)(t % size), rot_cs[2 * j],
+                                      rot_cs[2 * j + 1], size);
+        if (key < 0) continue;
+        const long long k = j * npix + key;
+        rows[off[k] + atomicAdd(&cursor[k], 1)] = m;   // order within a pixel: any (integer sums)
+    }
+}
+
+__global__ void __launch_bounds__(256)
+k_histogram_map(const int *__restrict__ ones, const int *__restrict__ multi,
+                const long long *__restrict__ ones_accum, const long long *__restrict__ multi_accum,
+                const int *__restrict__ place_ones, const int *__restrict__ place_multi,
+                const int *__restrict__ count_multi, long long n, const int *__restrict__ fstate,
+                const int *__restrict__ frot, long long num_rot, int size,
+                const long long *__restrict__ map_off, const int *__restrict__ map_rows,
+                long long n_ref, int *__restrict__ hist, int *err) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
+    const long long npix = (long long)size * size;
+    for (long long d = warp; d < n; d += nwarp) {
+        const int st = fstate[d];
+        if (st < 0) continue;
+        const int j = frot[d];
+        if (j < 0 || j >= num_rot) {
+            rspi_flag(err, RSPI_ERR_INDEX);
+            continue;
+        }
+        const long long *off = map_off + (long long)j * npix;
+        const int n_o = ones[d], n_m = multi[d];
+        const long long oa = ones_accum[d], ma = multi_accum[d];
+        for (int i = lane; i < n_o + n_m; i += 32) {
+            int p, cnt;
+            if (i < n_o) {
+                p = place_ones[oa + i];
+                cnt = 1;
+            } else {
+                p = place_multi[ma + i - n_o];
+                cnt = count_multi[ma + i - n_o];
+            }
+            if (p < 0 || p >= npix) {
+                rspi_flag(err, RSPI_ERR_INDEX);
+                continue;
+            }
+            for (long long e = off[p]; e < off[p + 1]; ++e)
+                atomicAdd(&hist[(long long)map_rows[e] * n_ref + st], cnt);
+        }
+    }
+}
+
 // Reference-sphere amplitude at pixel (qx, qy, qrad) for state (sx, sy, dia),
 // maxLP.py:238-243: ff(pi qrad dia) exp(2 pi i (qx sx + qy sy)).
 __device__ __forceinline__ double2 fref_value(double qx, double qy, double qrad, double sx,
@@ -995,6 +1086,41 @@ extern "C" int rspi_maxlp_histogram(const int *ones, const int *multi,
     k_histogram<<<rspi_blocks(n_data * 32, 256), 256, 0, stream>>>(
         ones, multi, ones_accum, multi_accum, place_ones, place_multi, count_multi, n_data,
         fstate, frot, rot_cs, (int)size, mask_idx, n_ref, hist, err);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_maxlp_pixel_map(const double *rot_cs, long long num_rot, long long size,
+                                    const int *mask_idx, int *cnt, long long *map_off,
+                                    int *map_rows, cudaStream_t stream) {
+    if (!rot_cs || !mask_idx || !cnt || !map_off || !map_rows || num_rot <= 0 || size <= 1 ||
+        size > 46340 || num_rot * size * size > 0x7fffffffLL)
+        return RSPI_ERR_ARG;
+    const long long n = num_rot * size * size;
+    const unsigned grid = rspi_blocks(n, 256);
+    cudaMemsetAsync(cnt, 0, sizeof(int) * n, stream);
+    k_pixel_map_count<<<grid, 256, 0, stream>>>(rot_cs, num_rot, (int)size, mask_idx, cnt);
+    const int st = rspi_scan_rows(cnt, n, map_off, stream);
+    if (st != RSPI_OK) return st;
+    cudaMemsetAsync(cnt, 0, sizeof(int) * n, stream);
+    k_pixel_map_fill<<<grid, 256, 0, stream>>>(rot_cs, num_rot, (int)size, mask_idx, map_off,
+                                               cnt, map_rows);
+    RSPI_RETURN_LAUNCH();
+}
+
+extern "C" int rspi_maxlp_histogram_map(const int *ones, const int *multi,
+                                        const long long *ones_accum, const long long *multi_accum,
+                                        const int *place_ones, const int *place_multi,
+                                        const int *count_multi, long long n_data,
+                                        const int *fstate, const int *frot, long long num_rot,
+                                        long long size, const long long *map_off,
+                                        const int *map_rows, long long n_ref, int *hist, int *err,
+                                        cudaStream_t stream) {
+    if (n_data <= 0 || size <= 1 || size > 46340 || num_rot <= 0 || n_ref <= 0 || !hist ||
+        !map_off || !map_rows || !fstate || !frot)
+        return RSPI_ERR_ARG;
+    k_histogram_map<<<rspi_blocks(n_data * 32, 256), 256, 0, stream>>>(
+        ones, multi, ones_accum, multi_accum, place_ones, place_multi, count_multi, n_data,
+        fstate, frot, num_rot, (int)size, map_off, map_rows, n_ref, hist, err);
     RSPI_RETURN_LAUNCH();
 }
 

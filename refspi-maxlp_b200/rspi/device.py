@@ -28,6 +28,8 @@ QUAD4_SMEM = 227 * 1024 - 1024   # shared bytes of the four-row tile (kernel lim
 QUAD4_MAX_PARTS = 4              # column parts of the four-row tile
 QUAD4_COLS = (QUAD4_SMEM // 16 - 8) // 8 * 8   # most columns of one part
 SETS_SWEEPS = 4                  # pair sweeps of the frame grouping (rspi_sets_group)
+PIXEL_MAP_MAX_ROT = 1024         # rotation tables the M-step's pixel map serves
+PIXEL_MAP_MAX = 1 << 26          # (rotation, detector pixel) entries of that map
 
 
 def quad4_parts(p_row, parts=None):
@@ -963,6 +965,22 @@ class MStep:
     def set_frame_params(self, fstate, frot, nstate):
         self.fstate, self.frot, self.nstate = fstate, frot, nstate
 
+    def pixel_map(self, rot_cs):
+        """Per rotation of ``rot_cs`` and detector pixel, the phaser rows whose
+        pixel maps onto it (rspi_maxlp_pixel_map), built once per rotation
+        table."""
+        key = (rot_cs.data_ptr(), tuple(rot_cs.shape))
+        if getattr(self, '_pixel_map', None) is not None and self._pixel_map[0] == key:
+            return self._pixel_map[1], self._pixel_map[2]
+        num_rot, npix, dev = int(rot_cs.shape[0]), self.size * self.size, self.device
+        cnt = torch.empty(num_rot * npix, dtype=_i32, device=dev)
+        off = torch.empty(num_rot * npix + 1, dtype=_i64, device=dev)
+        rows = torch.empty(max(1, num_rot * self.n_hist_rows), dtype=_i32, device=dev)
+        call('rspi_maxlp_pixel_map', ptr(rot_cs), num_rot, self.size, ptr(self.mask_idx),
+             ptr(cnt), ptr(off), ptr(rows), cur_stream())
+        self._pixel_map = (key, off, rows, rot_cs)   # rot_cs kept alive: the key is its address
+        return off, rows
+
     def histogram(self, n_cols, rot_cs):
         """Photons of every phaser pixel per reference state (a11):
         ``n_hist_rows`` x ``n_cols`` int32, from the current frame parameters."""
@@ -972,10 +990,22 @@ class MStep:
         hist = self.hist[:max(1, need)]
         hist.zero_()
         ph = self.ph
-        call('rspi_maxlp_histogram', ptr(ph.ones), ptr(ph.multi), ptr(ph.ones_accum), ptr(ph.multi_accum),
-            ptr(ph.place_ones), ptr(ph.place_multi), ptr(ph.count_multi), ph.num_data,
-            ptr(self.fstate), ptr(self.frot), ptr(rot_cs), self.size, ptr(self.mask_idx),
-            self.n_hist_rows, n_cols, ptr(hist), ptr(ph.err.t), cur_stream())
+        num_rot = int(rot_cs.shape[0])
+        if num_rot <= PIXEL_MAP_MAX_ROT and num_rot * self.size ** 2 <= PIXEL_MAP_MAX:
+            # a table of the rotations' pixel maps, built once per rotation
+            # table (the EMC's fixed angles)
+            off, rows = self.pixel_map(rot_cs)
+            call('rspi_maxlp_histogram_map', ptr(ph.ones), ptr(ph.multi), ptr(ph.ones_accum),
+                 ptr(ph.multi_accum), ptr(ph.place_ones), ptr(ph.place_multi),
+                 ptr(ph.count_multi), ph.num_data, ptr(self.fstate), ptr(self.frot), num_rot,
+                 self.size, ptr(off), ptr(rows), n_cols, ptr(hist), ptr(ph.err.t), cur_stream())
+        else:
+            # one rotation per frame (the phaser's own angles): the search per photon
+            call('rspi_maxlp_histogram', ptr(ph.ones), ptr(ph.multi), ptr(ph.ones_accum),
+                 ptr(ph.multi_accum), ptr(ph.place_ones), ptr(ph.place_multi),
+                 ptr(ph.count_multi), ph.num_data, ptr(self.fstate), ptr(self.frot), ptr(rot_cs),
+                 self.size, ptr(self.mask_idx), self.n_hist_rows, n_cols, ptr(hist),
+                 ptr(ph.err.t), cur_stream())
         if self.shard is not None:
             # sums over every rank's frames: the histogram of the whole dataset
             self.shard.reduce_histogram(hist, self.nstate)

@@ -33,6 +33,8 @@ SIGNATURES = {
     'rspi_frame_reduce': (I, [P, I, L, L, P, P, P, P]),
     'rspi_maxlp_frame_params': (I, [P, L, L, L, P, P, P, P, P]),
     'rspi_maxlp_histogram': (I, [P, P, P, P, P, P, P, L, P, P, P, L, P, L, L, P, P, P]),
+    'rspi_maxlp_pixel_map': (I, [P, L, L, P, P, P, P, P]),
+    'rspi_maxlp_histogram_map': (I, [P, P, P, P, P, P, P, L, P, P, L, L, P, P, L, P, P, P]),
     'rspi_maxlp_pattern': (I, [P, P, P, L, P, L, P, L, P, L, I, P, I, P, P]),
     'rspi_maxlp_pattern_screened': (I, [P, P, P, L, P, L, P, L, P, L, I, P, I, P, P, P]),
     'rspi_log2_error_max': (I, [F, F, P, P]),
@@ -133,7 +135,8 @@ KERNELS_PER_CALL = {
     'rspi_ll_entry_fill': 1, 'rspi_holo_slices': 1, 'rspi_vscale_init': 1,
     'rspi_rot_log_slices': 1, 'rspi_holo_pairs': 1, 'rspi_rot_log_slices_pairs': 1,
     'rspi_loglike': 1, 'rspi_frame_reduce': 1,
-    'rspi_maxlp_frame_params': 1, 'rspi_maxlp_histogram': 1, 'rspi_maxlp_pattern': 1,
+    'rspi_maxlp_frame_params': 1, 'rspi_maxlp_histogram': 1, 'rspi_maxlp_pixel_map': 3,
+    'rspi_maxlp_histogram_map': 1, 'rspi_maxlp_pattern': 1,
     'rspi_maxlp_pattern_screened': 1, 'rspi_log2_error_max': 1,
     'rspi_maxlp_pixel_frames': 1, 'rspi_maxlp_pixel_values': 1, 'rspi_maxlp_fcalc': 1,
     'rspi_sphere_ramp': 1, 'rspi_quad4_entry_groups': 1, 'rspi_quad4_entry_fill': 2,

@@ -213,3 +213,46 @@ def test_emc_adjoint_driven_mstep(tmp_path, kind):
     rec.run_iteration(2)
     assert rec._graph is not None
     assert np.all(np.isfinite(rec.model))
+
+
+@pytest.mark.parametrize('size,n,num_rot', [(20, 200, 12), (37, 300, 180), (24, 150, 7)])
+def test_pixel_map_histogram_equals_search(size, n, num_rot):
+    """The histogram from the per-rotation pixel map (rspi_maxlp_pixel_map +
+    rspi_maxlp_histogram_map) equals the per-photon search's
+    (rspi_maxlp_histogram) bit for bit, even detectors (the column-`size`
+    alias) included, and the oracle's photons per pixel."""
+    from rspi import geometry
+    from rspi.device import MStep, cur_stream, ptr
+    from rspi.lib import check
+    from helpers import random_photons
+    d = random_photons(size, n, 40. * size, size + n, empty_frames=(1,))
+    ds = E.parse_photons(d['ones'], d['multi'], d['place_ones'], d['place_multi'],
+                         d['count_multi'], size * size, False)
+    rng = np.random.default_rng(size)
+    n_ref = 5
+    rmax = rng.integers(0, n_ref * num_rot, n).astype('i4')
+    ph = _photons(ds)
+    ms = MStep(ph, size)
+    ms.frame_params_from_rmax(torch.from_numpy(rmax).cuda(), num_rot, n_ref)
+    rot = torch.from_numpy(geometry.phaser_rotation_table(np.arange(num_rot) * np.pi / num_rot)).cuda()
+    got = ms.histogram(n_ref, rot).clone()
+    want = torch.zeros_like(got)
+    check(ms.lib.rspi_maxlp_histogram(
+        ptr(ph.ones), ptr(ph.multi), ptr(ph.ones_accum), ptr(ph.multi_accum), ptr(ph.place_ones),
+        ptr(ph.place_multi), ptr(ph.count_multi), ph.num_data, ptr(ms.fstate), ptr(ms.frot),
+        ptr(rot), size, ptr(ms.mask_idx), ms.n_hist_rows, n_ref, ptr(want), ptr(ph.err.t),
+        cur_stream()), 'hist')
+    torch.cuda.synchronize()
+    ph.err.check('histogram')
+    assert ms._pixel_map is not None   # the map path ran
+    assert torch.equal(got, want)
+    hist = got.cpu().numpy().reshape(ms.n_hist_rows, n_ref)
+    kmat = E.sparse_frames(ds)
+    qx, qy, _, mask, rmask = M.get_qvals(size)
+    ang = (rmax % num_rot) * np.pi / num_rot
+    fstate = rmax // num_rot
+    rows = np.flatnonzero(mask | rmask)
+    for m in range(0, rows.size, 7):
+        k = M.photons_pixel(kmat, ang, int(rows[m]), size, qx, qy)
+        want_m = np.bincount(fstate, weights=k, minlength=n_ref).astype(np.int64)
+        assert np.array_equal(hist[m], want_m), rows[m]

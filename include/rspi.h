@@ -395,10 +395,10 @@ int rspi_screen_candidates_noalloc(const float *ll, long long n_rows, long long 
  * frames in another order: column c holds frame frame_of_col[c] (-1: none);
  * the outputs are per frame as in rspi_screen_candidates.  With cand_slot
  * (n_data * 32 ints of scratch) the matrix is read once: the counting pass
- * records each thread's candidate row when it has one, a compaction writes
- * those frames' lists, and only frames where one thread (rows r = t mod 32)
- * met two or more candidates are scanned again -- the same lists in the
- * same order as without it. */
+ * records each thread's candidate rows when it has one or two, a compaction
+ * writes those frames' lists, and only frames where one thread (rows
+ * r = t mod 32) met three or more candidates are scanned again -- the same
+ * lists in the same order as without it. */
 int rspi_screen_candidates_cols(const float *ll, long long n_rows, long long n_cols,
                                 const int *frame_of_col, long long n_data, const double *max32,
                                 const int *rmax32, const long long *frame_photons,

@@ -152,6 +152,14 @@ __device__ __forceinline__ double frame_eps(long long phot, long long rows, floa
     return U32 * ((double)(rows + 8) * sum_abs + fabs(maxll) + delta + 1.) + 1e-9 * sum_abs;
 }
 
+// cnt_part[d * RY + t]: thread t's candidate count of frame d, with its
+// second candidate's row when it has two: low 2 bits min(count, 3), above
+// them the count (3 or more) or the second row's step k (row t + RY k).
+__device__ __forceinline__ int cnt_pack(int c, int k2) {
+    return c <= 2 ? (c | (k2 << 2)) : (3 | (c << 2));
+}
+__device__ __forceinline__ int cnt_count(int v) { return (v & 3) < 3 ? (v & 3) : (v >> 2); }
+
 __global__ void __launch_bounds__(32 * RY)
 k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_x, long long stride,
              const int *__restrict__ frame_of_col,
@@ -168,7 +176,7 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_x, long
     // unless the columns are a permutation of the frames)
     const long long x = (long long)blockIdx.x * 32 + tx;
     const long long d = x >= n_x ? -1 : (frame_of_col ? (long long)frame_of_col[x] : x);
-    int c = 0, first = -1;
+    int c = 0, first = -1, second = 0;
     double nc = 0.;
     if (d >= 0) {
         const double m = max32[d];
@@ -185,7 +193,9 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_x, long
             for (int u = 0; u < 8; ++u) {
                 const double v = (double)v8[u];
                 if (v >= thr || r + u * RY == rm) {
-                    if (c++ == 0) first = (int)(r + u * RY);
+                    if (c == 0) first = (int)(r + u * RY);
+                    else if (c == 1) second = (int)(r + u * RY);
+                    ++c;
                 } else {
                     nc += (double)expf((float)(v - m));   // each term < exp(-delta)
                 }
@@ -194,14 +204,16 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_x, long
         for (; r < n_rows; r += RY) {
             const double v = (double)ll[r * stride + x];
             if (v >= thr || r == rm) {
-                if (c++ == 0) first = (int)r;
+                if (c == 0) first = (int)r;
+                else if (c == 1) second = (int)r;
+                ++c;
             } else {
                 nc += (double)expf((float)(v - m));   // each term < exp(-delta)
             }
         }
-        cnt_part[d * RY + ty] = c;
-        // the thread's candidate row when it has exactly one (-2: more)
-        if (cand_slot) cand_slot[d * RY + ty] = c > 1 ? -2 : first;
+        cnt_part[d * RY + ty] = cnt_pack(c, c == 2 ? (second - ty) / RY : 0);
+        // the thread's first candidate row when it has one or two (-2: more)
+        if (cand_slot) cand_slot[d * RY + ty] = c > 2 ? -2 : first;
         if (ty == 0) thr_out[d] = thr;
     }
     sc[ty][tx] = c;
@@ -230,8 +242,8 @@ k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_x, long 
     const long long x = (long long)blockIdx.x * 32 + tx;
     const long long d = x >= n_x ? -1 : (frame_of_col ? (long long)frame_of_col[x] : x);
     if (cand_slot) {
-        // only frames in which some thread had two or more candidates are
-        // filled here (k_cand_compact took the others)
+        // only frames in which some thread had three or more candidates
+        // are filled here (k_cand_compact took the others)
         __shared__ int over[32];
         if (ty == 0) over[tx] = 0;
         __syncthreads();
@@ -241,7 +253,7 @@ k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_x, long 
     }
     if (d < 0) return;
     long long pos = cand_off[d];
-    for (int k = 0; k < ty; ++k) pos += cnt_part[d * RY + k];
+    for (int k = 0; k < ty; ++k) pos += cnt_count(cnt_part[d * RY + k]);
     const double th = thr[d];
     const int rm = rmax32[d];
     auto take = [&](float v, long long r) {
@@ -267,8 +279,8 @@ k_cand_fill(const float *__restrict__ ll, long long n_rows, long long n_x, long 
     for (; r < n_rows; r += RY) take(ll[r * stride + x], r);
 }
 
-// One warp per frame whose threads of k_cand_count each found at most one
-// candidate: the recorded rows written in the order k_cand_fill writes them
+// One warp per frame whose threads of k_cand_count each found at most two
+// candidates: the recorded rows written in the order k_cand_fill writes them
 // (thread ty's rows, ty ascending), so both paths give the same list.
 __global__ void k_cand_compact(const int *__restrict__ cand_slot, const int *__restrict__ cnt_part,
                                const long long *__restrict__ cand_off, long long n_data,
@@ -280,18 +292,19 @@ __global__ void k_cand_compact(const int *__restrict__ cand_slot, const int *__r
     for (long long d = warp; d < n_data; d += nwarp) {
         const int slot = cand_slot[d * RY + lane];
         if (__any_sync(RSPI_FULL_MASK, slot == -2)) continue;   // k_cand_fill's frame
-        const int c = cnt_part[d * RY + lane];
+        const int v = cnt_part[d * RY + lane];
+        const int c = cnt_count(v);
         int pre = c;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const int v = __shfl_up_sync(RSPI_FULL_MASK, pre, o);
-            if (lane >= o) pre += v;
+            const int u = __shfl_up_sync(RSPI_FULL_MASK, pre, o);
+            if (lane >= o) pre += u;
         }
-        if (c == 1) {
-            const long long pos = cand_off[d] + pre - 1;
+        for (int k = 0; k < c; ++k) {
+            const long long pos = cand_off[d] + pre - c + k;
             if (pos < capacity) {
                 cand_d[pos] = (int)d;
-                cand_r[pos] = slot;
+                cand_r[pos] = k == 0 ? slot : lane + RY * (v >> 2);
             } else {
                 rspi_flag(err, RSPI_ERR_CAPACITY);
             }

@@ -612,8 +612,8 @@ def test_sets_fused_frame_maximum():
 @pytest.mark.parametrize('delta', [0., 20., 400.])
 def test_one_pass_candidates_equal_two_pass(delta):
     """The one-pass candidate selection (counting pass records each thread's
-    single candidate, compaction, a second scan only for frames where a
-    thread met several) gives the two-pass lists, in the same order, for
+    first two candidates, compaction, a second scan only for frames where a
+    thread met more) gives the two-pass lists, in the same order, for
     windows from the argmax alone to hundreds of candidates per frame."""
     from rspi.device import cur_stream, ptr
     from rspi.lib import call
@@ -642,8 +642,9 @@ def test_one_pass_candidates_equal_two_pass(delta):
     off, cd, _ = outs[0]
     assert np.array_equal(cd, np.repeat(np.arange(n), np.diff(off)))
     if delta >= 20.:
-        # some frames took the second scan
-        assert (np.diff(outs[0][0]) > 32).any() or delta == 20.
+        # some frames took the second scan (more than 64 candidates: some
+        # thread met three or more)
+        assert (np.diff(outs[0][0]) > 64).any() or delta == 20.
 
 
 @pytest.mark.parametrize('name,ds,need_scaling', CASES, ids=[c[0] for c in CASES])

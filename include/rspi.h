@@ -299,10 +299,10 @@ int rspi_sets_fill(const unsigned short *entries16, const long long *row_off16, 
  * holo_quads32 given (rspi_holo_quads32: per pixel i of every state the four
  * bilinear corners W[i], W[i + 1], W[i + size], W[i + size + 1] in FP32,
  * 16-byte aligned, 4 * n_states0 * size^2 floats): the interpolation and
- * the log in FP32, |L32 - L| <= 2^-24 (10 + 2 |L|), with values at or below
- * 2e-20 (and the in-detector test) in FP64 so the -1000 sentinel falls
- * where the reference's does; the caller's candidate threshold must cover
- * the extra error (rows + 12 with abs_max >= 1). */
+ * the log in FP32 (lg2.approx times ln 2), |L32 - L| <= 2^-24 (16 + 7 |L|),
+ * with values at or below 2e-20 (and the in-detector test) in FP64 so the
+ * -1000 sentinel falls where the reference's does; the caller's candidate
+ * threshold must cover the extra error (rows + 23 with abs_max >= 1). */
 int rspi_holo_quads32(const double *holo, long long n_states0, long long size,
                       float *holo_quads32, cudaStream_t stream);
 int rspi_rot_log_slices_sets(const double *holo_pairs, const float *holo_quads32,

@@ -219,13 +219,23 @@ k_rot_log_js(const double *__restrict__ holo, const double2 *__restrict__ hp, in
 // k_rot_log_sets computes them in FP64 from the paired copy.
 // k_rot_log_sets32 computes the value of each (state, rotation) in FP32
 // from an FP32 copy of the four corners: bilinear interpolation of positive
-// terms (|relative error| <= 9 * 2^-24: the FP32 roundings of W, the
-// weights and bg, four products and four sums) and logf (at most 1 ulp,
-// CUDA's documented bound), so |L32 - L| <= 2^-24 (10 + 2 |L|); the rotated
-// positions, floors and the in-detector test stay FP64, and an
+// terms (|relative error| <= 9u, u = 2^-24: the FP32 roundings of W, the
+// weights and bg, four products and four sums), then ln t = ln2 lg2(t)
+// with lg2.approx.f32 (|error| <= 2^-21 + 2^-22 |lg2|, checked over every
+// float of [2^-100, 2^100] by rspi_log2_error_max) and one FP32 product
+// by the float nearest ln 2 (2u relative with its own rounding):
+// |L32 - L| <= u (9.1 + 8 ln2 + (4 + 2.1) |L|) <= 2^-24 (16 + 7 |L|).  The
+// rotated positions, floors and the in-detector test stay FP64, and an
 // interpolated value at or below 2e-20 (or above 1e30) is computed in FP64
 // instead, so the -1000 sentinel is taken exactly where the reference takes
 // it.
+
+// ln t as ln2 * lg2.approx(t) for a normal positive t (the bound above).
+__device__ __forceinline__ float ln_fast(float t) {
+    float l;
+    asm("lg2.approx.f32 %0, %1;" : "=f"(l) : "f"(t));
+    return __fmul_rn(0x1.62e430p-1f, l);
+}
 
 // FP64 value of one (state, rotation, column) for the FP32 path's rare
 // fallback: the operations of the FP64 path (and of rot_log_value), the
@@ -330,7 +340,7 @@ k_rot_log_sets32(const double2 *__restrict__ hp, const float4 *__restrict__ hq, 
                     t += bf;
                     const bool in = (inmask >> q) & 1u;
                     const bool ok = t > 2.e-20f && t < 1.e30f;
-                    v[q] = !real ? 0.f : !in ? -1000.f : ok ? logf(t) : 0.f;
+                    v[q] = !real ? 0.f : !in ? -1000.f : ok ? ln_fast(t) : 0.f;
                     slow |= (unsigned)(real && in && !ok) << q;
                 }
                 if (slow) {

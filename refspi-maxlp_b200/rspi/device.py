@@ -631,7 +631,7 @@ class EStep:
             if self.wide is not None:
                 rows = torch.maximum(rows, self.wide['frame_groups'].to(_i64))
             if self.slice_math == 'fp32':
-                rows = rows + 12
+                rows = rows + 23
             self.row_off_eps = torch.cat([torch.zeros(1, dtype=_i64, device=self.device),
                                           torch.cumsum(rows, 0)])
             self._eps_key = key
@@ -675,8 +675,8 @@ class EStep:
             call('rspi_holo_pairs', ptr(self.holo), self.n_states0, self.size,
                  ptr(self.holo_pairs), s)
         if self.form != 'fp64':
-            # FP32 slice arithmetic: its per-value error bound 2^-24 (10 + 2|L|)
-            # is charged as 12 more summation steps of max(|L|, 1)
+            # FP32 slice arithmetic: its per-value error bound 2^-24 (16 + 7|L|)
+            # is charged as 23 more summation steps of max(|L|, 1)
             self.lmax.fill_(1. if self.slice_math == 'fp32' else 0.)
         if self.holo_quads32 is not None:
             call('rspi_holo_quads32', ptr(self.holo), self.n_states0, self.size,

@@ -183,6 +183,23 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_x, long
         const long long rows = row_off16[d + 1] - row_off16[d];
         const double thr = m - delta - 2. * frame_eps(phot[d], rows, *lmax, m, delta);
         const int rm = rmax32[d];
+        // FP32 forms of the test and the term, the same decisions and bits:
+        // v >= thr32 exactly when (double)v >= thr (thr32 the least float
+        // not below thr), and m is a float value (the FP32 matrix's
+        // maximum), so v - m in FP32 is the double difference rounded to
+        // float whenever exp of it is not zero
+        float thr32 = (float)thr;
+        if ((double)thr32 < thr) thr32 = nextafterf(thr32, INFINITY);
+        const float m32 = (float)m;
+        auto take = [&](float v, long long rr) {
+            if (v >= thr32 || rr == rm) {
+                if (c == 0) first = (int)rr;
+                else if (c == 1) second = (int)rr;
+                ++c;
+            } else {
+                nc += (double)expf(v - m32);   // each term < exp(-delta)
+            }
+        };
         // eight rows' loads in flight per thread, taken in row order
         long long r = ty;
         for (; r + 7 * RY < n_rows; r += 8 * RY) {
@@ -190,27 +207,9 @@ k_cand_count(const float *__restrict__ ll, long long n_rows, long long n_x, long
 #pragma unroll
             for (int u = 0; u < 8; ++u) v8[u] = __ldg(&ll[(r + u * RY) * stride + x]);
 #pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const double v = (double)v8[u];
-                if (v >= thr || r + u * RY == rm) {
-                    if (c == 0) first = (int)(r + u * RY);
-                    else if (c == 1) second = (int)(r + u * RY);
-                    ++c;
-                } else {
-                    nc += (double)expf((float)(v - m));   // each term < exp(-delta)
-                }
-            }
+            for (int u = 0; u < 8; ++u) take(v8[u], r + u * RY);
         }
-        for (; r < n_rows; r += RY) {
-            const double v = (double)ll[r * stride + x];
-            if (v >= thr || r == rm) {
-                if (c == 0) first = (int)r;
-                else if (c == 1) second = (int)r;
-                ++c;
-            } else {
-                nc += (double)expf((float)(v - m));   // each term < exp(-delta)
-            }
-        }
+        for (; r < n_rows; r += RY) take(ll[r * stride + x], r);
         cnt_part[d * RY + ty] = cnt_pack(c, c == 2 ? (second - ty) / RY : 0);
         // the thread's first candidate row when it has one or two (-2: more)
         if (cand_slot) cand_slot[d * RY + ty] = c > 2 ? -2 : first;

@@ -373,8 +373,8 @@ constexpr double LG2_EA = 0x1p-21;
 constexpr double LG2_ER = 0x1p-22;
 constexpr double U32 = 0x1p-24;                    // FP32 unit roundoff
 constexpr double LN2 = 0x1.62e42fefa39efp-1;       // the double nearest ln 2
-constexpr int PT_CHUNK = 16;                       // FP32 terms per FP64 add
-constexpr double G_CHUNK = 16.01 * U32;            // gamma_16 (+ the FP64 adds)
+constexpr int PT_CHUNK = 32;                       // FP32 terms per FP64 add
+constexpr double G_CHUNK = 32.01 * U32;            // gamma_32 (+ the FP64 adds)
 constexpr int NPART = 4;                           // partial sums per candidate
 static_assert(NPART == 4, "combine4 and sum_partials take four partial sums");
 constexpr int FIN_SPLIT = PT_THREADS / NPART;      // up to here: NPART threads each
@@ -452,8 +452,8 @@ __device__ __forceinline__ void screen_term(float2 xh, float2 xl, const float4 r
 //   re, im from hi + lo parts: error <= 2u |re| + 6 u^2 A, so while
 //   |f_c + r|^2 >= max(2^-24 A^2, 2^-100) (checked through the minimum g):
 //   |ln g32 - ln g| <= 6.5 u, i.e. 9.5 u in log2;
-//   lg2: LG2_EA + LG2_ER |l|; chunk sums: gamma_16 sum k |l|.
-//   E_c = ln2 (K (LG2_EA + 9.5u) + (LG2_ER + g16)(1 + g16) sum k|l|) / n
+//   lg2: LG2_EA + LG2_ER |l|; chunk sums: gamma_32 sum k |l|.
+//   E_c = ln2 (K (LG2_EA + 9.5u) + (LG2_ER + g32)(1 + g32) sum k|l|) / n
 //         + 2^-40 (FP64 rounding of both evaluations).
 template <bool SCREEN>
 __global__ void __launch_bounds__(PT_THREADS, 2)

@@ -333,12 +333,13 @@ __global__ void k_row_scatter(const int *__restrict__ cand_r, const long long *_
 }
 
 // A "direct" row: at most DIRECT_MAX candidates whose entry slots together
-// read no more values than the row holds.  Its candidates are evaluated by
+// read no more values than the row holds (16 measured faster than 4 at the
+// argmax-only window of a 185^2 detector).  Its candidates are evaluated by
 // k_rescore_direct, one warp per candidate anywhere on the GPU, each value
 // computed with rot_log_value where the sum reads it; k_rescore_rows skips
 // the row.  (With about one candidate per row, the argmax-only window's
 // usual case, a CTA per row kept one warp of the SM busy.)
-constexpr int DIRECT_MAX = 4;
+constexpr int DIRECT_MAX = 16;
 
 __device__ __forceinline__ bool row_direct(long long r, const long long *__restrict__ row_off,
                                            const int *__restrict__ row_cand,
